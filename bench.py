@@ -1,0 +1,340 @@
+"""Benchmark: D3Q27 K17 + esoteric-twist time step, Taylor-Green vortex 256^3 periodic, FP64.
+
+One "step" is one LBM time step over the whole 256^3 box (16.78 M fluid nodes). Metric: MLUPS
+(million fluid-node updates per second, whole job). The population array (3.62 GB in FP64) is
+far larger than the 126 MB L2, so no L2 flush is needed between steps.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank advances its own independent 256^3 box (replicas: the
+single-domain hot path has no data-path collective), timing is max over ranks, value = all
+ranks' node updates / that time ("scaling": "weak").
+
+The JSON line also carries:
+  roofline     : achieved HBM bytes/s of the collision kernel (432 B algorithmic per node update
+                 in FP64: 27 reads + 27 writes of 8 B) over its CUDA-event launch time, against the
+                 measured copy bandwidth of MEASURED_PEAKS.json
+  e2e          : the same metric through the public API with host buffers (pinned): initial
+                 fields host->device, the steps with the per-step FP64 kinetic energy read back to
+                 the host, final fields device->host, all inside the timed region
+  cpu_baseline : the reference's K17 header (oracle/_ref) driven over the same layout on this
+                 box's host cores, on a bounded sample of the workload
+  forms        : MLUPS of the FP32, FP16 and BF16 shifted-population storage forms
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_SIDE = 256
+U0 = 0.04
+RE = 1600.0
+BYTES_PER_NODE = {"f64": 432, "f32": 216, "f16": 108, "bf16": 108}
+METRIC = "MLUPS (TGV 256^3 D3Q27 K17, FP64)"
+
+
+def tgv_fields(n, u0, dtype=np.float64):
+    x = (np.arange(n) + 0.5) / n * 2 * np.pi - np.pi
+    Z, Y, X = np.meshgrid(x, x, x, indexing="ij")
+    rho = 3.0 * (u0 * u0 / 16.0) * (np.cos(2 * X) + np.cos(2 * Y)) * (np.cos(2 * Z) + 2.0)
+    ux = u0 * np.sin(X) * np.cos(Y) * np.cos(Z)
+    uy = -u0 * np.cos(X) * np.sin(Y) * np.cos(Z)
+    return [a.reshape(-1).astype(dtype) for a in (rho, ux, uy, np.zeros_like(ux))]
+
+
+def omega_tgv(n):
+    nu = U0 * n / (2 * np.pi * RE)
+    return 1.0 / (3.0 * nu + 0.5)
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                rows.append((float(parts[0]), float(parts[1]), parts[3:7]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() in ("active", "1")})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline(seconds=12.0, threads=None):
+    """The reference K17 header (oracle/_ref) over the ET layout, all host cores, bounded sample:
+    a 64^3 periodic TGV box, as many whole steps as fit in about `seconds`."""
+    from oracle import pyoracle
+    from virtualfluids_b200.grid import ListGrid
+    threads = threads or os.cpu_count()
+    n = 64
+    g = ListGrid(n, n, n, periodic=(True, True, True))
+    lv = pyoracle.OracleLevel(g, omega=omega_tgv(N_SIDE))
+    lv.init(*(np.concatenate([[0.0], a]) for a in tgv_fields(n, U0)))
+    ref = pyoracle.ref64()
+    kind = "reference" if ref is not None else "port"
+    nb = lv.nb
+    lim = np.full(3, 0.01)
+    steps, t0, even = 0, time.perf_counter(), 1
+    while True:
+        if ref is not None:
+            ref.ref_collision_sweep_f64(pyoracle.ptr(lv.f), lv.n, *(pyoracle.ptr(a) for a in nb), pyoracle.ptr(lv.fluid),
+                                        lv.fluid.size, even, lv.omega, pyoracle.ptr(lim), threads)
+        else:
+            pyoracle.lib().orc_collision(C.byref(lv.L), pyoracle.ptr(lv.fluid), lv.fluid.size, even, lv.omega,
+                                         pyoracle.ptr(lim), pyoracle.ptr(np.zeros(3)), 0, None, None, None, None,
+                                         threads)
+        even = 1 - even
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds and steps >= 2:
+            break
+    mlups = g.fluid.size * steps / el / 1e6
+    return {"value": round(mlups, 2), "unit": "MLUPS", "cores": threads, "kind": kind,
+            "sample": f"{steps} steps of TGV {n}^3 periodic (K17 FP64, reference header for the collision, "
+                      f"esoteric-twist layout), {el:.1f} s"}
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    cb = cpu_baseline(seconds=max(2.0, 3.0 * args.steps / 100.0))
+    line = {"metric": METRIC, "value": cb["value"], "unit": "MLUPS", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "Taylor-Green vortex periodic D3Q27 K17 (reference CPU path, bounded sample)",
+                       "nodes_per_step": 64 ** 3},
+            "impl": "reference", "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_SIDE)
+    ap.add_argument("--no-forms", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+
+    import virtualfluids_b200 as vfb
+    from virtualfluids_b200 import _native as N
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    n = args.n
+    nodes = n ** 3
+    omega = omega_tgv(n)
+    stream = torch.cuda.Stream(device=dev)
+    sp = C.c_void_p(stream.cuda_stream)
+    fields = tgv_fields(n, U0)
+
+    def barrier():
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not pg:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident throughput: K steps with the per-step FP64 energy kept on the device ----
+    box = vfb.Box(n, n, n, omega, storage="f64")
+    box.init(*(torch.from_numpy(a).to(dev) for a in fields), stream=sp)
+    energy = torch.zeros(2 * max(args.steps, args.warmup), dtype=torch.float64, device=dev)
+    box.step(args.warmup, energy=energy, stream=sp)
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            box.step(args.steps, energy=energy, stream=sp)
+            ev1.record(stream)
+        stream.synchronize()
+    barrier()
+    t_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    value = nodes * args.steps * world / (t_ms / 1e3) / 1e6
+    clocks = clk.summary()
+
+    # ---- the collision kernel alone: average launch time for the roofline ----
+    kb = min(args.steps, 200)
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        box.step(kb, stream=sp)
+        ev1.record(stream)
+    stream.synchronize()
+    k_ms = ev0.elapsed_time(ev1) / kb
+    peak, peak_kind = measured_peak()
+    achieved = BYTES_PER_NODE["f64"] * nodes / (k_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": None,
+                "kernel": "k17_box_kernel<double> (collision + ET streaming)", "kernel_ms": round(k_ms, 4),
+                "algorithmic_bytes_per_launch": BYTES_PER_NODE["f64"] * nodes}
+    e_host = energy[: 2 * args.steps].cpu().numpy()
+    del box
+    torch.cuda.empty_cache()
+
+    # ---- end to end through the public API with pinned host buffers ----
+    host_in = [torch.from_numpy(a).pin_memory() for a in fields]
+    host_out = [torch.empty(nodes, dtype=torch.float64).pin_memory() for _ in range(4)]
+    host_energy = torch.zeros(2 * args.steps, dtype=torch.float64).pin_memory()
+    box = vfb.Box(n, n, n, omega, storage="f64")
+    lib = N.lib()
+    # warm-up of the same path
+    N.check(lib.vfb_box_init(box._h, *(C.c_void_p(h.data_ptr()) for h in host_in), 1, sp))
+    N.check(lib.vfb_box_step(box._h, args.warmup, C.c_void_p(host_energy.data_ptr()), 1, sp))
+    stream.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    with torch.cuda.stream(stream):
+        ev0.record(stream)
+        N.check(lib.vfb_box_init(box._h, *(C.c_void_p(h.data_ptr()) for h in host_in), 1, sp))
+        N.check(lib.vfb_box_step(box._h, args.steps, C.c_void_p(host_energy.data_ptr()), 1, sp))
+        N.check(lib.vfb_box_fields(box._h, *(C.c_void_p(h.data_ptr()) for h in host_out), 1, sp))
+        ev1.record(stream)
+    stream.synchronize()
+    wall_e2e = time.perf_counter() - t0
+    barrier()
+    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    e2e_value = nodes * args.steps * world / (e2e_ms / 1e3) / 1e6
+    h2d = 4 * nodes * 8
+    d2h = 4 * nodes * 8 + 16 * args.steps
+    ek = host_energy.numpy()[1::2]
+    assert np.all(np.isfinite(host_out[1].numpy())) and ek[-1] < ek[0], "e2e run produced no decaying vortex"
+    del box
+    torch.cuda.empty_cache()
+
+    # ---- other storage forms (device resident) ----
+    forms = {}
+    if not args.no_forms:
+        for st in ("f32", "f16", "bf16"):
+            b = vfb.Box(n, n, n, omega, storage=st)
+            b.init(*(torch.from_numpy(a.astype(np.float32)).to(dev) for a in fields), stream=sp)
+            b.step(args.warmup, stream=sp)
+            ks = min(args.steps, 200)
+            with torch.cuda.stream(stream):
+                ev0.record(stream)
+                b.step(ks, stream=sp)
+                ev1.record(stream)
+            stream.synchronize()
+            ms = ev0.elapsed_time(ev1) / ks
+            forms[st] = {"mlups": round(nodes / (ms / 1e3) / 1e6, 1),
+                         "hbm_gbs": round(BYTES_PER_NODE[st] * nodes / (ms / 1e3) / 1e9, 1)}
+            del b
+            torch.cuda.empty_cache()
+
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cb = cpu_baseline()
+
+    if rank == 0:
+        launches = 2 * args.steps  # one collision + one energy reduction per timed step
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(t_ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"Taylor-Green vortex {n}^3 periodic, u0={U0}, Re={int(RE)}, D3Q27 K17 cumulant + "
+                                   f"esoteric-twist streaming, FP64, per-step FP64 kinetic energy",
+                       "nodes_per_gpu": nodes, "omega": omega, "replicas": world,
+                       "l2": "inputs larger than L2 (3.62 GB populations per GPU), no flush"},
+            "roofline": roofline,
+            "e2e": {"value": round(e2e_value, 1), "unit": "MLUPS", "h2d_bytes_per_step": h2d // args.steps,
+                    "d2h_bytes_per_step": d2h // args.steps, "wall_s": round(wall_e2e, 3)},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "forms": forms,
+            "kinetic_energy": {"first": float(e_host[1]), "last": float(e_host[-1])},
+        }
+        if cb:
+            line["cpu_baseline"] = cb
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,240 @@
+/*
+ * vfb.h — C ABI of the B200-native VirtualFluids GPU time-step hot path.
+ *
+ * Plain C: pointers, sizes and status codes; no exceptions and no C++ or torch types cross
+ * this boundary. Every entry point returns a vfb_status; vfb_last_error() gives a message for the
+ * calling thread. CUDA launches are asynchronous on the given stream (NULL = legacy stream);
+ * launch-configuration errors are reported at once, execution errors at the next synchronising
+ * call (vfb_synchronize, a reduction, a copy to the host).
+ *
+ * Two layers:
+ *  (1) Reference-layout entry points that take caller-owned device memory laid out as the
+ *      reference's LBMSimulationParameter (src/gpu/core/Parameter/Parameter.h:66-330): one
+ *      population array of 27*numberOfNodes, neighborX/Y/Z index lists, dummy node 0, BC node
+ *      lists with SoA q27 arrays. Each replaces one reference launcher (cited at the
+ *      declaration) and allocates nothing.
+ *  (2) Library-owned objects: a step driver with the reference's kernel/BC/scaling factory
+ *      semantics (vfb_simulation_*), and structured boxes (vfb_box_*) for full-box domains with
+ *      arithmetic neighbours, runtime storage formats and a fused FP64 energy reduction.
+ *
+ * "real" arrays (q27, boundary velocities, rhoBC, macroscopic outputs) are double when the
+ * level's storage is VFB_STORAGE_F64 and float for every other storage format, as the
+ * reference's `real` is double or float (src/basics/DataTypes.h:39-43).
+ */
+#ifndef VFB_H
+#define VFB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VFB_ABI_VERSION 1
+
+typedef enum vfb_status {
+    VFB_OK = 0,
+    VFB_ERR_INVALID_ARGUMENT = 1,
+    VFB_ERR_UNKNOWN_KERNEL = 2,   /* KernelFactoryImp::makeKernel throws (KernelFactoryImp.cpp:92-139) */
+    VFB_ERR_BC_UNSET = 3,         /* BoundaryConditionKernelManager ctor throws (BoundaryConditionKernelManager.cpp:67-80) */
+    VFB_ERR_SCALING_UNSET = 4,    /* GridScalingKernelManager ctor throws (GridScalingKernelManager.cpp:45-62) */
+    VFB_ERR_CUDA = 5,
+    VFB_ERR_OUT_OF_MEMORY = 6,
+    VFB_ERR_UNSUPPORTED = 7,      /* a variant the reference has that this build does not implement */
+    VFB_ERR_WATCHDOG = 8          /* non-finite populations or mass drift detected */
+} vfb_status;
+
+/* population storage (runtime choice; the reference fixes it at compile time) */
+typedef enum vfb_storage {
+    VFB_STORAGE_F64 = 0,   /* f - w in double, arithmetic in double */
+    VFB_STORAGE_F32 = 1,   /* f - w in float, arithmetic in float */
+    VFB_STORAGE_F16 = 2,   /* (f - w)/w in IEEE half, arithmetic in float */
+    VFB_STORAGE_BF16 = 3   /* (f - w)/w in bfloat16, arithmetic in float */
+} vfb_storage;
+
+/* rounding mode of the arithmetic */
+typedef enum vfb_arith {
+    VFB_ARITH_FAST = 0,    /* products contracted into FMAs (default) */
+    VFB_ARITH_EXACT = 1    /* every operation rounded separately, as the reference built without FMA */
+} vfb_arith;
+
+/* CollisionTemplate (src/gpu/core/Calculation/Calculation.h:55-67) */
+typedef enum vfb_collision_template {
+    VFB_COLLISION_DEFAULT = 0,
+    VFB_COLLISION_WRITE_MACRO_VARS = 1,
+    VFB_COLLISION_APPLY_BODY_FORCE = 2,
+    VFB_COLLISION_ALL_FEATURES = 3,
+    VFB_COLLISION_SUBDOMAIN_BORDER = 4
+} vfb_collision_template;
+
+/* D3Q27 directions used as outlet normals (src/lbm/constants/D3Q27.h:42-48) */
+enum { VFB_DIR_P00 = 1, VFB_DIR_M00 = 2, VFB_DIR_0P0 = 3, VFB_DIR_0M0 = 4, VFB_DIR_00P = 5, VFB_DIR_00M = 6 };
+
+/* GEO node types (src/gpu/core/Calculation/Calculation.h:39-45) */
+enum { VFB_GEO_SOLID = 15, VFB_GEO_VOID = 16, VFB_GEO_FLUID = 19 };
+
+/* One refinement level: the fields of LBMSimulationParameter the hot path reads. Device pointers. */
+typedef struct vfb_level {
+    int32_t storage;                  /* vfb_storage */
+    int32_t arith;                    /* vfb_arith */
+    int32_t is_even_timestep;         /* isEvenTimestep */
+    int32_t level;                    /* refinement level: forces are scaled by 2^-level */
+    uint64_t number_of_nodes;         /* numberOfNodes, including the dummy node 0 */
+    void *distributions;              /* distributions.f[0]: 27 * number_of_nodes elements */
+    const uint32_t *neighbor_x;       /* neighborX: node at +1 in x (0 = dummy) */
+    const uint32_t *neighbor_y;
+    const uint32_t *neighbor_z;
+    const uint32_t *type_of_grid_node;/* typeOfGridNode (init and macroscopic output) */
+    double omega;                     /* omega = 1 / (3 nu + 1/2) */
+    double forces[3];                 /* Parameter forcing (getForcesDev), by value */
+    double quadric_limiters[3];       /* P, M, D (getQuadricLimitersDev), by value; reference default 0.01 */
+    void *rho;                        /* real[number_of_nodes] macroscopic outputs (drho) */
+    void *velocity_x;
+    void *velocity_y;
+    void *velocity_z;
+    void *pressure;                   /* may be NULL */
+    void *body_force_x;               /* forceX_SP etc., only for body-force collision templates */
+    void *body_force_y;
+    void *body_force_z;
+} vfb_level;
+
+/* QforBoundaryConditions (src/gpu/core/Calculation/Calculation.h:105-117). Device pointers. */
+typedef struct vfb_bc {
+    const int32_t *k;                 /* BC node indices */
+    const void *q27;                  /* real[27 * number_of_bc_nodes], q of direction d at [d * n + i]; q in [0,1] = link cut */
+    uint32_t number_of_bc_nodes;
+    const void *vx, *vy, *vz;         /* real[n] wall velocity (velocity BCs only) */
+} vfb_bc;
+
+/* QforDirectionalBoundaryCondition (Calculation.h:119-127). Device pointers. */
+typedef struct vfb_directional_bc {
+    const int32_t *k;                 /* BC node indices */
+    const int32_t *k_neighbor;        /* kN: the neighbour one node inwards */
+    const void *rho_bc;               /* real[n] prescribed drho */
+    uint32_t number_of_bc_nodes;
+    int32_t direction;                /* VFB_DIR_*: outward normal of the outlet */
+} vfb_directional_bc;
+
+/* ---- library ------------------------------------------------------------------------------ */
+int vfb_abi_version(void);
+const char *vfb_last_error(void);
+const char *vfb_status_string(int status);
+int vfb_synchronize(void *stream);
+/* D3Q27 tables as the kernels use them (for host-side checks) */
+int vfb_lattice_tables(int32_t cx[27], int32_t cy[27], int32_t cz[27], int32_t inv[27], double w[27]);
+/* the omega-only K17 relaxation rates as precomputed on the host:
+   {OxyyPxzz, OxyyMxzz, Oxyz, factorA, factorB, 1/omega - 1/2} (K17CompressibleNavierStokes.h:251-273) */
+int vfb_k17_rates(double omega, double rates[6]);
+
+/* ---- kernel registry (Kernel/KernelTypes.h:35-46, KernelFactoryImp.cpp:92-139) -------------- */
+enum { VFB_KERNEL_K17_COMPRESSIBLE_NAVIER_STOKES = 1 };
+/* name -> id; unknown names give VFB_ERR_UNKNOWN_KERNEL ("KernelFactory does not know the KernelType.") */
+int vfb_kernel_lookup(const char *name, int32_t *kernel_id);
+/* number of registered kernels and their names */
+int vfb_kernel_count(void);
+const char *vfb_kernel_name(int index);
+
+/* ---- (1) reference-layout entry points ----------------------------------------------------- */
+
+/* K17CompressibleNavierStokes<None>::runOnIndices (Kernel/Compressible/NavierStokes/K17/
+   K17CompressibleNavierStokes.cu:102-145) launching runCollision (Utilities/RunCollision.cuh:75):
+   collision + esoteric-twist streaming of the listed fluid nodes, in place. */
+int vfb_k17_run_on_indices(const vfb_level *level, const uint32_t *fluid_node_indices, uint32_t size,
+                           int32_t collision_template, void *stream);
+
+/* NoSlipBounceBack (BoundaryConditions/NoSlip/NoSlip.cu:44) */
+int vfb_noslip_bounce_back(const vfb_level *level, const vfb_bc *bc, void *stream);
+/* NoSlipInterpolatedCompressible (NoSlip/NoSlip.cu:81) */
+int vfb_noslip_interpolated_compressible(const vfb_level *level, const vfb_bc *bc, void *stream);
+/* VelocityBounceBack (BoundaryConditions/Velocity/Velocity.cu:44) */
+int vfb_velocity_bounce_back(const vfb_level *level, const vfb_bc *bc, void *stream);
+/* VelocityInterpolatedCompressible (Velocity/Velocity.cu:87) */
+int vfb_velocity_interpolated_compressible(const vfb_level *level, const vfb_bc *bc, void *stream);
+/* PressureNonEquilibriumCompressible (BoundaryConditions/Pressure/Pressure.cu:63) */
+int vfb_pressure_non_equilibrium_compressible(const vfb_level *level, const vfb_directional_bc *bc, void *stream);
+
+/* InitNavierStokesCompressible::init (PreProcessor/PreProcessorStrategy/InitNavierStokesCompressible/
+   InitNavierStokesCompressible.cu:45): equilibrium from level->rho/velocity_* for the level's
+   current parity. PreProcessorImp::init (PreProcessorImp.cpp:50-58) calls it for the odd, then
+   the even parity. */
+int vfb_init_navier_stokes_compressible(const vfb_level *level, void *stream);
+/* calculateMacroscopicQuantitiesCompressible (PostProcessor/MacroscopicQuantities.cu:194) */
+int vfb_calc_macroscopic_compressible(const vfb_level *level, void *stream);
+/* FP64 sum over the listed nodes of (1 + drho) and 0.5 (1 + drho) |u|^2, into out[2] on the host.
+   The per-block partial sums go to caller-provided device workspace of
+   vfb_mass_energy_workspace_bytes(size) bytes. Synchronises the stream. */
+size_t vfb_mass_energy_workspace_bytes(uint32_t size);
+int vfb_mass_energy(const vfb_level *level, const uint32_t *node_indices, uint32_t size, void *workspace,
+                    size_t workspace_bytes, double out[2], void *stream);
+
+/* ---- boundary-condition factory (BoundaryConditions/BoundaryConditionFactory.h:50-130) ------ */
+typedef int (*vfb_bc_fn)(const vfb_level *level, const vfb_bc *bc, void *stream);
+typedef int (*vfb_directional_bc_fn)(const vfb_level *level, const vfb_directional_bc *bc, void *stream);
+/* enum values of BoundaryConditionFactory::VelocityBC / NoSlipBC / PressureBC */
+enum { VFB_VELOCITY_BOUNCE_BACK = 0, VFB_VELOCITY_INTERPOLATED_INCOMPRESSIBLE = 1, VFB_VELOCITY_INTERPOLATED_COMPRESSIBLE = 2,
+       VFB_VELOCITY_WITH_PRESSURE_INTERPOLATED_COMPRESSIBLE = 3, VFB_VELOCITY_NOT_SPECIFIED = 4 };
+enum { VFB_NOSLIP_DELAY_BOUNCE_BACK = 0, VFB_NOSLIP_BOUNCE_BACK = 1, VFB_NOSLIP_INTERPOLATED_INCOMPRESSIBLE = 2,
+       VFB_NOSLIP_INTERPOLATED_COMPRESSIBLE = 3 };
+enum { VFB_PRESSURE_NON_EQUILIBRIUM_INCOMPRESSIBLE = 0, VFB_PRESSURE_NON_EQUILIBRIUM_COMPRESSIBLE = 1,
+       VFB_PRESSURE_OUTFLOW_NON_REFLECTIVE = 2, VFB_PRESSURE_OUTFLOW_NON_REFLECTIVE_PRESSURE_CORRECTION = 3,
+       VFB_PRESSURE_NOT_SPECIFIED = 4 };
+/* The function for an enum value. *fn = NULL with VFB_OK means "no kernel" (NoSlipDelayBounceBack,
+   whose bounce-back happens through the dummy node; NotSpecified). Variants outside this build
+   return VFB_ERR_UNSUPPORTED. */
+int vfb_bc_factory_velocity(int32_t variant, vfb_bc_fn *fn);
+int vfb_bc_factory_noslip(int32_t variant, vfb_bc_fn *fn);
+int vfb_bc_factory_pressure(int32_t variant, vfb_directional_bc_fn *fn);
+
+/* ---- (2a) step driver: UpdateGrid27::updateGrid for one level (Calculation/UpdateGrid27.cpp:54-95) */
+typedef struct vfb_simulation vfb_simulation;
+/* kernel_name as Parameter::configureMainKernel; VFB_ERR_UNKNOWN_KERNEL for unknown names */
+int vfb_simulation_create(const char *kernel_name, vfb_simulation **out);
+int vfb_simulation_destroy(vfb_simulation *sim);
+/* the level description is copied; device memory stays caller-owned */
+int vfb_simulation_set_level(vfb_simulation *sim, const vfb_level *level, const uint32_t *fluid_node_indices,
+                             uint32_t number_of_fluid_nodes);
+/* BC lists (copied descriptors) and factory choices */
+int vfb_simulation_set_velocity_bc(vfb_simulation *sim, const vfb_bc *bc, int32_t variant);
+int vfb_simulation_set_noslip_bc(vfb_simulation *sim, const vfb_bc *bc, int32_t variant);
+int vfb_simulation_add_pressure_bc(vfb_simulation *sim, const vfb_directional_bc *bc, int32_t variant);
+/* checks the BoundaryConditionKernelManager rules: a BC with nodes but no kernel is VFB_ERR_BC_UNSET */
+int vfb_simulation_check(const vfb_simulation *sim);
+/* run steps: collision, velocity then no-slip BCs, parity toggle, pressure BCs */
+int vfb_simulation_run(vfb_simulation *sim, uint32_t steps, void *stream);
+int vfb_simulation_is_even_timestep(const vfb_simulation *sim, int32_t *is_even);
+
+/* ---- (2b) structured boxes --------------------------------------------------------------- */
+/* A full box of nx*ny*nz nodes, node k = x + nx (y + ny z), neighbours by index arithmetic.
+   Non-periodic axes need a mask whose border nodes are 0 (not collided). */
+typedef struct vfb_box_desc {
+    int32_t nx, ny, nz;
+    int32_t periodic_x, periodic_y, periodic_z;
+    int32_t storage;                  /* vfb_storage */
+    int32_t arith;                    /* vfb_arith */
+    double omega;
+    double forces[3];                 /* acceleration, applied as forces * 1/2 */
+    double quadric_limiters[3];
+    const uint8_t *mask;              /* optional host mask, nonzero = fluid; NULL = every node */
+} vfb_box_desc;
+typedef struct vfb_box vfb_box;
+int vfb_box_create(const vfb_box_desc *desc, vfb_box **out);
+int vfb_box_destroy(vfb_box *box);
+/* bytes the box holds on the device */
+int vfb_box_device_bytes(const vfb_box *box, uint64_t *bytes);
+/* equilibrium initialisation from drho, ux, uy, uz (real[nx*ny*nz]); host memory when from_host,
+   else device memory. Leaves the box at an even step. */
+int vfb_box_init(vfb_box *box, const void *rho, const void *ux, const void *uy, const void *uz, int32_t from_host,
+                 void *stream);
+/* advance `steps` time steps. energy (optional): FP64 {sum(1+drho), sum(0.5 (1+drho)|u|^2)} per
+   step, 2*steps doubles, host (pinned for asynchrony) when energy_on_host, else device. */
+int vfb_box_step(vfb_box *box, uint32_t steps, double *energy, int32_t energy_on_host, void *stream);
+/* macroscopic drho, ux, uy, uz (real[nx*ny*nz]) of the current state, to host or device memory */
+int vfb_box_fields(vfb_box *box, void *rho, void *ux, void *uy, void *uz, int32_t to_host, void *stream);
+/* raw access to the population planes for checks: pointer, plane pitch (elements), parity */
+int vfb_box_populations(const vfb_box *box, void **dist, uint64_t *pitch, int32_t *is_even);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,105 @@
+/*
+ * ORACLE — test infrastructure, not product code.
+ *
+ * A plain-C CPU restatement of the VirtualFluids GPU time-step hot path (D3Q27 K17 cumulant
+ * collision with in-place esoteric-twist streaming, the no-slip / velocity / pressure boundary
+ * kernels, equilibrium initialisation, macroscopic output and the FP64 reductions). It exists
+ * only so tests, the smoke check and the benchmark's CPU-baseline leg can check the CUDA
+ * library against the reference algorithm. Nothing in the shipped library links or calls it.
+ *
+ * Data layout is the reference GPU layout (src/gpu/core/Utilities/KernelUtilities.h:66-132,
+ * src/gpu/core/Cuda/CudaMemoryManager.cpp:146-168): populations are one array of 27*n reals,
+ * direction-major (f[dir*n + k]); n counts the dummy node 0; neighborX/Y/Z[k] give the node at
+ * +1 in x/y/z (src/gpu/GridGenerator/grid/GridImp.cpp:1012-1080).
+ */
+#ifndef VFB_ORACLE_H
+#define VFB_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* D3Q27 direction numbering of src/lbm/constants/D3Q27.h:42-72 */
+enum {
+    D_000 = 0, D_P00, D_M00, D_0P0, D_0M0, D_00P, D_00M,
+    D_PP0, D_MM0, D_PM0, D_MP0, D_P0P, D_M0M, D_P0M, D_M0P,
+    D_0PP, D_0MM, D_0PM, D_0MP,
+    D_PPP, D_MPP, D_PMP, D_MMP, D_PPM, D_MPM, D_PMM, D_MMM
+};
+
+extern const int ORC_CX[27], ORC_CY[27], ORC_CZ[27], ORC_INV[27];
+extern const double ORC_W[27];
+
+/* per-node K17 (src/lbm/collision/K17CompressibleNavierStokes.h:88) */
+void orc_k17_f64(double *f, double omega, const double *lim, double fx, double fy, double fz, double *macro);
+void orc_k17_f32(float *f, float omega, const float *lim, float fx, float fy, float fz, float *macro);
+void orc_k17_rates_f64(double omega, double rates[6]);
+void orc_k17_rates_f32(float omega, float rates[6]);
+double orc_density_f64(const double *f);
+void orc_macro_compressible_f64(const double *f, double *drho, double *one_over_rho, double *vx, double *vy, double *vz);
+
+/* chimera transforms, exposed for the reference's known-answer tests */
+void orc_chimera_f64(int which, double *abc, double v, double v2, double kinv, double k);
+
+/* one refinement level in the reference layout */
+typedef struct {
+    uint64_t n;             /* numberOfNodes, including the dummy node 0 */
+    double *f;              /* distributions.f[0], 27*n */
+    const uint32_t *nbx;    /* neighborX */
+    const uint32_t *nby;    /* neighborY */
+    const uint32_t *nbz;    /* neighborZ */
+} orc_level;
+
+/* esoteric-twist addressing (KernelUtilities.h:66-132, 221-378) */
+void orc_pointer_map(int is_even, int map[27]);
+uint32_t orc_read_index(const orc_level *L, uint32_t k, int dir);
+void orc_read_pre(const orc_level *L, uint32_t k, int is_even, double out[27]);
+void orc_write_post(orc_level *L, uint32_t k, int is_even, const double in[27]);
+
+/* RunCollision.cuh:75-143 with the K17 functor; force = forces*0.5*2^-level; macros optional */
+void orc_collision(orc_level *L, const uint32_t *idx, uint32_t n_idx, int is_even, double omega,
+                   const double lim[3], const double forces[3], int level,
+                   double *rho, double *vx, double *vy, double *vz, int n_threads);
+
+/* boundary conditions, QforBoundaryConditions layout: k[nbc], q27[dir*nbc + i] */
+void orc_bc_noslip_bounce_back(orc_level *L, const int32_t *k, const double *q27, uint32_t nbc, int is_even);
+void orc_bc_noslip_interpolated(orc_level *L, const int32_t *k, const double *q27, uint32_t nbc, int is_even, double omega);
+void orc_bc_velocity_bounce_back(orc_level *L, const int32_t *k, const double *q27, uint32_t nbc, int is_even,
+                                 const double *ux, const double *uy, const double *uz);
+void orc_bc_velocity_interpolated(orc_level *L, const int32_t *k, const double *q27, uint32_t nbc, int is_even,
+                                  double omega, const double *ux, const double *uy, const double *uz);
+void orc_bc_pressure_neq(orc_level *L, const int32_t *k, const int32_t *kN, const double *rho_bc, uint32_t nbc,
+                         int is_even, int direction);
+
+/* InitNavierStokesCompressible_Device.cu:44-215 for one parity; geo: skip 15 (solid) and 16 (void) */
+void orc_init(orc_level *L, const uint32_t *geo, const double *rho, const double *ux, const double *uy,
+              const double *uz, int is_even);
+/* MacroscopicQuantities.cu:194 compressible macros (rho, vx, vy, vz, pressure) for geo == 19 nodes */
+void orc_macros(const orc_level *L, const uint32_t *geo, int is_even, double *rho, double *vx, double *vy,
+                double *vz, double *press);
+/* FP64 global mass sum(1+drho) and kinetic energy sum(0.5*(1+drho)*u^2) over a node list */
+void orc_mass_energy(const orc_level *L, const uint32_t *idx, uint32_t n_idx, int is_even, double out[2]);
+
+/* one time step of a single level in the order of UpdateGrid27::updateGrid (UpdateGrid27.cpp:54-95) */
+typedef struct {
+    int32_t *k; double *q; uint32_t n;                 /* no-slip list */
+    int kind;                                          /* 0 none, 1 bounce-back, 2 interpolated */
+} orc_noslip;
+typedef struct {
+    int32_t *k; double *q; uint32_t n; double *ux, *uy, *uz;
+    int kind;                                          /* 0 none, 1 bounce-back, 2 interpolated */
+} orc_velocity;
+typedef struct {
+    int32_t *k; int32_t *kN; double *rho; uint32_t n; int direction;
+} orc_pressure;
+
+int orc_run(orc_level *L, const uint32_t *fluid, uint32_t n_fluid, int *is_even, double omega, const double lim[3],
+            const double forces[3], const orc_velocity *vel, const orc_noslip *ns, const orc_pressure *pr, int n_pr,
+            int steps, int n_threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,185 @@
+"""ORACLE — test infrastructure, not product code.
+
+ctypes binding of the plain-C oracle (liboracle.so, built by oracle/Makefile) and of the
+reference-header pins (_ref/libvfref64.so, _ref/libvfref32.so). Only the tests, the smoke check
+and the benchmark's CPU-baseline / reference legs use this module, and only as a checker or as
+the timed CPU baseline.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+REF64 = HERE / "_ref" / "libvfref64.so"
+REF32 = HERE / "_ref" / "libvfref32.so"
+
+_P = C.c_void_p
+_lib = None
+
+
+def build(reference: str | None = None) -> None:
+    """Build liboracle.so, and the reference pins when the reference tree is present."""
+    subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
+    ref = reference or "/root/reference"
+    if Path(ref).is_dir():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={ref}"], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = C.CDLL(str(LIB))
+        d, i, u = C.c_double, C.c_int, C.c_uint32
+        L.orc_k17_f64.argtypes = [_P, d, _P, d, d, d, _P]
+        L.orc_k17_f32.argtypes = [_P, C.c_float, _P, C.c_float, C.c_float, C.c_float, _P]
+        L.orc_k17_rates_f64.argtypes = [d, _P]
+        L.orc_density_f64.argtypes = [_P]
+        L.orc_density_f64.restype = d
+        L.orc_macro_compressible_f64.argtypes = [_P, _P, _P, _P, _P, _P]
+        L.orc_chimera_f64.argtypes = [i, _P, d, d, d, d]
+        L.orc_collision.argtypes = [_P, _P, u, i, d, _P, _P, i, _P, _P, _P, _P, i]
+        L.orc_bc_noslip_bounce_back.argtypes = [_P, _P, _P, u, i]
+        L.orc_bc_noslip_interpolated.argtypes = [_P, _P, _P, u, i, d]
+        L.orc_bc_velocity_bounce_back.argtypes = [_P, _P, _P, u, i, _P, _P, _P]
+        L.orc_bc_velocity_interpolated.argtypes = [_P, _P, _P, u, i, d, _P, _P, _P]
+        L.orc_bc_pressure_neq.argtypes = [_P, _P, _P, _P, u, i, i]
+        L.orc_init.argtypes = [_P, _P, _P, _P, _P, _P, i]
+        L.orc_macros.argtypes = [_P, _P, i, _P, _P, _P, _P, _P]
+        L.orc_mass_energy.argtypes = [_P, _P, u, i, _P]
+        _lib = L
+    return _lib
+
+
+def ref64():
+    if not REF64.exists():
+        return None
+    L = C.CDLL(str(REF64))
+    d = C.c_double
+    L.ref_k17_f64.argtypes = [_P, d, _P, d, d, d, _P]
+    L.ref_chimera_f64.argtypes = [C.c_int, _P, d, d, d, d]
+    L.ref_density_f64.argtypes = [_P]
+    L.ref_density_f64.restype = d
+    L.ref_macro_compressible_f64.argtypes = [_P, _P]
+    L.ref_incompressible_velocity_f64.argtypes = [_P, _P]
+    L.ref_collision_sweep_f64.argtypes = [_P, C.c_uint64, _P, _P, _P, _P, C.c_uint32, C.c_int, d, _P, C.c_int]
+    return L
+
+
+def ref32():
+    if not REF32.exists():
+        return None
+    L = C.CDLL(str(REF32))
+    f = C.c_float
+    L.ref_k17_f32.argtypes = [_P, f, _P, f, f, f, _P]
+    return L
+
+
+def ptr(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data) if a is not None else C.c_void_p(0)
+
+
+class _Level(C.Structure):
+    _fields_ = [("n", C.c_uint64), ("f", _P), ("nbx", _P), ("nby", _P), ("nbz", _P)]
+
+
+class _NoSlip(C.Structure):
+    _fields_ = [("k", _P), ("q", _P), ("n", C.c_uint32), ("kind", C.c_int)]
+
+
+class _Velocity(C.Structure):
+    _fields_ = [("k", _P), ("q", _P), ("n", C.c_uint32), ("ux", _P), ("uy", _P), ("uz", _P), ("kind", C.c_int)]
+
+
+class _Pressure(C.Structure):
+    _fields_ = [("k", _P), ("kN", _P), ("rho", _P), ("n", C.c_uint32), ("direction", C.c_int)]
+
+
+class OracleLevel:
+    """A level in the reference layout, advanced on the host by the oracle."""
+
+    def __init__(self, grid, omega, lim=(0.01, 0.01, 0.01), forces=(0.0, 0.0, 0.0), velocity_kind=1, noslip_kind=1):
+        self.grid = grid
+        self.n = grid.number_of_nodes
+        self.f = np.zeros(27 * self.n, dtype=np.float64)
+        self.nb = [np.ascontiguousarray(grid.neighbor[a].astype(np.uint32)) for a in range(3)]
+        self.geo = np.ascontiguousarray(grid.geo.astype(np.uint32))
+        self.fluid = np.ascontiguousarray(grid.fluid.astype(np.uint32))
+        self.omega = float(omega)
+        self.lim = np.array(lim, dtype=np.float64)
+        self.forces = np.array(forces, dtype=np.float64)
+        self.is_even = C.c_int(1)
+        self.L = _Level(self.n, self.f.ctypes.data, self.nb[0].ctypes.data, self.nb[1].ctypes.data, self.nb[2].ctypes.data)
+        self._keep = []
+        self.vel = None
+        self.ns = None
+        m = grid.merged("velocity")
+        if m is not None:
+            k, q, v = m
+            arrs = [np.ascontiguousarray(k.astype(np.int32)), np.ascontiguousarray(q.reshape(-1))] + \
+                   [np.ascontiguousarray(v[a].astype(np.float64)) for a in range(3)]
+            self._keep += arrs
+            self.vel = _Velocity(arrs[0].ctypes.data, arrs[1].ctypes.data, k.size, arrs[2].ctypes.data,
+                                 arrs[3].ctypes.data, arrs[4].ctypes.data, velocity_kind)
+        m = grid.merged("noslip")
+        if m is not None:
+            k, q, _ = m
+            arrs = [np.ascontiguousarray(k.astype(np.int32)), np.ascontiguousarray(q.reshape(-1))]
+            self._keep += arrs
+            self.ns = _NoSlip(arrs[0].ctypes.data, arrs[1].ctypes.data, k.size, noslip_kind)
+        from virtualfluids_b200.grid import SIDE_DIR
+        pr = []
+        for b in grid.bcs:
+            if b.kind != "pressure":
+                continue
+            arrs = [np.ascontiguousarray(b.k.astype(np.int32)), np.ascontiguousarray(b.k_neighbor.astype(np.int32)),
+                    np.full(b.k.size, float(b.rho))]
+            self._keep += arrs
+            pr.append(_Pressure(arrs[0].ctypes.data, arrs[1].ctypes.data, arrs[2].ctypes.data, b.k.size, SIDE_DIR[b.side]))
+        self.pr = (_Pressure * max(len(pr), 1))(*pr) if pr else None
+        self.n_pr = len(pr)
+
+    def init(self, rho=None, ux=None, uy=None, uz=None):
+        z = np.zeros(self.n)
+        arrs = [np.ascontiguousarray(a if a is not None else z, dtype=np.float64) for a in (rho, ux, uy, uz)]
+        lib().orc_init(C.byref(self.L), ptr(self.geo), *(ptr(a) for a in arrs), 0)
+        lib().orc_init(C.byref(self.L), ptr(self.geo), *(ptr(a) for a in arrs), 1)
+        self.is_even.value = 1
+
+    def run(self, steps, threads=0):
+        lib().orc_run.argtypes = [_P, _P, C.c_uint32, C.POINTER(C.c_int), C.c_double, _P, _P, _P, _P, _P, C.c_int,
+                                  C.c_int, C.c_int]
+        lib().orc_run(C.byref(self.L), ptr(self.fluid), self.fluid.size, C.byref(self.is_even), self.omega,
+                      ptr(self.lim), ptr(self.forces), C.byref(self.vel) if self.vel else None,
+                      C.byref(self.ns) if self.ns else None, self.pr, self.n_pr, int(steps), int(threads))
+
+    def macroscopic(self):
+        out = [np.zeros(self.n) for _ in range(5)]
+        lib().orc_macros(C.byref(self.L), ptr(self.geo), self.is_even.value, *(ptr(a) for a in out))
+        return dict(zip(("rho", "vx", "vy", "vz", "pressure"), out))
+
+    def mass_energy(self):
+        out = np.zeros(2)
+        lib().orc_mass_energy(C.byref(self.L), ptr(self.fluid), self.fluid.size, self.is_even.value, ptr(out))
+        return float(out[0]), float(out[1])
+
+
+def k17(f, omega, lim=(0.01, 0.01, 0.01), force=(0.0, 0.0, 0.0), dtype=np.float64):
+    """One-node K17 of the oracle: returns (post-collision f, macro[4])."""
+    if dtype == np.float64:
+        a = np.ascontiguousarray(f, dtype=np.float64).copy()
+        m = np.zeros(4)
+        lib().orc_k17_f64(ptr(a), omega, ptr(np.array(lim, dtype=np.float64)), *force, ptr(m))
+    else:
+        a = np.ascontiguousarray(f, dtype=np.float32).copy()
+        m = np.zeros(4, dtype=np.float32)
+        lib().orc_k17_f32(ptr(a), np.float32(omega), ptr(np.array(lim, dtype=np.float32)), *(np.float32(x) for x in force),
+                          ptr(m))
+    return a, m

@@ -1,0 +1,158 @@
+"""The C ABI library loads, exports what include/vfb.h declares, and its host logic follows the
+reference's registry / factory / manager semantics. No kernel runs here (CPU only)."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _declared_symbols():
+    text = (ROOT / "include" / "vfb.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(vfb_[a-z0-9_]+)\s*\(", text)) - {"vfb_bc_fn", "vfb_directional_bc_fn"})
+
+
+def test_library_exports_every_declared_symbol():
+    from virtualfluids_b200 import _native as N
+    lib = N.lib()
+    declared = _declared_symbols()
+    assert len(declared) >= 30
+    missing = [s for s in declared if not hasattr(lib, s)]
+    assert not missing, missing
+    # the Python binding covers the whole header
+    assert set(declared) == set(N.SIGNATURES), set(declared) ^ set(N.SIGNATURES)
+
+
+def test_abi_version_and_status_strings():
+    from virtualfluids_b200 import _native as N
+    assert N.lib().vfb_abi_version() == 1
+    assert N.lib().vfb_status_string(N.VFB_ERR_UNKNOWN_KERNEL) == b"KernelFactory does not know the KernelType."
+
+
+def test_lattice_tables_match_oracle(oracle):
+    from virtualfluids_b200 import _native as N
+    t = [np.zeros(27, dtype=np.int32) for _ in range(4)] + [np.zeros(27)]
+    N.check(N.lib().vfb_lattice_tables(*(C.c_void_p(a.ctypes.data) for a in t)))
+    L = C.CDLL(str(oracle.LIB))
+    for name, arr in zip(("ORC_CX", "ORC_CY", "ORC_CZ", "ORC_INV"), t[:4]):
+        ref = np.frombuffer((C.c_int * 27).in_dll(L, name), dtype=np.int32)
+        assert np.array_equal(arr, ref), name
+    w = np.frombuffer((C.c_double * 27).in_dll(L, "ORC_W"), dtype=np.float64)
+    assert np.array_equal(t[4], w)
+
+
+def test_host_rates_match_oracle_bitwise(oracle):
+    """The omega-only K17 rates precomputed on the host equal the per-node reference expressions."""
+    from virtualfluids_b200 import _native as N
+    lib = oracle.lib()
+    lib.orc_k17_rates_f64.argtypes = [C.c_double, C.c_void_p]
+    for om in np.linspace(0.55, 1.99, 97):
+        a, b = np.zeros(6), np.zeros(6)
+        N.check(N.lib().vfb_k17_rates(float(om), C.c_void_p(a.ctypes.data)))
+        lib.orc_k17_rates_f64(float(om), oracle.ptr(b))
+        assert np.array_equal(a, b), om
+
+
+def test_kernel_registry():
+    from virtualfluids_b200 import _native as N
+    kid = C.c_int32()
+    N.check(N.lib().vfb_kernel_lookup(b"K17CompressibleNavierStokes", C.byref(kid)))
+    assert kid.value == 1
+    assert N.lib().vfb_kernel_lookup(b"K15CompressibleNavierStokes", C.byref(kid)) == N.VFB_ERR_UNKNOWN_KERNEL
+    assert b"KernelFactory does not know the KernelType" in N.lib().vfb_last_error()
+    assert N.lib().vfb_kernel_count() == 1
+    assert N.lib().vfb_kernel_name(0) == b"K17CompressibleNavierStokes"
+    with pytest.raises(N.VfbError):
+        from virtualfluids_b200 import Parameter
+        Parameter().configure_main_kernel("NoSuchKernel")
+
+
+def test_bc_factory_semantics():
+    """BoundaryConditionFactoryTest.cpp: defaults give no kernel; each enum maps to its function."""
+    from virtualfluids_b200 import _native as N
+    lib = N.lib()
+    fn = C.c_void_p()
+    N.check(lib.vfb_bc_factory_noslip(N.NOSLIP_DELAY_BOUNCE_BACK, C.byref(fn)))
+    assert fn.value is None
+    N.check(lib.vfb_bc_factory_noslip(N.NOSLIP_BOUNCE_BACK, C.byref(fn)))
+    assert fn.value == C.cast(lib.vfb_noslip_bounce_back, C.c_void_p).value
+    N.check(lib.vfb_bc_factory_noslip(N.NOSLIP_INTERPOLATED_COMPRESSIBLE, C.byref(fn)))
+    assert fn.value == C.cast(lib.vfb_noslip_interpolated_compressible, C.c_void_p).value
+    N.check(lib.vfb_bc_factory_velocity(N.VELOCITY_BOUNCE_BACK, C.byref(fn)))
+    assert fn.value == C.cast(lib.vfb_velocity_bounce_back, C.c_void_p).value
+    N.check(lib.vfb_bc_factory_velocity(N.VELOCITY_INTERPOLATED_COMPRESSIBLE, C.byref(fn)))
+    assert fn.value == C.cast(lib.vfb_velocity_interpolated_compressible, C.c_void_p).value
+    N.check(lib.vfb_bc_factory_velocity(N.VELOCITY_NOT_SPECIFIED, C.byref(fn)))
+    assert fn.value is None
+    N.check(lib.vfb_bc_factory_pressure(N.PRESSURE_NON_EQUILIBRIUM_COMPRESSIBLE, C.byref(fn)))
+    assert fn.value == C.cast(lib.vfb_pressure_non_equilibrium_compressible, C.c_void_p).value
+    assert lib.vfb_bc_factory_velocity(N.VELOCITY_INTERPOLATED_INCOMPRESSIBLE, C.byref(fn)) == N.VFB_ERR_UNSUPPORTED
+    assert lib.vfb_bc_factory_noslip(99, C.byref(fn)) == N.VFB_ERR_INVALID_ARGUMENT
+
+
+def _fake_level(N):
+    """A level description with placeholder device addresses: only host checks run on it."""
+    L = N.Level()
+    L.storage, L.arith, L.is_even_timestep, L.level = N.STORAGE_F64, N.ARITH_FAST, 1, 0
+    L.number_of_nodes = 10
+    L.distributions = L.neighbor_x = L.neighbor_y = L.neighbor_z = 0x1000
+    L.omega = 1.5
+    return L
+
+
+def test_simulation_manager_rules():
+    """BCKernelManagerTest.cpp: a BC with nodes but no kernel is an error; none without nodes is fine."""
+    from virtualfluids_b200 import _native as N
+    lib = N.lib()
+    sim = C.c_void_p()
+    assert lib.vfb_simulation_create(b"K15CompressibleNavierStokes", C.byref(sim)) == N.VFB_ERR_UNKNOWN_KERNEL
+    N.check(lib.vfb_simulation_create(b"K17CompressibleNavierStokes", C.byref(sim)))
+    try:
+        assert lib.vfb_simulation_check(sim) == N.VFB_ERR_INVALID_ARGUMENT  # no level yet
+        L = _fake_level(N)
+        N.check(lib.vfb_simulation_set_level(sim, C.byref(L), C.c_void_p(0x2000), 5))
+        N.check(lib.vfb_simulation_check(sim))
+        bc = N.BC(0x3000, 0x4000, 0, 0, 0, 0)
+        N.check(lib.vfb_simulation_set_velocity_bc(sim, C.byref(bc), N.VELOCITY_NOT_SPECIFIED))
+        N.check(lib.vfb_simulation_check(sim))        # no nodes, no kernel: fine
+        bc.number_of_bc_nodes = 4
+        N.check(lib.vfb_simulation_set_velocity_bc(sim, C.byref(bc), N.VELOCITY_NOT_SPECIFIED))
+        assert lib.vfb_simulation_check(sim) == N.VFB_ERR_BC_UNSET
+        N.check(lib.vfb_simulation_set_velocity_bc(sim, C.byref(bc), N.VELOCITY_BOUNCE_BACK))
+        N.check(lib.vfb_simulation_check(sim))
+        nbc = N.BC(0x3000, 0x4000, 4, 0, 0, 0)
+        N.check(lib.vfb_simulation_set_noslip_bc(sim, C.byref(nbc), N.NOSLIP_DELAY_BOUNCE_BACK))
+        N.check(lib.vfb_simulation_check(sim))        # delayed bounce-back needs no kernel
+        pbc = N.DirectionalBC(0x3000, 0x3100, 0x3200, 3, N.DIR_P00)
+        N.check(lib.vfb_simulation_add_pressure_bc(sim, C.byref(pbc), N.PRESSURE_NOT_SPECIFIED))
+        assert lib.vfb_simulation_check(sim) == N.VFB_ERR_BC_UNSET
+    finally:
+        lib.vfb_simulation_destroy(sim)
+
+
+def test_argument_validation_without_launching():
+    from virtualfluids_b200 import _native as N
+    lib = N.lib()
+    L = _fake_level(N)
+    L.omega = 2.5
+    assert lib.vfb_k17_run_on_indices(C.byref(L), C.c_void_p(0x2000), 5, 0, None) == N.VFB_ERR_INVALID_ARGUMENT
+    L.omega = 1.5
+    L.storage = N.STORAGE_F16
+    L.arith = N.ARITH_EXACT
+    assert lib.vfb_k17_run_on_indices(C.byref(L), C.c_void_p(0x2000), 5, 0, None) == N.VFB_ERR_UNSUPPORTED
+    L.arith = N.ARITH_FAST
+    assert lib.vfb_k17_run_on_indices(C.byref(L), C.c_void_p(0x2000), 5, 9, None) == N.VFB_ERR_INVALID_ARGUMENT
+    assert lib.vfb_k17_run_on_indices(C.byref(L), None, 5, 0, None) == N.VFB_ERR_INVALID_ARGUMENT
+    # a write-macro template without output arrays
+    assert lib.vfb_k17_run_on_indices(C.byref(L), C.c_void_p(0x2000), 5, 1, None) == N.VFB_ERR_INVALID_ARGUMENT
+    pbc = N.DirectionalBC(0x3000, 0x3100, 0x3200, 3, 19)
+    assert lib.vfb_pressure_non_equilibrium_compressible(C.byref(L), C.byref(pbc), None) == N.VFB_ERR_INVALID_ARGUMENT
+    d = N.BoxDesc()
+    d.nx = d.ny = d.nz = 8
+    d.storage, d.omega = N.STORAGE_F64, 1.8
+    h = C.c_void_p()
+    assert lib.vfb_box_create(C.byref(d), C.byref(h)) == N.VFB_ERR_INVALID_ARGUMENT  # walls need a mask

@@ -1,0 +1,106 @@
+"""Structured boxes (arithmetic neighbours) against the oracle and across storage formats."""
+import numpy as np
+import pytest
+
+from virtualfluids_b200 import Box, ListGrid
+from virtualfluids_b200 import _native as N
+
+pytestmark = pytest.mark.gpu
+
+
+def tgv_fields(nx, ny, nz, u0):
+    """Taylor-Green vortex on [-pi, pi]^3 as apps/gpu/TaylorGreenVortex sets it up:
+    drho = 3 (u0^2/16)(cos 2x + cos 2y)(cos 2z + 2), u = u0 sin x cos y cos z, v = -u0 cos x sin y cos z, w = 0."""
+    x = (np.arange(nx) + 0.5) / nx * 2 * np.pi - np.pi
+    y = (np.arange(ny) + 0.5) / ny * 2 * np.pi - np.pi
+    z = (np.arange(nz) + 0.5) / nz * 2 * np.pi - np.pi
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    rho = 3.0 * (u0 * u0 / 16.0) * (np.cos(2 * X) + np.cos(2 * Y)) * (np.cos(2 * Z) + 2.0)
+    ux = u0 * np.sin(X) * np.cos(Y) * np.cos(Z)
+    uy = -u0 * np.cos(X) * np.sin(Y) * np.cos(Z)
+    uz = np.zeros_like(ux)
+    return [a.reshape(-1) for a in (rho, ux, uy, uz)]
+
+
+def _oracle_tgv(oracle, n, omega, steps, u0=0.04):
+    g = ListGrid(n, n, n, periodic=(True, True, True))
+    f = tgv_fields(n, n, n, u0)
+    full = [np.concatenate([[0.0], a]) for a in f]
+    lv = oracle.OracleLevel(g, omega=omega)
+    lv.init(*full)
+    energy = []
+    for _ in range(steps):
+        lv.run(1, threads=0)
+        energy.append(lv.mass_energy())
+    m = lv.macroscopic()
+    return {k: v[1:] for k, v in m.items()}, np.array(energy), f
+
+
+@pytest.mark.parametrize("arith", ["exact", "fast"])
+def test_box_matches_oracle(oracle, cuda, arith):
+    n, omega, steps = 24, 1.9, 30
+    ref, ref_energy, f = _oracle_tgv(oracle, n, omega, steps)
+    b = Box(n, n, n, omega, storage="f64", arith=arith)
+    b.init(*f)
+    energy = np.zeros((steps, 2))
+    b.step(steps, energy=energy)
+    got = b.fields()
+    for k in ("rho", "vx", "vy", "vz"):
+        if arith == "exact":
+            assert np.array_equal(got[k], ref[k]), k
+        else:
+            scale = np.abs(ref[k]).max()
+            assert np.abs(got[k] - ref[k]).max() <= 1e-12 * scale, k
+    # fused FP64 energy reduction against the oracle's reduction of the same state (the box's value
+    # at step t comes from the pre-collision state of step t, the oracle's after step t)
+    np.testing.assert_allclose(energy[1:, 0], ref_energy[:-1, 0], rtol=1e-13)
+    np.testing.assert_allclose(energy[1:, 1], ref_energy[:-1, 1], rtol=1e-11)
+
+
+def test_box_device_inputs_and_outputs(cuda):
+    import torch
+    n = 16
+    f = tgv_fields(n, n, n, 0.04)
+    a = Box(n, n, n, 1.9)
+    a.init(*f)
+    b = Box(n, n, n, 1.9)
+    b.init(*(torch.from_numpy(x).to(cuda) for x in f))
+    a.step(10)
+    e = torch.zeros(20, dtype=torch.float64, device=cuda)
+    b.step(10, energy=e)
+    out = [torch.empty(n ** 3, dtype=torch.float64, device=cuda) for _ in range(4)]
+    b.fields(out)
+    torch.cuda.synchronize()
+    ha = a.fields()
+    for k, t in zip(("rho", "vx", "vy", "vz"), out):
+        assert np.array_equal(ha[k], t.cpu().numpy())
+    assert torch.all(e[0::2] > 0)
+
+
+def _l2(a, b):
+    num = sum(np.sum((a[k].astype(np.float64) - b[k]) ** 2) for k in ("vx", "vy", "vz"))
+    den = sum(np.sum(b[k] ** 2) for k in ("vx", "vy", "vz"))
+    return np.sqrt(num / den)
+
+
+def test_storage_forms_against_fp64(cuda):
+    """TGV at u0=0.04, Re=1600: FP32, FP16 and BF16 shifted-population storage (FP32 arithmetic)
+    against the FP64 run, relative L2 velocity error after 500 steps."""
+    n, steps, u0 = 64, 500, 0.04
+    nu = u0 * n / (2 * np.pi * 1600)
+    omega = 1.0 / (3 * nu + 0.5)
+    f = tgv_fields(n, n, n, u0)
+    ref = Box(n, n, n, omega, storage="f64")
+    ref.init(*f)
+    ref.step(steps)
+    r = ref.fields()
+    errs = {}
+    for st in ("f32", "f16", "bf16"):
+        b = Box(n, n, n, omega, storage=st)
+        b.init(*(x.astype(np.float32) for x in f))
+        b.step(steps)
+        errs[st] = _l2(b.fields(), r)
+    print("relative L2 velocity error vs FP64:", errs)
+    assert errs["f32"] < 1e-5
+    assert errs["f16"] < 1e-2
+    assert errs["bf16"] < 5e-2

@@ -1,0 +1,167 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle, on the GPU.
+
+Tolerances: the exact arithmetic variant (no FMA contraction) must reproduce the oracle bit for
+bit; the default variant (FMA) must stay within 1e-12 relative L-inf in density and velocity
+(relative to the field's maximum magnitude), the bar of the FP64 form.
+"""
+import numpy as np
+import pytest
+
+from virtualfluids_b200 import BoundaryConditionFactory as BCF
+from virtualfluids_b200 import ListGrid, Parameter, Simulation
+from virtualfluids_b200 import _native as N
+
+pytestmark = pytest.mark.gpu
+
+FAST_TOL = 1e-12
+
+
+def smooth_fields(g, seed, amp_rho=1e-2, amp_u=0.03, modes=3):
+    rng = np.random.default_rng(seed)
+    x, y, z = (g.coords[a].astype(np.float64) for a in range(3))
+    out = []
+    for amp in (amp_rho, amp_u, amp_u, amp_u):
+        f = np.zeros(g.number_of_nodes)
+        for _ in range(modes):
+            k = rng.integers(0, 2, 3) + np.array([1, 0, 0])
+            ph = rng.uniform(0, 2 * np.pi, 3)
+            f += np.cos(2 * np.pi * k[0] * x / g.nx + ph[0]) * np.cos(2 * np.pi * k[1] * y / g.ny + ph[1]) \
+                * np.cos(2 * np.pi * k[2] * z / g.nz + ph[2])
+        f *= amp / modes
+        f[0] = 0.0
+        out.append(f)
+    return out
+
+
+def make_para(omega, storage=N.STORAGE_F64, arith=N.ARITH_FAST, forcing=(0.0, 0.0, 0.0)):
+    p = Parameter()
+    p.set_viscosity_lb((1.0 / omega - 0.5) / 3.0)
+    p.configure_main_kernel("K17CompressibleNavierStokes")
+    p.storage, p.arith = storage, arith
+    p.set_forcing(*forcing)
+    return p
+
+
+def rel_linf(a, b, mask):
+    scale = max(np.abs(b[mask]).max(), 1e-300)
+    return np.abs(a[mask] - b[mask]).max() / scale
+
+
+def run_both(oracle, grid, omega, steps, arith, bcf=None, fields=None, forcing=(0.0, 0.0, 0.0), vkind=1, nkind=1,
+             threads=0):
+    bcf = bcf or BCF()
+    sim = Simulation(make_para(omega, N.STORAGE_F64, arith, forcing), grid, bcf)
+    orc = oracle.OracleLevel(grid, omega=sim.para.omega, forces=forcing, velocity_kind=vkind, noslip_kind=nkind)
+    fields = fields or [None] * 4
+    sim.init(*fields)
+    orc.init(*fields)
+    sim.run(steps)
+    orc.run(steps, threads=threads)
+    return sim, orc
+
+
+def cavity(n, velocity=(0.05, 0.0, 0.0)):
+    g = ListGrid(n, n, n)
+    for s in ("PX", "MX", "PY", "MY", "MZ"):
+        g.add_side(s, "noslip")
+    g.add_side("PZ", "velocity", velocity=velocity)
+    return g
+
+
+def test_periodic_exact_is_bitwise(oracle, cuda):
+    g = ListGrid(12, 10, 8, periodic=(True, True, True))
+    sim, orc = run_both(oracle, g, 1.8, 20, N.ARITH_EXACT, fields=smooth_fields(g, 1))
+    assert np.array_equal(sim.populations(), orc.f)
+
+
+def test_periodic_fast_within_tolerance(oracle, cuda):
+    g = ListGrid(12, 10, 8, periodic=(True, True, True))
+    sim, orc = run_both(oracle, g, 1.8, 20, N.ARITH_FAST, fields=smooth_fields(g, 1))
+    a, b = sim.macroscopic(), orc.macroscopic()
+    fl = g.geo == N.GEO_FLUID
+    for k in ("rho", "vx", "vy", "vz"):
+        assert rel_linf(a[k], b[k], fl) <= FAST_TOL, k
+
+
+def test_forcing_exact_is_bitwise(oracle, cuda):
+    g = ListGrid(10, 8, 6, periodic=(True, True, True))
+    sim, orc = run_both(oracle, g, 1.9, 15, N.ARITH_EXACT, fields=smooth_fields(g, 2), forcing=(1e-5, -2e-6, 3e-6))
+    assert np.array_equal(sim.populations(), orc.f)
+
+
+def test_cavity_bounce_back_exact_is_bitwise(oracle, cuda):
+    """NoSlipBounceBack + VelocityBounceBack, as apps/gpu/DrivenCavity/DrivenCavity.cpp:145-146."""
+    g = cavity(12)
+    bcf = BCF()
+    bcf.set_no_slip_boundary_condition(BCF.NoSlipBC.NoSlipBounceBack)
+    bcf.set_velocity_boundary_condition(BCF.VelocityBC.VelocityBounceBack)
+    sim, orc = run_both(oracle, g, 1.7, 100, N.ARITH_EXACT, bcf=bcf)
+    assert np.array_equal(sim.populations(), orc.f)
+
+
+def _randomise_q(g, seed):
+    rng = np.random.default_rng(seed)
+    for b in g.bcs:
+        cut = b.q >= 0
+        b.q[cut] = rng.uniform(0.05, 0.95, cut.sum())
+
+
+def test_cavity_interpolated_exact_is_bitwise(oracle, cuda):
+    """NoSlipInterpolatedCompressible + VelocityInterpolatedCompressible with q in (0,1)."""
+    g = cavity(12)
+    _randomise_q(g, 5)
+    bcf = BCF()
+    bcf.set_no_slip_boundary_condition(BCF.NoSlipBC.NoSlipInterpolatedCompressible)
+    bcf.set_velocity_boundary_condition(BCF.VelocityBC.VelocityInterpolatedCompressible)
+    sim, orc = run_both(oracle, g, 1.7, 100, N.ARITH_EXACT, bcf=bcf, vkind=2, nkind=2)
+    assert np.array_equal(sim.populations(), orc.f)
+
+
+def test_channel_pressure_outlet_exact_is_bitwise(oracle, cuda):
+    """Velocity inlet (interpolated), PressureNonEquilibriumCompressible outlet, no-slip walls."""
+    g = ListGrid(16, 8, 8, periodic=(False, True, False))
+    g.add_side("MZ", "noslip")
+    g.add_side("PZ", "noslip")
+    g.add_side("MX", "velocity", velocity=(0.02, 0.0, 0.0))
+    g.add_side("PX", "pressure", rho=0.001)
+    bcf = BCF()
+    bcf.set_no_slip_boundary_condition(BCF.NoSlipBC.NoSlipInterpolatedCompressible)
+    bcf.set_velocity_boundary_condition(BCF.VelocityBC.VelocityInterpolatedCompressible)
+    bcf.set_pressure_boundary_condition(BCF.PressureBC.PressureNonEquilibriumCompressible)
+    sim, orc = run_both(oracle, g, 1.8, 120, N.ARITH_EXACT, bcf=bcf, vkind=2, nkind=2)
+    assert np.array_equal(sim.populations(), orc.f)
+    m = sim.macroscopic()
+    assert np.abs(m["vx"]).max() > 1e-3
+
+
+def test_mass_energy_and_macros_match_oracle(oracle, cuda):
+    g = cavity(10)
+    bcf = BCF()
+    bcf.set_no_slip_boundary_condition(BCF.NoSlipBC.NoSlipBounceBack)
+    bcf.set_velocity_boundary_condition(BCF.VelocityBC.VelocityBounceBack)
+    sim, orc = run_both(oracle, g, 1.7, 50, N.ARITH_EXACT, bcf=bcf)
+    a, b = sim.macroscopic(), orc.macroscopic()
+    for k in ("rho", "vx", "vy", "vz", "pressure"):
+        assert np.array_equal(a[k], b[k]), k
+    (m1, e1), (m2, e2) = sim.mass_energy(), orc.mass_energy()
+    assert abs(m1 - m2) <= 1e-13 * m2 and abs(e1 - e2) <= 1e-12 * e2
+
+
+def test_lid_driven_cavity_64_2000_steps(oracle, cuda):
+    """Config 1: 64^3 cavity, lid u=0.05 in +x, Re=100, FP64, 2000 steps. Fast arithmetic within
+    1e-12 relative L-inf of the oracle in drho and u; the global mass sum within 1e-12."""
+    n = 64
+    nu = 0.05 * n / 100.0
+    omega = 1.0 / (3.0 * nu + 0.5)
+    g = cavity(n)
+    bcf = BCF()
+    bcf.set_no_slip_boundary_condition(BCF.NoSlipBC.NoSlipBounceBack)
+    bcf.set_velocity_boundary_condition(BCF.VelocityBC.VelocityBounceBack)
+    sim, orc = run_both(oracle, g, omega, 2000, N.ARITH_FAST, bcf=bcf)
+    a, b = sim.macroscopic(), orc.macroscopic()
+    fl = g.geo == N.GEO_FLUID
+    errs = {k: rel_linf(a[k], b[k], fl) for k in ("rho", "vx", "vy", "vz")}
+    assert max(errs.values()) <= FAST_TOL, errs
+    (m1, _), (m2, _) = sim.mass_energy(), orc.mass_energy()
+    assert abs(m1 - m2) <= 1e-12 * m2
+    assert np.abs(b["vx"][fl]).max() > 0.01  # the flow is developed

@@ -1,0 +1,18 @@
+"""B200-native implementation of the VirtualFluids GPU time-step hot path.
+
+D3Q27 K17 cumulant collision with in-place esoteric-twist streaming, the bounce-back,
+interpolated, velocity and non-equilibrium pressure boundary kernels, and the FP64 reductions,
+as hand-written sm_100a CUDA behind the C ABI of ``include/vfb.h`` (``libvfb.so``). This package
+is the Python host side: set-up objects mirroring the reference's Parameter /
+BoundaryConditionFactory / Simulation, a builder for levels in the reference layout, and
+structured boxes. Importing it loads the native library; there is no fallback.
+"""
+from . import _native
+from ._native import VfbError, lib
+from .box import Box
+from .grid import ListGrid
+from .simulation import BoundaryConditionFactory, Parameter, Simulation
+
+__all__ = ["Box", "BoundaryConditionFactory", "ListGrid", "Parameter", "Simulation", "VfbError", "lib", "_native"]
+
+lib()  # fail at import when the native library is missing

@@ -1,0 +1,96 @@
+"""Structured boxes: full-box domains advanced by the arithmetic-neighbour kernels.
+
+A thin owner of a ``vfb_box`` handle (include/vfb.h). Inputs and outputs may be host numpy
+arrays (copied inside the call, as an end-to-end user would) or device torch tensors.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from .simulation import STORAGE
+
+
+def _dev_ptr(x):
+    return C.c_void_p(x.data_ptr())
+
+
+class Box:
+    def __init__(self, nx, ny, nz, omega, periodic=(True, True, True), storage="f64", arith="fast",
+                 forces=(0.0, 0.0, 0.0), quadric_limiters=(0.01, 0.01, 0.01), mask=None):
+        self.shape = (int(nx), int(ny), int(nz))
+        self.storage = STORAGE[storage] if isinstance(storage, str) else int(storage)
+        self.real = np.float64 if self.storage == N.STORAGE_F64 else np.float32
+        d = N.BoxDesc()
+        d.nx, d.ny, d.nz = self.shape
+        d.periodic_x, d.periodic_y, d.periodic_z = (int(bool(p)) for p in periodic)
+        d.storage = self.storage
+        d.arith = N.ARITH_EXACT if arith == "exact" else N.ARITH_FAST
+        d.omega = float(omega)
+        for i in range(3):
+            d.forces[i] = float(forces[i])
+            d.quadric_limiters[i] = float(quadric_limiters[i])
+        self._mask = None
+        if mask is not None:
+            self._mask = np.ascontiguousarray(np.asarray(mask, dtype=np.uint8).reshape(-1))
+            d.mask = self._mask.ctypes.data
+        h = C.c_void_p()
+        N.check(N.lib().vfb_box_create(C.byref(d), C.byref(h)))
+        self._h = h
+        self.n = nx * ny * nz
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib().vfb_box_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def device_bytes(self) -> int:
+        b = C.c_uint64()
+        N.check(N.lib().vfb_box_device_bytes(self._h, C.byref(b)))
+        return b.value
+
+    def init(self, rho, ux, uy, uz, stream=None):
+        """Equilibrium from drho and velocity fields (x fastest); numpy = host, torch = device."""
+        if isinstance(rho, np.ndarray):
+            arrs = [np.ascontiguousarray(a, dtype=self.real).reshape(-1) for a in (rho, ux, uy, uz)]
+            self._host_keep = arrs
+            ptrs = [C.c_void_p(a.ctypes.data) for a in arrs]
+            N.check(N.lib().vfb_box_init(self._h, *ptrs, 1, stream))
+            N.check(N.lib().vfb_synchronize(stream))
+        else:
+            N.check(N.lib().vfb_box_init(self._h, *(_dev_ptr(a) for a in (rho, ux, uy, uz)), 0, stream))
+
+    def step(self, steps: int, energy=None, stream=None):
+        """Advance; energy: None, host float64 array [steps, 2] or device float64 tensor."""
+        if energy is None:
+            N.check(N.lib().vfb_box_step(self._h, int(steps), None, 0, stream))
+        elif isinstance(energy, np.ndarray):
+            assert energy.dtype == np.float64 and energy.size >= 2 * steps
+            N.check(N.lib().vfb_box_step(self._h, int(steps), C.c_void_p(energy.ctypes.data), 1, stream))
+        else:
+            N.check(N.lib().vfb_box_step(self._h, int(steps), _dev_ptr(energy), 0, stream))
+
+    def fields(self, out=None, stream=None):
+        """drho, ux, uy, uz of the current state. Host numpy by default; device tensors if given."""
+        if out is None:
+            arrs = [np.empty(self.n, dtype=self.real) for _ in range(4)]
+            N.check(N.lib().vfb_box_fields(self._h, *(C.c_void_p(a.ctypes.data) for a in arrs), 1, stream))
+            N.check(N.lib().vfb_synchronize(stream))
+            return dict(zip(("rho", "vx", "vy", "vz"), arrs))
+        N.check(N.lib().vfb_box_fields(self._h, *(_dev_ptr(a) for a in out), 0, stream))
+        return out
+
+    def populations(self):
+        """(device pointer, plane pitch in elements, is_even) of the population array."""
+        p, pitch, ev = C.c_void_p(), C.c_uint64(), C.c_int32()
+        N.check(N.lib().vfb_box_populations(self._h, C.byref(p), C.byref(pitch), C.byref(ev)))
+        return p.value, pitch.value, ev.value

@@ -1,0 +1,734 @@
+// C ABI of the library (include/vfb.h): argument checks, dispatch on storage and arithmetic,
+// the kernel and boundary-condition registries, the step driver and structured boxes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "k17.cuh"
+#include "launch.h"
+#include "vfb.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int status, const std::string &msg)
+{
+    g_last_error = msg;
+    return status;
+}
+
+int cuda_status(cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess)
+        return VFB_OK;
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? VFB_ERR_OUT_OF_MEMORY : VFB_ERR_CUDA;
+}
+
+inline cudaStream_t as_stream(void *s) { return static_cast<cudaStream_t>(s); }
+
+bool storage_ok(int s) { return s >= VFB_STORAGE_F64 && s <= VFB_STORAGE_BF16; }
+size_t storage_bytes(int s) { return s == VFB_STORAGE_F64 ? 8 : s == VFB_STORAGE_F32 ? 4 : 2; }
+size_t real_bytes(int s) { return s == VFB_STORAGE_F64 ? 8 : 4; }
+
+int check_level(const vfb_level *L)
+{
+    if (!L)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "level is NULL");
+    if (!storage_ok(L->storage))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "unknown storage format");
+    if (L->arith != VFB_ARITH_FAST && L->arith != VFB_ARITH_EXACT)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "unknown arithmetic mode");
+    if (L->arith == VFB_ARITH_EXACT && L->storage > VFB_STORAGE_F32)
+        return fail(VFB_ERR_UNSUPPORTED, "exact arithmetic is built for F64 and F32 storage only");
+    if (!L->distributions || !L->neighbor_x || !L->neighbor_y || !L->neighbor_z)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "level distributions or neighbour lists are NULL");
+    if (L->number_of_nodes == 0 || L->number_of_nodes > 0xffffffffull)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "number_of_nodes must be in [1, 2^32)");
+    if (!(L->omega > 0.0 && L->omega < 2.0))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "omega must lie in (0, 2)");
+    return VFB_OK;
+}
+
+// call F with Launchers<S> of the chosen variant
+#define VFB_DISPATCH(storage, arith, CALL)                                                                            \
+    [&]() -> cudaError_t {                                                                                             \
+        if ((arith) == VFB_ARITH_EXACT) {                                                                              \
+            switch (storage) {                                                                                         \
+            case VFB_STORAGE_F64: { using LA = vfb::exact::Launchers<double>; return CALL; }                            \
+            case VFB_STORAGE_F32: { using LA = vfb::exact::Launchers<float>; return CALL; }                             \
+            default: return cudaErrorInvalidValue;                                                                     \
+            }                                                                                                          \
+        }                                                                                                              \
+        switch (storage) {                                                                                             \
+        case VFB_STORAGE_F64: { using LA = vfb::fast::Launchers<double>; return CALL; }                                 \
+        case VFB_STORAGE_F32: { using LA = vfb::fast::Launchers<float>; return CALL; }                                  \
+        case VFB_STORAGE_F16: { using LA = vfb::fast::Launchers<__half>; return CALL; }                                 \
+        case VFB_STORAGE_BF16: { using LA = vfb::fast::Launchers<__nv_bfloat16>; return CALL; }                         \
+        default: return cudaErrorInvalidValue;                                                                         \
+        }                                                                                                              \
+    }()
+
+struct KernelEntry {
+    const char *name;
+    int id;
+};
+// Kernel/KernelTypes.h:35-46 lists the reference's names; this build registers K17 (TurbulenceModel::None)
+const KernelEntry kKernels[] = { { "K17CompressibleNavierStokes", VFB_KERNEL_K17_COMPRESSIBLE_NAVIER_STOKES } };
+
+} // namespace
+
+// ---------------------------------------------------------------------------------------------
+// deterministic partial-sum reduction
+// ---------------------------------------------------------------------------------------------
+namespace vfb {
+__global__ void __launch_bounds__(1024) reduce_partials_kernel(const double *__restrict__ p, uint64_t blocks, double *out)
+{
+    __shared__ double sm[2][1024];
+    double m = 0.0, e = 0.0;
+    for (uint64_t b = threadIdx.x; b < blocks; b += blockDim.x) {
+        m += p[2 * b];
+        e += p[2 * b + 1];
+    }
+    sm[0][threadIdx.x] = m;
+    sm[1][threadIdx.x] = e;
+    __syncthreads();
+    for (unsigned s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            sm[0][threadIdx.x] += sm[0][threadIdx.x + s];
+            sm[1][threadIdx.x] += sm[1][threadIdx.x + s];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = sm[0][0];
+        out[1] = sm[1][0];
+    }
+}
+
+cudaError_t reduce_partials(const double *partials, uint64_t blocks, double *out, cudaStream_t s)
+{
+    reduce_partials_kernel<<<1, 1024, 0, s>>>(partials, blocks, out);
+    return cudaGetLastError();
+}
+} // namespace vfb
+
+// ---------------------------------------------------------------------------------------------
+// library
+// ---------------------------------------------------------------------------------------------
+extern "C" {
+
+int vfb_abi_version(void) { return VFB_ABI_VERSION; }
+
+const char *vfb_last_error(void) { return g_last_error.c_str(); }
+
+const char *vfb_status_string(int status)
+{
+    switch (status) {
+    case VFB_OK: return "ok";
+    case VFB_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case VFB_ERR_UNKNOWN_KERNEL: return "KernelFactory does not know the KernelType.";
+    case VFB_ERR_BC_UNSET: return "a boundary condition has nodes but no kernel";
+    case VFB_ERR_SCALING_UNSET: return "more than one level but no grid scaling kernel";
+    case VFB_ERR_CUDA: return "CUDA error";
+    case VFB_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case VFB_ERR_UNSUPPORTED: return "not supported by this build";
+    case VFB_ERR_WATCHDOG: return "non-finite populations or mass drift";
+    default: return "unknown status";
+    }
+}
+
+int vfb_synchronize(void *stream)
+{
+    return cuda_status(stream ? cudaStreamSynchronize(as_stream(stream)) : cudaDeviceSynchronize(), "synchronize");
+}
+
+int vfb_lattice_tables(int32_t cx[27], int32_t cy[27], int32_t cz[27], int32_t inv[27], double w[27])
+{
+    if (!cx || !cy || !cz || !inv || !w)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL table");
+    for (int d = 0; d < 27; ++d) {
+        cx[d] = vfb::cx(d);
+        cy[d] = vfb::cy(d);
+        cz[d] = vfb::cz(d);
+        inv[d] = vfb::inv(d);
+        w[d] = vfb::weight_t<double>(d);
+    }
+    return VFB_OK;
+}
+
+int vfb_k17_rates(double omega, double rates[6])
+{
+    if (!rates)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL rates");
+    const vfb::K17Rates<double> r = vfb::make_k17_rates<double>(omega, 0.01, 0.01, 0.01);
+    rates[0] = r.OxyyPxzz;
+    rates[1] = r.OxyyMxzz;
+    rates[2] = r.Oxyz;
+    rates[3] = r.factorA;
+    rates[4] = r.factorB;
+    rates[5] = -r.neg_iwm;
+    return VFB_OK;
+}
+
+int vfb_kernel_lookup(const char *name, int32_t *kernel_id)
+{
+    if (!name || !kernel_id)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL name or id");
+    for (const KernelEntry &e : kKernels)
+        if (std::strcmp(e.name, name) == 0) {
+            *kernel_id = e.id;
+            return VFB_OK;
+        }
+    return fail(VFB_ERR_UNKNOWN_KERNEL, std::string("KernelFactory does not know the KernelType: ") + name);
+}
+
+int vfb_kernel_count(void) { return (int)(sizeof(kKernels) / sizeof(kKernels[0])); }
+
+const char *vfb_kernel_name(int index)
+{
+    if (index < 0 || index >= vfb_kernel_count())
+        return nullptr;
+    return kKernels[index].name;
+}
+
+// ---------------------------------------------------------------------------------------------
+// (1) reference-layout entry points
+// ---------------------------------------------------------------------------------------------
+int vfb_k17_run_on_indices(const vfb_level *level, const uint32_t *idx, uint32_t size, int32_t tmpl, void *stream)
+{
+    int st = check_level(level);
+    if (st)
+        return st;
+    if (tmpl < VFB_COLLISION_DEFAULT || tmpl > VFB_COLLISION_SUBDOMAIN_BORDER)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "Invalid CollisionTemplate");
+    if (size && !idx)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "fluid node indices are NULL");
+    const bool wm = tmpl != VFB_COLLISION_DEFAULT && tmpl != VFB_COLLISION_APPLY_BODY_FORCE;
+    const bool bf = tmpl == VFB_COLLISION_APPLY_BODY_FORCE || tmpl == VFB_COLLISION_ALL_FEATURES || tmpl == VFB_COLLISION_SUBDOMAIN_BORDER;
+    if (wm && (!level->rho || !level->velocity_x || !level->velocity_y || !level->velocity_z))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "macroscopic output arrays are NULL");
+    if (bf && (!level->body_force_x || !level->body_force_y || !level->body_force_z))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "body force arrays are NULL");
+    const cudaError_t e = VFB_DISPATCH(level->storage, level->arith, LA::k17_list(level, idx, size, tmpl, as_stream(stream)));
+    return cuda_status(e, "K17CompressibleNavierStokes launch");
+}
+
+static int run_bc(const vfb_level *level, const vfb_bc *bc, int kind, bool velocity, void *stream)
+{
+    int st = check_level(level);
+    if (st)
+        return st;
+    if (!bc)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "bc is NULL");
+    if (bc->number_of_bc_nodes && (!bc->k || !bc->q27))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "bc node indices or q27 are NULL");
+    if (velocity && bc->number_of_bc_nodes && (!bc->vx || !bc->vy || !bc->vz))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "bc velocities are NULL");
+    const cudaError_t e = VFB_DISPATCH(level->storage, level->arith, LA::bc(level, bc, kind, as_stream(stream)));
+    return cuda_status(e, "boundary condition launch");
+}
+
+int vfb_noslip_bounce_back(const vfb_level *level, const vfb_bc *bc, void *stream)
+{
+    return run_bc(level, bc, vfb::kNoSlipBB, false, stream);
+}
+int vfb_noslip_interpolated_compressible(const vfb_level *level, const vfb_bc *bc, void *stream)
+{
+    return run_bc(level, bc, vfb::kNoSlipInterp, false, stream);
+}
+int vfb_velocity_bounce_back(const vfb_level *level, const vfb_bc *bc, void *stream)
+{
+    return run_bc(level, bc, vfb::kVelocityBB, true, stream);
+}
+int vfb_velocity_interpolated_compressible(const vfb_level *level, const vfb_bc *bc, void *stream)
+{
+    return run_bc(level, bc, vfb::kVelocityInterp, true, stream);
+}
+
+int vfb_pressure_non_equilibrium_compressible(const vfb_level *level, const vfb_directional_bc *bc, void *stream)
+{
+    int st = check_level(level);
+    if (st)
+        return st;
+    if (!bc)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "bc is NULL");
+    if (bc->direction < VFB_DIR_P00 || bc->direction > VFB_DIR_00M)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "direction must be one of the six face directions");
+    if (bc->number_of_bc_nodes && (!bc->k || !bc->k_neighbor || !bc->rho_bc))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "pressure bc arrays are NULL");
+    const cudaError_t e = VFB_DISPATCH(level->storage, level->arith, LA::pressure(level, bc, as_stream(stream)));
+    return cuda_status(e, "PressureNonEquilibriumCompressible launch");
+}
+
+int vfb_init_navier_stokes_compressible(const vfb_level *level, void *stream)
+{
+    int st = check_level(level);
+    if (st)
+        return st;
+    if (!level->type_of_grid_node || !level->rho || !level->velocity_x || !level->velocity_y || !level->velocity_z)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "init needs typeOfGridNode, rho and velocities");
+    const cudaError_t e = VFB_DISPATCH(level->storage, level->arith, LA::init_list(level, as_stream(stream)));
+    return cuda_status(e, "InitNavierStokesCompressible launch");
+}
+
+int vfb_calc_macroscopic_compressible(const vfb_level *level, void *stream)
+{
+    int st = check_level(level);
+    if (st)
+        return st;
+    if (!level->type_of_grid_node || !level->rho || !level->velocity_x || !level->velocity_y || !level->velocity_z)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "macroscopic output needs typeOfGridNode, rho and velocities");
+    const cudaError_t e = VFB_DISPATCH(level->storage, level->arith, LA::macros_list(level, as_stream(stream)));
+    return cuda_status(e, "calculateMacroscopicQuantitiesCompressible launch");
+}
+
+size_t vfb_mass_energy_workspace_bytes(uint32_t size)
+{
+    const uint64_t blocks = (size + 255u) / 256u;
+    return (size_t)(2 * blocks + 2) * sizeof(double);
+}
+
+int vfb_mass_energy(const vfb_level *level, const uint32_t *idx, uint32_t size, void *workspace, size_t workspace_bytes,
+                    double out[2], void *stream)
+{
+    int st = check_level(level);
+    if (st)
+        return st;
+    if (!out || (size && !idx) || !workspace)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (workspace_bytes < vfb_mass_energy_workspace_bytes(size))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "workspace too small");
+    if ((reinterpret_cast<uintptr_t>(workspace) & 7u) != 0)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "workspace must be 8-byte aligned");
+    const uint64_t blocks = (size + 255u) / 256u;
+    double *partials = static_cast<double *>(workspace);
+    double *result = partials + 2 * blocks;
+    cudaStream_t s = as_stream(stream);
+    if (size == 0) {
+        out[0] = out[1] = 0.0;
+        return VFB_OK;
+    }
+    cudaError_t e = VFB_DISPATCH(level->storage, level->arith, LA::energy_list(level, idx, size, partials, s));
+    if (e == cudaSuccess)
+        e = vfb::reduce_partials(partials, blocks, result, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, result, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s);
+    return cuda_status(e, "mass/energy reduction");
+}
+
+// ---------------------------------------------------------------------------------------------
+// boundary-condition factory
+// ---------------------------------------------------------------------------------------------
+int vfb_bc_factory_velocity(int32_t variant, vfb_bc_fn *fn)
+{
+    if (!fn)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL fn");
+    *fn = nullptr;
+    switch (variant) {
+    case VFB_VELOCITY_BOUNCE_BACK: *fn = vfb_velocity_bounce_back; return VFB_OK;
+    case VFB_VELOCITY_INTERPOLATED_COMPRESSIBLE: *fn = vfb_velocity_interpolated_compressible; return VFB_OK;
+    case VFB_VELOCITY_NOT_SPECIFIED: return VFB_OK;
+    case VFB_VELOCITY_INTERPOLATED_INCOMPRESSIBLE:
+    case VFB_VELOCITY_WITH_PRESSURE_INTERPOLATED_COMPRESSIBLE:
+        return fail(VFB_ERR_UNSUPPORTED, "velocity BC variant not built");
+    default: return fail(VFB_ERR_INVALID_ARGUMENT, "unknown VelocityBC");
+    }
+}
+
+int vfb_bc_factory_noslip(int32_t variant, vfb_bc_fn *fn)
+{
+    if (!fn)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL fn");
+    *fn = nullptr;
+    switch (variant) {
+    case VFB_NOSLIP_DELAY_BOUNCE_BACK: return VFB_OK; // BoundaryConditionFactory.cpp: empty function
+    case VFB_NOSLIP_BOUNCE_BACK: *fn = vfb_noslip_bounce_back; return VFB_OK;
+    case VFB_NOSLIP_INTERPOLATED_COMPRESSIBLE: *fn = vfb_noslip_interpolated_compressible; return VFB_OK;
+    case VFB_NOSLIP_INTERPOLATED_INCOMPRESSIBLE: return fail(VFB_ERR_UNSUPPORTED, "no-slip BC variant not built");
+    default: return fail(VFB_ERR_INVALID_ARGUMENT, "unknown NoSlipBC");
+    }
+}
+
+int vfb_bc_factory_pressure(int32_t variant, vfb_directional_bc_fn *fn)
+{
+    if (!fn)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL fn");
+    *fn = nullptr;
+    switch (variant) {
+    case VFB_PRESSURE_NON_EQUILIBRIUM_COMPRESSIBLE: *fn = vfb_pressure_non_equilibrium_compressible; return VFB_OK;
+    case VFB_PRESSURE_NOT_SPECIFIED: return VFB_OK;
+    case VFB_PRESSURE_NON_EQUILIBRIUM_INCOMPRESSIBLE:
+    case VFB_PRESSURE_OUTFLOW_NON_REFLECTIVE:
+    case VFB_PRESSURE_OUTFLOW_NON_REFLECTIVE_PRESSURE_CORRECTION:
+        return fail(VFB_ERR_UNSUPPORTED, "pressure BC variant not built");
+    default: return fail(VFB_ERR_INVALID_ARGUMENT, "unknown PressureBC");
+    }
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// (2a) step driver
+// ---------------------------------------------------------------------------------------------
+struct vfb_simulation {
+    int kernel_id = 0;
+    bool has_level = false;
+    vfb_level level{};
+    const uint32_t *fluid = nullptr;
+    uint32_t n_fluid = 0;
+    vfb_bc velocity{};
+    vfb_bc_fn velocity_fn = nullptr;
+    bool velocity_set = false;
+    vfb_bc noslip{};
+    vfb_bc_fn noslip_fn = nullptr;
+    bool noslip_set = false;
+    std::vector<vfb_directional_bc> pressure;
+    std::vector<vfb_directional_bc_fn> pressure_fn;
+};
+
+extern "C" {
+
+int vfb_simulation_create(const char *kernel_name, vfb_simulation **out)
+{
+    if (!out)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL out");
+    *out = nullptr;
+    int32_t id = 0;
+    int st = vfb_kernel_lookup(kernel_name, &id);
+    if (st)
+        return st;
+    vfb_simulation *s = new vfb_simulation();
+    s->kernel_id = id;
+    *out = s;
+    return VFB_OK;
+}
+
+int vfb_simulation_destroy(vfb_simulation *sim)
+{
+    delete sim;
+    return VFB_OK;
+}
+
+int vfb_simulation_set_level(vfb_simulation *sim, const vfb_level *level, const uint32_t *fluid, uint32_t n)
+{
+    if (!sim)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL simulation");
+    int st = check_level(level);
+    if (st)
+        return st;
+    if (n && !fluid)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "fluid node indices are NULL");
+    sim->level = *level;
+    sim->fluid = fluid;
+    sim->n_fluid = n;
+    sim->has_level = true;
+    return VFB_OK;
+}
+
+int vfb_simulation_set_velocity_bc(vfb_simulation *sim, const vfb_bc *bc, int32_t variant)
+{
+    if (!sim || !bc)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    vfb_bc_fn fn = nullptr;
+    int st = vfb_bc_factory_velocity(variant, &fn);
+    if (st)
+        return st;
+    sim->velocity = *bc;
+    sim->velocity_fn = fn;
+    sim->velocity_set = true;
+    return VFB_OK;
+}
+
+int vfb_simulation_set_noslip_bc(vfb_simulation *sim, const vfb_bc *bc, int32_t variant)
+{
+    if (!sim || !bc)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    vfb_bc_fn fn = nullptr;
+    int st = vfb_bc_factory_noslip(variant, &fn);
+    if (st)
+        return st;
+    sim->noslip = *bc;
+    sim->noslip_fn = fn;
+    sim->noslip_set = true;
+    return VFB_OK;
+}
+
+int vfb_simulation_add_pressure_bc(vfb_simulation *sim, const vfb_directional_bc *bc, int32_t variant)
+{
+    if (!sim || !bc)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    vfb_directional_bc_fn fn = nullptr;
+    int st = vfb_bc_factory_pressure(variant, &fn);
+    if (st)
+        return st;
+    sim->pressure.push_back(*bc);
+    sim->pressure_fn.push_back(fn);
+    return VFB_OK;
+}
+
+// BoundaryConditionKernelManager.cpp:67-80: a BC that has nodes needs a kernel; the delayed
+// no-slip bounce-back is the one BC whose "kernel" is deliberately empty.
+int vfb_simulation_check(const vfb_simulation *sim)
+{
+    if (!sim)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL simulation");
+    if (!sim->has_level)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "no level set");
+    if (sim->velocity_set && sim->velocity.number_of_bc_nodes > 0 && !sim->velocity_fn)
+        return fail(VFB_ERR_BC_UNSET, "Velocity boundary condition has nodes but no kernel");
+    for (size_t i = 0; i < sim->pressure.size(); ++i)
+        if (sim->pressure[i].number_of_bc_nodes > 0 && !sim->pressure_fn[i])
+            return fail(VFB_ERR_BC_UNSET, "Pressure boundary condition has nodes but no kernel");
+    return VFB_OK;
+}
+
+int vfb_simulation_run(vfb_simulation *sim, uint32_t steps, void *stream)
+{
+    int st = vfb_simulation_check(sim);
+    if (st)
+        return st;
+    vfb_level &L = sim->level;
+    for (uint32_t t = 0; t < steps; ++t) {
+        st = vfb_k17_run_on_indices(&L, sim->fluid, sim->n_fluid, VFB_COLLISION_DEFAULT, stream);
+        if (st)
+            return st;
+        if (sim->velocity_fn && sim->velocity.number_of_bc_nodes) {
+            st = sim->velocity_fn(&L, &sim->velocity, stream);
+            if (st)
+                return st;
+        }
+        if (sim->noslip_fn && sim->noslip.number_of_bc_nodes) {
+            st = sim->noslip_fn(&L, &sim->noslip, stream);
+            if (st)
+                return st;
+        }
+        L.is_even_timestep = !L.is_even_timestep;
+        for (size_t i = 0; i < sim->pressure.size(); ++i) {
+            if (!sim->pressure_fn[i] || !sim->pressure[i].number_of_bc_nodes)
+                continue;
+            st = sim->pressure_fn[i](&L, &sim->pressure[i], stream);
+            if (st)
+                return st;
+        }
+    }
+    return VFB_OK;
+}
+
+int vfb_simulation_is_even_timestep(const vfb_simulation *sim, int32_t *is_even)
+{
+    if (!sim || !is_even)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    *is_even = sim->level.is_even_timestep;
+    return VFB_OK;
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// (2b) structured boxes
+// ---------------------------------------------------------------------------------------------
+struct vfb_box {
+    vfb_box_desc desc{};
+    vfb::BoxState state{};
+    bool even = true;
+    uint64_t n = 0;
+    void *dist = nullptr;
+    uint8_t *mask = nullptr;
+    double *partials = nullptr;     // per-block energy partials of one step
+    uint64_t blocks = 0;
+    double *energy_ring = nullptr;  // per-step results before they are copied out
+    uint32_t ring_steps = 0;
+    void *staging = nullptr;        // 4 real fields for init and output
+};
+
+namespace {
+constexpr uint32_t kRingSteps = 1024;
+
+void box_free(vfb_box *b)
+{
+    if (!b)
+        return;
+    cudaFree(b->dist);
+    cudaFree(b->mask);
+    cudaFree(b->partials);
+    cudaFree(b->energy_ring);
+    cudaFree(b->staging);
+}
+} // namespace
+
+extern "C" {
+
+int vfb_box_create(const vfb_box_desc *d, vfb_box **out)
+{
+    if (!d || !out)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    if (d->nx < 2 || d->ny < 2 || d->nz < 2 || d->ny > 65535 || d->nz > 65535)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "box extents must be >= 2 (ny, nz <= 65535)");
+    const uint64_t n = (uint64_t)d->nx * d->ny * d->nz;
+    if (n >= 0xffffffffull)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "box has too many nodes for 32-bit indices");
+    if (!storage_ok(d->storage))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "unknown storage format");
+    if (d->arith != VFB_ARITH_FAST && d->arith != VFB_ARITH_EXACT)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "unknown arithmetic mode");
+    if (d->arith == VFB_ARITH_EXACT && d->storage > VFB_STORAGE_F32)
+        return fail(VFB_ERR_UNSUPPORTED, "exact arithmetic is built for F64 and F32 storage only");
+    if (!(d->omega > 0.0 && d->omega < 2.0))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "omega must lie in (0, 2)");
+    if ((!d->periodic_x || !d->periodic_y || !d->periodic_z) && !d->mask)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "a non-periodic box needs a mask with a solid border");
+    vfb_box *b = new vfb_box();
+    b->desc = *d;
+    b->desc.mask = nullptr;
+    b->n = n;
+    // planes padded to 256 bytes so every plane starts aligned
+    const size_t sb = storage_bytes(d->storage);
+    const uint64_t align_el = 256 / sb;
+    const uint64_t pitch = (n + align_el - 1) / align_el * align_el;
+    cudaError_t e = cudaMalloc(&b->dist, pitch * 27 * sb);
+    if (e == cudaSuccess && d->mask) {
+        e = cudaMalloc((void **)&b->mask, n);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(b->mask, d->mask, n, cudaMemcpyHostToDevice);
+    }
+    vfb::BoxState &s = b->state;
+    s.dist = b->dist;
+    s.pitch = pitch;
+    s.nx = d->nx;
+    s.ny = d->ny;
+    s.nz = d->nz;
+    s.periodic_x = d->periodic_x;
+    s.periodic_y = d->periodic_y;
+    s.periodic_z = d->periodic_z;
+    s.mask = b->mask;
+    s.omega = d->omega;
+    s.fx = d->forces[0] * 0.5;
+    s.fy = d->forces[1] * 0.5;
+    s.fz = d->forces[2] * 0.5;
+    for (int i = 0; i < 3; ++i)
+        s.lim[i] = d->quadric_limiters[i];
+    b->blocks = vfb::box_blocks(s);
+    if (e == cudaSuccess)
+        e = cudaMalloc((void **)&b->partials, 2 * b->blocks * sizeof(double));
+    if (e == cudaSuccess)
+        e = cudaMalloc((void **)&b->energy_ring, 2 * (size_t)kRingSteps * sizeof(double));
+    b->ring_steps = kRingSteps;
+    if (e == cudaSuccess)
+        e = cudaMalloc(&b->staging, 4 * n * real_bytes(d->storage));
+    if (e != cudaSuccess) {
+        box_free(b);
+        delete b;
+        return cuda_status(e, "box allocation");
+    }
+    *out = b;
+    return VFB_OK;
+}
+
+int vfb_box_destroy(vfb_box *box)
+{
+    box_free(box);
+    delete box;
+    return VFB_OK;
+}
+
+int vfb_box_device_bytes(const vfb_box *box, uint64_t *bytes)
+{
+    if (!box || !bytes)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    const uint64_t sb = storage_bytes(box->desc.storage);
+    *bytes = box->state.pitch * 27 * sb + (box->mask ? box->n : 0) + 2 * box->blocks * 8 + 2 * (uint64_t)box->ring_steps * 8
+           + 4 * box->n * real_bytes(box->desc.storage);
+    return VFB_OK;
+}
+
+int vfb_box_init(vfb_box *box, const void *rho, const void *ux, const void *uy, const void *uz, int32_t from_host,
+                 void *stream)
+{
+    if (!box || !rho || !ux || !uy || !uz)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    cudaStream_t s = as_stream(stream);
+    const size_t rb = real_bytes(box->desc.storage), fb = box->n * rb;
+    const void *f[4] = { rho, ux, uy, uz };
+    const void *dev[4];
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < 4 && e == cudaSuccess; ++i) {
+        if (from_host) {
+            void *dst = static_cast<char *>(box->staging) + i * fb;
+            e = cudaMemcpyAsync(dst, f[i], fb, cudaMemcpyHostToDevice, s);
+            dev[i] = dst;
+        } else {
+            dev[i] = f[i];
+        }
+    }
+    // PreProcessorImp::init (PreProcessorImp.cpp:50-58): odd parity, then even
+    if (e == cudaSuccess)
+        e = VFB_DISPATCH(box->desc.storage, box->desc.arith, LA::box_init(box->state, false, dev[0], dev[1], dev[2], dev[3], s));
+    if (e == cudaSuccess)
+        e = VFB_DISPATCH(box->desc.storage, box->desc.arith, LA::box_init(box->state, true, dev[0], dev[1], dev[2], dev[3], s));
+    box->even = true;
+    return cuda_status(e, "box init");
+}
+
+int vfb_box_step(vfb_box *box, uint32_t steps, double *energy, int32_t energy_on_host, void *stream)
+{
+    if (!box)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL box");
+    cudaStream_t s = as_stream(stream);
+    cudaError_t e = cudaSuccess;
+    uint32_t done = 0;
+    while (done < steps && e == cudaSuccess) {
+        const uint32_t chunk = energy && energy_on_host ? std::min<uint32_t>(steps - done, box->ring_steps) : steps - done;
+        for (uint32_t t = 0; t < chunk && e == cudaSuccess; ++t) {
+            double *partials = energy ? box->partials : nullptr;
+            e = VFB_DISPATCH(box->desc.storage, box->desc.arith, LA::box_collide(box->state, box->even, partials, s));
+            if (e == cudaSuccess && energy) {
+                double *dst = energy_on_host ? box->energy_ring + 2 * t : energy + 2 * (uint64_t)(done + t);
+                e = vfb::reduce_partials(box->partials, box->blocks, dst, s);
+            }
+            box->even = !box->even;
+        }
+        if (e == cudaSuccess && energy && energy_on_host)
+            e = cudaMemcpyAsync(energy + 2 * (uint64_t)done, box->energy_ring, 2 * sizeof(double) * chunk,
+                                cudaMemcpyDeviceToHost, s);
+        done += chunk;
+    }
+    return cuda_status(e, "box step");
+}
+
+int vfb_box_fields(vfb_box *box, void *rho, void *ux, void *uy, void *uz, int32_t to_host, void *stream)
+{
+    if (!box || !rho || !ux || !uy || !uz)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    cudaStream_t s = as_stream(stream);
+    const size_t rb = real_bytes(box->desc.storage), fb = box->n * rb;
+    void *out[4] = { rho, ux, uy, uz };
+    void *dev[4];
+    for (int i = 0; i < 4; ++i)
+        dev[i] = to_host ? static_cast<char *>(box->staging) + i * fb : out[i];
+    cudaError_t e = VFB_DISPATCH(box->desc.storage, box->desc.arith,
+                                 LA::box_macros(box->state, box->even, dev[0], dev[1], dev[2], dev[3], s));
+    for (int i = 0; i < 4 && e == cudaSuccess && to_host; ++i)
+        e = cudaMemcpyAsync(out[i], dev[i], fb, cudaMemcpyDeviceToHost, s);
+    return cuda_status(e, "box fields");
+}
+
+int vfb_box_populations(const vfb_box *box, void **dist, uint64_t *pitch, int32_t *is_even)
+{
+    if (!box || !dist || !pitch || !is_even)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    *dist = box->dist;
+    *pitch = box->state.pitch;
+    *is_even = box->even ? 1 : 0;
+    return VFB_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,332 @@
+// K17 cumulant collision of one D3Q27 node, register resident.
+//
+// Algorithm: src/lbm/collision/K17CompressibleNavierStokes.h:88-591 (TurbulenceModel::None),
+// with the chimera transforms of src/lbm/ChimeraTransformation.h:58-121 and the pyramid
+// macroscopic sums of src/lbm/MacroscopicQuantities.h:55-137. The floating-point expression
+// trees are kept as in the reference so that a build without FMA contraction (-fmad=false)
+// reproduces the reference's host arithmetic bit for bit; the default build contracts
+// products into FMAs.
+//
+// Differences in *work*, not in results:
+//  * the omega-only rates (five rational functions and 1/omega - 1/2) are computed once on the
+//    host and passed in (K17Rates);
+//  * with the relaxation rates O4 = O5 = O6 = 1 that the reference hard-codes, the pre-collision
+//    4th, 5th and 6th order cumulants are multiplied by zero (4th) or relaxed to exactly zero
+//    (5th, 6th), so they are not computed here; for finite inputs this changes no value.
+#pragma once
+#include "lattice.cuh"
+
+namespace vfb {
+
+template <class T>
+struct K17Rates {
+    T omega;
+    T OxyyPxzz, OxyyMxzz, Oxyz; // 3rd order rates (K17...h:251-255)
+    T factorA, factorB;         // 4th order diffusion parameters (K17...h:272-273)
+    T neg_iwm;                  // -(1/omega - 1/2)
+    T qP, qM, qD;               // quadric limiters (Parameter.cpp:69 default 0.01)
+};
+
+// host computation of the omega-only rates, expression for expression as the reference
+template <class T>
+inline K17Rates<T> make_k17_rates(T omega, T qP, T qM, T qD)
+{
+    K17Rates<T> r;
+    const T w = omega;
+    r.omega = w;
+    r.OxyyPxzz = T(8) * (T(-2) + w) * (T(1) + T(2) * w) / (T(-8) - T(14) * w + T(7) * w * w);
+    r.OxyyMxzz = T(8) * (T(-2) + w) * (T(-7) + T(4) * w) / (T(56) - T(50) * w + T(9) * w * w);
+    r.Oxyz = T(24) * (T(-2) + w) * (T(-2) - T(7) * w + T(3) * w * w) / (T(48) + T(152) * w - T(130) * w * w + T(29) * w * w * w);
+    r.factorA = (T(4) + T(2) * w - T(3) * w * w) / (T(2) - T(7) * w + T(5) * w * w);
+    r.factorB = (T(4) + T(28) * w - T(14) * w * w) / (T(6) - T(21) * w + T(15) * w * w);
+    r.neg_iwm = -(T(1) / w - T(0.5));
+    r.qP = qP;
+    r.qM = qM;
+    r.qD = qD;
+    return r;
+}
+
+namespace k17detail {
+
+template <class T>
+__device__ __forceinline__ void fwd_k(T &a, T &b, T &c, T v, T v2, T kinv, T k)
+{
+    const T s2 = a + c;
+    const T s1 = c - a;
+    T s0 = s2 + b;
+    a = s0;
+    s0 *= kinv;
+    s0 += T(1);
+    b = (s1 * kinv - s0 * v) * k;
+    c = ((s2 - T(2) * s1 * v) * kinv + v2 * s0) * k;
+}
+template <class T>
+__device__ __forceinline__ void bwd_k(T &a, T &b, T &c, T v, T v2, T kinv, T k)
+{
+    const T h = T(0.5);
+    const T r0 = (((c - b) * h + b * v) * kinv + (a * kinv + T(1)) * (v2 - v) * h) * k;
+    const T r1 = (((a - c) - T(2) * b * v) * kinv + (a * kinv + T(1)) * (-v2)) * k;
+    c = (((c + b) * h + b * v) * kinv + (a * kinv + T(1)) * (v2 + v) * h) * k;
+    a = r0;
+    b = r1;
+}
+template <class T>
+__device__ __forceinline__ void fwd(T &a, T &b, T &c, T v, T v2)
+{
+    const T s1 = (a + c) + b;
+    const T s2 = c - a;
+    c = (c + a) + (v2 * s1 - T(2) * v * s2);
+    b = s2 - v * s1;
+    a = s1;
+}
+template <class T>
+__device__ __forceinline__ void bwd(T &a, T &b, T &c, T v, T v2)
+{
+    const T h = T(0.5);
+    const T ra = (c + a * (v2 - v)) * h + b * (v - h);
+    const T rb = ((a - c) - a * v2) - T(2) * b * v;
+    c = (c + a * (v2 + v)) * h + b * (v + h);
+    b = rb;
+    a = ra;
+}
+
+// chimera constants, as the reference writes them (c36o1, c1o36, c9o4, c4o9, ...)
+template <class T> __device__ __forceinline__ T kinv_z(int a, int b)
+{
+    return (a != 1 && b != 1) ? T(36) : (a == 1 && b == 1) ? T(9) / T(4) : T(9);
+}
+template <class T> __device__ __forceinline__ T k_z(int a, int b)
+{
+    return (a != 1 && b != 1) ? T(1) / T(36) : (a == 1 && b == 1) ? T(4) / T(9) : T(1) / T(9);
+}
+template <class T> __device__ __forceinline__ T kinv_y(int a, int c)
+{
+    return a != 1 ? (c == 0 ? T(6) : T(18)) : (c == 0 ? T(3) / T(2) : T(9) / T(2));
+}
+template <class T> __device__ __forceinline__ T k_y(int a, int c)
+{
+    return a != 1 ? (c == 0 ? T(1) / T(6) : T(1) / T(18)) : (c == 0 ? T(2) / T(3) : T(2) / T(9));
+}
+
+} // namespace k17detail
+
+// pyramid density (MacroscopicQuantities.h:55), f in direction order
+template <class T>
+__device__ __forceinline__ T density_pyramid(const T *f)
+{
+    const T corners = ((f[19] + f[26]) + (f[24] + f[21])) + ((f[20] + f[25]) + (f[22] + f[23]));
+    const T edges = (((f[18] + f[17]) + (f[16] + f[15])) + ((f[14] + f[13]) + (f[12] + f[11]))) + ((f[10] + f[9]) + (f[8] + f[7]));
+    const T faces = ((f[2] + f[1]) + (f[4] + f[3])) + (f[6] + f[5]);
+    return ((corners + edges) + f[0]) + faces;
+}
+template <class T>
+__device__ __forceinline__ T momentum_x(const T *f)
+{
+    return ((((f[19] - f[26]) + (f[21] - f[24])) + ((f[25] - f[20]) + (f[23] - f[22])))
+          + (((f[13] - f[14]) + (f[11] - f[12])) + ((f[9] - f[10]) + (f[7] - f[8]))))
+          + (f[1] - f[2]);
+}
+template <class T>
+__device__ __forceinline__ T momentum_y(const T *f)
+{
+    return ((((f[19] - f[26]) + (f[24] - f[21])) + ((f[20] - f[25]) + (f[23] - f[22])))
+          + (((f[17] - f[18]) + (f[15] - f[16])) + ((f[10] - f[9]) + (f[7] - f[8]))))
+          + (f[3] - f[4]);
+}
+template <class T>
+__device__ __forceinline__ T momentum_z(const T *f)
+{
+    return ((((f[19] - f[26]) + (f[21] - f[24])) + ((f[20] - f[25]) + (f[22] - f[23])))
+          + (((f[18] - f[17]) + (f[15] - f[16])) + ((f[14] - f[13]) + (f[11] - f[12]))))
+          + (f[5] - f[6]);
+}
+
+// In place on f[27] (direction order). fx, fy, fz: half the acceleration, already scaled.
+// Returns drho and the velocity including the half force (MacroscopicValues).
+template <class T, bool EXACT>
+__device__ __forceinline__ void k17_collide(T *f, const K17Rates<T> &r, T fx, T fy, T fz, T &drho_out, T &vx_out,
+                                            T &vy_out, T &vz_out)
+{
+    using namespace k17detail;
+    const T drho = density_pyramid(f);
+    const T oneOverRho = T(1) / (drho + T(1));
+    T vx = momentum_x(f) * oneOverRho;
+    T vy = momentum_y(f) * oneOverRho;
+    T vz = momentum_z(f) * oneOverRho;
+    vx += fx;
+    vy += fy;
+    vz += fz;
+    const T vx2 = vx * vx, vy2 = vy * vy, vz2 = vz * vz;
+
+    T m[27];
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        m[m3(d)] = f[d];
+#define M(a, b, c) m[(a) * 9 + (b) * 3 + (c)]
+
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+            fwd_k(M(a, b, 0), M(a, b, 1), M(a, b, 2), vz, vz2, kinv_z<T>(a, b), k_z<T>(a, b));
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; c += 1) {
+            if (c == 1)
+                fwd(M(a, 0, 1), M(a, 1, 1), M(a, 2, 1), vy, vy2);
+            else
+                fwd_k(M(a, 0, c), M(a, 1, c), M(a, 2, c), vy, vy2, kinv_y<T>(a, c), k_y<T>(a, c));
+        }
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            if (b == 0 && c == 0)
+                fwd_k(M(0, 0, 0), M(1, 0, 0), M(2, 0, 0), vx, vx2, T(1), T(1));
+            else if (b == 2 && c == 2) // K17...h:222: K^-1 = 3, K = 1/9 on this line
+                fwd_k(M(0, 2, 2), M(1, 2, 2), M(2, 2, 2), vx, vx2, T(3), T(1) / T(9));
+            else if ((b == 2 && c == 0) || (b == 0 && c == 2))
+                fwd_k(M(0, b, c), M(1, b, c), M(2, b, c), vx, vx2, T(3), T(1) / T(3));
+            else
+                fwd(M(0, b, c), M(1, b, c), M(2, b, c), vx, vx2);
+        }
+
+    const T c13 = T(1) / T(3), c19 = T(1) / T(9), c23 = T(2) / T(3), c127 = T(1) / T(27), h = T(0.5);
+    const T omega = r.omega;
+
+    // second and third order linear combinations (K17...h:323-335)
+    T mxxPyyPzz = M(2, 0, 0) + M(0, 2, 0) + M(0, 0, 2);
+    T mxxMyy = M(2, 0, 0) - M(0, 2, 0);
+    T mxxMzz = M(2, 0, 0) - M(0, 0, 2);
+    T mxxyPyzz = M(2, 1, 0) + M(0, 1, 2);
+    T mxxyMyzz = M(2, 1, 0) - M(0, 1, 2);
+    T mxxzPyyz = M(2, 0, 1) + M(0, 2, 1);
+    T mxxzMyyz = M(2, 0, 1) - M(0, 2, 1);
+    T mxyyPxzz = M(1, 2, 0) + M(1, 0, 2);
+    T mxyyMxzz = M(1, 2, 0) - M(1, 0, 2);
+
+    // velocity gradients times rho (K17...h:347-352), OxxPyyPzz = 1
+    const T Dxy = -T(3) * omega * M(1, 1, 0);
+    const T Dxz = -T(3) * omega * M(1, 0, 1);
+    const T Dyz = -T(3) * omega * M(0, 1, 1);
+    const T dxux = h * (-omega) * (mxxMyy + mxxMzz) + h * T(1) * (M(0, 0, 0) - mxxPyyPzz);
+    const T dyuy = dxux + omega * (T(3) / T(2)) * mxxMyy;
+    const T dzuz = dxux + omega * (T(3) / T(2)) * mxxMzz;
+
+    // second order relaxation with correction (K17...h:375-387)
+    mxxPyyPzz += T(1) * (M(0, 0, 0) - mxxPyyPzz) - T(3) * (T(1) - h * T(1)) * (vx2 * dxux + vy2 * dyuy + vz2 * dzuz);
+    mxxMyy += omega * (-mxxMyy) - T(3) * (T(1) + h * (-omega)) * (vx2 * dxux - vy2 * dyuy);
+    mxxMzz += omega * (-mxxMzz) - T(3) * (T(1) + h * (-omega)) * (vx2 * dxux - vz2 * dzuz);
+    M(0, 1, 1) += omega * (-M(0, 1, 1));
+    M(1, 0, 1) += omega * (-M(1, 0, 1));
+    M(1, 1, 0) += omega * (-M(1, 1, 0));
+
+    // third order with the quartic limiter (K17...h:397-410)
+    T wadj;
+    wadj = r.Oxyz + (T(1) - r.Oxyz) * fabs(M(1, 1, 1)) / (fabs(M(1, 1, 1)) + r.qD);
+    M(1, 1, 1) += wadj * (-M(1, 1, 1));
+    wadj = r.OxyyPxzz + (T(1) - r.OxyyPxzz) * fabs(mxxyPyzz) / (fabs(mxxyPyzz) + r.qP);
+    mxxyPyzz += wadj * (-mxxyPyzz);
+    wadj = r.OxyyMxzz + (T(1) - r.OxyyMxzz) * fabs(mxxyMyzz) / (fabs(mxxyMyzz) + r.qM);
+    mxxyMyzz += wadj * (-mxxyMyzz);
+    wadj = r.OxyyPxzz + (T(1) - r.OxyyPxzz) * fabs(mxxzPyyz) / (fabs(mxxzPyyz) + r.qP);
+    mxxzPyyz += wadj * (-mxxzPyyz);
+    wadj = r.OxyyMxzz + (T(1) - r.OxyyMxzz) * fabs(mxxzMyyz) / (fabs(mxxzMyyz) + r.qM);
+    mxxzMyyz += wadj * (-mxxzMyyz);
+    wadj = r.OxyyPxzz + (T(1) - r.OxyyPxzz) * fabs(mxyyPxzz) / (fabs(mxyyPxzz) + r.qP);
+    mxyyPxzz += wadj * (-mxyyPxzz);
+    wadj = r.OxyyMxzz + (T(1) - r.OxyyMxzz) * fabs(mxyyMxzz) / (fabs(mxyyMxzz) + r.qM);
+    mxyyMxzz += wadj * (-mxyyMxzz);
+
+    // back from the linear combinations (K17...h:424-433)
+    M(2, 0, 0) = c13 * (mxxMyy + mxxMzz + mxxPyyPzz);
+    M(0, 2, 0) = c13 * (-T(2) * mxxMyy + mxxMzz + mxxPyyPzz);
+    M(0, 0, 2) = c13 * (mxxMyy - T(2) * mxxMzz + mxxPyyPzz);
+    M(2, 1, 0) = (mxxyMyzz + mxxyPyzz) * h;
+    M(0, 1, 2) = (-mxxyMyzz + mxxyPyzz) * h;
+    M(2, 0, 1) = (mxxzMyyz + mxxzPyyz) * h;
+    M(0, 2, 1) = (-mxxzMyyz + mxxzPyyz) * h;
+    M(1, 2, 0) = (mxyyMxzz + mxyyPxzz) * h;
+    M(1, 0, 2) = (-mxyyMxzz + mxyyPxzz) * h;
+
+    // post-collision 4th order cumulants: modified equilibrium (K17...h:443-448)
+    const T cm022 = r.neg_iwm * (dyuy + dzuz) * c23 * r.factorA;
+    const T cm202 = r.neg_iwm * (dxux + dzuz) * c23 * r.factorA;
+    const T cm220 = r.neg_iwm * (dyuy + dxux) * c23 * r.factorA;
+    const T cm112 = r.neg_iwm * Dxy * c13 * r.factorB;
+    const T cm121 = r.neg_iwm * Dxz * c13 * r.factorB;
+    const T cm211 = r.neg_iwm * Dyz * c13 * r.factorB;
+    // 5th and 6th order post-collision cumulants are zero
+    const T z = T(0);
+
+    // central moments from post-collision cumulants (K17...h:469-505)
+    M(2, 1, 1) = cm211 + c13 * ((T(3) * M(2, 0, 0) + T(1)) * M(0, 1, 1) + T(6) * M(1, 1, 0) * M(1, 0, 1)) * oneOverRho;
+    M(1, 2, 1) = cm121 + c13 * ((T(3) * M(0, 2, 0) + T(1)) * M(1, 0, 1) + T(6) * M(1, 1, 0) * M(0, 1, 1)) * oneOverRho;
+    M(1, 1, 2) = cm112 + c13 * ((T(3) * M(0, 0, 2) + T(1)) * M(1, 1, 0) + T(6) * M(1, 0, 1) * M(0, 1, 1)) * oneOverRho;
+    M(2, 2, 0) = cm220 + (((M(2, 0, 0) * M(0, 2, 0) + T(2) * M(1, 1, 0) * M(1, 1, 0)) * T(9) + T(3) * (M(2, 0, 0) + M(0, 2, 0))) * oneOverRho - (drho * oneOverRho)) * c19;
+    M(2, 0, 2) = cm202 + (((M(2, 0, 0) * M(0, 0, 2) + T(2) * M(1, 0, 1) * M(1, 0, 1)) * T(9) + T(3) * (M(2, 0, 0) + M(0, 0, 2))) * oneOverRho - (drho * oneOverRho)) * c19;
+    M(0, 2, 2) = cm022 + (((M(0, 0, 2) * M(0, 2, 0) + T(2) * M(0, 1, 1) * M(0, 1, 1)) * T(9) + T(3) * (M(0, 0, 2) + M(0, 2, 0))) * oneOverRho - (drho * oneOverRho)) * c19;
+
+    const T t122 = c13 * (T(3) * (M(0, 0, 2) * M(1, 2, 0) + M(0, 2, 0) * M(1, 0, 2) + T(4) * M(0, 1, 1) * M(1, 1, 1) + T(2) * (M(1, 0, 1) * M(0, 2, 1) + M(1, 1, 0) * M(0, 1, 2))) + (M(1, 2, 0) + M(1, 0, 2))) * oneOverRho;
+    const T t212 = c13 * (T(3) * (M(0, 0, 2) * M(2, 1, 0) + M(2, 0, 0) * M(0, 1, 2) + T(4) * M(1, 0, 1) * M(1, 1, 1) + T(2) * (M(0, 1, 1) * M(2, 0, 1) + M(1, 1, 0) * M(1, 0, 2))) + (M(2, 1, 0) + M(0, 1, 2))) * oneOverRho;
+    const T t221 = c13 * (T(3) * (M(2, 0, 0) * M(0, 2, 1) + M(0, 2, 0) * M(2, 0, 1) + T(4) * M(1, 1, 0) * M(1, 1, 1) + T(2) * (M(1, 0, 1) * M(1, 2, 0) + M(0, 1, 1) * M(2, 1, 0))) + (M(0, 2, 1) + M(2, 0, 1))) * oneOverRho;
+    M(1, 2, 2) = EXACT ? z + t122 : t122;
+    M(2, 1, 2) = EXACT ? z + t212 : t212;
+    M(2, 2, 1) = EXACT ? z + t221 : t221;
+
+    const T b222 = (-T(4) * M(1, 1, 1) * M(1, 1, 1) - (M(2, 0, 0) * M(0, 2, 2) + M(0, 2, 0) * M(2, 0, 2) + M(0, 0, 2) * M(2, 2, 0))
+                    - T(4) * (M(0, 1, 1) * M(2, 1, 1) + M(1, 0, 1) * M(1, 2, 1) + M(1, 1, 0) * M(1, 1, 2))
+                    - T(2) * (M(1, 2, 0) * M(1, 0, 2) + M(2, 1, 0) * M(0, 1, 2) + M(2, 0, 1) * M(0, 2, 1))) * oneOverRho
+                 + (T(4) * (M(1, 0, 1) * M(1, 0, 1) * M(0, 2, 0) + M(0, 1, 1) * M(0, 1, 1) * M(2, 0, 0) + M(1, 1, 0) * M(1, 1, 0) * M(0, 0, 2))
+                    + T(2) * (M(2, 0, 0) * M(0, 2, 0) * M(0, 0, 2)) + T(16) * M(1, 1, 0) * M(1, 0, 1) * M(0, 1, 1)) * oneOverRho * oneOverRho
+                 - c13 * (M(0, 2, 2) + M(2, 0, 2) + M(2, 2, 0)) * oneOverRho - c19 * (M(2, 0, 0) + M(0, 2, 0) + M(0, 0, 2)) * oneOverRho
+                 + (T(2) * (M(1, 0, 1) * M(1, 0, 1) + M(0, 1, 1) * M(0, 1, 1) + M(1, 1, 0) * M(1, 1, 0))
+                    + (M(0, 0, 2) * M(0, 2, 0) + M(0, 0, 2) * M(2, 0, 0) + M(0, 2, 0) * M(2, 0, 0)) + c13 * (M(0, 0, 2) + M(0, 2, 0) + M(2, 0, 0))) * oneOverRho * oneOverRho * c23
+                 + c127 * ((drho * drho - drho) * oneOverRho * oneOverRho);
+    M(2, 2, 2) = EXACT ? z - b222 : -b222;
+
+    // first moments change sign (K17...h:512-514)
+    M(1, 0, 0) = -M(1, 0, 0);
+    M(0, 1, 0) = -M(0, 1, 0);
+    M(0, 0, 1) = -M(0, 0, 1);
+
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            if (b == 0 && c == 0)
+                bwd_k(M(0, 0, 0), M(1, 0, 0), M(2, 0, 0), vx, vx2, T(1), T(1));
+            else if (b == 2 && c == 2)
+                bwd_k(M(0, 2, 2), M(1, 2, 2), M(2, 2, 2), vx, vx2, T(9), T(1) / T(9));
+            else if ((b == 2 && c == 0) || (b == 0 && c == 2))
+                bwd_k(M(0, b, c), M(1, b, c), M(2, b, c), vx, vx2, T(3), T(1) / T(3));
+            else
+                bwd(M(0, b, c), M(1, b, c), M(2, b, c), vx, vx2);
+        }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            if (c == 1)
+                bwd(M(a, 0, 1), M(a, 1, 1), M(a, 2, 1), vy, vy2);
+            else
+                bwd_k(M(a, 0, c), M(a, 1, c), M(a, 2, c), vy, vy2, kinv_y<T>(a, c), k_y<T>(a, c));
+        }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+            bwd_k(M(a, b, 0), M(a, b, 1), M(a, b, 2), vz, vz2, kinv_z<T>(a, b), k_z<T>(a, b));
+#undef M
+
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        f[d] = m[m3(d)];
+    drho_out = drho;
+    vx_out = vx;
+    vy_out = vy;
+    vz_out = vz;
+}
+
+} // namespace vfb

@@ -1,0 +1,608 @@
+// Device kernels of the time step, templated over storage type, parity and features.
+//
+// This header is compiled twice into the library: once with contraction off (-fmad=false,
+// namespace vfb::exact) and once with the default FMA contraction (namespace vfb::fast). The
+// first reproduces the reference's operation-by-operation rounding; the second is the default.
+//
+// Every direction loop is fully unrolled, so direction-dependent constants (plane, shift class,
+// weight, inverse) fold and the 27 populations stay in registers.
+#pragma once
+#include <cstdint>
+
+#include "k17.cuh"
+#include "storage.cuh"
+
+#ifndef VFB_NS
+#error "VFB_NS must name the compilation variant"
+#endif
+
+namespace vfb {
+namespace VFB_NS {
+
+// ---------------------------------------------------------------------------------------------
+// argument packs
+// ---------------------------------------------------------------------------------------------
+template <class C>
+struct ListCollideArgs {
+    void *dist;                 // distributions.f[0]
+    uint64_t n;                 // numberOfNodes (plane stride)
+    const uint32_t *nbx, *nby, *nbz;
+    const uint32_t *idx;        // fluid node indices
+    uint32_t n_idx;
+    K17Rates<C> rates;
+    C fx, fy, fz;               // forces * 1/2 * 2^-level (RunCollision.cuh:112-114)
+    C force0, force1, force2;   // forces, for the body-force variant
+    C force_factor;             // 2^-level
+    C *bfx, *bfy, *bfz;         // per-node body force (reset after use)
+    C *rho, *vx, *vy, *vz;      // macroscopic outputs
+};
+
+template <class C>
+struct BoxCollideArgs {
+    void *dist;                 // 27 planes of `pitch` elements, node k = x + nx (y + ny z)
+    uint64_t pitch;
+    int nx, ny, nz;
+    int periodic_x, periodic_y, periodic_z;
+    const uint8_t *mask;        // optional: nonzero = collide (fluid); nullptr = every node
+    K17Rates<C> rates;
+    C fx, fy, fz;
+    double *energy_partials;    // optional: per block {sum(1+drho), sum(0.5 (1+drho) u^2)}
+    C *rho, *vx, *vy, *vz;      // optional macroscopic outputs
+};
+
+struct BCArgs {
+    void *dist;
+    uint64_t n;
+    const uint32_t *nbx, *nby, *nbz;
+    const int32_t *k;           // BC node indices
+    const void *q27;            // q27[dir * nbc + i], compute type
+    uint32_t nbc;
+    const void *ux, *uy, *uz;   // wall / inlet velocity per BC node, compute type
+    double omega;
+};
+
+struct PressureArgs {
+    void *dist;
+    uint64_t n;
+    const uint32_t *nbx, *nby, *nbz;
+    const int32_t *k, *kN;
+    const void *rho_bc;
+    uint32_t nbc;
+    int direction;
+};
+
+// ---------------------------------------------------------------------------------------------
+// addressing
+// ---------------------------------------------------------------------------------------------
+
+// ListIndices (KernelUtilities.h:221-250) by shift class: bit0 x+1, bit1 y+1, bit2 z+1
+__device__ __forceinline__ void list_nodes(uint32_t k, const uint32_t *__restrict__ nbx, const uint32_t *__restrict__ nby,
+                                           const uint32_t *__restrict__ nbz, uint32_t (&nodes)[8])
+{
+    const uint32_t kx = __ldg(nbx + k), ky = __ldg(nby + k), kz = __ldg(nbz + k);
+    const uint32_t kxy = __ldg(nby + kx);
+    nodes[0] = k;
+    nodes[1] = kx;
+    nodes[2] = ky;
+    nodes[3] = kxy;
+    nodes[4] = kz;
+    nodes[5] = __ldg(nbz + kx);
+    nodes[6] = __ldg(nbz + ky);
+    nodes[7] = __ldg(nbz + kxy);
+}
+
+template <class S, bool EVEN>
+__device__ __forceinline__ void gather_pre(const S *__restrict__ base, uint64_t n, const uint32_t (&nodes)[8],
+                                           typename Codec<S>::compute (&f)[27])
+{
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        f[d] = Codec<S>::load(base + (uint64_t)plane<EVEN>(d) * n + nodes[shift_class(d)], d);
+}
+
+// setPostCollisionDistribution (KernelUtilities.h:350): the slot of d receives f[inv d]
+template <class S, bool EVEN>
+__device__ __forceinline__ void scatter_post(S *__restrict__ base, uint64_t n, const uint32_t (&nodes)[8],
+                                             const typename Codec<S>::compute (&f)[27])
+{
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        Codec<S>::store(base + (uint64_t)plane<EVEN>(d) * n + nodes[shift_class(d)], f[inv(d)], d);
+}
+
+// getPostCollisionDistribution (KernelUtilities.h:283): post[d] leaves the node along d
+template <class S, bool EVEN>
+__device__ __forceinline__ void gather_post(const S *base, uint64_t n, const uint32_t (&nodes)[8],
+                                            typename Codec<S>::compute (&post)[27])
+{
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        post[d] = Codec<S>::load(base + (uint64_t)plane<EVEN>(inv(d)) * n + nodes[shift_class(inv(d))], d);
+}
+
+// ---------------------------------------------------------------------------------------------
+// collision + streaming, reference layout (RunCollision.cuh:75-143)
+// ---------------------------------------------------------------------------------------------
+template <class S, bool EXACT, bool EVEN, bool WRITE_MACRO, bool BODY_FORCE>
+__global__ void __launch_bounds__(128) k17_list_kernel(ListCollideArgs<typename Codec<S>::compute> a)
+{
+    using C = typename Codec<S>::compute;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n_idx)
+        return;
+    const uint32_t k = __ldg(a.idx + i);
+    C fx = a.fx, fy = a.fy, fz = a.fz;
+    if (BODY_FORCE) {
+        fx = (a.force0 + a.bfx[k]) * C(0.5) * a.force_factor;
+        fy = (a.force1 + a.bfy[k]) * C(0.5) * a.force_factor;
+        fz = (a.force2 + a.bfz[k]) * C(0.5) * a.force_factor;
+        a.bfx[k] = C(0);
+        a.bfy[k] = C(0);
+        a.bfz[k] = C(0);
+    }
+    uint32_t nodes[8];
+    list_nodes(k, a.nbx, a.nby, a.nbz, nodes);
+    S *base = static_cast<S *>(a.dist);
+    C f[27];
+    gather_pre<S, EVEN>(base, a.n, nodes, f);
+    C drho, vx, vy, vz;
+    k17_collide<C, EXACT>(f, a.rates, fx, fy, fz, drho, vx, vy, vz);
+    if (WRITE_MACRO) {
+        a.vx[k] = vx;
+        a.vy[k] = vy;
+        a.vz[k] = vz;
+        a.rho[k] = drho;
+    }
+    scatter_post<S, EVEN>(base, a.n, nodes, f);
+}
+
+// ---------------------------------------------------------------------------------------------
+// collision + streaming on a structured box: neighbours by index arithmetic, one node per
+// thread, x fastest so every direction plane is read and written by whole warps in order.
+// ---------------------------------------------------------------------------------------------
+template <class S, bool EXACT, bool EVEN, bool MASK, bool ENERGY, bool WRITE_MACRO>
+__global__ void __launch_bounds__(128) k17_box_kernel(BoxCollideArgs<typename Codec<S>::compute> a)
+{
+    using C = typename Codec<S>::compute;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    const bool active_x = x < a.nx;
+    const uint64_t row = (uint64_t)a.nx * ((uint64_t)y + (uint64_t)a.ny * (uint64_t)z);
+    const uint32_t k = (uint32_t)(row + (uint64_t)x);
+    bool active = active_x;
+    if (MASK && active)
+        active = __ldg(a.mask + k) != 0;
+
+    C drho = C(0), vx = C(0), vy = C(0), vz = C(0);
+    if (active) {
+        // +1 neighbours, wrapping on periodic axes (the mask keeps walled boxes inside)
+        const int xp = (x + 1 < a.nx) ? x + 1 : (a.periodic_x ? 0 : x);
+        const int yp = (y + 1 < a.ny) ? y + 1 : (a.periodic_y ? 0 : y);
+        const int zp = (z + 1 < a.nz) ? z + 1 : (a.periodic_z ? 0 : z);
+        const uint32_t sx = (uint32_t)(xp - x);
+        const uint32_t sy = (uint32_t)((yp - y) * a.nx);
+        const uint32_t sz = (uint32_t)((int64_t)(zp - z) * a.nx * a.ny);
+        uint32_t nodes[8];
+        nodes[0] = k;
+        nodes[1] = k + sx;
+        nodes[2] = k + sy;
+        nodes[3] = k + sx + sy;
+        nodes[4] = k + sz;
+        nodes[5] = k + sx + sz;
+        nodes[6] = k + sy + sz;
+        nodes[7] = k + sx + sy + sz;
+        S *base = static_cast<S *>(a.dist);
+        C f[27];
+        gather_pre<S, EVEN>(base, a.pitch, nodes, f);
+        k17_collide<C, EXACT>(f, a.rates, a.fx, a.fy, a.fz, drho, vx, vy, vz);
+        if (WRITE_MACRO) {
+            a.rho[k] = drho;
+            a.vx[k] = vx;
+            a.vy[k] = vy;
+            a.vz[k] = vz;
+        }
+        scatter_post<S, EVEN>(base, a.pitch, nodes, f);
+    }
+
+    if (ENERGY) {
+        // FP64 block partials of mass and kinetic energy, fixed reduction order
+        double m = active ? 1.0 + (double)drho : 0.0;
+        double e = active ? 0.5 * (1.0 + (double)drho) * ((double)vx * vx + (double)vy * vy + (double)vz * vz) : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            m += __shfl_down_sync(0xffffffffu, m, o);
+            e += __shfl_down_sync(0xffffffffu, e, o);
+        }
+        __shared__ double sm[2][4];
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (lane == 0) {
+            sm[0][warp] = m;
+            sm[1][warp] = e;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double mm = 0.0, ee = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+                mm += sm[0][w];
+                ee += sm[1][w];
+            }
+            const uint64_t b = blockIdx.x + (uint64_t)gridDim.x * (blockIdx.y + (uint64_t)gridDim.y * blockIdx.z);
+            a.energy_partials[2 * b] = mm;
+            a.energy_partials[2 * b + 1] = ee;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// boundary conditions (one thread per BC node)
+// ---------------------------------------------------------------------------------------------
+template <class C>
+__device__ __forceinline__ bool q_active(C q)
+{
+    return q >= C(0) && q <= C(1);
+}
+
+// NoSlipBounceBack_Device (NoSlip/NoSlipBounceBack.cu:44-179) and VelocityBounceBack_Device
+// (Velocity/VelocityBounceBack.cu:44-188): for every link with q in [0,1] the population leaving
+// along d comes back as inv(d) into the slot the node reads on the next step; the velocity
+// variant adds 6 w (c_inv(d) . u_w) (coefficients 4/9, 1/9, 1/36).
+template <class S, bool EVEN, bool VELOCITY>
+__global__ void __launch_bounds__(128) bc_bounce_back_kernel(BCArgs a)
+{
+    using C = typename Codec<S>::compute;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nbc)
+        return;
+    const uint32_t node = (uint32_t)a.k[i];
+    uint32_t nodes[8];
+    list_nodes(node, a.nbx, a.nby, a.nbz, nodes);
+    S *base = static_cast<S *>(a.dist);
+    C post[27];
+    gather_post<S, EVEN>(base, a.n, nodes, post);
+    const C *q27 = static_cast<const C *>(a.q27);
+    C ux = C(0), uy = C(0), uz = C(0);
+    if (VELOCITY) {
+        ux = static_cast<const C *>(a.ux)[i];
+        uy = static_cast<const C *>(a.uy)[i];
+        uz = static_cast<const C *>(a.uz)[i];
+    }
+#pragma unroll
+    for (int d = 1; d < 27; ++d) {
+        const C q = q27[(uint64_t)d * a.nbc + i];
+        if (q_active(q)) {
+            const int e = inv(d);
+            C v = post[d];
+            if (VELOCITY) {
+                const C coef = order(d) == 1 ? C(4) / C(9) : order(d) == 2 ? C(1) / C(9) : C(1) / C(36);
+                C cu = C(0);
+                // c_e . u spelled as the reference: signed sum x, y, z
+                {
+                    bool first = true;
+                    if (cx(e) != 0) { cu = cx(e) > 0 ? ux : -ux; first = false; }
+                    if (cy(e) != 0) { cu = first ? (cy(e) > 0 ? uy : -uy) : (cy(e) > 0 ? cu + uy : cu - uy); first = false; }
+                    if (cz(e) != 0) { cu = first ? (cz(e) > 0 ? uz : -uz) : (cz(e) > 0 ? cu + uz : cu - uz); }
+                }
+                v = v + coef * cu;
+            }
+            // next parity: slot of direction e at its own read node
+            Codec<S>::store(base + (uint64_t)plane<!EVEN>(e) * a.n + nodes[shift_class(e)], v, e);
+        }
+    }
+}
+
+template <int D, class C>
+__device__ __forceinline__ C cdot(C ux, C uy, C uz)
+{
+    C s = C(0);
+    bool first = true;
+    if (cx(D) != 0) { s = cx(D) > 0 ? ux : -ux; first = false; }
+    if (cy(D) != 0) { s = first ? (cy(D) > 0 ? uy : -uy) : (cy(D) > 0 ? s + uy : s - uy); first = false; }
+    if (cz(D) != 0) { s = first ? (cz(D) > 0 ? uz : -uz) : (cz(D) > 0 ? s + uz : s - uz); }
+    return s;
+}
+
+__device__ __forceinline__ int dir_sum_term(int d, int axis) { return axis == 0 ? cx(d) : axis == 1 ? cy(d) : cz(d); }
+
+// signed sum c_d . u with a runtime-unrolled d
+template <class C>
+__device__ __forceinline__ C cdot_rt(int d, C ux, C uy, C uz)
+{
+    C s = C(0);
+    bool first = true;
+    if (cx(d) != 0) { s = cx(d) > 0 ? ux : -ux; first = false; }
+    if (cy(d) != 0) { s = first ? (cy(d) > 0 ? uy : -uy) : (cy(d) > 0 ? s + uy : s - uy); first = false; }
+    if (cz(d) != 0) { s = first ? (cz(d) > 0 ? uz : -uz) : (cz(d) > 0 ? s + uz : s - uz); }
+    return s;
+}
+
+// NoSlipInterpolatedCompressible_Device (NoSlip/NoSlipInterpolatedCompressible.cu:44-381) and
+// VelocityInterpolatedCompressible_Device (Velocity/VelocityInterpolatedCompressible.cu:44-420),
+// with the helper formulas of KernelUtilities.h:171-197
+template <class S, bool EVEN, bool VELOCITY>
+__global__ void __launch_bounds__(128) bc_interpolated_kernel(BCArgs a)
+{
+    using C = typename Codec<S>::compute;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nbc)
+        return;
+    const uint32_t node = (uint32_t)a.k[i];
+    uint32_t nodes[8];
+    list_nodes(node, a.nbx, a.nby, a.nbz, nodes);
+    S *base = static_cast<S *>(a.dist);
+    C p[27];
+    gather_post<S, EVEN>(base, a.n, nodes, p);
+    // plain-sum density and grouped momenta (NoSlipInterpolatedCompressible.cu:134-153)
+    const C drho = p[21] + p[20] + p[19] + p[22] + p[25] + p[24] + p[23] + p[26] + p[17] + p[18] + p[15] + p[16] + p[13]
+                 + p[14] + p[11] + p[12] + p[9] + p[10] + p[7] + p[8] + p[5] + p[6] + p[3] + p[4] + p[1] + p[2] + p[0];
+    const C r = C(1) + drho;
+    const C vx = (((((p[21] - p[24]) - (p[20] - p[25])) + ((p[19] - p[26]) - (p[22] - p[23]))) + ((p[13] - p[14]) + (p[11] - p[12])))
+                  + ((p[9] - p[10]) + (p[7] - p[8]))) + (p[1] - p[2]);
+    const C vy = (((((-(p[21] - p[24])) + (p[20] - p[25])) + ((p[19] - p[26]) - (p[22] - p[23]))) + ((p[17] - p[18]) + (p[15] - p[16])))
+                  + ((-(p[9] - p[10])) + (p[7] - p[8]))) + (p[3] - p[4]);
+    const C vz = (((((p[21] - p[24]) + (p[20] - p[25])) + ((p[19] - p[26]) + (p[22] - p[23]))) + ((-(p[17] - p[18])) + (p[15] - p[16])))
+                  + ((p[11] - p[12]) - (p[13] - p[14]))) + (p[5] - p[6]);
+    const C ux1 = vx / r, uy1 = vy / r, uz1 = vz / r;
+    const C cu_sq = C(1.5) * (ux1 * ux1 + uy1 * uy1 + uz1 * uz1) * (C(1) + drho);
+    const C omega = (C)a.omega;
+    const C *q27 = static_cast<const C *>(a.q27);
+    C bx = C(0), by = C(0), bz = C(0);
+    if (VELOCITY) {
+        bx = static_cast<const C *>(a.ux)[i];
+        by = static_cast<const C *>(a.uy)[i];
+        bz = static_cast<const C *>(a.uz)[i];
+    }
+#pragma unroll
+    for (int d = 1; d < 27; ++d) {
+        const C q = q27[(uint64_t)d * a.nbc + i];
+        if (q_active(q)) {
+            const C w = weight_t<C>(d);
+            const C vel = cdot_rt<C>(d, ux1, uy1, uz1);
+            const C feq = w * (drho + C(4.5) * vel * vel * (C(1) + drho) - cu_sq);
+            const C f = p[d], fi = p[inv(d)];
+            C v;
+            if (VELOCITY) {
+                const C vbc = cdot_rt<C>(d, bx, by, bz);
+                v = (C(1) - q) / (C(1) + q) * (f - fi + (f + fi - C(2) * feq * omega) / (C(1) - omega)) * C(0.5)
+                  + (q * (f + fi) - C(6) * w * vbc) / (C(1) + q);
+            } else {
+                v = (C(1) - q) / (C(1) + q) * (f - fi + (f + fi - C(2) * feq * omega) / (C(1) - omega)) * C(0.5)
+                  + (q * (f + fi)) / (C(1) + q);
+            }
+            const int e = inv(d);
+            Codec<S>::store(base + (uint64_t)plane<!EVEN>(e) * a.n + nodes[shift_class(e)], v, e);
+        }
+    }
+}
+
+// feq - w of one direction in the form of the init and pressure kernels
+template <class C>
+__device__ __forceinline__ C feq_shifted(int d, C drho, C ux, C uy, C uz, C cusq)
+{
+    if (d == 0)
+        return weight_t<C>(0) * (drho - (drho + C(1)) * cusq);
+    const C cu = cdot_rt<C>(d, ux, uy, uz);
+    return weight_t<C>(d) * (drho + (drho + C(1)) * (C(3) * cu + C(4.5) * cu * cu - cusq));
+}
+
+// PressureNonEquilibriumCompressible_Device (Pressure/PressureNonEquilibriumCompressible.cu:45-314).
+// The reference's __syncthreads() between the neighbour reads and the writes (:174) sits in
+// divergent code and orders nothing that needs ordering (no thread writes a slot another thread
+// of the launch reads), so it has no counterpart here.
+template <class S, bool EVEN>
+__global__ void __launch_bounds__(128) bc_pressure_neq_kernel(PressureArgs a)
+{
+    using C = typename Codec<S>::compute;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nbc)
+        return;
+    uint32_t nn[8], nk[8];
+    list_nodes((uint32_t)a.kN[i], a.nbx, a.nby, a.nbz, nn);
+    list_nodes((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, nk);
+    S *base = static_cast<S *>(a.dist);
+    C f[27];
+    gather_pre<S, EVEN>(base, a.n, nn, f);
+    const C drho1 = density_pyramid(f);
+    const C inv_rho = C(1) / (drho1 + C(1));
+    const C vx = momentum_x(f) * inv_rho, vy = momentum_y(f) * inv_rho, vz = momentum_z(f) * inv_rho;
+    const C cusq = C(1.5) * (vx * vx + vy * vy + vz * vz);
+    const C rbc = static_cast<const C *>(a.rho_bc)[i];
+    const int axis = cx(a.direction) != 0 ? 0 : (cy(a.direction) != 0 ? 1 : 2);
+    const int sgn = axis == 0 ? cx(a.direction) : (axis == 1 ? cy(a.direction) : cz(a.direction));
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        C v = f[d] - feq_shifted<C>(d, drho1, vx, vy, vz, cusq);
+        v = v + feq_shifted<C>(d, rbc, vx, vy, vz, cusq);
+        const int c = axis == 0 ? cx(d) : (axis == 1 ? cy(d) : cz(d));
+        if (c != sgn)
+            Codec<S>::store(base + (uint64_t)plane<EVEN>(d) * a.n + nk[shift_class(d)], v, d);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// initialisation and output
+// ---------------------------------------------------------------------------------------------
+
+// InitNavierStokesCompressible_Device (InitNavierStokesCompressible_Device.cu:44-215):
+// equilibrium f - w of the node's (rho, u) into the node's read slots of one parity
+template <class S, bool EVEN>
+__global__ void __launch_bounds__(128) init_list_kernel(void *dist, uint64_t n, const uint32_t *nbx, const uint32_t *nby,
+                                                        const uint32_t *nbz, const uint32_t *geo, const void *rho,
+                                                        const void *ux, const void *uy, const void *uz)
+{
+    using C = typename Codec<S>::compute;
+    const uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (k >= n)
+        return;
+    const uint32_t g = geo[k];
+    if (g == kGeoSolid || g == kGeoVoid)
+        return;
+    uint32_t nodes[8];
+    list_nodes((uint32_t)k, nbx, nby, nbz, nodes);
+    const C drho = static_cast<const C *>(rho)[k];
+    const C vx = static_cast<const C *>(ux)[k], vy = static_cast<const C *>(uy)[k], vz = static_cast<const C *>(uz)[k];
+    const C cu_sq = C(1.5) * (vx * vx + vy * vy + vz * vz);
+    S *base = static_cast<S *>(dist);
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        C v;
+        if (d == 0) {
+            v = weight_t<C>(0) * (drho - cu_sq * (C(1) + drho));
+        } else {
+            const C cu = cdot_rt<C>(d, vx, vy, vz);
+            v = weight_t<C>(d) * (drho + (C(1) + drho) * (C(3) * cu + C(4.5) * cu * cu - cu_sq));
+        }
+        Codec<S>::store(base + (uint64_t)plane<EVEN>(d) * n + nodes[shift_class(d)], v, d);
+    }
+}
+
+// the same equilibrium initialisation on a structured box (every node, or the masked ones)
+template <class S, bool EVEN>
+__global__ void __launch_bounds__(128) init_box_kernel(BoxCollideArgs<typename Codec<S>::compute> a, const void *rho,
+                                                       const void *ux, const void *uy, const void *uz)
+{
+    using C = typename Codec<S>::compute;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y, z = blockIdx.z;
+    if (x >= a.nx)
+        return;
+    const uint32_t k = (uint32_t)((uint64_t)a.nx * ((uint64_t)y + (uint64_t)a.ny * z) + x);
+    if (a.mask && a.mask[k] == 0)
+        return;
+    const int xp = (x + 1 < a.nx) ? x + 1 : (a.periodic_x ? 0 : x);
+    const int yp = (y + 1 < a.ny) ? y + 1 : (a.periodic_y ? 0 : y);
+    const int zp = (z + 1 < a.nz) ? z + 1 : (a.periodic_z ? 0 : z);
+    const uint32_t sx = (uint32_t)(xp - x), sy = (uint32_t)((yp - y) * a.nx), sz = (uint32_t)((int64_t)(zp - z) * a.nx * a.ny);
+    const uint32_t nodes[8] = { k, k + sx, k + sy, k + sx + sy, k + sz, k + sx + sz, k + sy + sz, k + sx + sy + sz };
+    const C drho = static_cast<const C *>(rho)[k];
+    const C vx = static_cast<const C *>(ux)[k], vy = static_cast<const C *>(uy)[k], vz = static_cast<const C *>(uz)[k];
+    const C cu_sq = C(1.5) * (vx * vx + vy * vy + vz * vz);
+    S *base = static_cast<S *>(a.dist);
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        C v;
+        if (d == 0) {
+            v = weight_t<C>(0) * (drho - cu_sq * (C(1) + drho));
+        } else {
+            const C cu = cdot_rt<C>(d, vx, vy, vz);
+            v = weight_t<C>(d) * (drho + (C(1) + drho) * (C(3) * cu + C(4.5) * cu * cu - cu_sq));
+        }
+        Codec<S>::store(base + (uint64_t)plane<EVEN>(d) * a.pitch + nodes[shift_class(d)], v, d);
+    }
+}
+
+// calculateMacroscopicQuantitiesCompressible_device (PostProcessor/MacroscopicQuantities.cu:194)
+template <class S, bool EVEN>
+__global__ void __launch_bounds__(128) macros_list_kernel(const void *dist, uint64_t n, const uint32_t *nbx,
+                                                          const uint32_t *nby, const uint32_t *nbz, const uint32_t *geo,
+                                                          void *rho_o, void *vx_o, void *vy_o, void *vz_o, void *p_o)
+{
+    using C = typename Codec<S>::compute;
+    const uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (k >= n)
+        return;
+    C *rho = static_cast<C *>(rho_o), *vx = static_cast<C *>(vx_o), *vy = static_cast<C *>(vy_o), *vz = static_cast<C *>(vz_o);
+    C *press = static_cast<C *>(p_o);
+    if (press)
+        press[k] = C(0);
+    rho[k] = C(0);
+    vx[k] = C(0);
+    vy[k] = C(0);
+    vz[k] = C(0);
+    if (geo[k] != kGeoFluid)
+        return;
+    uint32_t nodes[8];
+    list_nodes((uint32_t)k, nbx, nby, nbz, nodes);
+    C f[27];
+    gather_pre<S, EVEN>(static_cast<const S *>(dist), n, nodes, f);
+    const C r = density_pyramid(f);
+    const C ux = momentum_x(f) / (r + C(1)), uy = momentum_y(f) / (r + C(1)), uz = momentum_z(f) / (r + C(1));
+    rho[k] = r;
+    vx[k] = ux;
+    vy[k] = uy;
+    vz[k] = uz;
+    if (press) {
+        // getPressure (MacroscopicQuantities.h:139)
+        press[k] = (f[1] + f[2] + f[3] + f[4] + f[5] + f[6]
+                    + C(2) * (f[7] + f[8] + f[9] + f[10] + f[11] + f[12] + f[13] + f[14] + f[15] + f[16] + f[17] + f[18])
+                    + C(3) * (f[19] + f[22] + f[21] + f[20] + f[23] + f[26] + f[25] + f[24])
+                    - r - (ux * ux + uy * uy + uz * uz) * (C(1) + r)) * C(0.5) + r;
+    }
+}
+
+// macroscopic fields of a structured box, written in compute type, from the pre-collision state
+template <class S, bool EVEN>
+__global__ void __launch_bounds__(128) macros_box_kernel(BoxCollideArgs<typename Codec<S>::compute> a)
+{
+    using C = typename Codec<S>::compute;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y, z = blockIdx.z;
+    if (x >= a.nx)
+        return;
+    const uint32_t k = (uint32_t)((uint64_t)a.nx * ((uint64_t)y + (uint64_t)a.ny * z) + x);
+    if (a.mask && a.mask[k] == 0) {
+        a.rho[k] = C(0);
+        a.vx[k] = C(0);
+        a.vy[k] = C(0);
+        a.vz[k] = C(0);
+        return;
+    }
+    const int xp = (x + 1 < a.nx) ? x + 1 : (a.periodic_x ? 0 : x);
+    const int yp = (y + 1 < a.ny) ? y + 1 : (a.periodic_y ? 0 : y);
+    const int zp = (z + 1 < a.nz) ? z + 1 : (a.periodic_z ? 0 : z);
+    const uint32_t sx = (uint32_t)(xp - x), sy = (uint32_t)((yp - y) * a.nx), sz = (uint32_t)((int64_t)(zp - z) * a.nx * a.ny);
+    const uint32_t nodes[8] = { k, k + sx, k + sy, k + sx + sy, k + sz, k + sx + sz, k + sy + sz, k + sx + sy + sz };
+    C f[27];
+    gather_pre<S, EVEN>(static_cast<const S *>(a.dist), a.pitch, nodes, f);
+    const C r = density_pyramid(f);
+    a.rho[k] = r;
+    a.vx[k] = momentum_x(f) / (r + C(1));
+    a.vy[k] = momentum_y(f) / (r + C(1));
+    a.vz[k] = momentum_z(f) / (r + C(1));
+}
+
+// FP64 mass and kinetic energy over a node list: per-block partials in a fixed order
+template <class S, bool EVEN>
+__global__ void __launch_bounds__(256) energy_list_kernel(const void *dist, uint64_t n, const uint32_t *nbx,
+                                                          const uint32_t *nby, const uint32_t *nbz, const uint32_t *idx,
+                                                          uint32_t n_idx, double *partials)
+{
+    using C = typename Codec<S>::compute;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double m = 0.0, e = 0.0;
+    if (i < n_idx) {
+        uint32_t nodes[8];
+        list_nodes(__ldg(idx + i), nbx, nby, nbz, nodes);
+        C f[27];
+        gather_pre<S, EVEN>(static_cast<const S *>(dist), n, nodes, f);
+        const C r = density_pyramid(f);
+        const C inv_rho = C(1) / (r + C(1));
+        const double ux = momentum_x(f) * inv_rho, uy = momentum_y(f) * inv_rho, uz = momentum_z(f) * inv_rho;
+        m = 1.0 + (double)r;
+        e = 0.5 * (1.0 + (double)r) * (ux * ux + uy * uy + uz * uz);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        m += __shfl_down_sync(0xffffffffu, m, o);
+        e += __shfl_down_sync(0xffffffffu, e, o);
+    }
+    __shared__ double sm[2][8];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        sm[0][warp] = m;
+        sm[1][warp] = e;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double mm = 0.0, ee = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            mm += sm[0][w];
+            ee += sm[1][w];
+        }
+        partials[2 * blockIdx.x] = mm;
+        partials[2 * blockIdx.x + 1] = ee;
+    }
+}
+
+} // namespace VFB_NS
+} // namespace vfb

@@ -1,0 +1,71 @@
+// Host-side launch layer between the C ABI (abi.cu) and the device kernels (kernels.cuh).
+//
+// The kernels are compiled in one translation unit per (arithmetic variant, storage type);
+// each unit defines Launchers<S> of its variant namespace. abi.cu dispatches on the runtime
+// storage and arithmetic choice.
+#pragma once
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "vfb.h"
+
+namespace vfb {
+
+// a structured box as the kernels see it
+struct BoxState {
+    void *dist;
+    uint64_t pitch;               // elements per direction plane
+    int nx, ny, nz;
+    int periodic_x, periodic_y, periodic_z;
+    const uint8_t *mask;          // device, nullable
+    double omega;
+    double fx, fy, fz;            // half acceleration
+    double lim[3];
+};
+
+// block shape of the box kernels: x extent of a block (multiple of 32, at most 128)
+inline int box_block_x(int nx)
+{
+    int b = ((nx + 31) / 32) * 32;
+    return b > 128 ? 128 : b;
+}
+inline uint64_t box_blocks(const BoxState &b)
+{
+    const int bx = box_block_x(b.nx);
+    return (uint64_t)((b.nx + bx - 1) / bx) * (uint64_t)b.ny * (uint64_t)b.nz;
+}
+
+#define VFB_DECLARE_LAUNCHERS                                                                                        \
+    template <class S>                                                                                               \
+    struct Launchers {                                                                                               \
+        static cudaError_t k17_list(const vfb_level *L, const uint32_t *idx, uint32_t n, int tmpl, cudaStream_t s); \
+        static cudaError_t bc(const vfb_level *L, const vfb_bc *bc, int kind, cudaStream_t s);                     \
+        static cudaError_t pressure(const vfb_level *L, const vfb_directional_bc *bc, cudaStream_t s);             \
+        static cudaError_t init_list(const vfb_level *L, cudaStream_t s);                                          \
+        static cudaError_t macros_list(const vfb_level *L, cudaStream_t s);                                        \
+        static cudaError_t energy_list(const vfb_level *L, const uint32_t *idx, uint32_t n, double *partials,     \
+                                       cudaStream_t s);                                                            \
+        static cudaError_t box_collide(const BoxState &b, bool even, double *partials, cudaStream_t s);            \
+        static cudaError_t box_init(const BoxState &b, bool even, const void *rho, const void *ux, const void *uy, \
+                                    const void *uz, cudaStream_t s);                                               \
+        static cudaError_t box_macros(const BoxState &b, bool even, void *rho, void *ux, void *uy, void *uz,       \
+                                      cudaStream_t s);                                                             \
+    };
+
+// BC kinds of Launchers::bc
+enum BCKind : int { kNoSlipBB = 0, kNoSlipInterp = 1, kVelocityBB = 2, kVelocityInterp = 3 };
+
+namespace fast {
+VFB_DECLARE_LAUNCHERS
+}
+namespace exact {
+VFB_DECLARE_LAUNCHERS
+}
+
+// deterministic reduction of per-block {mass, energy} partials into out[2] (device)
+cudaError_t reduce_partials(const double *partials, uint64_t blocks, double *out, cudaStream_t s);
+
+} // namespace vfb

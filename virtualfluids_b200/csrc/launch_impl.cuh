@@ -1,0 +1,276 @@
+// Definitions of Launchers<S> for one arithmetic variant (VFB_NS, VFB_EXACT). Included by the
+// per-storage translation units, which explicitly instantiate one storage type each.
+#pragma once
+#include "kernels.cuh"
+#include "launch.h"
+
+#ifndef VFB_EXACT
+#error "VFB_EXACT must be defined"
+#endif
+
+namespace vfb {
+namespace VFB_NS {
+
+namespace {
+inline unsigned grid1d(uint64_t n, unsigned block) { return (unsigned)((n + block - 1) / block); }
+
+template <class C>
+K17Rates<C> rates_of(double omega, const double lim[3])
+{
+    return make_k17_rates<C>((C)omega, (C)lim[0], (C)lim[1], (C)lim[2]);
+}
+
+// RunCollision.cuh:112-114: forces * c1o2 * forceFactor, forceFactor = 1/2^level (KernelUtilities.h:56)
+template <class C>
+C force_factor(int level)
+{
+    C f = C(1);
+    for (int i = 1; i <= level; ++i)
+        f *= C(2);
+    return C(1) / f;
+}
+} // namespace
+
+template <class S>
+cudaError_t Launchers<S>::k17_list(const vfb_level *L, const uint32_t *idx, uint32_t n, int tmpl, cudaStream_t s)
+{
+    using C = typename Codec<S>::compute;
+    if (n == 0)
+        return cudaSuccess;
+    ListCollideArgs<C> a;
+    a.dist = L->distributions;
+    a.n = L->number_of_nodes;
+    a.nbx = L->neighbor_x;
+    a.nby = L->neighbor_y;
+    a.nbz = L->neighbor_z;
+    a.idx = idx;
+    a.n_idx = n;
+    a.rates = rates_of<C>(L->omega, L->quadric_limiters);
+    const C ff = force_factor<C>(L->level);
+    a.fx = (C)L->forces[0] * C(0.5) * ff;
+    a.fy = (C)L->forces[1] * C(0.5) * ff;
+    a.fz = (C)L->forces[2] * C(0.5) * ff;
+    a.force0 = (C)L->forces[0];
+    a.force1 = (C)L->forces[1];
+    a.force2 = (C)L->forces[2];
+    a.force_factor = ff;
+    a.bfx = static_cast<C *>(L->body_force_x);
+    a.bfy = static_cast<C *>(L->body_force_y);
+    a.bfz = static_cast<C *>(L->body_force_z);
+    a.rho = static_cast<C *>(L->rho);
+    a.vx = static_cast<C *>(L->velocity_x);
+    a.vy = static_cast<C *>(L->velocity_y);
+    a.vz = static_cast<C *>(L->velocity_z);
+    const bool wm = tmpl == VFB_COLLISION_WRITE_MACRO_VARS || tmpl == VFB_COLLISION_ALL_FEATURES || tmpl == VFB_COLLISION_SUBDOMAIN_BORDER;
+    const bool bf = tmpl == VFB_COLLISION_APPLY_BODY_FORCE || tmpl == VFB_COLLISION_ALL_FEATURES || tmpl == VFB_COLLISION_SUBDOMAIN_BORDER;
+    const unsigned B = 128, G = grid1d(n, B);
+    const bool even = L->is_even_timestep != 0;
+#define VFB_K17L(E, W, F) k17_list_kernel<S, VFB_EXACT, E, W, F><<<G, B, 0, s>>>(a)
+    if (even) {
+        if (wm && bf) VFB_K17L(true, true, true);
+        else if (wm) VFB_K17L(true, true, false);
+        else if (bf) VFB_K17L(true, false, true);
+        else VFB_K17L(true, false, false);
+    } else {
+        if (wm && bf) VFB_K17L(false, true, true);
+        else if (wm) VFB_K17L(false, true, false);
+        else if (bf) VFB_K17L(false, false, true);
+        else VFB_K17L(false, false, false);
+    }
+#undef VFB_K17L
+    return cudaGetLastError();
+}
+
+template <class S>
+cudaError_t Launchers<S>::bc(const vfb_level *L, const vfb_bc *bc, int kind, cudaStream_t s)
+{
+    if (bc->number_of_bc_nodes == 0)
+        return cudaSuccess;
+    BCArgs a;
+    a.dist = L->distributions;
+    a.n = L->number_of_nodes;
+    a.nbx = L->neighbor_x;
+    a.nby = L->neighbor_y;
+    a.nbz = L->neighbor_z;
+    a.k = bc->k;
+    a.q27 = bc->q27;
+    a.nbc = bc->number_of_bc_nodes;
+    a.ux = bc->vx;
+    a.uy = bc->vy;
+    a.uz = bc->vz;
+    a.omega = L->omega;
+    const unsigned B = 128, G = grid1d(a.nbc, B);
+    const bool even = L->is_even_timestep != 0;
+    switch (kind) {
+    case kNoSlipBB:
+        if (even) bc_bounce_back_kernel<S, true, false><<<G, B, 0, s>>>(a);
+        else bc_bounce_back_kernel<S, false, false><<<G, B, 0, s>>>(a);
+        break;
+    case kVelocityBB:
+        if (even) bc_bounce_back_kernel<S, true, true><<<G, B, 0, s>>>(a);
+        else bc_bounce_back_kernel<S, false, true><<<G, B, 0, s>>>(a);
+        break;
+    case kNoSlipInterp:
+        if (even) bc_interpolated_kernel<S, true, false><<<G, B, 0, s>>>(a);
+        else bc_interpolated_kernel<S, false, false><<<G, B, 0, s>>>(a);
+        break;
+    case kVelocityInterp:
+        if (even) bc_interpolated_kernel<S, true, true><<<G, B, 0, s>>>(a);
+        else bc_interpolated_kernel<S, false, true><<<G, B, 0, s>>>(a);
+        break;
+    default:
+        return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <class S>
+cudaError_t Launchers<S>::pressure(const vfb_level *L, const vfb_directional_bc *bc, cudaStream_t s)
+{
+    if (bc->number_of_bc_nodes == 0)
+        return cudaSuccess;
+    PressureArgs a;
+    a.dist = L->distributions;
+    a.n = L->number_of_nodes;
+    a.nbx = L->neighbor_x;
+    a.nby = L->neighbor_y;
+    a.nbz = L->neighbor_z;
+    a.k = bc->k;
+    a.kN = bc->k_neighbor;
+    a.rho_bc = bc->rho_bc;
+    a.nbc = bc->number_of_bc_nodes;
+    a.direction = bc->direction;
+    const unsigned B = 128, G = grid1d(a.nbc, B);
+    if (L->is_even_timestep) bc_pressure_neq_kernel<S, true><<<G, B, 0, s>>>(a);
+    else bc_pressure_neq_kernel<S, false><<<G, B, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <class S>
+cudaError_t Launchers<S>::init_list(const vfb_level *L, cudaStream_t s)
+{
+    const unsigned B = 128, G = grid1d(L->number_of_nodes, B);
+    if (L->is_even_timestep)
+        init_list_kernel<S, true><<<G, B, 0, s>>>(L->distributions, L->number_of_nodes, L->neighbor_x, L->neighbor_y,
+                                                  L->neighbor_z, L->type_of_grid_node, L->rho, L->velocity_x,
+                                                  L->velocity_y, L->velocity_z);
+    else
+        init_list_kernel<S, false><<<G, B, 0, s>>>(L->distributions, L->number_of_nodes, L->neighbor_x, L->neighbor_y,
+                                                   L->neighbor_z, L->type_of_grid_node, L->rho, L->velocity_x,
+                                                   L->velocity_y, L->velocity_z);
+    return cudaGetLastError();
+}
+
+template <class S>
+cudaError_t Launchers<S>::macros_list(const vfb_level *L, cudaStream_t s)
+{
+    const unsigned B = 128, G = grid1d(L->number_of_nodes, B);
+    if (L->is_even_timestep)
+        macros_list_kernel<S, true><<<G, B, 0, s>>>(L->distributions, L->number_of_nodes, L->neighbor_x, L->neighbor_y,
+                                                    L->neighbor_z, L->type_of_grid_node, L->rho, L->velocity_x,
+                                                    L->velocity_y, L->velocity_z, L->pressure);
+    else
+        macros_list_kernel<S, false><<<G, B, 0, s>>>(L->distributions, L->number_of_nodes, L->neighbor_x, L->neighbor_y,
+                                                     L->neighbor_z, L->type_of_grid_node, L->rho, L->velocity_x,
+                                                     L->velocity_y, L->velocity_z, L->pressure);
+    return cudaGetLastError();
+}
+
+template <class S>
+cudaError_t Launchers<S>::energy_list(const vfb_level *L, const uint32_t *idx, uint32_t n, double *partials,
+                                      cudaStream_t s)
+{
+    if (n == 0)
+        return cudaSuccess;
+    const unsigned B = 256, G = grid1d(n, B);
+    if (L->is_even_timestep)
+        energy_list_kernel<S, true><<<G, B, 0, s>>>(L->distributions, L->number_of_nodes, L->neighbor_x, L->neighbor_y,
+                                                    L->neighbor_z, idx, n, partials);
+    else
+        energy_list_kernel<S, false><<<G, B, 0, s>>>(L->distributions, L->number_of_nodes, L->neighbor_x, L->neighbor_y,
+                                                     L->neighbor_z, idx, n, partials);
+    return cudaGetLastError();
+}
+
+namespace {
+template <class C>
+BoxCollideArgs<C> box_args(const BoxState &b)
+{
+    BoxCollideArgs<C> a;
+    a.dist = b.dist;
+    a.pitch = b.pitch;
+    a.nx = b.nx;
+    a.ny = b.ny;
+    a.nz = b.nz;
+    a.periodic_x = b.periodic_x;
+    a.periodic_y = b.periodic_y;
+    a.periodic_z = b.periodic_z;
+    a.mask = b.mask;
+    a.rates = rates_of<C>(b.omega, b.lim);
+    a.fx = (C)b.fx;
+    a.fy = (C)b.fy;
+    a.fz = (C)b.fz;
+    a.energy_partials = nullptr;
+    a.rho = a.vx = a.vy = a.vz = nullptr;
+    return a;
+}
+inline dim3 box_grid(const BoxState &b)
+{
+    const int bx = box_block_x(b.nx);
+    return dim3((unsigned)((b.nx + bx - 1) / bx), (unsigned)b.ny, (unsigned)b.nz);
+}
+} // namespace
+
+template <class S>
+cudaError_t Launchers<S>::box_collide(const BoxState &b, bool even, double *partials, cudaStream_t s)
+{
+    using C = typename Codec<S>::compute;
+    BoxCollideArgs<C> a = box_args<C>(b);
+    a.energy_partials = partials;
+    const dim3 G = box_grid(b), B(box_block_x(b.nx));
+    const bool mask = b.mask != nullptr, energy = partials != nullptr;
+#define VFB_K17B(E, M, N) k17_box_kernel<S, VFB_EXACT, E, M, N, false><<<G, B, 0, s>>>(a)
+    if (even) {
+        if (mask && energy) VFB_K17B(true, true, true);
+        else if (mask) VFB_K17B(true, true, false);
+        else if (energy) VFB_K17B(true, false, true);
+        else VFB_K17B(true, false, false);
+    } else {
+        if (mask && energy) VFB_K17B(false, true, true);
+        else if (mask) VFB_K17B(false, true, false);
+        else if (energy) VFB_K17B(false, false, true);
+        else VFB_K17B(false, false, false);
+    }
+#undef VFB_K17B
+    return cudaGetLastError();
+}
+
+template <class S>
+cudaError_t Launchers<S>::box_init(const BoxState &b, bool even, const void *rho, const void *ux, const void *uy,
+                                   const void *uz, cudaStream_t s)
+{
+    using C = typename Codec<S>::compute;
+    BoxCollideArgs<C> a = box_args<C>(b);
+    const dim3 G = box_grid(b), B(box_block_x(b.nx));
+    if (even) init_box_kernel<S, true><<<G, B, 0, s>>>(a, rho, ux, uy, uz);
+    else init_box_kernel<S, false><<<G, B, 0, s>>>(a, rho, ux, uy, uz);
+    return cudaGetLastError();
+}
+
+template <class S>
+cudaError_t Launchers<S>::box_macros(const BoxState &b, bool even, void *rho, void *ux, void *uy, void *uz, cudaStream_t s)
+{
+    using C = typename Codec<S>::compute;
+    BoxCollideArgs<C> a = box_args<C>(b);
+    a.rho = static_cast<C *>(rho);
+    a.vx = static_cast<C *>(ux);
+    a.vy = static_cast<C *>(uy);
+    a.vz = static_cast<C *>(uz);
+    const dim3 G = box_grid(b), B(box_block_x(b.nx));
+    if (even) macros_box_kernel<S, true><<<G, B, 0, s>>>(a);
+    else macros_box_kernel<S, false><<<G, B, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+} // namespace VFB_NS
+} // namespace vfb

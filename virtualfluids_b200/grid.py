@@ -1,0 +1,179 @@
+"""Host-side construction of levels in the reference GPU layout.
+
+A box of fluid nodes is laid out as the reference's GridGenerator lays out a uniform grid
+(src/gpu/GridGenerator/grid/GridImp.cpp):
+
+* sparse node list in x-fastest order, shifted by one so that node 0 is the dummy sink that
+  every missing neighbour points to (GridImp.cpp:974, getNodeValues :2146-2185);
+* a one-node layer of stopper nodes around the fluid on every non-periodic side; stoppers are
+  in the node list but never collided (geo GEO_SOLID);
+* neighborX/Y/Z[k] = the node at +1 in x/y/z, wrapped on periodic axes (setNeighborIndices
+  :1012-1032, getNeighborIndex :1071-1080); stoppers get their in-grid +1 neighbours only
+  (setStopperNeighborCoords :1034-1057);
+* boundary-condition nodes are the fluid nodes of the outermost fluid layer of a side, with
+  q = 1/2 on every link that points along the side normal into a stopper, and q = -1 elsewhere
+  (Side::setQs, Side.cpp:149-167); a diagonal link already owned by a side set earlier is not
+  repeated (Side::resetDiagonalsInCaseOfOtherBC, Side.cpp:185-210);
+* pressure BC nodes carry the index of the node one step inwards (Side::setPressureNeighborIndices,
+  Side.cpp:89-110) and the side's D3Q27 direction (LevelGridBuilder.cpp:721-724).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as N
+
+# D3Q27 components in reference numbering (src/lbm/constants/D3Q27.h:42-72)
+CX = np.array([0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1])
+CY = np.array([0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1, 1, 1, -1, -1, 1, 1, -1, -1])
+CZ = np.array([0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 1, 1, 1, 1, -1, -1, -1, -1])
+INV = np.array([0, 2, 1, 4, 3, 6, 5, 8, 7, 10, 9, 12, 11, 14, 13, 16, 15, 18, 17, 26, 25, 24, 23, 22, 21, 20, 19])
+W = np.array([8 / 27] + [2 / 27] * 6 + [1 / 54] * 12 + [1 / 216] * 8)
+
+# side name -> (axis, sign); D3Q27 direction of the side (Side.h:111-115)
+SIDES = {"MX": (0, -1), "PX": (0, 1), "MY": (1, -1), "PY": (1, 1), "MZ": (2, -1), "PZ": (2, 1)}
+SIDE_DIR = {"MX": N.DIR_M00, "PX": N.DIR_P00, "MY": N.DIR_0M0, "PY": N.DIR_0P0, "MZ": N.DIR_00M, "PZ": N.DIR_00P}
+
+
+@dataclass
+class SideBC:
+    side: str
+    kind: str                       # "noslip", "velocity", "pressure"
+    k: np.ndarray                   # int32 node indices
+    q: np.ndarray                   # float64 [27, n]
+    velocity: tuple = (0.0, 0.0, 0.0)
+    rho: float = 0.0
+    k_neighbor: np.ndarray | None = None
+
+
+@dataclass
+class ListGrid:
+    """One level of a fluid box nx*ny*nz in the reference layout (see module docstring)."""
+    nx: int
+    ny: int
+    nz: int
+    periodic: tuple = (False, False, False)
+    number_of_nodes: int = 0
+    neighbor: np.ndarray | None = None      # uint32 [3, n]
+    geo: np.ndarray | None = None           # uint32 [n]
+    fluid: np.ndarray | None = None         # uint32 fluid node indices
+    coords: np.ndarray | None = None        # int64 [3, n] fluid-box coordinates (shell at -1 / n)
+    bcs: list = field(default_factory=list)
+
+    def __post_init__(self):
+        self.shell = tuple(0 if p else 1 for p in self.periodic)
+        self.dims = (self.nx + 2 * self.shell[0], self.ny + 2 * self.shell[1], self.nz + 2 * self.shell[2])
+        Dx, Dy, Dz = self.dims
+        n_grid = Dx * Dy * Dz
+        self.number_of_nodes = n_grid + 1
+        i = np.arange(n_grid, dtype=np.int64)
+        gx, gy, gz = i % Dx, (i // Dx) % Dy, i // (Dx * Dy)
+        # coordinates in fluid-box units: fluid nodes 0..n-1, shell at -1 and n
+        coords = np.zeros((3, self.number_of_nodes), dtype=np.int64)
+        coords[0, 1:] = gx - self.shell[0]
+        coords[1, 1:] = gy - self.shell[1]
+        coords[2, 1:] = gz - self.shell[2]
+        coords[:, 0] = -(10 ** 9)
+        self.coords = coords
+        fluid_mask = np.zeros(self.number_of_nodes, dtype=bool)
+        fluid_mask[1:] = ((coords[0, 1:] >= 0) & (coords[0, 1:] < self.nx) & (coords[1, 1:] >= 0) & (coords[1, 1:] < self.ny)
+                          & (coords[2, 1:] >= 0) & (coords[2, 1:] < self.nz))
+        self.geo = np.where(fluid_mask, N.GEO_FLUID, N.GEO_SOLID).astype(np.uint32)
+        self.fluid = np.nonzero(fluid_mask)[0].astype(np.uint32)
+        nb = np.zeros((3, self.number_of_nodes), dtype=np.uint32)
+        g = [gx, gy, gz]
+        for a in range(3):
+            nxt = g[a] + 1
+            if self.periodic[a]:
+                nxt = np.where(nxt >= self.dims[a], 0, nxt)
+                ok = np.ones_like(nxt, dtype=bool)
+            else:
+                ok = nxt < self.dims[a]
+            comp = list(g)
+            comp[a] = np.where(ok, nxt, 0)
+            idx = comp[0] + Dx * (comp[1] + Dy * comp[2]) + 1
+            nb[a, 1:] = np.where(ok, idx, 0).astype(np.uint32)
+        self.neighbor = nb
+        self._bc_sides_set = []
+
+    # -- indexing ----------------------------------------------------------------------------
+    def node_index(self, x, y, z):
+        """Node index of fluid-box coordinates (shell allowed on non-periodic axes)."""
+        Dx, Dy, _ = self.dims
+        gx = np.asarray(x) + self.shell[0]
+        gy = np.asarray(y) + self.shell[1]
+        gz = np.asarray(z) + self.shell[2]
+        return (gx + Dx * (gy + Dy * gz) + 1).astype(np.int64)
+
+    def is_stopper(self, x, y, z):
+        inside = ((x >= 0) & (x < self.nx) & (y >= 0) & (y < self.ny) & (z >= 0) & (z < self.nz))
+        return ~inside
+
+    # -- boundary conditions (Side::addIndices / setQs) ---------------------------------------
+    def _side_nodes(self, side):
+        axis, sign = SIDES[side]
+        if self.periodic[axis]:
+            raise ValueError(f"side {side} lies on a periodic axis")
+        ext = (self.nx, self.ny, self.nz)
+        layer = ext[axis] - 1 if sign > 0 else 0
+        sel = self.fluid[self.coords[axis, self.fluid] == layer]
+        return sel.astype(np.int64)
+
+    def _neighbour_coords(self, x, y, z, d):
+        nx_, ny_, nz_ = x + CX[d], y + CY[d], z + CZ[d]
+        # Side::correctNeighborForPeriodicBoundaries: wrap on periodic axes
+        if self.periodic[0]:
+            nx_ = nx_ % self.nx
+        if self.periodic[1]:
+            ny_ = ny_ % self.ny
+        if self.periodic[2]:
+            nz_ = nz_ % self.nz
+        return nx_, ny_, nz_
+
+    def add_side(self, side, kind, velocity=(0.0, 0.0, 0.0), rho=0.0):
+        """Set a BC on a side, in the order the reference's app sets them."""
+        axis, sign = SIDES[side]
+        nodes = self._side_nodes(side)
+        x, y, z = self.coords[0, nodes], self.coords[1, nodes], self.coords[2, nodes]
+        q = np.full((27, nodes.size), -1.0)
+        normal = np.zeros(3, dtype=int)
+        normal[axis] = sign
+        for d in range(1, 27):
+            c = np.array([CX[d], CY[d], CZ[d]])
+            if c @ normal <= 0:
+                continue
+            stop = self.is_stopper(*self._neighbour_coords(x, y, z, d))
+            qd = np.where(stop, 0.5, -1.0)
+            # resetDiagonalsInCaseOfOtherBC: links along the normal of a side set before, on nodes
+            # that lie on that side too, stay with the earlier side
+            for other in self._bc_sides_set:
+                oa, os_ = SIDES[other]
+                onormal = np.zeros(3, dtype=int)
+                onormal[oa] = os_
+                if c @ onormal <= 0:
+                    continue
+                ocoords = [x.copy(), y.copy(), z.copy()]
+                ocoords[oa] = ocoords[oa] + os_
+                on_other = self.is_stopper(*ocoords)
+                qd = np.where((qd == 0.5) & on_other, -1.0, qd)
+            q[d] = qd
+        bc = SideBC(side=side, kind=kind, k=nodes.astype(np.int32), q=q, velocity=tuple(velocity), rho=rho)
+        if kind == "pressure":
+            inward = [x.copy(), y.copy(), z.copy()]
+            inward[axis] = inward[axis] - sign
+            bc.k_neighbor = self.node_index(*inward).astype(np.int32)
+        self.bcs.append(bc)
+        self._bc_sides_set.append(side)
+        return bc
+
+    def merged(self, kind):
+        """All BCs of one kind concatenated, as allocArrays_BoundaryValues fills one struct per kind."""
+        parts = [b for b in self.bcs if b.kind == kind]
+        if not parts:
+            return None
+        k = np.concatenate([b.k for b in parts])
+        q = np.concatenate([b.q for b in parts], axis=1)
+        vel = np.concatenate([np.tile(np.array(b.velocity)[:, None], (1, b.k.size)) for b in parts], axis=1)
+        return k, q, vel

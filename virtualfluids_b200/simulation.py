@@ -1,0 +1,259 @@
+"""Python mirror of the reference's set-up surface for the hot path, over the C ABI.
+
+Names and meanings follow the reference so that a set-up reads like one of its apps
+(apps/gpu/DrivenCavity/DrivenCavity.cpp:95-146):
+
+* :class:`Parameter` — the subset of ``Parameter`` the time step reads (viscosity, main kernel,
+  quadric limiters, forcing; src/gpu/core/Parameter/Parameter.h, Parameter.cpp:69-70, 395-422);
+* :class:`BoundaryConditionFactory` — the enums and setters of
+  src/gpu/core/BoundaryConditions/BoundaryConditionFactory.h:50-178;
+* :class:`Simulation` — allocation, initialisation (PreProcessorImp::init) and the time loop
+  (UpdateGrid27::updateGrid) of one level, driving ``vfb_simulation_*`` of the native library.
+
+Device memory is held in torch tensors (plumbing only); every kernel runs in ``libvfb.so``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+
+import numpy as np
+
+from . import _native as N
+from .grid import ListGrid
+
+STORAGE = {"f64": N.STORAGE_F64, "f32": N.STORAGE_F32, "f16": N.STORAGE_F16, "bf16": N.STORAGE_BF16}
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def storage_dtype(storage: int):
+    t = _torch()
+    return {N.STORAGE_F64: t.float64, N.STORAGE_F32: t.float32, N.STORAGE_F16: t.float16, N.STORAGE_BF16: t.bfloat16}[storage]
+
+
+def real_dtype(storage: int):
+    t = _torch()
+    return t.float64 if storage == N.STORAGE_F64 else t.float32
+
+
+class Parameter:
+    """Subset of the reference Parameter used by the collision, BC and init kernels."""
+
+    def __init__(self):
+        self.viscosity_lb = 0.0
+        self.velocity_lb = 0.0
+        self.main_kernel = None
+        self.quadric_limiters = (0.01, 0.01, 0.01)  # Parameter.cpp:69 defaults
+        self.forcing = (0.0, 0.0, 0.0)
+        self.storage = N.STORAGE_F64
+        self.arith = N.ARITH_FAST
+
+    def set_viscosity_lb(self, nu: float):
+        self.viscosity_lb = float(nu)
+
+    def set_velocity_lb(self, u: float):
+        self.velocity_lb = float(u)
+
+    def configure_main_kernel(self, name: str):
+        """Parameter::configureMainKernel (Parameter.cpp:1216); unknown names fail at once."""
+        kid = C.c_int32()
+        N.check(N.lib().vfb_kernel_lookup(name.encode(), C.byref(kid)))
+        self.main_kernel = name
+
+    def set_quadric_limiters(self, p: float, m: float, d: float):
+        self.quadric_limiters = (float(p), float(m), float(d))
+
+    def set_forcing(self, fx: float, fy: float, fz: float):
+        self.forcing = (float(fx), float(fy), float(fz))
+
+    @property
+    def omega(self) -> float:
+        """omega = 1 / (3 nu + 1/2) (Parameter.cpp:406)."""
+        return 1.0 / (3.0 * self.viscosity_lb + 0.5)
+
+
+class BoundaryConditionFactory:
+    """Enums and setters of the reference BoundaryConditionFactory."""
+
+    class VelocityBC(enum.IntEnum):
+        VelocityBounceBack = N.VELOCITY_BOUNCE_BACK
+        VelocityInterpolatedIncompressible = N.VELOCITY_INTERPOLATED_INCOMPRESSIBLE
+        VelocityInterpolatedCompressible = N.VELOCITY_INTERPOLATED_COMPRESSIBLE
+        VelocityWithPressureInterpolatedCompressible = N.VELOCITY_WITH_PRESSURE_INTERPOLATED_COMPRESSIBLE
+        NotSpecified = N.VELOCITY_NOT_SPECIFIED
+
+    class NoSlipBC(enum.IntEnum):
+        NoSlipDelayBounceBack = N.NOSLIP_DELAY_BOUNCE_BACK
+        NoSlipBounceBack = N.NOSLIP_BOUNCE_BACK
+        NoSlipInterpolatedIncompressible = N.NOSLIP_INTERPOLATED_INCOMPRESSIBLE
+        NoSlipInterpolatedCompressible = N.NOSLIP_INTERPOLATED_COMPRESSIBLE
+
+    class PressureBC(enum.IntEnum):
+        PressureNonEquilibriumIncompressible = N.PRESSURE_NON_EQUILIBRIUM_INCOMPRESSIBLE
+        PressureNonEquilibriumCompressible = N.PRESSURE_NON_EQUILIBRIUM_COMPRESSIBLE
+        OutflowNonReflective = N.PRESSURE_OUTFLOW_NON_REFLECTIVE
+        OutflowNonReflectivePressureCorrection = N.PRESSURE_OUTFLOW_NON_REFLECTIVE_PRESSURE_CORRECTION
+        NotSpecified = N.PRESSURE_NOT_SPECIFIED
+
+    def __init__(self):
+        # defaults of the reference (BoundaryConditionFactory.h:168-176)
+        self.velocity = self.VelocityBC.NotSpecified
+        self.noslip = self.NoSlipBC.NoSlipDelayBounceBack
+        self.pressure = self.PressureBC.NotSpecified
+
+    def set_velocity_boundary_condition(self, v):
+        self.velocity = self.VelocityBC(v)
+
+    def set_no_slip_boundary_condition(self, v):
+        self.noslip = self.NoSlipBC(v)
+
+    def set_pressure_boundary_condition(self, v):
+        self.pressure = self.PressureBC(v)
+
+    def velocity_function(self):
+        fn = C.c_void_p()
+        N.check(N.lib().vfb_bc_factory_velocity(int(self.velocity), C.byref(fn)))
+        return fn.value
+
+    def noslip_function(self):
+        fn = C.c_void_p()
+        N.check(N.lib().vfb_bc_factory_noslip(int(self.noslip), C.byref(fn)))
+        return fn.value
+
+    def pressure_function(self):
+        fn = C.c_void_p()
+        N.check(N.lib().vfb_bc_factory_pressure(int(self.pressure), C.byref(fn)))
+        return fn.value
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
+
+
+class Simulation:
+    """One level of a uniform grid advanced by the native step driver."""
+
+    def __init__(self, para: Parameter, grid: ListGrid, bc_factory: BoundaryConditionFactory, device="cuda"):
+        if para.main_kernel is None:
+            raise N.VfbError(N.VFB_ERR_UNKNOWN_KERNEL, "no main kernel configured")
+        t = _torch()
+        self.para, self.grid, self.bcf = para, grid, bc_factory
+        self.device = device
+        sd, rd = storage_dtype(para.storage), real_dtype(para.storage)
+        n = grid.number_of_nodes
+        self.dist = t.zeros(27 * n, dtype=sd, device=device)
+        self.nb = [t.from_numpy(grid.neighbor[a].astype(np.int32)).to(device) for a in range(3)]
+        self.geo = t.from_numpy(grid.geo.astype(np.int32)).to(device)
+        self.fluid = t.from_numpy(grid.fluid.astype(np.int32)).to(device)
+        self.rho = t.zeros(n, dtype=rd, device=device)
+        self.vx = t.zeros(n, dtype=rd, device=device)
+        self.vy = t.zeros(n, dtype=rd, device=device)
+        self.vz = t.zeros(n, dtype=rd, device=device)
+        self.press = t.zeros(n, dtype=rd, device=device)
+        L = N.Level()
+        L.storage = para.storage
+        L.arith = para.arith
+        L.is_even_timestep = 1
+        L.level = 0
+        L.number_of_nodes = n
+        L.distributions = self.dist.data_ptr()
+        L.neighbor_x, L.neighbor_y, L.neighbor_z = (x.data_ptr() for x in self.nb)
+        L.type_of_grid_node = self.geo.data_ptr()
+        L.omega = para.omega
+        for i in range(3):
+            L.forces[i] = para.forcing[i]
+            L.quadric_limiters[i] = para.quadric_limiters[i]
+        L.rho, L.velocity_x, L.velocity_y, L.velocity_z = (x.data_ptr() for x in (self.rho, self.vx, self.vy, self.vz))
+        L.pressure = self.press.data_ptr()
+        self.level = L
+        self._keep = []
+        self._bcs = {}
+        for kind in ("velocity", "noslip"):
+            m = grid.merged(kind)
+            if m is None:
+                continue
+            k, q, vel = m
+            kt = t.from_numpy(k.astype(np.int32)).to(device)
+            qt = t.from_numpy(q.reshape(-1)).to(device=device, dtype=rd)
+            vt = [t.from_numpy(vel[a].copy()).to(device=device, dtype=rd) for a in range(3)]
+            bc = N.BC(kt.data_ptr(), qt.data_ptr(), k.size, vt[0].data_ptr(), vt[1].data_ptr(), vt[2].data_ptr())
+            self._keep += [kt, qt] + vt
+            self._bcs[kind] = bc
+        self._pressure = []
+        for b in grid.bcs:
+            if b.kind != "pressure":
+                continue
+            kt = t.from_numpy(b.k.astype(np.int32)).to(device)
+            knt = t.from_numpy(b.k_neighbor.astype(np.int32)).to(device)
+            rt = t.full((b.k.size,), float(b.rho), dtype=rd, device=device)
+            from .grid import SIDE_DIR
+            self._keep += [kt, knt, rt]
+            self._pressure.append(N.DirectionalBC(kt.data_ptr(), knt.data_ptr(), rt.data_ptr(), b.k.size, SIDE_DIR[b.side]))
+        sim = C.c_void_p()
+        N.check(N.lib().vfb_simulation_create(para.main_kernel.encode(), C.byref(sim)))
+        self._sim = sim
+        N.check(N.lib().vfb_simulation_set_level(sim, C.byref(L), _ptr(self.fluid), int(grid.fluid.size)))
+        if "velocity" in self._bcs:
+            N.check(N.lib().vfb_simulation_set_velocity_bc(sim, C.byref(self._bcs["velocity"]), int(bc_factory.velocity)))
+        if "noslip" in self._bcs:
+            N.check(N.lib().vfb_simulation_set_noslip_bc(sim, C.byref(self._bcs["noslip"]), int(bc_factory.noslip)))
+        for p in self._pressure:
+            N.check(N.lib().vfb_simulation_add_pressure_bc(sim, C.byref(p), int(bc_factory.pressure)))
+        N.check(N.lib().vfb_simulation_check(sim))
+
+    def close(self):
+        if getattr(self, "_sim", None):
+            N.lib().vfb_simulation_destroy(self._sim)
+            self._sim = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init(self, rho=None, vx=None, vy=None, vz=None):
+        """PreProcessorImp::init: equilibrium for the odd, then the even parity; starts even."""
+        t = _torch()
+        rd = real_dtype(self.para.storage)
+        for arr, dst in ((rho, self.rho), (vx, self.vx), (vy, self.vy), (vz, self.vz)):
+            if arr is None:
+                dst.zero_()
+            else:
+                dst.copy_(t.as_tensor(np.asarray(arr), dtype=rd))
+        L = self.level
+        L.is_even_timestep = 0
+        N.check(N.lib().vfb_init_navier_stokes_compressible(C.byref(L), None))
+        L.is_even_timestep = 1
+        N.check(N.lib().vfb_init_navier_stokes_compressible(C.byref(L), None))
+        N.check(N.lib().vfb_simulation_set_level(self._sim, C.byref(L), _ptr(self.fluid), int(self.grid.fluid.size)))
+
+    def run(self, steps: int):
+        N.check(N.lib().vfb_simulation_run(self._sim, int(steps), None))
+        ev = C.c_int32()
+        N.check(N.lib().vfb_simulation_is_even_timestep(self._sim, C.byref(ev)))
+        self.level.is_even_timestep = ev.value
+
+    def macroscopic(self):
+        """drho, vx, vy, vz, pressure of every node (zeros on non-fluid nodes), as numpy."""
+        N.check(N.lib().vfb_calc_macroscopic_compressible(C.byref(self.level), None))
+        N.check(N.lib().vfb_synchronize(None))
+        return {k: v.double().cpu().numpy() for k, v in
+                (("rho", self.rho), ("vx", self.vx), ("vy", self.vy), ("vz", self.vz), ("pressure", self.press))}
+
+    def mass_energy(self):
+        t = _torch()
+        nbytes = N.lib().vfb_mass_energy_workspace_bytes(int(self.grid.fluid.size))
+        ws = t.empty((nbytes + 7) // 8, dtype=t.float64, device=self.device)
+        out = (C.c_double * 2)()
+        N.check(N.lib().vfb_mass_energy(C.byref(self.level), _ptr(self.fluid), int(self.grid.fluid.size),
+                                        C.c_void_p(ws.data_ptr()), nbytes, out, None))
+        return out[0], out[1]
+
+    def populations(self):
+        N.check(N.lib().vfb_synchronize(None))
+        return self.dist.double().cpu().numpy()
