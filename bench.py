@@ -181,6 +181,9 @@ def main():
     ap.add_argument("--n", type=int, default=N_SIDE)
     ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--arith", default="fast", choices=["fast", "exact"],
+                    help="exact: every operation rounded as the reference's host build (bitwise oracle parity)")
+    ap.add_argument("--kernel", default="auto", choices=["auto", "direct", "tma"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -223,7 +226,8 @@ def main():
         return float(t.item())
 
     # ---- device-resident throughput: K steps with the per-step FP64 energy kept on the device ----
-    box = vfb.Box(n, n, n, omega, storage="f64")
+    box = vfb.Box(n, n, n, omega, storage="f64", arith=args.arith)
+    box.set_kernel_variant(args.kernel)
     box.init(*(torch.from_numpy(a).to(dev) for a in fields), stream=sp)
     energy = torch.zeros(2 * max(args.steps, args.warmup), dtype=torch.float64, device=dev)
     box.step(args.warmup, energy=energy, stream=sp)
@@ -255,6 +259,7 @@ def main():
                 "kernel": "k17_box_kernel<double> (collision + ET streaming)", "kernel_ms": round(k_ms, 4),
                 "algorithmic_bytes_per_launch": BYTES_PER_NODE["f64"] * nodes}
     e_host = energy[: 2 * args.steps].cpu().numpy()
+    box.status()
     del box
     torch.cuda.empty_cache()
 
@@ -262,7 +267,8 @@ def main():
     host_in = [torch.from_numpy(a).pin_memory() for a in fields]
     host_out = [torch.empty(nodes, dtype=torch.float64).pin_memory() for _ in range(4)]
     host_energy = torch.zeros(2 * args.steps, dtype=torch.float64).pin_memory()
-    box = vfb.Box(n, n, n, omega, storage="f64")
+    box = vfb.Box(n, n, n, omega, storage="f64", arith=args.arith)
+    box.set_kernel_variant(args.kernel)
     lib = N.lib()
     # warm-up of the same path
     N.check(lib.vfb_box_init(box._h, *(C.c_void_p(h.data_ptr()) for h in host_in), 1, sp))
@@ -293,6 +299,7 @@ def main():
     if not args.no_forms:
         for st in ("f32", "f16", "bf16"):
             b = vfb.Box(n, n, n, omega, storage=st)
+            b.set_kernel_variant(args.kernel)
             b.init(*(torch.from_numpy(a.astype(np.float32)).to(dev) for a in fields), stream=sp)
             b.step(args.warmup, stream=sp)
             ks = min(args.steps, 200)
@@ -319,7 +326,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"Taylor-Green vortex {n}^3 periodic, u0={U0}, Re={int(RE)}, D3Q27 K17 cumulant + "
                                    f"esoteric-twist streaming, FP64, per-step FP64 kinetic energy",
-                       "nodes_per_gpu": nodes, "omega": omega, "replicas": world,
+                       "nodes_per_gpu": nodes, "omega": omega, "replicas": world, "arith": args.arith,
+                       "kernel": args.kernel,
                        "l2": "inputs larger than L2 (3.62 GB populations per GPU), no flush"},
             "roofline": roofline,
             "e2e": {"value": round(e2e_value, 1), "unit": "MLUPS", "h2d_bytes_per_step": h2d // args.steps,

@@ -231,6 +231,11 @@ int vfb_box_init(vfb_box *box, const void *rho, const void *ux, const void *uy, 
 int vfb_box_step(vfb_box *box, uint32_t steps, double *energy, int32_t energy_on_host, void *stream);
 /* macroscopic drho, ux, uy, uz (real[nx*ny*nz]) of the current state, to host or device memory */
 int vfb_box_fields(vfb_box *box, void *rho, void *ux, void *uy, void *uz, int32_t to_host, void *stream);
+/* synchronises the stream and reads the status word the box's kernels set on a failed internal wait
+   (0 = fine); returns VFB_ERR_CUDA when it is nonzero */
+int vfb_box_status(vfb_box *box, int32_t *device_status, void *stream);
+/* collision kernel: 0 = choose (TMA-staged when nx % 128 == 0), 1 = direct loads, 2 = TMA-staged */
+int vfb_box_set_kernel_variant(vfb_box *box, int32_t variant);
 /* raw access to the population planes for checks: pointer, plane pitch (elements), parity */
 int vfb_box_populations(const vfb_box *box, void **dist, uint64_t *pitch, int32_t *is_even);
 

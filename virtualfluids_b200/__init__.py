@@ -5,7 +5,8 @@ interpolated, velocity and non-equilibrium pressure boundary kernels, and the FP
 as hand-written sm_100a CUDA behind the C ABI of ``include/vfb.h`` (``libvfb.so``). This package
 is the Python host side: set-up objects mirroring the reference's Parameter /
 BoundaryConditionFactory / Simulation, a builder for levels in the reference layout, and
-structured boxes. Importing it loads the native library; there is no fallback.
+structured boxes. The native library is loaded on first use (``lib()``) and a missing or stale
+library raises there; there is no fallback.
 """
 from . import _native
 from ._native import VfbError, lib
@@ -14,5 +15,3 @@ from .grid import ListGrid
 from .simulation import BoundaryConditionFactory, Parameter, Simulation
 
 __all__ = ["Box", "BoundaryConditionFactory", "ListGrid", "Parameter", "Simulation", "VfbError", "lib", "_native"]
-
-lib()  # fail at import when the native library is missing

@@ -128,6 +128,8 @@ SIGNATURES = {
     "vfb_box_init": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "vfb_box_step": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_int32, C.c_void_p]),
     "vfb_box_fields": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    "vfb_box_status": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.c_void_p]),
+    "vfb_box_set_kernel_variant": (C.c_int, [C.c_void_p, C.c_int32]),
     "vfb_box_populations": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64),
                                       C.POINTER(C.c_int32)]),
 }

@@ -89,6 +89,16 @@ class Box:
         N.check(N.lib().vfb_box_fields(self._h, *(_dev_ptr(a) for a in out), 0, stream))
         return out
 
+    def status(self, stream=None) -> int:
+        """Synchronise and check the device status word; raises if a kernel gave up waiting."""
+        v = C.c_int32()
+        N.check(N.lib().vfb_box_status(self._h, C.byref(v), stream))
+        return v.value
+
+    def set_kernel_variant(self, variant: str):
+        """'auto', 'direct' (plain loads) or 'tma' (bulk copies staged in shared memory)."""
+        N.check(N.lib().vfb_box_set_kernel_variant(self._h, {"auto": 0, "direct": 1, "tma": 2}[variant]))
+
     def populations(self):
         """(device pointer, plane pitch in elements, is_even) of the population array."""
         p, pitch, ev = C.c_void_p(), C.c_uint64(), C.c_int32()

@@ -547,6 +547,7 @@ struct vfb_box {
     double *energy_ring = nullptr;  // per-step results before they are copied out
     uint32_t ring_steps = 0;
     void *staging = nullptr;        // 4 real fields for init and output
+    int *status = nullptr;          // device status word of the kernels (DeviceError)
 };
 
 namespace {
@@ -561,6 +562,7 @@ void box_free(vfb_box *b)
     cudaFree(b->partials);
     cudaFree(b->energy_ring);
     cudaFree(b->staging);
+    cudaFree(b->status);
 }
 } // namespace
 
@@ -624,6 +626,12 @@ int vfb_box_create(const vfb_box_desc *d, vfb_box **out)
     b->ring_steps = kRingSteps;
     if (e == cudaSuccess)
         e = cudaMalloc(&b->staging, 4 * n * real_bytes(d->storage));
+    if (e == cudaSuccess)
+        e = cudaMalloc((void **)&b->status, sizeof(int));
+    if (e == cudaSuccess)
+        e = cudaMemset(b->status, 0, sizeof(int));
+    s.status = b->status;
+    s.variant = 0;
     if (e != cudaSuccess) {
         box_free(b);
         delete b;
@@ -689,10 +697,12 @@ int vfb_box_step(vfb_box *box, uint32_t steps, double *energy, int32_t energy_on
         const uint32_t chunk = energy && energy_on_host ? std::min<uint32_t>(steps - done, box->ring_steps) : steps - done;
         for (uint32_t t = 0; t < chunk && e == cudaSuccess; ++t) {
             double *partials = energy ? box->partials : nullptr;
-            e = VFB_DISPATCH(box->desc.storage, box->desc.arith, LA::box_collide(box->state, box->even, partials, s));
+            uint64_t n_partials = 0;
+            e = VFB_DISPATCH(box->desc.storage, box->desc.arith,
+                             LA::box_collide(box->state, box->even, partials, &n_partials, s));
             if (e == cudaSuccess && energy) {
                 double *dst = energy_on_host ? box->energy_ring + 2 * t : energy + 2 * (uint64_t)(done + t);
-                e = vfb::reduce_partials(box->partials, box->blocks, dst, s);
+                e = vfb::reduce_partials(box->partials, n_partials, dst, s);
             }
             box->even = !box->even;
         }
@@ -719,6 +729,33 @@ int vfb_box_fields(vfb_box *box, void *rho, void *ux, void *uy, void *uz, int32_
     for (int i = 0; i < 4 && e == cudaSuccess && to_host; ++i)
         e = cudaMemcpyAsync(out[i], dev[i], fb, cudaMemcpyDeviceToHost, s);
     return cuda_status(e, "box fields");
+}
+
+int vfb_box_status(vfb_box *box, int32_t *device_status, void *stream)
+{
+    if (!box || !device_status)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    int v = 0;
+    cudaError_t e = cudaMemcpyAsync(&v, box->status, sizeof(int), cudaMemcpyDeviceToHost, as_stream(stream));
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(as_stream(stream));
+    *device_status = v;
+    int st = cuda_status(e, "box status");
+    if (st)
+        return st;
+    if (v != 0)
+        return fail(VFB_ERR_CUDA, "a kernel of this box gave up waiting for its staged copies");
+    return VFB_OK;
+}
+
+int vfb_box_set_kernel_variant(vfb_box *box, int32_t variant)
+{
+    if (!box || variant < 0 || variant > 2)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "variant must be 0 (choose), 1 (direct loads) or 2 (TMA-staged)");
+    if (variant == 2 && box->desc.nx % 128 != 0)
+        return fail(VFB_ERR_UNSUPPORTED, "the TMA-staged kernel needs nx % 128 == 0");
+    box->state.variant = variant;
+    return VFB_OK;
 }
 
 int vfb_box_populations(const vfb_box *box, void **dist, uint64_t *pitch, int32_t *is_even)

@@ -11,6 +11,7 @@
 
 #include "k17.cuh"
 #include "storage.cuh"
+#include "tma.cuh"
 
 #ifndef VFB_NS
 #error "VFB_NS must name the compilation variant"
@@ -230,6 +231,175 @@ __global__ void __launch_bounds__(128) k17_box_kernel(BoxCollideArgs<typename Co
             const uint64_t b = blockIdx.x + (uint64_t)gridDim.x * (blockIdx.y + (uint64_t)gridDim.y * blockIdx.z);
             a.energy_partials[2 * b] = mm;
             a.energy_partials[2 * b + 1] = ee;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// The same collision + streaming with the populations of the next tile staged in shared memory by
+// bulk asynchronous copies (TMA) while the current tile computes.
+//
+// Persistent blocks of 128 threads walk the tiles (128 nodes of one x-row) of the box. For every
+// tile one thread issues 27 one-dimensional bulk copies, one per direction plane, of the row
+// segment the tile reads (shifted by one node in x, y or z for directions with negative
+// components; the x-shifted ones copy 16 extra bytes); an mbarrier counts the bytes in. With two
+// stages the copies of tile i+1 are in flight while tile i computes, so memory latency overlaps
+// the FP64 arithmetic instead of stalling the warps. Results go straight to global memory: in
+// the esoteric twist each node writes exactly the slots it read, so the stores of one tile never
+// touch slots another tile still has to load.
+// Requires nx % 128 == 0 (rows split into whole tiles, 16-byte aligned rows).
+// ---------------------------------------------------------------------------------------------
+template <class S>
+struct TmaTile {
+    static constexpr int BX = 128;
+    static constexpr int EXTRA = 16 / (int)sizeof(S);
+    static constexpr int ROW = BX + EXTRA;
+    static constexpr int STAGES = 2;
+    static constexpr uint32_t STAGE_ELEMS = 27u * ROW;
+    static constexpr size_t SMEM = STAGES * STAGE_ELEMS * sizeof(S) + STAGES * sizeof(uint64_t);
+};
+
+template <class S, bool EVEN, class A>
+__device__ __forceinline__ void tma_issue_tile(const A &a, int64_t t, S *stage, uint64_t *bar)
+{
+    using T = TmaTile<S>;
+    const int tiles_x = a.nx / T::BX;
+    const int xt = (int)(t % tiles_x);
+    const int64_t r = t / tiles_x;
+    const int y = (int)(r % a.ny), z = (int)(r / a.ny);
+    const int x0 = xt * T::BX;
+    const int yp = (y + 1 < a.ny) ? y + 1 : (a.periodic_y ? 0 : y);
+    const int zp = (z + 1 < a.nz) ? z + 1 : (a.periodic_z ? 0 : z);
+    const bool row_end = x0 + T::BX == a.nx;
+    uint32_t total = 0;
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        total += T::BX * (uint32_t)sizeof(S) + ((cx(d) < 0 && (!row_end || a.periodic_x)) ? 16u : 0u);
+    mbar_arrive_expect_tx(bar, total);
+    const S *base = static_cast<const S *>(a.dist);
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        const int yy = cy(d) < 0 ? yp : y, zz = cz(d) < 0 ? zp : z;
+        const S *row = base + (uint64_t)plane<EVEN>(d) * a.pitch + (uint64_t)a.nx * ((uint64_t)yy + (uint64_t)a.ny * zz);
+        S *dst = stage + d * T::ROW;
+        if (cx(d) < 0 && !row_end) {
+            bulk_copy_g2s(dst, row + x0, (T::BX + T::EXTRA) * (uint32_t)sizeof(S), bar);
+        } else {
+            bulk_copy_g2s(dst, row + x0, T::BX * (uint32_t)sizeof(S), bar);
+            if (cx(d) < 0 && a.periodic_x) // x + 1 of the last node wraps to x = 0 of the same row
+                bulk_copy_g2s(dst + T::BX, row, 16u, bar);
+        }
+    }
+}
+
+template <class S, bool EXACT, bool EVEN, bool MASK, bool ENERGY>
+__global__ void __launch_bounds__(128) k17_box_tma_kernel(BoxCollideArgs<typename Codec<S>::compute> a, int *status)
+{
+    using C = typename Codec<S>::compute;
+    using T = TmaTile<S>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    S *buf = reinterpret_cast<S *>(smem_raw);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + T::STAGES * T::STAGE_ELEMS * sizeof(S));
+    const int tid = threadIdx.x;
+    const int tiles_x = a.nx / T::BX;
+    const int64_t ntiles = (int64_t)tiles_x * a.ny * a.nz;
+
+    if (tid == 0) {
+        for (int s = 0; s < T::STAGES; ++s)
+            mbar_init(&bar[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int s = 0; s < T::STAGES; ++s) {
+            const int64_t t = blockIdx.x + (int64_t)s * gridDim.x;
+            if (t < ntiles)
+                tma_issue_tile<S, EVEN>(a, t, buf + s * T::STAGE_ELEMS, &bar[s]);
+        }
+    }
+
+    double m_acc = 0.0, e_acc = 0.0;
+    uint32_t parity = 0; // bit s: parity of the next phase of stage s
+    bool failed = false;
+    int i = 0;
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+        const int s = i & 1;
+        const bool ok = mbar_wait(&bar[s], (parity >> s) & 1u);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        parity ^= 1u << s;
+
+        const int xt = (int)(t % tiles_x);
+        const int64_t r = t / tiles_x;
+        const int y = (int)(r % a.ny), z = (int)(r / a.ny);
+        const int x = xt * T::BX + tid;
+        const uint32_t k = (uint32_t)((uint64_t)a.nx * ((uint64_t)y + (uint64_t)a.ny * z) + x);
+        const bool active = !MASK || __ldg(a.mask + k) != 0;
+        if (active) {
+            const S *sb = buf + s * T::STAGE_ELEMS;
+            C f[27];
+#pragma unroll
+            for (int d = 0; d < 27; ++d)
+                f[d] = Codec<S>::load(sb + d * T::ROW + tid + (cx(d) < 0 ? 1 : 0), d);
+            C drho, vx, vy, vz;
+            k17_collide<C, EXACT>(f, a.rates, a.fx, a.fy, a.fz, drho, vx, vy, vz);
+            const int xp = (x + 1 < a.nx) ? x + 1 : (a.periodic_x ? 0 : x);
+            const int yp = (y + 1 < a.ny) ? y + 1 : (a.periodic_y ? 0 : y);
+            const int zp = (z + 1 < a.nz) ? z + 1 : (a.periodic_z ? 0 : z);
+            const uint32_t sx = (uint32_t)(xp - x);
+            const uint32_t sy = (uint32_t)((yp - y) * a.nx);
+            const uint32_t sz = (uint32_t)((int64_t)(zp - z) * a.nx * a.ny);
+            const uint32_t nodes[8] = { k, k + sx, k + sy, k + sx + sy, k + sz, k + sx + sz, k + sy + sz, k + sx + sy + sz };
+            scatter_post<S, EVEN>(static_cast<S *>(a.dist), a.pitch, nodes, f);
+            if (ENERGY) {
+                m_acc += 1.0 + (double)drho;
+                e_acc += 0.5 * (1.0 + (double)drho) * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
+            }
+        }
+        __syncthreads(); // every thread is done with stage s
+        if (tid == 0) {
+            const int64_t tn = t + (int64_t)T::STAGES * gridDim.x;
+            if (tn < ntiles) {
+                fence_proxy_async_smem();
+                tma_issue_tile<S, EVEN>(a, tn, buf + s * T::STAGE_ELEMS, &bar[s]);
+            }
+        }
+    }
+
+    if (failed) {
+        if (tid == 0) {
+            atomicExch(status, (int)kDevWaitTimeout);
+            // let copies still in flight land before the block's shared memory is released
+            for (int s = 0; s < T::STAGES; ++s)
+                mbar_wait(&bar[s], (parity >> s) & 1u, 1u << 16);
+        }
+        __syncthreads();
+        return;
+    }
+
+    if (ENERGY) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            m_acc += __shfl_down_sync(0xffffffffu, m_acc, o);
+            e_acc += __shfl_down_sync(0xffffffffu, e_acc, o);
+        }
+        __shared__ double red[2][4];
+        const int warp = tid >> 5, lane = tid & 31;
+        if (lane == 0) {
+            red[0][warp] = m_acc;
+            red[1][warp] = e_acc;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double mm = 0.0, ee = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+                mm += red[0][w];
+                ee += red[1][w];
+            }
+            a.energy_partials[2 * blockIdx.x] = mm;
+            a.energy_partials[2 * blockIdx.x + 1] = ee;
         }
     }
 }

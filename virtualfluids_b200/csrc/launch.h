@@ -24,6 +24,8 @@ struct BoxState {
     double omega;
     double fx, fy, fz;            // half acceleration
     double lim[3];
+    int variant;                  // 0: choose, 1: direct loads, 2: TMA-staged (needs nx % 128 == 0)
+    int *status;                  // device status word (DeviceError), nullable
 };
 
 // block shape of the box kernels: x extent of a block (multiple of 32, at most 128)
@@ -48,7 +50,8 @@ inline uint64_t box_blocks(const BoxState &b)
         static cudaError_t macros_list(const vfb_level *L, cudaStream_t s);                                        \
         static cudaError_t energy_list(const vfb_level *L, const uint32_t *idx, uint32_t n, double *partials,     \
                                        cudaStream_t s);                                                            \
-        static cudaError_t box_collide(const BoxState &b, bool even, double *partials, cudaStream_t s);            \
+        static cudaError_t box_collide(const BoxState &b, bool even, double *partials, uint64_t *n_partials,        \
+                                       cudaStream_t s);                                                            \
         static cudaError_t box_init(const BoxState &b, bool even, const void *rho, const void *ux, const void *uy, \
                                     const void *uz, cudaStream_t s);                                               \
         static cudaError_t box_macros(const BoxState &b, bool even, void *rho, void *ux, void *uy, void *uz,       \

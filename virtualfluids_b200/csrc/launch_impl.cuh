@@ -1,6 +1,8 @@
 // Definitions of Launchers<S> for one arithmetic variant (VFB_NS, VFB_EXACT). Included by the
 // per-storage translation units, which explicitly instantiate one storage type each.
 #pragma once
+#include <algorithm>
+
 #include "kernels.cuh"
 #include "launch.h"
 
@@ -221,14 +223,70 @@ inline dim3 box_grid(const BoxState &b)
 }
 } // namespace
 
+namespace {
+int sm_count()
+{
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    }
+    return n;
+}
+
+// launch one TMA-staged instantiation: persistent grid sized by occupancy
+template <class S, bool E, bool M, bool N>
+cudaError_t launch_box_tma(const BoxCollideArgs<typename Codec<S>::compute> &a, int *status, uint64_t *n_partials,
+                           cudaStream_t s)
+{
+    auto kern = k17_box_tma_kernel<S, VFB_EXACT, E, M, N>;
+    static int blocks_per_sm = -1;
+    if (blocks_per_sm < 0) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TmaTile<S>::SMEM);
+        if (e != cudaSuccess)
+            return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, 128, TmaTile<S>::SMEM);
+        if (e != cudaSuccess)
+            return e;
+        if (blocks_per_sm < 1)
+            blocks_per_sm = 1;
+    }
+    const int64_t ntiles = (int64_t)(a.nx / TmaTile<S>::BX) * a.ny * a.nz;
+    const int64_t grid = std::min<int64_t>(ntiles, (int64_t)blocks_per_sm * sm_count());
+    kern<<<(unsigned)grid, 128, TmaTile<S>::SMEM, s>>>(a, status);
+    if (n_partials)
+        *n_partials = (uint64_t)grid;
+    return cudaGetLastError();
+}
+} // namespace
+
 template <class S>
-cudaError_t Launchers<S>::box_collide(const BoxState &b, bool even, double *partials, cudaStream_t s)
+cudaError_t Launchers<S>::box_collide(const BoxState &b, bool even, double *partials, uint64_t *n_partials, cudaStream_t s)
 {
     using C = typename Codec<S>::compute;
     BoxCollideArgs<C> a = box_args<C>(b);
     a.energy_partials = partials;
-    const dim3 G = box_grid(b), B(box_block_x(b.nx));
     const bool mask = b.mask != nullptr, energy = partials != nullptr;
+    const bool tma = b.variant != 1 && (b.nx % TmaTile<S>::BX) == 0 && b.status != nullptr;
+    if (tma) {
+#define VFB_K17T(E, M, N) return launch_box_tma<S, E, M, N>(a, b.status, n_partials, s)
+        if (even) {
+            if (mask && energy) VFB_K17T(true, true, true);
+            else if (mask) VFB_K17T(true, true, false);
+            else if (energy) VFB_K17T(true, false, true);
+            else VFB_K17T(true, false, false);
+        } else {
+            if (mask && energy) VFB_K17T(false, true, true);
+            else if (mask) VFB_K17T(false, true, false);
+            else if (energy) VFB_K17T(false, false, true);
+            else VFB_K17T(false, false, false);
+        }
+#undef VFB_K17T
+    }
+    const dim3 G = box_grid(b), B(box_block_x(b.nx));
+    if (n_partials)
+        *n_partials = (uint64_t)G.x * G.y * G.z;
 #define VFB_K17B(E, M, N) k17_box_kernel<S, VFB_EXACT, E, M, N, false><<<G, B, 0, s>>>(a)
     if (even) {
         if (mask && energy) VFB_K17B(true, true, true);

@@ -1,0 +1,65 @@
+// Bulk asynchronous copies (TMA, cp.async.bulk) and mbarriers for sm_100a, with bounded waits.
+//
+// Every wait on an mbarrier gives up after a fixed number of polls and reports failure, so a
+// copy that never lands ends the kernel with an error flag instead of a hang.
+#pragma once
+#include <cstdint>
+
+namespace vfb {
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+// make initialised barriers visible to the async proxy
+__device__ __forceinline__ void fence_barrier_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// order this thread's earlier generic-proxy shared-memory accesses before later async-proxy ones
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+// 1-D bulk copy global -> shared, completion counted on the mbarrier (16-byte aligned, size % 16 == 0)
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+// bounded wait for the phase with the given parity to complete; false after `max_polls` polls
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t max_polls = (1u << 22))
+{
+    const uint32_t addr = smem_addr(bar);
+    for (uint32_t i = 0; i < max_polls; ++i) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(addr), "r"(parity)
+                     : "memory");
+        if (done)
+            return true;
+    }
+    return false;
+}
+
+// error codes a kernel can leave in its status word
+enum DeviceError : int { kDevOk = 0, kDevWaitTimeout = 1 };
+
+} // namespace vfb
