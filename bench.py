@@ -183,7 +183,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--arith", default="fast", choices=["fast", "exact"],
                     help="exact: every operation rounded as the reference's host build (bitwise oracle parity)")
-    ap.add_argument("--kernel", default="auto", choices=["auto", "direct", "tma"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "direct", "tma", "async"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -299,7 +299,8 @@ def main():
     if not args.no_forms:
         for st in ("f32", "f16", "bf16"):
             b = vfb.Box(n, n, n, omega, storage=st)
-            b.set_kernel_variant(args.kernel)
+            if args.kernel != "async" or st == "f32":
+                b.set_kernel_variant(args.kernel)
             b.init(*(torch.from_numpy(a.astype(np.float32)).to(dev) for a in fields), stream=sp)
             b.step(args.warmup, stream=sp)
             ks = min(args.steps, 200)

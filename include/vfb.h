@@ -234,7 +234,9 @@ int vfb_box_fields(vfb_box *box, void *rho, void *ux, void *uy, void *uz, int32_
 /* synchronises the stream and reads the status word the box's kernels set on a failed internal wait
    (0 = fine); returns VFB_ERR_CUDA when it is nonzero */
 int vfb_box_status(vfb_box *box, int32_t *device_status, void *stream);
-/* collision kernel: 0 = choose (TMA-staged when nx % 128 == 0), 1 = direct loads, 2 = TMA-staged */
+/* collision kernel: 0 = choose (per-thread asynchronous copies for F64/F32 storage, direct loads for
+   16-bit storage), 1 = direct loads, 2 = TMA-staged warp tiles (nx % 32 == 0),
+   3 = per-thread asynchronous copies (F64 and F32 storage) */
 int vfb_box_set_kernel_variant(vfb_box *box, int32_t variant);
 /* raw access to the population planes for checks: pointer, plane pitch (elements), parity */
 int vfb_box_populations(const vfb_box *box, void **dist, uint64_t *pitch, int32_t *is_even);

@@ -96,8 +96,9 @@ class Box:
         return v.value
 
     def set_kernel_variant(self, variant: str):
-        """'auto', 'direct' (plain loads) or 'tma' (bulk copies staged in shared memory)."""
-        N.check(N.lib().vfb_box_set_kernel_variant(self._h, {"auto": 0, "direct": 1, "tma": 2}[variant]))
+        """'auto', 'direct' (plain loads), 'tma' (bulk copies staged in shared memory) or 'async'
+        (per-thread asynchronous copies of the next node)."""
+        N.check(N.lib().vfb_box_set_kernel_variant(self._h, {"auto": 0, "direct": 1, "tma": 2, "async": 3}[variant]))
 
     def populations(self):
         """(device pointer, plane pitch in elements, is_even) of the population array."""

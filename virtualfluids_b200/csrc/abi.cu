@@ -750,10 +750,13 @@ int vfb_box_status(vfb_box *box, int32_t *device_status, void *stream)
 
 int vfb_box_set_kernel_variant(vfb_box *box, int32_t variant)
 {
-    if (!box || variant < 0 || variant > 2)
-        return fail(VFB_ERR_INVALID_ARGUMENT, "variant must be 0 (choose), 1 (direct loads) or 2 (TMA-staged)");
-    if (variant == 2 && box->desc.nx % 128 != 0)
-        return fail(VFB_ERR_UNSUPPORTED, "the TMA-staged kernel needs nx % 128 == 0");
+    if (!box || variant < 0 || variant > 3)
+        return fail(VFB_ERR_INVALID_ARGUMENT,
+                    "variant must be 0 (choose), 1 (direct loads), 2 (TMA-staged) or 3 (per-thread async copies)");
+    if (variant == 3 && box->desc.storage > VFB_STORAGE_F32)
+        return fail(VFB_ERR_UNSUPPORTED, "per-thread async copies move 4 or 8 bytes: F64 and F32 storage only");
+    if (variant == 2 && box->desc.nx % 32 != 0)
+        return fail(VFB_ERR_UNSUPPORTED, "the TMA-staged kernel needs nx % 32 == 0");
     box->state.variant = variant;
     return VFB_OK;
 }

@@ -49,7 +49,7 @@ inline K17Rates<T> make_k17_rates(T omega, T qP, T qM, T qD)
 namespace k17detail {
 
 template <class T>
-__device__ __forceinline__ void fwd_k(T &a, T &b, T &c, T v, T v2, T kinv, T k)
+__host__ __device__ __forceinline__ void fwd_k(T &a, T &b, T &c, T v, T v2, T kinv, T k)
 {
     const T s2 = a + c;
     const T s1 = c - a;
@@ -61,7 +61,7 @@ __device__ __forceinline__ void fwd_k(T &a, T &b, T &c, T v, T v2, T kinv, T k)
     c = ((s2 - T(2) * s1 * v) * kinv + v2 * s0) * k;
 }
 template <class T>
-__device__ __forceinline__ void bwd_k(T &a, T &b, T &c, T v, T v2, T kinv, T k)
+__host__ __device__ __forceinline__ void bwd_k(T &a, T &b, T &c, T v, T v2, T kinv, T k)
 {
     const T h = T(0.5);
     const T r0 = (((c - b) * h + b * v) * kinv + (a * kinv + T(1)) * (v2 - v) * h) * k;
@@ -71,7 +71,7 @@ __device__ __forceinline__ void bwd_k(T &a, T &b, T &c, T v, T v2, T kinv, T k)
     b = r1;
 }
 template <class T>
-__device__ __forceinline__ void fwd(T &a, T &b, T &c, T v, T v2)
+__host__ __device__ __forceinline__ void fwd(T &a, T &b, T &c, T v, T v2)
 {
     const T s1 = (a + c) + b;
     const T s2 = c - a;
@@ -80,7 +80,7 @@ __device__ __forceinline__ void fwd(T &a, T &b, T &c, T v, T v2)
     a = s1;
 }
 template <class T>
-__device__ __forceinline__ void bwd(T &a, T &b, T &c, T v, T v2)
+__host__ __device__ __forceinline__ void bwd(T &a, T &b, T &c, T v, T v2)
 {
     const T h = T(0.5);
     const T ra = (c + a * (v2 - v)) * h + b * (v - h);
@@ -91,19 +91,19 @@ __device__ __forceinline__ void bwd(T &a, T &b, T &c, T v, T v2)
 }
 
 // chimera constants, as the reference writes them (c36o1, c1o36, c9o4, c4o9, ...)
-template <class T> __device__ __forceinline__ T kinv_z(int a, int b)
+template <class T> __host__ __device__ __forceinline__ T kinv_z(int a, int b)
 {
     return (a != 1 && b != 1) ? T(36) : (a == 1 && b == 1) ? T(9) / T(4) : T(9);
 }
-template <class T> __device__ __forceinline__ T k_z(int a, int b)
+template <class T> __host__ __device__ __forceinline__ T k_z(int a, int b)
 {
     return (a != 1 && b != 1) ? T(1) / T(36) : (a == 1 && b == 1) ? T(4) / T(9) : T(1) / T(9);
 }
-template <class T> __device__ __forceinline__ T kinv_y(int a, int c)
+template <class T> __host__ __device__ __forceinline__ T kinv_y(int a, int c)
 {
     return a != 1 ? (c == 0 ? T(6) : T(18)) : (c == 0 ? T(3) / T(2) : T(9) / T(2));
 }
-template <class T> __device__ __forceinline__ T k_y(int a, int c)
+template <class T> __host__ __device__ __forceinline__ T k_y(int a, int c)
 {
     return a != 1 ? (c == 0 ? T(1) / T(6) : T(1) / T(18)) : (c == 0 ? T(2) / T(3) : T(2) / T(9));
 }
@@ -112,7 +112,7 @@ template <class T> __device__ __forceinline__ T k_y(int a, int c)
 
 // pyramid density (MacroscopicQuantities.h:55), f in direction order
 template <class T>
-__device__ __forceinline__ T density_pyramid(const T *f)
+__host__ __device__ __forceinline__ T density_pyramid(const T *f)
 {
     const T corners = ((f[19] + f[26]) + (f[24] + f[21])) + ((f[20] + f[25]) + (f[22] + f[23]));
     const T edges = (((f[18] + f[17]) + (f[16] + f[15])) + ((f[14] + f[13]) + (f[12] + f[11]))) + ((f[10] + f[9]) + (f[8] + f[7]));
@@ -120,21 +120,21 @@ __device__ __forceinline__ T density_pyramid(const T *f)
     return ((corners + edges) + f[0]) + faces;
 }
 template <class T>
-__device__ __forceinline__ T momentum_x(const T *f)
+__host__ __device__ __forceinline__ T momentum_x(const T *f)
 {
     return ((((f[19] - f[26]) + (f[21] - f[24])) + ((f[25] - f[20]) + (f[23] - f[22])))
           + (((f[13] - f[14]) + (f[11] - f[12])) + ((f[9] - f[10]) + (f[7] - f[8]))))
           + (f[1] - f[2]);
 }
 template <class T>
-__device__ __forceinline__ T momentum_y(const T *f)
+__host__ __device__ __forceinline__ T momentum_y(const T *f)
 {
     return ((((f[19] - f[26]) + (f[24] - f[21])) + ((f[20] - f[25]) + (f[23] - f[22])))
           + (((f[17] - f[18]) + (f[15] - f[16])) + ((f[10] - f[9]) + (f[7] - f[8]))))
           + (f[3] - f[4]);
 }
 template <class T>
-__device__ __forceinline__ T momentum_z(const T *f)
+__host__ __device__ __forceinline__ T momentum_z(const T *f)
 {
     return ((((f[19] - f[26]) + (f[21] - f[24])) + ((f[20] - f[25]) + (f[22] - f[23])))
           + (((f[18] - f[17]) + (f[15] - f[16])) + ((f[14] - f[13]) + (f[11] - f[12]))))
@@ -144,7 +144,7 @@ __device__ __forceinline__ T momentum_z(const T *f)
 // In place on f[27] (direction order). fx, fy, fz: half the acceleration, already scaled.
 // Returns drho and the velocity including the half force (MacroscopicValues).
 template <class T, bool EXACT>
-__device__ __forceinline__ void k17_collide(T *f, const K17Rates<T> &r, T fx, T fy, T fz, T &drho_out, T &vx_out,
+__host__ __device__ __forceinline__ void k17_collide(T *f, const K17Rates<T> &r, T fx, T fy, T fz, T &drho_out, T &vx_out,
                                             T &vy_out, T &vz_out)
 {
     using namespace k17detail;
@@ -329,4 +329,302 @@ __device__ __forceinline__ void k17_collide(T *f, const K17Rates<T> &r, T fx, T 
     vz_out = vz;
 }
 
+// ---------------------------------------------------------------------------------------------
+// The same collision, rearranged for fewer floating-point instructions (the FMA variant).
+//
+// Mathematically identical to k17_collide, rounded differently:
+//  * the well-conditioned chimera transforms are used in their K-offset form,
+//    b' = m1 - v (m0 + K), c' = m2 - 2 v m1 + v^2 (m0 + K) (forward) and the matching backward
+//    form -- the reference's forwardChimeraWithK / backwardChimeraWithK
+//    (src/lbm/ChimeraTransformation.h:124-150) -- since (x K^-1 + 1) K = x + K;
+//  * density and momenta share the 13 pair sums and differences f_d +- f_inv(d);
+//  * the eight reciprocals of a node (1/rho and the seven quartic-limiter denominators) come from
+//    one division (product of the denominators, then back-substitution);
+//  * omega-only products are folded into single constants.
+// ---------------------------------------------------------------------------------------------
+template <class T>
+struct K17FastConst {
+    T omega;
+    T OxyyPxzz, OxyyMxzz, Oxyz;
+    T kA;       // -(1/omega - 1/2) * 2/3 * factorA
+    T kB;       // -(1/omega - 1/2) * 1/3 * factorB
+    T qP, qM, qD;
+};
+
+template <class T>
+__host__ __device__ inline K17FastConst<T> make_k17_fast_const(const K17Rates<T> &r)
+{
+    K17FastConst<T> c;
+    c.omega = r.omega;
+    c.OxyyPxzz = r.OxyyPxzz;
+    c.OxyyMxzz = r.OxyyMxzz;
+    c.Oxyz = r.Oxyz;
+    c.kA = r.neg_iwm * (T(2) / T(3)) * r.factorA;
+    c.kB = r.neg_iwm * (T(1) / T(3)) * r.factorB;
+    c.qP = r.qP;
+    c.qM = r.qM;
+    c.qD = r.qD;
+    return c;
+}
+
+namespace k17detail {
+// forward transform along one line with offset K (K = 0: the plain central-moment transform)
+template <class T>
+__host__ __device__ __forceinline__ void fwdK(T &a, T &b, T &c, T v, T v2, T twov, T K)
+{
+    const T apc = a + c;
+    const T m1 = c - a;
+    const T m0 = apc + b;
+    const T w = m0 + K;
+    a = m0;
+    b = fma(-v, w, m1);
+    c = fma(v2, w, fma(-twov, m1, apc));
+}
+// backward transform with offset K
+template <class T>
+__host__ __device__ __forceinline__ void bwdK(T &a, T &b, T &c, T v, T v2mv, T v2pv, T twov, T v2, T K)
+{
+    const T w = a + K;
+    const T hb = T(0.5) * b, hc = T(0.5) * c;
+    const T hw = T(0.5) * w;
+    const T r0 = fma(hw, v2mv, fma(b, v, hc - hb));
+    const T r1 = fma(-v2, w, fma(-twov, b, a - c));
+    c = fma(hw, v2pv, fma(b, v, hc + hb));
+    a = r0;
+    b = r1;
+}
+// 1/x: IEEE division in double; the fast approximate division in float
+template <class T>
+__host__ __device__ __forceinline__ T fast_rcp(T x)
+{
+    return T(1) / x;
+}
+template <>
+__host__ __device__ __forceinline__ float fast_rcp<float>(float x)
+{
+#ifdef __CUDA_ARCH__
+    return __fdividef(1.0f, x);
+#else
+    return 1.0f / x;
+#endif
+}
+
+// the seven limiter reciprocals: in double one division and back-substitution through the
+// running products (the denominators are >= the limiters, so the product stays far above the
+// double range limit); in float seven fast divisions (a float product could underflow)
+template <class T>
+__host__ __device__ __forceinline__ void limiter_inverses(const T (&d)[7], T (&iv)[7])
+{
+    const T p1 = d[0] * d[1], p2 = p1 * d[2], p3 = p2 * d[3], p4 = p3 * d[4], p5 = p4 * d[5], p6 = p5 * d[6];
+    T rr = T(1) / p6;
+    iv[6] = rr * p5;
+    rr *= d[6];
+    iv[5] = rr * p4;
+    rr *= d[5];
+    iv[4] = rr * p3;
+    rr *= d[4];
+    iv[3] = rr * p2;
+    rr *= d[3];
+    iv[2] = rr * p1;
+    rr *= d[2];
+    iv[1] = rr * d[0];
+    iv[0] = rr * d[1];
+}
+template <>
+__host__ __device__ __forceinline__ void limiter_inverses<float>(const float (&d)[7], float (&iv)[7])
+{
+#pragma unroll
+    for (int i = 0; i < 7; ++i)
+        iv[i] = fast_rcp<float>(d[i]);
+}
+} // namespace k17detail
+
+template <class T>
+__host__ __device__ __forceinline__ void k17_collide_fast(T *f, const K17FastConst<T> &r, T fx, T fy, T fz, T &drho_out,
+                                                 T &vx_out, T &vy_out, T &vz_out)
+{
+    using namespace k17detail;
+    // pair sums / differences, canonical direction first
+    const T s1 = f[1] + f[2], t1 = f[1] - f[2];       // P00
+    const T s3 = f[3] + f[4], t3 = f[3] - f[4];       // 0P0
+    const T s5 = f[5] + f[6], t5 = f[5] - f[6];       // 00P
+    const T s7 = f[7] + f[8], t7 = f[7] - f[8];       // PP0
+    const T s9 = f[9] + f[10], t9 = f[9] - f[10];     // PM0
+    const T s11 = f[11] + f[12], t11 = f[11] - f[12]; // P0P
+    const T s13 = f[13] + f[14], t13 = f[13] - f[14]; // P0M
+    const T s15 = f[15] + f[16], t15 = f[15] - f[16]; // 0PP
+    const T s17 = f[17] + f[18], t17 = f[17] - f[18]; // 0PM
+    const T s19 = f[19] + f[26], t19 = f[19] - f[26]; // PPP
+    const T s21 = f[21] + f[24], t21 = f[21] - f[24]; // PMP
+    const T s23 = f[23] + f[22], t23 = f[23] - f[22]; // PPM
+    const T s25 = f[25] + f[20], t25 = f[25] - f[20]; // PMM
+    const T drho = ((((s19 + s21) + (s23 + s25)) + ((s7 + s9) + (s11 + s13))) + ((s15 + s17) + (s1 + s3))) + (s5 + f[0]);
+    const T jx = (((t19 + t21) + (t23 + t25)) + ((t7 + t9) + (t11 + t13))) + t1;
+    const T jy = (((t19 - t21) + (t23 - t25)) + ((t7 - t9) + (t15 + t17))) + t3;
+    const T jz = (((t19 + t21) - (t23 + t25)) + ((t11 - t13) + (t15 - t17))) + t5;
+
+    const T oneOverRho = fast_rcp(drho + T(1));
+    const T vx = fma(jx, oneOverRho, fx), vy = fma(jy, oneOverRho, fy), vz = fma(jz, oneOverRho, fz);
+    const T vx2 = vx * vx, vy2 = vy * vy, vz2 = vz * vz;
+    const T twovx = T(2) * vx, twovy = T(2) * vy, twovz = T(2) * vz;
+
+    T m[27];
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        m[m3(d)] = f[d];
+#define M(a, b, c) m[(a) * 9 + (b) * 3 + (c)]
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+            fwdK(M(a, b, 0), M(a, b, 1), M(a, b, 2), vz, vz2, twovz, k_z<T>(a, b));
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            fwdK(M(a, 0, c), M(a, 1, c), M(a, 2, c), vy, vy2, twovy, c == 1 ? T(0) : k_y<T>(a, c));
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const T K = (b == 0 && c == 0) ? T(1) : ((b == 2 || c == 2) && b != 1 && c != 1) ? T(1) / T(3) : T(0);
+            fwdK(M(0, b, c), M(1, b, c), M(2, b, c), vx, vx2, twovx, K);
+        }
+    // K17...h:222 transforms the (2,2) x-line with K^-1 = 3 but K = 1/9: the offset is 1/K^-1 = 1/3
+    // and the two higher moments come out scaled by K^-1 K = 1/3
+    M(1, 2, 2) *= T(1) / T(3);
+    M(2, 2, 2) *= T(1) / T(3);
+
+    const T c13 = T(1) / T(3), c19 = T(1) / T(9), c23 = T(2) / T(3), c127 = T(1) / T(27), h = T(0.5);
+    const T omega = r.omega;
+
+    T mxxPyyPzz = M(2, 0, 0) + M(0, 2, 0) + M(0, 0, 2);
+    T mxxMyy = M(2, 0, 0) - M(0, 2, 0);
+    T mxxMzz = M(2, 0, 0) - M(0, 0, 2);
+    T mxxyPyzz = M(2, 1, 0) + M(0, 1, 2);
+    T mxxyMyzz = M(2, 1, 0) - M(0, 1, 2);
+    T mxxzPyyz = M(2, 0, 1) + M(0, 2, 1);
+    T mxxzMyyz = M(2, 0, 1) - M(0, 2, 1);
+    T mxyyPxzz = M(1, 2, 0) + M(1, 0, 2);
+    T mxyyMxzz = M(1, 2, 0) - M(1, 0, 2);
+
+    const T m3omega = -T(3) * omega;
+    const T Dxy = m3omega * M(1, 1, 0);
+    const T Dxz = m3omega * M(1, 0, 1);
+    const T Dyz = m3omega * M(0, 1, 1);
+    const T dxux = fma(-h * omega, mxxMyy + mxxMzz, h * (M(0, 0, 0) - mxxPyyPzz));
+    const T o32 = omega * T(1.5);
+    const T dyuy = fma(o32, mxxMyy, dxux);
+    const T dzuz = fma(o32, mxxMzz, dxux);
+
+    const T c3h = T(3) * (T(1) - h * omega);
+    mxxPyyPzz += (M(0, 0, 0) - mxxPyyPzz) - T(1.5) * (vx2 * dxux + vy2 * dyuy + vz2 * dzuz);
+    mxxMyy = fma(-omega, mxxMyy, mxxMyy) - c3h * (vx2 * dxux - vy2 * dyuy);
+    mxxMzz = fma(-omega, mxxMzz, mxxMzz) - c3h * (vx2 * dxux - vz2 * dzuz);
+    const T omo = T(1) - omega;
+    M(0, 1, 1) *= omo;
+    M(1, 0, 1) *= omo;
+    M(1, 1, 0) *= omo;
+
+    // quartic limiters: seven reciprocals from one division
+    const T a0 = fabs(M(1, 1, 1)), a1 = fabs(mxxyPyzz), a2 = fabs(mxxyMyzz), a3 = fabs(mxxzPyyz);
+    const T a4 = fabs(mxxzMyyz), a5 = fabs(mxyyPxzz), a6 = fabs(mxyyMxzz);
+    const T dd[7] = { a0 + r.qD, a1 + r.qP, a2 + r.qM, a3 + r.qP, a4 + r.qM, a5 + r.qP, a6 + r.qM };
+    T iv[7];
+    limiter_inverses<T>(dd, iv);
+    const T i0 = iv[0], i1 = iv[1], i2 = iv[2], i3 = iv[3], i4 = iv[4], i5 = iv[5], i6 = iv[6];
+    // m += (O + (1-O) |m|/(|m|+q)) (-m)
+    M(1, 1, 1) -= fma(T(1) - r.Oxyz, a0 * i0, r.Oxyz) * M(1, 1, 1);
+    mxxyPyzz -= fma(T(1) - r.OxyyPxzz, a1 * i1, r.OxyyPxzz) * mxxyPyzz;
+    mxxyMyzz -= fma(T(1) - r.OxyyMxzz, a2 * i2, r.OxyyMxzz) * mxxyMyzz;
+    mxxzPyyz -= fma(T(1) - r.OxyyPxzz, a3 * i3, r.OxyyPxzz) * mxxzPyyz;
+    mxxzMyyz -= fma(T(1) - r.OxyyMxzz, a4 * i4, r.OxyyMxzz) * mxxzMyyz;
+    mxyyPxzz -= fma(T(1) - r.OxyyPxzz, a5 * i5, r.OxyyPxzz) * mxyyPxzz;
+    mxyyMxzz -= fma(T(1) - r.OxyyMxzz, a6 * i6, r.OxyyMxzz) * mxyyMxzz;
+
+    M(2, 0, 0) = c13 * (mxxMyy + mxxMzz + mxxPyyPzz);
+    M(0, 2, 0) = c13 * (-T(2) * mxxMyy + mxxMzz + mxxPyyPzz);
+    M(0, 0, 2) = c13 * (mxxMyy - T(2) * mxxMzz + mxxPyyPzz);
+    M(2, 1, 0) = (mxxyMyzz + mxxyPyzz) * h;
+    M(0, 1, 2) = (mxxyPyzz - mxxyMyzz) * h;
+    M(2, 0, 1) = (mxxzMyyz + mxxzPyyz) * h;
+    M(0, 2, 1) = (mxxzPyyz - mxxzMyyz) * h;
+    M(1, 2, 0) = (mxyyMxzz + mxyyPxzz) * h;
+    M(1, 0, 2) = (mxyyPxzz - mxyyMxzz) * h;
+
+    const T cm022 = r.kA * (dyuy + dzuz);
+    const T cm202 = r.kA * (dxux + dzuz);
+    const T cm220 = r.kA * (dyuy + dxux);
+    const T cm112 = r.kB * Dxy;
+    const T cm121 = r.kB * Dxz;
+    const T cm211 = r.kB * Dyz;
+
+    const T c13r = c13 * oneOverRho;
+    const T drr = drho * oneOverRho;
+    M(2, 1, 1) = fma(c13r, (T(3) * M(2, 0, 0) + T(1)) * M(0, 1, 1) + T(6) * M(1, 1, 0) * M(1, 0, 1), cm211);
+    M(1, 2, 1) = fma(c13r, (T(3) * M(0, 2, 0) + T(1)) * M(1, 0, 1) + T(6) * M(1, 1, 0) * M(0, 1, 1), cm121);
+    M(1, 1, 2) = fma(c13r, (T(3) * M(0, 0, 2) + T(1)) * M(1, 1, 0) + T(6) * M(1, 0, 1) * M(0, 1, 1), cm112);
+    M(2, 2, 0) = cm220 + ((T(9) * (M(2, 0, 0) * M(0, 2, 0) + T(2) * M(1, 1, 0) * M(1, 1, 0)) + T(3) * (M(2, 0, 0) + M(0, 2, 0))) * oneOverRho - drr) * c19;
+    M(2, 0, 2) = cm202 + ((T(9) * (M(2, 0, 0) * M(0, 0, 2) + T(2) * M(1, 0, 1) * M(1, 0, 1)) + T(3) * (M(2, 0, 0) + M(0, 0, 2))) * oneOverRho - drr) * c19;
+    M(0, 2, 2) = cm022 + ((T(9) * (M(0, 0, 2) * M(0, 2, 0) + T(2) * M(0, 1, 1) * M(0, 1, 1)) + T(3) * (M(0, 0, 2) + M(0, 2, 0))) * oneOverRho - drr) * c19;
+    M(1, 2, 2) = c13r * (T(3) * (M(0, 0, 2) * M(1, 2, 0) + M(0, 2, 0) * M(1, 0, 2) + T(4) * M(0, 1, 1) * M(1, 1, 1) + T(2) * (M(1, 0, 1) * M(0, 2, 1) + M(1, 1, 0) * M(0, 1, 2))) + (M(1, 2, 0) + M(1, 0, 2)));
+    M(2, 1, 2) = c13r * (T(3) * (M(0, 0, 2) * M(2, 1, 0) + M(2, 0, 0) * M(0, 1, 2) + T(4) * M(1, 0, 1) * M(1, 1, 1) + T(2) * (M(0, 1, 1) * M(2, 0, 1) + M(1, 1, 0) * M(1, 0, 2))) + (M(2, 1, 0) + M(0, 1, 2)));
+    M(2, 2, 1) = c13r * (T(3) * (M(2, 0, 0) * M(0, 2, 1) + M(0, 2, 0) * M(2, 0, 1) + T(4) * M(1, 1, 0) * M(1, 1, 1) + T(2) * (M(1, 0, 1) * M(1, 2, 0) + M(0, 1, 1) * M(2, 1, 0))) + (M(0, 2, 1) + M(2, 0, 1)));
+    const T r2 = oneOverRho * oneOverRho;
+    M(2, 2, 2) = -((-T(4) * M(1, 1, 1) * M(1, 1, 1) - (M(2, 0, 0) * M(0, 2, 2) + M(0, 2, 0) * M(2, 0, 2) + M(0, 0, 2) * M(2, 2, 0))
+                    - T(4) * (M(0, 1, 1) * M(2, 1, 1) + M(1, 0, 1) * M(1, 2, 1) + M(1, 1, 0) * M(1, 1, 2))
+                    - T(2) * (M(1, 2, 0) * M(1, 0, 2) + M(2, 1, 0) * M(0, 1, 2) + M(2, 0, 1) * M(0, 2, 1))) * oneOverRho
+                   + (T(4) * (M(1, 0, 1) * M(1, 0, 1) * M(0, 2, 0) + M(0, 1, 1) * M(0, 1, 1) * M(2, 0, 0) + M(1, 1, 0) * M(1, 1, 0) * M(0, 0, 2))
+                      + T(2) * (M(2, 0, 0) * M(0, 2, 0) * M(0, 0, 2)) + T(16) * M(1, 1, 0) * M(1, 0, 1) * M(0, 1, 1)) * r2
+                   - (c13 * (M(0, 2, 2) + M(2, 0, 2) + M(2, 2, 0)) + c19 * (M(2, 0, 0) + M(0, 2, 0) + M(0, 0, 2))) * oneOverRho
+                   + (T(2) * (M(1, 0, 1) * M(1, 0, 1) + M(0, 1, 1) * M(0, 1, 1) + M(1, 1, 0) * M(1, 1, 0))
+                      + (M(0, 0, 2) * M(0, 2, 0) + M(0, 0, 2) * M(2, 0, 0) + M(0, 2, 0) * M(2, 0, 0)) + c13 * (M(0, 0, 2) + M(0, 2, 0) + M(2, 0, 0))) * r2 * c23
+                   + c127 * ((drho * drho - drho) * r2));
+
+    M(1, 0, 0) = -M(1, 0, 0);
+    M(0, 1, 0) = -M(0, 1, 0);
+    M(0, 0, 1) = -M(0, 0, 1);
+
+    const T x2mv = vx2 - vx, x2pv = vx2 + vx, y2mv = vy2 - vy, y2pv = vy2 + vy, z2mv = vz2 - vz, z2pv = vz2 + vz;
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const T K = (b == 0 && c == 0) ? T(1) : (b == 2 && c == 2) ? T(1) / T(9)
+                      : ((b == 2 && c == 0) || (b == 0 && c == 2)) ? T(1) / T(3) : T(0);
+            bwdK(M(0, b, c), M(1, b, c), M(2, b, c), vx, x2mv, x2pv, twovx, vx2, K);
+        }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            bwdK(M(a, 0, c), M(a, 1, c), M(a, 2, c), vy, y2mv, y2pv, twovy, vy2, c == 1 ? T(0) : k_y<T>(a, c));
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+            bwdK(M(a, b, 0), M(a, b, 1), M(a, b, 2), vz, z2mv, z2pv, twovz, vz2, k_z<T>(a, b));
+#undef M
+
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        f[d] = m[m3(d)];
+    drho_out = drho;
+    vx_out = vx;
+    vy_out = vy;
+    vz_out = vz;
+}
+
+} // namespace vfb
+
+namespace vfb {
+// the collision of the chosen arithmetic variant
+template <class T, bool EXACT>
+__host__ __device__ __forceinline__ void collide(T *f, const K17Rates<T> &r, T fx, T fy, T fz, T &drho, T &vx, T &vy, T &vz)
+{
+    if constexpr (EXACT)
+        k17_collide<T, true>(f, r, fx, fy, fz, drho, vx, vy, vz);
+    else
+        k17_collide_fast<T>(f, make_k17_fast_const(r), fx, fy, fz, drho, vx, vy, vz);
+}
 } // namespace vfb

@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(128) k17_list_kernel(ListCollideArgs<typename 
     C f[27];
     gather_pre<S, EVEN>(base, a.n, nodes, f);
     C drho, vx, vy, vz;
-    k17_collide<C, EXACT>(f, a.rates, fx, fy, fz, drho, vx, vy, vz);
+    collide<C, EXACT>(f, a.rates, fx, fy, fz, drho, vx, vy, vz);
     if (WRITE_MACRO) {
         a.vx[k] = vx;
         a.vy[k] = vy;
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(128) k17_box_kernel(BoxCollideArgs<typename Co
         S *base = static_cast<S *>(a.dist);
         C f[27];
         gather_pre<S, EVEN>(base, a.pitch, nodes, f);
-        k17_collide<C, EXACT>(f, a.rates, a.fx, a.fy, a.fz, drho, vx, vy, vz);
+        collide<C, EXACT>(f, a.rates, a.fx, a.fy, a.fz, drho, vx, vy, vz);
         if (WRITE_MACRO) {
             a.rho[k] = drho;
             a.vx[k] = vx;
@@ -207,7 +207,8 @@ __global__ void __launch_bounds__(128) k17_box_kernel(BoxCollideArgs<typename Co
     }
 
     if (ENERGY) {
-        // FP64 block partials of mass and kinetic energy, fixed reduction order
+        // FP64 partials of mass and kinetic energy per warp (fixed reduction order, no block barrier,
+        // so the warps of a block retire independently)
         double m = active ? 1.0 + (double)drho : 0.0;
         double e = active ? 0.5 * (1.0 + (double)drho) * ((double)vx * vx + (double)vy * vy + (double)vz * vz) : 0.0;
 #pragma unroll
@@ -215,22 +216,11 @@ __global__ void __launch_bounds__(128) k17_box_kernel(BoxCollideArgs<typename Co
             m += __shfl_down_sync(0xffffffffu, m, o);
             e += __shfl_down_sync(0xffffffffu, e, o);
         }
-        __shared__ double sm[2][4];
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        if (lane == 0) {
-            sm[0][warp] = m;
-            sm[1][warp] = e;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double mm = 0.0, ee = 0.0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-                mm += sm[0][w];
-                ee += sm[1][w];
-            }
+        if ((threadIdx.x & 31) == 0) {
             const uint64_t b = blockIdx.x + (uint64_t)gridDim.x * (blockIdx.y + (uint64_t)gridDim.y * blockIdx.z);
-            a.energy_partials[2 * b] = mm;
-            a.energy_partials[2 * b + 1] = ee;
+            const uint64_t w = b * (blockDim.x >> 5) + (threadIdx.x >> 5);
+            a.energy_partials[2 * w] = m;
+            a.energy_partials[2 * w + 1] = e;
         }
     }
 }
@@ -239,28 +229,33 @@ __global__ void __launch_bounds__(128) k17_box_kernel(BoxCollideArgs<typename Co
 // The same collision + streaming with the populations of the next tile staged in shared memory by
 // bulk asynchronous copies (TMA) while the current tile computes.
 //
-// Persistent blocks of 128 threads walk the tiles (128 nodes of one x-row) of the box. For every
-// tile one thread issues 27 one-dimensional bulk copies, one per direction plane, of the row
-// segment the tile reads (shifted by one node in x, y or z for directions with negative
-// components; the x-shifted ones copy 16 extra bytes); an mbarrier counts the bytes in. With two
-// stages the copies of tile i+1 are in flight while tile i computes, so memory latency overlaps
-// the FP64 arithmetic instead of stalling the warps. Results go straight to global memory: in
-// the esoteric twist each node writes exactly the slots it read, so the stores of one tile never
-// touch slots another tile still has to load.
-// Requires nx % 128 == 0 (rows split into whole tiles, 16-byte aligned rows).
+// Every warp runs its own pipeline: it walks warp tiles (32 consecutive nodes of one x-row) of
+// the box, and for each tile 27 lanes issue one 1-D bulk copy each (one per direction plane) of
+// the row segment the tile reads, shifted by one node in x, y or z for directions with negative
+// components (the x-shifted ones copy 16 extra bytes). A per-warp mbarrier counts the bytes in.
+// With two stages the copies of tile i+1 are in flight while tile i computes, so memory latency
+// overlaps the arithmetic, and no warp ever waits for another (no block-wide barrier in the
+// loop). Results go straight to global memory: in the esoteric twist each node writes exactly
+// the slots it read, so the stores of one tile never touch slots another tile still has to load.
+// Requires nx % 32 == 0 (rows split into whole warp tiles, 16-byte aligned rows).
 // ---------------------------------------------------------------------------------------------
 template <class S>
 struct TmaTile {
-    static constexpr int BX = 128;
-    static constexpr int EXTRA = 16 / (int)sizeof(S);
+    static constexpr int BX = 32;                        // nodes per warp tile
+    static constexpr int WARPS = 4;                      // warps per block
+    static constexpr int EXTRA = 16 / (int)sizeof(S);    // 16 bytes of elements
     static constexpr int ROW = BX + EXTRA;
     static constexpr int STAGES = 2;
     static constexpr uint32_t STAGE_ELEMS = 27u * ROW;
-    static constexpr size_t SMEM = STAGES * STAGE_ELEMS * sizeof(S) + STAGES * sizeof(uint64_t);
+    static constexpr uint32_t WARP_ELEMS = STAGES * STAGE_ELEMS;
+    static constexpr size_t SMEM = WARPS * (WARP_ELEMS * sizeof(S) + STAGES * sizeof(uint64_t));
 };
 
+// issue the copies of tile t into one stage: lane 0 announces the bytes, lanes 0..26 copy one
+// direction each (the announcement precedes the copies in program order of lane 0 and the
+// warp-synchronous __syncwarp orders the other lanes after it)
 template <class S, bool EVEN, class A>
-__device__ __forceinline__ void tma_issue_tile(const A &a, int64_t t, S *stage, uint64_t *bar)
+__device__ __forceinline__ void tma_issue_tile(const A &a, int64_t t, S *stage, uint64_t *bar, int lane)
 {
     using T = TmaTile<S>;
     const int tiles_x = a.nx / T::BX;
@@ -268,25 +263,27 @@ __device__ __forceinline__ void tma_issue_tile(const A &a, int64_t t, S *stage, 
     const int64_t r = t / tiles_x;
     const int y = (int)(r % a.ny), z = (int)(r / a.ny);
     const int x0 = xt * T::BX;
-    const int yp = (y + 1 < a.ny) ? y + 1 : (a.periodic_y ? 0 : y);
-    const int zp = (z + 1 < a.nz) ? z + 1 : (a.periodic_z ? 0 : z);
     const bool row_end = x0 + T::BX == a.nx;
-    uint32_t total = 0;
-#pragma unroll
-    for (int d = 0; d < 27; ++d)
-        total += T::BX * (uint32_t)sizeof(S) + ((cx(d) < 0 && (!row_end || a.periodic_x)) ? 16u : 0u);
-    mbar_arrive_expect_tx(bar, total);
-    const S *base = static_cast<const S *>(a.dist);
-#pragma unroll
-    for (int d = 0; d < 27; ++d) {
-        const int yy = cy(d) < 0 ? yp : y, zz = cz(d) < 0 ? zp : z;
-        const S *row = base + (uint64_t)plane<EVEN>(d) * a.pitch + (uint64_t)a.nx * ((uint64_t)yy + (uint64_t)a.ny * zz);
+    if (lane == 0) {
+        // 9 directions point negative in x: they copy 16 more bytes (the wrap copy at a row end)
+        const uint32_t extra = (!row_end || a.periodic_x) ? 16u : 0u;
+        mbar_arrive_expect_tx(bar, 27u * T::BX * (uint32_t)sizeof(S) + 9u * extra);
+    }
+    __syncwarp();
+    if (lane < 27) {
+        const int d = lane;
+        const int ddx = cx(d), ddy = cy(d), ddz = cz(d);
+        const int yy = ddy < 0 ? ((y + 1 < a.ny) ? y + 1 : (a.periodic_y ? 0 : y)) : y;
+        const int zz = ddz < 0 ? ((z + 1 < a.nz) ? z + 1 : (a.periodic_z ? 0 : z)) : z;
+        const int pl = EVEN ? d : inv(d);
+        const S *row = static_cast<const S *>(a.dist) + (uint64_t)pl * a.pitch
+                     + (uint64_t)a.nx * ((uint64_t)yy + (uint64_t)a.ny * zz);
         S *dst = stage + d * T::ROW;
-        if (cx(d) < 0 && !row_end) {
+        if (ddx < 0 && !row_end) {
             bulk_copy_g2s(dst, row + x0, (T::BX + T::EXTRA) * (uint32_t)sizeof(S), bar);
         } else {
             bulk_copy_g2s(dst, row + x0, T::BX * (uint32_t)sizeof(S), bar);
-            if (cx(d) < 0 && a.periodic_x) // x + 1 of the last node wraps to x = 0 of the same row
+            if (ddx < 0 && a.periodic_x) // x + 1 of the last node wraps to x = 0 of the same row
                 bulk_copy_g2s(dst + T::BX, row, 16u, bar);
         }
     }
@@ -298,34 +295,34 @@ __global__ void __launch_bounds__(128) k17_box_tma_kernel(BoxCollideArgs<typenam
     using C = typename Codec<S>::compute;
     using T = TmaTile<S>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    S *buf = reinterpret_cast<S *>(smem_raw);
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + T::STAGES * T::STAGE_ELEMS * sizeof(S));
-    const int tid = threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    S *buf = reinterpret_cast<S *>(smem_raw) + warp * T::WARP_ELEMS;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + T::WARPS * T::WARP_ELEMS * sizeof(S)) + warp * T::STAGES;
     const int tiles_x = a.nx / T::BX;
     const int64_t ntiles = (int64_t)tiles_x * a.ny * a.nz;
+    const int64_t first = (int64_t)blockIdx.x * T::WARPS + warp;
+    const int64_t stride = (int64_t)gridDim.x * T::WARPS;
 
-    if (tid == 0) {
+    if (lane == 0) {
         for (int s = 0; s < T::STAGES; ++s)
             mbar_init(&bar[s], 1);
         fence_barrier_init();
     }
-    __syncthreads();
-    if (tid == 0) {
-        for (int s = 0; s < T::STAGES; ++s) {
-            const int64_t t = blockIdx.x + (int64_t)s * gridDim.x;
-            if (t < ntiles)
-                tma_issue_tile<S, EVEN>(a, t, buf + s * T::STAGE_ELEMS, &bar[s]);
-        }
+    __syncwarp();
+    for (int s = 0; s < T::STAGES; ++s) {
+        const int64_t t = first + s * stride;
+        if (t < ntiles)
+            tma_issue_tile<S, EVEN>(a, t, buf + s * T::STAGE_ELEMS, &bar[s], lane);
     }
 
     double m_acc = 0.0, e_acc = 0.0;
     uint32_t parity = 0; // bit s: parity of the next phase of stage s
     bool failed = false;
     int i = 0;
-    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+    for (int64_t t = first; t < ntiles; t += stride, ++i) {
         const int s = i & 1;
         const bool ok = mbar_wait(&bar[s], (parity >> s) & 1u);
-        if (__syncthreads_or(!ok)) {
+        if (__any_sync(0xffffffffu, !ok)) {
             failed = true;
             break;
         }
@@ -334,7 +331,7 @@ __global__ void __launch_bounds__(128) k17_box_tma_kernel(BoxCollideArgs<typenam
         const int xt = (int)(t % tiles_x);
         const int64_t r = t / tiles_x;
         const int y = (int)(r % a.ny), z = (int)(r / a.ny);
-        const int x = xt * T::BX + tid;
+        const int x = xt * T::BX + lane;
         const uint32_t k = (uint32_t)((uint64_t)a.nx * ((uint64_t)y + (uint64_t)a.ny * z) + x);
         const bool active = !MASK || __ldg(a.mask + k) != 0;
         if (active) {
@@ -342,9 +339,9 @@ __global__ void __launch_bounds__(128) k17_box_tma_kernel(BoxCollideArgs<typenam
             C f[27];
 #pragma unroll
             for (int d = 0; d < 27; ++d)
-                f[d] = Codec<S>::load(sb + d * T::ROW + tid + (cx(d) < 0 ? 1 : 0), d);
+                f[d] = Codec<S>::load(sb + d * T::ROW + lane + (cx(d) < 0 ? 1 : 0), d);
             C drho, vx, vy, vz;
-            k17_collide<C, EXACT>(f, a.rates, a.fx, a.fy, a.fz, drho, vx, vy, vz);
+            collide<C, EXACT>(f, a.rates, a.fx, a.fy, a.fz, drho, vx, vy, vz);
             const int xp = (x + 1 < a.nx) ? x + 1 : (a.periodic_x ? 0 : x);
             const int yp = (y + 1 < a.ny) ? y + 1 : (a.periodic_y ? 0 : y);
             const int zp = (z + 1 < a.nz) ? z + 1 : (a.periodic_z ? 0 : z);
@@ -358,26 +355,143 @@ __global__ void __launch_bounds__(128) k17_box_tma_kernel(BoxCollideArgs<typenam
                 e_acc += 0.5 * (1.0 + (double)drho) * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
             }
         }
-        __syncthreads(); // every thread is done with stage s
-        if (tid == 0) {
-            const int64_t tn = t + (int64_t)T::STAGES * gridDim.x;
-            if (tn < ntiles) {
-                fence_proxy_async_smem();
-                tma_issue_tile<S, EVEN>(a, tn, buf + s * T::STAGE_ELEMS, &bar[s]);
-            }
-        }
+        // the warp is done reading stage s: order those generic-proxy reads before the async-proxy
+        // writes of the next copies into it
+        fence_proxy_async_smem();
+        __syncwarp();
+        const int64_t tn = t + (int64_t)T::STAGES * stride;
+        if (tn < ntiles)
+            tma_issue_tile<S, EVEN>(a, tn, buf + s * T::STAGE_ELEMS, &bar[s], lane);
     }
 
     if (failed) {
-        if (tid == 0) {
+        if (lane == 0) {
             atomicExch(status, (int)kDevWaitTimeout);
             // let copies still in flight land before the block's shared memory is released
             for (int s = 0; s < T::STAGES; ++s)
                 mbar_wait(&bar[s], (parity >> s) & 1u, 1u << 16);
         }
-        __syncthreads();
-        return;
+        __syncwarp();
     }
+
+    if (ENERGY) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            m_acc += __shfl_down_sync(0xffffffffu, m_acc, o);
+            e_acc += __shfl_down_sync(0xffffffffu, e_acc, o);
+        }
+        __shared__ double red[2][T::WARPS];
+        if (lane == 0) {
+            red[0][warp] = m_acc;
+            red[1][warp] = e_acc;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double mm = 0.0, ee = 0.0;
+            for (int w = 0; w < T::WARPS; ++w) {
+                mm += red[0][w];
+                ee += red[1][w];
+            }
+            a.energy_partials[2 * blockIdx.x] = mm;
+            a.energy_partials[2 * blockIdx.x + 1] = ee;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Collision + streaming with a per-thread software pipeline through shared memory: while a thread
+// computes its node of tile i, cp.async copies of the 27 populations of its node of tile i+1 are
+// in flight into slots of shared memory only this thread uses. Memory latency overlaps the
+// arithmetic without extra registers and without any synchronisation between threads.
+// Persistent blocks of 128 threads walk tiles of 128 nodes of an x-row. F64 and F32 storage
+// (cp.async moves 4 or 8 bytes per copy).
+// ---------------------------------------------------------------------------------------------
+template <class S>
+struct AsyncTile {
+    static constexpr int BX = 128;
+    static constexpr size_t SMEM = 2 * 27 * BX * sizeof(S);
+};
+
+template <class S, bool EVEN, class A>
+__device__ __forceinline__ void async_issue_node(const A &a, int64_t t, int tid, S *stage, uint32_t &k_out, bool &active)
+{
+    const int tiles_x = (a.nx + AsyncTile<S>::BX - 1) / AsyncTile<S>::BX;
+    const int xt = (int)(t % tiles_x);
+    const int64_t r = t / tiles_x;
+    const int y = (int)(r % a.ny), z = (int)(r / a.ny);
+    const int x = xt * AsyncTile<S>::BX + tid;
+    active = x < a.nx;
+    const uint32_t k = (uint32_t)((uint64_t)a.nx * ((uint64_t)y + (uint64_t)a.ny * z) + (active ? x : 0));
+    k_out = k;
+    if (!active)
+        return;
+    const int xp = (x + 1 < a.nx) ? x + 1 : (a.periodic_x ? 0 : x);
+    const int yp = (y + 1 < a.ny) ? y + 1 : (a.periodic_y ? 0 : y);
+    const int zp = (z + 1 < a.nz) ? z + 1 : (a.periodic_z ? 0 : z);
+    const uint32_t sx = (uint32_t)(xp - x), sy = (uint32_t)((yp - y) * a.nx), sz = (uint32_t)((int64_t)(zp - z) * a.nx * a.ny);
+    const uint32_t nodes[8] = { k, k + sx, k + sy, k + sx + sy, k + sz, k + sx + sz, k + sy + sz, k + sx + sy + sz };
+    const S *base = static_cast<const S *>(a.dist);
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        cp_async<(int)sizeof(S)>(stage + d * AsyncTile<S>::BX + tid,
+                                 base + (uint64_t)plane<EVEN>(d) * a.pitch + nodes[shift_class(d)]);
+}
+
+template <class S, bool EXACT, bool EVEN, bool MASK, bool ENERGY>
+__global__ void __launch_bounds__(128) k17_box_async_kernel(BoxCollideArgs<typename Codec<S>::compute> a)
+{
+    using C = typename Codec<S>::compute;
+    constexpr int BX = AsyncTile<S>::BX;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    S *buf = reinterpret_cast<S *>(smem_raw);
+    const int tid = threadIdx.x;
+    const int tiles_x = (a.nx + BX - 1) / BX;
+    const int64_t ntiles = (int64_t)tiles_x * a.ny * a.nz;
+
+    double m_acc = 0.0, e_acc = 0.0;
+    uint32_t k_cur = 0, k_next = 0;
+    bool act_cur = false, act_next = false;
+    int64_t t = blockIdx.x;
+    if (t < ntiles)
+        async_issue_node<S, EVEN>(a, t, tid, buf, k_cur, act_cur);
+    cp_async_commit();
+    for (int i = 0; t < ntiles; t += gridDim.x, ++i) {
+        const int s = i & 1;
+        const int64_t tn = t + gridDim.x;
+        if (tn < ntiles)
+            async_issue_node<S, EVEN>(a, tn, tid, buf + (s ^ 1) * 27 * BX, k_next, act_next);
+        cp_async_commit();
+        cp_async_wait<1>(); // this thread's copies of tile t have landed
+        bool active = act_cur;
+        if (MASK && active)
+            active = __ldg(a.mask + k_cur) != 0;
+        if (active) {
+            const S *sb = buf + s * 27 * BX;
+            C f[27];
+#pragma unroll
+            for (int d = 0; d < 27; ++d)
+                f[d] = Codec<S>::load(sb + d * BX + tid, d);
+            C drho, vx, vy, vz;
+            collide<C, EXACT>(f, a.rates, a.fx, a.fy, a.fz, drho, vx, vy, vz);
+            const uint32_t k = k_cur;
+            const int x = (int)(k % (uint32_t)a.nx);
+            const int y = (int)((k / (uint32_t)a.nx) % (uint32_t)a.ny);
+            const int z = (int)(k / ((uint32_t)a.nx * (uint32_t)a.ny));
+            const int xp = (x + 1 < a.nx) ? x + 1 : (a.periodic_x ? 0 : x);
+            const int yp = (y + 1 < a.ny) ? y + 1 : (a.periodic_y ? 0 : y);
+            const int zp = (z + 1 < a.nz) ? z + 1 : (a.periodic_z ? 0 : z);
+            const uint32_t sx = (uint32_t)(xp - x), sy = (uint32_t)((yp - y) * a.nx), sz = (uint32_t)((int64_t)(zp - z) * a.nx * a.ny);
+            const uint32_t nodes[8] = { k, k + sx, k + sy, k + sx + sy, k + sz, k + sx + sz, k + sy + sz, k + sx + sy + sz };
+            scatter_post<S, EVEN>(static_cast<S *>(a.dist), a.pitch, nodes, f);
+            if (ENERGY) {
+                m_acc += 1.0 + (double)drho;
+                e_acc += 0.5 * (1.0 + (double)drho) * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
+            }
+        }
+        k_cur = k_next;
+        act_cur = act_next;
+    }
+    cp_async_wait<0>();
 
     if (ENERGY) {
 #pragma unroll
@@ -394,7 +508,7 @@ __global__ void __launch_bounds__(128) k17_box_tma_kernel(BoxCollideArgs<typenam
         __syncthreads();
         if (tid == 0) {
             double mm = 0.0, ee = 0.0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            for (int w = 0; w < 4; ++w) {
                 mm += red[0][w];
                 ee += red[1][w];
             }

@@ -24,7 +24,7 @@ struct BoxState {
     double omega;
     double fx, fy, fz;            // half acceleration
     double lim[3];
-    int variant;                  // 0: choose, 1: direct loads, 2: TMA-staged (needs nx % 128 == 0)
+    int variant;                  // 0: choose, 1: direct loads, 2: TMA-staged (nx % 32 == 0), 3: async copies
     int *status;                  // device status word (DeviceError), nullable
 };
 
@@ -34,10 +34,12 @@ inline int box_block_x(int nx)
     int b = ((nx + 31) / 32) * 32;
     return b > 128 ? 128 : b;
 }
+// upper bound of the per-step energy partials any box kernel writes (one per warp of the direct
+// kernel's grid; the persistent kernels write fewer)
 inline uint64_t box_blocks(const BoxState &b)
 {
     const int bx = box_block_x(b.nx);
-    return (uint64_t)((b.nx + bx - 1) / bx) * (uint64_t)b.ny * (uint64_t)b.nz;
+    return (uint64_t)((b.nx + bx - 1) / bx) * (uint64_t)b.ny * (uint64_t)b.nz * (uint64_t)(bx / 32);
 }
 
 #define VFB_DECLARE_LAUNCHERS                                                                                        \

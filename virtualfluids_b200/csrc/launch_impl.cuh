@@ -246,15 +246,38 @@ cudaError_t launch_box_tma(const BoxCollideArgs<typename Codec<S>::compute> &a, 
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TmaTile<S>::SMEM);
         if (e != cudaSuccess)
             return e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, 128, TmaTile<S>::SMEM);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, 32 * TmaTile<S>::WARPS, TmaTile<S>::SMEM);
         if (e != cudaSuccess)
             return e;
         if (blocks_per_sm < 1)
             blocks_per_sm = 1;
     }
-    const int64_t ntiles = (int64_t)(a.nx / TmaTile<S>::BX) * a.ny * a.nz;
+    const int64_t warp_tiles = (int64_t)(a.nx / TmaTile<S>::BX) * a.ny * a.nz;
+    const int64_t blocks_needed = (warp_tiles + TmaTile<S>::WARPS - 1) / TmaTile<S>::WARPS;
+    const int64_t grid = std::min<int64_t>(blocks_needed, (int64_t)blocks_per_sm * sm_count());
+    kern<<<(unsigned)grid, 32 * TmaTile<S>::WARPS, TmaTile<S>::SMEM, s>>>(a, status);
+    if (n_partials)
+        *n_partials = (uint64_t)grid;
+    return cudaGetLastError();
+}
+template <class S, bool E, bool M, bool N>
+cudaError_t launch_box_async(const BoxCollideArgs<typename Codec<S>::compute> &a, uint64_t *n_partials, cudaStream_t s)
+{
+    auto kern = k17_box_async_kernel<S, VFB_EXACT, E, M, N>;
+    static int blocks_per_sm = -1;
+    if (blocks_per_sm < 0) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)AsyncTile<S>::SMEM);
+        if (e != cudaSuccess)
+            return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, 128, AsyncTile<S>::SMEM);
+        if (e != cudaSuccess)
+            return e;
+        if (blocks_per_sm < 1)
+            blocks_per_sm = 1;
+    }
+    const int64_t ntiles = (int64_t)((a.nx + AsyncTile<S>::BX - 1) / AsyncTile<S>::BX) * a.ny * a.nz;
     const int64_t grid = std::min<int64_t>(ntiles, (int64_t)blocks_per_sm * sm_count());
-    kern<<<(unsigned)grid, 128, TmaTile<S>::SMEM, s>>>(a, status);
+    kern<<<(unsigned)grid, 128, AsyncTile<S>::SMEM, s>>>(a);
     if (n_partials)
         *n_partials = (uint64_t)grid;
     return cudaGetLastError();
@@ -268,7 +291,24 @@ cudaError_t Launchers<S>::box_collide(const BoxState &b, bool even, double *part
     BoxCollideArgs<C> a = box_args<C>(b);
     a.energy_partials = partials;
     const bool mask = b.mask != nullptr, energy = partials != nullptr;
-    const bool tma = b.variant != 1 && (b.nx % TmaTile<S>::BX) == 0 && b.status != nullptr;
+    if constexpr (sizeof(S) >= 4) {
+        if (b.variant == 3 || b.variant == 0) {
+#define VFB_K17A(E, M, N) return launch_box_async<S, E, M, N>(a, n_partials, s)
+        if (even) {
+            if (mask && energy) VFB_K17A(true, true, true);
+            else if (mask) VFB_K17A(true, true, false);
+            else if (energy) VFB_K17A(true, false, true);
+            else VFB_K17A(true, false, false);
+        } else {
+            if (mask && energy) VFB_K17A(false, true, true);
+            else if (mask) VFB_K17A(false, true, false);
+            else if (energy) VFB_K17A(false, false, true);
+            else VFB_K17A(false, false, false);
+        }
+#undef VFB_K17A
+        }
+    }
+    const bool tma = b.variant == 2 && (b.nx % TmaTile<S>::BX) == 0 && b.status != nullptr;
     if (tma) {
 #define VFB_K17T(E, M, N) return launch_box_tma<S, E, M, N>(a, b.status, n_partials, s)
         if (even) {
@@ -286,7 +326,7 @@ cudaError_t Launchers<S>::box_collide(const BoxState &b, bool even, double *part
     }
     const dim3 G = box_grid(b), B(box_block_x(b.nx));
     if (n_partials)
-        *n_partials = (uint64_t)G.x * G.y * G.z;
+        *n_partials = (uint64_t)G.x * G.y * G.z * (B.x / 32);
 #define VFB_K17B(E, M, N) k17_box_kernel<S, VFB_EXACT, E, M, N, false><<<G, B, 0, s>>>(a)
     if (even) {
         if (mask && energy) VFB_K17B(true, true, true);

@@ -59,6 +59,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32
     return false;
 }
 
+// per-thread asynchronous global -> shared copies (cp.async, 4 or 8 bytes)
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void *dst, const void *src)
+{
+    static_assert(BYTES == 4 || BYTES == 8 || BYTES == 16, "cp.async copies 4, 8 or 16 bytes");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_addr(dst)), "l"(src), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 // error codes a kernel can leave in its status word
 enum DeviceError : int { kDevOk = 0, kDevWaitTimeout = 1 };
 
