@@ -368,28 +368,30 @@ __host__ __device__ inline K17FastConst<T> make_k17_fast_const(const K17Rates<T>
 }
 
 namespace k17detail {
-// forward transform along one line with offset K (K = 0: the plain central-moment transform)
+// forward transform along one line with offset K (K = 0: the plain central-moment transform);
+// K is a constant of the unrolled loops, so the K = 0 lines carry no offset addition
 template <class T>
 __host__ __device__ __forceinline__ void fwdK(T &a, T &b, T &c, T v, T v2, T twov, T K)
 {
     const T apc = a + c;
     const T m1 = c - a;
     const T m0 = apc + b;
-    const T w = m0 + K;
+    const T w = K == T(0) ? m0 : m0 + K;
     a = m0;
     b = fma(-v, w, m1);
     c = fma(v2, w, fma(-twov, m1, apc));
 }
-// backward transform with offset K
+// backward transform with offset K: a' = ((c - b) + w (v^2 - v))/2 + b v,
+// b' = (a - c) - 2 b v - w v^2, c' = ((c + b) + w (v^2 + v))/2 + b v, w = a + K
 template <class T>
 __host__ __device__ __forceinline__ void bwdK(T &a, T &b, T &c, T v, T v2mv, T v2pv, T twov, T v2, T K)
 {
-    const T w = a + K;
-    const T hb = T(0.5) * b, hc = T(0.5) * c;
-    const T hw = T(0.5) * w;
-    const T r0 = fma(hw, v2mv, fma(b, v, hc - hb));
-    const T r1 = fma(-v2, w, fma(-twov, b, a - c));
-    c = fma(hw, v2pv, fma(b, v, hc + hb));
+    (void)twov;
+    const T w = K == T(0) ? a : a + K;
+    const T bv = b * v;
+    const T r0 = fma(T(0.5), fma(w, v2mv, c - b), bv);
+    const T r1 = fma(-v2, w, fma(T(-2), bv, a - c));
+    c = fma(T(0.5), fma(w, v2pv, c + b), bv);
     a = r0;
     b = r1;
 }
