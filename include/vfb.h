@@ -168,6 +168,17 @@ size_t vfb_mass_energy_workspace_bytes(uint32_t size);
 int vfb_mass_energy(const vfb_level *level, const uint32_t *node_indices, uint32_t size, void *workspace,
                     size_t workspace_bytes, double out[2], void *stream);
 
+/* The same reduction for callers that cannot allocate device memory or hand the library any: no
+   counterpart in the reference. The per-block partial sums live in a fixed array inside the
+   library's device memory (about 1 MiB on every GPU that loads the library, held until the
+   process exits), so the node count is limited to VFB_NO_ALLOC_MAX_NODES; larger sizes are
+   rejected with VFB_ERR_INVALID_ARGUMENT. The first call on a device looks the array's device
+   address up (make it before any stream capture). All calls share the array, so calls that
+   overlap on the GPU race; each call overwrites what it reads back. Synchronises the stream. */
+#define VFB_NO_ALLOC_MAX_NODES (1u << 24)
+int vfb_mass_energy_no_alloc(const vfb_level *level, const uint32_t *node_indices, uint32_t size, double out[2],
+                             void *stream);
+
 /* ---- boundary-condition factory (BoundaryConditions/BoundaryConditionFactory.h:50-130) ------ */
 typedef int (*vfb_bc_fn)(const vfb_level *level, const vfb_bc *bc, void *stream);
 typedef int (*vfb_directional_bc_fn)(const vfb_level *level, const vfb_directional_bc *bc, void *stream);

@@ -110,6 +110,7 @@ SIGNATURES = {
     "vfb_mass_energy_workspace_bytes": (C.c_size_t, [C.c_uint32]),
     "vfb_mass_energy": (C.c_int, [C.POINTER(Level), C.c_void_p, C.c_uint32, C.c_void_p, C.c_size_t, C.c_void_p,
                                   C.c_void_p]),
+    "vfb_mass_energy_no_alloc": (C.c_int, [C.POINTER(Level), C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     "vfb_bc_factory_velocity": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),
     "vfb_bc_factory_noslip": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),
     "vfb_bc_factory_pressure": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),

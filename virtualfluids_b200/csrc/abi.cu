@@ -111,6 +111,8 @@ __global__ void __launch_bounds__(1024) reduce_partials_kernel(const double *__r
     }
 }
 
+void set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
+
 cudaError_t reduce_partials(const double *partials, uint64_t blocks, double *out, cudaStream_t s)
 {
     reduce_partials_kernel<<<1, 1024, 0, s>>>(partials, blocks, out);

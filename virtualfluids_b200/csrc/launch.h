@@ -70,6 +70,9 @@ namespace exact {
 VFB_DECLARE_LAUNCHERS
 }
 
+// message for vfb_last_error() of the calling thread
+void set_last_error(const char *msg);
+
 // deterministic reduction of per-block {mass, energy} partials into out[2] (device)
 cudaError_t reduce_partials(const double *partials, uint64_t blocks, double *out, cudaStream_t s);
 
