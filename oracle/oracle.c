@@ -423,3 +423,265 @@ int orc_run(orc_level *L, const uint32_t *fluid, uint32_t n_fluid, int *is_even,
     }
     return 0;
 }
+
+/* ---------------- refinement ---------------- */
+
+/* MomentsOnSourceNode::calculate (InterpolationCoefficients.h:74-146): macroscopic values and the
+   non-equilibrium second moments, k_ab = -3 omega (sum c_a c_b f / rho - u_a u_b) and
+   k_aaMbb = -3/2 omega (sum (c_a^2 - c_b^2) f / rho - (u_a^2 - u_b^2)) */
+void orc_interp_node_moments(const double *f, double omega, double out9[9])
+{
+    double drho, inv, vx, vy, vz;
+    orc_macro_compressible_f64(f, &drho, &inv, &vx, &vy, &vz);
+    double sxy = 0.0, syz = 0.0, sxz = 0.0, sxxyy = 0.0, sxxzz = 0.0;
+    for (int d = 0; d < 27; ++d) {
+        const int cx = ORC_CX[d], cy = ORC_CY[d], cz = ORC_CZ[d];
+        sxy += (double)(cx * cy) * f[d];
+        syz += (double)(cy * cz) * f[d];
+        sxz += (double)(cx * cz) * f[d];
+        sxxyy += (double)(cx * cx - cy * cy) * f[d];
+        sxxzz += (double)(cx * cx - cz * cz) * f[d];
+    }
+    out9[0] = drho;
+    out9[1] = vx;
+    out9[2] = vy;
+    out9[3] = vz;
+    out9[4] = -3.0 * omega * (sxy * inv - vx * vy);
+    out9[5] = -3.0 * omega * (syz * inv - vy * vz);
+    out9[6] = -3.0 * omega * (sxz * inv - vx * vz);
+    out9[7] = -1.5 * omega * (sxxyy * inv - (vx * vx - vy * vy));
+    out9[8] = -1.5 * omega * (sxxzz * inv - (vx * vx - vz * vz));
+}
+
+/* coefficient order: for u (a), v (b), w (c): 000 100 010 001 200 020 002 110 101 011 (3 x 10),
+   then d000 d100 d010 d001 d110 d101 d011, then a111 b111 c111 d111, LaplaceRho (42) */
+enum { C_A = 0, C_B = 10, C_C = 20, C_D = 30, C_111 = 37, C_LAPLACE = 41 };
+enum { K000 = 0, K100, K010, K001, K200, K020, K002, K110, K101, K011 };
+
+/* the sum of q over the corners with the sign pattern s_x^px s_y^py s_z^pz */
+static double pattern_sum(const double *mom8x9, int q, int px, int py, int pz)
+{
+    double s = 0.0;
+    for (int c = 0; c < 8; ++c) {
+        const int sx = (c & 1) ? 1 : -1, sy = (c & 2) ? 1 : -1, sz = (c & 4) ? 1 : -1;
+        const int sign = (px ? sx : 1) * (py ? sy : 1) * (pz ? sz : 1);
+        s += sign > 0 ? mom8x9[c * 9 + q] : -mom8x9[c * 9 + q];
+    }
+    return s;
+}
+
+void orc_interp_coefficients(const double *m, double xo, double yo, double zo, double out[42])
+{
+    /* trilinear part of u, v, w (quantities 1..3) and drho (0): mean, gradients, cross terms */
+    double mean[4];
+    const int base[4] = { C_D, C_A, C_B, C_C };
+    for (int q = 0; q < 4; ++q) {
+        mean[q] = pattern_sum(m, q, 0, 0, 0) / 8.0;
+        const int b = base[q];
+        double g100 = pattern_sum(m, q, 1, 0, 0) / 4.0, g010 = pattern_sum(m, q, 0, 1, 0) / 4.0;
+        double g001 = pattern_sum(m, q, 0, 0, 1) / 4.0;
+        double g110 = pattern_sum(m, q, 1, 1, 0) / 2.0, g101 = pattern_sum(m, q, 1, 0, 1) / 2.0;
+        double g011 = pattern_sum(m, q, 0, 1, 1) / 2.0, g111 = pattern_sum(m, q, 1, 1, 1);
+        if (q == 0) {
+            out[C_D + 0] = mean[0];
+            out[C_D + 1] = g100;
+            out[C_D + 2] = g010;
+            out[C_D + 3] = g001;
+            out[C_D + 4] = g110;
+            out[C_D + 5] = g101;
+            out[C_D + 6] = g011;
+            out[C_111 + 3] = g111;
+        } else {
+            out[b + K100] = g100;
+            out[b + K010] = g010;
+            out[b + K001] = g001;
+            out[b + K110] = g110;
+            out[b + K101] = g101;
+            out[b + K011] = g011;
+            out[C_111 + q - 1] = g111;
+        }
+    }
+    /* quadratic terms from the non-equilibrium moments (4 kxy, 5 kyz, 6 kxz, 7 kxxMyy, 8 kxxMzz)
+       and the cross derivatives of the other two components (continuity) */
+    const double a110 = out[C_A + K110], a101 = out[C_A + K101];
+    const double b110 = out[C_B + K110], b011 = out[C_B + K011];
+    const double c101 = out[C_C + K101], c011 = out[C_C + K011];
+    out[C_A + K200] = (b110 + c101) / 4.0 + (pattern_sum(m, 7, 1, 0, 0) + pattern_sum(m, 8, 1, 0, 0)) / 16.0;
+    out[C_A + K020] = -b110 / 2.0 + pattern_sum(m, 4, 0, 1, 0) / 8.0;
+    out[C_A + K002] = -c101 / 2.0 + pattern_sum(m, 6, 0, 0, 1) / 8.0;
+    out[C_B + K200] = -a110 / 2.0 + pattern_sum(m, 4, 1, 0, 0) / 8.0;
+    out[C_B + K020] = (a110 + c011) / 4.0 + (-2.0 * pattern_sum(m, 7, 0, 1, 0) + pattern_sum(m, 8, 0, 1, 0)) / 16.0;
+    out[C_B + K002] = -c011 / 2.0 + pattern_sum(m, 5, 0, 0, 1) / 8.0;
+    out[C_C + K200] = -a101 / 2.0 + pattern_sum(m, 6, 1, 0, 0) / 8.0;
+    out[C_C + K020] = -b011 / 2.0 + pattern_sum(m, 5, 0, 1, 0) / 8.0;
+    out[C_C + K002] = (a101 + b011) / 4.0 + (pattern_sum(m, 7, 0, 0, 1) - 2.0 * pattern_sum(m, 8, 0, 0, 1)) / 16.0;
+    /* the corner values see the quadratic terms at x^2 = y^2 = z^2 = 1/4 */
+    for (int q = 1; q < 4; ++q) {
+        const int b = base[q];
+        out[b + K000] = mean[q] - (out[b + K200] + out[b + K020] + out[b + K002]) / 4.0;
+    }
+    out[C_LAPLACE] = (xo != 0.0 || yo != 0.0 || zo != 0.0)
+                         ? 0.0
+                         : -3.0 * (out[C_A + K100] * out[C_A + K100] + out[C_B + K010] * out[C_B + K010] + out[C_C + K001] * out[C_C + K001])
+                               - 6.0 * (out[C_B + K100] * out[C_A + K010] + out[C_C + K100] * out[C_A + K001] + out[C_C + K010] * out[C_B + K001]);
+    /* move the expansion point by the offset (refinement into walls) */
+    for (int q = 1; q < 4; ++q) {
+        double *a = out + base[q];
+        a[K000] = a[K000] + xo * a[K100] + yo * a[K010] + zo * a[K001] + xo * xo * a[K200] + yo * yo * a[K020]
+                + zo * zo * a[K002] + xo * yo * a[K110] + xo * zo * a[K101] + yo * zo * a[K011];
+        const double g100 = a[K100] + 2.0 * xo * a[K200] + yo * a[K110] + zo * a[K101];
+        const double g010 = a[K010] + 2.0 * yo * a[K020] + xo * a[K110] + zo * a[K011];
+        const double g001 = a[K001] + 2.0 * zo * a[K002] + xo * a[K101] + yo * a[K011];
+        a[K100] = g100;
+        a[K010] = g010;
+        a[K001] = g001;
+    }
+    double *d = out + C_D;
+    d[0] = d[0] + xo * d[1] + yo * d[2] + zo * d[3] + xo * yo * d[4] + xo * zo * d[5] + yo * zo * d[6];
+    const double d100 = d[1] + yo * d[4] + zo * d[5], d010 = d[2] + xo * d[4] + zo * d[6], d001 = d[3] + xo * d[5] + yo * d[6];
+    d[1] = d100;
+    d[2] = d010;
+    d[3] = d001;
+}
+
+/* interpolateCF (InterpolationCF.h:57-314) at (x, y, z) and interpolateFC (InterpolationFC.h:56-269)
+   at the cell centre: density and velocity from the polynomials, second-order central moments from
+   the strain rate scaled by -eps/omega (1 + drho), higher orders at equilibrium, then the backward
+   chimera transform to f - w */
+void orc_interp_point(const double *c, double omega, double eps, double x, double y, double z, int fc, double out[27])
+{
+    const double *a = c + C_A, *b = c + C_B, *w = c + C_C, *d = c + C_D;
+    double press, u[3], g[3][3]; /* g[i][j] = d u_i / d x_j */
+    if (fc) {
+        press = d[0] - 2.0 * c[C_LAPLACE] / 8.0;
+        u[0] = a[K000];
+        u[1] = b[K000];
+        u[2] = w[K000];
+        const double *p[3] = { a, b, w };
+        for (int i = 0; i < 3; ++i) {
+            g[i][0] = p[i][K100];
+            g[i][1] = p[i][K010];
+            g[i][2] = p[i][K001];
+        }
+    } else {
+        press = d[0] + x * d[1] + y * d[2] + z * d[3] + x * y * d[4] + x * z * d[5] + y * z * d[6] + x * y * z * c[C_111 + 3]
+              + 3.0 * x * x * c[C_LAPLACE];
+        const double *p[3] = { a, b, w };
+        for (int i = 0; i < 3; ++i) {
+            const double *q = p[i];
+            const double q111 = c[C_111 + i];
+            u[i] = q[K000] + x * q[K100] + y * q[K010] + z * q[K001] + x * x * q[K200] + y * y * q[K020] + z * z * q[K002]
+                 + x * y * q[K110] + x * z * q[K101] + y * z * q[K011] + x * y * z * q111;
+            g[i][0] = q[K100] + 2.0 * x * q[K200] + y * q[K110] + z * q[K101] + y * z * q111;
+            g[i][1] = q[K010] + 2.0 * y * q[K020] + x * q[K110] + z * q[K011] + x * z * q111;
+            g[i][2] = q[K001] + 2.0 * z * q[K002] + x * q[K101] + y * q[K011] + x * y * q111;
+        }
+    }
+    const double s = eps / omega * (1.0 + press);
+    double F3[3][3][3];
+    memset(F3, 0, sizeof(F3));
+#define M(i, j, k) F3[i][j][k]
+    const double mxxMyy = -2.0 / 3.0 * (g[0][0] - g[1][1]) * s;
+    const double mxxMzz = -2.0 / 3.0 * (g[0][0] - g[2][2]) * s;
+    M(0, 1, 1) = -1.0 / 3.0 * (g[1][2] + g[2][1]) * s;
+    M(1, 0, 1) = -1.0 / 3.0 * (g[0][2] + g[2][0]) * s;
+    M(1, 1, 0) = -1.0 / 3.0 * (g[0][1] + g[1][0]) * s;
+    M(0, 0, 0) = press;
+    M(2, 0, 0) = (mxxMyy + mxxMzz + press) / 3.0;
+    M(0, 2, 0) = (-2.0 * mxxMyy + mxxMzz + press) / 3.0;
+    M(0, 0, 2) = (mxxMyy - 2.0 * mxxMzz + press) / 3.0;
+    M(0, 2, 2) = M(2, 0, 2) = M(2, 2, 0) = press / 9.0;
+    M(2, 2, 2) = press / 27.0;
+    const double vx = u[0], vy = u[1], vz = u[2], vx2 = vx * vx, vy2 = vy * vy, vz2 = vz * vz;
+    static const double kinvZ[3][3] = { { 36, 9, 36 }, { 9, 9.0 / 4.0, 9 }, { 36, 9, 36 } };
+    static const double kY[3][2] = { { 1.0 / 6, 1.0 / 18 }, { 2.0 / 3.0, 2.0 / 9.0 }, { 1.0 / 6, 1.0 / 18 } };
+    static const double kinvY[3][2] = { { 6, 18 }, { 1.5, 4.5 }, { 6, 18 } };
+    for (int jb = 0; jb < 3; ++jb)
+        for (int kc = 0; kc < 3; ++kc) {
+            if (jb == 0 && kc == 0)
+                chim_bwd_k_f64(&M(0, 0, 0), &M(1, 0, 0), &M(2, 0, 0), vx, vx2, 1.0, 1.0);
+            else if (jb == 2 && kc == 2)
+                chim_bwd_k_f64(&M(0, 2, 2), &M(1, 2, 2), &M(2, 2, 2), vx, vx2, 9.0, 1.0 / 9);
+            else if ((jb == 2 && kc == 0) || (jb == 0 && kc == 2))
+                chim_bwd_k_f64(&M(0, jb, kc), &M(1, jb, kc), &M(2, jb, kc), vx, vx2, 3.0, 1.0 / 3);
+            else
+                chim_bwd_f64(&M(0, jb, kc), &M(1, jb, kc), &M(2, jb, kc), vx, vx2);
+        }
+    for (int ia = 0; ia < 3; ++ia)
+        for (int kc = 0; kc < 3; ++kc) {
+            if (kc == 1)
+                chim_bwd_f64(&M(ia, 0, 1), &M(ia, 1, 1), &M(ia, 2, 1), vy, vy2);
+            else
+                chim_bwd_k_f64(&M(ia, 0, kc), &M(ia, 1, kc), &M(ia, 2, kc), vy, vy2, kinvY[ia][kc / 2], kY[ia][kc / 2]);
+        }
+    for (int ia = 0; ia < 3; ++ia)
+        for (int jb = 0; jb < 3; ++jb)
+            chim_bwd_k_f64(&M(ia, jb, 0), &M(ia, jb, 1), &M(ia, jb, 2), vz, vz2, kinvZ[ia][jb], 1.0 / kinvZ[ia][jb]);
+    for (int dd = 0; dd < 27; ++dd)
+        out[dd] = F3[ORC_CX[dd] + 1][ORC_CY[dd] + 1][ORC_CZ[dd] + 1];
+#undef M
+}
+
+/* node of corner (ix, iy, iz) of a cell whose MMM node is `base`, stepping x, then y, then z */
+static uint32_t cell_corner(const orc_level *L, uint32_t base, int ix, int iy, int iz)
+{
+    uint32_t k = base;
+    if (ix) k = L->nbx[k];
+    if (iy) k = L->nby[k];
+    if (iz) k = L->nbz[k];
+    return k;
+}
+
+static void cell_moments(const orc_level *L, uint32_t base, int is_even, double omega, double mom[72])
+{
+    for (int c = 0; c < 8; ++c) {
+        double f[27];
+        orc_read_pre(L, cell_corner(L, base, c & 1, (c >> 1) & 1, (c >> 2) & 1), is_even, f);
+        orc_interp_node_moments(f, omega, mom + 9 * c);
+    }
+}
+
+/* setPreCollisionDistribution of all 27 directions of node k */
+static void write_pre_all(orc_level *L, uint32_t k, int is_even, const double f[27])
+{
+    int map[27];
+    orc_pointer_map(is_even, map);
+    for (int d = 0; d < 27; ++d)
+        write_pre_dir(L, k, map, d, f[d]);
+}
+
+/* scaleCoarseToFineCompressible_Device (scaleCoarseToFineCompressible.cu:305-528): moments of the
+   coarse cell at the coarse parity, populations of the eight fine nodes at (+-1/4)^3 written at the
+   even parity of the fine level, epsilon 1/2 */
+void orc_scale_cf(orc_level *coarse, orc_level *fine, const uint32_t *coarse_cells, const uint32_t *fine_cells,
+                  uint32_t n_cells, const double *ox, const double *oy, const double *oz, int coarse_is_even,
+                  double omega_coarse, double omega_fine)
+{
+    for (uint32_t i = 0; i < n_cells; ++i) {
+        double mom[72], coef[42];
+        cell_moments(coarse, coarse_cells[i], coarse_is_even, omega_coarse, mom);
+        orc_interp_coefficients(mom, ox[i], oy[i], oz[i], coef);
+        for (int c = 0; c < 8; ++c) {
+            const int ix = c & 1, iy = (c >> 1) & 1, iz = (c >> 2) & 1;
+            double f[27];
+            orc_interp_point(coef, omega_fine, 0.5, ix ? 0.25 : -0.25, iy ? 0.25 : -0.25, iz ? 0.25 : -0.25, 0, f);
+            write_pre_all(fine, cell_corner(fine, fine_cells[i], ix, iy, iz), 1, f);
+        }
+    }
+}
+
+/* scaleFineToCoarseCompressible_Device (scaleFineToCoarseCompressible.cu:76-124): moments of the fine
+   cell at the even parity, populations of the coarse node at the cell centre written at the coarse
+   parity, epsilon 2 */
+void orc_scale_fc(orc_level *coarse, orc_level *fine, const uint32_t *coarse_cells, const uint32_t *fine_cells,
+                  uint32_t n_cells, const double *ox, const double *oy, const double *oz, int coarse_is_even,
+                  double omega_coarse, double omega_fine)
+{
+    for (uint32_t i = 0; i < n_cells; ++i) {
+        double mom[72], coef[42], f[27];
+        cell_moments(fine, fine_cells[i], 1, omega_fine, mom);
+        orc_interp_coefficients(mom, ox[i], oy[i], oz[i], coef);
+        orc_interp_point(coef, omega_coarse, 2.0, 0.0, 0.0, 0.0, 1, f);
+        write_pre_all(coarse, coarse_cells[i], coarse_is_even, f);
+    }
+}

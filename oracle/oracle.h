@@ -3,7 +3,8 @@
  *
  * A plain-C CPU restatement of the VirtualFluids GPU time-step hot path (D3Q27 K17 cumulant
  * collision with in-place esoteric-twist streaming, the no-slip / velocity / pressure boundary
- * kernels, equilibrium initialisation, macroscopic output and the FP64 reductions). It exists
+ * kernels, equilibrium initialisation, macroscopic output, the FP64 reductions and the
+ * interpolation between refinement levels). It exists
  * only so tests, the smoke check and the benchmark's CPU-baseline leg can check the CUDA
  * library against the reference algorithm. Nothing in the shipped library links or calls it.
  *
@@ -94,6 +95,27 @@ typedef struct {
 typedef struct {
     int32_t *k; int32_t *kN; double *rho; uint32_t n; int direction;
 } orc_pressure;
+
+/* ---- refinement: interpolation between levels ----
+   Second-order moment interpolation of src/lbm/interpolation/InterpolationCoefficients.h:74-438 and
+   src/lbm/refinement/Interpolation{CF,FC}.h, restated with the coefficients written as sign-pattern
+   sums over the eight cell corners. Corner c = ix + 2 iy + 4 iz sits at (ix, iy, iz) - 1/2. */
+/* moments of one source node: {drho, ux, uy, uz, kxy, kyz, kxz, kxxMyy, kxxMzz} */
+void orc_interp_node_moments(const double *f, double omega, double out9[9]);
+/* coefficients of the cell from the eight corners' moments, in the member order of
+   InterpolationCoefficients: a, b, c (000 100 010 001 200 020 002 110 101 011 each),
+   d000 d100 d010 d001 d110 d101 d011, a111 b111 c111 d111, LaplaceRho */
+void orc_interp_coefficients(const double *mom8x9, double xoff, double yoff, double zoff, double out42[42]);
+/* populations (f - w) at (x, y, z) of the cell from its coefficients; fc != 0: the fine-to-coarse form */
+void orc_interp_point(const double *coef42, double omega_target, double eps, double x, double y, double z, int fc,
+                      double out27[27]);
+/* scaleCoarseToFineCompressible / scaleFineToCoarseCompressible (GridScaling/scale*.cu) for a list of cells */
+void orc_scale_cf(orc_level *coarse, orc_level *fine, const uint32_t *coarse_cells, const uint32_t *fine_cells,
+                  uint32_t n_cells, const double *ox, const double *oy, const double *oz, int coarse_is_even,
+                  double omega_coarse, double omega_fine);
+void orc_scale_fc(orc_level *coarse, orc_level *fine, const uint32_t *coarse_cells, const uint32_t *fine_cells,
+                  uint32_t n_cells, const double *ox, const double *oy, const double *oz, int coarse_is_even,
+                  double omega_coarse, double omega_fine);
 
 int orc_run(orc_level *L, const uint32_t *fluid, uint32_t n_fluid, int *is_even, double omega, const double lim[3],
             const double forces[3], const orc_velocity *vel, const orc_noslip *ns, const orc_pressure *pr, int n_pr,

@@ -54,6 +54,11 @@ def lib():
         L.orc_init.argtypes = [_P, _P, _P, _P, _P, _P, i]
         L.orc_macros.argtypes = [_P, _P, i, _P, _P, _P, _P, _P]
         L.orc_mass_energy.argtypes = [_P, _P, u, i, _P]
+        L.orc_interp_node_moments.argtypes = [_P, d, _P]
+        L.orc_interp_coefficients.argtypes = [_P, d, d, d, _P]
+        L.orc_interp_point.argtypes = [_P, d, d, d, d, d, i, _P]
+        L.orc_scale_cf.argtypes = [_P, _P, _P, _P, u, _P, _P, _P, i, d, d]
+        L.orc_scale_fc.argtypes = [_P, _P, _P, _P, u, _P, _P, _P, i, d, d]
         _lib = L
     return _lib
 
@@ -70,6 +75,9 @@ def ref64():
     L.ref_macro_compressible_f64.argtypes = [_P, _P]
     L.ref_incompressible_velocity_f64.argtypes = [_P, _P]
     L.ref_collision_sweep_f64.argtypes = [_P, C.c_uint64, _P, _P, _P, _P, C.c_uint32, C.c_int, d, _P, C.c_int]
+    L.ref_interp_coefficients_f64.argtypes = [_P, d, d, d, d, _P]
+    L.ref_interp_cf_f64.argtypes = [_P, d, d, d, d, d, d, d, d, _P]
+    L.ref_interp_fc_f64.argtypes = [_P, d, d, d, d, d, _P]
     return L
 
 
@@ -183,3 +191,39 @@ def k17(f, omega, lim=(0.01, 0.01, 0.01), force=(0.0, 0.0, 0.0), dtype=np.float6
         lib().orc_k17_f32(ptr(a), np.float32(omega), ptr(np.array(lim, dtype=np.float32)), *(np.float32(x) for x in force),
                           ptr(m))
     return a, m
+
+
+# corners of an interpolation cell in the oracle's order c = ix + 2 iy + 4 iz, and their position in
+# the reference's visiting order MMM, MMP, PMP, PMM, MPM, MPP, PPP, PPM
+REF_CORNER_ORDER = [0, 4, 5, 1, 2, 6, 7, 3]
+
+
+def interp_coefficients(f8, omega, offset=(0.0, 0.0, 0.0)):
+    """Oracle coefficients of one cell (42, the member order of InterpolationCoefficients)."""
+    L = lib()
+    mom = np.zeros((8, 9))
+    for c in range(8):
+        L.orc_interp_node_moments(ptr(np.ascontiguousarray(f8[c], dtype=np.float64)), omega, ptr(mom[c]))
+    coef = np.zeros(42)
+    L.orc_interp_coefficients(ptr(mom), *(float(x) for x in offset), ptr(coef))
+    return coef
+
+
+def interp_cf_cell(f8, omega_coarse, omega_fine, offset=(0.0, 0.0, 0.0)):
+    """Oracle coarse-to-fine for one cell: f8[c] (oracle corner order) -> 8 fine nodes' populations."""
+    L = lib()
+    coef = interp_coefficients(f8, omega_coarse, offset)
+    out = np.zeros((8, 27))
+    for c in range(8):
+        pos = [0.25 if (c >> a) & 1 else -0.25 for a in range(3)]
+        L.orc_interp_point(ptr(coef), omega_fine, 0.5, *pos, 0, ptr(out[c]))
+    return out
+
+
+def interp_fc_cell(f8, omega_fine, omega_coarse, offset=(0.0, 0.0, 0.0)):
+    """Oracle fine-to-coarse for one cell: f8[c] (oracle corner order) -> the coarse node's populations."""
+    L = lib()
+    coef = interp_coefficients(f8, omega_fine, offset)
+    out = np.zeros(27)
+    L.orc_interp_point(ptr(coef), omega_coarse, 2.0, 0.0, 0.0, 0.0, 1, ptr(out))
+    return out

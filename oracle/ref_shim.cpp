@@ -13,6 +13,9 @@
  *   vf::lbm::runK17CompressibleNavierStokes<None>   src/lbm/collision/K17CompressibleNavierStokes.h:88
  *   vf::lbm::{forward,backward}{Inverse,}Chimera*   src/lbm/ChimeraTransformation.h:58-150
  *   vf::lbm::getDensity / getCompressibleMacroscopicValues  src/lbm/MacroscopicQuantities.h:55-137
+ *   vf::lbm::MomentsOnSourceNodeSet::calculate*, calculateCoefficients
+ *                                                   src/lbm/interpolation/InterpolationCoefficients.h:74-438
+ *   vf::lbm::interpolateCF / interpolateFC          src/lbm/refinement/InterpolationCF.h:57, InterpolationFC.h:56
  */
 #include <cstdint>
 #include <cstring>
@@ -20,6 +23,9 @@
 #include <lbm/ChimeraTransformation.h>
 #include <lbm/MacroscopicQuantities.h>
 #include <lbm/collision/K17CompressibleNavierStokes.h>
+#include <lbm/interpolation/InterpolationCoefficients.h>
+#include <lbm/refinement/InterpolationCF.h>
+#include <lbm/refinement/InterpolationFC.h>
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -88,6 +94,56 @@ void REF_FN(incompressible_velocity)(const real *f, real *out3)
     out3[0] = vf::lbm::getIncompressibleVelocityX1(f);
     out3[1] = vf::lbm::getIncompressibleVelocityX2(f);
     out3[2] = vf::lbm::getIncompressibleVelocityX3(f);
+}
+
+/* the eight source nodes of an interpolation cell, in the order MMM, MMP, PMP, PMM, MPM, MPP, PPP, PPM
+   (ScalingUtilities.h:53-200 visits them in this order); f8 = 8 x 27 populations */
+static vf::lbm::MomentsOnSourceNodeSet moments_of(const real *f8, real omega)
+{
+    vf::lbm::MomentsOnSourceNodeSet m;
+    m.calculateMMM(f8 + 0 * 27, omega);
+    m.calculateMMP(f8 + 1 * 27, omega);
+    m.calculatePMP(f8 + 2 * 27, omega);
+    m.calculatePMM(f8 + 3 * 27, omega);
+    m.calculateMPM(f8 + 4 * 27, omega);
+    m.calculateMPP(f8 + 5 * 27, omega);
+    m.calculatePPP(f8 + 6 * 27, omega);
+    m.calculatePPM(f8 + 7 * 27, omega);
+    return m;
+}
+
+/* all coefficients in the member order of InterpolationCoefficients (InterpolationCoefficients.h:63-71) */
+void REF_FN(interp_coefficients)(const real *f8, real omega, real xoff, real yoff, real zoff, real *out46)
+{
+    vf::lbm::MomentsOnSourceNodeSet m = moments_of(f8, omega);
+    vf::lbm::InterpolationCoefficients c;
+    m.calculateCoefficients(c, xoff, yoff, zoff);
+    const real v[46] = { c.a000, c.a100, c.a010, c.a001, c.a200, c.a020, c.a002, c.a110, c.a101, c.a011,
+                         c.b000, c.b100, c.b010, c.b001, c.b200, c.b020, c.b002, c.b110, c.b101, c.b011,
+                         c.c000, c.c100, c.c010, c.c001, c.c200, c.c020, c.c002, c.c110, c.c101, c.c011,
+                         c.d000, c.d100, c.d010, c.d001, c.d110, c.d101, c.d011,
+                         c.a111, c.b111, c.c111, c.d111, c.LaplaceRho, 0, 0, 0, 0 };
+    std::memcpy(out46, v, sizeof(v));
+}
+
+/* coarse -> fine for one cell: moments with omega_source, populations at (x, y, z) with omega_target,
+   epsilon 1/2 (scaleCoarseToFineCompressible.cu:46-300 / InterpolationCF.h:57) */
+void REF_FN(interp_cf)(const real *f8, real omega_coarse, real omega_fine, real xoff, real yoff, real zoff,
+                       real x, real y, real z, real *out27)
+{
+    vf::lbm::MomentsOnSourceNodeSet m = moments_of(f8, omega_coarse);
+    vf::lbm::InterpolationCoefficients c;
+    m.calculateCoefficients(c, xoff, yoff, zoff);
+    vf::lbm::interpolateCF(out27, omega_fine, vf::basics::constant::c1o2, c, x, y, z);
+}
+
+/* fine -> coarse for one cell: epsilon 2, evaluated at the cell centre (scaleFineToCoarseCompressible.cu:46-70) */
+void REF_FN(interp_fc)(const real *f8, real omega_fine, real omega_coarse, real xoff, real yoff, real zoff, real *out27)
+{
+    vf::lbm::MomentsOnSourceNodeSet m = moments_of(f8, omega_fine);
+    vf::lbm::InterpolationCoefficients c;
+    m.calculateCoefficients(c, xoff, yoff, zoff);
+    vf::lbm::interpolateFC(out27, vf::basics::constant::c2o1, omega_coarse, c);
 }
 
 #ifdef VF_DOUBLE_ACCURACY

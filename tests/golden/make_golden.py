@@ -1,6 +1,6 @@
 """Generate the golden vectors of tests/golden/ from the reference's own arithmetic.
 
-Runs the reference's K17, chimera and macroscopic headers, compiled for the host from the
+Runs the reference's K17, chimera, macroscopic and interpolation headers, compiled for the host from the
 reference tree by oracle/Makefile (target `ref`), on seeded random inputs and stores inputs
 and outputs. The committed .npz files let the oracle be pinned on machines that do not have
 the reference tree. Usage:
@@ -84,6 +84,30 @@ def main():
         r64.ref_macro_compressible_f64(pyoracle.ptr(f_in[i].copy()), pyoracle.ptr(macro[i]))
     np.savez_compressed(ROOT / "tests/golden/chimera_macro_reference.npz", chim_in=chim_in, v=v, kinv=kin,
                         chim_out=chim_out, f_in=f_in, density=dens, macro=macro)
+
+    # refinement interpolation: eight source nodes of a cell in the reference's visiting order
+    # MMM, MMP, PMP, PMM, MPM, MPP, PPP, PPM; coefficients, coarse-to-fine populations of the eight
+    # fine nodes at (+-1/4)^3 (oracle corner order c = ix + 2 iy + 4 iz) and the fine-to-coarse ones
+    nc = 96
+    f8 = np.zeros((nc, 8, 27))
+    for i in range(nc):
+        f8[i] = _cases(rng, 8) * (1.0 if i % 4 else 3.0)
+    om = rng.uniform(1.2, 1.95, (nc, 2))
+    offs = np.zeros((nc, 3))
+    offs[1::3] = rng.choice([-0.5, 0.0, 0.5], (len(offs[1::3]), 3))
+    offs[2::3] = rng.uniform(-0.5, 0.5, (len(offs[2::3]), 3))
+    coef = np.zeros((nc, 46))
+    cf = np.zeros((nc, 8, 27))
+    fc = np.zeros((nc, 27))
+    for i in range(nc):
+        src = np.ascontiguousarray(f8[i][pyoracle.REF_CORNER_ORDER])
+        r64.ref_interp_coefficients_f64(pyoracle.ptr(src), om[i, 0], *offs[i], pyoracle.ptr(coef[i]))
+        for c in range(8):
+            pos = [0.25 if (c >> a) & 1 else -0.25 for a in range(3)]
+            r64.ref_interp_cf_f64(pyoracle.ptr(src), om[i, 0], om[i, 1], *offs[i], *pos, pyoracle.ptr(cf[i, c]))
+        r64.ref_interp_fc_f64(pyoracle.ptr(src), om[i, 1], om[i, 0], *offs[i], pyoracle.ptr(fc[i]))
+    np.savez_compressed(ROOT / "tests/golden/interpolation_reference.npz", f8=f8, omega=om, offset=offs,
+                        coef=coef, cf=cf, fc=fc)
     print("wrote", ROOT / "tests/golden")
 
 

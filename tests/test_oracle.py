@@ -152,3 +152,61 @@ def test_oracle_cavity_bounce_back_conserves_mass(oracle):
     m1, e1 = lv.mass_energy()
     assert abs(m1 - m0) < 1e-10 * m0   # velocity bounce-back with a tangential lid injects no mass
     assert e1 > 0.0                     # the lid drives the flow
+
+
+# refinement interpolation (InterpolationCoefficients.h, InterpolationCF.h, InterpolationFC.h).
+# The oracle forms the same polynomial with its sums in another order, so the pin is a tolerance:
+# per cell, the largest deviation relative to the largest population.
+INTERP_TOL = 1e-13
+
+
+def _rel(a, b):
+    return float(np.abs(np.asarray(a) - np.asarray(b)).max() / max(np.abs(b).max(), 1e-300))
+
+
+def test_interpolation_matches_reference_golden(oracle):
+    g = np.load(GOLDEN / "interpolation_reference.npz")
+    for i in range(g["f8"].shape[0]):
+        f8, (oc, of), off = g["f8"][i], g["omega"][i], tuple(g["offset"][i])
+        coef = oracle.interp_coefficients(f8, oc, off)
+        ref = g["coef"][i][:42]
+        assert np.abs(coef - ref).max() <= INTERP_TOL * np.abs(ref).max(), i
+        assert _rel(oracle.interp_cf_cell(f8, oc, of, off), g["cf"][i]) <= INTERP_TOL, i
+        assert _rel(oracle.interp_fc_cell(f8, of, oc, off), g["fc"][i]) <= INTERP_TOL, i
+
+
+def test_interpolation_matches_reference_header_live(oracle):
+    r64 = oracle.ref64()
+    if r64 is None:
+        pytest.skip("reference pins not built here (golden vectors cover this)")
+    rng = np.random.default_rng(11)
+    W = np.array([8 / 27] + [2 / 27] * 6 + [1 / 54] * 12 + [1 / 216] * 8)
+    for i in range(300):
+        f8 = rng.normal(0, 1e-2, (8, 27)) * W + rng.normal(0, 1e-2, (8, 1)) * W
+        oc, of = rng.uniform(1.0, 1.99, 2)
+        off = (0.0, 0.0, 0.0) if i % 2 else tuple(rng.uniform(-0.5, 0.5, 3))
+        src = np.ascontiguousarray(f8[oracle.REF_CORNER_ORDER])
+        mine = oracle.interp_cf_cell(f8, oc, of, off)
+        for c in range(8):
+            pos = [0.25 if (c >> a) & 1 else -0.25 for a in range(3)]
+            out = np.zeros(27)
+            r64.ref_interp_cf_f64(oracle.ptr(src), oc, of, *off, *pos, oracle.ptr(out))
+            assert _rel(mine[c], out) <= INTERP_TOL, (i, c)
+        out = np.zeros(27)
+        r64.ref_interp_fc_f64(oracle.ptr(src), of, oc, *off, oracle.ptr(out))
+        assert _rel(oracle.interp_fc_cell(f8, of, oc, off), out) <= INTERP_TOL, i
+
+
+def test_interpolation_of_a_uniform_state_is_that_state(oracle):
+    """A cell whose eight corners hold one resting state gives that state back on both sides
+    (the strain rate is zero, so only the equilibrium survives)."""
+    W = np.array([8 / 27] + [2 / 27] * 6 + [1 / 54] * 12 + [1 / 216] * 8)
+    f8 = np.zeros((8, 27))
+    assert np.abs(oracle.interp_cf_cell(f8, 1.7, 1.8)).max() == 0.0
+    assert np.abs(oracle.interp_fc_cell(f8, 1.8, 1.7)).max() == 0.0
+    rho = 0.01
+    f8 = np.tile(W * rho, (8, 1))
+    out = oracle.interp_cf_cell(f8, 1.7, 1.8)
+    for c in range(8):
+        assert np.allclose(out[c], W * rho, rtol=0, atol=1e-16)
+    assert np.allclose(oracle.interp_fc_cell(f8, 1.8, 1.7), W * rho, rtol=0, atol=1e-16)
