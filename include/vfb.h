@@ -154,6 +154,33 @@ int vfb_velocity_interpolated_compressible(const vfb_level *level, const vfb_bc 
 /* PressureNonEquilibriumCompressible (BoundaryConditions/Pressure/Pressure.cu:63) */
 int vfb_pressure_non_equilibrium_compressible(const vfb_level *level, const vfb_directional_bc *bc, void *stream);
 
+/* ICells and ICellNeigh (src/gpu/core/Calculation/Calculation.h:72-87): the interpolation cells
+   between a coarse level and the fine level nested in it. Device pointers. */
+typedef struct vfb_interpolation_cells {
+    const uint32_t *fine_cell_indices;    /* fineCellIndices: MMM node of the cell on the fine level */
+    const uint32_t *coarse_cell_indices;  /* coarseCellIndices: coarse-to-fine: MMM node of the coarse cell;
+                                             fine-to-coarse: the coarse node at the cell centre */
+    uint32_t number_of_cells;
+} vfb_interpolation_cells;
+typedef struct vfb_interpolation_cell_neighbor {
+    const void *x, *y, *z;                /* real[number_of_cells]: offset of the expansion point (0 in the bulk) */
+} vfb_interpolation_cell_neighbor;
+
+/* scaleCoarseToFineCompressible<false> (GridScaling/Scaling.cu:106-138, kernel
+   scaleCoarseToFineCompressible.cu:305-528): second-order moment interpolation of each coarse cell
+   at the coarse level's parity (omega of the coarse level) into the pre-collision populations of
+   its eight fine nodes at the even parity (omega of the fine level). Both levels share storage and
+   arithmetic. Turbulent viscosity (the <true> instantiation) is not built. */
+int vfb_scale_coarse_to_fine_compressible(const vfb_level *coarse, const vfb_level *fine,
+                                          const vfb_interpolation_cells *cells,
+                                          const vfb_interpolation_cell_neighbor *offsets, void *stream);
+/* scaleFineToCoarseCompressible<false> (GridScaling/Scaling.cu:156-188, kernel
+   scaleFineToCoarseCompressible.cu:76-124): each fine cell at the even parity into the coarse node
+   at its centre, written at the coarse level's parity. */
+int vfb_scale_fine_to_coarse_compressible(const vfb_level *coarse, const vfb_level *fine,
+                                          const vfb_interpolation_cells *cells,
+                                          const vfb_interpolation_cell_neighbor *offsets, void *stream);
+
 /* InitNavierStokesCompressible::init (PreProcessor/PreProcessorStrategy/InitNavierStokesCompressible/
    InitNavierStokesCompressible.cu:45): equilibrium from level->rho/velocity_* for the level's
    current parity. PreProcessorImp::init (PreProcessorImp.cpp:50-58) calls it for the odd, then
@@ -196,6 +223,16 @@ enum { VFB_PRESSURE_NON_EQUILIBRIUM_INCOMPRESSIBLE = 0, VFB_PRESSURE_NON_EQUILIB
 int vfb_bc_factory_velocity(int32_t variant, vfb_bc_fn *fn);
 int vfb_bc_factory_noslip(int32_t variant, vfb_bc_fn *fn);
 int vfb_bc_factory_pressure(int32_t variant, vfb_directional_bc_fn *fn);
+
+/* ---- grid-scaling factory (GridScaling/GridScalingFactory.h:47-66) ----------------------- */
+typedef int (*vfb_scaling_fn)(const vfb_level *coarse, const vfb_level *fine, const vfb_interpolation_cells *cells,
+                              const vfb_interpolation_cell_neighbor *offsets, void *stream);
+/* enum values of GridScalingFactory::GridScaling */
+enum { VFB_SCALE_COMPRESSIBLE = 0, VFB_SCALE_NOT_SPECIFIED = 1 };
+/* getGridScalingFC / getGridScalingCF. NotSpecified gives *fn = NULL with VFB_OK; a turbulent
+   viscosity request gives VFB_ERR_UNSUPPORTED. */
+int vfb_scaling_factory_fine_to_coarse(int32_t variant, int32_t has_turbulent_viscosity, vfb_scaling_fn *fn);
+int vfb_scaling_factory_coarse_to_fine(int32_t variant, int32_t has_turbulent_viscosity, vfb_scaling_fn *fn);
 
 /* ---- (2a) step driver: UpdateGrid27::updateGrid for one level (Calculation/UpdateGrid27.cpp:54-95) */
 typedef struct vfb_simulation vfb_simulation;

@@ -156,3 +156,44 @@ def test_argument_validation_without_launching():
     d.storage, d.omega = N.STORAGE_F64, 1.8
     h = C.c_void_p()
     assert lib.vfb_box_create(C.byref(d), C.byref(h)) == N.VFB_ERR_INVALID_ARGUMENT  # walls need a mask
+
+
+def test_grid_scaling_factory_semantics():
+    """GridScalingFactoryTest.cpp: NotSpecified gives no function; ScaleCompressible gives the
+    compressible scaling of each direction; turbulent viscosity is not built here."""
+    from virtualfluids_b200 import _native as N
+    lib = N.lib()
+    fn = C.c_void_p()
+    N.check(lib.vfb_scaling_factory_fine_to_coarse(N.SCALE_NOT_SPECIFIED, 0, C.byref(fn)))
+    assert fn.value is None
+    N.check(lib.vfb_scaling_factory_coarse_to_fine(N.SCALE_NOT_SPECIFIED, 0, C.byref(fn)))
+    assert fn.value is None
+    N.check(lib.vfb_scaling_factory_fine_to_coarse(N.SCALE_COMPRESSIBLE, 0, C.byref(fn)))
+    assert fn.value == C.cast(lib.vfb_scale_fine_to_coarse_compressible, C.c_void_p).value
+    N.check(lib.vfb_scaling_factory_coarse_to_fine(N.SCALE_COMPRESSIBLE, 0, C.byref(fn)))
+    assert fn.value == C.cast(lib.vfb_scale_coarse_to_fine_compressible, C.c_void_p).value
+    assert lib.vfb_scaling_factory_coarse_to_fine(N.SCALE_COMPRESSIBLE, 1, C.byref(fn)) == N.VFB_ERR_UNSUPPORTED
+    assert lib.vfb_scaling_factory_fine_to_coarse(7, 0, C.byref(fn)) == N.VFB_ERR_INVALID_ARGUMENT
+
+
+def test_scaling_argument_validation_without_launching():
+    from virtualfluids_b200 import _native as N
+    lib = N.lib()
+    coarse, fine = _fake_level(N), _fake_level(N)
+    fine.distributions = 0x5000
+    cells = N.InterpolationCells(0x6000, 0x6100, 4)
+    off = N.InterpolationCellNeighbor(0x6200, 0x6300, 0x6400)
+    for name in ("vfb_scale_coarse_to_fine_compressible", "vfb_scale_fine_to_coarse_compressible"):
+        f = getattr(lib, name)
+        assert f(C.byref(coarse), C.byref(fine), None, C.byref(off), None) == N.VFB_ERR_INVALID_ARGUMENT
+        fine.storage = N.STORAGE_F32
+        assert f(C.byref(coarse), C.byref(fine), C.byref(cells), C.byref(off), None) == N.VFB_ERR_INVALID_ARGUMENT
+        fine.storage = N.STORAGE_F64
+        fine.distributions = coarse.distributions
+        assert f(C.byref(coarse), C.byref(fine), C.byref(cells), C.byref(off), None) == N.VFB_ERR_INVALID_ARGUMENT
+        fine.distributions = 0x5000
+        bad = N.InterpolationCellNeighbor(0x6200, 0, 0x6400)
+        assert f(C.byref(coarse), C.byref(fine), C.byref(cells), C.byref(bad), None) == N.VFB_ERR_INVALID_ARGUMENT
+        # no cells: nothing to launch, nothing to check
+        empty = N.InterpolationCells(0, 0, 0)
+        assert f(C.byref(coarse), C.byref(fine), C.byref(empty), C.byref(bad), None) == N.VFB_OK

@@ -1,7 +1,8 @@
 """B200-native implementation of the VirtualFluids GPU time-step hot path.
 
 D3Q27 K17 cumulant collision with in-place esoteric-twist streaming, the bounce-back,
-interpolated, velocity and non-equilibrium pressure boundary kernels, and the FP64 reductions,
+interpolated, velocity and non-equilibrium pressure boundary kernels, the interpolation between
+refinement levels and the FP64 reductions,
 as hand-written sm_100a CUDA behind the C ABI of ``include/vfb.h`` (``libvfb.so``). This package
 is the Python host side: set-up objects mirroring the reference's Parameter /
 BoundaryConditionFactory / Simulation, a builder for levels in the reference layout, and
@@ -12,6 +13,8 @@ from . import _native
 from ._native import VfbError, lib
 from .box import Box
 from .grid import ListGrid
-from .simulation import BoundaryConditionFactory, Parameter, Simulation
+from .simulation import (BoundaryConditionFactory, GridScalingFactory, InterpolationCells, Parameter, Simulation,
+                         scale_coarse_to_fine, scale_fine_to_coarse)
 
-__all__ = ["Box", "BoundaryConditionFactory", "ListGrid", "Parameter", "Simulation", "VfbError", "lib", "_native"]
+__all__ = ["Box", "BoundaryConditionFactory", "GridScalingFactory", "InterpolationCells", "ListGrid", "Parameter",
+           "Simulation", "VfbError", "lib", "scale_coarse_to_fine", "scale_fine_to_coarse", "_native"]

@@ -48,6 +48,9 @@ PRESSURE_NON_EQUILIBRIUM_COMPRESSIBLE = 1
 PRESSURE_OUTFLOW_NON_REFLECTIVE = 2
 PRESSURE_OUTFLOW_NON_REFLECTIVE_PRESSURE_CORRECTION = 3
 PRESSURE_NOT_SPECIFIED = 4
+# GridScalingFactory::GridScaling (GridScalingFactory.h:50-56)
+SCALE_COMPRESSIBLE = 0
+SCALE_NOT_SPECIFIED = 1
 
 
 class VfbError(RuntimeError):
@@ -78,6 +81,15 @@ class DirectionalBC(C.Structure):
                 ("number_of_bc_nodes", C.c_uint32), ("direction", C.c_int32)]
 
 
+class InterpolationCells(C.Structure):
+    _fields_ = [("fine_cell_indices", C.c_void_p), ("coarse_cell_indices", C.c_void_p),
+                ("number_of_cells", C.c_uint32)]
+
+
+class InterpolationCellNeighbor(C.Structure):
+    _fields_ = [("x", C.c_void_p), ("y", C.c_void_p), ("z", C.c_void_p)]
+
+
 class BoxDesc(C.Structure):
     _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
                 ("periodic_x", C.c_int32), ("periodic_y", C.c_int32), ("periodic_z", C.c_int32),
@@ -105,6 +117,12 @@ SIGNATURES = {
     "vfb_velocity_bounce_back": (C.c_int, [C.POINTER(Level), C.POINTER(BC), C.c_void_p]),
     "vfb_velocity_interpolated_compressible": (C.c_int, [C.POINTER(Level), C.POINTER(BC), C.c_void_p]),
     "vfb_pressure_non_equilibrium_compressible": (C.c_int, [C.POINTER(Level), C.POINTER(DirectionalBC), C.c_void_p]),
+    "vfb_scale_coarse_to_fine_compressible": (C.c_int, [C.POINTER(Level), C.POINTER(Level),
+                                                        C.POINTER(InterpolationCells),
+                                                        C.POINTER(InterpolationCellNeighbor), C.c_void_p]),
+    "vfb_scale_fine_to_coarse_compressible": (C.c_int, [C.POINTER(Level), C.POINTER(Level),
+                                                        C.POINTER(InterpolationCells),
+                                                        C.POINTER(InterpolationCellNeighbor), C.c_void_p]),
     "vfb_init_navier_stokes_compressible": (C.c_int, [C.POINTER(Level), C.c_void_p]),
     "vfb_calc_macroscopic_compressible": (C.c_int, [C.POINTER(Level), C.c_void_p]),
     "vfb_mass_energy_workspace_bytes": (C.c_size_t, [C.c_uint32]),
@@ -114,6 +132,8 @@ SIGNATURES = {
     "vfb_bc_factory_velocity": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),
     "vfb_bc_factory_noslip": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),
     "vfb_bc_factory_pressure": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),
+    "vfb_scaling_factory_fine_to_coarse": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
+    "vfb_scaling_factory_coarse_to_fine": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
     "vfb_simulation_create": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
     "vfb_simulation_destroy": (C.c_int, [C.c_void_p]),
     "vfb_simulation_set_level": (C.c_int, [C.c_void_p, C.POINTER(Level), C.c_void_p, C.c_uint32]),

@@ -268,6 +268,45 @@ int vfb_pressure_non_equilibrium_compressible(const vfb_level *level, const vfb_
     return cuda_status(e, "PressureNonEquilibriumCompressible launch");
 }
 
+static int run_scaling(const vfb_level *coarse, const vfb_level *fine, const vfb_interpolation_cells *cells,
+                       const vfb_interpolation_cell_neighbor *offsets, bool fine_to_coarse, void *stream)
+{
+    int st = check_level(coarse);
+    if (st)
+        return st;
+    st = check_level(fine);
+    if (st)
+        return st;
+    if (!cells || !offsets)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "cells or offsets is NULL");
+    if (coarse->storage != fine->storage || coarse->arith != fine->arith)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "coarse and fine level must share storage and arithmetic");
+    if (coarse->distributions == fine->distributions)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "coarse and fine level share one population array");
+    if (cells->number_of_cells &&
+        (!cells->fine_cell_indices || !cells->coarse_cell_indices || !offsets->x || !offsets->y || !offsets->z))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "interpolation cell arrays are NULL");
+    if (cells->number_of_cells > (1u << 28))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "number_of_cells must be below 2^28");
+    const cudaError_t e = VFB_DISPATCH(coarse->storage, coarse->arith,
+                                       LA::scale(coarse, fine, cells, offsets, fine_to_coarse, as_stream(stream)));
+    return cuda_status(e, fine_to_coarse ? "scaleFineToCoarseCompressible launch" : "scaleCoarseToFineCompressible launch");
+}
+
+int vfb_scale_coarse_to_fine_compressible(const vfb_level *coarse, const vfb_level *fine,
+                                          const vfb_interpolation_cells *cells,
+                                          const vfb_interpolation_cell_neighbor *offsets, void *stream)
+{
+    return run_scaling(coarse, fine, cells, offsets, false, stream);
+}
+
+int vfb_scale_fine_to_coarse_compressible(const vfb_level *coarse, const vfb_level *fine,
+                                          const vfb_interpolation_cells *cells,
+                                          const vfb_interpolation_cell_neighbor *offsets, void *stream)
+{
+    return run_scaling(coarse, fine, cells, offsets, true, stream);
+}
+
 int vfb_init_navier_stokes_compressible(const vfb_level *level, void *stream)
 {
     int st = check_level(level);
@@ -373,6 +412,35 @@ int vfb_bc_factory_pressure(int32_t variant, vfb_directional_bc_fn *fn)
         return fail(VFB_ERR_UNSUPPORTED, "pressure BC variant not built");
     default: return fail(VFB_ERR_INVALID_ARGUMENT, "unknown PressureBC");
     }
+}
+
+// ---------------------------------------------------------------------------------------------
+// grid-scaling factory (GridScalingFactory.cpp: ScaleCompressible -> scale*Compressible<turb>)
+// ---------------------------------------------------------------------------------------------
+static int scaling_factory(int32_t variant, int32_t turbulent, vfb_scaling_fn impl, vfb_scaling_fn *fn)
+{
+    if (!fn)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL fn");
+    *fn = nullptr;
+    switch (variant) {
+    case VFB_SCALE_COMPRESSIBLE:
+        if (turbulent)
+            return fail(VFB_ERR_UNSUPPORTED, "grid scaling with turbulent viscosity not built");
+        *fn = impl;
+        return VFB_OK;
+    case VFB_SCALE_NOT_SPECIFIED: return VFB_OK;
+    default: return fail(VFB_ERR_INVALID_ARGUMENT, "unknown GridScaling");
+    }
+}
+
+int vfb_scaling_factory_fine_to_coarse(int32_t variant, int32_t has_turbulent_viscosity, vfb_scaling_fn *fn)
+{
+    return scaling_factory(variant, has_turbulent_viscosity, vfb_scale_fine_to_coarse_compressible, fn);
+}
+
+int vfb_scaling_factory_coarse_to_fine(int32_t variant, int32_t has_turbulent_viscosity, vfb_scaling_fn *fn)
+{
+    return scaling_factory(variant, has_turbulent_viscosity, vfb_scale_coarse_to_fine_compressible, fn);
 }
 
 } // extern "C"

@@ -9,6 +9,7 @@
 #pragma once
 #include <cstdint>
 
+#include "interp.cuh"
 #include "k17.cuh"
 #include "storage.cuh"
 #include "tma.cuh"
@@ -886,6 +887,143 @@ __global__ void __launch_bounds__(256) energy_list_kernel(const void *dist, uint
         partials[2 * blockIdx.x] = mm;
         partials[2 * blockIdx.x + 1] = ee;
     }
+}
+
+
+// ---------------------------------------------------------------------------------------------
+// refinement: interpolation between a coarse level and the fine level nested in it
+// (GridScaling/scaleCoarseToFineCompressible.cu:305-528, scaleFineToCoarseCompressible.cu:76-124)
+//
+// Eight lanes per interpolation cell, one per corner (interp.cuh): each lane gathers its own
+// corner's 27 populations, so a cell's source reads are spread over eight threads instead of one,
+// and the coefficient sums are formed by shuffles in a fixed corner order.
+// ---------------------------------------------------------------------------------------------
+struct ScaleArgs {
+    void *dist_coarse, *dist_fine;
+    uint64_t n_coarse, n_fine;
+    const uint32_t *nbx_c, *nby_c, *nbz_c;
+    const uint32_t *nbx_f, *nby_f, *nbz_f;
+    const uint32_t *coarse_cells;   // CF: MMM node of the coarse cell; FC: the coarse node at the cell centre
+    const uint32_t *fine_cells;     // MMM node of the fine cell
+    uint32_t n_cells;
+    const void *ox, *oy, *oz;       // offsets of the expansion point, compute type (ICellNeigh)
+    double omega_coarse, omega_fine;
+};
+
+// corner c = ix + 2 iy + 4 iz of the cell whose MMM node is `base`, stepping x, then y, then z
+__device__ __forceinline__ uint32_t cell_corner(uint32_t base, int c, const uint32_t *__restrict__ nbx,
+                                                const uint32_t *__restrict__ nby, const uint32_t *__restrict__ nbz)
+{
+    uint32_t k = base;
+    if (c & 1)
+        k = __ldg(nbx + k);
+    if (c & 2)
+        k = __ldg(nby + k);
+    if (c & 4)
+        k = __ldg(nbz + k);
+    return k;
+}
+
+// coefficients of the cell of this lane's group: moments of the corner at node k (pre-collision
+// populations of parity EVEN), gathered over the group by shuffles. Every lane of the warp calls it.
+template <class S, bool EVEN>
+__device__ __forceinline__ void cell_coefficients_of_group(const S *base, uint64_t n, uint32_t k, bool valid,
+                                                           const uint32_t *nbx, const uint32_t *nby,
+                                                           const uint32_t *nbz, typename Codec<S>::compute omega,
+                                                           typename Codec<S>::compute xo, typename Codec<S>::compute yo,
+                                                           typename Codec<S>::compute zo,
+                                                           InterpCoef<typename Codec<S>::compute> &coef)
+{
+    using C = typename Codec<S>::compute;
+    C m[9];
+    if (valid) {
+        uint32_t nodes[8];
+        list_nodes(k, nbx, nby, nbz, nodes);
+        C f[27];
+        gather_pre<S, EVEN>(base, n, nodes, f);
+        interp_node_moments(f, omega, m);
+    } else {
+#pragma unroll
+        for (int i = 0; i < 9; ++i)
+            m[i] = C(0);
+    }
+    CellSums<C> sums;
+    gather_cell_sums(sums, m, (int)(threadIdx.x & 31u) & ~7);
+    cell_coefficients(sums, xo, yo, zo, coef);
+}
+
+// scaleCoarseToFineCompressible_Device: moments of the coarse cell at the coarse parity with
+// omega_coarse; the fine node of this lane's corner sits at (+-1/4)^3 in coarse-cell units and
+// receives the interpolated populations (epsilon 1/2, omega_fine) as its pre-collision
+// populations of the even parity
+template <class S, bool COARSE_EVEN>
+__global__ void __launch_bounds__(128) scale_cf_kernel(ScaleArgs a)
+{
+    using C = typename Codec<S>::compute;
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t cell = t >> 3;
+    const int corner = (int)(t & 7u);
+    const bool valid = cell < a.n_cells;
+    uint32_t k = 0;
+    C xo = C(0), yo = C(0), zo = C(0);
+    if (valid) {
+        k = cell_corner(__ldg(a.coarse_cells + cell), corner, a.nbx_c, a.nby_c, a.nbz_c);
+        xo = static_cast<const C *>(a.ox)[cell];
+        yo = static_cast<const C *>(a.oy)[cell];
+        zo = static_cast<const C *>(a.oz)[cell];
+    }
+    InterpCoef<C> coef;
+    cell_coefficients_of_group<S, COARSE_EVEN>(static_cast<const S *>(a.dist_coarse), a.n_coarse, k, valid, a.nbx_c,
+                                               a.nby_c, a.nbz_c, (C)a.omega_coarse, xo, yo, zo, coef);
+    if (!valid)
+        return;
+    const C q = C(0.25);
+    C f[27];
+    interp_point<C, false>(coef, (C)a.omega_fine, C(0.5), (corner & 1) ? q : -q, (corner & 2) ? q : -q,
+                           (corner & 4) ? q : -q, f);
+    uint32_t nodes[8];
+    list_nodes(cell_corner(__ldg(a.fine_cells + cell), corner, a.nbx_f, a.nby_f, a.nbz_f), a.nbx_f, a.nby_f, a.nbz_f,
+               nodes);
+    S *fine = static_cast<S *>(a.dist_fine);
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        Codec<S>::store(fine + (uint64_t)plane<true>(d) * a.n_fine + nodes[shift_class(d)], f[d], d);
+}
+
+// scaleFineToCoarseCompressible_Device: moments of the fine cell at the even parity with
+// omega_fine; the coarse node at the cell centre receives the interpolated populations
+// (epsilon 2, omega_coarse) as its pre-collision populations of the coarse parity. The eight lanes
+// of the cell share the 27 stores.
+template <class S, bool COARSE_EVEN>
+__global__ void __launch_bounds__(128) scale_fc_kernel(ScaleArgs a)
+{
+    using C = typename Codec<S>::compute;
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t cell = t >> 3;
+    const int corner = (int)(t & 7u);
+    const bool valid = cell < a.n_cells;
+    uint32_t k = 0;
+    C xo = C(0), yo = C(0), zo = C(0);
+    if (valid) {
+        k = cell_corner(__ldg(a.fine_cells + cell), corner, a.nbx_f, a.nby_f, a.nbz_f);
+        xo = static_cast<const C *>(a.ox)[cell];
+        yo = static_cast<const C *>(a.oy)[cell];
+        zo = static_cast<const C *>(a.oz)[cell];
+    }
+    InterpCoef<C> coef;
+    cell_coefficients_of_group<S, true>(static_cast<const S *>(a.dist_fine), a.n_fine, k, valid, a.nbx_f, a.nby_f,
+                                        a.nbz_f, (C)a.omega_fine, xo, yo, zo, coef);
+    if (!valid)
+        return;
+    C f[27];
+    interp_point<C, true>(coef, (C)a.omega_coarse, C(2), C(0), C(0), C(0), f);
+    uint32_t nodes[8];
+    list_nodes(__ldg(a.coarse_cells + cell), a.nbx_c, a.nby_c, a.nbz_c, nodes);
+    S *coarse = static_cast<S *>(a.dist_coarse);
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        if ((d & 7) == corner)
+            Codec<S>::store(coarse + (uint64_t)plane<COARSE_EVEN>(d) * a.n_coarse + nodes[shift_class(d)], f[d], d);
 }
 
 } // namespace VFB_NS

@@ -58,6 +58,8 @@ inline uint64_t box_blocks(const BoxState &b)
                                     const void *uz, cudaStream_t s);                                               \
         static cudaError_t box_macros(const BoxState &b, bool even, void *rho, void *ux, void *uy, void *uz,       \
                                       cudaStream_t s);                                                             \
+        static cudaError_t scale(const vfb_level *coarse, const vfb_level *fine, const vfb_interpolation_cells *cells, \
+                                 const vfb_interpolation_cell_neighbor *offsets, bool fine_to_coarse, cudaStream_t s); \
     };
 
 // BC kinds of Launchers::bc

@@ -149,6 +149,44 @@ cudaError_t Launchers<S>::pressure(const vfb_level *L, const vfb_directional_bc 
 }
 
 template <class S>
+cudaError_t Launchers<S>::scale(const vfb_level *coarse, const vfb_level *fine, const vfb_interpolation_cells *cells,
+                                const vfb_interpolation_cell_neighbor *offsets, bool fine_to_coarse, cudaStream_t s)
+{
+    if (cells->number_of_cells == 0)
+        return cudaSuccess;
+    ScaleArgs a;
+    a.dist_coarse = coarse->distributions;
+    a.dist_fine = fine->distributions;
+    a.n_coarse = coarse->number_of_nodes;
+    a.n_fine = fine->number_of_nodes;
+    a.nbx_c = coarse->neighbor_x;
+    a.nby_c = coarse->neighbor_y;
+    a.nbz_c = coarse->neighbor_z;
+    a.nbx_f = fine->neighbor_x;
+    a.nby_f = fine->neighbor_y;
+    a.nbz_f = fine->neighbor_z;
+    a.coarse_cells = cells->coarse_cell_indices;
+    a.fine_cells = cells->fine_cell_indices;
+    a.n_cells = cells->number_of_cells;
+    a.ox = offsets->x;
+    a.oy = offsets->y;
+    a.oz = offsets->z;
+    a.omega_coarse = coarse->omega;
+    a.omega_fine = fine->omega;
+    // eight lanes per cell
+    const unsigned B = 128, G = grid1d((uint64_t)a.n_cells * 8u, B);
+    const bool even = coarse->is_even_timestep != 0;
+    if (fine_to_coarse) {
+        if (even) scale_fc_kernel<S, true><<<G, B, 0, s>>>(a);
+        else scale_fc_kernel<S, false><<<G, B, 0, s>>>(a);
+    } else {
+        if (even) scale_cf_kernel<S, true><<<G, B, 0, s>>>(a);
+        else scale_cf_kernel<S, false><<<G, B, 0, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+template <class S>
 cudaError_t Launchers<S>::init_list(const vfb_level *L, cudaStream_t s)
 {
     const unsigned B = 128, G = grid1d(L->number_of_nodes, B);
@@ -262,34 +300,70 @@ cudaError_t launch_box_tma(const BoxCollideArgs<typename Codec<S>::compute> &a, 
 }
 // Three resident blocks per SM: with four (possible when the compiler needs no more than 128
 // registers) the 4 x 55 KB of staging leave almost no L1 and the kernel runs ~25 % slower on B200.
-// The carve-out asks for the shared-memory configuration of three blocks, leaving the rest to L1.
+// Each block therefore asks for a third of the smallest shared-memory configuration that holds
+// three blocks' staging (padding the dynamic allocation), so a fourth block never fits whatever
+// configuration the driver picks, and the carve-out asks for that configuration, leaving the rest
+// of the SM's 256 KB to L1.
 constexpr int kAsyncBlocksPerSm = 3;
+
+struct AsyncLaunchShape {
+    int blocks_per_sm;
+    int dyn_smem;
+};
+
+// shared-memory capacities (KB) an SM of compute capability 10.0 can be configured to
+inline int smem_config_bytes(int need)
+{
+    static const int kb[] = { 0, 8, 16, 32, 64, 100, 132, 164, 196, 228 };
+    for (int c : kb)
+        if (c * 1024 >= need)
+            return c * 1024;
+    return 228 * 1024;
+}
+
+template <class K>
+cudaError_t async_launch_shape(K kern, size_t smem, AsyncLaunchShape &out)
+{
+    int dev = 0, max_smem = 0, reserved = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const int cfg = std::min(smem_config_bytes(kAsyncBlocksPerSm * ((int)smem + reserved)), max_smem);
+    int dyn = (cfg / kAsyncBlocksPerSm - reserved) & ~127;
+    dyn = std::max(dyn, (int)smem);
+    if (optin > 0)
+        dyn = std::min(dyn, optin);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    if (e != cudaSuccess)
+        return e;
+    if (max_smem > 0)
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             std::min(100, (cfg * 100 + max_smem - 1) / max_smem));
+    int bps = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, 128, dyn);
+    if (e != cudaSuccess)
+        return e;
+    out.blocks_per_sm = std::max(1, std::min(bps, kAsyncBlocksPerSm));
+    out.dyn_smem = dyn;
+    return cudaSuccess;
+}
 
 template <class S, bool E, bool M, bool N>
 cudaError_t launch_box_async(const BoxCollideArgs<typename Codec<S>::compute> &a, uint64_t *n_partials, cudaStream_t s)
 {
     auto kern = k17_box_async_kernel<S, VFB_EXACT, E, M, N>;
-    static int blocks_per_sm = -1;
-    if (blocks_per_sm < 0) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)AsyncTile<S>::SMEM);
+    static AsyncLaunchShape shape = { -1, 0 };
+    if (shape.blocks_per_sm < 0) {
+        AsyncLaunchShape sh;
+        const cudaError_t e = async_launch_shape(kern, AsyncTile<S>::SMEM, sh);
         if (e != cudaSuccess)
             return e;
-        int dev = 0, max_smem = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-        if (max_smem > 0) {
-            const int want = (int)(kAsyncBlocksPerSm * (AsyncTile<S>::SMEM + 1024));
-            const int pct = std::min(100, (want * 100 + max_smem - 1) / max_smem);
-            cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
-        }
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, 128, AsyncTile<S>::SMEM);
-        if (e != cudaSuccess)
-            return e;
-        blocks_per_sm = std::max(1, std::min(blocks_per_sm, kAsyncBlocksPerSm));
+        shape = sh;
     }
     const int64_t ntiles = (int64_t)((a.nx + AsyncTile<S>::BX - 1) / AsyncTile<S>::BX) * a.ny * a.nz;
-    const int64_t grid = std::min<int64_t>(ntiles, (int64_t)blocks_per_sm * sm_count());
-    kern<<<(unsigned)grid, 128, AsyncTile<S>::SMEM, s>>>(a);
+    const int64_t grid = std::min<int64_t>(ntiles, (int64_t)shape.blocks_per_sm * sm_count());
+    kern<<<(unsigned)grid, 128, shape.dyn_smem, s>>>(a);
     if (n_partials)
         *n_partials = (uint64_t)grid;
     return cudaGetLastError();

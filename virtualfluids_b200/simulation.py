@@ -130,6 +130,75 @@ class BoundaryConditionFactory:
         return fn.value
 
 
+class GridScalingFactory:
+    """GridScalingFactory (src/gpu/core/GridScaling/GridScalingFactory.h:47-66): the choice of the
+    interpolation between levels; NotSpecified by default."""
+
+    class GridScaling(enum.IntEnum):
+        ScaleCompressible = N.SCALE_COMPRESSIBLE
+        NotSpecified = N.SCALE_NOT_SPECIFIED
+
+    def __init__(self):
+        self.grid_scaling_type = self.GridScaling.NotSpecified
+
+    def set_scaling_factory(self, grid_scaling_type):
+        self.grid_scaling_type = self.GridScaling(grid_scaling_type)
+
+    def get_grid_scaling_fc(self, has_turbulent_viscosity: bool = False):
+        fn = C.c_void_p()
+        N.check(N.lib().vfb_scaling_factory_fine_to_coarse(int(self.grid_scaling_type), int(has_turbulent_viscosity),
+                                                             C.byref(fn)))
+        return fn.value
+
+    def get_grid_scaling_cf(self, has_turbulent_viscosity: bool = False):
+        fn = C.c_void_p()
+        N.check(N.lib().vfb_scaling_factory_coarse_to_fine(int(self.grid_scaling_type), int(has_turbulent_viscosity),
+                                                             C.byref(fn)))
+        return fn.value
+
+
+class InterpolationCells:
+    """ICells + ICellNeigh (src/gpu/core/Calculation/Calculation.h:72-87) on the device.
+
+    fine_cell_indices: MMM node of each cell on the fine level; coarse_cell_indices: the MMM node
+    of the coarse cell (coarse to fine) or the coarse node at the cell centre (fine to coarse);
+    offsets: (3, n) offsets of the expansion point, 0 in the bulk."""
+
+    def __init__(self, fine_cell_indices, coarse_cell_indices, offsets=None, storage=N.STORAGE_F64, device="cuda"):
+        t = _torch()
+        fine_cell_indices = np.asarray(fine_cell_indices)
+        coarse_cell_indices = np.asarray(coarse_cell_indices)
+        n = fine_cell_indices.size
+        if coarse_cell_indices.size != n:
+            raise ValueError("fine and coarse cell lists differ in length")
+        off = np.zeros((3, n)) if offsets is None else np.asarray(offsets, dtype=np.float64).reshape(3, n)
+        rd = real_dtype(storage)
+        self.fine = t.from_numpy(fine_cell_indices.astype(np.int32)).to(device)
+        self.coarse = t.from_numpy(coarse_cell_indices.astype(np.int32)).to(device)
+        self.offsets = [t.from_numpy(off[a].copy()).to(device=device, dtype=rd) for a in range(3)]
+        self.cells = N.InterpolationCells(self.fine.data_ptr(), self.coarse.data_ptr(), n)
+        self.neighbor = N.InterpolationCellNeighbor(*(o.data_ptr() for o in self.offsets))
+
+    @property
+    def number_of_cells(self) -> int:
+        return int(self.cells.number_of_cells)
+
+
+def _run_scaling(name, coarse, fine, cells, stream):
+    N.check(getattr(N.lib(), name)(C.byref(coarse.level), C.byref(fine.level), C.byref(cells.cells),
+                                   C.byref(cells.neighbor), stream))
+
+
+def scale_coarse_to_fine(coarse, fine, cells: InterpolationCells, stream=None):
+    """scaleCoarseToFineCompressible (GridScaling/Scaling.cu:106) between two Simulation levels."""
+    _run_scaling("vfb_scale_coarse_to_fine_compressible", coarse, fine, cells, stream)
+
+
+def scale_fine_to_coarse(coarse, fine, cells: InterpolationCells, stream=None):
+    """scaleFineToCoarseCompressible (GridScaling/Scaling.cu:156) between two Simulation levels."""
+    _run_scaling("vfb_scale_fine_to_coarse_compressible", coarse, fine, cells, stream)
+
+
 def _ptr(t):
     return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
 
