@@ -42,6 +42,10 @@ N_SIDE = 256
 U0 = 0.04
 RE = 1600.0
 BYTES_PER_NODE = {"f64": 432, "f32": 216, "f16": 108, "bf16": 108}
+# DRAM bytes (read + write) per node of one launch of the FP64 direct-load collision kernel, from
+# one ncu capture at 128^3 (profiles/k17_box_kernel_f64_tgv128.md: 453.0 MB + 395.8 MB over
+# 2,097,152 nodes); traffic grows with the node count, so it is scaled to the bench's box
+NCU_DRAM_BYTES_PER_NODE_F64 = (453.033728e6 + 395.824384e6) / 2097152
 METRIC = "MLUPS (TGV 256^3 D3Q27 K17, FP64)"
 
 
@@ -233,12 +237,14 @@ def main():
     box.step(args.warmup, energy=energy, stream=sp)
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = box.kernel_launches()
     with ClockSampler(local) as clk:
         with torch.cuda.stream(stream):
             ev0.record(stream)
             box.step(args.steps, energy=energy, stream=sp)
             ev1.record(stream)
         stream.synchronize()
+    launches = box.kernel_launches() - launches0
     barrier()
     t_ms = max_over_ranks(ev0.elapsed_time(ev1))
     value = nodes * args.steps * world / (t_ms / 1e3) / 1e6
@@ -255,7 +261,10 @@ def main():
     peak, peak_kind = measured_peak()
     achieved = BYTES_PER_NODE["f64"] * nodes / (k_ms / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": None,
+                "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                "traffic": round(NCU_DRAM_BYTES_PER_NODE_F64 * nodes) if args.kernel in ("auto", "direct") else None,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 128^3 launch, "
+                                  "scaled by nodes",
                 "kernel": "k17_box_kernel<double> (collision + ET streaming)", "kernel_ms": round(k_ms, 4),
                 "algorithmic_bytes_per_launch": BYTES_PER_NODE["f64"] * nodes}
     e_host = energy[: 2 * args.steps].cpu().numpy()
@@ -320,7 +329,6 @@ def main():
         cb = cpu_baseline()
 
     if rank == 0:
-        launches = 2 * args.steps  # one collision + one energy reduction per timed step
         line = {
             "metric": METRIC, "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(t_ms / args.steps, 4), "higher_is_better": True,

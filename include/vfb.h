@@ -181,6 +181,26 @@ int vfb_scale_fine_to_coarse_compressible(const vfb_level *coarse, const vfb_lev
                                           const vfb_interpolation_cells *cells,
                                           const vfb_interpolation_cell_neighbor *offsets, void *stream);
 
+/* DragLiftPostD27 (PostProcessor/DragLift.cu:558-567, kernel :50-301): per geometry BC node, minus
+   the momentum carried by the post-collision populations that leave the node through its cut
+   links (q in [0, 1]), in double; called after the collision and before the geometry BC
+   (BoundaryConditionKernelManager.cpp:258-276). drag_x/y/z: double[number_of_bc_nodes], device. */
+int vfb_drag_lift_post_27(const vfb_level *level, const vfb_bc *geometry_bc, double *drag_x, double *drag_y,
+                          double *drag_z, void *stream);
+/* DragLiftPreD27 (DragLift.cu:569-578, kernel :304-555): after the parity swap, minus the momentum of
+   the populations each geometry node reads next, each weighted by the cut link of the opposite
+   direction (BoundaryConditionKernelManager.cpp:148-172). */
+int vfb_drag_lift_pre_27(const vfb_level *level, const vfb_bc *geometry_bc, double *drag_x, double *drag_y,
+                         double *drag_z, void *stream);
+/* calcDragLift (PostProcessor/DragLift.cpp:52-73): the force on the geometry, the FP64 sum over the
+   nodes of pre - post, formed on the device in a fixed order and copied to force[3] on the host
+   (the coefficient 2 F / (rho u^2 A) is left to the caller, whose area it needs). Device
+   workspace of vfb_drag_lift_workspace_bytes(n) bytes. Synchronises the stream. */
+size_t vfb_drag_lift_workspace_bytes(uint32_t n);
+int vfb_drag_lift_force(const double *pre_x, const double *pre_y, const double *pre_z, const double *post_x,
+                        const double *post_y, const double *post_z, uint32_t n, void *workspace, size_t workspace_bytes,
+                        double force[3], void *stream);
+
 /* InitNavierStokesCompressible::init (PreProcessor/PreProcessorStrategy/InitNavierStokesCompressible/
    InitNavierStokesCompressible.cu:45): equilibrium from level->rho/velocity_* for the level's
    current parity. PreProcessorImp::init (PreProcessorImp.cpp:50-58) calls it for the odd, then
@@ -246,9 +266,19 @@ int vfb_simulation_set_level(vfb_simulation *sim, const vfb_level *level, const 
 int vfb_simulation_set_velocity_bc(vfb_simulation *sim, const vfb_bc *bc, int32_t variant);
 int vfb_simulation_set_noslip_bc(vfb_simulation *sim, const vfb_bc *bc, int32_t variant);
 int vfb_simulation_add_pressure_bc(vfb_simulation *sim, const vfb_directional_bc *bc, int32_t variant);
+/* the geometry BC list (BoundaryConditionFactory::setGeometryBoundaryCondition with a NoSlipBC
+   value); it runs after the no-slip BC, as runGeoBCKernelPost (UpdateGrid27.cpp:247-248) */
+int vfb_simulation_set_geometry_bc(vfb_simulation *sim, const vfb_bc *bc, int32_t variant);
+/* drag and lift on the geometry nodes every step (Parameter::setCalcDragLift): DragLiftPost27 before
+   the geometry BC, DragLiftPre27 and the FP64 sum after the parity swap, the force of step t into
+   force_history[3 * (t % history_steps)] (device, no host synchronisation). Caller-owned device
+   workspace of vfb_simulation_drag_lift_workspace_bytes(geometry nodes) bytes; NULL disables. */
+size_t vfb_simulation_drag_lift_workspace_bytes(uint32_t number_of_geometry_nodes);
+int vfb_simulation_set_drag_lift(vfb_simulation *sim, void *workspace, size_t workspace_bytes, double *force_history,
+                                 uint32_t history_steps);
 /* checks the BoundaryConditionKernelManager rules: a BC with nodes but no kernel is VFB_ERR_BC_UNSET */
 int vfb_simulation_check(const vfb_simulation *sim);
-/* run steps: collision, velocity then no-slip BCs, parity toggle, pressure BCs */
+/* run steps: collision, velocity, no-slip then geometry BCs, parity toggle, drag/lift, pressure BCs */
 int vfb_simulation_run(vfb_simulation *sim, uint32_t steps, void *stream);
 int vfb_simulation_is_even_timestep(const vfb_simulation *sim, int32_t *is_even);
 
@@ -282,10 +312,16 @@ int vfb_box_fields(vfb_box *box, void *rho, void *ux, void *uy, void *uz, int32_
 /* synchronises the stream and reads the status word the box's kernels set on a failed internal wait
    (0 = fine); returns VFB_ERR_CUDA when it is nonzero */
 int vfb_box_status(vfb_box *box, int32_t *device_status, void *stream);
-/* collision kernel: 0 = choose (per-thread asynchronous copies for F64/F32 storage, direct loads for
-   16-bit storage), 1 = direct loads, 2 = TMA-staged warp tiles (nx % 32 == 0),
+/* collision kernel: 0 = choose (direct loads, the fastest measured on B200 for every storage),
+   1 = direct loads, 2 = TMA-staged warp tiles (nx % 32 == 0),
    3 = per-thread asynchronous copies (F64 and F32 storage) */
 int vfb_box_set_kernel_variant(vfb_box *box, int32_t variant);
+/* number of kernels vfb_box_step has launched for this box so far (collision and reductions) */
+int vfb_box_kernel_launches(const vfb_box *box, uint64_t *count);
+/* launch shape of the per-thread asynchronous-copy kernel: resident blocks per SM (0 = 3) and the
+   shared-memory configuration in KB each block pads its staging to a share of (0 = no padding,
+   only a carve-out hint; else 64, 100, 132, 164, 196 or 228). Results do not depend on it. */
+int vfb_box_set_launch_shape(vfb_box *box, int32_t blocks_per_sm, int32_t smem_kb);
 /* raw access to the population planes for checks: pointer, plane pitch (elements), parity */
 int vfb_box_populations(const vfb_box *box, void **dist, uint64_t *pitch, int32_t *is_even);
 

@@ -123,6 +123,12 @@ SIGNATURES = {
     "vfb_scale_fine_to_coarse_compressible": (C.c_int, [C.POINTER(Level), C.POINTER(Level),
                                                         C.POINTER(InterpolationCells),
                                                         C.POINTER(InterpolationCellNeighbor), C.c_void_p]),
+    "vfb_drag_lift_post_27": (C.c_int, [C.POINTER(Level), C.POINTER(BC), C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p]),
+    "vfb_drag_lift_pre_27": (C.c_int, [C.POINTER(Level), C.POINTER(BC), C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p]),
+    "vfb_drag_lift_workspace_bytes": (C.c_size_t, [C.c_uint32]),
+    "vfb_drag_lift_force": (C.c_int, [C.c_void_p] * 6 + [C.c_uint32, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
     "vfb_init_navier_stokes_compressible": (C.c_int, [C.POINTER(Level), C.c_void_p]),
     "vfb_calc_macroscopic_compressible": (C.c_int, [C.POINTER(Level), C.c_void_p]),
     "vfb_mass_energy_workspace_bytes": (C.c_size_t, [C.c_uint32]),
@@ -140,6 +146,9 @@ SIGNATURES = {
     "vfb_simulation_set_velocity_bc": (C.c_int, [C.c_void_p, C.POINTER(BC), C.c_int32]),
     "vfb_simulation_set_noslip_bc": (C.c_int, [C.c_void_p, C.POINTER(BC), C.c_int32]),
     "vfb_simulation_add_pressure_bc": (C.c_int, [C.c_void_p, C.POINTER(DirectionalBC), C.c_int32]),
+    "vfb_simulation_set_geometry_bc": (C.c_int, [C.c_void_p, C.POINTER(BC), C.c_int32]),
+    "vfb_simulation_drag_lift_workspace_bytes": (C.c_size_t, [C.c_uint32]),
+    "vfb_simulation_set_drag_lift": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_uint32]),
     "vfb_simulation_check": (C.c_int, [C.c_void_p]),
     "vfb_simulation_run": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p]),
     "vfb_simulation_is_even_timestep": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
@@ -151,6 +160,8 @@ SIGNATURES = {
     "vfb_box_fields": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "vfb_box_status": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.c_void_p]),
     "vfb_box_set_kernel_variant": (C.c_int, [C.c_void_p, C.c_int32]),
+    "vfb_box_kernel_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    "vfb_box_set_launch_shape": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "vfb_box_populations": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64),
                                       C.POINTER(C.c_int32)]),
 }

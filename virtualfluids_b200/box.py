@@ -100,6 +100,17 @@ class Box:
         (per-thread asynchronous copies of the next node)."""
         N.check(N.lib().vfb_box_set_kernel_variant(self._h, {"auto": 0, "direct": 1, "tma": 2, "async": 3}[variant]))
 
+    def kernel_launches(self) -> int:
+        """Kernels vfb_box_step has launched for this box so far."""
+        c = C.c_uint64()
+        N.check(N.lib().vfb_box_kernel_launches(self._h, C.byref(c)))
+        return c.value
+
+    def set_launch_shape(self, blocks_per_sm: int = 0, smem_kb: int = 0):
+        """Launch shape of the asynchronous-copy kernel (resident blocks per SM, shared-memory
+        configuration in KB to pad to; 0 = defaults). Results do not depend on it."""
+        N.check(N.lib().vfb_box_set_launch_shape(self._h, int(blocks_per_sm), int(smem_kb)))
+
     def populations(self):
         """(device pointer, plane pitch in elements, is_even) of the population array."""
         p, pitch, ev = C.c_void_p(), C.c_uint64(), C.c_int32()

@@ -87,11 +87,15 @@ const KernelEntry kKernels[] = { { "K17CompressibleNavierStokes", VFB_KERNEL_K17
 // deterministic partial-sum reduction
 // ---------------------------------------------------------------------------------------------
 namespace vfb {
-__global__ void __launch_bounds__(1024) reduce_partials_kernel(const double *__restrict__ p, uint64_t blocks, double *out)
+// block g sums the partial pairs [g * chunk, min((g + 1) * chunk, blocks)) into out[2g], out[2g + 1]:
+// each thread strides through the chunk, then a fixed shared-memory tree (blockDim a power of two)
+__global__ void __launch_bounds__(1024) reduce_partials_kernel(const double *__restrict__ p, uint64_t blocks,
+                                                               uint64_t chunk, double *out)
 {
     __shared__ double sm[2][1024];
+    const uint64_t lo = blockIdx.x * chunk, hi = lo + chunk < blocks ? lo + chunk : blocks;
     double m = 0.0, e = 0.0;
-    for (uint64_t b = threadIdx.x; b < blocks; b += blockDim.x) {
+    for (uint64_t b = lo + threadIdx.x; b < hi; b += blockDim.x) {
         m += p[2 * b];
         e += p[2 * b + 1];
     }
@@ -106,16 +110,92 @@ __global__ void __launch_bounds__(1024) reduce_partials_kernel(const double *__r
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        out[0] = sm[0][0];
-        out[1] = sm[1][0];
+        out[2 * blockIdx.x] = sm[0][0];
+        out[2 * blockIdx.x + 1] = sm[1][0];
     }
+}
+
+// calcDragLift (DragLift.cpp:66-73): per block, the sums of pre - post over its nodes (three
+// doubles, a fixed shared-memory tree); a second pass adds the blocks in order
+struct DragSumArgs {
+    const double *pre[3], *post[3];
+};
+
+__global__ void __launch_bounds__(256) drag_lift_sum_kernel(DragSumArgs a, uint32_t n, double *partials)
+{
+    __shared__ double sm[3][256];
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        sm[c][threadIdx.x] = i < n ? a.pre[c][i] - a.post[c][i] : 0.0;
+    __syncthreads();
+    for (unsigned s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                sm[c][threadIdx.x] += sm[c][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x < 3)
+        partials[3 * blockIdx.x + threadIdx.x] = sm[threadIdx.x][0];
+}
+
+__global__ void __launch_bounds__(256) drag_lift_total_kernel(const double *__restrict__ partials, uint32_t blocks,
+                                                              double *out)
+{
+    __shared__ double sm[3][256];
+    double acc[3] = { 0.0, 0.0, 0.0 };
+    for (uint32_t b = threadIdx.x; b < blocks; b += blockDim.x)
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+            acc[a] += partials[3 * b + a];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        sm[a][threadIdx.x] = acc[a];
+    __syncthreads();
+    for (unsigned s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                sm[a][threadIdx.x] += sm[a][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x < 3)
+        out[threadIdx.x] = sm[threadIdx.x][0];
+}
+
+cudaError_t drag_lift_sum(const double *const pre[3], const double *const post[3], uint32_t n, double *scratch,
+                          double *out, cudaStream_t s)
+{
+    const uint32_t blocks = (n + 255u) / 256u;
+    if (blocks == 0)
+        return cudaMemsetAsync(out, 0, 3 * sizeof(double), s);
+    DragSumArgs a;
+    for (int c = 0; c < 3; ++c) {
+        a.pre[c] = pre[c];
+        a.post[c] = post[c];
+    }
+    drag_lift_sum_kernel<<<blocks, 256, 0, s>>>(a, n, scratch);
+    drag_lift_total_kernel<<<1, 256, 0, s>>>(scratch, blocks, out);
+    return cudaGetLastError();
 }
 
 void set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
 
 cudaError_t reduce_partials(const double *partials, uint64_t blocks, double *out, cudaStream_t s)
 {
-    reduce_partials_kernel<<<1, 1024, 0, s>>>(partials, blocks, out);
+    reduce_partials_kernel<<<1, 1024, 0, s>>>(partials, blocks, blocks, out);
+    return cudaGetLastError();
+}
+
+cudaError_t reduce_partials_wide(const double *partials, uint64_t blocks, double *scratch, double *out, cudaStream_t s)
+{
+    if (blocks <= kReduceDirect)
+        return reduce_partials(partials, blocks, out, s);
+    const uint64_t g = std::min<uint64_t>(kReduceMaxChunks, (blocks + 2047) / 2048);
+    const uint64_t chunk = (blocks + g - 1) / g;
+    reduce_partials_kernel<<<(unsigned)g, 256, 0, s>>>(partials, blocks, chunk, scratch);
+    reduce_partials_kernel<<<1, 1024, 0, s>>>(scratch, g, g, out);
     return cudaGetLastError();
 }
 } // namespace vfb
@@ -307,6 +387,59 @@ int vfb_scale_fine_to_coarse_compressible(const vfb_level *coarse, const vfb_lev
     return run_scaling(coarse, fine, cells, offsets, true, stream);
 }
 
+static int run_drag_lift(const vfb_level *level, const vfb_bc *bc, bool pre, double *dx, double *dy, double *dz,
+                         void *stream)
+{
+    int st = check_level(level);
+    if (st)
+        return st;
+    if (!bc)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "geometry bc is NULL");
+    if (bc->number_of_bc_nodes && (!bc->k || !bc->q27 || !dx || !dy || !dz))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "drag/lift arrays are NULL");
+    const cudaError_t e = VFB_DISPATCH(level->storage, level->arith, LA::drag_lift(level, bc, pre, dx, dy, dz, as_stream(stream)));
+    return cuda_status(e, pre ? "DragLiftPre27 launch" : "DragLiftPost27 launch");
+}
+
+int vfb_drag_lift_post_27(const vfb_level *level, const vfb_bc *geometry_bc, double *drag_x, double *drag_y,
+                          double *drag_z, void *stream)
+{
+    return run_drag_lift(level, geometry_bc, false, drag_x, drag_y, drag_z, stream);
+}
+
+int vfb_drag_lift_pre_27(const vfb_level *level, const vfb_bc *geometry_bc, double *drag_x, double *drag_y,
+                         double *drag_z, void *stream)
+{
+    return run_drag_lift(level, geometry_bc, true, drag_x, drag_y, drag_z, stream);
+}
+
+size_t vfb_drag_lift_workspace_bytes(uint32_t n)
+{
+    return (size_t)(3 * ((n + 255u) / 256u) + 3) * sizeof(double);
+}
+
+int vfb_drag_lift_force(const double *pre_x, const double *pre_y, const double *pre_z, const double *post_x,
+                        const double *post_y, const double *post_z, uint32_t n, void *workspace, size_t workspace_bytes,
+                        double force[3], void *stream)
+{
+    if (!force || !workspace || (n && (!pre_x || !pre_y || !pre_z || !post_x || !post_y || !post_z)))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (workspace_bytes < vfb_drag_lift_workspace_bytes(n))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "workspace too small");
+    if ((reinterpret_cast<uintptr_t>(workspace) & 7u) != 0)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "workspace must be 8-byte aligned");
+    cudaStream_t s = as_stream(stream);
+    double *scratch = static_cast<double *>(workspace);
+    double *result = scratch + 3 * ((n + 255u) / 256u);
+    const double *pre[3] = { pre_x, pre_y, pre_z }, *post[3] = { post_x, post_y, post_z };
+    cudaError_t e = vfb::drag_lift_sum(pre, post, n, scratch, result, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(force, result, 3 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s);
+    return cuda_status(e, "drag/lift sum");
+}
+
 int vfb_init_navier_stokes_compressible(const vfb_level *level, void *stream)
 {
     int st = check_level(level);
@@ -462,6 +595,14 @@ struct vfb_simulation {
     bool noslip_set = false;
     std::vector<vfb_directional_bc> pressure;
     std::vector<vfb_directional_bc_fn> pressure_fn;
+    vfb_bc geometry{};
+    vfb_bc_fn geometry_fn = nullptr;
+    bool geometry_set = false;
+    // drag and lift on the geometry nodes (caller-owned device memory)
+    double *drag_work = nullptr;      // pre x, y, z; post x, y, z (6 * n); block partials
+    double *drag_history = nullptr;   // 3 doubles per step, ring of drag_history_len steps
+    uint32_t drag_history_len = 0;
+    uint64_t drag_steps = 0;
 };
 
 extern "C" {
@@ -546,6 +687,51 @@ int vfb_simulation_add_pressure_bc(vfb_simulation *sim, const vfb_directional_bc
 
 // BoundaryConditionKernelManager.cpp:67-80: a BC that has nodes needs a kernel; the delayed
 // no-slip bounce-back is the one BC whose "kernel" is deliberately empty.
+int vfb_simulation_set_geometry_bc(vfb_simulation *sim, const vfb_bc *bc, int32_t variant)
+{
+    if (!sim || !bc)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    vfb_bc_fn fn = nullptr;
+    int st = vfb_bc_factory_noslip(variant, &fn);
+    if (st)
+        return st;
+    sim->geometry = *bc;
+    sim->geometry_fn = fn;
+    sim->geometry_set = true;
+    return VFB_OK;
+}
+
+size_t vfb_simulation_drag_lift_workspace_bytes(uint32_t number_of_geometry_nodes)
+{
+    return (size_t)6 * number_of_geometry_nodes * sizeof(double) + vfb_drag_lift_workspace_bytes(number_of_geometry_nodes);
+}
+
+int vfb_simulation_set_drag_lift(vfb_simulation *sim, void *workspace, size_t workspace_bytes, double *force_history,
+                                 uint32_t history_steps)
+{
+    if (!sim)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL simulation");
+    if (!workspace) {
+        sim->drag_work = nullptr;
+        sim->drag_history = nullptr;
+        sim->drag_history_len = 0;
+        return VFB_OK;
+    }
+    if (!sim->geometry_set)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "drag and lift need a geometry boundary condition");
+    if (!force_history || history_steps == 0)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "drag and lift need a force history of at least one step");
+    if (workspace_bytes < vfb_simulation_drag_lift_workspace_bytes(sim->geometry.number_of_bc_nodes))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "workspace too small");
+    if ((reinterpret_cast<uintptr_t>(workspace) & 7u) != 0)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "workspace must be 8-byte aligned");
+    sim->drag_work = static_cast<double *>(workspace);
+    sim->drag_history = force_history;
+    sim->drag_history_len = history_steps;
+    sim->drag_steps = 0;
+    return VFB_OK;
+}
+
 int vfb_simulation_check(const vfb_simulation *sim)
 {
     if (!sim)
@@ -558,6 +744,39 @@ int vfb_simulation_check(const vfb_simulation *sim)
         if (sim->pressure[i].number_of_bc_nodes > 0 && !sim->pressure_fn[i])
             return fail(VFB_ERR_BC_UNSET, "Pressure boundary condition has nodes but no kernel");
     return VFB_OK;
+}
+
+static int run_geometry_post(vfb_simulation *sim, void *stream)
+{
+    vfb_level &L = sim->level;
+    const uint32_t ng = sim->geometry.number_of_bc_nodes;
+    if (!sim->geometry_set || ng == 0)
+        return VFB_OK;
+    if (sim->drag_work) {
+        double *w = sim->drag_work;
+        int st = vfb_drag_lift_post_27(&L, &sim->geometry, w + 3 * (size_t)ng, w + 4 * (size_t)ng, w + 5 * (size_t)ng, stream);
+        if (st)
+            return st;
+    }
+    return sim->geometry_fn ? sim->geometry_fn(&L, &sim->geometry, stream) : VFB_OK;
+}
+
+static int run_geometry_pre(vfb_simulation *sim, void *stream)
+{
+    vfb_level &L = sim->level;
+    const uint32_t ng = sim->geometry.number_of_bc_nodes;
+    if (!sim->geometry_set || ng == 0 || !sim->drag_work)
+        return VFB_OK;
+    double *w = sim->drag_work;
+    int st = vfb_drag_lift_pre_27(&L, &sim->geometry, w, w + ng, w + 2 * (size_t)ng, stream);
+    if (st)
+        return st;
+    const double *pre[3] = { w, w + ng, w + 2 * (size_t)ng };
+    const double *post[3] = { w + 3 * (size_t)ng, w + 4 * (size_t)ng, w + 5 * (size_t)ng };
+    double *out = sim->drag_history + 3 * (sim->drag_steps % sim->drag_history_len);
+    const cudaError_t e = vfb::drag_lift_sum(pre, post, ng, w + 6 * (size_t)ng, out, as_stream(stream));
+    ++sim->drag_steps;
+    return cuda_status(e, "drag/lift sum");
 }
 
 int vfb_simulation_run(vfb_simulation *sim, uint32_t steps, void *stream)
@@ -580,7 +799,13 @@ int vfb_simulation_run(vfb_simulation *sim, uint32_t steps, void *stream)
             if (st)
                 return st;
         }
+        st = run_geometry_post(sim, stream);
+        if (st)
+            return st;
         L.is_even_timestep = !L.is_even_timestep;
+        st = run_geometry_pre(sim, stream);
+        if (st)
+            return st;
         for (size_t i = 0; i < sim->pressure.size(); ++i) {
             if (!sim->pressure_fn[i] || !sim->pressure[i].number_of_bc_nodes)
                 continue;
@@ -618,6 +843,7 @@ struct vfb_box {
     uint32_t ring_steps = 0;
     void *staging = nullptr;        // 4 real fields for init and output
     int *status = nullptr;          // device status word of the kernels (DeviceError)
+    uint64_t launches = 0;          // kernels this box has launched
 };
 
 namespace {
@@ -690,7 +916,7 @@ int vfb_box_create(const vfb_box_desc *d, vfb_box **out)
         s.lim[i] = d->quadric_limiters[i];
     b->blocks = vfb::box_blocks(s);
     if (e == cudaSuccess)
-        e = cudaMalloc((void **)&b->partials, 2 * b->blocks * sizeof(double));
+        e = cudaMalloc((void **)&b->partials, 2 * (b->blocks + vfb::kReduceMaxChunks) * sizeof(double));
     if (e == cudaSuccess)
         e = cudaMalloc((void **)&b->energy_ring, 2 * (size_t)kRingSteps * sizeof(double));
     b->ring_steps = kRingSteps;
@@ -702,6 +928,8 @@ int vfb_box_create(const vfb_box_desc *d, vfb_box **out)
         e = cudaMemset(b->status, 0, sizeof(int));
     s.status = b->status;
     s.variant = 0;
+    s.async_blocks_per_sm = 0;
+    s.async_smem_kb = 0;
     if (e != cudaSuccess) {
         box_free(b);
         delete b;
@@ -770,9 +998,11 @@ int vfb_box_step(vfb_box *box, uint32_t steps, double *energy, int32_t energy_on
             uint64_t n_partials = 0;
             e = VFB_DISPATCH(box->desc.storage, box->desc.arith,
                              LA::box_collide(box->state, box->even, partials, &n_partials, s));
+            ++box->launches;
             if (e == cudaSuccess && energy) {
                 double *dst = energy_on_host ? box->energy_ring + 2 * t : energy + 2 * (uint64_t)(done + t);
-                e = vfb::reduce_partials(box->partials, n_partials, dst, s);
+                e = vfb::reduce_partials_wide(box->partials, n_partials, box->partials + 2 * box->blocks, dst, s);
+                box->launches += n_partials > vfb::kReduceDirect ? 2 : 1;
             }
             box->even = !box->even;
         }
@@ -828,6 +1058,28 @@ int vfb_box_set_kernel_variant(vfb_box *box, int32_t variant)
     if (variant == 2 && box->desc.nx % 32 != 0)
         return fail(VFB_ERR_UNSUPPORTED, "the TMA-staged kernel needs nx % 32 == 0");
     box->state.variant = variant;
+    return VFB_OK;
+}
+
+int vfb_box_kernel_launches(const vfb_box *box, uint64_t *count)
+{
+    if (!box || !count)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    *count = box->launches;
+    return VFB_OK;
+}
+
+int vfb_box_set_launch_shape(vfb_box *box, int32_t blocks_per_sm, int32_t smem_kb)
+{
+    if (!box)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "box is NULL");
+    if (blocks_per_sm < 0 || blocks_per_sm > 8)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "blocks_per_sm must lie in [0, 8]");
+    static const int kb[] = { 0, 64, 100, 132, 164, 196, 228 };
+    if (std::find(std::begin(kb), std::end(kb), smem_kb) == std::end(kb))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "smem_kb must be 0, 64, 100, 132, 164, 196 or 228");
+    box->state.async_blocks_per_sm = blocks_per_sm;
+    box->state.async_smem_kb = smem_kb;
     return VFB_OK;
 }
 

@@ -1026,5 +1026,76 @@ __global__ void __launch_bounds__(128) scale_fc_kernel(ScaleArgs a)
             Codec<S>::store(coarse + (uint64_t)plane<COARSE_EVEN>(d) * a.n_coarse + nodes[shift_class(d)], f[d], d);
 }
 
+
+// ---------------------------------------------------------------------------------------------
+// drag and lift by momentum exchange (PostProcessor/DragLift.cu:50-555)
+// ---------------------------------------------------------------------------------------------
+struct DragArgs {
+    const void *dist;
+    uint64_t n;
+    const uint32_t *nbx, *nby, *nbz;
+    const int32_t *k;           // geometry BC node indices
+    const void *q27;            // q27[dir * nbc + i], compute type
+    uint32_t nbc;
+    double *dx, *dy, *dz;       // per node
+};
+
+// the pairs of the reference's bracket structure, per axis: four corner pairs, four edge pairs,
+// the face pair; each (plus direction, minus direction)
+__device__ __forceinline__ int drag_pair(int axis, int i, int side)
+{
+    constexpr int P[3][9][2] = {
+        { { 25, 20 }, { 23, 22 }, { 21, 24 }, { 19, 26 }, { 13, 14 }, { 11, 12 }, { 9, 10 }, { 7, 8 }, { 1, 2 } },
+        { { 20, 25 }, { 23, 22 }, { 24, 21 }, { 19, 26 }, { 17, 18 }, { 15, 16 }, { 10, 9 }, { 7, 8 }, { 3, 4 } },
+        { { 20, 25 }, { 22, 23 }, { 21, 24 }, { 19, 26 }, { 18, 17 }, { 15, 16 }, { 14, 13 }, { 11, 12 }, { 5, 6 } }
+    };
+    return P[axis][i][side];
+}
+
+// minus the momentum sum of one axis, in double, with the reference's association:
+// ((((c1 + c2) + c3) + c4) + (((e1 + e2) + e3) + e4)) + face, each term (f_p on_p) - (f_m on_m)
+__device__ __forceinline__ double drag_axis(const double (&f)[27], const double (&on)[27], int axis)
+{
+    double t[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const int p = drag_pair(axis, i, 0), m = drag_pair(axis, i, 1);
+        t[i] = (f[p] * on[p]) - (f[m] * on[m]);
+    }
+    return -(((((t[0] + t[1]) + t[2]) + t[3]) + (((t[4] + t[5]) + t[6]) + t[7])) + t[8]);
+}
+
+// DragLiftPost27 (PRE = false): after the collision, the post-collision populations leaving the
+// node along each cut link d (q_d in [0, 1]). DragLiftPre27 (PRE = true): after the parity swap,
+// the pre-collision populations the node reads next, each weighted by the cut link of the opposite
+// direction.
+template <class S, bool EVEN, bool PRE>
+__global__ void __launch_bounds__(128) drag_lift_kernel(DragArgs a)
+{
+    using C = typename Codec<S>::compute;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nbc)
+        return;
+    uint32_t nodes[8];
+    list_nodes((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, nodes);
+    const S *base = static_cast<const S *>(a.dist);
+    C fc[27];
+    if constexpr (PRE)
+        gather_pre<S, EVEN>(base, a.n, nodes, fc);
+    else
+        gather_post<S, EVEN>(base, a.n, nodes, fc);
+    const C *q = static_cast<const C *>(a.q27);
+    double f[27], on[27];
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        f[d] = (double)fc[d];
+        const C qd = q[(uint64_t)(PRE ? inv(d) : d) * a.nbc + i];
+        on[d] = (qd >= C(0) && qd <= C(1)) ? 1.0 : 0.0;
+    }
+    a.dx[i] = drag_axis(f, on, 0);
+    a.dy[i] = drag_axis(f, on, 1);
+    a.dz[i] = drag_axis(f, on, 2);
+}
+
 } // namespace VFB_NS
 } // namespace vfb

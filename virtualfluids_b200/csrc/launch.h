@@ -25,6 +25,8 @@ struct BoxState {
     double fx, fy, fz;            // half acceleration
     double lim[3];
     int variant;                  // 0: choose, 1: direct loads, 2: TMA-staged (nx % 32 == 0), 3: async copies
+    int async_blocks_per_sm;      // async kernel: resident blocks per SM (0: 3)
+    int async_smem_kb;            // async kernel: shared-memory configuration to pad to (0: carve-out hint only)
     int *status;                  // device status word (DeviceError), nullable
 };
 
@@ -58,6 +60,8 @@ inline uint64_t box_blocks(const BoxState &b)
                                     const void *uz, cudaStream_t s);                                               \
         static cudaError_t box_macros(const BoxState &b, bool even, void *rho, void *ux, void *uy, void *uz,       \
                                       cudaStream_t s);                                                             \
+        static cudaError_t drag_lift(const vfb_level *L, const vfb_bc *bc, bool pre, double *dx, double *dy,        \
+                                     double *dz, cudaStream_t s);                                                  \
         static cudaError_t scale(const vfb_level *coarse, const vfb_level *fine, const vfb_interpolation_cells *cells, \
                                  const vfb_interpolation_cell_neighbor *offsets, bool fine_to_coarse, cudaStream_t s); \
     };
@@ -77,5 +81,14 @@ void set_last_error(const char *msg);
 
 // deterministic reduction of per-block {mass, energy} partials into out[2] (device)
 cudaError_t reduce_partials(const double *partials, uint64_t blocks, double *out, cudaStream_t s);
+// calcDragLift's sum of pre - post over n nodes (x, y, z arrays of n doubles each) into out[3]
+// on the device; scratch holds 3 * ceil(n / 256) doubles; a fixed order for a given n
+cudaError_t drag_lift_sum(const double *const pre[3], const double *const post[3], uint32_t n, double *scratch,
+                          double *out, cudaStream_t s);
+
+// the same for many partials: up to kReduceMaxChunks blocks reduce contiguous chunks into scratch
+// (2 * kReduceMaxChunks doubles), one block reduces those; a fixed order for a given count
+constexpr uint64_t kReduceDirect = 8192, kReduceMaxChunks = 1024;
+cudaError_t reduce_partials_wide(const double *partials, uint64_t blocks, double *scratch, double *out, cudaStream_t s);
 
 } // namespace vfb

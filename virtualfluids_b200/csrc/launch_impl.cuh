@@ -149,6 +149,36 @@ cudaError_t Launchers<S>::pressure(const vfb_level *L, const vfb_directional_bc 
 }
 
 template <class S>
+cudaError_t Launchers<S>::drag_lift(const vfb_level *L, const vfb_bc *bc, bool pre, double *dx, double *dy, double *dz,
+                                    cudaStream_t s)
+{
+    if (bc->number_of_bc_nodes == 0)
+        return cudaSuccess;
+    DragArgs a;
+    a.dist = L->distributions;
+    a.n = L->number_of_nodes;
+    a.nbx = L->neighbor_x;
+    a.nby = L->neighbor_y;
+    a.nbz = L->neighbor_z;
+    a.k = bc->k;
+    a.q27 = bc->q27;
+    a.nbc = bc->number_of_bc_nodes;
+    a.dx = dx;
+    a.dy = dy;
+    a.dz = dz;
+    const unsigned B = 128, G = grid1d(a.nbc, B);
+    const bool even = L->is_even_timestep != 0;
+    if (pre) {
+        if (even) drag_lift_kernel<S, true, true><<<G, B, 0, s>>>(a);
+        else drag_lift_kernel<S, false, true><<<G, B, 0, s>>>(a);
+    } else {
+        if (even) drag_lift_kernel<S, true, false><<<G, B, 0, s>>>(a);
+        else drag_lift_kernel<S, false, false><<<G, B, 0, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+template <class S>
 cudaError_t Launchers<S>::scale(const vfb_level *coarse, const vfb_level *fine, const vfb_interpolation_cells *cells,
                                 const vfb_interpolation_cell_neighbor *offsets, bool fine_to_coarse, cudaStream_t s)
 {
@@ -298,67 +328,66 @@ cudaError_t launch_box_tma(const BoxCollideArgs<typename Codec<S>::compute> &a, 
         *n_partials = (uint64_t)grid;
     return cudaGetLastError();
 }
-// Three resident blocks per SM: with four (possible when the compiler needs no more than 128
-// registers) the 4 x 55 KB of staging leave almost no L1 and the kernel runs ~25 % slower on B200.
-// Each block therefore asks for a third of the smallest shared-memory configuration that holds
-// three blocks' staging (padding the dynamic allocation), so a fourth block never fits whatever
-// configuration the driver picks, and the carve-out asks for that configuration, leaving the rest
-// of the SM's 256 KB to L1.
+// Resident blocks per SM and the shared-memory configuration of the persistent async kernel.
+// Every block holds 2 x 27 x 128 populations of staging (55 KB in F64). By default three blocks
+// run per SM and the carve-out only hints at the configuration that holds three blocks' staging,
+// leaving the rest to L1 (four blocks, possible when the compiler needs no more than 128
+// registers, leave almost no L1). With an explicit configuration (smem_kb) each block pads its
+// dynamic allocation to a share of it, so no more than the asked number of blocks can be resident
+// whatever configuration the driver picks; the box autotuner chooses among such shapes.
 constexpr int kAsyncBlocksPerSm = 3;
 
 struct AsyncLaunchShape {
-    int blocks_per_sm;
-    int dyn_smem;
+    int target_bps = -1, target_kb = -1;   // the request the cached shape was made for
+    int blocks_per_sm = 0;
+    int dyn_smem = 0;
 };
 
-// shared-memory capacities (KB) an SM of compute capability 10.0 can be configured to
-inline int smem_config_bytes(int need)
-{
-    static const int kb[] = { 0, 8, 16, 32, 64, 100, 132, 164, 196, 228 };
-    for (int c : kb)
-        if (c * 1024 >= need)
-            return c * 1024;
-    return 228 * 1024;
-}
-
 template <class K>
-cudaError_t async_launch_shape(K kern, size_t smem, AsyncLaunchShape &out)
+cudaError_t async_launch_shape(K kern, size_t smem, int bps, int cfg_kb, AsyncLaunchShape &out)
 {
     int dev = 0, max_smem = 0, reserved = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
     cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const int cfg = std::min(smem_config_bytes(kAsyncBlocksPerSm * ((int)smem + reserved)), max_smem);
-    int dyn = (cfg / kAsyncBlocksPerSm - reserved) & ~127;
-    dyn = std::max(dyn, (int)smem);
-    if (optin > 0)
-        dyn = std::min(dyn, optin);
+    int dyn = (int)smem, cfg = bps * ((int)smem + reserved);
+    if (cfg_kb > 0) {
+        cfg = std::min(cfg_kb * 1024, max_smem);
+        dyn = std::max((int)smem, (cfg / bps - reserved) & ~127);
+        if (optin > 0)
+            dyn = std::min(dyn, optin);
+    }
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
     if (e != cudaSuccess)
         return e;
     if (max_smem > 0)
         cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
                              std::min(100, (cfg * 100 + max_smem - 1) / max_smem));
-    int bps = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, 128, dyn);
+    int occ = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 128, dyn);
     if (e != cudaSuccess)
         return e;
-    out.blocks_per_sm = std::max(1, std::min(bps, kAsyncBlocksPerSm));
+    out.blocks_per_sm = std::max(1, std::min(occ, bps));
     out.dyn_smem = dyn;
     return cudaSuccess;
 }
 
 template <class S, bool E, bool M, bool N>
-cudaError_t launch_box_async(const BoxCollideArgs<typename Codec<S>::compute> &a, uint64_t *n_partials, cudaStream_t s)
+cudaError_t launch_box_async(const BoxCollideArgs<typename Codec<S>::compute> &a, int bps, int cfg_kb,
+                             uint64_t *n_partials, cudaStream_t s)
 {
     auto kern = k17_box_async_kernel<S, VFB_EXACT, E, M, N>;
-    static AsyncLaunchShape shape = { -1, 0 };
-    if (shape.blocks_per_sm < 0) {
+    static AsyncLaunchShape shape;
+    if (bps <= 0)
+        bps = kAsyncBlocksPerSm;
+    if (shape.target_bps != bps || shape.target_kb != cfg_kb) {
         AsyncLaunchShape sh;
-        const cudaError_t e = async_launch_shape(kern, AsyncTile<S>::SMEM, sh);
+        const cudaError_t e = async_launch_shape(kern, AsyncTile<S>::SMEM, bps, cfg_kb, sh);
         if (e != cudaSuccess)
             return e;
+        sh.target_bps = bps;
+        sh.target_kb = cfg_kb;
         shape = sh;
     }
     const int64_t ntiles = (int64_t)((a.nx + AsyncTile<S>::BX - 1) / AsyncTile<S>::BX) * a.ny * a.nz;
@@ -378,8 +407,8 @@ cudaError_t Launchers<S>::box_collide(const BoxState &b, bool even, double *part
     a.energy_partials = partials;
     const bool mask = b.mask != nullptr, energy = partials != nullptr;
     if constexpr (sizeof(S) >= 4) {
-        if (b.variant == 3 || b.variant == 0) {
-#define VFB_K17A(E, M, N) return launch_box_async<S, E, M, N>(a, n_partials, s)
+        if (b.variant == 3) {
+#define VFB_K17A(E, M, N) return launch_box_async<S, E, M, N>(a, b.async_blocks_per_sm, b.async_smem_kb, n_partials, s)
         if (even) {
             if (mask && energy) VFB_K17A(true, true, true);
             else if (mask) VFB_K17A(true, true, false);
