@@ -397,12 +397,30 @@ void orc_mass_energy(const orc_level *L, const uint32_t *idx, uint32_t n_idx, in
     out[1] = ekin;
 }
 
-/* UpdateGrid27::updateGrid for one level (UpdateGrid27.cpp:54-95): collision, post-collision
-   velocity then no-slip BCs, parity toggle, pre-collision pressure BCs */
-int orc_run(orc_level *L, const uint32_t *fluid, uint32_t n_fluid, int *is_even, double omega, const double lim[3],
-            const double forces[3], const orc_velocity *vel, const orc_noslip *ns, const orc_pressure *pr, int n_pr,
-            int steps, int n_threads)
+static void run_noslip(orc_level *L, const orc_noslip *ns, int is_even, double omega)
 {
+    if (!ns || !ns->n)
+        return;
+    if (ns->kind == 1)
+        orc_bc_noslip_bounce_back(L, ns->k, ns->q, ns->n, is_even);
+    else if (ns->kind == 2)
+        orc_bc_noslip_interpolated(L, ns->k, ns->q, ns->n, is_even, omega);
+}
+
+/* UpdateGrid27::updateGrid for one level (UpdateGrid27.cpp:54-95, postCollisionBC :227-252,
+   preCollisionBC :288-300): collision; velocity, no-slip and geometry BCs (with the drag's post part
+   before the geometry BC); parity toggle; the drag's pre part and sum; pressure BCs */
+int orc_run_geo(orc_level *L, const uint32_t *fluid, uint32_t n_fluid, int *is_even, double omega, const double lim[3],
+                const double forces[3], const orc_velocity *vel, const orc_noslip *ns, const orc_noslip *geo,
+                double *drag_history, const orc_pressure *pr, int n_pr, int steps, int n_threads)
+{
+    const uint32_t ng = geo ? geo->n : 0;
+    double *work = NULL;
+    if (drag_history && ng) {
+        work = (double *)malloc(sizeof(double) * 6 * ng);
+        if (!work)
+            return -1;
+    }
     for (int t = 0; t < steps; ++t) {
         orc_collision(L, fluid, n_fluid, *is_even, omega, lim, forces, 0, NULL, NULL, NULL, NULL, n_threads);
         if (vel && vel->n) {
@@ -411,17 +429,28 @@ int orc_run(orc_level *L, const uint32_t *fluid, uint32_t n_fluid, int *is_even,
             else if (vel->kind == 2)
                 orc_bc_velocity_interpolated(L, vel->k, vel->q, vel->n, *is_even, omega, vel->ux, vel->uy, vel->uz);
         }
-        if (ns && ns->n) {
-            if (ns->kind == 1)
-                orc_bc_noslip_bounce_back(L, ns->k, ns->q, ns->n, *is_even);
-            else if (ns->kind == 2)
-                orc_bc_noslip_interpolated(L, ns->k, ns->q, ns->n, *is_even, omega);
-        }
+        run_noslip(L, ns, *is_even, omega);
+        if (work)
+            orc_drag_lift_post(L, geo->k, geo->q, ng, *is_even, work + 3 * ng, work + 4 * ng, work + 5 * ng);
+        run_noslip(L, geo, *is_even, omega);
         *is_even = !*is_even;
+        if (work) {
+            orc_drag_lift_pre(L, geo->k, geo->q, ng, *is_even, work, work + ng, work + 2 * ng);
+            orc_drag_lift_sum(work, work + ng, work + 2 * ng, work + 3 * ng, work + 4 * ng, work + 5 * ng, ng,
+                              drag_history + 3 * (size_t)t);
+        }
         for (int p = 0; p < n_pr; ++p)
             orc_bc_pressure_neq(L, pr[p].k, pr[p].kN, pr[p].rho, pr[p].n, *is_even, pr[p].direction);
     }
+    free(work);
     return 0;
+}
+
+int orc_run(orc_level *L, const uint32_t *fluid, uint32_t n_fluid, int *is_even, double omega, const double lim[3],
+            const double forces[3], const orc_velocity *vel, const orc_noslip *ns, const orc_pressure *pr, int n_pr,
+            int steps, int n_threads)
+{
+    return orc_run_geo(L, fluid, n_fluid, is_even, omega, lim, forces, vel, ns, NULL, NULL, pr, n_pr, steps, n_threads);
 }
 
 /* ---------------- refinement ---------------- */
@@ -684,4 +713,74 @@ void orc_scale_fc(orc_level *coarse, orc_level *fine, const uint32_t *coarse_cel
         orc_interp_point(coef, omega_coarse, 2.0, 0.0, 0.0, 0.0, 1, f);
         write_pre_all(coarse, coarse_cells[i], coarse_is_even, f);
     }
+}
+
+/* ---------------- drag and lift (PostProcessor/DragLift.cu, DragLift.cpp) ---------------- */
+
+/* the bracket structure of dragX / dragY / dragZ (DragLift.cu:264-290): per axis four corner pairs,
+   four edge pairs and the face pair, each pair (plus direction, minus direction) */
+static const int DRAG_PAIRS[3][9][2] = {
+    { { D_PMM, D_MPP }, { D_PPM, D_MMP }, { D_PMP, D_MPM }, { D_PPP, D_MMM },
+      { D_P0M, D_M0P }, { D_P0P, D_M0M }, { D_PM0, D_MP0 }, { D_PP0, D_MM0 }, { D_P00, D_M00 } },
+    { { D_MPP, D_PMM }, { D_PPM, D_MMP }, { D_MPM, D_PMP }, { D_PPP, D_MMM },
+      { D_0PM, D_0MP }, { D_0PP, D_0MM }, { D_MP0, D_PM0 }, { D_PP0, D_MM0 }, { D_0P0, D_0M0 } },
+    { { D_MPP, D_PMM }, { D_MMP, D_PPM }, { D_PMP, D_MPM }, { D_PPP, D_MMM },
+      { D_0MP, D_0PM }, { D_0PP, D_0MM }, { D_M0P, D_P0M }, { D_P0P, D_M0M }, { D_00P, D_00M } }
+};
+
+static double drag_axis(const double f[27], const double on[27], int axis)
+{
+    double t[9];
+    for (int i = 0; i < 9; ++i) {
+        const int p = DRAG_PAIRS[axis][i][0], m = DRAG_PAIRS[axis][i][1];
+        t[i] = (f[p] * on[p]) - (f[m] * on[m]);
+    }
+    return ((((t[0] + t[1]) + t[2]) + t[3]) + (((t[4] + t[5]) + t[6]) + t[7])) + t[8];
+}
+
+/* DragLiftPost27 (DragLift.cu:50-301): after the collision, minus the momentum of the populations
+   leaving each geometry node through its cut links (q in [0, 1]) */
+void orc_drag_lift_post(const orc_level *L, const int32_t *k, const double *q27, uint32_t nbc, int is_even,
+                        double *dx, double *dy, double *dz)
+{
+    for (uint32_t i = 0; i < nbc; ++i) {
+        double f[27], on[27];
+        read_post(L, (uint32_t)k[i], is_even, f);
+        for (int d = 0; d < 27; ++d)
+            on[d] = q_active(q27[(uint64_t)d * nbc + i]) ? 1.0 : 0.0;
+        dx[i] = -drag_axis(f, on, 0);
+        dy[i] = -drag_axis(f, on, 1);
+        dz[i] = -drag_axis(f, on, 2);
+    }
+}
+
+/* DragLiftPre27 (DragLift.cu:304-555): after the parity swap, the populations about to be read by
+   each geometry node, weighted by the cut link of the opposite direction */
+void orc_drag_lift_pre(const orc_level *L, const int32_t *k, const double *q27, uint32_t nbc, int is_even,
+                       double *dx, double *dy, double *dz)
+{
+    for (uint32_t i = 0; i < nbc; ++i) {
+        double f[27], on[27];
+        orc_read_pre(L, (uint32_t)k[i], is_even, f);
+        for (int d = 0; d < 27; ++d)
+            on[d] = q_active(q27[(uint64_t)ORC_INV[d] * nbc + i]) ? 1.0 : 0.0;
+        dx[i] = -drag_axis(f, on, 0);
+        dy[i] = -drag_axis(f, on, 1);
+        dz[i] = -drag_axis(f, on, 2);
+    }
+}
+
+/* calcDragLift (DragLift.cpp:52-73): the force as the node-ordered FP64 sum of pre - post */
+void orc_drag_lift_sum(const double *pre_x, const double *pre_y, const double *pre_z, const double *post_x,
+                       const double *post_y, const double *post_z, uint32_t nbc, double force[3])
+{
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    for (uint32_t i = 0; i < nbc; ++i) {
+        fx += pre_x[i] - post_x[i];
+        fy += pre_y[i] - post_y[i];
+        fz += pre_z[i] - post_z[i];
+    }
+    force[0] = fx;
+    force[1] = fy;
+    force[2] = fz;
 }

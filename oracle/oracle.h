@@ -117,6 +117,22 @@ void orc_scale_fc(orc_level *coarse, orc_level *fine, const uint32_t *coarse_cel
                   uint32_t n_cells, const double *ox, const double *oy, const double *oz, int coarse_is_even,
                   double omega_coarse, double omega_fine);
 
+/* drag and lift (PostProcessor/DragLift.cu:50-555, DragLift.cpp:52-73): per geometry BC node, the
+   post part (after the collision, current parity) and the pre part (after the parity swap); the
+   force is the node-ordered FP64 sum of pre - post */
+void orc_drag_lift_post(const orc_level *L, const int32_t *k, const double *q27, uint32_t nbc, int is_even,
+                        double *dx, double *dy, double *dz);
+void orc_drag_lift_pre(const orc_level *L, const int32_t *k, const double *q27, uint32_t nbc, int is_even,
+                       double *dx, double *dy, double *dz);
+void orc_drag_lift_sum(const double *pre_x, const double *pre_y, const double *pre_z, const double *post_x,
+                       const double *post_y, const double *post_z, uint32_t nbc, double force[3]);
+
+/* the step with a geometry BC list (no-slip kinds) and, when drag_history is given, the drag force
+   of every step into drag_history[3 * step] */
+int orc_run_geo(orc_level *L, const uint32_t *fluid, uint32_t n_fluid, int *is_even, double omega, const double lim[3],
+                const double forces[3], const orc_velocity *vel, const orc_noslip *ns, const orc_noslip *geo,
+                double *drag_history, const orc_pressure *pr, int n_pr, int steps, int n_threads);
+
 int orc_run(orc_level *L, const uint32_t *fluid, uint32_t n_fluid, int *is_even, double omega, const double lim[3],
             const double forces[3], const orc_velocity *vel, const orc_noslip *ns, const orc_pressure *pr, int n_pr,
             int steps, int n_threads);

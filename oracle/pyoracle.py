@@ -1,7 +1,8 @@
 """ORACLE — test infrastructure, not product code.
 
-ctypes binding of the plain-C oracle (liboracle.so, built by oracle/Makefile) and of the
-reference-header pins (_ref/libvfref64.so, _ref/libvfref32.so). Only the tests, the smoke check
+ctypes binding of the plain-C oracle (liboracle.so, built by oracle/Makefile), of the
+reference-header pins (_ref/libvfref64.so, _ref/libvfref32.so) and of the reference's own CUDA
+kernels (_ref/libvfref_gpu64.so, run on the GPU). Only the tests, the smoke check
 and the benchmark's CPU-baseline / reference legs use this module, and only as a checker or as
 the timed CPU baseline.
 """
@@ -18,6 +19,7 @@ HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
 REF64 = HERE / "_ref" / "libvfref64.so"
 REF32 = HERE / "_ref" / "libvfref32.so"
+REFGPU = HERE / "_ref" / "libvfref_gpu64.so"
 
 _P = C.c_void_p
 _lib = None
@@ -90,6 +92,27 @@ def ref32():
     return L
 
 
+def refgpu():
+    """The reference's own CUDA kernels (FP64, built from the reference tree), or None."""
+    if not REFGPU.exists():
+        return None
+    L = C.CDLL(str(REFGPU))
+    u, i, d, u64 = C.c_uint32, C.c_int, C.c_double, C.c_uint64
+    L.refgpu_k17.argtypes = [_P, u64, _P, _P, _P, _P, u, i, d, _P, _P, d]
+    L.refgpu_noslip_bounce_back.argtypes = [_P, _P, _P, u, _P, _P, _P, u64, i]
+    L.refgpu_noslip_interpolated.argtypes = [_P, _P, _P, u, d, _P, _P, _P, u64, i]
+    L.refgpu_velocity_bounce_back.argtypes = [_P, _P, _P, _P, _P, _P, u, _P, _P, _P, u64, i]
+    L.refgpu_velocity_interpolated.argtypes = [_P, _P, _P, _P, _P, _P, u, d, _P, _P, _P, u64, i]
+    L.refgpu_pressure_neq.argtypes = [_P, _P, _P, _P, i, _P, _P, _P, u64, i, i]
+    L.refgpu_init.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P, u, _P, i]
+    L.refgpu_macros.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P, _P, u64, _P, i]
+    L.refgpu_scale_cf.argtypes = [_P] * 8 + [u64, u64, i, _P, _P, u, d, d, _P, _P, _P]
+    L.refgpu_scale_fc.argtypes = [_P] * 8 + [u64, u64, i, _P, _P, u, d, d, _P, _P, _P]
+    L.refgpu_drag_lift_post.argtypes = [_P, _P, _P, i, _P, _P, _P, _P, _P, _P, u64, i]
+    L.refgpu_drag_lift_pre.argtypes = [_P, _P, _P, i, _P, _P, _P, _P, _P, _P, u64, i]
+    return L
+
+
 def ptr(a: np.ndarray):
     return C.c_void_p(a.ctypes.data) if a is not None else C.c_void_p(0)
 
@@ -113,7 +136,8 @@ class _Pressure(C.Structure):
 class OracleLevel:
     """A level in the reference layout, advanced on the host by the oracle."""
 
-    def __init__(self, grid, omega, lim=(0.01, 0.01, 0.01), forces=(0.0, 0.0, 0.0), velocity_kind=1, noslip_kind=1):
+    def __init__(self, grid, omega, lim=(0.01, 0.01, 0.01), forces=(0.0, 0.0, 0.0), velocity_kind=1, noslip_kind=1,
+                 geometry_kind=0, drag_lift=False):
         self.grid = grid
         self.n = grid.number_of_nodes
         self.f = np.zeros(27 * self.n, dtype=np.float64)
@@ -142,6 +166,15 @@ class OracleLevel:
             arrs = [np.ascontiguousarray(k.astype(np.int32)), np.ascontiguousarray(q.reshape(-1))]
             self._keep += arrs
             self.ns = _NoSlip(arrs[0].ctypes.data, arrs[1].ctypes.data, k.size, noslip_kind)
+        self.geo_bc = None
+        m = grid.merged("geometry")
+        if m is not None:
+            k, q, _ = m
+            arrs = [np.ascontiguousarray(k.astype(np.int32)), np.ascontiguousarray(q.reshape(-1))]
+            self._keep += arrs
+            self.geo_bc = _NoSlip(arrs[0].ctypes.data, arrs[1].ctypes.data, k.size, geometry_kind)
+        self.drag_lift = drag_lift and self.geo_bc is not None
+        self.drag_history = []
         from virtualfluids_b200.grid import SIDE_DIR
         pr = []
         for b in grid.bcs:
@@ -162,11 +195,17 @@ class OracleLevel:
         self.is_even.value = 1
 
     def run(self, steps, threads=0):
-        lib().orc_run.argtypes = [_P, _P, C.c_uint32, C.POINTER(C.c_int), C.c_double, _P, _P, _P, _P, _P, C.c_int,
-                                  C.c_int, C.c_int]
-        lib().orc_run(C.byref(self.L), ptr(self.fluid), self.fluid.size, C.byref(self.is_even), self.omega,
-                      ptr(self.lim), ptr(self.forces), C.byref(self.vel) if self.vel else None,
-                      C.byref(self.ns) if self.ns else None, self.pr, self.n_pr, int(steps), int(threads))
+        lib().orc_run_geo.argtypes = [_P, _P, C.c_uint32, C.POINTER(C.c_int), C.c_double, _P, _P, _P, _P, _P, _P, _P,
+                                      C.c_int, C.c_int, C.c_int]
+        hist = np.zeros((int(steps), 3)) if self.drag_lift else None
+        rc = lib().orc_run_geo(C.byref(self.L), ptr(self.fluid), self.fluid.size, C.byref(self.is_even), self.omega,
+                               ptr(self.lim), ptr(self.forces), C.byref(self.vel) if self.vel else None,
+                               C.byref(self.ns) if self.ns else None, C.byref(self.geo_bc) if self.geo_bc else None,
+                               ptr(hist) if hist is not None else None, self.pr, self.n_pr, int(steps), int(threads))
+        if rc != 0:
+            raise MemoryError("oracle step driver could not allocate its drag workspace")
+        if hist is not None:
+            self.drag_history.extend(hist)
 
     def macroscopic(self):
         out = [np.zeros(self.n) for _ in range(5)]

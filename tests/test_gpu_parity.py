@@ -176,3 +176,62 @@ def test_lid_driven_cavity_64_2000_steps(oracle, cuda, arith):
     else:
         assert max(errs.values()) <= 1e-6, errs
         assert abs(m1 - m2) <= 1e-12 * m2
+
+
+def _cube_channel(n=(24, 12, 12)):
+    """Channel with an interpolated velocity inlet, a pressure outlet, no-slip walls in z and a
+    box obstacle on the bottom wall whose faces lie between nodes (exact-geometry q)."""
+    g = ListGrid(*n, periodic=(False, True, False))
+    g.add_side("MZ", "noslip")
+    g.add_side("PZ", "noslip")
+    g.add_side("MX", "velocity", velocity=(0.02, 0.0, 0.0))
+    g.add_side("PX", "pressure", rho=0.0)
+    g.add_box_obstacle((7.3, 3.6, -0.5), (11.6, 7.8, 4.4))
+    bcf = BCF()
+    bcf.set_no_slip_boundary_condition(BCF.NoSlipBC.NoSlipInterpolatedCompressible)
+    bcf.set_velocity_boundary_condition(BCF.VelocityBC.VelocityInterpolatedCompressible)
+    bcf.set_pressure_boundary_condition(BCF.PressureBC.PressureNonEquilibriumCompressible)
+    bcf.set_geometry_boundary_condition(BCF.NoSlipBC.NoSlipInterpolatedCompressible)
+    return g, bcf
+
+
+@pytest.mark.parametrize("arith", [N.ARITH_EXACT, N.ARITH_FAST])
+def test_obstacle_geometry_bc_and_drag_lift(oracle, cuda, arith):
+    """Geometry BC (interpolated bounce-back on an obstacle) and the FP64 drag/lift of every step
+    (DragLiftPost27 / DragLiftPre27 / calcDragLift). Exact arithmetic gives bit-identical
+    populations; the per-step force is an FP64 sum formed in another order on the device, held to
+    1e-12 of its magnitude (exact) and to the FMA tolerance of the flow (fast)."""
+    g, bcf = _cube_channel()
+    steps = 60
+    sim = Simulation(make_para(1.8, N.STORAGE_F64, arith), g, bcf)
+    orc = oracle.OracleLevel(g, omega=sim.para.omega, velocity_kind=2, noslip_kind=2, geometry_kind=2, drag_lift=True)
+    sim.init()
+    orc.init()
+    sim.enable_drag_lift(history_steps=steps)
+    sim.run(steps)
+    orc.run(steps)
+    got = sim.drag_lift_history()
+    want = np.array(orc.drag_history)
+    assert got.shape == want.shape == (steps, 3)
+    assert want[-1, 0] > 0.0  # drag along the flow
+    scale = np.abs(want).max(axis=0)
+    if arith == N.ARITH_EXACT:
+        assert np.array_equal(sim.populations(), orc.f)
+        assert np.all(np.abs(got - want) <= 1e-12 * scale)
+    else:
+        assert np.all(np.abs(got - want) <= 1e-9 * scale)
+
+
+def test_drag_lift_history_ring_keeps_the_last_steps(oracle, cuda):
+    g, bcf = _cube_channel()
+    sim = Simulation(make_para(1.8, N.STORAGE_F64, N.ARITH_EXACT), g, bcf)
+    orc = oracle.OracleLevel(g, omega=sim.para.omega, velocity_kind=2, noslip_kind=2, geometry_kind=2, drag_lift=True)
+    sim.init()
+    orc.init()
+    sim.enable_drag_lift(history_steps=7)
+    sim.run(10)
+    sim.run(5)
+    orc.run(15)
+    got = sim.drag_lift_history()
+    want = np.array(orc.drag_history)[-7:]
+    assert np.all(np.abs(got - want) <= 1e-12 * np.abs(want).max(axis=0))

@@ -40,7 +40,7 @@ SIDE_DIR = {"MX": N.DIR_M00, "PX": N.DIR_P00, "MY": N.DIR_0M0, "PY": N.DIR_0P0, 
 @dataclass
 class SideBC:
     side: str
-    kind: str                       # "noslip", "velocity", "pressure"
+    kind: str                       # "noslip", "velocity", "pressure", "geometry"
     k: np.ndarray                   # int32 node indices
     q: np.ndarray                   # float64 [27, n]
     velocity: tuple = (0.0, 0.0, 0.0)
@@ -166,6 +166,51 @@ class ListGrid:
             bc.k_neighbor = self.node_index(*inward).astype(np.int32)
         self.bcs.append(bc)
         self._bc_sides_set.append(side)
+        return bc
+
+    # -- obstacles (GridImp::calculateQs, GridImp.cpp:1561) ---------------------------------
+    def add_box_obstacle(self, lo, hi, kind="geometry"):
+        """An axis-aligned solid box [lo, hi] (fluid-box coordinates; faces may lie between nodes).
+
+        Nodes inside become solid and leave the fluid list. Every fluid node with a link d whose
+        end node lies inside gets q_d = the ray parameter t in (0, 1] at which p + t c_d enters the
+        box (exact ray-box intersection); such nodes form a BC list of the given kind, by default
+        the geometry BC (Parameter's geometryBC)."""
+        lo = np.asarray(lo, dtype=np.float64)
+        hi = np.asarray(hi, dtype=np.float64)
+        c = self.coords.astype(np.float64)
+        inside = np.ones(self.number_of_nodes, dtype=bool)
+        for a in range(3):
+            inside &= (c[a] >= lo[a]) & (c[a] <= hi[a])
+        inside[0] = False
+        was_fluid = self.geo == N.GEO_FLUID
+        solid = inside & was_fluid
+        self.geo = np.where(solid, N.GEO_SOLID, self.geo).astype(np.uint32)
+        self.fluid = np.nonzero(self.geo == N.GEO_FLUID)[0].astype(np.uint32)
+        for b in self.bcs:
+            keep = ~solid[b.k]
+            b.k, b.q = b.k[keep], b.q[:, keep]
+            if b.k_neighbor is not None:
+                b.k_neighbor = b.k_neighbor[keep]
+        nodes = self.fluid.astype(np.int64)
+        x, y, z = (self.coords[a, nodes] for a in range(3))
+        q = np.full((27, nodes.size), -1.0)
+        for d in range(1, 27):
+            ex, ey, ez = self._neighbour_coords(x, y, z, d)
+            hit = (ex >= lo[0]) & (ex <= hi[0]) & (ey >= lo[1]) & (ey <= hi[1]) & (ez >= lo[2]) & (ez <= hi[2])
+            if not hit.any():
+                continue
+            t = np.zeros(nodes.size)
+            for a, (p, cd) in enumerate(((x, CX[d]), (y, CY[d]), (z, CZ[d]))):
+                if cd == 0:
+                    continue
+                face = lo[a] if cd > 0 else hi[a]
+                ta = (face - p) / cd
+                t = np.maximum(t, np.where((p < lo[a]) | (p > hi[a]), ta, 0.0))
+            q[d] = np.where(hit, np.clip(t, 0.0, 1.0), -1.0)
+        cut = (q >= 0).any(axis=0)
+        bc = SideBC(side="obstacle", kind=kind, k=nodes[cut].astype(np.int32), q=q[:, cut])
+        self.bcs.append(bc)
         return bc
 
     def merged(self, kind):

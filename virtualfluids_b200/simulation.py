@@ -104,6 +104,7 @@ class BoundaryConditionFactory:
         self.velocity = self.VelocityBC.NotSpecified
         self.noslip = self.NoSlipBC.NoSlipDelayBounceBack
         self.pressure = self.PressureBC.NotSpecified
+        self.geometry = self.NoSlipBC.NoSlipDelayBounceBack
 
     def set_velocity_boundary_condition(self, v):
         self.velocity = self.VelocityBC(v)
@@ -113,6 +114,10 @@ class BoundaryConditionFactory:
 
     def set_pressure_boundary_condition(self, v):
         self.pressure = self.PressureBC(v)
+
+    def set_geometry_boundary_condition(self, v):
+        """setGeometryBoundaryCondition with a NoSlipBC value (the no-slip kernels on the geometry list)."""
+        self.geometry = self.NoSlipBC(v)
 
     def velocity_function(self):
         fn = C.c_void_p()
@@ -241,7 +246,7 @@ class Simulation:
         self.level = L
         self._keep = []
         self._bcs = {}
-        for kind in ("velocity", "noslip"):
+        for kind in ("velocity", "noslip", "geometry"):
             m = grid.merged(kind)
             if m is None:
                 continue
@@ -270,6 +275,9 @@ class Simulation:
             N.check(N.lib().vfb_simulation_set_velocity_bc(sim, C.byref(self._bcs["velocity"]), int(bc_factory.velocity)))
         if "noslip" in self._bcs:
             N.check(N.lib().vfb_simulation_set_noslip_bc(sim, C.byref(self._bcs["noslip"]), int(bc_factory.noslip)))
+        if "geometry" in self._bcs:
+            N.check(N.lib().vfb_simulation_set_geometry_bc(sim, C.byref(self._bcs["geometry"]), int(bc_factory.geometry)))
+        self._drag = None
         for p in self._pressure:
             N.check(N.lib().vfb_simulation_add_pressure_bc(sim, C.byref(p), int(bc_factory.pressure)))
         N.check(N.lib().vfb_simulation_check(sim))
@@ -303,6 +311,7 @@ class Simulation:
 
     def run(self, steps: int):
         N.check(N.lib().vfb_simulation_run(self._sim, int(steps), None))
+        self._drag_steps = getattr(self, "_drag_steps", 0) + int(steps) if self._drag is not None else 0
         ev = C.c_int32()
         N.check(N.lib().vfb_simulation_is_even_timestep(self._sim, C.byref(ev)))
         self.level.is_even_timestep = ev.value
@@ -322,6 +331,31 @@ class Simulation:
         N.check(N.lib().vfb_mass_energy(C.byref(self.level), _ptr(self.fluid), int(self.grid.fluid.size),
                                         C.c_void_p(ws.data_ptr()), nbytes, out, None))
         return out[0], out[1]
+
+    def enable_drag_lift(self, history_steps: int):
+        """Parameter::setCalcDragLift: the drag/lift force on the geometry every step, kept on the
+        device for the last history_steps steps."""
+        t = _torch()
+        if "geometry" not in self._bcs:
+            raise N.VfbError(N.VFB_ERR_INVALID_ARGUMENT, "drag and lift need a geometry boundary condition")
+        ng = int(self._bcs["geometry"].number_of_bc_nodes)
+        nbytes = N.lib().vfb_simulation_drag_lift_workspace_bytes(ng)
+        ws = t.zeros((nbytes + 7) // 8, dtype=t.float64, device=self.device)
+        hist = t.zeros(3 * int(history_steps), dtype=t.float64, device=self.device)
+        N.check(N.lib().vfb_simulation_set_drag_lift(self._sim, C.c_void_p(ws.data_ptr()), nbytes,
+                                                     C.c_void_p(hist.data_ptr()), int(history_steps)))
+        self._drag = (ws, hist, int(history_steps), 0)
+
+    def drag_lift_history(self):
+        """(steps, 3) forces of the steps run since drag/lift was enabled (the last history_steps)."""
+        ws, hist, length, _ = self._drag
+        N.check(N.lib().vfb_synchronize(None))
+        h = hist.view(length, 3).cpu().numpy()
+        done = self._drag_steps
+        if done <= length:
+            return h[:done].copy()
+        start = done % length
+        return np.concatenate([h[start:], h[:start]])
 
     def populations(self):
         N.check(N.lib().vfb_synchronize(None))
