@@ -325,6 +325,67 @@ int vfb_box_set_launch_shape(vfb_box *box, int32_t blocks_per_sm, int32_t smem_k
 /* raw access to the population planes for checks: pointer, plane pitch (elements), parity */
 int vfb_box_populations(const vfb_box *box, void **dist, uint64_t *pitch, int32_t *is_even);
 
+/* ---- (2c) domain pools: batches of independent boxes in one persistent launch ---------------
+   No counterpart in the reference (one level of one domain per Simulation there). A pool owns one
+   device arena sized at creation; domains of uneven sizes are carved from it and released again,
+   so a serving loop can admit solves against the HBM budget. Every step advances all active
+   domains with one persistent kernel that walks a work list of node blocks (domain, first node);
+   each domain computes exactly what a vfb_box of the same description computes. */
+typedef struct vfb_pool_desc {
+    int32_t storage;                  /* vfb_storage */
+    int32_t arith;                    /* vfb_arith */
+    uint64_t arena_bytes;             /* device bytes for populations and masks */
+    uint32_t max_domains;
+} vfb_pool_desc;
+typedef struct vfb_domain_desc {
+    int32_t nx, ny, nz;
+    int32_t periodic_x, periodic_y, periodic_z;  /* on a non-periodic axis the first and last layers
+                                                    are solid walls (NoSlipDelayBounceBack) */
+    double omega;
+    double forces[3];                 /* acceleration, applied as forces * 1/2 */
+    double quadric_limiters[3];
+} vfb_domain_desc;
+typedef struct vfb_pool vfb_pool;
+int vfb_pool_create(const vfb_pool_desc *desc, vfb_pool **out);
+int vfb_pool_destroy(vfb_pool *pool);
+/* device bytes one domain of this description takes in the arena (admission checks) */
+int vfb_pool_domain_bytes(const vfb_pool *pool, const vfb_domain_desc *desc, int32_t has_mask, uint64_t *bytes);
+/* carve a domain from the arena; mask (optional, host, nx*ny*nz bytes, nonzero = fluid) adds solid
+   nodes inside. VFB_ERR_OUT_OF_MEMORY when the arena has no room: nothing is changed then. The
+   domain takes part in steps once it is initialised. */
+int vfb_pool_add_domain(vfb_pool *pool, const vfb_domain_desc *desc, const uint8_t *mask, uint32_t *id);
+/* the domain stops taking part in steps; its arena range and id become reusable once the pool's
+   stream has drained (the next vfb_pool_step that changes the work list, or vfb_pool_synchronize).
+   All calls on one pool must use one stream. */
+int vfb_pool_remove_domain(vfb_pool *pool, uint32_t id);
+/* waits for the pool's stream and makes the ranges of removed domains reusable */
+int vfb_pool_synchronize(vfb_pool *pool, void *stream);
+/* equilibrium initialisation of both parities from drho, ux, uy, uz (real[nx*ny*nz], host when
+   from_host, else device); activates the domain. Host fields pass through a staging buffer the
+   pool keeps outside the arena (grown when a larger domain than before is staged). */
+int vfb_pool_init_domain(vfb_pool *pool, uint32_t id, const void *rho, const void *ux, const void *uy, const void *uz,
+                         int32_t from_host, void *stream);
+/* advance every active domain by `steps` time steps (one persistent launch per step; with the
+   graph option the launches of 16 steps are replayed from one captured CUDA graph) */
+int vfb_pool_step(vfb_pool *pool, uint32_t steps, void *stream);
+/* drho, ux, uy, uz (real[nx*ny*nz]) of one domain, to host or device memory */
+int vfb_pool_domain_fields(vfb_pool *pool, uint32_t id, void *rho, void *ux, void *uy, void *uz, int32_t to_host,
+                           void *stream);
+/* launch shape: threads per block (64, 128 or 256), nodes per thread per work item (1..8), resident
+   blocks per SM (0 = as many as fit), CUDA-graph replay (0/1) */
+int vfb_pool_set_launch(vfb_pool *pool, int32_t threads_per_block, int32_t nodes_per_thread, int32_t blocks_per_sm,
+                        int32_t use_graph);
+int vfb_pool_get_launch(const vfb_pool *pool, int32_t out4[4]);
+/* the autotuner: times trial_steps steps of the current domains for each launch shape of a fixed
+   candidate set and keeps the fastest (results do not depend on the shape). It advances the active
+   domains by the steps it runs: call it before initialising them, or accept the extra steps. */
+int vfb_pool_autotune(vfb_pool *pool, uint32_t trial_steps, void *stream, double *best_ms_per_step);
+/* active domains, their nodes, and arena bytes in use / free */
+int vfb_pool_stats(const vfb_pool *pool, uint32_t *active_domains, uint64_t *active_nodes, uint64_t *used_bytes,
+                   uint64_t *free_bytes);
+/* kernels the pool has launched (graph replays count their kernels) */
+int vfb_pool_kernel_launches(const vfb_pool *pool, uint64_t *count);
+
 #ifdef __cplusplus
 }
 #endif

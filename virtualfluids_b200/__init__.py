@@ -13,8 +13,9 @@ from . import _native
 from ._native import VfbError, lib
 from .box import Box
 from .grid import ListGrid
+from .pool import Pool
 from .simulation import (BoundaryConditionFactory, GridScalingFactory, InterpolationCells, Parameter, Simulation,
                          scale_coarse_to_fine, scale_fine_to_coarse)
 
-__all__ = ["Box", "BoundaryConditionFactory", "GridScalingFactory", "InterpolationCells", "ListGrid", "Parameter",
+__all__ = ["Box", "BoundaryConditionFactory", "GridScalingFactory", "InterpolationCells", "ListGrid", "Parameter", "Pool",
            "Simulation", "VfbError", "lib", "scale_coarse_to_fine", "scale_fine_to_coarse", "_native"]

@@ -97,6 +97,16 @@ class BoxDesc(C.Structure):
                 ("forces", C.c_double * 3), ("quadric_limiters", C.c_double * 3), ("mask", C.c_void_p)]
 
 
+class PoolDesc(C.Structure):
+    _fields_ = [("storage", C.c_int32), ("arith", C.c_int32), ("arena_bytes", C.c_uint64), ("max_domains", C.c_uint32)]
+
+
+class DomainDesc(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+                ("periodic_x", C.c_int32), ("periodic_y", C.c_int32), ("periodic_z", C.c_int32),
+                ("omega", C.c_double), ("forces", C.c_double * 3), ("quadric_limiters", C.c_double * 3)]
+
+
 BC_FN = C.CFUNCTYPE(C.c_int, C.POINTER(Level), C.POINTER(BC), C.c_void_p)
 DBC_FN = C.CFUNCTYPE(C.c_int, C.POINTER(Level), C.POINTER(DirectionalBC), C.c_void_p)
 
@@ -164,6 +174,23 @@ SIGNATURES = {
     "vfb_box_set_launch_shape": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "vfb_box_populations": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64),
                                       C.POINTER(C.c_int32)]),
+    "vfb_pool_create": (C.c_int, [C.POINTER(PoolDesc), C.POINTER(C.c_void_p)]),
+    "vfb_pool_destroy": (C.c_int, [C.c_void_p]),
+    "vfb_pool_domain_bytes": (C.c_int, [C.c_void_p, C.POINTER(DomainDesc), C.c_int32, C.POINTER(C.c_uint64)]),
+    "vfb_pool_add_domain": (C.c_int, [C.c_void_p, C.POINTER(DomainDesc), C.c_void_p, C.POINTER(C.c_uint32)]),
+    "vfb_pool_remove_domain": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "vfb_pool_synchronize": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "vfb_pool_init_domain": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_int32, C.c_void_p]),
+    "vfb_pool_step": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p]),
+    "vfb_pool_domain_fields": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_int32, C.c_void_p]),
+    "vfb_pool_set_launch": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "vfb_pool_get_launch": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "vfb_pool_autotune": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(C.c_double)]),
+    "vfb_pool_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                 C.POINTER(C.c_uint64)]),
+    "vfb_pool_kernel_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
 }
 
 _lib = None

@@ -1097,5 +1097,76 @@ __global__ void __launch_bounds__(128) drag_lift_kernel(DragArgs a)
     a.dz[i] = drag_axis(f, on, 2);
 }
 
+
+// ---------------------------------------------------------------------------------------------
+// domain pool: thousands of independent boxes of uneven sizes advanced by one persistent launch
+// driven by a work list of node blocks
+// ---------------------------------------------------------------------------------------------
+template <class C>
+struct PoolDomain {
+    uint64_t dist_offset;        // elements from the arena start to plane 0 of this domain
+    uint64_t pitch;              // elements per direction plane
+    uint64_t mask_offset;        // bytes from the arena start to the node mask (nonzero = fluid)
+    int nx, ny, nz;
+    int flags;                   // bits 0-2: periodic x/y/z, bit 3: has a mask
+    K17Rates<C> rates;
+    C fx, fy, fz;                // half accelerations
+};
+
+enum : int { kPoolPeriodicX = 1, kPoolPeriodicY = 2, kPoolPeriodicZ = 4, kPoolMask = 8 };
+
+template <class C>
+struct PoolArgs {
+    void *arena;
+    const PoolDomain<C> *domains;
+    const uint2 *items;          // {domain, first local node} per node block
+    const uint32_t *n_items;     // device word, so a captured step keeps working after list changes
+    int nodes_per_thread;
+};
+
+template <class S, bool EXACT, bool EVEN>
+__global__ void __launch_bounds__(256) k17_pool_kernel(PoolArgs<typename Codec<S>::compute> a)
+{
+    using C = typename Codec<S>::compute;
+    const uint32_t n_items = __ldg(a.n_items);
+    const uint32_t span = blockDim.x * (uint32_t)a.nodes_per_thread;
+    for (uint32_t w = blockIdx.x; w < n_items; w += gridDim.x) {
+        const uint2 it = a.items[w];
+        const PoolDomain<C> &dm = a.domains[it.x];
+        const int nx = dm.nx, ny = dm.ny, nz = dm.nz, flags = dm.flags;
+        const uint32_t nodes_total = (uint32_t)nx * (uint32_t)ny * (uint32_t)nz;
+        S *base = static_cast<S *>(a.arena) + dm.dist_offset;
+        const uint8_t *mask = (flags & kPoolMask) ? static_cast<const uint8_t *>(a.arena) + dm.mask_offset : nullptr;
+        const uint32_t end = min(it.y + span, nodes_total);
+#pragma unroll 1
+        for (uint32_t k = it.y + threadIdx.x; k < end; k += blockDim.x) {
+            if (mask && __ldg(mask + k) == 0)
+                continue;
+            const uint32_t x = k % (uint32_t)nx, yz = k / (uint32_t)nx;
+            const uint32_t y = yz % (uint32_t)ny, z = yz / (uint32_t)ny;
+            const int xp = ((int)x + 1 < nx) ? (int)x + 1 : ((flags & kPoolPeriodicX) ? 0 : (int)x);
+            const int yp = ((int)y + 1 < ny) ? (int)y + 1 : ((flags & kPoolPeriodicY) ? 0 : (int)y);
+            const int zp = ((int)z + 1 < nz) ? (int)z + 1 : ((flags & kPoolPeriodicZ) ? 0 : (int)z);
+            const uint32_t sx = (uint32_t)(xp - (int)x);
+            const uint32_t sy = (uint32_t)((yp - (int)y) * nx);
+            const uint32_t sz = (uint32_t)((int64_t)(zp - (int)z) * nx * ny);
+            uint32_t nodes[8];
+            nodes[0] = k;
+            nodes[1] = k + sx;
+            nodes[2] = k + sy;
+            nodes[3] = k + sx + sy;
+            nodes[4] = k + sz;
+            nodes[5] = k + sx + sz;
+            nodes[6] = k + sy + sz;
+            nodes[7] = k + sx + sy + sz;
+            C f[27];
+            gather_pre<S, EVEN>(base, dm.pitch, nodes, f);
+            C drho, vx, vy, vz;
+            collide<C, EXACT>(f, dm.rates, dm.fx, dm.fy, dm.fz, drho, vx, vy, vz);
+            scatter_post<S, EVEN>(base, dm.pitch, nodes, f);
+        }
+    }
+}
+
 } // namespace VFB_NS
 } // namespace vfb

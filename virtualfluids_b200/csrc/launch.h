@@ -60,6 +60,14 @@ inline uint64_t box_blocks(const BoxState &b)
                                     const void *uz, cudaStream_t s);                                               \
         static cudaError_t box_macros(const BoxState &b, bool even, void *rho, void *ux, void *uy, void *uz,       \
                                       cudaStream_t s);                                                             \
+        static cudaError_t pool_collide(void *arena, const void *domains, const uint2 *items,                      \
+                                        const uint32_t *n_items, int nodes_per_thread, bool even, unsigned grid,   \
+                                        unsigned block, cudaStream_t s);                                           \
+        static const void *pool_kernel(bool even);                                                                \
+        static size_t pool_domain_bytes();                                                                        \
+        static void pool_domain(void *out, uint64_t dist_offset, uint64_t pitch, uint64_t mask_offset, int nx,     \
+                                int ny, int nz, int flags, double omega, const double lim[3],                      \
+                                const double half_force[3]);                                                       \
         static cudaError_t drag_lift(const vfb_level *L, const vfb_bc *bc, bool pre, double *dx, double *dy,        \
                                      double *dz, cudaStream_t s);                                                  \
         static cudaError_t scale(const vfb_level *coarse, const vfb_level *fine, const vfb_interpolation_cells *cells, \

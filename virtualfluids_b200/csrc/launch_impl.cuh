@@ -2,6 +2,7 @@
 // per-storage translation units, which explicitly instantiate one storage type each.
 #pragma once
 #include <algorithm>
+#include <cstring>
 
 #include "kernels.cuh"
 #include "launch.h"
@@ -146,6 +147,57 @@ cudaError_t Launchers<S>::pressure(const vfb_level *L, const vfb_directional_bc 
     if (L->is_even_timestep) bc_pressure_neq_kernel<S, true><<<G, B, 0, s>>>(a);
     else bc_pressure_neq_kernel<S, false><<<G, B, 0, s>>>(a);
     return cudaGetLastError();
+}
+
+template <class S>
+cudaError_t Launchers<S>::pool_collide(void *arena, const void *domains, const uint2 *items, const uint32_t *n_items,
+                                       int nodes_per_thread, bool even, unsigned grid, unsigned block, cudaStream_t s)
+{
+    using C = typename Codec<S>::compute;
+    PoolArgs<C> a;
+    a.arena = arena;
+    a.domains = static_cast<const PoolDomain<C> *>(domains);
+    a.items = items;
+    a.n_items = n_items;
+    a.nodes_per_thread = nodes_per_thread;
+    if (even) k17_pool_kernel<S, VFB_EXACT, true><<<grid, block, 0, s>>>(a);
+    else k17_pool_kernel<S, VFB_EXACT, false><<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <class S>
+const void *Launchers<S>::pool_kernel(bool even)
+{
+    return even ? reinterpret_cast<const void *>(k17_pool_kernel<S, VFB_EXACT, true>)
+                : reinterpret_cast<const void *>(k17_pool_kernel<S, VFB_EXACT, false>);
+}
+
+template <class S>
+size_t Launchers<S>::pool_domain_bytes()
+{
+    return sizeof(PoolDomain<typename Codec<S>::compute>);
+}
+
+// the domain record in the compute type of S, with the rates and forces rounded as the box path
+// rounds them (so a domain in the pool and the same box alone compute the same bits)
+template <class S>
+void Launchers<S>::pool_domain(void *out, uint64_t dist_offset, uint64_t pitch, uint64_t mask_offset, int nx, int ny,
+                               int nz, int flags, double omega, const double lim[3], const double half_force[3])
+{
+    using C = typename Codec<S>::compute;
+    PoolDomain<C> d;
+    d.dist_offset = dist_offset;
+    d.pitch = pitch;
+    d.mask_offset = mask_offset;
+    d.nx = nx;
+    d.ny = ny;
+    d.nz = nz;
+    d.flags = flags;
+    d.rates = rates_of<C>(omega, lim);
+    d.fx = (C)half_force[0];
+    d.fy = (C)half_force[1];
+    d.fz = (C)half_force[2];
+    std::memcpy(out, &d, sizeof(d));
 }
 
 template <class S>

@@ -1,0 +1,142 @@
+"""Domain pools: many independent boxes of uneven sizes advanced together (``vfb_pool_*``).
+
+A pool owns one device arena sized at creation. Domains are carved from it and released again,
+so a request loop can admit solves against an HBM budget; every step advances all active domains
+with one persistent kernel over a work list of node blocks, replayed from a captured CUDA graph.
+Each domain computes exactly what a :class:`~virtualfluids_b200.box.Box` of the same description
+computes. No counterpart in the reference, which runs one domain per simulation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+
+_STORAGE = {"f64": N.STORAGE_F64, "f32": N.STORAGE_F32, "f16": N.STORAGE_F16, "bf16": N.STORAGE_BF16}
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        return None
+    if isinstance(stream, C.c_void_p):
+        return stream
+    return C.c_void_p(int(getattr(stream, "cuda_stream", stream)))
+
+
+class Pool:
+    def __init__(self, arena_bytes: int, storage: str = "f32", arith: str = "fast", max_domains: int = 8192):
+        d = N.PoolDesc(_STORAGE[storage], N.ARITH_EXACT if arith == "exact" else N.ARITH_FAST, int(arena_bytes),
+                       int(max_domains))
+        h = C.c_void_p()
+        N.check(N.lib().vfb_pool_create(C.byref(d), C.byref(h)))
+        self._h = h
+        self.storage = storage
+        self.real = np.float64 if storage == "f64" else np.float32
+        self.domains = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib().vfb_pool_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def desc(shape, omega, periodic=(True, True, True), forces=(0.0, 0.0, 0.0), limiters=(0.01, 0.01, 0.01)):
+        d = N.DomainDesc()
+        d.nx, d.ny, d.nz = (int(v) for v in shape)
+        d.periodic_x, d.periodic_y, d.periodic_z = (int(bool(v)) for v in periodic)
+        d.omega = float(omega)
+        for i in range(3):
+            d.forces[i] = float(forces[i])
+            d.quadric_limiters[i] = float(limiters[i])
+        return d
+
+    def domain_bytes(self, shape, omega=1.8, periodic=(True, True, True), has_mask=False) -> int:
+        b = C.c_uint64()
+        N.check(N.lib().vfb_pool_domain_bytes(self._h, C.byref(self.desc(shape, omega, periodic)), int(has_mask),
+                                              C.byref(b)))
+        return b.value
+
+    def add(self, shape, omega, periodic=(True, True, True), forces=(0.0, 0.0, 0.0), mask=None) -> int:
+        """Carve a domain; raises VfbError(VFB_ERR_OUT_OF_MEMORY) when the arena has no room."""
+        d = self.desc(shape, omega, periodic, forces)
+        m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
+        i = C.c_uint32()
+        N.check(N.lib().vfb_pool_add_domain(self._h, C.byref(d), m.ctypes.data if m is not None else None, C.byref(i)))
+        self.domains[i.value] = tuple(int(v) for v in shape)
+        return i.value
+
+    def try_add(self, *args, **kwargs):
+        try:
+            return self.add(*args, **kwargs)
+        except N.VfbError as e:
+            if e.status == N.VFB_ERR_OUT_OF_MEMORY:
+                return None
+            raise
+
+    def remove(self, domain: int):
+        N.check(N.lib().vfb_pool_remove_domain(self._h, int(domain)))
+        self.domains.pop(domain, None)
+
+    def synchronize(self, stream=None):
+        N.check(N.lib().vfb_pool_synchronize(self._h, _stream_ptr(stream)))
+
+    def init(self, domain: int, rho=None, ux=None, uy=None, uz=None, stream=None):
+        """Equilibrium from host arrays (numpy) or device tensors (torch); None = zero."""
+        shape = self.domains[domain]
+        n = shape[0] * shape[1] * shape[2]
+        arrs = [rho, ux, uy, uz]
+        if any(a is not None and hasattr(a, "data_ptr") for a in arrs):
+            import torch
+            dt = torch.float64 if self.real == np.float64 else torch.float32
+            dev = next(a.device for a in arrs if a is not None and hasattr(a, "data_ptr"))
+            keep = [a.to(dt).contiguous() if a is not None else torch.zeros(n, dtype=dt, device=dev) for a in arrs]
+            N.check(N.lib().vfb_pool_init_domain(self._h, int(domain), *(C.c_void_p(t.data_ptr()) for t in keep), 0,
+                                                 _stream_ptr(stream)))
+            return
+        keep = [np.ascontiguousarray(a if a is not None else np.zeros(n), dtype=self.real).reshape(-1) for a in arrs]
+        N.check(N.lib().vfb_pool_init_domain(self._h, int(domain), *(a.ctypes.data for a in keep), 1,
+                                             _stream_ptr(stream)))
+
+    def step(self, steps: int, stream=None):
+        N.check(N.lib().vfb_pool_step(self._h, int(steps), _stream_ptr(stream)))
+
+    def fields(self, domain: int, stream=None):
+        """drho, ux, uy, uz of one domain as numpy arrays of shape (nz, ny, nx)."""
+        shape = self.domains[domain]
+        n = shape[0] * shape[1] * shape[2]
+        out = [np.zeros(n, dtype=self.real) for _ in range(4)]
+        N.check(N.lib().vfb_pool_domain_fields(self._h, int(domain), *(a.ctypes.data for a in out), 1,
+                                               _stream_ptr(stream)))
+        return [a.reshape(shape[2], shape[1], shape[0]) for a in out]
+
+    def set_launch(self, threads=128, nodes_per_thread=1, blocks_per_sm=0, use_graph=True):
+        N.check(N.lib().vfb_pool_set_launch(self._h, int(threads), int(nodes_per_thread), int(blocks_per_sm),
+                                            int(use_graph)))
+
+    def launch(self):
+        out = (C.c_int32 * 4)()
+        N.check(N.lib().vfb_pool_get_launch(self._h, out))
+        return {"threads": out[0], "nodes_per_thread": out[1], "blocks_per_sm": out[2], "use_graph": bool(out[3])}
+
+    def autotune(self, trial_steps=10, stream=None) -> float:
+        ms = C.c_double()
+        N.check(N.lib().vfb_pool_autotune(self._h, int(trial_steps), _stream_ptr(stream), C.byref(ms)))
+        return ms.value
+
+    def stats(self):
+        a, n, u, f = C.c_uint32(), C.c_uint64(), C.c_uint64(), C.c_uint64()
+        N.check(N.lib().vfb_pool_stats(self._h, C.byref(a), C.byref(n), C.byref(u), C.byref(f)))
+        return {"active_domains": a.value, "active_nodes": n.value, "used_bytes": u.value, "free_bytes": f.value}
+
+    def kernel_launches(self) -> int:
+        c = C.c_uint64()
+        N.check(N.lib().vfb_pool_kernel_launches(self._h, C.byref(c)))
+        return c.value
