@@ -176,6 +176,93 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_batch(args):
+    """Config 4: rectangular-duct Poiseuille domains of uneven sizes in one domain pool, advanced by
+    one persistent launch per step (CUDA-graph replay, autotuned launch shape), FP32 and FP16
+    storage. With --check-steps S > 0 every domain also runs S steps in FP64, FP32 and FP16 and its
+    x-averaged profile is compared with the analytic start-up series and with the FP64 run."""
+    import torch
+
+    from virtualfluids_b200 import Pool
+    from virtualfluids_b200.workloads import duct_batch, duct_transient
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    specs = duct_batch(args.domains, seed=20261203 + rank)
+    fluid = sum(d["fluid_nodes"] for d in specs)
+
+    def build(storage):
+        probe = Pool(1 << 20, storage=storage, max_domains=1)
+        need = sum(probe.domain_bytes(d["shape"], d["omega"], periodic=(True, False, False), has_mask=True)
+                   for d in specs)
+        probe.close()
+        pool = Pool(need + (1 << 20), storage=storage, max_domains=len(specs))
+        ids = []
+        for d in specs:
+            i = pool.add(d["shape"], d["omega"], periodic=(True, False, False), forces=(d["g"], 0.0, 0.0))
+            pool.init(i, stream=stream)
+            ids.append(i)
+        return pool, ids
+
+    forms = {}
+    for storage in ("f32", "f16"):
+        pool, ids = build(storage)
+        tuned = pool.autotune(trial_steps=3, stream=stream)
+        pool.step(args.warmup, stream=stream)
+        stream.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = pool.kernel_launches()
+        with ClockSampler(local) as clk:
+            ev0.record(stream)
+            pool.step(args.steps, stream=stream)
+            ev1.record(stream)
+            stream.synchronize()
+        ms = ev0.elapsed_time(ev1) / args.steps
+        forms[storage] = {"mlups": round(fluid / (ms / 1e3) / 1e6, 1), "ms_per_step": round(ms, 4),
+                          "hbm_gbs_algorithmic": round(BYTES_PER_NODE[storage] * fluid / (ms / 1e3) / 1e9, 1),
+                          "launch": pool.launch(), "autotune_ms_per_step": round(tuned, 4),
+                          "gpu_launches": pool.kernel_launches() - l0, "clocks": clk.summary()}
+        pool.close()
+        del pool
+        torch.cuda.empty_cache()
+    check = None
+    if args.check_steps > 0:
+        prof = {}
+        for storage in ("f64", "f32", "f16"):
+            pool, ids = build(storage)
+            pool.step(args.check_steps, stream=stream)
+            stream.synchronize()
+            prof[storage] = [pool.fields(i, stream=stream)[1].mean(axis=2)[1:-1, 1:-1].astype(np.float64) for i in ids]
+            pool.close()
+            del pool
+            torch.cuda.empty_cache()
+        ana, e32, e16 = [], [], []
+        for k, d in enumerate(specs):
+            ref = duct_transient(d["shape"][1], d["shape"][2], d["g"], d["nu"], args.check_steps, terms=31)[1:-1, 1:-1]
+            u64 = prof["f64"][k]
+            nrm = np.sqrt((u64 ** 2).sum())
+            ana.append(np.sqrt(((u64 - ref) ** 2).sum()) / np.sqrt((ref ** 2).sum()))
+            e32.append(np.sqrt(((prof["f32"][k] - u64) ** 2).sum()) / nrm)
+            e16.append(np.sqrt(((prof["f16"][k] - u64) ** 2).sum()) / nrm)
+        q = lambda v: {"median": float(np.median(v)), "p99": float(np.quantile(v, 0.99)), "max": float(np.max(v))}
+        check = {"steps": args.check_steps, "fp64_vs_analytic_rel_l2": q(ana), "fp32_vs_fp64_rel_l2": q(e32),
+                 "fp16_vs_fp64_rel_l2": q(e16)}
+    if rank == 0:
+        line = {"metric": "MLUPS (4096 rectangular ducts, one domain pool, FP32 storage)",
+                "value": forms["f32"]["mlups"], "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": forms["f32"]["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"{args.domains} ducts, sides log-uniform in [16, 96], periodic x, walls y/z, "
+                                       "body force for u_max 0.03, Re uniform in [max(10, 42 u_max H), 500]",
+                           "domains": args.domains, "fluid_nodes": fluid,
+                           "l2": "inputs larger than L2, no flush"},
+                "forms": forms, "gpu_launches": forms["f32"]["gpu_launches"]}
+        if check:
+            line["check"] = check
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -188,10 +275,17 @@ def main():
     ap.add_argument("--arith", default="fast", choices=["fast", "exact"],
                     help="exact: every operation rounded as the reference's host build (bitwise oracle parity)")
     ap.add_argument("--kernel", default="auto", choices=["auto", "direct", "tma", "async"])
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch"],
+                    help="tgv: the headline (TGV 256^3 FP64); batch: 4096 ducts in one domain pool")
+    ap.add_argument("--domains", type=int, default=4096)
+    ap.add_argument("--check-steps", type=int, default=0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "batch":
+        run_batch(args)
         return
 
     import torch

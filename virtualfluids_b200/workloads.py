@@ -1,0 +1,124 @@
+"""Synthetic workloads with the shapes of the benchmark configurations, and their analytic checks.
+
+* :func:`tgv_fields` — Taylor-Green vortex initial fields on a periodic box (the reference's TGV
+  app, apps/gpu/TaylorGreenVortex, on [-pi, pi]^3);
+* :func:`duct_batch` — rectangular-duct Poiseuille domains of uneven sizes for the batched sweep,
+  with :func:`duct_series` (steady) and :func:`duct_transient` (start-up from rest) profiles;
+* :func:`porous_block` — a cube of random non-overlapping spheres at a target porosity, with the
+  exact sphere q of every cut link, for the serving stream.
+
+All generators are seeded; the analytic profiles follow from the mathematics of the problems
+(eigenfunction series of the Poisson and heat equations on a rectangle).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+# K17 is unstable above this viscosity (a shear wave grows at nu = 0.04); Parameter warns above it
+K17_NU_MAX = 1.0 / 42.0
+
+
+def tgv_fields(n, u0, dtype=np.float64):
+    """drho, ux, uy, uz (x fastest) of the Taylor-Green vortex on an n^3 periodic box."""
+    x = (np.arange(n) + 0.5) / n * 2 * np.pi - np.pi
+    Z, Y, X = np.meshgrid(x, x, x, indexing="ij")
+    rho = 3.0 * (u0 * u0 / 16.0) * (np.cos(2 * X) + np.cos(2 * Y)) * (np.cos(2 * Z) + 2.0)
+    ux = u0 * np.sin(X) * np.cos(Y) * np.cos(Z)
+    uy = -u0 * np.cos(X) * np.sin(Y) * np.cos(Z)
+    return [a.reshape(-1).astype(dtype) for a in (rho, ux, uy, np.zeros_like(ux))]
+
+
+def _duct_axes(ny, nz):
+    """Half-widths and node coordinates of a duct whose first and last layers in y and z are solid
+    walls; the no-slip planes lie half-way between the walls and the first fluid nodes."""
+    a, b = (ny - 2) / 2.0, (nz - 2) / 2.0
+    y = np.arange(ny) - (ny - 1) / 2.0
+    z = np.arange(nz) - (nz - 1) / 2.0
+    Z, Y = np.meshgrid(z, y, indexing="ij")
+    return a, b, Y, Z
+
+
+def duct_series(ny, nz, g, nu, terms=101):
+    """Steady u(z, y) of a duct driven by the body force g along x (Poisson problem
+    nu lap u = -g, u = 0 on the walls), as the single cosine/cosh series."""
+    a, b, Y, Z = _duct_axes(ny, nz)
+    return _series(a, b, Y, Z, g, nu, terms)
+
+
+def _series(a, b, Y, Z, g, nu, terms):
+    u = np.zeros_like(np.asarray(Y, dtype=np.float64))
+    az = np.abs(Z)
+    for n in range(1, terms + 1, 2):
+        k = n * np.pi / (2 * a)
+        # cosh(k z) / cosh(k b) without overflow
+        ratio = np.exp(k * (az - b)) * (1 + np.exp(-2 * k * az)) / (1 + np.exp(-2 * k * b))
+        u = u + (-1) ** ((n - 1) // 2) / n ** 3 * (1 - ratio) * np.cos(k * Y)
+    return 16 * a * a * g / (nu * np.pi ** 3) * u
+
+
+def duct_transient(ny, nz, g, nu, t, terms=61):
+    """u(z, y, t) after the start-up from rest under the body force g: the double series
+    sum g_mn / (nu l_mn) (1 - exp(-nu l_mn t)) cos(m pi y / 2a) cos(n pi z / 2b) over odd m, n, with
+    g_mn = 16 g (-1)^((m + n) / 2 - 1) / (m n pi^2) and l_mn = (m pi / 2a)^2 + (n pi / 2b)^2."""
+    a, b, Y, Z = _duct_axes(ny, nz)
+    u = np.zeros_like(Y)
+    for m in range(1, terms + 1, 2):
+        km = m * np.pi / (2 * a)
+        cy = np.cos(km * Y)
+        for n in range(1, terms + 1, 2):
+            kn = n * np.pi / (2 * b)
+            lam = km * km + kn * kn
+            gmn = 16.0 * g * (-1) ** ((m + n) // 2 - 1) / (m * n * np.pi ** 2)
+            u += gmn / (nu * lam) * (1.0 - np.exp(-nu * lam * t)) * cy * np.cos(kn * Z)
+    return u
+
+
+def duct_peak_per_force(ny, nz, nu):
+    """Steady centre-line velocity (at the duct axis) per unit body force."""
+    return float(_series((ny - 2) / 2.0, (nz - 2) / 2.0, 0.0, 0.0, 1.0, nu, 101))
+
+
+def duct_batch(count, seed=20261203, sides=(16, 96), re_range=(10.0, 500.0), u_max=0.03):
+    """Rectangular ducts for the batched sweep: each side log-uniform in `sides`, periodic in x with
+    walls in y and z, Re = u_max H / nu uniform with H the smaller cross-section side, the body force
+    set so the steady centre-line velocity is u_max. Re is drawn from [max(Re_lo, 42 u_max H), Re_hi]
+    so that nu stays within K17's stable range (nu <= 1/42)."""
+    rng = np.random.default_rng(seed)
+    lo, hi = math.log(sides[0]), math.log(sides[1])
+    out = []
+    for _ in range(count):
+        nx, ny, nz = (int(round(math.exp(v))) for v in rng.uniform(lo, hi, 3))
+        H = min(ny, nz) - 2
+        re_lo = max(re_range[0], u_max * H / K17_NU_MAX)
+        re = float(rng.uniform(re_lo, max(re_lo, re_range[1])))
+        nu = u_max * H / re
+        g = u_max / duct_peak_per_force(ny, nz, nu)
+        out.append({"shape": (nx, ny, nz), "nu": nu, "omega": 1.0 / (3.0 * nu + 0.5), "g": g, "re": re,
+                    "fluid_nodes": nx * (ny - 2) * (nz - 2)})
+    return out
+
+
+def porous_block(side, seed, porosity=None, radius=(3.0, 8.0), max_tries=20000):
+    """A side^3 block of random non-overlapping spheres added one at a time until the solid fraction
+    reaches 1 - porosity (porosity uniform in [0.5, 0.9] when not given). Returns the node mask
+    (x fastest, nonzero = fluid), the spheres (cx, cy, cz, r) and the porosity reached."""
+    rng = np.random.default_rng(seed)
+    if porosity is None:
+        porosity = float(rng.uniform(0.5, 0.9))
+    z, y, x = np.meshgrid(np.arange(side), np.arange(side), np.arange(side), indexing="ij")
+    solid = np.zeros((side, side, side), dtype=bool)
+    spheres = []
+    target = (1.0 - porosity) * side ** 3
+    tries = 0
+    while solid.sum() < target and tries < max_tries:
+        tries += 1
+        r = float(rng.uniform(*radius))
+        c = rng.uniform(r, side - 1 - r, 3)
+        if any((c[0] - s[0]) ** 2 + (c[1] - s[1]) ** 2 + (c[2] - s[2]) ** 2 < (r + s[3]) ** 2 for s in spheres):
+            continue
+        spheres.append((float(c[0]), float(c[1]), float(c[2]), r))
+        solid |= (x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2 <= r * r
+    mask = (~solid).astype(np.uint8).reshape(-1)
+    return mask, spheres, float(mask.mean())
