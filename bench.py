@@ -263,6 +263,134 @@ def run_batch(args):
         print(json.dumps(line), flush=True)
 
 
+def run_tgv_forms(args):
+    """Config 2 accuracy: the 256^3 Taylor-Green vortex for --form-steps steps in FP64, FP32, FP16
+    and BF16 storage (FMA arithmetic), the FP64 kinetic-energy decay every 100 steps, and the L2 /
+    L-inf velocity error of each form against the FP64 run at steps 1000, 5000 and 10000 (relative
+    to the FP64 field's RMS / maximum speed)."""
+    import torch
+
+    import virtualfluids_b200 as vfb
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.n
+    fields = tgv_fields(n, U0)
+    checkpoints = [c for c in (1000, 5000, 10000) if c <= args.form_steps]
+    every = 100
+    ref = {}
+    out = {}
+    for st in ("f64", "f32", "f16", "bf16"):
+        dt = torch.float64 if st == "f64" else torch.float32
+        box = vfb.Box(n, n, n, omega_tgv(n), storage=st)
+        box.init(*(torch.from_numpy(a).to(dev, dt) for a in fields))
+        done, ek, errs = 0, [], {}
+        t0 = time.perf_counter()
+        for c in checkpoints:
+            while done < c:
+                k = min(every, c - done)
+                e = np.zeros((k, 2))
+                box.step(k, energy=e)
+                ek.append(float(e[-1, 1]))
+                done += k
+            f = box.fields()
+            u = np.stack([f["vx"], f["vy"], f["vz"]]).astype(np.float64)
+            if st == "f64":
+                ref[c] = u
+            else:
+                d = u - ref[c]
+                rms = np.sqrt((ref[c] ** 2).sum(axis=0).mean())
+                errs[c] = {"l2_rel": float(np.sqrt((d ** 2).sum(axis=0).mean()) / rms),
+                           "linf_rel": float(np.sqrt((d ** 2).sum(axis=0)).max() / np.sqrt((ref[c] ** 2).sum(axis=0)).max())}
+        out[st] = {"wall_s": round(time.perf_counter() - t0, 2), "kinetic_energy_every_100_steps": ek}
+        if errs:
+            out[st]["velocity_error_vs_fp64"] = errs
+        del box
+        torch.cuda.empty_cache()
+    if rank == 0:
+        line = {"metric": "TGV 256^3 kinetic-energy decay and velocity error of the storage forms against FP64",
+                "value": out.get("f16", {}).get("velocity_error_vs_fp64", {}).get(checkpoints[-1], {}).get("l2_rel"),
+                "unit": "relative L2 velocity error (FP16 storage, last checkpoint)", "n_gpus": world,
+                "steps": args.form_steps, "warmup": 0, "ms_per_step": None, "higher_is_better": False,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32/f16/bf16", "data": "synthetic",
+                "config": {"workload": f"Taylor-Green vortex {n}^3, u0={U0}, Re={int(RE)}", "checkpoints": checkpoints},
+                "forms": out}
+        print(json.dumps(line), flush=True)
+
+
+def run_serving(args):
+    """Config 5: a Poisson stream of porous-block solves served by continuous batching in one domain
+    pool whose arena is the HBM budget. Offered loads are fractions of the measured capacity (node
+    updates per second of a full pool / the mean work of a request). Reports p50/p99 time to
+    solution and aggregate MLUPS in FP32 and FP16 storage, and the permeability error against each
+    request solved alone in FP64."""
+    import dataclasses
+
+    import torch
+
+    from virtualfluids_b200 import Pool
+    from virtualfluids_b200.serving import Server, poisson_stream, solve_alone
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    base = poisson_stream(args.requests, rate=1.0, seed=20261203 + rank)
+    for r in base:
+        r.geometry()
+    mean_work = float(np.mean([r.side ** 3 * r.steps for r in base]))
+    budget = int(args.hbm_gb * (1 << 30))
+    out = {}
+    k64 = [solve_alone(r, storage="f64")[0] for r in base]
+    for storage in ("f32", "f16"):
+        # capacity: a pool filled with the stream's first requests, timed over 50 steps
+        s = torch.cuda.Stream()
+        cal = Pool(budget, storage=storage, max_domains=len(base))
+        nodes = 0
+        for r in base:
+            d = cal.try_add((r.side,) * 3, 1.0 / (3 * r.nu + 0.5), forces=(r.g, 0, 0), mask=r.geometry())
+            if d is None:
+                break
+            cal.init(d, stream=s)
+            nodes += r.side ** 3
+        cal.step(4, stream=s)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        cal.step(50, stream=s)
+        e1.record(s)
+        s.synchronize()
+        throughput = nodes * 50 / (e0.elapsed_time(e1) / 1e3)
+        cal.close()
+        capacity = throughput / mean_work
+        out[storage] = {"capacity_requests_per_s": round(capacity, 4), "node_updates_per_s": round(throughput, 1)}
+        for load in args.loads:
+            reqs = [dataclasses.replace(r, arrival=r.arrival / (load * capacity)) for r in base]
+            srv = Server(budget, storage=storage, max_domains=len(base))
+            with ClockSampler(local) as clk:
+                results, st = srv.run(reqs, realtime=True)
+            srv.close()
+            err = [abs(res.permeability - k) / abs(k) for res, k in zip(results, k64)]
+            out[storage][f"load_{load}"] = {
+                "offered_requests_per_s": round(load * capacity, 4), "p50_s": round(st["p50_s"], 3),
+                "p99_s": round(st["p99_s"], 3), "mlups": round(st["mlups"], 1), "wall_s": round(st["wall_s"], 2),
+                "peak_concurrent": st["peak_concurrent"], "gpu_launches": st["gpu_launches"],
+                "permeability_rel_err_vs_fp64": {"median": float(np.median(err)), "max": float(np.max(err))},
+                "clocks": clk.summary()}
+            torch.cuda.empty_cache()
+    if rank == 0:
+        f32 = out["f32"][f"load_{args.loads[0]}"]
+        line = {"metric": f"p50/p99 time to solution and MLUPS, porous-block serving stream ({args.requests} "
+                          f"requests, {args.hbm_gb} GB HBM budget, FP32)",
+                "value": f32["mlups"], "unit": "MLUPS", "n_gpus": world, "steps": None, "warmup": None,
+                "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "Poisson arrivals; cube side U{32..192}; random non-overlapping spheres r in "
+                                       "[3, 8] at porosity U[0.5, 0.9] (jammed packings stop near 0.7); body force "
+                                       "equivalent to the pressure drop along x; steps U{1000..20000}; nu = 1/60",
+                           "requests": args.requests, "hbm_budget_gb": args.hbm_gb, "loads": args.loads},
+                "serving": out}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -275,10 +403,15 @@ def main():
     ap.add_argument("--arith", default="fast", choices=["fast", "exact"],
                     help="exact: every operation rounded as the reference's host build (bitwise oracle parity)")
     ap.add_argument("--kernel", default="auto", choices=["auto", "direct", "tma", "async"])
-    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch"],
-                    help="tgv: the headline (TGV 256^3 FP64); batch: 4096 ducts in one domain pool")
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "serving", "tgv-forms"],
+                    help="tgv: the headline (TGV 256^3 FP64); batch: 4096 ducts in one domain pool; "
+                         "serving: a Poisson stream of porous-block solves; tgv-forms: storage-form accuracy")
+    ap.add_argument("--form-steps", type=int, default=10000)
     ap.add_argument("--domains", type=int, default=4096)
     ap.add_argument("--check-steps", type=int, default=0)
+    ap.add_argument("--requests", type=int, default=32)
+    ap.add_argument("--hbm-gb", type=float, default=24.0)
+    ap.add_argument("--loads", type=float, nargs="+", default=[0.5, 0.9])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -286,6 +419,12 @@ def main():
         return
     if args.workload == "batch":
         run_batch(args)
+        return
+    if args.workload == "serving":
+        run_serving(args)
+        return
+    if args.workload == "tgv-forms":
+        run_tgv_forms(args)
         return
 
     import torch

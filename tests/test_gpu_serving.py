@@ -1,0 +1,58 @@
+"""Serving on the GPU: continuous batching of porous-block solves in one domain pool.
+
+Requests of different sizes and step counts are admitted as memory frees up, advance together,
+and leave when done. Each result must be the same alone and in the mix (bit for bit: the pool's
+kernels treat every domain independently), and the FP16-storage permeability must stay close to
+the FP64 one.
+"""
+import numpy as np
+import pytest
+
+from virtualfluids_b200.serving import Request, Server, poisson_stream, solve_alone
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_stream(n=7, seed=5):
+    reqs = poisson_stream(n, rate=1000.0, seed=seed, sides=(20, 40), steps=(100, 600))
+    for r in reqs:
+        r.geometry()
+    return reqs
+
+
+def test_each_result_is_the_same_alone_and_in_the_mix(cuda):
+    reqs = _small_stream()
+    # an arena that holds about three of these solves at a time, so later ones queue for memory
+    per = max(r.side for r in reqs) ** 3 * (27 * 4 + 1) + 4096
+    srv = Server(3 * per, storage="f32", keep_fields=True)
+    results, stats = srv.run(reqs, realtime=False)
+    srv.close()
+    assert stats["peak_concurrent"] >= 2
+    assert all(r.finished >= r.admitted >= 0 for r in results)
+    for req, res in zip(reqs, results):
+        perm, ux = solve_alone(req, storage="f32")
+        assert np.array_equal(res.ux, ux), req.rid
+        assert res.permeability == perm and perm > 0
+
+
+def test_requests_arriving_during_others_are_admitted_before_those_finish(cuda):
+    reqs = poisson_stream(6, rate=40.0, seed=11, sides=(24, 40), steps=(2000, 3000))
+    for r in reqs:
+        r.geometry()
+    srv = Server(1 << 30, storage="f32")
+    results, stats = srv.run(reqs, realtime=True)
+    srv.close()
+    overlapped = any(later.admitted < earlier.finished
+                     for i, earlier in enumerate(results) for later in results[i + 1:])
+    assert overlapped
+    assert stats["p99_s"] >= stats["p50_s"] > 0 and stats["mlups"] > 0
+
+
+def test_fp16_storage_permeability_close_to_fp64(cuda):
+    req = Request(rid=0, arrival=0.0, side=40, steps=3000, seed=3, porosity=0.8)
+    k64, _ = solve_alone(req, storage="f64")
+    k16, _ = solve_alone(req, storage="f16")
+    k32, _ = solve_alone(req, storage="f32")
+    assert k64 > 0
+    assert abs(k32 - k64) <= 1e-4 * k64
+    assert abs(k16 - k64) <= 1e-2 * k64

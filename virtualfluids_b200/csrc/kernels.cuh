@@ -9,6 +9,7 @@
 #pragma once
 #include <cstdint>
 
+#include "addr.h"
 #include "interp.cuh"
 #include "k17.cuh"
 #include "storage.cuh"
@@ -52,10 +53,14 @@ struct BoxCollideArgs {
     C *rho, *vx, *vy, *vz;      // optional macroscopic outputs
 };
 
+// where a node's eight slot nodes are: from the neighbour lists (reference layout), or, when
+// nbx is null, by index arithmetic on the structured box `box`
+
 struct BCArgs {
     void *dist;
-    uint64_t n;
+    uint64_t n;                 // plane stride
     const uint32_t *nbx, *nby, *nbz;
+    NodeAddr box;
     const int32_t *k;           // BC node indices
     const void *q27;            // q27[dir * nbc + i], compute type
     uint32_t nbc;
@@ -67,6 +72,7 @@ struct PressureArgs {
     void *dist;
     uint64_t n;
     const uint32_t *nbx, *nby, *nbz;
+    NodeAddr box;
     const int32_t *k, *kN;
     const void *rho_bc;
     uint32_t nbc;
@@ -91,6 +97,36 @@ __device__ __forceinline__ void list_nodes(uint32_t k, const uint32_t *__restric
     nodes[5] = __ldg(nbz + kx);
     nodes[6] = __ldg(nbz + ky);
     nodes[7] = __ldg(nbz + kxy);
+}
+
+// the eight slot nodes of a node on a structured box
+__device__ __forceinline__ void box_nodes(uint32_t k, const NodeAddr &b, uint32_t (&nodes)[8])
+{
+    const uint32_t x = k % (uint32_t)b.nx, yz = k / (uint32_t)b.nx;
+    const uint32_t y = yz % (uint32_t)b.ny, z = yz / (uint32_t)b.ny;
+    const int xp = ((int)x + 1 < b.nx) ? (int)x + 1 : ((b.periodic & 1) ? 0 : (int)x);
+    const int yp = ((int)y + 1 < b.ny) ? (int)y + 1 : ((b.periodic & 2) ? 0 : (int)y);
+    const int zp = ((int)z + 1 < b.nz) ? (int)z + 1 : ((b.periodic & 4) ? 0 : (int)z);
+    const uint32_t sx = (uint32_t)(xp - (int)x);
+    const uint32_t sy = (uint32_t)((yp - (int)y) * b.nx);
+    const uint32_t sz = (uint32_t)((int64_t)(zp - (int)z) * b.nx * b.ny);
+    nodes[0] = k;
+    nodes[1] = k + sx;
+    nodes[2] = k + sy;
+    nodes[3] = k + sx + sy;
+    nodes[4] = k + sz;
+    nodes[5] = k + sx + sz;
+    nodes[6] = k + sy + sz;
+    nodes[7] = k + sx + sy + sz;
+}
+
+__device__ __forceinline__ void node_slots(uint32_t k, const uint32_t *nbx, const uint32_t *nby, const uint32_t *nbz,
+                                           const NodeAddr &b, uint32_t (&nodes)[8])
+{
+    if (nbx)
+        list_nodes(k, nbx, nby, nbz, nodes);
+    else
+        box_nodes(k, b, nodes);
 }
 
 template <class S, bool EVEN>
@@ -541,7 +577,7 @@ __global__ void __launch_bounds__(128) bc_bounce_back_kernel(BCArgs a)
         return;
     const uint32_t node = (uint32_t)a.k[i];
     uint32_t nodes[8];
-    list_nodes(node, a.nbx, a.nby, a.nbz, nodes);
+    node_slots(node, a.nbx, a.nby, a.nbz, a.box, nodes);
     S *base = static_cast<S *>(a.dist);
     C post[27];
     gather_post<S, EVEN>(base, a.n, nodes, post);
@@ -613,7 +649,7 @@ __global__ void __launch_bounds__(128) bc_interpolated_kernel(BCArgs a)
         return;
     const uint32_t node = (uint32_t)a.k[i];
     uint32_t nodes[8];
-    list_nodes(node, a.nbx, a.nby, a.nbz, nodes);
+    node_slots(node, a.nbx, a.nby, a.nbz, a.box, nodes);
     S *base = static_cast<S *>(a.dist);
     C p[27];
     gather_post<S, EVEN>(base, a.n, nodes, p);
@@ -682,8 +718,8 @@ __global__ void __launch_bounds__(128) bc_pressure_neq_kernel(PressureArgs a)
     if (i >= a.nbc)
         return;
     uint32_t nn[8], nk[8];
-    list_nodes((uint32_t)a.kN[i], a.nbx, a.nby, a.nbz, nn);
-    list_nodes((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, nk);
+    node_slots((uint32_t)a.kN[i], a.nbx, a.nby, a.nbz, a.box, nn);
+    node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.box, nk);
     S *base = static_cast<S *>(a.dist);
     C f[27];
     gather_pre<S, EVEN>(base, a.n, nn, f);
@@ -1034,6 +1070,7 @@ struct DragArgs {
     const void *dist;
     uint64_t n;
     const uint32_t *nbx, *nby, *nbz;
+    NodeAddr box;
     const int32_t *k;           // geometry BC node indices
     const void *q27;            // q27[dir * nbc + i], compute type
     uint32_t nbc;
@@ -1077,7 +1114,7 @@ __global__ void __launch_bounds__(128) drag_lift_kernel(DragArgs a)
     if (i >= a.nbc)
         return;
     uint32_t nodes[8];
-    list_nodes((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, nodes);
+    node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.box, nodes);
     const S *base = static_cast<const S *>(a.dist);
     C fc[27];
     if constexpr (PRE)
@@ -1166,6 +1203,50 @@ __global__ void __launch_bounds__(256) k17_pool_kernel(PoolArgs<typename Codec<S
             scatter_post<S, EVEN>(base, dm.pitch, nodes, f);
         }
     }
+}
+
+
+// ---------------------------------------------------------------------------------------------
+// seeded per-step perturbation of a velocity inlet: u_i(t) = u0_i (1 + a (2 U - 1)), U uniform in
+// [0, 1) from the counter-based Philox-4x32-10 generator (Salmon et al., SC'11) keyed by the seed,
+// counted by (node, step)
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t mulhilo(uint32_t a, uint32_t b, uint32_t &hi)
+{
+    const uint64_t p = (uint64_t)a * b;
+    hi = (uint32_t)(p >> 32);
+    return (uint32_t)p;
+}
+
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi0, hi1;
+        const uint32_t lo0 = mulhilo(0xD2511F53u, c.x, hi0);
+        const uint32_t lo1 = mulhilo(0xCD9E8D57u, c.z, hi1);
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += 0x9E3779B9u;
+        k.y += 0xBB67AE85u;
+    }
+    return c;
+}
+
+template <class C>
+__global__ void __launch_bounds__(256) inlet_perturbation_kernel(const C *base_x, const C *base_y, const C *base_z,
+                                                                 C *ux, C *uy, C *uz, uint32_t n, uint64_t seed,
+                                                                 uint64_t step, double amplitude)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const uint4 r = philox4x32_10(make_uint4(i, (uint32_t)step, (uint32_t)(step >> 32), 0u),
+                                  make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+    const double u01 = (double)r.x * (1.0 / 4294967296.0);
+    const C factor = (C)(1.0 + amplitude * (2.0 * u01 - 1.0));
+    ux[i] = base_x[i] * factor;
+    uy[i] = base_y[i] * factor;
+    uz[i] = base_z[i] * factor;
 }
 
 } // namespace VFB_NS

@@ -10,6 +10,7 @@
 
 #include <cstdint>
 
+#include "addr.h"
 #include "vfb.h"
 
 namespace vfb {
@@ -48,8 +49,12 @@ inline uint64_t box_blocks(const BoxState &b)
     template <class S>                                                                                               \
     struct Launchers {                                                                                               \
         static cudaError_t k17_list(const vfb_level *L, const uint32_t *idx, uint32_t n, int tmpl, cudaStream_t s); \
-        static cudaError_t bc(const vfb_level *L, const vfb_bc *bc, int kind, cudaStream_t s);                     \
-        static cudaError_t pressure(const vfb_level *L, const vfb_directional_bc *bc, cudaStream_t s);             \
+        static cudaError_t bc(const vfb_level *L, const vfb_bc *bc, int kind, cudaStream_t s,                        \
+                              const NodeAddr *box = nullptr);                                                        \
+        static cudaError_t pressure(const vfb_level *L, const vfb_directional_bc *bc, cudaStream_t s,                \
+                                    const NodeAddr *box = nullptr);                                                  \
+        static cudaError_t inlet_perturbation(const void *base, void *vel, uint32_t n, uint64_t seed,                \
+                                              uint64_t step, double amplitude, cudaStream_t s);                      \
         static cudaError_t init_list(const vfb_level *L, cudaStream_t s);                                          \
         static cudaError_t macros_list(const vfb_level *L, cudaStream_t s);                                        \
         static cudaError_t energy_list(const vfb_level *L, const uint32_t *idx, uint32_t n, double *partials,     \
@@ -69,7 +74,7 @@ inline uint64_t box_blocks(const BoxState &b)
                                 int ny, int nz, int flags, double omega, const double lim[3],                      \
                                 const double half_force[3]);                                                       \
         static cudaError_t drag_lift(const vfb_level *L, const vfb_bc *bc, bool pre, double *dx, double *dy,        \
-                                     double *dz, cudaStream_t s);                                                  \
+                                     double *dz, cudaStream_t s, const NodeAddr *box = nullptr);                     \
         static cudaError_t scale(const vfb_level *coarse, const vfb_level *fine, const vfb_interpolation_cells *cells, \
                                  const vfb_interpolation_cell_neighbor *offsets, bool fine_to_coarse, cudaStream_t s); \
     };

@@ -85,16 +85,17 @@ cudaError_t Launchers<S>::k17_list(const vfb_level *L, const uint32_t *idx, uint
 }
 
 template <class S>
-cudaError_t Launchers<S>::bc(const vfb_level *L, const vfb_bc *bc, int kind, cudaStream_t s)
+cudaError_t Launchers<S>::bc(const vfb_level *L, const vfb_bc *bc, int kind, cudaStream_t s, const NodeAddr *box)
 {
     if (bc->number_of_bc_nodes == 0)
         return cudaSuccess;
     BCArgs a;
     a.dist = L->distributions;
     a.n = L->number_of_nodes;
-    a.nbx = L->neighbor_x;
-    a.nby = L->neighbor_y;
-    a.nbz = L->neighbor_z;
+    a.nbx = box ? nullptr : L->neighbor_x;
+    a.nby = box ? nullptr : L->neighbor_y;
+    a.nbz = box ? nullptr : L->neighbor_z;
+    a.box = box ? *box : NodeAddr{ 0, 0, 0, 0 };
     a.k = bc->k;
     a.q27 = bc->q27;
     a.nbc = bc->number_of_bc_nodes;
@@ -128,16 +129,18 @@ cudaError_t Launchers<S>::bc(const vfb_level *L, const vfb_bc *bc, int kind, cud
 }
 
 template <class S>
-cudaError_t Launchers<S>::pressure(const vfb_level *L, const vfb_directional_bc *bc, cudaStream_t s)
+cudaError_t Launchers<S>::pressure(const vfb_level *L, const vfb_directional_bc *bc, cudaStream_t s,
+                                   const NodeAddr *box)
 {
     if (bc->number_of_bc_nodes == 0)
         return cudaSuccess;
     PressureArgs a;
     a.dist = L->distributions;
     a.n = L->number_of_nodes;
-    a.nbx = L->neighbor_x;
-    a.nby = L->neighbor_y;
-    a.nbz = L->neighbor_z;
+    a.nbx = box ? nullptr : L->neighbor_x;
+    a.nby = box ? nullptr : L->neighbor_y;
+    a.nbz = box ? nullptr : L->neighbor_z;
+    a.box = box ? *box : NodeAddr{ 0, 0, 0, 0 };
     a.k = bc->k;
     a.kN = bc->k_neighbor;
     a.rho_bc = bc->rho_bc;
@@ -202,16 +205,17 @@ void Launchers<S>::pool_domain(void *out, uint64_t dist_offset, uint64_t pitch, 
 
 template <class S>
 cudaError_t Launchers<S>::drag_lift(const vfb_level *L, const vfb_bc *bc, bool pre, double *dx, double *dy, double *dz,
-                                    cudaStream_t s)
+                                    cudaStream_t s, const NodeAddr *box)
 {
     if (bc->number_of_bc_nodes == 0)
         return cudaSuccess;
     DragArgs a;
     a.dist = L->distributions;
     a.n = L->number_of_nodes;
-    a.nbx = L->neighbor_x;
-    a.nby = L->neighbor_y;
-    a.nbz = L->neighbor_z;
+    a.nbx = box ? nullptr : L->neighbor_x;
+    a.nby = box ? nullptr : L->neighbor_y;
+    a.nbz = box ? nullptr : L->neighbor_z;
+    a.box = box ? *box : NodeAddr{ 0, 0, 0, 0 };
     a.k = bc->k;
     a.q27 = bc->q27;
     a.nbc = bc->number_of_bc_nodes;
@@ -265,6 +269,20 @@ cudaError_t Launchers<S>::scale(const vfb_level *coarse, const vfb_level *fine, 
         if (even) scale_cf_kernel<S, true><<<G, B, 0, s>>>(a);
         else scale_cf_kernel<S, false><<<G, B, 0, s>>>(a);
     }
+    return cudaGetLastError();
+}
+
+template <class S>
+cudaError_t Launchers<S>::inlet_perturbation(const void *base, void *vel, uint32_t n, uint64_t seed, uint64_t step,
+                                             double amplitude, cudaStream_t s)
+{
+    using C = typename Codec<S>::compute;
+    if (n == 0)
+        return cudaSuccess;
+    const C *b = static_cast<const C *>(base);
+    C *v = static_cast<C *>(vel);
+    inlet_perturbation_kernel<C><<<grid1d(n, 256), 256, 0, s>>>(b, b + n, b + 2 * (uint64_t)n, v, v + n, v + 2 * (uint64_t)n,
+                                                                n, seed, step, amplitude);
     return cudaGetLastError();
 }
 
