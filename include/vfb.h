@@ -316,6 +316,23 @@ int vfb_box_status(vfb_box *box, int32_t *device_status, void *stream);
    1 = direct loads, 2 = TMA-staged warp tiles (nx % 32 == 0),
    3 = per-thread asynchronous copies (F64 and F32 storage) */
 int vfb_box_set_kernel_variant(vfb_box *box, int32_t variant);
+/* Boundary conditions on a box, run by vfb_box_step in the order of vfb_simulation_run: velocity,
+   no-slip, geometry (with the drag's post part before it), parity toggle, the drag's pre part and
+   sum, pressure. Node indices are box indices k = x + nx (y + ny z) of fluid (mask nonzero) nodes;
+   q27[d * n + i], velocities and rho are host arrays of the box's real type, copied into the box.
+   variant: the VelocityBC / NoSlipBC / PressureBC enum values. A new call replaces the list. */
+enum { VFB_BOX_BC_VELOCITY = 0, VFB_BOX_BC_NOSLIP = 1, VFB_BOX_BC_GEOMETRY = 2 };
+int vfb_box_set_bc(vfb_box *box, int32_t kind, int32_t variant, const int32_t *k, const void *q27, uint32_t n,
+                   const void *ux, const void *uy, const void *uz);
+int vfb_box_add_pressure_bc(vfb_box *box, int32_t variant, const int32_t *k, const int32_t *k_neighbor, const void *rho,
+                            uint32_t n, int32_t direction);
+/* a seeded perturbation of the velocity BC every step: u_i(t) = u_i (1 + amplitude (2 U - 1)), U
+   uniform in [0, 1) from the counter-based Philox-4x32-10 generator keyed by seed and counted by
+   (BC node, step) */
+int vfb_box_set_velocity_perturbation(vfb_box *box, uint64_t seed, double amplitude);
+/* FP64 drag/lift on the geometry list every step (DragLiftPost27 / DragLiftPre27 / calcDragLift):
+   the force of step t (counted from this call) into force_history[3 * (t % history_steps)], device */
+int vfb_box_set_drag_lift(vfb_box *box, double *force_history, uint32_t history_steps);
 /* number of kernels vfb_box_step has launched for this box so far (collision and reductions) */
 int vfb_box_kernel_launches(const vfb_box *box, uint64_t *count);
 /* launch shape of the per-thread asynchronous-copy kernel: resident blocks per SM (0 = 3) and the

@@ -235,3 +235,44 @@ def test_drag_lift_history_ring_keeps_the_last_steps(oracle, cuda):
     got = sim.drag_lift_history()
     want = np.array(orc.drag_history)[-7:]
     assert np.all(np.abs(got - want) <= 1e-12 * np.abs(want).max(axis=0))
+
+
+def test_box_with_boundary_conditions_matches_the_list_path(oracle, cuda):
+    """Box.from_grid: the same level as a structured box with BC lists in box indices computes the
+    list path's fields and drag bit for bit (exact arithmetic)."""
+    from virtualfluids_b200 import Box
+    g, bcf = _cube_channel()
+    steps = 40
+    sim = Simulation(make_para(1.8, N.STORAGE_F64, N.ARITH_EXACT), g, bcf)
+    sim.init()
+    sim.enable_drag_lift(history_steps=steps)
+    sim.run(steps)
+    box = Box.from_grid(g, sim.para.omega, bcf, storage="f64", arith="exact")
+    Dx, Dy, Dz = g.dims
+    z = np.zeros(Dx * Dy * Dz)
+    box.init(z, z, z, z)
+    box.enable_drag_lift(history_steps=steps)
+    box.step(steps)
+    f = box.fields()
+    m = sim.macroscopic()
+    fl = g.geo[1:] == N.GEO_FLUID
+    for key in ("rho", "vx", "vy", "vz"):
+        assert np.array_equal(f[key][fl], m[key][1:][fl]), key
+    assert np.array_equal(box.drag_lift_history(), sim.drag_lift_history())
+
+
+def test_box_inlet_perturbation_is_seeded(cuda):
+    from virtualfluids_b200 import Box
+    g, bcf = _cube_channel()
+    runs = []
+    for seed in (7, 7, 8):
+        box = Box.from_grid(g, 1.8, bcf, storage="f32")
+        Dx, Dy, Dz = g.dims
+        z = np.zeros(Dx * Dy * Dz)
+        box.init(z, z, z, z)
+        box.set_velocity_perturbation(seed, 0.01)
+        box.step(30)
+        runs.append(box.fields()["vx"])
+    assert np.array_equal(runs[0], runs[1])
+    assert not np.array_equal(runs[0], runs[2])
+    assert np.abs(runs[0] - runs[2]).max() < 1e-3

@@ -49,6 +49,7 @@ PRESSURE_OUTFLOW_NON_REFLECTIVE = 2
 PRESSURE_OUTFLOW_NON_REFLECTIVE_PRESSURE_CORRECTION = 3
 PRESSURE_NOT_SPECIFIED = 4
 # GridScalingFactory::GridScaling (GridScalingFactory.h:50-56)
+BOX_BC_VELOCITY, BOX_BC_NOSLIP, BOX_BC_GEOMETRY = 0, 1, 2
 SCALE_COMPRESSIBLE = 0
 SCALE_NOT_SPECIFIED = 1
 
@@ -170,6 +171,12 @@ SIGNATURES = {
     "vfb_box_fields": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "vfb_box_status": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.c_void_p]),
     "vfb_box_set_kernel_variant": (C.c_int, [C.c_void_p, C.c_int32]),
+    "vfb_box_set_bc": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
+                                 C.c_void_p, C.c_void_p]),
+    "vfb_box_add_pressure_bc": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                          C.c_int32]),
+    "vfb_box_set_velocity_perturbation": (C.c_int, [C.c_void_p, C.c_uint64, C.c_double]),
+    "vfb_box_set_drag_lift": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
     "vfb_box_kernel_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     "vfb_box_set_launch_shape": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "vfb_box_populations": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64),

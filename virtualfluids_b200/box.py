@@ -71,6 +71,8 @@ class Box:
 
     def step(self, steps: int, energy=None, stream=None):
         """Advance; energy: None, host float64 array [steps, 2] or device float64 tensor."""
+        if getattr(self, "_drag_len", 0):
+            self._drag_done += int(steps)
         if energy is None:
             N.check(N.lib().vfb_box_step(self._h, int(steps), None, 0, stream))
         elif isinstance(energy, np.ndarray):
@@ -99,6 +101,72 @@ class Box:
         """'auto', 'direct' (plain loads), 'tma' (bulk copies staged in shared memory) or 'async'
         (per-thread asynchronous copies of the next node)."""
         N.check(N.lib().vfb_box_set_kernel_variant(self._h, {"auto": 0, "direct": 1, "tma": 2, "async": 3}[variant]))
+
+    # -- boundary conditions (vfb_box_set_bc / vfb_box_add_pressure_bc) -------------------------
+    def set_bc(self, kind: str, k, q27, variant, velocity=None):
+        """kind: 'velocity', 'noslip' or 'geometry'; k: box node indices; q27: (27, n) q values;
+        velocity: (3, n) wall velocities for 'velocity'; variant: the factory enum value."""
+        kk = np.ascontiguousarray(np.asarray(k, dtype=np.int32).reshape(-1))
+        n = kk.size
+        q = np.ascontiguousarray(np.asarray(q27, dtype=self.real).reshape(27, n))
+        vel = [None, None, None]
+        if kind == "velocity":
+            v = np.asarray(velocity, dtype=self.real).reshape(3, n)
+            vel = [np.ascontiguousarray(v[a]) for a in range(3)]
+        code = {"velocity": N.BOX_BC_VELOCITY, "noslip": N.BOX_BC_NOSLIP, "geometry": N.BOX_BC_GEOMETRY}[kind]
+        N.check(N.lib().vfb_box_set_bc(self._h, code, int(variant), kk.ctypes.data, q.ctypes.data, n,
+                                       *(a.ctypes.data if a is not None else None for a in vel)))
+        if kind == "geometry":
+            self._geometry_nodes = n
+
+    def add_pressure_bc(self, k, k_neighbor, rho, direction, variant=N.PRESSURE_NON_EQUILIBRIUM_COMPRESSIBLE):
+        kk = np.ascontiguousarray(np.asarray(k, dtype=np.int32).reshape(-1))
+        kn = np.ascontiguousarray(np.asarray(k_neighbor, dtype=np.int32).reshape(-1))
+        r = np.ascontiguousarray(np.broadcast_to(np.asarray(rho, dtype=self.real), kk.shape))
+        N.check(N.lib().vfb_box_add_pressure_bc(self._h, int(variant), kk.ctypes.data, kn.ctypes.data, r.ctypes.data,
+                                                kk.size, int(direction)))
+
+    def set_velocity_perturbation(self, seed: int, amplitude: float):
+        N.check(N.lib().vfb_box_set_velocity_perturbation(self._h, int(seed), float(amplitude)))
+
+    def enable_drag_lift(self, history_steps: int, device="cuda"):
+        import torch
+        self._drag_hist = torch.zeros(3 * int(history_steps), dtype=torch.float64, device=device)
+        self._drag_len = int(history_steps)
+        self._drag_done = 0
+        N.check(N.lib().vfb_box_set_drag_lift(self._h, C.c_void_p(self._drag_hist.data_ptr()), self._drag_len))
+
+    def drag_lift_history(self):
+        """(steps, 3) FP64 forces of the steps since enable_drag_lift (the last history_steps)."""
+        N.check(N.lib().vfb_synchronize(None))
+        h = self._drag_hist.view(self._drag_len, 3).cpu().numpy()
+        done = self._drag_done
+        if done <= self._drag_len:
+            return h[:done].copy()
+        start = done % self._drag_len
+        return np.concatenate([h[start:], h[:start]])
+
+    @classmethod
+    def from_grid(cls, grid, omega, bc_factory, storage="f64", arith="fast", forces=(0.0, 0.0, 0.0)):
+        """The structured-box form of a ListGrid level: the box spans the grid with its stopper shell
+        (box node k = list node k + 1), the mask marks the fluid nodes, and the grid's BC lists
+        become box BC lists with the factory's kernels. It computes what the list form computes."""
+        Dx, Dy, Dz = grid.dims
+        mask = (grid.geo[1:] == N.GEO_FLUID).astype(np.uint8)
+        box = cls(Dx, Dy, Dz, omega, periodic=grid.periodic, storage=storage, arith=arith, forces=forces, mask=mask)
+        for kind, variant in (("velocity", bc_factory.velocity), ("noslip", bc_factory.noslip),
+                              ("geometry", bc_factory.geometry)):
+            m = grid.merged(kind)
+            if m is None:
+                continue
+            k, q, vel = m
+            box.set_bc(kind, k.astype(np.int64) - 1, q, int(variant), velocity=vel if kind == "velocity" else None)
+        from .grid import SIDE_DIR
+        for b in grid.bcs:
+            if b.kind == "pressure":
+                box.add_pressure_bc(b.k.astype(np.int64) - 1, b.k_neighbor.astype(np.int64) - 1, b.rho,
+                                    SIDE_DIR[b.side], variant=int(bc_factory.pressure))
+        return box
 
     def kernel_launches(self) -> int:
         """Kernels vfb_box_step has launched for this box so far."""

@@ -844,15 +844,51 @@ struct vfb_box {
     void *staging = nullptr;        // 4 real fields for init and output
     int *status = nullptr;          // device status word of the kernels (DeviceError)
     uint64_t launches = 0;          // kernels this box has launched
+    uint64_t steps = 0;             // time steps done (counter of the inlet perturbation)
+    // boundary conditions in box indices (device copies owned by the box)
+    struct List {
+        vfb_bc bc{};
+        vfb_bc_fn fn = nullptr;
+        int kind = -1;              // vfb::BCKind, -1 = no kernel
+        std::vector<void *> owned;
+    } velocity, noslip, geometry;
+    struct Pressure {
+        vfb_directional_bc bc{};
+        std::vector<void *> owned;
+    };
+    std::vector<Pressure> pressure;
+    void *velocity_base = nullptr;  // unperturbed inlet velocities (3 x n reals)
+    uint64_t perturb_seed = 0;
+    double perturb_amplitude = 0.0;
+    double *drag_work = nullptr;    // 6 n doubles + sum scratch
+    double *drag_history = nullptr;
+    uint32_t drag_history_len = 0;
+    uint64_t drag_steps = 0;
 };
 
 namespace {
 constexpr uint32_t kRingSteps = 1024;
 
+void free_list(vfb_box::List &l)
+{
+    for (void *p : l.owned)
+        cudaFree(p);
+    l = vfb_box::List();
+}
+
 void box_free(vfb_box *b)
 {
     if (!b)
         return;
+    free_list(b->velocity);
+    free_list(b->noslip);
+    free_list(b->geometry);
+    for (auto &p : b->pressure)
+        for (void *q : p.owned)
+            cudaFree(q);
+    b->pressure.clear();
+    cudaFree(b->velocity_base);
+    cudaFree(b->drag_work);
     cudaFree(b->dist);
     cudaFree(b->mask);
     cudaFree(b->partials);
@@ -984,6 +1020,97 @@ int vfb_box_init(vfb_box *box, const void *rho, const void *ux, const void *uy, 
     return cuda_status(e, "box init");
 }
 
+namespace {
+
+// the box as a level of the boundary, drag and init launchers (plane stride = pitch; neighbours by
+// index arithmetic)
+vfb_level box_level(const vfb_box *b)
+{
+    vfb_level L{};
+    L.storage = b->desc.storage;
+    L.arith = b->desc.arith;
+    L.is_even_timestep = b->even ? 1 : 0;
+    L.number_of_nodes = b->state.pitch;
+    L.distributions = b->dist;
+    L.omega = b->desc.omega;
+    return L;
+}
+
+vfb::NodeAddr box_addr(const vfb_box *b)
+{
+    return vfb::NodeAddr{ b->desc.nx, b->desc.ny, b->desc.nz,
+                          (b->desc.periodic_x ? 1 : 0) | (b->desc.periodic_y ? 2 : 0) | (b->desc.periodic_z ? 4 : 0) };
+}
+
+cudaError_t box_run_list(vfb_box *b, const vfb_box::List &l, cudaStream_t s)
+{
+    if (l.kind < 0 || l.bc.number_of_bc_nodes == 0)
+        return cudaSuccess;
+    const vfb_level L = box_level(b);
+    const vfb::NodeAddr a = box_addr(b);
+    ++b->launches;
+    return VFB_DISPATCH(b->desc.storage, b->desc.arith, LA::bc(&L, &l.bc, l.kind, s, &a));
+}
+
+// one step's boundary work around the collision, in the order of vfb_simulation_run
+cudaError_t box_post_collision(vfb_box *b, cudaStream_t s)
+{
+    cudaError_t e = cudaSuccess;
+    if (b->velocity_base && b->velocity.bc.number_of_bc_nodes) {
+        e = VFB_DISPATCH(b->desc.storage, b->desc.arith,
+                         LA::inlet_perturbation(b->velocity_base, const_cast<void *>(b->velocity.bc.vx),
+                                                b->velocity.bc.number_of_bc_nodes, b->perturb_seed, b->steps,
+                                                b->perturb_amplitude, s));
+        ++b->launches;
+    }
+    if (e == cudaSuccess)
+        e = box_run_list(b, b->velocity, s);
+    if (e == cudaSuccess)
+        e = box_run_list(b, b->noslip, s);
+    const uint32_t ng = b->geometry.bc.number_of_bc_nodes;
+    if (e == cudaSuccess && b->drag_work && ng) {
+        const vfb_level L = box_level(b);
+        const vfb::NodeAddr a = box_addr(b);
+        double *w = b->drag_work;
+        e = VFB_DISPATCH(b->desc.storage, b->desc.arith,
+                         LA::drag_lift(&L, &b->geometry.bc, false, w + 3 * (size_t)ng, w + 4 * (size_t)ng,
+                                       w + 5 * (size_t)ng, s, &a));
+        ++b->launches;
+    }
+    if (e == cudaSuccess)
+        e = box_run_list(b, b->geometry, s);
+    return e;
+}
+
+cudaError_t box_pre_collision(vfb_box *b, cudaStream_t s)
+{
+    cudaError_t e = cudaSuccess;
+    const uint32_t ng = b->geometry.bc.number_of_bc_nodes;
+    if (b->drag_work && ng) {
+        const vfb_level L = box_level(b);
+        const vfb::NodeAddr a = box_addr(b);
+        double *w = b->drag_work;
+        e = VFB_DISPATCH(b->desc.storage, b->desc.arith,
+                         LA::drag_lift(&L, &b->geometry.bc, true, w, w + ng, w + 2 * (size_t)ng, s, &a));
+        const double *pre[3] = { w, w + ng, w + 2 * (size_t)ng };
+        const double *post[3] = { w + 3 * (size_t)ng, w + 4 * (size_t)ng, w + 5 * (size_t)ng };
+        if (e == cudaSuccess)
+            e = vfb::drag_lift_sum(pre, post, ng, w + 6 * (size_t)ng,
+                                   b->drag_history + 3 * (b->drag_steps % b->drag_history_len), s);
+        b->launches += 3;
+        ++b->drag_steps;
+    }
+    for (size_t i = 0; i < b->pressure.size() && e == cudaSuccess; ++i) {
+        const vfb_level L = box_level(b);
+        const vfb::NodeAddr a = box_addr(b);
+        e = VFB_DISPATCH(b->desc.storage, b->desc.arith, LA::pressure(&L, &b->pressure[i].bc, s, &a));
+        ++b->launches;
+    }
+    return e;
+}
+
+} // namespace
+
 int vfb_box_step(vfb_box *box, uint32_t steps, double *energy, int32_t energy_on_host, void *stream)
 {
     if (!box)
@@ -1004,7 +1131,12 @@ int vfb_box_step(vfb_box *box, uint32_t steps, double *energy, int32_t energy_on
                 e = vfb::reduce_partials_wide(box->partials, n_partials, box->partials + 2 * box->blocks, dst, s);
                 box->launches += n_partials > vfb::kReduceDirect ? 2 : 1;
             }
+            if (e == cudaSuccess)
+                e = box_post_collision(box, s);
             box->even = !box->even;
+            if (e == cudaSuccess)
+                e = box_pre_collision(box, s);
+            ++box->steps;
         }
         if (e == cudaSuccess && energy && energy_on_host)
             e = cudaMemcpyAsync(energy + 2 * (uint64_t)done, box->energy_ring, 2 * sizeof(double) * chunk,
@@ -1058,6 +1190,170 @@ int vfb_box_set_kernel_variant(vfb_box *box, int32_t variant)
     if (variant == 2 && box->desc.nx % 32 != 0)
         return fail(VFB_ERR_UNSUPPORTED, "the TMA-staged kernel needs nx % 32 == 0");
     box->state.variant = variant;
+    return VFB_OK;
+}
+
+int vfb_box_set_bc(vfb_box *box, int32_t kind, int32_t variant, const int32_t *k, const void *q27, uint32_t n,
+                   const void *ux, const void *uy, const void *uz)
+{
+    if (!box)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL box");
+    if (kind != VFB_BOX_BC_VELOCITY && kind != VFB_BOX_BC_NOSLIP && kind != VFB_BOX_BC_GEOMETRY)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "kind must be VFB_BOX_BC_VELOCITY, _NOSLIP or _GEOMETRY");
+    if (n && (!k || !q27))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "node indices or q are NULL");
+    if (kind == VFB_BOX_BC_VELOCITY && n && (!ux || !uy || !uz))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "a velocity BC needs the wall velocities");
+    int bc_kind = -1;
+    if (kind == VFB_BOX_BC_VELOCITY) {
+        switch (variant) {
+        case VFB_VELOCITY_BOUNCE_BACK: bc_kind = vfb::kVelocityBB; break;
+        case VFB_VELOCITY_INTERPOLATED_COMPRESSIBLE: bc_kind = vfb::kVelocityInterp; break;
+        case VFB_VELOCITY_NOT_SPECIFIED: break;
+        default: return fail(VFB_ERR_UNSUPPORTED, "velocity BC variant not built for boxes");
+        }
+    } else {
+        switch (variant) {
+        case VFB_NOSLIP_DELAY_BOUNCE_BACK: break;
+        case VFB_NOSLIP_BOUNCE_BACK: bc_kind = vfb::kNoSlipBB; break;
+        case VFB_NOSLIP_INTERPOLATED_COMPRESSIBLE: bc_kind = vfb::kNoSlipInterp; break;
+        default: return fail(VFB_ERR_UNSUPPORTED, "no-slip BC variant not built for boxes");
+        }
+    }
+    const uint64_t nn = (uint64_t)box->desc.nx * box->desc.ny * box->desc.nz;
+    for (uint32_t i = 0; i < n; ++i)
+        if (k[i] < 0 || (uint64_t)k[i] >= nn)
+            return fail(VFB_ERR_INVALID_ARGUMENT, "a BC node index lies outside the box");
+    vfb_box::List &l = kind == VFB_BOX_BC_VELOCITY ? box->velocity : kind == VFB_BOX_BC_NOSLIP ? box->noslip : box->geometry;
+    free_list(l);
+    if (kind == VFB_BOX_BC_VELOCITY) {
+        cudaFree(box->velocity_base);
+        box->velocity_base = nullptr;
+    }
+    if (kind == VFB_BOX_BC_GEOMETRY) {
+        cudaFree(box->drag_work);
+        box->drag_work = nullptr;
+        box->drag_history = nullptr;
+    }
+    const size_t rb = real_bytes(box->desc.storage);
+    void *dk = nullptr, *dq = nullptr, *dv = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (n) {
+        e = cudaMalloc(&dk, n * sizeof(int32_t));
+        if (e == cudaSuccess)
+            e = cudaMemcpy(dk, k, n * sizeof(int32_t), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMalloc(&dq, (size_t)27 * n * rb);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(dq, q27, (size_t)27 * n * rb, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && kind == VFB_BOX_BC_VELOCITY) {
+            e = cudaMalloc(&dv, (size_t)3 * n * rb);
+            const void *src[3] = { ux, uy, uz };
+            for (int a = 0; a < 3 && e == cudaSuccess; ++a)
+                e = cudaMemcpy(static_cast<char *>(dv) + a * n * rb, src[a], n * rb, cudaMemcpyHostToDevice);
+        }
+    }
+    if (e != cudaSuccess) {
+        cudaFree(dk);
+        cudaFree(dq);
+        cudaFree(dv);
+        return cuda_status(e, "box BC upload");
+    }
+    l.owned = { dk, dq, dv };
+    l.bc.k = static_cast<const int32_t *>(dk);
+    l.bc.q27 = dq;
+    l.bc.number_of_bc_nodes = n;
+    if (dv) {
+        l.bc.vx = dv;
+        l.bc.vy = static_cast<char *>(dv) + n * rb;
+        l.bc.vz = static_cast<char *>(dv) + 2 * n * rb;
+    }
+    l.kind = bc_kind;
+    return VFB_OK;
+}
+
+int vfb_box_add_pressure_bc(vfb_box *box, int32_t variant, const int32_t *k, const int32_t *k_neighbor, const void *rho,
+                            uint32_t n, int32_t direction)
+{
+    if (!box)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL box");
+    if (variant != VFB_PRESSURE_NON_EQUILIBRIUM_COMPRESSIBLE)
+        return fail(VFB_ERR_UNSUPPORTED, "pressure BC variant not built for boxes");
+    if (direction < VFB_DIR_P00 || direction > VFB_DIR_00M)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "direction must be one of the six face directions");
+    if (n && (!k || !k_neighbor || !rho))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "pressure BC arrays are NULL");
+    const uint64_t nn = (uint64_t)box->desc.nx * box->desc.ny * box->desc.nz;
+    for (uint32_t i = 0; i < n; ++i)
+        if (k[i] < 0 || (uint64_t)k[i] >= nn || k_neighbor[i] < 0 || (uint64_t)k_neighbor[i] >= nn)
+            return fail(VFB_ERR_INVALID_ARGUMENT, "a pressure BC node index lies outside the box");
+    const size_t rb = real_bytes(box->desc.storage);
+    vfb_box::Pressure p;
+    void *dk = nullptr, *dn = nullptr, *dr = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (n) {
+        e = cudaMalloc(&dk, n * sizeof(int32_t));
+        if (e == cudaSuccess) e = cudaMemcpy(dk, k, n * sizeof(int32_t), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMalloc(&dn, n * sizeof(int32_t));
+        if (e == cudaSuccess) e = cudaMemcpy(dn, k_neighbor, n * sizeof(int32_t), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMalloc(&dr, n * rb);
+        if (e == cudaSuccess) e = cudaMemcpy(dr, rho, n * rb, cudaMemcpyHostToDevice);
+    }
+    if (e != cudaSuccess) {
+        cudaFree(dk);
+        cudaFree(dn);
+        cudaFree(dr);
+        return cuda_status(e, "box pressure BC upload");
+    }
+    p.owned = { dk, dn, dr };
+    p.bc = vfb_directional_bc{ static_cast<const int32_t *>(dk), static_cast<const int32_t *>(dn), dr, n, direction };
+    box->pressure.push_back(p);
+    return VFB_OK;
+}
+
+int vfb_box_set_velocity_perturbation(vfb_box *box, uint64_t seed, double amplitude)
+{
+    if (!box)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL box");
+    const uint32_t n = box->velocity.bc.number_of_bc_nodes;
+    if (!n)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "set the velocity BC first");
+    if (!(amplitude >= 0.0 && amplitude < 1.0))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "amplitude must lie in [0, 1)");
+    const size_t bytes = (size_t)3 * n * real_bytes(box->desc.storage);
+    if (!box->velocity_base) {
+        cudaError_t e = cudaMalloc(&box->velocity_base, bytes);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(box->velocity_base, box->velocity.bc.vx, bytes, cudaMemcpyDeviceToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(box->velocity_base);
+            box->velocity_base = nullptr;
+            return cuda_status(e, "box velocity perturbation");
+        }
+    }
+    box->perturb_seed = seed;
+    box->perturb_amplitude = amplitude;
+    return VFB_OK;
+}
+
+int vfb_box_set_drag_lift(vfb_box *box, double *force_history, uint32_t history_steps)
+{
+    if (!box)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL box");
+    const uint32_t ng = box->geometry.bc.number_of_bc_nodes;
+    if (!ng)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "drag and lift need a geometry BC with nodes");
+    if (!force_history || !history_steps)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "drag and lift need a force history of at least one step");
+    if (!box->drag_work) {
+        const cudaError_t e = cudaMalloc((void **)&box->drag_work,
+                                         6 * (size_t)ng * sizeof(double) + vfb_drag_lift_workspace_bytes(ng));
+        if (e != cudaSuccess)
+            return cuda_status(e, "box drag workspace");
+    }
+    box->drag_history = force_history;
+    box->drag_history_len = history_steps;
+    box->drag_steps = 0;
     return VFB_OK;
 }
 

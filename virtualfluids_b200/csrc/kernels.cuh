@@ -145,7 +145,7 @@ __device__ __forceinline__ void scatter_post(S *__restrict__ base, uint64_t n, c
 {
 #pragma unroll
     for (int d = 0; d < 27; ++d)
-        Codec<S>::store(base + (uint64_t)plane<EVEN>(d) * n + nodes[shift_class(d)], f[inv(d)], d);
+        Codec<S>::store_at(base, (uint64_t)plane<EVEN>(d) * n + nodes[shift_class(d)], f[inv(d)], d);
 }
 
 // getPostCollisionDistribution (KernelUtilities.h:283): post[d] leaves the node along d
@@ -607,7 +607,7 @@ __global__ void __launch_bounds__(128) bc_bounce_back_kernel(BCArgs a)
                 v = v + coef * cu;
             }
             // next parity: slot of direction e at its own read node
-            Codec<S>::store(base + (uint64_t)plane<!EVEN>(e) * a.n + nodes[shift_class(e)], v, e);
+            Codec<S>::store_at(base, (uint64_t)plane<!EVEN>(e) * a.n + nodes[shift_class(e)], v, e);
         }
     }
 }
@@ -691,7 +691,7 @@ __global__ void __launch_bounds__(128) bc_interpolated_kernel(BCArgs a)
                   + (q * (f + fi)) / (C(1) + q);
             }
             const int e = inv(d);
-            Codec<S>::store(base + (uint64_t)plane<!EVEN>(e) * a.n + nodes[shift_class(e)], v, e);
+            Codec<S>::store_at(base, (uint64_t)plane<!EVEN>(e) * a.n + nodes[shift_class(e)], v, e);
         }
     }
 }
@@ -736,7 +736,7 @@ __global__ void __launch_bounds__(128) bc_pressure_neq_kernel(PressureArgs a)
         v = v + feq_shifted<C>(d, rbc, vx, vy, vz, cusq);
         const int c = axis == 0 ? cx(d) : (axis == 1 ? cy(d) : cz(d));
         if (c != sgn)
-            Codec<S>::store(base + (uint64_t)plane<EVEN>(d) * a.n + nk[shift_class(d)], v, d);
+            Codec<S>::store_at(base, (uint64_t)plane<EVEN>(d) * a.n + nk[shift_class(d)], v, d);
     }
 }
 
@@ -773,7 +773,7 @@ __global__ void __launch_bounds__(128) init_list_kernel(void *dist, uint64_t n, 
             const C cu = cdot_rt<C>(d, vx, vy, vz);
             v = weight_t<C>(d) * (drho + (C(1) + drho) * (C(3) * cu + C(4.5) * cu * cu - cu_sq));
         }
-        Codec<S>::store(base + (uint64_t)plane<EVEN>(d) * n + nodes[shift_class(d)], v, d);
+        Codec<S>::store_at(base, (uint64_t)plane<EVEN>(d) * n + nodes[shift_class(d)], v, d);
     }
 }
 
@@ -808,7 +808,7 @@ __global__ void __launch_bounds__(128) init_box_kernel(BoxCollideArgs<typename C
             const C cu = cdot_rt<C>(d, vx, vy, vz);
             v = weight_t<C>(d) * (drho + (C(1) + drho) * (C(3) * cu + C(4.5) * cu * cu - cu_sq));
         }
-        Codec<S>::store(base + (uint64_t)plane<EVEN>(d) * a.pitch + nodes[shift_class(d)], v, d);
+        Codec<S>::store_at(base, (uint64_t)plane<EVEN>(d) * a.pitch + nodes[shift_class(d)], v, d);
     }
 }
 
@@ -1023,7 +1023,7 @@ __global__ void __launch_bounds__(128) scale_cf_kernel(ScaleArgs a)
     S *fine = static_cast<S *>(a.dist_fine);
 #pragma unroll
     for (int d = 0; d < 27; ++d)
-        Codec<S>::store(fine + (uint64_t)plane<true>(d) * a.n_fine + nodes[shift_class(d)], f[d], d);
+        Codec<S>::store_at(fine, (uint64_t)plane<true>(d) * a.n_fine + nodes[shift_class(d)], f[d], d);
 }
 
 // scaleFineToCoarseCompressible_Device: moments of the fine cell at the even parity with
@@ -1059,7 +1059,7 @@ __global__ void __launch_bounds__(128) scale_fc_kernel(ScaleArgs a)
 #pragma unroll
     for (int d = 0; d < 27; ++d)
         if ((d & 7) == corner)
-            Codec<S>::store(coarse + (uint64_t)plane<COARSE_EVEN>(d) * a.n_coarse + nodes[shift_class(d)], f[d], d);
+            Codec<S>::store_at(coarse, (uint64_t)plane<COARSE_EVEN>(d) * a.n_coarse + nodes[shift_class(d)], f[d], d);
 }
 
 

@@ -10,12 +10,15 @@
 // Dividing by the lattice weight puts all 27 directions on one scale, O(drho + 3 c.u), so the
 // 16-bit formats spend their exponent range on the same magnitudes for every direction and
 // small corner populations do not fall into the subnormal range. 1/w is 27/8, 27/2, 54 or 216.
+// The 16-bit formats round stochastically (below).
 //
 // The direction argument d is always a loop index of a fully unrolled 27-direction loop, so
 // weight(d) folds to a constant.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+
+#include <cstdint>
 
 #include "lattice.cuh"
 
@@ -31,6 +34,7 @@ struct Codec<double> {
     using compute = double;
     __device__ __forceinline__ static double load(const double *p, int) { return *p; }
     __device__ __forceinline__ static void store(double *p, double v, int) { *p = v; }
+    __device__ __forceinline__ static void store_at(double *base, uint64_t off, double v, int) { base[off] = v; }
 };
 
 template <>
@@ -38,13 +42,46 @@ struct Codec<float> {
     using compute = float;
     __device__ __forceinline__ static float load(const float *p, int) { return *p; }
     __device__ __forceinline__ static void store(float *p, float v, int) { *p = v; }
+    __device__ __forceinline__ static void store_at(float *base, uint64_t off, float v, int) { base[off] = v; }
 };
+
+// Stochastic rounding of the 16-bit stores. Rounding to nearest drops every change smaller than
+// half a unit in the last place, so flows driven by small forces stall (a duct under a body force
+// of 1e-6 per step ends percents away from FP64); rounding up or down with probability
+// proportional to the distance keeps every store unbiased. The random bits are a hash of the
+// value's bits and the slot's offset in its population array, so a run stays reproducible bit for
+// bit (the same domain computes the same bits wherever its array lives), and they change whenever
+// the value does. The conversion is sm_100a's cvt.rs (operand a lands in the upper half).
+__device__ __forceinline__ uint32_t sr_bits(float v, uint64_t off)
+{
+    // two odd multipliers carry the value's (noisy) low mantissa bits and the slot offset into
+    // every bit position; cheap, because the 16-bit forms are bound by arithmetic
+    return (__float_as_uint(v) * 0x9E3779B1u) ^ ((uint32_t)off * 0x85EBCA77u) ^ (uint32_t)(off >> 32);
+}
+
+__device__ __forceinline__ __half half_sr(float v, uint32_t rbits)
+{
+    uint32_t d;
+    asm("cvt.rs.f16x2.f32 %0, %1, %1, %2;" : "=r"(d) : "f"(v), "r"(rbits));
+    return __ushort_as_half((unsigned short)(d >> 16));
+}
+
+__device__ __forceinline__ __nv_bfloat16 bf16_sr(float v, uint32_t rbits)
+{
+    uint32_t d;
+    asm("cvt.rs.bf16x2.f32 %0, %1, %1, %2;" : "=r"(d) : "f"(v), "r"(rbits));
+    return __ushort_as_bfloat16((unsigned short)(d >> 16));
+}
 
 template <>
 struct Codec<__half> {
     using compute = float;
     __device__ __forceinline__ static float load(const __half *p, int d) { return __half2float(*p) * float(weight(d)); }
-    __device__ __forceinline__ static void store(__half *p, float v, int d) { *p = __float2half_rn(v * float(1.0 / weight(d))); }
+    __device__ __forceinline__ static void store_at(__half *base, uint64_t off, float v, int d)
+    {
+        const float s = v * float(1.0 / weight(d));
+        base[off] = half_sr(s, sr_bits(s, off));
+    }
 };
 
 template <>
@@ -54,9 +91,10 @@ struct Codec<__nv_bfloat16> {
     {
         return __bfloat162float(*p) * float(weight(d));
     }
-    __device__ __forceinline__ static void store(__nv_bfloat16 *p, float v, int d)
+    __device__ __forceinline__ static void store_at(__nv_bfloat16 *base, uint64_t off, float v, int d)
     {
-        *p = __float2bfloat16_rn(v * float(1.0 / weight(d)));
+        const float s = v * float(1.0 / weight(d));
+        base[off] = bf16_sr(s, sr_bits(s, off));
     }
 };
 

@@ -43,7 +43,7 @@ class SideBC:
     kind: str                       # "noslip", "velocity", "pressure", "geometry"
     k: np.ndarray                   # int32 node indices
     q: np.ndarray                   # float64 [27, n]
-    velocity: tuple = (0.0, 0.0, 0.0)
+    velocity: tuple | np.ndarray = (0.0, 0.0, 0.0)   # constant, or (3, n) per node
     rho: float = 0.0
     k_neighbor: np.ndarray | None = None
 
@@ -133,10 +133,13 @@ class ListGrid:
         return nx_, ny_, nz_
 
     def add_side(self, side, kind, velocity=(0.0, 0.0, 0.0), rho=0.0):
-        """Set a BC on a side, in the order the reference's app sets them."""
+        """Set a BC on a side, in the order the reference's app sets them. velocity may be a
+        function of the side nodes' fluid-box coordinates (x, y, z) returning (ux, uy, uz) arrays."""
         axis, sign = SIDES[side]
         nodes = self._side_nodes(side)
         x, y, z = self.coords[0, nodes], self.coords[1, nodes], self.coords[2, nodes]
+        if callable(velocity):
+            velocity = np.array([np.broadcast_to(np.asarray(c, dtype=np.float64), x.shape) for c in velocity(x, y, z)])
         q = np.full((27, nodes.size), -1.0)
         normal = np.zeros(3, dtype=int)
         normal[axis] = sign
@@ -159,7 +162,8 @@ class ListGrid:
                 on_other = self.is_stopper(*ocoords)
                 qd = np.where((qd == 0.5) & on_other, -1.0, qd)
             q[d] = qd
-        bc = SideBC(side=side, kind=kind, k=nodes.astype(np.int32), q=q, velocity=tuple(velocity), rho=rho)
+        vel = velocity if isinstance(velocity, np.ndarray) else tuple(velocity)
+        bc = SideBC(side=side, kind=kind, k=nodes.astype(np.int32), q=q, velocity=vel, rho=rho)
         if kind == "pressure":
             inward = [x.copy(), y.copy(), z.copy()]
             inward[axis] = inward[axis] - sign
@@ -192,7 +196,13 @@ class ListGrid:
             b.k, b.q = b.k[keep], b.q[:, keep]
             if b.k_neighbor is not None:
                 b.k_neighbor = b.k_neighbor[keep]
-        nodes = self.fluid.astype(np.int64)
+        near = np.ones(self.fluid.size, dtype=bool)
+        for a in range(3):
+            ca = self.coords[a, self.fluid]
+            near &= (ca >= np.floor(lo[a]) - 1) & (ca <= np.ceil(hi[a]) + 1)
+        if any(self.periodic):
+            near[:] = True          # wrapped neighbours can reach the box from the far side
+        nodes = self.fluid[near].astype(np.int64)
         x, y, z = (self.coords[a, nodes] for a in range(3))
         q = np.full((27, nodes.size), -1.0)
         for d in range(1, 27):
@@ -220,5 +230,7 @@ class ListGrid:
             return None
         k = np.concatenate([b.k for b in parts])
         q = np.concatenate([b.q for b in parts], axis=1)
-        vel = np.concatenate([np.tile(np.array(b.velocity)[:, None], (1, b.k.size)) for b in parts], axis=1)
+        vel = np.concatenate([np.asarray(b.velocity, dtype=np.float64) if isinstance(b.velocity, np.ndarray)
+                              else np.tile(np.array(b.velocity, dtype=np.float64)[:, None], (1, b.k.size))
+                              for b in parts], axis=1)
         return k, q, vel

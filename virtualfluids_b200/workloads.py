@@ -156,3 +156,29 @@ def porous_block(side, seed, porosity=None, radius=(3.0, 8.0), max_tries=40000):
     mask = (~solid).astype(np.uint8).reshape(-1)
     spheres = [(float(c[0]), float(c[1]), float(c[2]), float(r)) for c, r in zip(centres, radii)]
     return mask, spheres, float(mask.mean())
+
+
+def cube_duct(nx=512, ny=256, nz=256, cube=32, x0=128, u_max=0.05, re=3000.0):
+    """Config 3: duct flow past a wall-mounted cube. Fluid box nx x ny x nz (stopper shell around
+    it); no-slip walls on the y and z faces (interpolated bounce-back, q = 1/2); the inlet at x = 0
+    carries u_x = u_max 16 eta (1 - eta) zeta (1 - zeta) (eta, zeta the cross-section coordinates
+    between the wall planes); the outlet at x = nx - 1 holds drho = 0 (non-equilibrium pressure BC,
+    direction P00); the cube of side `cube` sits on the z = 0 wall, x in [x0, x0 + cube), centred
+    in y, with its faces half-way between nodes (exact-geometry q = 1/2) and is the geometry BC of
+    the drag. Re = u_max cube / nu. Returns (grid, omega, meta)."""
+    from .grid import ListGrid
+    g = ListGrid(nx, ny, nz, periodic=(False, False, False))
+    for side in ("MY", "PY", "MZ", "PZ"):
+        g.add_side(side, "noslip")
+
+    def inlet(x, y, z):
+        eta = (y + 0.5) / ny
+        zeta = (z + 0.5) / nz
+        return (u_max * 16.0 * eta * (1 - eta) * zeta * (1 - zeta), np.zeros_like(eta), np.zeros_like(eta))
+
+    g.add_side("MX", "velocity", velocity=inlet)
+    g.add_side("PX", "pressure", rho=0.0)
+    y0 = (ny - cube) / 2.0
+    g.add_box_obstacle((x0 - 0.5, y0 - 0.5, -0.5), (x0 + cube - 0.5, y0 + cube - 0.5, cube - 0.5))
+    nu = u_max * cube / re
+    return g, 1.0 / (3.0 * nu + 0.5), {"nu": nu, "u_max": u_max, "cube": cube, "area": float(cube * cube)}
