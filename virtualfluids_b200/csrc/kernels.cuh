@@ -143,9 +143,18 @@ template <class S, bool EVEN>
 __device__ __forceinline__ void scatter_post(S *__restrict__ base, uint64_t n, const uint32_t (&nodes)[8],
                                              const typename Codec<S>::compute (&f)[27])
 {
+    if constexpr (Codec<S>::kPairs) {
+        // 16-bit storage: two directions share one stochastic-rounding conversion
 #pragma unroll
-    for (int d = 0; d < 27; ++d)
-        Codec<S>::store_at(base, (uint64_t)plane<EVEN>(d) * n + nodes[shift_class(d)], f[inv(d)], d);
+        for (int d = 0; d + 1 < 27; d += 2)
+            Codec<S>::store_pair_at(base, (uint64_t)plane<EVEN>(d) * n + nodes[shift_class(d)], f[inv(d)], d,
+                                    (uint64_t)plane<EVEN>(d + 1) * n + nodes[shift_class(d + 1)], f[inv(d + 1)], d + 1);
+        Codec<S>::store_at(base, (uint64_t)plane<EVEN>(26) * n + nodes[shift_class(26)], f[inv(26)], 26);
+    } else {
+#pragma unroll
+        for (int d = 0; d < 27; ++d)
+            Codec<S>::store_at(base, (uint64_t)plane<EVEN>(d) * n + nodes[shift_class(d)], f[inv(d)], d);
+    }
 }
 
 // getPostCollisionDistribution (KernelUtilities.h:283): post[d] leaves the node along d

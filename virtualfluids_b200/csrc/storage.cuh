@@ -32,6 +32,7 @@ struct Codec;
 template <>
 struct Codec<double> {
     using compute = double;
+    static constexpr bool kPairs = false;
     __device__ __forceinline__ static double load(const double *p, int) { return *p; }
     __device__ __forceinline__ static void store(double *p, double v, int) { *p = v; }
     __device__ __forceinline__ static void store_at(double *base, uint64_t off, double v, int) { base[off] = v; }
@@ -40,6 +41,7 @@ struct Codec<double> {
 template <>
 struct Codec<float> {
     using compute = float;
+    static constexpr bool kPairs = false;
     __device__ __forceinline__ static float load(const float *p, int) { return *p; }
     __device__ __forceinline__ static void store(float *p, float v, int) { *p = v; }
     __device__ __forceinline__ static void store_at(float *base, uint64_t off, float v, int) { base[off] = v; }
@@ -66,6 +68,21 @@ __device__ __forceinline__ __half half_sr(float v, uint32_t rbits)
     return __ushort_as_half((unsigned short)(d >> 16));
 }
 
+// two values in one conversion: a to the upper, b to the lower half of the result
+__device__ __forceinline__ uint32_t half2_sr(float a, float b, uint32_t rbits)
+{
+    uint32_t d;
+    asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(a), "f"(b), "r"(rbits));
+    return d;
+}
+
+__device__ __forceinline__ uint32_t bf162_sr(float a, float b, uint32_t rbits)
+{
+    uint32_t d;
+    asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(a), "f"(b), "r"(rbits));
+    return d;
+}
+
 __device__ __forceinline__ __nv_bfloat16 bf16_sr(float v, uint32_t rbits)
 {
     uint32_t d;
@@ -76,6 +93,15 @@ __device__ __forceinline__ __nv_bfloat16 bf16_sr(float v, uint32_t rbits)
 template <>
 struct Codec<__half> {
     using compute = float;
+    static constexpr bool kPairs = true;
+    __device__ __forceinline__ static void store_pair_at(__half *base, uint64_t off0, float v0, int d0, uint64_t off1,
+                                                         float v1, int d1)
+    {
+        const float s0 = v0 * float(1.0 / weight(d0)), s1 = v1 * float(1.0 / weight(d1));
+        const uint32_t h = half2_sr(s0, s1, sr_bits(s0, off0) ^ (__float_as_uint(s1) * 0xC2B2AE35u));
+        base[off0] = __ushort_as_half((unsigned short)(h >> 16));
+        base[off1] = __ushort_as_half((unsigned short)(h & 0xffffu));
+    }
     __device__ __forceinline__ static float load(const __half *p, int d) { return __half2float(*p) * float(weight(d)); }
     __device__ __forceinline__ static void store_at(__half *base, uint64_t off, float v, int d)
     {
@@ -87,6 +113,15 @@ struct Codec<__half> {
 template <>
 struct Codec<__nv_bfloat16> {
     using compute = float;
+    static constexpr bool kPairs = true;
+    __device__ __forceinline__ static void store_pair_at(__nv_bfloat16 *base, uint64_t off0, float v0, int d0,
+                                                         uint64_t off1, float v1, int d1)
+    {
+        const float s0 = v0 * float(1.0 / weight(d0)), s1 = v1 * float(1.0 / weight(d1));
+        const uint32_t h = bf162_sr(s0, s1, sr_bits(s0, off0) ^ (__float_as_uint(s1) * 0xC2B2AE35u));
+        base[off0] = __ushort_as_bfloat16((unsigned short)(h >> 16));
+        base[off1] = __ushort_as_bfloat16((unsigned short)(h & 0xffffu));
+    }
     __device__ __forceinline__ static float load(const __nv_bfloat16 *p, int d)
     {
         return __bfloat162float(*p) * float(weight(d));
