@@ -120,6 +120,22 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def max_over_ranks_of(x, pg, device):
+    """The largest of every rank's x (each rank's device time; the job's time is the slowest rank)."""
+    if not pg:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_mlups(units_per_rank, world, slowest_ms):
+    """Replicas: every rank advances its own box, so the job's rate is all ranks' node updates over
+    the slowest rank's time."""
+    return units_per_rank * world / (slowest_ms / 1e3) / 1e6
+
+
 def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -520,11 +536,7 @@ def main():
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if not pg:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks_of(x, pg, dev)
 
     # ---- device-resident throughput: K steps with the per-step FP64 energy kept on the device ----
     box = vfb.Box(n, n, n, omega, storage="f64", arith=args.arith)
@@ -544,7 +556,7 @@ def main():
     launches = box.kernel_launches() - launches0
     barrier()
     t_ms = max_over_ranks(ev0.elapsed_time(ev1))
-    value = nodes * args.steps * world / (t_ms / 1e3) / 1e6
+    value = whole_job_mlups(nodes * args.steps, world, t_ms)
     clocks = clk.summary()
 
     # ---- the collision kernel alone: average launch time for the roofline ----
@@ -592,7 +604,7 @@ def main():
     wall_e2e = time.perf_counter() - t0
     barrier()
     e2e_ms = max_over_ranks(ev0.elapsed_time(ev1))
-    e2e_value = nodes * args.steps * world / (e2e_ms / 1e3) / 1e6
+    e2e_value = whole_job_mlups(nodes * args.steps, world, e2e_ms)
     h2d = 4 * nodes * 8
     d2h = 4 * nodes * 8 + 16 * args.steps
     ek = host_energy.numpy()[1::2]
