@@ -97,6 +97,7 @@ typedef struct vfb_level {
     void *body_force_x;               /* forceX_SP etc., only for body-force collision templates */
     void *body_force_y;
     void *body_force_z;
+    double outflow_pressure_correction_factor; /* outflowPressureCorrectionFactor (OutflowNonReflectivePressureCorrection) */
 } vfb_level;
 
 /* QforBoundaryConditions (src/gpu/core/Calculation/Calculation.h:105-117). Device pointers. */
@@ -153,6 +154,20 @@ int vfb_velocity_bounce_back(const vfb_level *level, const vfb_bc *bc, void *str
 int vfb_velocity_interpolated_compressible(const vfb_level *level, const vfb_bc *bc, void *stream);
 /* PressureNonEquilibriumCompressible (BoundaryConditions/Pressure/Pressure.cu:63) */
 int vfb_pressure_non_equilibrium_compressible(const vfb_level *level, const vfb_directional_bc *bc, void *stream);
+/* PressureNonEquilibriumIncompressible (Pressure/Pressure.cu:43) */
+int vfb_pressure_non_equilibrium_incompressible(const vfb_level *level, const vfb_directional_bc *bc, void *stream);
+/* OutflowNonReflecting (BoundaryConditions/Outflow/Outflow.cu:43) */
+int vfb_outflow_non_reflecting(const vfb_level *level, const vfb_directional_bc *bc, void *stream);
+/* OutflowNonReflectingPressureCorrection (Outflow/Outflow.cu:64), with the level's
+   outflow_pressure_correction_factor */
+int vfb_outflow_non_reflecting_pressure_correction(const vfb_level *level, const vfb_directional_bc *bc, void *stream);
+/* NoSlipInterpolatedIncompressible (NoSlip/NoSlip.cu:62) */
+int vfb_noslip_interpolated_incompressible(const vfb_level *level, const vfb_bc *bc, void *stream);
+/* VelocityInterpolatedIncompressible (Velocity/Velocity.cu:65) */
+int vfb_velocity_interpolated_incompressible(const vfb_level *level, const vfb_bc *bc, void *stream);
+/* VelocityWithPressureInterpolatedCompressible (Velocity/Velocity.cu:109); the BC's q27 / velocity
+   arrays as the velocity BC */
+int vfb_velocity_with_pressure_interpolated_compressible(const vfb_level *level, const vfb_bc *bc, void *stream);
 
 /* ICells and ICellNeigh (src/gpu/core/Calculation/Calculation.h:72-87): the interpolation cells
    between a coarse level and the fine level nested in it. Device pointers. */
@@ -326,6 +341,8 @@ int vfb_box_set_bc(vfb_box *box, int32_t kind, int32_t variant, const int32_t *k
                    const void *ux, const void *uy, const void *uz);
 int vfb_box_add_pressure_bc(vfb_box *box, int32_t variant, const int32_t *k, const int32_t *k_neighbor, const void *rho,
                             uint32_t n, int32_t direction);
+/* outflowPressureCorrectionFactor of the box's OutflowNonReflectivePressureCorrection lists */
+int vfb_box_set_outflow_pressure_correction(vfb_box *box, double factor);
 /* a seeded perturbation of the velocity BC every step: u_i(t) = u_i (1 + amplitude (2 U - 1)), U
    uniform in [0, 1) from the counter-based Philox-4x32-10 generator keyed by seed and counted by
    (BC node, step) */

@@ -105,6 +105,11 @@ def refgpu():
     L.refgpu_velocity_interpolated.argtypes = [_P, _P, _P, _P, _P, _P, u, d, _P, _P, _P, u64, i]
     L.refgpu_pressure_neq.argtypes = [_P, _P, _P, _P, i, _P, _P, _P, u64, i, i]
     L.refgpu_init.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P, u, _P, i]
+    L.refgpu_noslip_interpolated_incompressible.argtypes = [_P, _P, _P, u, d, _P, _P, _P, u64, i]
+    L.refgpu_velocity_interpolated_incompressible.argtypes = [_P, _P, _P, _P, _P, _P, u, d, _P, _P, _P, u64, i]
+    L.refgpu_velocity_with_pressure.argtypes = [_P, _P, _P, _P, _P, _P, u, d, _P, _P, _P, u64, i]
+    L.refgpu_pressure_neq_incompressible.argtypes = [_P, _P, _P, _P, i, _P, _P, _P, u64, i, i]
+    L.refgpu_outflow.argtypes = [_P, _P, _P, _P, i, d, _P, _P, _P, u64, i, i, i, d]
     L.refgpu_macros.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P, _P, u64, _P, i]
     L.refgpu_scale_cf.argtypes = [_P] * 8 + [u64, u64, i, _P, _P, u, d, d, _P, _P, _P]
     L.refgpu_scale_fc.argtypes = [_P] * 8 + [u64, u64, i, _P, _P, u, d, d, _P, _P, _P]

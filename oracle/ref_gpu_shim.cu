@@ -17,6 +17,10 @@
  *   VelocityBounceBack_Device                      BoundaryConditions/Velocity/VelocityBounceBack.cu:44
  *   VelocityInterpolatedCompressible_Device        BoundaryConditions/Velocity/VelocityInterpolatedCompressible.cu:44
  *   PressureNonEquilibriumCompressible_Device      BoundaryConditions/Pressure/PressureNonEquilibriumCompressible.cu:45
+ *   NoSlipInterpolatedIncompressible_Device, VelocityInterpolatedIncompressible_Device,
+ *   VelocityWithPressureInterpolatedCompressible_Device, PressureNonEquilibriumIncompressible_Device,
+ *   OutflowNonReflecting_Device, OutflowNonReflectingPressureCorrection_Device
+ *                                                  BoundaryConditions/{NoSlip,Velocity,Pressure,Outflow}/
  *   InitNavierStokesCompressible_Device            PreProcessor/PreProcessorStrategy/InitNavierStokesCompressible/
  *                                                  InitNavierStokesCompressible_Device.cu:44
  *   calculateMacroscopicQuantitiesCompressible_device  PostProcessor/MacroscopicQuantities.cu:194
@@ -36,6 +40,12 @@
 #include "BoundaryConditions/Pressure/PressureNonEquilibriumCompressible.cu"
 #include "BoundaryConditions/Velocity/VelocityBounceBack.cu"
 #include "BoundaryConditions/Velocity/VelocityInterpolatedCompressible.cu"
+#include "BoundaryConditions/Velocity/VelocityInterpolatedIncompressible.cu"
+#include "BoundaryConditions/Velocity/VelocityWithPressureInterpolatedCompressible.cu"
+#include "BoundaryConditions/NoSlip/NoSlipInterpolatedIncompressible.cu"
+#include "BoundaryConditions/Pressure/PressureNonEquilibriumIncompressible.cu"
+#include "BoundaryConditions/Outflow/OutflowNonReflecting.cu"
+#include "BoundaryConditions/Outflow/OutflowNonReflectingPressureCorrection.cu"
 #include "GridScaling/scaleCoarseToFineCompressible.cu"
 #include "GridScaling/scaleFineToCoarseCompressible.cu"
 #include "PostProcessor/DragLift.cu"
@@ -129,6 +139,61 @@ int refgpu_pressure_neq(real *rho_bc, real *dist, int *k, int *kn, int nbc, unsi
         return 0;
     PressureNonEquilibriumCompressible_Device<<<blocks_for((uint64_t)nbc), kThreads>>>(
         rho_bc, dist, k, kn, nbc, nbx, nby, nbz, n, is_even != 0, (size_t)direction);
+    return done();
+}
+
+int refgpu_noslip_interpolated_incompressible(real *dist, int *k, real *q, unsigned nbc, real omega, unsigned *nbx,
+                                              unsigned *nby, unsigned *nbz, uint64_t n, int is_even)
+{
+    if (nbc == 0)
+        return 0;
+    NoSlipInterpolatedIncompressible_Device<<<blocks_for(nbc), kThreads>>>(dist, k, q, nbc, omega, nbx, nby, nbz, n,
+                                                                             is_even != 0);
+    return done();
+}
+
+int refgpu_velocity_interpolated_incompressible(real *vx, real *vy, real *vz, real *dist, int *k, real *q, unsigned nbc,
+                                                real omega, unsigned *nbx, unsigned *nby, unsigned *nbz, uint64_t n,
+                                                int is_even)
+{
+    if (nbc == 0)
+        return 0;
+    VelocityInterpolatedIncompressible_Device<<<blocks_for(nbc), kThreads>>>(vx, vy, vz, dist, k, q, nbc, omega, nbx,
+                                                                               nby, nbz, n, is_even != 0);
+    return done();
+}
+
+int refgpu_velocity_with_pressure(real *vx, real *vy, real *vz, real *dist, int *k, real *q, unsigned nbc, real omega,
+                                  unsigned *nbx, unsigned *nby, unsigned *nbz, uint64_t n, int is_even)
+{
+    if (nbc == 0)
+        return 0;
+    VelocityWithPressureInterpolatedCompressible_Device<<<blocks_for(nbc), kThreads>>>(
+        vx, vy, vz, dist, k, q, nbc, omega, nbx, nby, nbz, n, is_even != 0);
+    return done();
+}
+
+int refgpu_pressure_neq_incompressible(real *rho_bc, real *dist, int *k, int *kn, int nbc, unsigned *nbx, unsigned *nby,
+                                       unsigned *nbz, uint64_t n, int is_even, int direction)
+{
+    if (nbc == 0)
+        return 0;
+    PressureNonEquilibriumIncompressible_Device<<<blocks_for((uint64_t)nbc), kThreads>>>(
+        rho_bc, dist, k, kn, nbc, nbx, nby, nbz, n, is_even != 0, (size_t)direction);
+    return done();
+}
+
+int refgpu_outflow(real *rho_bc, real *dist, int *k, int *kn, int nbc, real omega, unsigned *nbx, unsigned *nby,
+                   unsigned *nbz, uint64_t n, int is_even, int direction, int correction, real factor)
+{
+    if (nbc == 0)
+        return 0;
+    if (correction)
+        OutflowNonReflectingPressureCorrection_Device<<<blocks_for((uint64_t)nbc), kThreads>>>(
+            rho_bc, dist, k, kn, nbc, omega, nbx, nby, nbz, n, is_even != 0, direction, factor);
+    else
+        OutflowNonReflecting_Device<<<blocks_for((uint64_t)nbc), kThreads>>>(rho_bc, dist, k, kn, nbc, omega, nbx, nby,
+                                                                              nbz, n, is_even != 0, direction);
     return done();
 }
 

@@ -90,8 +90,20 @@ def test_bc_factory_semantics():
     assert fn.value is None
     N.check(lib.vfb_bc_factory_pressure(N.PRESSURE_NON_EQUILIBRIUM_COMPRESSIBLE, C.byref(fn)))
     assert fn.value == C.cast(lib.vfb_pressure_non_equilibrium_compressible, C.c_void_p).value
-    assert lib.vfb_bc_factory_velocity(N.VELOCITY_INTERPOLATED_INCOMPRESSIBLE, C.byref(fn)) == N.VFB_ERR_UNSUPPORTED
+    for factory, variant, name in (
+            (lib.vfb_bc_factory_velocity, N.VELOCITY_INTERPOLATED_INCOMPRESSIBLE, "vfb_velocity_interpolated_incompressible"),
+            (lib.vfb_bc_factory_velocity, N.VELOCITY_WITH_PRESSURE_INTERPOLATED_COMPRESSIBLE,
+             "vfb_velocity_with_pressure_interpolated_compressible"),
+            (lib.vfb_bc_factory_noslip, N.NOSLIP_INTERPOLATED_INCOMPRESSIBLE, "vfb_noslip_interpolated_incompressible"),
+            (lib.vfb_bc_factory_pressure, N.PRESSURE_NON_EQUILIBRIUM_INCOMPRESSIBLE,
+             "vfb_pressure_non_equilibrium_incompressible"),
+            (lib.vfb_bc_factory_pressure, N.PRESSURE_OUTFLOW_NON_REFLECTIVE, "vfb_outflow_non_reflecting"),
+            (lib.vfb_bc_factory_pressure, N.PRESSURE_OUTFLOW_NON_REFLECTIVE_PRESSURE_CORRECTION,
+             "vfb_outflow_non_reflecting_pressure_correction")):
+        N.check(factory(variant, C.byref(fn)))
+        assert fn.value == C.cast(getattr(lib, name), C.c_void_p).value, name
     assert lib.vfb_bc_factory_noslip(99, C.byref(fn)) == N.VFB_ERR_INVALID_ARGUMENT
+    assert lib.vfb_bc_factory_pressure(99, C.byref(fn)) == N.VFB_ERR_INVALID_ARGUMENT
 
 
 def _fake_level(N):

@@ -38,7 +38,7 @@ def _p(t):
 class RefLevel:
     """One level on the device, advanced by the reference's kernels in UpdateGrid27 order."""
 
-    def __init__(self, grid, omega, vkind, nkind, gkind=0, forces=(0.0, 0.0, 0.0)):
+    def __init__(self, grid, omega, vkind, nkind, gkind=0, forces=(0.0, 0.0, 0.0), pkind=0, correction=0.0):
         import torch
         dev = torch.device("cuda", 0)
         self.t = torch
@@ -67,7 +67,7 @@ class RefLevel:
                                       torch.from_numpy(b.k_neighbor.astype(np.int32)).to(dev),
                                       torch.full((b.k.size,), float(b.rho), dtype=torch.float64, device=dev),
                                       b.k.size, SIDE_DIR[b.side]))
-        self.vkind, self.nkind, self.gkind = vkind, nkind, gkind
+        self.vkind, self.nkind, self.gkind, self.pkind, self.correction = vkind, nkind, gkind, pkind, correction
 
     def init(self, ref, rho=None, ux=None, uy=None, uz=None):
         z = np.zeros(self.n)
@@ -86,6 +86,9 @@ class RefLevel:
         elif kind == 2:
             assert ref.refgpu_noslip_interpolated(_p(self.dist), _p(k), _p(q), nbc, self.omega, *nb, self.n,
                                                   self.is_even) == 0
+        elif kind == 3:
+            assert ref.refgpu_noslip_interpolated_incompressible(_p(self.dist), _p(k), _p(q), nbc, self.omega, *nb,
+                                                                 self.n, self.is_even) == 0
 
     def step(self, ref, drag=None):
         nb = [_p(x) for x in self.nb]
@@ -97,8 +100,10 @@ class RefLevel:
                 assert ref.refgpu_velocity_bounce_back(*(_p(a) for a in v), _p(self.dist), _p(k), _p(q), nbc, *nb,
                                                        self.n, self.is_even) == 0
             else:
-                assert ref.refgpu_velocity_interpolated(*(_p(a) for a in v), _p(self.dist), _p(k), _p(q), nbc,
-                                                        self.omega, *nb, self.n, self.is_even) == 0
+                fn = {2: ref.refgpu_velocity_interpolated, 3: ref.refgpu_velocity_interpolated_incompressible,
+                      4: ref.refgpu_velocity_with_pressure}[self.vkind]
+                assert fn(*(_p(a) for a in v), _p(self.dist), _p(k), _p(q), nbc, self.omega, *nb, self.n,
+                          self.is_even) == 0
         if "noslip" in self.bcs:
             self._noslip(ref, self.bcs["noslip"], self.nkind)
         if "geometry" in self.bcs:
@@ -113,8 +118,15 @@ class RefLevel:
             assert ref.refgpu_drag_lift_pre(_p(self.dist), _p(k), _p(q), nbc, *(_p(a) for a in drag[:3]), *nb,
                                             self.n, self.is_even) == 0
         for k, kn, rho, nbc, direction in self.pressure:
-            assert ref.refgpu_pressure_neq(_p(rho), _p(self.dist), _p(k), _p(kn), nbc, *nb, self.n, self.is_even,
-                                           direction) == 0
+            if self.pkind == 0:
+                assert ref.refgpu_pressure_neq(_p(rho), _p(self.dist), _p(k), _p(kn), nbc, *nb, self.n,
+                                               self.is_even, direction) == 0
+            elif self.pkind == 1:
+                assert ref.refgpu_pressure_neq_incompressible(_p(rho), _p(self.dist), _p(k), _p(kn), nbc, *nb,
+                                                              self.n, self.is_even, direction) == 0
+            else:
+                assert ref.refgpu_outflow(_p(rho), _p(self.dist), _p(k), _p(kn), nbc, self.omega, *nb, self.n,
+                                          self.is_even, direction, int(self.pkind == 3), self.correction) == 0
 
 
 def _para(omega, forcing=(0.0, 0.0, 0.0)):
@@ -292,3 +304,38 @@ def test_scaling_matches_reference_gpu_kernels(ref, cuda, fine_to_coarse):
     got = (coarse if fine_to_coarse else fine).populations()
     want = (dc if fine_to_coarse else df).cpu().numpy()
     assert np.abs(got - want).max() <= 1e-13 * np.abs(want).max()
+
+
+@pytest.mark.parametrize("vkind,nkind,pkind", [(3, 3, 1), (4, 2, 2), (2, 2, 3), (4, 3, 3)],
+                         ids=["incompressible", "with_pressure_outflow", "outflow_correction", "mixed"])
+def test_remaining_bc_variants_match_reference_gpu_kernels_bitwise(ref, cuda, vkind, nkind, pkind):
+    """VelocityInterpolatedIncompressible / VelocityWithPressureInterpolatedCompressible,
+    NoSlipInterpolatedIncompressible, PressureNonEquilibriumIncompressible, OutflowNonReflecting and
+    OutflowNonReflectingPressureCorrection through the factory, against the reference's kernels."""
+    import torch
+    g = ListGrid(20, 10, 10, periodic=(False, True, False))
+    g.add_side("MZ", "noslip")
+    g.add_side("PZ", "noslip")
+    g.add_side("MX", "velocity", velocity=(0.02, 0.0, 0.0))
+    g.add_side("PX", "pressure", rho=0.001)
+    bcf = BCF()
+    bcf.set_velocity_boundary_condition({2: BCF.VelocityBC.VelocityInterpolatedCompressible,
+                                         3: BCF.VelocityBC.VelocityInterpolatedIncompressible,
+                                         4: BCF.VelocityBC.VelocityWithPressureInterpolatedCompressible}[vkind])
+    bcf.set_no_slip_boundary_condition({2: BCF.NoSlipBC.NoSlipInterpolatedCompressible,
+                                        3: BCF.NoSlipBC.NoSlipInterpolatedIncompressible}[nkind])
+    bcf.set_pressure_boundary_condition({1: BCF.PressureBC.PressureNonEquilibriumIncompressible,
+                                         2: BCF.PressureBC.OutflowNonReflective,
+                                         3: BCF.PressureBC.OutflowNonReflectivePressureCorrection}[pkind])
+    para = _para(1.8)
+    para.set_outflow_pressure_correction_factor(0.5)
+    sim = Simulation(para, g, bcf)
+    rl = RefLevel(g, sim.para.omega, vkind, nkind, pkind=pkind, correction=0.5)
+    sim.init()
+    rl.init(ref)
+    for _ in range(40):
+        rl.step(ref)
+    sim.run(40)
+    torch.cuda.synchronize()
+    assert np.array_equal(sim.populations(), rl.dist.cpu().numpy())
+    assert np.abs(sim.macroscopic()["vx"]).max() > 1e-3

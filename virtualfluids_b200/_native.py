@@ -69,6 +69,7 @@ class Level(C.Structure):
         ("quadric_limiters", C.c_double * 3), ("rho", C.c_void_p), ("velocity_x", C.c_void_p),
         ("velocity_y", C.c_void_p), ("velocity_z", C.c_void_p), ("pressure", C.c_void_p),
         ("body_force_x", C.c_void_p), ("body_force_y", C.c_void_p), ("body_force_z", C.c_void_p),
+        ("outflow_pressure_correction_factor", C.c_double),
     ]
 
 
@@ -140,6 +141,13 @@ SIGNATURES = {
                                        C.c_void_p]),
     "vfb_drag_lift_workspace_bytes": (C.c_size_t, [C.c_uint32]),
     "vfb_drag_lift_force": (C.c_int, [C.c_void_p] * 6 + [C.c_uint32, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
+    "vfb_pressure_non_equilibrium_incompressible": (C.c_int, [C.POINTER(Level), C.POINTER(DirectionalBC), C.c_void_p]),
+    "vfb_outflow_non_reflecting": (C.c_int, [C.POINTER(Level), C.POINTER(DirectionalBC), C.c_void_p]),
+    "vfb_outflow_non_reflecting_pressure_correction": (C.c_int, [C.POINTER(Level), C.POINTER(DirectionalBC),
+                                                                 C.c_void_p]),
+    "vfb_noslip_interpolated_incompressible": (C.c_int, [C.POINTER(Level), C.POINTER(BC), C.c_void_p]),
+    "vfb_velocity_interpolated_incompressible": (C.c_int, [C.POINTER(Level), C.POINTER(BC), C.c_void_p]),
+    "vfb_velocity_with_pressure_interpolated_compressible": (C.c_int, [C.POINTER(Level), C.POINTER(BC), C.c_void_p]),
     "vfb_init_navier_stokes_compressible": (C.c_int, [C.POINTER(Level), C.c_void_p]),
     "vfb_calc_macroscopic_compressible": (C.c_int, [C.POINTER(Level), C.c_void_p]),
     "vfb_mass_energy_workspace_bytes": (C.c_size_t, [C.c_uint32]),
@@ -175,6 +183,7 @@ SIGNATURES = {
                                  C.c_void_p, C.c_void_p]),
     "vfb_box_add_pressure_bc": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                           C.c_int32]),
+    "vfb_box_set_outflow_pressure_correction": (C.c_int, [C.c_void_p, C.c_double]),
     "vfb_box_set_velocity_perturbation": (C.c_int, [C.c_void_p, C.c_uint64, C.c_double]),
     "vfb_box_set_drag_lift": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
     "vfb_box_kernel_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),

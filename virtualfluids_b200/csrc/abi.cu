@@ -333,7 +333,21 @@ int vfb_velocity_interpolated_compressible(const vfb_level *level, const vfb_bc 
     return run_bc(level, bc, vfb::kVelocityInterp, true, stream);
 }
 
-int vfb_pressure_non_equilibrium_compressible(const vfb_level *level, const vfb_directional_bc *bc, void *stream)
+int vfb_noslip_interpolated_incompressible(const vfb_level *level, const vfb_bc *bc, void *stream)
+{
+    return run_bc(level, bc, vfb::kNoSlipInterpIncomp, false, stream);
+}
+int vfb_velocity_interpolated_incompressible(const vfb_level *level, const vfb_bc *bc, void *stream)
+{
+    return run_bc(level, bc, vfb::kVelocityInterpIncomp, true, stream);
+}
+int vfb_velocity_with_pressure_interpolated_compressible(const vfb_level *level, const vfb_bc *bc, void *stream)
+{
+    return run_bc(level, bc, vfb::kVelocityWithPressure, true, stream);
+}
+
+static int run_directional(const vfb_level *level, const vfb_directional_bc *bc, int kind, const char *what,
+                           void *stream)
 {
     int st = check_level(level);
     if (st)
@@ -342,10 +356,29 @@ int vfb_pressure_non_equilibrium_compressible(const vfb_level *level, const vfb_
         return fail(VFB_ERR_INVALID_ARGUMENT, "bc is NULL");
     if (bc->direction < VFB_DIR_P00 || bc->direction > VFB_DIR_00M)
         return fail(VFB_ERR_INVALID_ARGUMENT, "direction must be one of the six face directions");
-    if (bc->number_of_bc_nodes && (!bc->k || !bc->k_neighbor || !bc->rho_bc))
+    if (bc->number_of_bc_nodes && (!bc->k || !bc->k_neighbor || (!bc->rho_bc && kind < vfb::kOutflowNonReflecting)))
         return fail(VFB_ERR_INVALID_ARGUMENT, "pressure bc arrays are NULL");
-    const cudaError_t e = VFB_DISPATCH(level->storage, level->arith, LA::pressure(level, bc, as_stream(stream)));
-    return cuda_status(e, "PressureNonEquilibriumCompressible launch");
+    const cudaError_t e = VFB_DISPATCH(level->storage, level->arith,
+                                       LA::pressure(level, bc, as_stream(stream), nullptr, kind));
+    return cuda_status(e, what);
+}
+
+int vfb_pressure_non_equilibrium_compressible(const vfb_level *level, const vfb_directional_bc *bc, void *stream)
+{
+    return run_directional(level, bc, vfb::kPressureNeqComp, "PressureNonEquilibriumCompressible launch", stream);
+}
+int vfb_pressure_non_equilibrium_incompressible(const vfb_level *level, const vfb_directional_bc *bc, void *stream)
+{
+    return run_directional(level, bc, vfb::kPressureNeqIncomp, "PressureNonEquilibriumIncompressible launch", stream);
+}
+int vfb_outflow_non_reflecting(const vfb_level *level, const vfb_directional_bc *bc, void *stream)
+{
+    return run_directional(level, bc, vfb::kOutflowNonReflecting, "OutflowNonReflecting launch", stream);
+}
+int vfb_outflow_non_reflecting_pressure_correction(const vfb_level *level, const vfb_directional_bc *bc, void *stream)
+{
+    return run_directional(level, bc, vfb::kOutflowPressureCorrection, "OutflowNonReflectingPressureCorrection launch",
+                           stream);
 }
 
 static int run_scaling(const vfb_level *coarse, const vfb_level *fine, const vfb_interpolation_cells *cells,
@@ -510,9 +543,10 @@ int vfb_bc_factory_velocity(int32_t variant, vfb_bc_fn *fn)
     case VFB_VELOCITY_BOUNCE_BACK: *fn = vfb_velocity_bounce_back; return VFB_OK;
     case VFB_VELOCITY_INTERPOLATED_COMPRESSIBLE: *fn = vfb_velocity_interpolated_compressible; return VFB_OK;
     case VFB_VELOCITY_NOT_SPECIFIED: return VFB_OK;
-    case VFB_VELOCITY_INTERPOLATED_INCOMPRESSIBLE:
+    case VFB_VELOCITY_INTERPOLATED_INCOMPRESSIBLE: *fn = vfb_velocity_interpolated_incompressible; return VFB_OK;
     case VFB_VELOCITY_WITH_PRESSURE_INTERPOLATED_COMPRESSIBLE:
-        return fail(VFB_ERR_UNSUPPORTED, "velocity BC variant not built");
+        *fn = vfb_velocity_with_pressure_interpolated_compressible;
+        return VFB_OK;
     default: return fail(VFB_ERR_INVALID_ARGUMENT, "unknown VelocityBC");
     }
 }
@@ -526,7 +560,7 @@ int vfb_bc_factory_noslip(int32_t variant, vfb_bc_fn *fn)
     case VFB_NOSLIP_DELAY_BOUNCE_BACK: return VFB_OK; // BoundaryConditionFactory.cpp: empty function
     case VFB_NOSLIP_BOUNCE_BACK: *fn = vfb_noslip_bounce_back; return VFB_OK;
     case VFB_NOSLIP_INTERPOLATED_COMPRESSIBLE: *fn = vfb_noslip_interpolated_compressible; return VFB_OK;
-    case VFB_NOSLIP_INTERPOLATED_INCOMPRESSIBLE: return fail(VFB_ERR_UNSUPPORTED, "no-slip BC variant not built");
+    case VFB_NOSLIP_INTERPOLATED_INCOMPRESSIBLE: *fn = vfb_noslip_interpolated_incompressible; return VFB_OK;
     default: return fail(VFB_ERR_INVALID_ARGUMENT, "unknown NoSlipBC");
     }
 }
@@ -539,10 +573,11 @@ int vfb_bc_factory_pressure(int32_t variant, vfb_directional_bc_fn *fn)
     switch (variant) {
     case VFB_PRESSURE_NON_EQUILIBRIUM_COMPRESSIBLE: *fn = vfb_pressure_non_equilibrium_compressible; return VFB_OK;
     case VFB_PRESSURE_NOT_SPECIFIED: return VFB_OK;
-    case VFB_PRESSURE_NON_EQUILIBRIUM_INCOMPRESSIBLE:
-    case VFB_PRESSURE_OUTFLOW_NON_REFLECTIVE:
+    case VFB_PRESSURE_NON_EQUILIBRIUM_INCOMPRESSIBLE: *fn = vfb_pressure_non_equilibrium_incompressible; return VFB_OK;
+    case VFB_PRESSURE_OUTFLOW_NON_REFLECTIVE: *fn = vfb_outflow_non_reflecting; return VFB_OK;
     case VFB_PRESSURE_OUTFLOW_NON_REFLECTIVE_PRESSURE_CORRECTION:
-        return fail(VFB_ERR_UNSUPPORTED, "pressure BC variant not built");
+        *fn = vfb_outflow_non_reflecting_pressure_correction;
+        return VFB_OK;
     default: return fail(VFB_ERR_INVALID_ARGUMENT, "unknown PressureBC");
     }
 }
@@ -854,8 +889,10 @@ struct vfb_box {
     } velocity, noslip, geometry;
     struct Pressure {
         vfb_directional_bc bc{};
+        int kind = 0;                 // vfb::PressureKind
         std::vector<void *> owned;
     };
+    double outflow_correction = 0.0;
     std::vector<Pressure> pressure;
     void *velocity_base = nullptr;  // unperturbed inlet velocities (3 x n reals)
     uint64_t perturb_seed = 0;
@@ -1103,7 +1140,10 @@ cudaError_t box_pre_collision(vfb_box *b, cudaStream_t s)
     for (size_t i = 0; i < b->pressure.size() && e == cudaSuccess; ++i) {
         const vfb_level L = box_level(b);
         const vfb::NodeAddr a = box_addr(b);
-        e = VFB_DISPATCH(b->desc.storage, b->desc.arith, LA::pressure(&L, &b->pressure[i].bc, s, &a));
+        vfb_level Lp = L;
+        Lp.outflow_pressure_correction_factor = b->outflow_correction;
+        e = VFB_DISPATCH(b->desc.storage, b->desc.arith,
+                         LA::pressure(&Lp, &b->pressure[i].bc, s, &a, b->pressure[i].kind));
         ++b->launches;
     }
     return e;
@@ -1209,6 +1249,8 @@ int vfb_box_set_bc(vfb_box *box, int32_t kind, int32_t variant, const int32_t *k
         switch (variant) {
         case VFB_VELOCITY_BOUNCE_BACK: bc_kind = vfb::kVelocityBB; break;
         case VFB_VELOCITY_INTERPOLATED_COMPRESSIBLE: bc_kind = vfb::kVelocityInterp; break;
+        case VFB_VELOCITY_INTERPOLATED_INCOMPRESSIBLE: bc_kind = vfb::kVelocityInterpIncomp; break;
+        case VFB_VELOCITY_WITH_PRESSURE_INTERPOLATED_COMPRESSIBLE: bc_kind = vfb::kVelocityWithPressure; break;
         case VFB_VELOCITY_NOT_SPECIFIED: break;
         default: return fail(VFB_ERR_UNSUPPORTED, "velocity BC variant not built for boxes");
         }
@@ -1217,6 +1259,7 @@ int vfb_box_set_bc(vfb_box *box, int32_t kind, int32_t variant, const int32_t *k
         case VFB_NOSLIP_DELAY_BOUNCE_BACK: break;
         case VFB_NOSLIP_BOUNCE_BACK: bc_kind = vfb::kNoSlipBB; break;
         case VFB_NOSLIP_INTERPOLATED_COMPRESSIBLE: bc_kind = vfb::kNoSlipInterp; break;
+        case VFB_NOSLIP_INTERPOLATED_INCOMPRESSIBLE: bc_kind = vfb::kNoSlipInterpIncomp; break;
         default: return fail(VFB_ERR_UNSUPPORTED, "no-slip BC variant not built for boxes");
         }
     }
@@ -1277,8 +1320,14 @@ int vfb_box_add_pressure_bc(vfb_box *box, int32_t variant, const int32_t *k, con
 {
     if (!box)
         return fail(VFB_ERR_INVALID_ARGUMENT, "NULL box");
-    if (variant != VFB_PRESSURE_NON_EQUILIBRIUM_COMPRESSIBLE)
-        return fail(VFB_ERR_UNSUPPORTED, "pressure BC variant not built for boxes");
+    int pkind = 0;
+    switch (variant) {
+    case VFB_PRESSURE_NON_EQUILIBRIUM_COMPRESSIBLE: pkind = vfb::kPressureNeqComp; break;
+    case VFB_PRESSURE_NON_EQUILIBRIUM_INCOMPRESSIBLE: pkind = vfb::kPressureNeqIncomp; break;
+    case VFB_PRESSURE_OUTFLOW_NON_REFLECTIVE: pkind = vfb::kOutflowNonReflecting; break;
+    case VFB_PRESSURE_OUTFLOW_NON_REFLECTIVE_PRESSURE_CORRECTION: pkind = vfb::kOutflowPressureCorrection; break;
+    default: return fail(VFB_ERR_UNSUPPORTED, "pressure BC variant not built for boxes");
+    }
     if (direction < VFB_DIR_P00 || direction > VFB_DIR_00M)
         return fail(VFB_ERR_INVALID_ARGUMENT, "direction must be one of the six face directions");
     if (n && (!k || !k_neighbor || !rho))
@@ -1307,7 +1356,16 @@ int vfb_box_add_pressure_bc(vfb_box *box, int32_t variant, const int32_t *k, con
     }
     p.owned = { dk, dn, dr };
     p.bc = vfb_directional_bc{ static_cast<const int32_t *>(dk), static_cast<const int32_t *>(dn), dr, n, direction };
+    p.kind = pkind;
     box->pressure.push_back(p);
+    return VFB_OK;
+}
+
+int vfb_box_set_outflow_pressure_correction(vfb_box *box, double factor)
+{
+    if (!box)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL box");
+    box->outflow_correction = factor;
     return VFB_OK;
 }
 

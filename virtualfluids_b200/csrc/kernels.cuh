@@ -648,8 +648,16 @@ __device__ __forceinline__ C cdot_rt(int d, C ux, C uy, C uz)
 
 // NoSlipInterpolatedCompressible_Device (NoSlip/NoSlipInterpolatedCompressible.cu:44-381) and
 // VelocityInterpolatedCompressible_Device (Velocity/VelocityInterpolatedCompressible.cu:44-420),
-// with the helper formulas of KernelUtilities.h:171-197
-template <class S, bool EVEN, bool VELOCITY>
+// with the helper formulas of KernelUtilities.h:171-210. FORM selects the variant:
+//   kBCCompressible  — the two kernels above;
+//   kBCIncompressible — NoSlipInterpolatedIncompressible.cu:44-387 / VelocityInterpolatedIncompressible.cu:44-497:
+//                       the momenta are not divided by rho and cu_sq does not carry (1 + drho); feq drops
+//                       (1 + drho) in the velocity kernel only (the no-slip one calls getEquilibriumForBC);
+//   kBCWithPressure  — VelocityWithPressureInterpolatedCompressible.cu:44-422: the compressible
+//                       form minus w drho (getInterpolatedDistributionForVeloWithPressureBC).
+enum : int { kBCCompressible = 0, kBCIncompressible = 1, kBCWithPressure = 2 };
+
+template <class S, bool EVEN, bool VELOCITY, int FORM = kBCCompressible>
 __global__ void __launch_bounds__(128) bc_interpolated_kernel(BCArgs a)
 {
     using C = typename Codec<S>::compute;
@@ -672,8 +680,11 @@ __global__ void __launch_bounds__(128) bc_interpolated_kernel(BCArgs a)
                   + ((-(p[9] - p[10])) + (p[7] - p[8]))) + (p[3] - p[4]);
     const C vz = (((((p[21] - p[24]) + (p[20] - p[25])) + ((p[19] - p[26]) + (p[22] - p[23]))) + ((-(p[17] - p[18])) + (p[15] - p[16])))
                   + ((p[11] - p[12]) - (p[13] - p[14]))) + (p[5] - p[6]);
-    const C ux1 = vx / r, uy1 = vy / r, uz1 = vz / r;
-    const C cu_sq = C(1.5) * (ux1 * ux1 + uy1 * uy1 + uz1 * uz1) * (C(1) + drho);
+    const C ux1 = FORM == kBCIncompressible ? vx : vx / r;
+    const C uy1 = FORM == kBCIncompressible ? vy : vy / r;
+    const C uz1 = FORM == kBCIncompressible ? vz : vz / r;
+    const C cu_sq = FORM == kBCIncompressible ? C(1.5) * (ux1 * ux1 + uy1 * uy1 + uz1 * uz1)
+                                              : C(1.5) * (ux1 * ux1 + uy1 * uy1 + uz1 * uz1) * (C(1) + drho);
     const C omega = (C)a.omega;
     const C *q27 = static_cast<const C *>(a.q27);
     C bx = C(0), by = C(0), bz = C(0);
@@ -688,13 +699,18 @@ __global__ void __launch_bounds__(128) bc_interpolated_kernel(BCArgs a)
         if (q_active(q)) {
             const C w = weight_t<C>(d);
             const C vel = cdot_rt<C>(d, ux1, uy1, uz1);
-            const C feq = w * (drho + C(4.5) * vel * vel * (C(1) + drho) - cu_sq);
+            // the incompressible velocity kernel writes feq inline without (1 + drho); the
+            // incompressible no-slip kernel keeps getEquilibriumForBC, which carries it
+            const C feq = (FORM == kBCIncompressible && VELOCITY) ? w * (drho + C(4.5) * vel * vel - cu_sq)
+                                                                  : w * (drho + C(4.5) * vel * vel * (C(1) + drho) - cu_sq);
             const C f = p[d], fi = p[inv(d)];
             C v;
             if (VELOCITY) {
                 const C vbc = cdot_rt<C>(d, bx, by, bz);
                 v = (C(1) - q) / (C(1) + q) * (f - fi + (f + fi - C(2) * feq * omega) / (C(1) - omega)) * C(0.5)
                   + (q * (f + fi) - C(6) * w * vbc) / (C(1) + q);
+                if (FORM == kBCWithPressure)
+                    v = v - w * drho;
             } else {
                 v = (C(1) - q) / (C(1) + q) * (f - fi + (f + fi - C(2) * feq * omega) / (C(1) - omega)) * C(0.5)
                   + (q * (f + fi)) / (C(1) + q);
@@ -719,7 +735,9 @@ __device__ __forceinline__ C feq_shifted(int d, C drho, C ux, C uy, C uz, C cusq
 // The reference's __syncthreads() between the neighbour reads and the writes (:174) sits in
 // divergent code and orders nothing that needs ordering (no thread writes a slot another thread
 // of the launch reads), so it has no counterpart here.
-template <class S, bool EVEN>
+// INCOMP: PressureNonEquilibriumIncompressible_Device (Pressure/PressureNonEquilibriumIncompressible.cu:45-314),
+// the same with getIncompressibleMacroscopicValues (u = momentum, not divided by rho)
+template <class S, bool EVEN, bool INCOMP = false>
 __global__ void __launch_bounds__(128) bc_pressure_neq_kernel(PressureArgs a)
 {
     using C = typename Codec<S>::compute;
@@ -733,8 +751,17 @@ __global__ void __launch_bounds__(128) bc_pressure_neq_kernel(PressureArgs a)
     C f[27];
     gather_pre<S, EVEN>(base, a.n, nn, f);
     const C drho1 = density_pyramid(f);
-    const C inv_rho = C(1) / (drho1 + C(1));
-    const C vx = momentum_x(f) * inv_rho, vy = momentum_y(f) * inv_rho, vz = momentum_z(f) * inv_rho;
+    C vx, vy, vz;
+    if (INCOMP) {
+        vx = momentum_x(f);
+        vy = momentum_y(f);
+        vz = momentum_z(f);
+    } else {
+        const C inv_rho = C(1) / (drho1 + C(1));
+        vx = momentum_x(f) * inv_rho;
+        vy = momentum_y(f) * inv_rho;
+        vz = momentum_z(f) * inv_rho;
+    }
     const C cusq = C(1.5) * (vx * vx + vy * vy + vz * vz);
     const C rbc = static_cast<const C *>(a.rho_bc)[i];
     const int axis = cx(a.direction) != 0 ? 0 : (cy(a.direction) != 0 ? 1 : 2);
@@ -746,6 +773,53 @@ __global__ void __launch_bounds__(128) bc_pressure_neq_kernel(PressureArgs a)
         const int c = axis == 0 ? cx(d) : (axis == 1 ? cy(d) : cz(d));
         if (c != sgn)
             Codec<S>::store_at(base, (uint64_t)plane<EVEN>(d) * a.n + nk[shift_class(d)], v, d);
+    }
+}
+
+// OutflowNonReflecting_Device (Outflow/OutflowNonReflecting.cu:50-276) and, with CORRECTION,
+// OutflowNonReflectingPressureCorrection_Device (OutflowNonReflectingPressureCorrection.cu:53-241).
+// Reads the node's and the inward neighbour's populations at the current parity and writes the
+// nine directions pointing away from the outlet normal into the other parity:
+//   f_d <- fN_d cs + (1 - cs) f_d  [- w_d c drho(f)],  cs = 1 / sqrtf(3).
+// The corrected form reads fN with the neighbour index only for the unshifted slots and the node's
+// own shifted slots otherwise (OutflowNonReflectingPressureCorrection.cu:75-81 take the shifted
+// neighbours of k, not of kN); the same slots are read here.
+template <class S, bool EVEN, bool CORRECTION>
+__global__ void __launch_bounds__(128) bc_outflow_kernel(PressureArgs a, double correction)
+{
+    using C = typename Codec<S>::compute;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nbc)
+        return;
+    uint32_t nk[8], nn[8];
+    node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.box, nk);
+    if (CORRECTION) {
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+            nn[c] = nk[c];
+        nn[0] = (uint32_t)a.kN[i];
+    } else {
+        node_slots((uint32_t)a.kN[i], a.nbx, a.nby, a.nbz, a.box, nn);
+    }
+    S *base = static_cast<S *>(a.dist);
+    C f[27], fn[27];
+    gather_pre<S, EVEN>(base, a.n, nk, f);
+    gather_pre<S, EVEN>(base, a.n, nn, fn);
+    const C cs = C(1) / (C)sqrtf(3.0f);
+    C rho_corr = C(0);
+    if (CORRECTION)
+        rho_corr = (C)correction * density_pyramid(f);
+    const int axis = cx(a.direction) != 0 ? 0 : (cy(a.direction) != 0 ? 1 : 2);
+    const int sgn = axis == 0 ? cx(a.direction) : (axis == 1 ? cy(a.direction) : cz(a.direction));
+#pragma unroll
+    for (int d = 1; d < 27; ++d) {
+        const int c = axis == 0 ? cx(d) : (axis == 1 ? cy(d) : cz(d));
+        if (c != -sgn)
+            continue;
+        C v = fn[d] * cs + (C(1) - cs) * f[d];
+        if (CORRECTION)
+            v = v - weight_t<C>(d) * rho_corr;
+        Codec<S>::store_at(base, (uint64_t)plane<!EVEN>(d) * a.n + nk[shift_class(d)], v, d);
     }
 }
 

@@ -52,7 +52,7 @@ inline uint64_t box_blocks(const BoxState &b)
         static cudaError_t bc(const vfb_level *L, const vfb_bc *bc, int kind, cudaStream_t s,                        \
                               const NodeAddr *box = nullptr);                                                        \
         static cudaError_t pressure(const vfb_level *L, const vfb_directional_bc *bc, cudaStream_t s,                \
-                                    const NodeAddr *box = nullptr);                                                  \
+                                    const NodeAddr *box = nullptr, int kind = 0);                                    \
         static cudaError_t inlet_perturbation(const void *base, void *vel, uint32_t n, uint64_t seed,                \
                                               uint64_t step, double amplitude, cudaStream_t s);                      \
         static cudaError_t init_list(const vfb_level *L, cudaStream_t s);                                          \
@@ -80,7 +80,11 @@ inline uint64_t box_blocks(const BoxState &b)
     };
 
 // BC kinds of Launchers::bc
-enum BCKind : int { kNoSlipBB = 0, kNoSlipInterp = 1, kVelocityBB = 2, kVelocityInterp = 3 };
+enum BCKind : int { kNoSlipBB = 0, kNoSlipInterp = 1, kVelocityBB = 2, kVelocityInterp = 3, kNoSlipInterpIncomp = 4,
+                    kVelocityInterpIncomp = 5, kVelocityWithPressure = 6 };
+// pressure-list kernels of Launchers::pressure
+enum PressureKind : int { kPressureNeqComp = 0, kPressureNeqIncomp = 1, kOutflowNonReflecting = 2,
+                          kOutflowPressureCorrection = 3 };
 
 namespace fast {
 VFB_DECLARE_LAUNCHERS

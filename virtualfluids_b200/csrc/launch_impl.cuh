@@ -122,6 +122,18 @@ cudaError_t Launchers<S>::bc(const vfb_level *L, const vfb_bc *bc, int kind, cud
         if (even) bc_interpolated_kernel<S, true, true><<<G, B, 0, s>>>(a);
         else bc_interpolated_kernel<S, false, true><<<G, B, 0, s>>>(a);
         break;
+    case kNoSlipInterpIncomp:
+        if (even) bc_interpolated_kernel<S, true, false, kBCIncompressible><<<G, B, 0, s>>>(a);
+        else bc_interpolated_kernel<S, false, false, kBCIncompressible><<<G, B, 0, s>>>(a);
+        break;
+    case kVelocityInterpIncomp:
+        if (even) bc_interpolated_kernel<S, true, true, kBCIncompressible><<<G, B, 0, s>>>(a);
+        else bc_interpolated_kernel<S, false, true, kBCIncompressible><<<G, B, 0, s>>>(a);
+        break;
+    case kVelocityWithPressure:
+        if (even) bc_interpolated_kernel<S, true, true, kBCWithPressure><<<G, B, 0, s>>>(a);
+        else bc_interpolated_kernel<S, false, true, kBCWithPressure><<<G, B, 0, s>>>(a);
+        break;
     default:
         return cudaErrorInvalidValue;
     }
@@ -130,7 +142,7 @@ cudaError_t Launchers<S>::bc(const vfb_level *L, const vfb_bc *bc, int kind, cud
 
 template <class S>
 cudaError_t Launchers<S>::pressure(const vfb_level *L, const vfb_directional_bc *bc, cudaStream_t s,
-                                   const NodeAddr *box)
+                                   const NodeAddr *box, int kind)
 {
     if (bc->number_of_bc_nodes == 0)
         return cudaSuccess;
@@ -147,8 +159,28 @@ cudaError_t Launchers<S>::pressure(const vfb_level *L, const vfb_directional_bc 
     a.nbc = bc->number_of_bc_nodes;
     a.direction = bc->direction;
     const unsigned B = 128, G = grid1d(a.nbc, B);
-    if (L->is_even_timestep) bc_pressure_neq_kernel<S, true><<<G, B, 0, s>>>(a);
-    else bc_pressure_neq_kernel<S, false><<<G, B, 0, s>>>(a);
+    const bool even = L->is_even_timestep != 0;
+    const double corr = L->outflow_pressure_correction_factor;
+    switch (kind) {
+    case kPressureNeqComp:
+        if (even) bc_pressure_neq_kernel<S, true><<<G, B, 0, s>>>(a);
+        else bc_pressure_neq_kernel<S, false><<<G, B, 0, s>>>(a);
+        break;
+    case kPressureNeqIncomp:
+        if (even) bc_pressure_neq_kernel<S, true, true><<<G, B, 0, s>>>(a);
+        else bc_pressure_neq_kernel<S, false, true><<<G, B, 0, s>>>(a);
+        break;
+    case kOutflowNonReflecting:
+        if (even) bc_outflow_kernel<S, true, false><<<G, B, 0, s>>>(a, corr);
+        else bc_outflow_kernel<S, false, false><<<G, B, 0, s>>>(a, corr);
+        break;
+    case kOutflowPressureCorrection:
+        if (even) bc_outflow_kernel<S, true, true><<<G, B, 0, s>>>(a, corr);
+        else bc_outflow_kernel<S, false, true><<<G, B, 0, s>>>(a, corr);
+        break;
+    default:
+        return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 

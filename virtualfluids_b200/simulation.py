@@ -51,6 +51,7 @@ class Parameter:
         self.forcing = (0.0, 0.0, 0.0)
         self.storage = N.STORAGE_F64
         self.arith = N.ARITH_FAST
+        self.outflow_pressure_correction_factor = 0.0
 
     def set_viscosity_lb(self, nu: float):
         self.viscosity_lb = float(nu)
@@ -66,6 +67,10 @@ class Parameter:
 
     def set_quadric_limiters(self, p: float, m: float, d: float):
         self.quadric_limiters = (float(p), float(m), float(d))
+
+    def set_outflow_pressure_correction_factor(self, factor: float):
+        """Parameter::setOutflowPressureCorrectionFactor (OutflowNonReflectivePressureCorrection)."""
+        self.outflow_pressure_correction_factor = float(factor)
 
     def set_forcing(self, fx: float, fy: float, fz: float):
         self.forcing = (float(fx), float(fy), float(fz))
@@ -243,6 +248,7 @@ class Simulation:
             L.quadric_limiters[i] = para.quadric_limiters[i]
         L.rho, L.velocity_x, L.velocity_y, L.velocity_z = (x.data_ptr() for x in (self.rho, self.vx, self.vy, self.vz))
         L.pressure = self.press.data_ptr()
+        L.outflow_pressure_correction_factor = para.outflow_pressure_correction_factor
         self.level = L
         self._keep = []
         self._bcs = {}
