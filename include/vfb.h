@@ -252,9 +252,9 @@ enum { VFB_NOSLIP_DELAY_BOUNCE_BACK = 0, VFB_NOSLIP_BOUNCE_BACK = 1, VFB_NOSLIP_
 enum { VFB_PRESSURE_NON_EQUILIBRIUM_INCOMPRESSIBLE = 0, VFB_PRESSURE_NON_EQUILIBRIUM_COMPRESSIBLE = 1,
        VFB_PRESSURE_OUTFLOW_NON_REFLECTIVE = 2, VFB_PRESSURE_OUTFLOW_NON_REFLECTIVE_PRESSURE_CORRECTION = 3,
        VFB_PRESSURE_NOT_SPECIFIED = 4 };
-/* The function for an enum value. *fn = NULL with VFB_OK means "no kernel" (NoSlipDelayBounceBack,
-   whose bounce-back happens through the dummy node; NotSpecified). Variants outside this build
-   return VFB_ERR_UNSUPPORTED. */
+/* The function for an enum value; every variant of the three enums has one. *fn = NULL with
+   VFB_OK means "no kernel" (NoSlipDelayBounceBack, whose bounce-back happens through the dummy
+   node; NotSpecified). A value outside the enum gives VFB_ERR_INVALID_ARGUMENT. */
 int vfb_bc_factory_velocity(int32_t variant, vfb_bc_fn *fn);
 int vfb_bc_factory_noslip(int32_t variant, vfb_bc_fn *fn);
 int vfb_bc_factory_pressure(int32_t variant, vfb_directional_bc_fn *fn);
