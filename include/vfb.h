@@ -269,15 +269,34 @@ enum { VFB_SCALE_COMPRESSIBLE = 0, VFB_SCALE_NOT_SPECIFIED = 1 };
 int vfb_scaling_factory_fine_to_coarse(int32_t variant, int32_t has_turbulent_viscosity, vfb_scaling_fn *fn);
 int vfb_scaling_factory_coarse_to_fine(int32_t variant, int32_t has_turbulent_viscosity, vfb_scaling_fn *fn);
 
-/* ---- (2a) step driver: UpdateGrid27::updateGrid for one level (Calculation/UpdateGrid27.cpp:54-95) */
+/* ---- (2a) step driver: UpdateGrid27::updateGrid (Calculation/UpdateGrid27.cpp:54-95) over one or more
+   refinement levels ----------------------------------------------------------------------------- */
 typedef struct vfb_simulation vfb_simulation;
+#define VFB_MAX_LEVELS 16
 /* kernel_name as Parameter::configureMainKernel; VFB_ERR_UNKNOWN_KERNEL for unknown names */
 int vfb_simulation_create(const char *kernel_name, vfb_simulation **out);
 int vfb_simulation_destroy(vfb_simulation *sim);
-/* the level description is copied; device memory stays caller-owned */
+/* the level that vfb_simulation_set_level and the BC, geometry and drag/lift setters below
+   configure: 0 (the coarsest, the default) up to the number of levels, which adds a finer level
+   (Parameter::getParD(level)) */
+int vfb_simulation_use_level(vfb_simulation *sim, int32_t level);
+int vfb_simulation_number_of_levels(const vfb_simulation *sim, int32_t *number_of_levels);
+/* the selected level's description, copied; device memory stays caller-owned; level->level must be
+   the selected level (forces are scaled by 2^-level) */
 int vfb_simulation_set_level(vfb_simulation *sim, const vfb_level *level, const uint32_t *fluid_node_indices,
                              uint32_t number_of_fluid_nodes);
-/* BC lists (copied descriptors) and factory choices */
+/* GridScalingFactory::setScalingFactory (VFB_SCALE_*); with more than one level a run without it is
+   VFB_ERR_SCALING_UNSET ("There is more than one level, but no scalingFactory was provided.") */
+int vfb_simulation_set_scaling_factory(vfb_simulation *sim, int32_t variant, int32_t has_turbulent_viscosity);
+/* the interpolation cells between coarse_level and coarse_level + 1 (both added before), the coarse level's
+   fineToCoarse / neighborFineToCoarse and coarseToFine / neighborCoarseToFine (descriptors copied,
+   device arrays caller-owned); unset pairs have no cells */
+int vfb_simulation_set_interpolation_cells(vfb_simulation *sim, int32_t coarse_level,
+                                           const vfb_interpolation_cells *fine_to_coarse,
+                                           const vfb_interpolation_cell_neighbor *fine_to_coarse_offsets,
+                                           const vfb_interpolation_cells *coarse_to_fine,
+                                           const vfb_interpolation_cell_neighbor *coarse_to_fine_offsets);
+/* BC lists of the selected level (copied descriptors) and factory choices */
 int vfb_simulation_set_velocity_bc(vfb_simulation *sim, const vfb_bc *bc, int32_t variant);
 int vfb_simulation_set_noslip_bc(vfb_simulation *sim, const vfb_bc *bc, int32_t variant);
 int vfb_simulation_add_pressure_bc(vfb_simulation *sim, const vfb_directional_bc *bc, int32_t variant);
@@ -291,11 +310,17 @@ int vfb_simulation_set_geometry_bc(vfb_simulation *sim, const vfb_bc *bc, int32_
 size_t vfb_simulation_drag_lift_workspace_bytes(uint32_t number_of_geometry_nodes);
 int vfb_simulation_set_drag_lift(vfb_simulation *sim, void *workspace, size_t workspace_bytes, double *force_history,
                                  uint32_t history_steps);
-/* checks the BoundaryConditionKernelManager rules: a BC with nodes but no kernel is VFB_ERR_BC_UNSET */
+/* checks the BoundaryConditionKernelManager rules (a BC with nodes but no kernel is VFB_ERR_BC_UNSET)
+   and the GridScalingKernelManager ones (VFB_ERR_SCALING_UNSET); every level set, one storage and
+   arithmetic for all */
 int vfb_simulation_check(const vfb_simulation *sim);
-/* run steps: collision, velocity, no-slip then geometry BCs, parity toggle, drag/lift, pressure BCs */
+/* run steps of the coarsest level. A level's step: collision, velocity, no-slip then geometry BCs,
+   parity toggle, drag/lift, pressure BCs. A level with a finer one lets that one take two steps
+   first and after its own step interpolates fine to coarse, then coarse to fine. */
 int vfb_simulation_run(vfb_simulation *sim, uint32_t steps, void *stream);
+/* parity of the coarsest level / of a given level */
 int vfb_simulation_is_even_timestep(const vfb_simulation *sim, int32_t *is_even);
+int vfb_simulation_level_is_even_timestep(const vfb_simulation *sim, int32_t level, int32_t *is_even);
 
 /* ---- (2b) structured boxes --------------------------------------------------------------- */
 /* A full box of nx*ny*nz nodes, node k = x + nx (y + ny z), neighbours by index arithmetic.

@@ -414,6 +414,15 @@ int orc_run_geo(orc_level *L, const uint32_t *fluid, uint32_t n_fluid, int *is_e
                 const double forces[3], const orc_velocity *vel, const orc_noslip *ns, const orc_noslip *geo,
                 double *drag_history, const orc_pressure *pr, int n_pr, int steps, int n_threads)
 {
+    return orc_run_level(L, 0, fluid, n_fluid, is_even, omega, lim, forces, vel, ns, geo, drag_history, pr, n_pr, steps,
+                         n_threads);
+}
+
+int orc_run_level(orc_level *L, int level, const uint32_t *fluid, uint32_t n_fluid, int *is_even, double omega,
+                  const double lim[3], const double forces[3], const orc_velocity *vel, const orc_noslip *ns,
+                  const orc_noslip *geo, double *drag_history, const orc_pressure *pr, int n_pr, int steps,
+                  int n_threads)
+{
     const uint32_t ng = geo ? geo->n : 0;
     double *work = NULL;
     if (drag_history && ng) {
@@ -422,7 +431,7 @@ int orc_run_geo(orc_level *L, const uint32_t *fluid, uint32_t n_fluid, int *is_e
             return -1;
     }
     for (int t = 0; t < steps; ++t) {
-        orc_collision(L, fluid, n_fluid, *is_even, omega, lim, forces, 0, NULL, NULL, NULL, NULL, n_threads);
+        orc_collision(L, fluid, n_fluid, *is_even, omega, lim, forces, level, NULL, NULL, NULL, NULL, n_threads);
         if (vel && vel->n) {
             if (vel->kind == 1)
                 orc_bc_velocity_bounce_back(L, vel->k, vel->q, vel->n, *is_even, vel->ux, vel->uy, vel->uz);

@@ -133,6 +133,12 @@ int orc_run_geo(orc_level *L, const uint32_t *fluid, uint32_t n_fluid, int *is_e
                 const double forces[3], const orc_velocity *vel, const orc_noslip *ns, const orc_noslip *geo,
                 double *drag_history, const orc_pressure *pr, int n_pr, int steps, int n_threads);
 
+/* the same for a refinement level: forces scaled by 2^-level (KernelUtilities.h getForceFactor) */
+int orc_run_level(orc_level *L, int level, const uint32_t *fluid, uint32_t n_fluid, int *is_even, double omega,
+                  const double lim[3], const double forces[3], const orc_velocity *vel, const orc_noslip *ns,
+                  const orc_noslip *geo, double *drag_history, const orc_pressure *pr, int n_pr, int steps,
+                  int n_threads);
+
 int orc_run(orc_level *L, const uint32_t *fluid, uint32_t n_fluid, int *is_even, double omega, const double lim[3],
             const double forces[3], const orc_velocity *vel, const orc_noslip *ns, const orc_pressure *pr, int n_pr,
             int steps, int n_threads);

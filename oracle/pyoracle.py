@@ -142,8 +142,9 @@ class OracleLevel:
     """A level in the reference layout, advanced on the host by the oracle."""
 
     def __init__(self, grid, omega, lim=(0.01, 0.01, 0.01), forces=(0.0, 0.0, 0.0), velocity_kind=1, noslip_kind=1,
-                 geometry_kind=0, drag_lift=False):
+                 geometry_kind=0, drag_lift=False, level=0):
         self.grid = grid
+        self.level = int(level)
         self.n = grid.number_of_nodes
         self.f = np.zeros(27 * self.n, dtype=np.float64)
         self.nb = [np.ascontiguousarray(grid.neighbor[a].astype(np.uint32)) for a in range(3)]
@@ -200,13 +201,13 @@ class OracleLevel:
         self.is_even.value = 1
 
     def run(self, steps, threads=0):
-        lib().orc_run_geo.argtypes = [_P, _P, C.c_uint32, C.POINTER(C.c_int), C.c_double, _P, _P, _P, _P, _P, _P, _P,
-                                      C.c_int, C.c_int, C.c_int]
+        lib().orc_run_level.argtypes = [_P, C.c_int, _P, C.c_uint32, C.POINTER(C.c_int), C.c_double, _P, _P, _P, _P,
+                                        _P, _P, _P, C.c_int, C.c_int, C.c_int]
         hist = np.zeros((int(steps), 3)) if self.drag_lift else None
-        rc = lib().orc_run_geo(C.byref(self.L), ptr(self.fluid), self.fluid.size, C.byref(self.is_even), self.omega,
-                               ptr(self.lim), ptr(self.forces), C.byref(self.vel) if self.vel else None,
-                               C.byref(self.ns) if self.ns else None, C.byref(self.geo_bc) if self.geo_bc else None,
-                               ptr(hist) if hist is not None else None, self.pr, self.n_pr, int(steps), int(threads))
+        rc = lib().orc_run_level(C.byref(self.L), self.level, ptr(self.fluid), self.fluid.size, C.byref(self.is_even),
+                                 self.omega, ptr(self.lim), ptr(self.forces), C.byref(self.vel) if self.vel else None,
+                                 C.byref(self.ns) if self.ns else None, C.byref(self.geo_bc) if self.geo_bc else None,
+                                 ptr(hist) if hist is not None else None, self.pr, self.n_pr, int(steps), int(threads))
         if rc != 0:
             raise MemoryError("oracle step driver could not allocate its drag workspace")
         if hist is not None:
@@ -221,6 +222,43 @@ class OracleLevel:
         out = np.zeros(2)
         lib().orc_mass_energy(C.byref(self.L), ptr(self.fluid), self.fluid.size, self.is_even.value, ptr(out))
         return float(out[0]), float(out[1])
+
+
+class OracleMultiLevel:
+    """Nested refinement levels advanced on the host: UpdateGrid27::updateGrid's recursion
+    (UpdateGrid27.cpp:54-95; a level with a finer one lets it take two steps first) followed by
+    Refinement_noExchange (RefinementStrategy.cpp:169-178: fine to coarse, then coarse to fine).
+    omega of level l is 1 / (3 nu 2^l + 1/2) (Parameter.cpp:404-406); forces scale by 2^-l."""
+
+    def __init__(self, mgrid, nu, lim=(0.01, 0.01, 0.01), forces=(0.0, 0.0, 0.0), velocity_kind=1, noslip_kind=1):
+        self.levels = [OracleLevel(g, 1.0 / (3.0 * (nu * 2.0 ** l) + 0.5), lim, forces, velocity_kind, noslip_kind,
+                                   level=l) for l, g in enumerate(mgrid.levels)]
+        self.cells = []
+        for it in mgrid.interfaces:
+            arrs = [np.ascontiguousarray(a.astype(np.uint32)) for a in (it.coarse_fc, it.fine_fc, it.coarse_cf, it.fine_cf)]
+            offs = [np.ascontiguousarray(o[a], dtype=np.float64) for o in (it.offsets_fc, it.offsets_cf) for a in range(3)]
+            self.cells.append((arrs, offs))
+
+    def init(self, level, rho=None, ux=None, uy=None, uz=None):
+        self.levels[level].init(rho, ux, uy, uz)
+
+    def run(self, steps):
+        for _ in range(int(steps)):
+            self._update(0)
+
+    def _update(self, l):
+        finer = l + 1 < len(self.levels)
+        if finer:
+            self._update(l + 1)
+            self._update(l + 1)
+        self.levels[l].run(1)
+        if finer:
+            c, f = self.levels[l], self.levels[l + 1]
+            (cfc, ffc, ccf, fcf), offs = self.cells[l]
+            lib().orc_scale_fc(C.byref(c.L), C.byref(f.L), ptr(cfc), ptr(ffc), cfc.size, *(ptr(o) for o in offs[:3]),
+                               c.is_even.value, c.omega, f.omega)
+            lib().orc_scale_cf(C.byref(c.L), C.byref(f.L), ptr(ccf), ptr(fcf), ccf.size, *(ptr(o) for o in offs[3:]),
+                               c.is_even.value, c.omega, f.omega)
 
 
 def k17(f, omega, lim=(0.01, 0.01, 0.01), force=(0.0, 0.0, 0.0), dtype=np.float64):

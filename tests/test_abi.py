@@ -146,6 +146,51 @@ def test_simulation_manager_rules():
         lib.vfb_simulation_destroy(sim)
 
 
+def test_multilevel_driver_rules():
+    """Levels are added one at a time; vfb_level::level must be the level's index; more than one
+    level needs the scaling factory (GridScalingKernelManager.cpp:45-62) and, where a pair of levels
+    has interpolation cells, a function for them (checkScalingFunction); one storage for all."""
+    from virtualfluids_b200 import _native as N
+    lib = N.lib()
+    sim = C.c_void_p()
+    N.check(lib.vfb_simulation_create(b"K17CompressibleNavierStokes", C.byref(sim)))
+    try:
+        L0, L1 = _fake_level(N), _fake_level(N)
+        N.check(lib.vfb_simulation_set_level(sim, C.byref(L0), C.c_void_p(0x2000), 5))
+        assert lib.vfb_simulation_use_level(sim, 2) == N.VFB_ERR_INVALID_ARGUMENT     # skips level 1
+        assert lib.vfb_simulation_use_level(sim, -1) == N.VFB_ERR_INVALID_ARGUMENT
+        N.check(lib.vfb_simulation_use_level(sim, 1))
+        n = C.c_int32()
+        N.check(lib.vfb_simulation_number_of_levels(sim, C.byref(n)))
+        assert n.value == 2
+        assert lib.vfb_simulation_check(sim) == N.VFB_ERR_INVALID_ARGUMENT           # level 1 not set
+        assert lib.vfb_simulation_set_level(sim, C.byref(L1), C.c_void_p(0x2000), 5) == N.VFB_ERR_INVALID_ARGUMENT
+        L1.level = 1
+        N.check(lib.vfb_simulation_set_level(sim, C.byref(L1), C.c_void_p(0x2000), 5))
+        assert lib.vfb_simulation_check(sim) == N.VFB_ERR_SCALING_UNSET
+        assert "no scalingFactory" in N.lib().vfb_last_error().decode()
+        cells = N.InterpolationCells(0x5000, 0x5100, 7)
+        offs = N.InterpolationCellNeighbor(0x5200, 0x5300, 0x5400)
+        assert lib.vfb_simulation_set_interpolation_cells(sim, 1, C.byref(cells), C.byref(offs), C.byref(cells),
+                                                          C.byref(offs)) == N.VFB_ERR_INVALID_ARGUMENT  # finest level
+        N.check(lib.vfb_simulation_set_interpolation_cells(sim, 0, C.byref(cells), C.byref(offs), C.byref(cells),
+                                                           C.byref(offs)))
+        N.check(lib.vfb_simulation_set_scaling_factory(sim, N.SCALE_NOT_SPECIFIED, 0))
+        assert lib.vfb_simulation_check(sim) == N.VFB_ERR_SCALING_UNSET               # cells but no function
+        assert lib.vfb_simulation_set_scaling_factory(sim, N.SCALE_COMPRESSIBLE, 1) == N.VFB_ERR_UNSUPPORTED
+        N.check(lib.vfb_simulation_set_scaling_factory(sim, N.SCALE_COMPRESSIBLE, 0))
+        N.check(lib.vfb_simulation_check(sim))
+        L1.storage = N.STORAGE_F32
+        N.check(lib.vfb_simulation_set_level(sim, C.byref(L1), C.c_void_p(0x2000), 5))
+        assert lib.vfb_simulation_check(sim) == N.VFB_ERR_INVALID_ARGUMENT            # mixed storage
+        ev = C.c_int32()
+        N.check(lib.vfb_simulation_level_is_even_timestep(sim, 1, C.byref(ev)))
+        assert ev.value == 1
+        assert lib.vfb_simulation_level_is_even_timestep(sim, 2, C.byref(ev)) == N.VFB_ERR_INVALID_ARGUMENT
+    finally:
+        lib.vfb_simulation_destroy(sim)
+
+
 def test_argument_validation_without_launching():
     from virtualfluids_b200 import _native as N
     lib = N.lib()

@@ -12,10 +12,11 @@ library raises there; there is no fallback.
 from . import _native
 from ._native import VfbError, lib
 from .box import Box
-from .grid import ListGrid
+from .grid import Interface, ListGrid, MultiLevelGrid, refine_box
 from .pool import Pool
 from .simulation import (BoundaryConditionFactory, GridScalingFactory, InterpolationCells, Parameter, Simulation,
                          scale_coarse_to_fine, scale_fine_to_coarse)
 
-__all__ = ["Box", "BoundaryConditionFactory", "GridScalingFactory", "InterpolationCells", "ListGrid", "Parameter", "Pool",
-           "Simulation", "VfbError", "lib", "scale_coarse_to_fine", "scale_fine_to_coarse", "_native"]
+__all__ = ["Box", "BoundaryConditionFactory", "GridScalingFactory", "Interface", "InterpolationCells", "ListGrid",
+           "MultiLevelGrid", "Parameter", "Pool", "Simulation", "VfbError", "lib", "refine_box", "scale_coarse_to_fine",
+           "scale_fine_to_coarse", "_native"]

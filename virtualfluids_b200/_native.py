@@ -171,6 +171,14 @@ SIGNATURES = {
     "vfb_simulation_check": (C.c_int, [C.c_void_p]),
     "vfb_simulation_run": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p]),
     "vfb_simulation_is_even_timestep": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "vfb_simulation_level_is_even_timestep": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
+    "vfb_simulation_use_level": (C.c_int, [C.c_void_p, C.c_int32]),
+    "vfb_simulation_number_of_levels": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "vfb_simulation_set_scaling_factory": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+    "vfb_simulation_set_interpolation_cells": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(InterpolationCells),
+                                                         C.POINTER(InterpolationCellNeighbor),
+                                                         C.POINTER(InterpolationCells),
+                                                         C.POINTER(InterpolationCellNeighbor)]),
     "vfb_box_create": (C.c_int, [C.POINTER(BoxDesc), C.POINTER(C.c_void_p)]),
     "vfb_box_destroy": (C.c_int, [C.c_void_p]),
     "vfb_box_device_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),

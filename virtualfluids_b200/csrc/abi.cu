@@ -616,8 +616,10 @@ int vfb_scaling_factory_coarse_to_fine(int32_t variant, int32_t has_turbulent_vi
 // ---------------------------------------------------------------------------------------------
 // (2a) step driver
 // ---------------------------------------------------------------------------------------------
-struct vfb_simulation {
-    int kernel_id = 0;
+namespace {
+// One refinement level of the driver: the LBMSimulationParameter fields of that level and its BC
+// lists (Parameter::getParD(level)).
+struct SimLevel {
     bool has_level = false;
     vfb_level level{};
     const uint32_t *fluid = nullptr;
@@ -638,7 +640,23 @@ struct vfb_simulation {
     double *drag_history = nullptr;   // 3 doubles per step, ring of drag_history_len steps
     uint32_t drag_history_len = 0;
     uint64_t drag_steps = 0;
+    // interpolation cells between this level and the next finer one (fineToCoarse,
+    // neighborFineToCoarse, coarseToFine, neighborCoarseToFine of the coarse level)
+    vfb_interpolation_cells fc{}, cf{};
+    vfb_interpolation_cell_neighbor fc_offsets{}, cf_offsets{};
 };
+} // namespace
+
+struct vfb_simulation {
+    int kernel_id = 0;
+    std::vector<SimLevel> levels = std::vector<SimLevel>(1);
+    int32_t cursor = 0;               // the level the setters configure
+    bool scaling_set = false;         // GridScalingFactory given
+    vfb_scaling_fn scale_fc = nullptr;
+    vfb_scaling_fn scale_cf = nullptr;
+};
+
+static SimLevel &current(vfb_simulation *sim) { return sim->levels[(size_t)sim->cursor]; }
 
 extern "C" {
 
@@ -663,6 +681,26 @@ int vfb_simulation_destroy(vfb_simulation *sim)
     return VFB_OK;
 }
 
+int vfb_simulation_use_level(vfb_simulation *sim, int32_t level)
+{
+    if (!sim)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL simulation");
+    if (level < 0 || level > (int32_t)sim->levels.size() || level >= VFB_MAX_LEVELS)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "levels are added one at a time, from the coarsest, up to VFB_MAX_LEVELS");
+    if (level == (int32_t)sim->levels.size())
+        sim->levels.emplace_back();
+    sim->cursor = level;
+    return VFB_OK;
+}
+
+int vfb_simulation_number_of_levels(const vfb_simulation *sim, int32_t *n)
+{
+    if (!sim || !n)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    *n = (int32_t)sim->levels.size();
+    return VFB_OK;
+}
+
 int vfb_simulation_set_level(vfb_simulation *sim, const vfb_level *level, const uint32_t *fluid, uint32_t n)
 {
     if (!sim)
@@ -672,10 +710,13 @@ int vfb_simulation_set_level(vfb_simulation *sim, const vfb_level *level, const 
         return st;
     if (n && !fluid)
         return fail(VFB_ERR_INVALID_ARGUMENT, "fluid node indices are NULL");
-    sim->level = *level;
-    sim->fluid = fluid;
-    sim->n_fluid = n;
-    sim->has_level = true;
+    if (level->level != sim->cursor)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "vfb_level::level must equal the selected level");
+    SimLevel &S = current(sim);
+    S.level = *level;
+    S.fluid = fluid;
+    S.n_fluid = n;
+    S.has_level = true;
     return VFB_OK;
 }
 
@@ -687,9 +728,10 @@ int vfb_simulation_set_velocity_bc(vfb_simulation *sim, const vfb_bc *bc, int32_
     int st = vfb_bc_factory_velocity(variant, &fn);
     if (st)
         return st;
-    sim->velocity = *bc;
-    sim->velocity_fn = fn;
-    sim->velocity_set = true;
+    SimLevel &S = current(sim);
+    S.velocity = *bc;
+    S.velocity_fn = fn;
+    S.velocity_set = true;
     return VFB_OK;
 }
 
@@ -701,9 +743,10 @@ int vfb_simulation_set_noslip_bc(vfb_simulation *sim, const vfb_bc *bc, int32_t 
     int st = vfb_bc_factory_noslip(variant, &fn);
     if (st)
         return st;
-    sim->noslip = *bc;
-    sim->noslip_fn = fn;
-    sim->noslip_set = true;
+    SimLevel &S = current(sim);
+    S.noslip = *bc;
+    S.noslip_fn = fn;
+    S.noslip_set = true;
     return VFB_OK;
 }
 
@@ -715,8 +758,9 @@ int vfb_simulation_add_pressure_bc(vfb_simulation *sim, const vfb_directional_bc
     int st = vfb_bc_factory_pressure(variant, &fn);
     if (st)
         return st;
-    sim->pressure.push_back(*bc);
-    sim->pressure_fn.push_back(fn);
+    SimLevel &S = current(sim);
+    S.pressure.push_back(*bc);
+    S.pressure_fn.push_back(fn);
     return VFB_OK;
 }
 
@@ -730,9 +774,10 @@ int vfb_simulation_set_geometry_bc(vfb_simulation *sim, const vfb_bc *bc, int32_
     int st = vfb_bc_factory_noslip(variant, &fn);
     if (st)
         return st;
-    sim->geometry = *bc;
-    sim->geometry_fn = fn;
-    sim->geometry_set = true;
+    SimLevel &S = current(sim);
+    S.geometry = *bc;
+    S.geometry_fn = fn;
+    S.geometry_set = true;
     return VFB_OK;
 }
 
@@ -746,24 +791,66 @@ int vfb_simulation_set_drag_lift(vfb_simulation *sim, void *workspace, size_t wo
 {
     if (!sim)
         return fail(VFB_ERR_INVALID_ARGUMENT, "NULL simulation");
+    SimLevel &S = current(sim);
     if (!workspace) {
-        sim->drag_work = nullptr;
-        sim->drag_history = nullptr;
-        sim->drag_history_len = 0;
+        S.drag_work = nullptr;
+        S.drag_history = nullptr;
+        S.drag_history_len = 0;
         return VFB_OK;
     }
-    if (!sim->geometry_set)
+    if (!S.geometry_set)
         return fail(VFB_ERR_INVALID_ARGUMENT, "drag and lift need a geometry boundary condition");
     if (!force_history || history_steps == 0)
         return fail(VFB_ERR_INVALID_ARGUMENT, "drag and lift need a force history of at least one step");
-    if (workspace_bytes < vfb_simulation_drag_lift_workspace_bytes(sim->geometry.number_of_bc_nodes))
+    if (workspace_bytes < vfb_simulation_drag_lift_workspace_bytes(S.geometry.number_of_bc_nodes))
         return fail(VFB_ERR_INVALID_ARGUMENT, "workspace too small");
     if ((reinterpret_cast<uintptr_t>(workspace) & 7u) != 0)
         return fail(VFB_ERR_INVALID_ARGUMENT, "workspace must be 8-byte aligned");
-    sim->drag_work = static_cast<double *>(workspace);
-    sim->drag_history = force_history;
-    sim->drag_history_len = history_steps;
-    sim->drag_steps = 0;
+    S.drag_work = static_cast<double *>(workspace);
+    S.drag_history = force_history;
+    S.drag_history_len = history_steps;
+    S.drag_steps = 0;
+    return VFB_OK;
+}
+
+int vfb_simulation_set_scaling_factory(vfb_simulation *sim, int32_t variant, int32_t has_turbulent_viscosity)
+{
+    if (!sim)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL simulation");
+    vfb_scaling_fn fc = nullptr, cf = nullptr;
+    int st = vfb_scaling_factory_fine_to_coarse(variant, has_turbulent_viscosity, &fc);
+    if (st)
+        return st;
+    st = vfb_scaling_factory_coarse_to_fine(variant, has_turbulent_viscosity, &cf);
+    if (st)
+        return st;
+    sim->scale_fc = fc;
+    sim->scale_cf = cf;
+    sim->scaling_set = true;
+    return VFB_OK;
+}
+
+int vfb_simulation_set_interpolation_cells(vfb_simulation *sim, int32_t coarse_level,
+                                           const vfb_interpolation_cells *fine_to_coarse,
+                                           const vfb_interpolation_cell_neighbor *fine_to_coarse_offsets,
+                                           const vfb_interpolation_cells *coarse_to_fine,
+                                           const vfb_interpolation_cell_neighbor *coarse_to_fine_offsets)
+{
+    if (!sim || !fine_to_coarse || !fine_to_coarse_offsets || !coarse_to_fine || !coarse_to_fine_offsets)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (coarse_level < 0 || coarse_level + 1 >= (int32_t)sim->levels.size())
+        return fail(VFB_ERR_INVALID_ARGUMENT, "coarse_level and the level above it must have been added");
+    const vfb_interpolation_cells *c[2] = { fine_to_coarse, coarse_to_fine };
+    const vfb_interpolation_cell_neighbor *o[2] = { fine_to_coarse_offsets, coarse_to_fine_offsets };
+    for (int i = 0; i < 2; ++i)
+        if (c[i]->number_of_cells &&
+            (!c[i]->fine_cell_indices || !c[i]->coarse_cell_indices || !o[i]->x || !o[i]->y || !o[i]->z))
+            return fail(VFB_ERR_INVALID_ARGUMENT, "interpolation cell arrays are NULL");
+    SimLevel &S = sim->levels[(size_t)coarse_level];
+    S.fc = *fine_to_coarse;
+    S.fc_offsets = *fine_to_coarse_offsets;
+    S.cf = *coarse_to_fine;
+    S.cf_offsets = *coarse_to_fine_offsets;
     return VFB_OK;
 }
 
@@ -771,47 +858,127 @@ int vfb_simulation_check(const vfb_simulation *sim)
 {
     if (!sim)
         return fail(VFB_ERR_INVALID_ARGUMENT, "NULL simulation");
-    if (!sim->has_level)
-        return fail(VFB_ERR_INVALID_ARGUMENT, "no level set");
-    if (sim->velocity_set && sim->velocity.number_of_bc_nodes > 0 && !sim->velocity_fn)
-        return fail(VFB_ERR_BC_UNSET, "Velocity boundary condition has nodes but no kernel");
-    for (size_t i = 0; i < sim->pressure.size(); ++i)
-        if (sim->pressure[i].number_of_bc_nodes > 0 && !sim->pressure_fn[i])
-            return fail(VFB_ERR_BC_UNSET, "Pressure boundary condition has nodes but no kernel");
+    const size_t nl = sim->levels.size();
+    for (size_t l = 0; l < nl; ++l) {
+        const SimLevel &S = sim->levels[l];
+        if (!S.has_level)
+            return fail(VFB_ERR_INVALID_ARGUMENT, "level " + std::to_string(l) + " is not set");
+        if (S.velocity_set && S.velocity.number_of_bc_nodes > 0 && !S.velocity_fn)
+            return fail(VFB_ERR_BC_UNSET, "Velocity boundary condition has nodes but no kernel");
+        for (size_t i = 0; i < S.pressure.size(); ++i)
+            if (S.pressure[i].number_of_bc_nodes > 0 && !S.pressure_fn[i])
+                return fail(VFB_ERR_BC_UNSET, "Pressure boundary condition has nodes but no kernel");
+        if (S.level.storage != sim->levels[0].level.storage || S.level.arith != sim->levels[0].level.arith)
+            return fail(VFB_ERR_INVALID_ARGUMENT, "all levels must share storage and arithmetic");
+    }
+    // GridScalingKernelManager ctor (GridScalingKernelManager.cpp:45-62, checkScalingFunction)
+    if (nl > 1) {
+        if (!sim->scaling_set)
+            return fail(VFB_ERR_SCALING_UNSET, "There is more than one level, but no scalingFactory was provided.");
+        for (size_t l = 0; l + 1 < nl; ++l) {
+            if (!sim->scale_fc && sim->levels[l].fc.number_of_cells > 0)
+                return fail(VFB_ERR_SCALING_UNSET, "The scaling function scalingFineToCoarse was not set!");
+            if (!sim->scale_cf && sim->levels[l].cf.number_of_cells > 0)
+                return fail(VFB_ERR_SCALING_UNSET, "The scaling function scalingCoarseToFine was not set!");
+        }
+    }
     return VFB_OK;
 }
 
-static int run_geometry_post(vfb_simulation *sim, void *stream)
+static int run_geometry_post(SimLevel &S, void *stream)
 {
-    vfb_level &L = sim->level;
-    const uint32_t ng = sim->geometry.number_of_bc_nodes;
-    if (!sim->geometry_set || ng == 0)
+    vfb_level &L = S.level;
+    const uint32_t ng = S.geometry.number_of_bc_nodes;
+    if (!S.geometry_set || ng == 0)
         return VFB_OK;
-    if (sim->drag_work) {
-        double *w = sim->drag_work;
-        int st = vfb_drag_lift_post_27(&L, &sim->geometry, w + 3 * (size_t)ng, w + 4 * (size_t)ng, w + 5 * (size_t)ng, stream);
+    if (S.drag_work) {
+        double *w = S.drag_work;
+        int st = vfb_drag_lift_post_27(&L, &S.geometry, w + 3 * (size_t)ng, w + 4 * (size_t)ng, w + 5 * (size_t)ng, stream);
         if (st)
             return st;
     }
-    return sim->geometry_fn ? sim->geometry_fn(&L, &sim->geometry, stream) : VFB_OK;
+    return S.geometry_fn ? S.geometry_fn(&L, &S.geometry, stream) : VFB_OK;
 }
 
-static int run_geometry_pre(vfb_simulation *sim, void *stream)
+static int run_geometry_pre(SimLevel &S, void *stream)
 {
-    vfb_level &L = sim->level;
-    const uint32_t ng = sim->geometry.number_of_bc_nodes;
-    if (!sim->geometry_set || ng == 0 || !sim->drag_work)
+    vfb_level &L = S.level;
+    const uint32_t ng = S.geometry.number_of_bc_nodes;
+    if (!S.geometry_set || ng == 0 || !S.drag_work)
         return VFB_OK;
-    double *w = sim->drag_work;
-    int st = vfb_drag_lift_pre_27(&L, &sim->geometry, w, w + ng, w + 2 * (size_t)ng, stream);
+    double *w = S.drag_work;
+    int st = vfb_drag_lift_pre_27(&L, &S.geometry, w, w + ng, w + 2 * (size_t)ng, stream);
     if (st)
         return st;
     const double *pre[3] = { w, w + ng, w + 2 * (size_t)ng };
     const double *post[3] = { w + 3 * (size_t)ng, w + 4 * (size_t)ng, w + 5 * (size_t)ng };
-    double *out = sim->drag_history + 3 * (sim->drag_steps % sim->drag_history_len);
+    double *out = S.drag_history + 3 * (S.drag_steps % S.drag_history_len);
     const cudaError_t e = vfb::drag_lift_sum(pre, post, ng, w + 6 * (size_t)ng, out, as_stream(stream));
-    ++sim->drag_steps;
+    ++S.drag_steps;
     return cuda_status(e, "drag/lift sum");
+}
+
+// one time step of one level: collision, post-collision BCs (velocity, no-slip, geometry), parity
+// toggle, pre-collision BCs (pressure) (UpdateGrid27.cpp:66-84)
+static int step_level(SimLevel &S, void *stream)
+{
+    vfb_level &L = S.level;
+    int st = vfb_k17_run_on_indices(&L, S.fluid, S.n_fluid, VFB_COLLISION_DEFAULT, stream);
+    if (st)
+        return st;
+    if (S.velocity_fn && S.velocity.number_of_bc_nodes) {
+        st = S.velocity_fn(&L, &S.velocity, stream);
+        if (st)
+            return st;
+    }
+    if (S.noslip_fn && S.noslip.number_of_bc_nodes) {
+        st = S.noslip_fn(&L, &S.noslip, stream);
+        if (st)
+            return st;
+    }
+    st = run_geometry_post(S, stream);
+    if (st)
+        return st;
+    L.is_even_timestep = !L.is_even_timestep;
+    st = run_geometry_pre(S, stream);
+    if (st)
+        return st;
+    for (size_t i = 0; i < S.pressure.size(); ++i) {
+        if (!S.pressure_fn[i] || !S.pressure[i].number_of_bc_nodes)
+            continue;
+        st = S.pressure_fn[i](&L, &S.pressure[i], stream);
+        if (st)
+            return st;
+    }
+    return VFB_OK;
+}
+
+// UpdateGrid27::updateGrid (UpdateGrid27.cpp:54-95): a level that has a finer one first lets it
+// take two steps, then takes its own, then interpolates fine to coarse and coarse to fine
+// (Refinement_noExchange, RefinementStrategy.cpp:169-178).
+static int update_level(vfb_simulation *sim, size_t l, void *stream)
+{
+    const bool has_finer = l + 1 < sim->levels.size();
+    int st;
+    if (has_finer) {
+        if ((st = update_level(sim, l + 1, stream)) != VFB_OK)
+            return st;
+        if ((st = update_level(sim, l + 1, stream)) != VFB_OK)
+            return st;
+    }
+    SimLevel &S = sim->levels[l];
+    if ((st = step_level(S, stream)) != VFB_OK)
+        return st;
+    if (has_finer) {
+        SimLevel &F = sim->levels[l + 1];
+        if (sim->scale_fc && S.fc.number_of_cells &&
+            (st = sim->scale_fc(&S.level, &F.level, &S.fc, &S.fc_offsets, stream)) != VFB_OK)
+            return st;
+        if (sim->scale_cf && S.cf.number_of_cells &&
+            (st = sim->scale_cf(&S.level, &F.level, &S.cf, &S.cf_offsets, stream)) != VFB_OK)
+            return st;
+    }
+    return VFB_OK;
 }
 
 int vfb_simulation_run(vfb_simulation *sim, uint32_t steps, void *stream)
@@ -819,44 +986,24 @@ int vfb_simulation_run(vfb_simulation *sim, uint32_t steps, void *stream)
     int st = vfb_simulation_check(sim);
     if (st)
         return st;
-    vfb_level &L = sim->level;
-    for (uint32_t t = 0; t < steps; ++t) {
-        st = vfb_k17_run_on_indices(&L, sim->fluid, sim->n_fluid, VFB_COLLISION_DEFAULT, stream);
-        if (st)
+    for (uint32_t t = 0; t < steps; ++t)
+        if ((st = update_level(sim, 0, stream)) != VFB_OK)
             return st;
-        if (sim->velocity_fn && sim->velocity.number_of_bc_nodes) {
-            st = sim->velocity_fn(&L, &sim->velocity, stream);
-            if (st)
-                return st;
-        }
-        if (sim->noslip_fn && sim->noslip.number_of_bc_nodes) {
-            st = sim->noslip_fn(&L, &sim->noslip, stream);
-            if (st)
-                return st;
-        }
-        st = run_geometry_post(sim, stream);
-        if (st)
-            return st;
-        L.is_even_timestep = !L.is_even_timestep;
-        st = run_geometry_pre(sim, stream);
-        if (st)
-            return st;
-        for (size_t i = 0; i < sim->pressure.size(); ++i) {
-            if (!sim->pressure_fn[i] || !sim->pressure[i].number_of_bc_nodes)
-                continue;
-            st = sim->pressure_fn[i](&L, &sim->pressure[i], stream);
-            if (st)
-                return st;
-        }
-    }
     return VFB_OK;
 }
 
 int vfb_simulation_is_even_timestep(const vfb_simulation *sim, int32_t *is_even)
 {
+    return vfb_simulation_level_is_even_timestep(sim, 0, is_even);
+}
+
+int vfb_simulation_level_is_even_timestep(const vfb_simulation *sim, int32_t level, int32_t *is_even)
+{
     if (!sim || !is_even)
         return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
-    *is_even = sim->level.is_even_timestep;
+    if (level < 0 || level >= (int32_t)sim->levels.size())
+        return fail(VFB_ERR_INVALID_ARGUMENT, "no such level");
+    *is_even = sim->levels[(size_t)level].level.is_even_timestep;
     return VFB_OK;
 }
 

@@ -234,3 +234,113 @@ class ListGrid:
                               else np.tile(np.array(b.velocity, dtype=np.float64)[:, None], (1, b.k.size))
                               for b in parts], axis=1)
         return k, q, vel
+
+
+# -- refinement (GridGenerator/grid/GridInterface.cpp) ------------------------------------------
+@dataclass
+class Interface:
+    """The interpolation cells between a coarse level and the fine level nested in it, as the
+    reference's GridInterface finds them and LevelGridBuilder hands them to the coarse level's
+    fineToCoarse / coarseToFine (ICells) and neighborFineToCoarse / neighborCoarseToFine (ICellNeigh).
+
+    coarse to fine: coarse_cf is the MMM corner of each coarse cell, fine_cf the MMM one of the
+    eight fine nodes inside it; fine to coarse: coarse_fc is the coarse node at the centre of each
+    fine cell, fine_fc that cell's MMM fine node. Offsets are (3, n), zero for cells whose corners
+    are all fluid (findOffsetCF / findOffsetFC give direction 000 there)."""
+    coarse_cf: np.ndarray
+    fine_cf: np.ndarray
+    coarse_fc: np.ndarray
+    fine_fc: np.ndarray
+    offsets_cf: np.ndarray
+    offsets_fc: np.ndarray
+
+
+@dataclass
+class MultiLevelGrid:
+    """Nested levels: levels[0] is the coarsest; levels[l + 1] covers a box of levels[l] at half
+    the spacing; interfaces[l] couples levels l and l + 1. origin[l] and spacing[l] place fluid node
+    (0, 0, 0) of level l and its node distance in units of the coarsest spacing."""
+    levels: list
+    interfaces: list
+    origin: list
+    spacing: list
+
+    @classmethod
+    def uniform(cls, grid: ListGrid):
+        return cls([grid], [], [np.zeros(3)], [1.0])
+
+    def refine(self, lo, hi):
+        """Add a finer level over the cells [lo, hi) (per axis, fluid-box coordinates of the
+        currently finest level) and return it."""
+        fine, iface = refine_box(self.levels[-1], lo, hi)
+        h = self.spacing[-1]
+        self.origin.append(self.origin[-1] + (np.asarray(lo, dtype=np.float64) + 0.25) * h)
+        self.spacing.append(h / 2.0)
+        self.levels.append(fine)
+        self.interfaces.append(iface)
+        return fine
+
+    def positions(self, level):
+        """(3, number_of_nodes) node positions of a level in units of the coarsest spacing."""
+        g = self.levels[level]
+        return self.origin[level][:, None] + g.coords.astype(np.float64) * self.spacing[level]
+
+
+def refine_box(coarse: ListGrid, lo, hi):
+    """A fine level over the coarse cells [lo, hi) of `coarse` and the interpolation cells between
+    them, by the rules of GridInterface (GridInterface.cpp:59-205) for a refined box whose
+    interface lies in the fluid:
+
+    * fine nodes sit at coarse positions + 1/4 + i/2 (getCoarseToFineIndexOnFineGrid,
+      getFineToCoarseIndexOnFineGrid :237-257), a 2(hi - lo) cube per axis with a stopper shell;
+    * coarse-to-fine cells (findInterfaceCF :59-90) are the coarse cells of the box whose
+      27-neighbourhood leaves it: its outer cell layer. Their corners are the CFC nodes
+      [lo, hi]^3 minus [lo + 2, hi - 2]^3, and their fine nodes the fine level's two outer layers;
+    * fine-to-coarse cells (findInterfaceFC :125-157) are centred on the coarse nodes next to a
+      CFC node that are not CFC themselves: the shell of [lo + 2, hi - 2]^3;
+    * coarse nodes under the fine level that are neither (findOverlapStopper :159-205: the
+      stopper shell and the nodes removed below it) leave the coarse level's fluid-node list.
+
+    lo and hi must keep the interface two nodes away from the coarse level's edges and leave at
+    least four cells: 2 <= lo, lo + 4 <= hi <= n - 3 on every axis."""
+    lo = np.asarray(lo, dtype=np.int64)
+    hi = np.asarray(hi, dtype=np.int64)
+    ext = np.array([coarse.nx, coarse.ny, coarse.nz])
+    if lo.shape != (3,) or hi.shape != (3,):
+        raise ValueError("lo and hi are three cell coordinates")
+    if (lo < 2).any() or (hi > ext - 3).any() or (hi - lo < 4).any():
+        raise ValueError("the refined box needs 2 <= lo, lo + 4 <= hi <= n - 3 on every axis")
+    c = coarse.coords
+    fluid = coarse.geo == N.GEO_FLUID
+    box = [(c[a] >= lo[a]) & (c[a] <= hi[a]) for a in range(3)]
+    inner2 = [(c[a] >= lo[a] + 2) & (c[a] <= hi[a] - 2) for a in range(3)]
+    inner3 = [(c[a] >= lo[a] + 3) & (c[a] <= hi[a] - 3) for a in range(3)]
+    in_box = box[0] & box[1] & box[2]
+    in2 = inner2[0] & inner2[1] & inner2[2]
+    in3 = inner3[0] & inner3[1] & inner3[2]
+    if not fluid[in_box].all():
+        raise ValueError("the refined box must lie in the fluid")
+    fine = ListGrid(int(2 * (hi[0] - lo[0])), int(2 * (hi[1] - lo[1])), int(2 * (hi[2] - lo[2])),
+                    periodic=(False, False, False))
+    # coarse-to-fine: cells (MMM corner c) in [lo, hi - 1]^3 on the outer layer
+    cells = [(c[a] >= lo[a]) & (c[a] <= hi[a] - 1) for a in range(3)]
+    cell_in = cells[0] & cells[1] & cells[2]
+    shell = np.zeros_like(cell_in)
+    for a in range(3):
+        shell |= (c[a] == lo[a]) | (c[a] == hi[a] - 1)
+    cf_coarse = np.nonzero(cell_in & shell)[0]
+    cf_fine = fine.node_index(*(2 * (c[a, cf_coarse] - lo[a]) for a in range(3)))
+    # fine-to-coarse: the shell of [lo + 2, hi - 2]^3
+    shell2 = np.zeros_like(in2)
+    for a in range(3):
+        shell2 |= (c[a] == lo[a] + 2) | (c[a] == hi[a] - 2)
+    fc_coarse = np.nonzero(in2 & shell2)[0]
+    fc_fine = fine.node_index(*(2 * (c[a, fc_coarse] - lo[a]) - 1 for a in range(3)))
+    # the coarse nodes below the fine-to-coarse shell are not collided any more
+    keep = np.ones(coarse.number_of_nodes, dtype=bool)
+    keep[in3] = False
+    coarse.fluid = coarse.fluid[keep[coarse.fluid]]
+    iface = Interface(coarse_cf=cf_coarse.astype(np.uint32), fine_cf=cf_fine.astype(np.uint32),
+                      coarse_fc=fc_coarse.astype(np.uint32), fine_fc=fc_fine.astype(np.uint32),
+                      offsets_cf=np.zeros((3, cf_coarse.size)), offsets_fc=np.zeros((3, fc_coarse.size)))
+    return fine, iface

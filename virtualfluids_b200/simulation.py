@@ -8,7 +8,8 @@ Names and meanings follow the reference so that a set-up reads like one of its a
 * :class:`BoundaryConditionFactory` — the enums and setters of
   src/gpu/core/BoundaryConditions/BoundaryConditionFactory.h:50-178;
 * :class:`Simulation` — allocation, initialisation (PreProcessorImp::init) and the time loop
-  (UpdateGrid27::updateGrid) of one level, driving ``vfb_simulation_*`` of the native library.
+  (UpdateGrid27::updateGrid) of one level or of nested refinement levels, driving
+  ``vfb_simulation_*`` of the native library.
 
 Device memory is held in torch tensors (plumbing only); every kernel runs in ``libvfb.so``.
 """
@@ -20,7 +21,7 @@ import enum
 import numpy as np
 
 from . import _native as N
-from .grid import ListGrid
+from .grid import ListGrid, MultiLevelGrid
 
 STORAGE = {"f64": N.STORAGE_F64, "f32": N.STORAGE_F32, "f16": N.STORAGE_F16, "bf16": N.STORAGE_BF16}
 
@@ -79,6 +80,10 @@ class Parameter:
     def omega(self) -> float:
         """omega = 1 / (3 nu + 1/2) (Parameter.cpp:406)."""
         return 1.0 / (3.0 * self.viscosity_lb + 0.5)
+
+    def omega_of_level(self, level: int) -> float:
+        """omega of a refinement level: nu 2^level in that level's units (Parameter.cpp:404-406)."""
+        return 1.0 / (3.0 * (self.viscosity_lb * 2.0 ** level) + 0.5)
 
 
 class BoundaryConditionFactory:
@@ -213,15 +218,12 @@ def _ptr(t):
     return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
 
 
-class Simulation:
-    """One level of a uniform grid advanced by the native step driver."""
+class _LevelState:
+    """Device arrays of one level (LBMSimulationParameter of that level) and its BC lists."""
 
-    def __init__(self, para: Parameter, grid: ListGrid, bc_factory: BoundaryConditionFactory, device="cuda"):
-        if para.main_kernel is None:
-            raise N.VfbError(N.VFB_ERR_UNKNOWN_KERNEL, "no main kernel configured")
+    def __init__(self, para: Parameter, grid: ListGrid, level: int, device):
         t = _torch()
-        self.para, self.grid, self.bcf = para, grid, bc_factory
-        self.device = device
+        self.grid = grid
         sd, rd = storage_dtype(para.storage), real_dtype(para.storage)
         n = grid.number_of_nodes
         self.dist = t.zeros(27 * n, dtype=sd, device=device)
@@ -237,12 +239,12 @@ class Simulation:
         L.storage = para.storage
         L.arith = para.arith
         L.is_even_timestep = 1
-        L.level = 0
+        L.level = level
         L.number_of_nodes = n
         L.distributions = self.dist.data_ptr()
         L.neighbor_x, L.neighbor_y, L.neighbor_z = (x.data_ptr() for x in self.nb)
         L.type_of_grid_node = self.geo.data_ptr()
-        L.omega = para.omega
+        L.omega = para.omega_of_level(level)
         for i in range(3):
             L.forces[i] = para.forcing[i]
             L.quadric_limiters[i] = para.quadric_limiters[i]
@@ -250,8 +252,8 @@ class Simulation:
         L.pressure = self.press.data_ptr()
         L.outflow_pressure_correction_factor = para.outflow_pressure_correction_factor
         self.level = L
-        self._keep = []
-        self._bcs = {}
+        self.keep = []
+        self.bcs = {}
         for kind in ("velocity", "noslip", "geometry"):
             m = grid.merged(kind)
             if m is None:
@@ -261,31 +263,68 @@ class Simulation:
             qt = t.from_numpy(q.reshape(-1)).to(device=device, dtype=rd)
             vt = [t.from_numpy(vel[a].copy()).to(device=device, dtype=rd) for a in range(3)]
             bc = N.BC(kt.data_ptr(), qt.data_ptr(), k.size, vt[0].data_ptr(), vt[1].data_ptr(), vt[2].data_ptr())
-            self._keep += [kt, qt] + vt
-            self._bcs[kind] = bc
-        self._pressure = []
+            self.keep += [kt, qt] + vt
+            self.bcs[kind] = bc
+        self.pressure = []
+        from .grid import SIDE_DIR
         for b in grid.bcs:
             if b.kind != "pressure":
                 continue
             kt = t.from_numpy(b.k.astype(np.int32)).to(device)
             knt = t.from_numpy(b.k_neighbor.astype(np.int32)).to(device)
             rt = t.full((b.k.size,), float(b.rho), dtype=rd, device=device)
-            from .grid import SIDE_DIR
-            self._keep += [kt, knt, rt]
-            self._pressure.append(N.DirectionalBC(kt.data_ptr(), knt.data_ptr(), rt.data_ptr(), b.k.size, SIDE_DIR[b.side]))
+            self.keep += [kt, knt, rt]
+            self.pressure.append(N.DirectionalBC(kt.data_ptr(), knt.data_ptr(), rt.data_ptr(), b.k.size, SIDE_DIR[b.side]))
+
+
+class Simulation:
+    """The time loop (UpdateGrid27::updateGrid) of a uniform grid or of nested refinement levels,
+    driven by ``vfb_simulation_*`` of the native library.
+
+    grid is a :class:`ListGrid` (one level) or a :class:`MultiLevelGrid`; with more than one level
+    the scaling factory (GridScalingFactory) chooses the interpolation between them, as the
+    reference's ``Simulation(para, gridBuilder, bcFactory, scalingFactory)``. The attributes
+    ``grid``, ``level``, ``dist``, ``rho`` ... are those of the coarsest level; ``levels`` holds all."""
+
+    def __init__(self, para: Parameter, grid, bc_factory: BoundaryConditionFactory,
+                 scaling_factory: GridScalingFactory | None = None, device="cuda"):
+        if para.main_kernel is None:
+            raise N.VfbError(N.VFB_ERR_UNKNOWN_KERNEL, "no main kernel configured")
+        t = _torch()
+        self.para, self.bcf, self.device = para, bc_factory, device
+        self.multilevel = grid if isinstance(grid, MultiLevelGrid) else MultiLevelGrid.uniform(grid)
+        self.levels = [_LevelState(para, g, i, device) for i, g in enumerate(self.multilevel.levels)]
+        base = self.levels[0]
+        self.grid, self.level, self.dist, self.fluid = base.grid, base.level, base.dist, base.fluid
+        self.nb, self.geo = base.nb, base.geo
+        self.rho, self.vx, self.vy, self.vz, self.press = base.rho, base.vx, base.vy, base.vz, base.press
+        self._bcs = base.bcs
         sim = C.c_void_p()
         N.check(N.lib().vfb_simulation_create(para.main_kernel.encode(), C.byref(sim)))
         self._sim = sim
-        N.check(N.lib().vfb_simulation_set_level(sim, C.byref(L), _ptr(self.fluid), int(grid.fluid.size)))
-        if "velocity" in self._bcs:
-            N.check(N.lib().vfb_simulation_set_velocity_bc(sim, C.byref(self._bcs["velocity"]), int(bc_factory.velocity)))
-        if "noslip" in self._bcs:
-            N.check(N.lib().vfb_simulation_set_noslip_bc(sim, C.byref(self._bcs["noslip"]), int(bc_factory.noslip)))
-        if "geometry" in self._bcs:
-            N.check(N.lib().vfb_simulation_set_geometry_bc(sim, C.byref(self._bcs["geometry"]), int(bc_factory.geometry)))
+        for i, S in enumerate(self.levels):
+            N.check(N.lib().vfb_simulation_use_level(sim, i))
+            N.check(N.lib().vfb_simulation_set_level(sim, C.byref(S.level), _ptr(S.fluid), int(S.grid.fluid.size)))
+            if "velocity" in S.bcs:
+                N.check(N.lib().vfb_simulation_set_velocity_bc(sim, C.byref(S.bcs["velocity"]), int(bc_factory.velocity)))
+            if "noslip" in S.bcs:
+                N.check(N.lib().vfb_simulation_set_noslip_bc(sim, C.byref(S.bcs["noslip"]), int(bc_factory.noslip)))
+            if "geometry" in S.bcs:
+                N.check(N.lib().vfb_simulation_set_geometry_bc(sim, C.byref(S.bcs["geometry"]),
+                                                               int(bc_factory.geometry)))
+            for p in S.pressure:
+                N.check(N.lib().vfb_simulation_add_pressure_bc(sim, C.byref(p), int(bc_factory.pressure)))
+        self._cells = []
+        if scaling_factory is not None:
+            N.check(N.lib().vfb_simulation_set_scaling_factory(sim, int(scaling_factory.grid_scaling_type), 0))
+        for i, iface in enumerate(self.multilevel.interfaces):
+            fc = InterpolationCells(iface.fine_fc, iface.coarse_fc, iface.offsets_fc, storage=para.storage, device=device)
+            cf = InterpolationCells(iface.fine_cf, iface.coarse_cf, iface.offsets_cf, storage=para.storage, device=device)
+            self._cells.append((fc, cf))
+            N.check(N.lib().vfb_simulation_set_interpolation_cells(sim, i, C.byref(fc.cells), C.byref(fc.neighbor),
+                                                                   C.byref(cf.cells), C.byref(cf.neighbor)))
+        N.check(N.lib().vfb_simulation_use_level(sim, 0))
         self._drag = None
-        for p in self._pressure:
-            N.check(N.lib().vfb_simulation_add_pressure_bc(sim, C.byref(p), int(bc_factory.pressure)))
         N.check(N.lib().vfb_simulation_check(sim))
 
     def close(self):
@@ -299,43 +338,51 @@ class Simulation:
         except Exception:
             pass
 
-    def init(self, rho=None, vx=None, vy=None, vz=None):
-        """PreProcessorImp::init: equilibrium for the odd, then the even parity; starts even."""
+    def init(self, rho=None, vx=None, vy=None, vz=None, level=0):
+        """PreProcessorImp::init of one level: equilibrium for the odd, then the even parity; starts even."""
         t = _torch()
+        S = self.levels[level]
         rd = real_dtype(self.para.storage)
-        for arr, dst in ((rho, self.rho), (vx, self.vx), (vy, self.vy), (vz, self.vz)):
+        for arr, dst in ((rho, S.rho), (vx, S.vx), (vy, S.vy), (vz, S.vz)):
             if arr is None:
                 dst.zero_()
             else:
                 dst.copy_(t.as_tensor(np.asarray(arr), dtype=rd))
-        L = self.level
+        L = S.level
         L.is_even_timestep = 0
         N.check(N.lib().vfb_init_navier_stokes_compressible(C.byref(L), None))
         L.is_even_timestep = 1
         N.check(N.lib().vfb_init_navier_stokes_compressible(C.byref(L), None))
-        N.check(N.lib().vfb_simulation_set_level(self._sim, C.byref(L), _ptr(self.fluid), int(self.grid.fluid.size)))
+        N.check(N.lib().vfb_simulation_use_level(self._sim, level))
+        N.check(N.lib().vfb_simulation_set_level(self._sim, C.byref(L), _ptr(S.fluid), int(S.grid.fluid.size)))
+        N.check(N.lib().vfb_simulation_use_level(self._sim, 0))
 
     def run(self, steps: int):
+        """steps time steps of the coarsest level (each finer level takes twice its coarser one's)."""
         N.check(N.lib().vfb_simulation_run(self._sim, int(steps), None))
         self._drag_steps = getattr(self, "_drag_steps", 0) + int(steps) if self._drag is not None else 0
-        ev = C.c_int32()
-        N.check(N.lib().vfb_simulation_is_even_timestep(self._sim, C.byref(ev)))
-        self.level.is_even_timestep = ev.value
+        for i, S in enumerate(self.levels):
+            ev = C.c_int32()
+            N.check(N.lib().vfb_simulation_level_is_even_timestep(self._sim, i, C.byref(ev)))
+            S.level.is_even_timestep = ev.value
 
-    def macroscopic(self):
-        """drho, vx, vy, vz, pressure of every node (zeros on non-fluid nodes), as numpy."""
-        N.check(N.lib().vfb_calc_macroscopic_compressible(C.byref(self.level), None))
+    def macroscopic(self, level=0):
+        """drho, vx, vy, vz, pressure of every node of a level (zeros on non-fluid nodes), as numpy."""
+        S = self.levels[level]
+        N.check(N.lib().vfb_calc_macroscopic_compressible(C.byref(S.level), None))
         N.check(N.lib().vfb_synchronize(None))
         return {k: v.double().cpu().numpy() for k, v in
-                (("rho", self.rho), ("vx", self.vx), ("vy", self.vy), ("vz", self.vz), ("pressure", self.press))}
+                (("rho", S.rho), ("vx", S.vx), ("vy", S.vy), ("vz", S.vz), ("pressure", S.press))}
 
-    def mass_energy(self):
+    def mass_energy(self, level=0):
         t = _torch()
-        nbytes = N.lib().vfb_mass_energy_workspace_bytes(int(self.grid.fluid.size))
+        S = self.levels[level]
+        nf = int(S.grid.fluid.size)
+        nbytes = N.lib().vfb_mass_energy_workspace_bytes(nf)
         ws = t.empty((nbytes + 7) // 8, dtype=t.float64, device=self.device)
         out = (C.c_double * 2)()
-        N.check(N.lib().vfb_mass_energy(C.byref(self.level), _ptr(self.fluid), int(self.grid.fluid.size),
-                                        C.c_void_p(ws.data_ptr()), nbytes, out, None))
+        N.check(N.lib().vfb_mass_energy(C.byref(S.level), _ptr(S.fluid), nf, C.c_void_p(ws.data_ptr()), nbytes, out,
+                                        None))
         return out[0], out[1]
 
     def enable_drag_lift(self, history_steps: int):
@@ -363,6 +410,6 @@ class Simulation:
         start = done % length
         return np.concatenate([h[start:], h[:start]])
 
-    def populations(self):
+    def populations(self, level=0):
         N.check(N.lib().vfb_synchronize(None))
-        return self.dist.double().cpu().numpy()
+        return self.levels[level].dist.double().cpu().numpy()
