@@ -281,6 +281,11 @@ int vfb_simulation_destroy(vfb_simulation *sim);
    (Parameter::getParD(level)) */
 int vfb_simulation_use_level(vfb_simulation *sim, int32_t level);
 int vfb_simulation_number_of_levels(const vfb_simulation *sim, int32_t *number_of_levels);
+/* Neighbour slot tables (default on): vfb_simulation_set_level builds, in library-owned device
+   memory (28 bytes per fluid node), the seven +1 neighbours of every fluid node, which the driver's
+   collision then reads with one coalesced load each instead of the neighborX/Y/Z chain; same
+   results. Set the level again after changing its neighbour arrays or fluid-node list. 0 frees them. */
+int vfb_simulation_set_neighbor_tables(vfb_simulation *sim, int32_t enable);
 /* the selected level's description, copied; device memory stays caller-owned; level->level must be
    the selected level (forces are scaled by 2^-level) */
 int vfb_simulation_set_level(vfb_simulation *sim, const vfb_level *level, const uint32_t *fluid_node_indices,

@@ -124,6 +124,7 @@ def test_simulation_manager_rules():
     assert lib.vfb_simulation_create(b"K15CompressibleNavierStokes", C.byref(sim)) == N.VFB_ERR_UNKNOWN_KERNEL
     N.check(lib.vfb_simulation_create(b"K17CompressibleNavierStokes", C.byref(sim)))
     try:
+        N.check(lib.vfb_simulation_set_neighbor_tables(sim, 0))   # host checks only: no device tables
         assert lib.vfb_simulation_check(sim) == N.VFB_ERR_INVALID_ARGUMENT  # no level yet
         L = _fake_level(N)
         N.check(lib.vfb_simulation_set_level(sim, C.byref(L), C.c_void_p(0x2000), 5))
@@ -155,6 +156,7 @@ def test_multilevel_driver_rules():
     sim = C.c_void_p()
     N.check(lib.vfb_simulation_create(b"K17CompressibleNavierStokes", C.byref(sim)))
     try:
+        N.check(lib.vfb_simulation_set_neighbor_tables(sim, 0))
         L0, L1 = _fake_level(N), _fake_level(N)
         N.check(lib.vfb_simulation_set_level(sim, C.byref(L0), C.c_void_p(0x2000), 5))
         assert lib.vfb_simulation_use_level(sim, 2) == N.VFB_ERR_INVALID_ARGUMENT     # skips level 1

@@ -276,3 +276,23 @@ def test_box_inlet_perturbation_is_seeded(cuda):
     assert np.array_equal(runs[0], runs[1])
     assert not np.array_equal(runs[0], runs[2])
     assert np.abs(runs[0] - runs[2]).max() < 1e-3
+
+
+@pytest.mark.parametrize("storage", [N.STORAGE_F64, N.STORAGE_F16], ids=["f64", "f16"])
+def test_neighbor_slot_tables_change_nothing(cuda, storage):
+    """The driver's neighbour slot tables give the same bits as the neighborX/Y/Z chain."""
+    g = ListGrid(12, 10, 9)
+    for side in ("MX", "PX", "MY", "PY", "MZ"):
+        g.add_side(side, "noslip")
+    g.add_side("PZ", "velocity", velocity=(0.05, 0.01, 0.0))
+    bcf = BCF()
+    bcf.set_velocity_boundary_condition(BCF.VelocityBC.VelocityInterpolatedCompressible)
+    bcf.set_no_slip_boundary_condition(BCF.NoSlipBC.NoSlipInterpolatedCompressible)
+    out = []
+    for tables in (False, True):
+        sim = Simulation(make_para(1.8, storage), g, bcf, neighbor_tables=tables)
+        sim.init(*smooth_fields(g, 5))
+        sim.run(7)
+        out.append(sim.populations())
+        sim.close()
+    assert np.array_equal(out[0], out[1])

@@ -282,7 +282,16 @@ const char *vfb_kernel_name(int index)
 // ---------------------------------------------------------------------------------------------
 // (1) reference-layout entry points
 // ---------------------------------------------------------------------------------------------
+static int run_k17(const vfb_level *level, const uint32_t *idx, uint32_t size, int32_t tmpl, const uint32_t *slots,
+                   void *stream);
+
 int vfb_k17_run_on_indices(const vfb_level *level, const uint32_t *idx, uint32_t size, int32_t tmpl, void *stream)
+{
+    return run_k17(level, idx, size, tmpl, nullptr, stream);
+}
+
+static int run_k17(const vfb_level *level, const uint32_t *idx, uint32_t size, int32_t tmpl, const uint32_t *slots,
+                   void *stream)
 {
     int st = check_level(level);
     if (st)
@@ -297,7 +306,8 @@ int vfb_k17_run_on_indices(const vfb_level *level, const uint32_t *idx, uint32_t
         return fail(VFB_ERR_INVALID_ARGUMENT, "macroscopic output arrays are NULL");
     if (bf && (!level->body_force_x || !level->body_force_y || !level->body_force_z))
         return fail(VFB_ERR_INVALID_ARGUMENT, "body force arrays are NULL");
-    const cudaError_t e = VFB_DISPATCH(level->storage, level->arith, LA::k17_list(level, idx, size, tmpl, as_stream(stream)));
+    const cudaError_t e = VFB_DISPATCH(level->storage, level->arith,
+                                       LA::k17_list(level, idx, size, tmpl, as_stream(stream), slots));
     return cuda_status(e, "K17CompressibleNavierStokes launch");
 }
 
@@ -644,6 +654,44 @@ struct SimLevel {
     // neighborFineToCoarse, coarseToFine, neighborCoarseToFine of the coarse level)
     vfb_interpolation_cells fc{}, cf{};
     vfb_interpolation_cell_neighbor fc_offsets{}, cf_offsets{};
+    // neighbour slot table of the fluid-node list (library-owned, built by set_level)
+    uint32_t *slots = nullptr;
+    size_t slots_nodes = 0;
+    const void *slots_key[4] = { nullptr, nullptr, nullptr, nullptr };
+
+    void free_slots()
+    {
+        if (slots)
+            cudaFree(slots);
+        slots = nullptr;
+        slots_nodes = 0;
+        for (auto &p : slots_key)
+            p = nullptr;
+    }
+    ~SimLevel() { free_slots(); }
+    SimLevel() = default;
+    SimLevel(const SimLevel &) = delete;
+    SimLevel &operator=(const SimLevel &) = delete;
+    SimLevel(SimLevel &&o) noexcept { *this = std::move(o); }
+    SimLevel &operator=(SimLevel &&o) noexcept
+    {
+        if (this != &o) {
+            free_slots();
+            has_level = o.has_level; level = o.level; fluid = o.fluid; n_fluid = o.n_fluid;
+            velocity = o.velocity; velocity_fn = o.velocity_fn; velocity_set = o.velocity_set;
+            noslip = o.noslip; noslip_fn = o.noslip_fn; noslip_set = o.noslip_set;
+            pressure = std::move(o.pressure); pressure_fn = std::move(o.pressure_fn);
+            geometry = o.geometry; geometry_fn = o.geometry_fn; geometry_set = o.geometry_set;
+            drag_work = o.drag_work; drag_history = o.drag_history; drag_history_len = o.drag_history_len;
+            drag_steps = o.drag_steps; fc = o.fc; cf = o.cf; fc_offsets = o.fc_offsets; cf_offsets = o.cf_offsets;
+            slots = o.slots; slots_nodes = o.slots_nodes;
+            for (int i = 0; i < 4; ++i)
+                slots_key[i] = o.slots_key[i];
+            o.slots = nullptr;
+            o.slots_nodes = 0;
+        }
+        return *this;
+    }
 };
 } // namespace
 
@@ -651,12 +699,65 @@ struct vfb_simulation {
     int kernel_id = 0;
     std::vector<SimLevel> levels = std::vector<SimLevel>(1);
     int32_t cursor = 0;               // the level the setters configure
+    bool neighbor_tables = true;      // build slot tables for the collision
     bool scaling_set = false;         // GridScalingFactory given
     vfb_scaling_fn scale_fc = nullptr;
     vfb_scaling_fn scale_cf = nullptr;
 };
 
 static SimLevel &current(vfb_simulation *sim) { return sim->levels[(size_t)sim->cursor]; }
+
+// the seven +1 neighbour nodes (x, y, xy, z, xz, yz, xyz) of every listed node, stored per slot so
+// that the collision reads them with one coalesced load each instead of the neighborX/Y/Z chain
+// (the order of the kernels' ListIndices: slot bit 0 = +x, bit 1 = +y, bit 2 = +z)
+__global__ void list_slots_kernel(const uint32_t *__restrict__ idx, uint32_t n_idx, const uint32_t *__restrict__ nbx,
+                                  const uint32_t *__restrict__ nby, const uint32_t *__restrict__ nbz,
+                                  uint32_t *__restrict__ slots)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_idx)
+        return;
+    const uint32_t k = __ldg(idx + i);
+    const uint32_t kx = __ldg(nbx + k), ky = __ldg(nby + k), kz = __ldg(nbz + k);
+    const uint32_t kxy = __ldg(nby + kx);
+    const uint32_t out[7] = { kx, ky, kxy, kz, __ldg(nbz + kx), __ldg(nbz + ky), __ldg(nbz + kxy) };
+#pragma unroll
+    for (int j = 0; j < 7; ++j)
+        slots[(size_t)j * n_idx + i] = out[j];
+}
+
+// The slot table of a level (the seven +1 neighbours of each fluid node, one array per slot),
+// rebuilt when the fluid list or the neighbour arrays change. It costs 28 bytes per fluid node and
+// replaces the four-deep chain of dependent neighborX/Y/Z loads in every collision.
+static int build_slots(vfb_simulation *sim, SimLevel &S)
+{
+    const void *key[4] = { S.fluid, S.level.neighbor_x, S.level.neighbor_y, S.level.neighbor_z };
+    if (!sim->neighbor_tables || S.n_fluid == 0) {
+        S.free_slots();
+        return VFB_OK;
+    }
+    if (S.slots && S.slots_nodes == S.n_fluid && std::equal(key, key + 4, S.slots_key))
+        return VFB_OK;
+    S.free_slots();
+    if (cudaMalloc(&S.slots, (size_t)7 * S.n_fluid * sizeof(uint32_t)) != cudaSuccess) {
+        cudaGetLastError();
+        S.slots = nullptr;
+        return fail(VFB_ERR_OUT_OF_MEMORY, "no device memory for the neighbour slot table");
+    }
+    const unsigned B = 256, G = (unsigned)((S.n_fluid + B - 1) / B);
+    list_slots_kernel<<<G, B>>>(S.fluid, S.n_fluid, S.level.neighbor_x, S.level.neighbor_y, S.level.neighbor_z,
+                                S.slots);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaDeviceSynchronize();   // visible to every stream the level is later run on
+    if (e != cudaSuccess) {
+        S.free_slots();
+        return cuda_status(e, "neighbour slot table");
+    }
+    S.slots_nodes = S.n_fluid;
+    std::copy(key, key + 4, S.slots_key);
+    return VFB_OK;
+}
 
 extern "C" {
 
@@ -693,6 +794,21 @@ int vfb_simulation_use_level(vfb_simulation *sim, int32_t level)
     return VFB_OK;
 }
 
+int vfb_simulation_set_neighbor_tables(vfb_simulation *sim, int32_t enable)
+{
+    if (!sim)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL simulation");
+    sim->neighbor_tables = enable != 0;
+    for (SimLevel &S : sim->levels) {
+        if (!S.has_level)
+            continue;
+        int st = build_slots(sim, S);
+        if (st)
+            return st;
+    }
+    return VFB_OK;
+}
+
 int vfb_simulation_number_of_levels(const vfb_simulation *sim, int32_t *n)
 {
     if (!sim || !n)
@@ -717,7 +833,7 @@ int vfb_simulation_set_level(vfb_simulation *sim, const vfb_level *level, const 
     S.fluid = fluid;
     S.n_fluid = n;
     S.has_level = true;
-    return VFB_OK;
+    return build_slots(sim, S);
 }
 
 int vfb_simulation_set_velocity_bc(vfb_simulation *sim, const vfb_bc *bc, int32_t variant)
@@ -923,7 +1039,7 @@ static int run_geometry_pre(SimLevel &S, void *stream)
 static int step_level(SimLevel &S, void *stream)
 {
     vfb_level &L = S.level;
-    int st = vfb_k17_run_on_indices(&L, S.fluid, S.n_fluid, VFB_COLLISION_DEFAULT, stream);
+    int st = run_k17(&L, S.fluid, S.n_fluid, VFB_COLLISION_DEFAULT, S.slots, stream);
     if (st)
         return st;
     if (S.velocity_fn && S.velocity.number_of_bc_nodes) {

@@ -32,6 +32,7 @@ struct ListCollideArgs {
     const uint32_t *nbx, *nby, *nbz;
     const uint32_t *idx;        // fluid node indices
     uint32_t n_idx;
+    const uint32_t *slots;      // optional: the seven +1 neighbour nodes of idx[i] at [(j - 1) n_idx + i]
     K17Rates<C> rates;
     C fx, fy, fz;               // forces * 1/2 * 2^-level (RunCollision.cuh:112-114)
     C force0, force1, force2;   // forces, for the body-force variant
@@ -188,7 +189,15 @@ __global__ void __launch_bounds__(128) k17_list_kernel(ListCollideArgs<typename 
         a.bfz[k] = C(0);
     }
     uint32_t nodes[8];
-    list_nodes(k, a.nbx, a.nby, a.nbz, nodes);
+    if (a.slots) {
+        // neighbour table built once per level: one coalesced load per slot, no dependent chain
+        nodes[0] = k;
+#pragma unroll
+        for (int j = 1; j < 8; ++j)
+            nodes[j] = __ldg(a.slots + (size_t)(j - 1) * a.n_idx + i);
+    } else {
+        list_nodes(k, a.nbx, a.nby, a.nbz, nodes);
+    }
     S *base = static_cast<S *>(a.dist);
     C f[27];
     gather_pre<S, EVEN>(base, a.n, nodes, f);

@@ -48,7 +48,8 @@ inline uint64_t box_blocks(const BoxState &b)
 #define VFB_DECLARE_LAUNCHERS                                                                                        \
     template <class S>                                                                                               \
     struct Launchers {                                                                                               \
-        static cudaError_t k17_list(const vfb_level *L, const uint32_t *idx, uint32_t n, int tmpl, cudaStream_t s); \
+        static cudaError_t k17_list(const vfb_level *L, const uint32_t *idx, uint32_t n, int tmpl, cudaStream_t s,   \
+                                    const uint32_t *slots = nullptr);                                        \
         static cudaError_t bc(const vfb_level *L, const vfb_bc *bc, int kind, cudaStream_t s,                        \
                               const NodeAddr *box = nullptr);                                                        \
         static cudaError_t pressure(const vfb_level *L, const vfb_directional_bc *bc, cudaStream_t s,                \

@@ -35,7 +35,8 @@ C force_factor(int level)
 } // namespace
 
 template <class S>
-cudaError_t Launchers<S>::k17_list(const vfb_level *L, const uint32_t *idx, uint32_t n, int tmpl, cudaStream_t s)
+cudaError_t Launchers<S>::k17_list(const vfb_level *L, const uint32_t *idx, uint32_t n, int tmpl, cudaStream_t s,
+                                   const uint32_t *slots)
 {
     using C = typename Codec<S>::compute;
     if (n == 0)
@@ -48,6 +49,7 @@ cudaError_t Launchers<S>::k17_list(const vfb_level *L, const uint32_t *idx, uint
     a.nbz = L->neighbor_z;
     a.idx = idx;
     a.n_idx = n;
+    a.slots = slots;
     a.rates = rates_of<C>(L->omega, L->quadric_limiters);
     const C ff = force_factor<C>(L->level);
     a.fx = (C)L->forces[0] * C(0.5) * ff;
