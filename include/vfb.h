@@ -398,7 +398,7 @@ int vfb_box_populations(const vfb_box *box, void **dist, uint64_t *pitch, int32_
 typedef struct vfb_pool_desc {
     int32_t storage;                  /* vfb_storage */
     int32_t arith;                    /* vfb_arith */
-    uint64_t arena_bytes;             /* device bytes for populations and masks */
+    uint64_t arena_bytes;             /* device bytes for populations, masks and BC lists */
     uint32_t max_domains;
 } vfb_pool_desc;
 typedef struct vfb_domain_desc {
@@ -418,6 +418,29 @@ int vfb_pool_domain_bytes(const vfb_pool *pool, const vfb_domain_desc *desc, int
    nodes inside. VFB_ERR_OUT_OF_MEMORY when the arena has no room: nothing is changed then. The
    domain takes part in steps once it is initialised. */
 int vfb_pool_add_domain(vfb_pool *pool, const vfb_domain_desc *desc, const uint8_t *mask, uint32_t *id);
+/* Boundary-condition lists of a pool domain, host arrays copied into the arena with the domain (they
+   count against the budget and stay resident). Node indices are box indices k = x + nx (y + ny z) of
+   fluid nodes. Every step runs them for all domains at once: the no-slip list after the collision
+   (NoSlipInterpolatedCompressible, NoSlipInterpolatedCompressible.cu:44-381), the pressure list after
+   the parity swap (PressureNonEquilibriumCompressible, PressureNonEquilibriumCompressible.cu:45-314,
+   one outward normal per node, so inlet and outlet share a list). Other variants give
+   VFB_ERR_UNSUPPORTED. A domain computes what a vfb_box with the same lists computes. */
+typedef struct vfb_domain_bcs {
+    int32_t noslip_variant;           /* VFB_NOSLIP_INTERPOLATED_COMPRESSIBLE */
+    const int32_t *noslip_k;
+    const double *noslip_q27;         /* q of direction d of node i at [d * n + i]; q in [0, 1] = cut link */
+    uint32_t number_of_noslip_nodes;
+    int32_t pressure_variant;         /* VFB_PRESSURE_NON_EQUILIBRIUM_COMPRESSIBLE */
+    const int32_t *pressure_k;
+    const int32_t *pressure_k_neighbor; /* the node one step inwards */
+    const double *pressure_rho;       /* prescribed drho */
+    const int32_t *pressure_direction;  /* VFB_DIR_*: outward normal */
+    uint32_t number_of_pressure_nodes;
+} vfb_domain_bcs;
+int vfb_pool_add_domain_with_bcs(vfb_pool *pool, const vfb_domain_desc *desc, const uint8_t *mask,
+                                 const vfb_domain_bcs *bcs, uint32_t *id);
+int vfb_pool_domain_bytes_with_bcs(const vfb_pool *pool, const vfb_domain_desc *desc, int32_t has_mask,
+                                   uint32_t number_of_noslip_nodes, uint32_t number_of_pressure_nodes, uint64_t *bytes);
 /* the domain stops taking part in steps; its arena range and id become reusable once the pool's
    stream has drained (the next vfb_pool_step that changes the work list, or vfb_pool_synchronize).
    All calls on one pool must use one stream. */

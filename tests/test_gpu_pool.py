@@ -169,3 +169,64 @@ def test_duct_poiseuille_domains_reach_the_analytic_profile(cuda):
         ref = _duct_series(ny, nz, g, nu)[1:-1, 1:-1]
         err = np.sqrt(((u - ref) ** 2).sum() / (ref ** 2).sum())
         assert err < 0.02, (ny, nz, nu, err)
+
+
+def _porous_alone(g, omega, storage, arith, steps, seed):
+    b = Box(*g["shape"], omega, periodic=(False, True, True), storage=storage, arith=arith, mask=g["mask"])
+    k, q = g["bcs"]["noslip"]
+    b.set_bc("noslip", k, q, N.NOSLIP_INTERPOLATED_COMPRESSIBLE)
+    pk, pkn, prho, pdir = g["bcs"]["pressure"]
+    for d in (N.DIR_M00, N.DIR_P00):
+        sel = pdir == d
+        b.add_pressure_bc(pk[sel], pkn[sel], prho[sel], d)
+    b.init(*_fields(g["shape"], seed, amp_u=0.005))
+    b.step(steps)
+    f = b.fields()
+    nx, ny, nz = g["shape"]
+    return [f[key].reshape(nz, ny, nx) for key in ("rho", "vx", "vy", "vz")]
+
+
+@pytest.mark.parametrize("storage,arith", [("f64", "exact"), ("f32", "fast"), ("f16", "fast")])
+def test_pool_boundary_condition_lists_match_boxes_alone_bitwise(cuda, storage, arith):
+    """Porous blocks between pressure planes with exact sphere q: the pool's per-domain no-slip and
+    pressure lists (one launch each for all domains) compute what a box with the same lists does."""
+    from virtualfluids_b200.workloads import porous_block_bcs
+    geos = [porous_block_bcs(side, seed, porosity=0.75) for side, seed in ((20, 1), (28, 2), (24, 3))]
+    steps, omegas = 41, (1.8, 1.7, 1.9)
+    s = _stream()
+    pool = Pool(1 << 28, storage=storage, arith=arith, max_domains=8)
+    plain = pool.add((12, 10, 8), 1.8)           # a domain without lists shares the steps
+    pool.init(plain, *_fields((12, 10, 8), 9), stream=s)
+    ids = []
+    for i, g in enumerate(geos):
+        assert g["bcs"]["noslip"][0].size > 0
+        d = pool.add(g["shape"], omegas[i], periodic=(False, True, True), mask=g["mask"], bcs=g["bcs"])
+        pool.init(d, *_fields(g["shape"], 20 + i, amp_u=0.005), stream=s)
+        ids.append(d)
+    pool.step(steps, stream=s)
+    s.synchronize()
+    assert pool.kernel_launches() >= 3 * steps
+    for i, g in enumerate(geos):
+        got = pool.fields(ids[i], stream=s)
+        want = _porous_alone(g, omegas[i], storage, arith, steps, 20 + i)
+        nx, ny, nz = g["shape"]
+        fl = g["mask"].reshape(nz, ny, nx) != 0
+        for a, b in zip(got, want):
+            assert np.array_equal(a[fl], b[fl]), (i, storage)
+        assert np.abs(got[1][fl]).max() > 0
+
+
+def test_pool_rejects_bad_boundary_condition_lists(cuda):
+    from virtualfluids_b200.workloads import porous_block_bcs
+    g = porous_block_bcs(20, 1, porosity=0.8)
+    pool = Pool(1 << 26, storage="f32", max_domains=4)
+    k, q = g["bcs"]["noslip"]
+    solid = int(np.nonzero(g["mask"] == 0)[0][0])
+    for bad in ({"noslip": (np.array([solid]), np.zeros((27, 1)))},
+                {"noslip": (np.array([10 ** 7]), np.zeros((27, 1)))},
+                {"pressure": (np.array([30]), np.array([10 ** 8]), 0.0, N.DIR_M00)},
+                {"pressure": (np.array([30]), np.array([31]), 0.0, 7)}):
+        with pytest.raises(N.VfbError) as e:
+            pool.add(g["shape"], 1.8, periodic=(False, True, True), mask=g["mask"], bcs=bad)
+        assert e.value.status == N.VFB_ERR_INVALID_ARGUMENT
+    assert pool.stats()["used_bytes"] == 0

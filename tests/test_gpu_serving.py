@@ -1,9 +1,10 @@
 """Serving on the GPU: continuous batching of porous-block solves in one domain pool.
 
 Requests of different sizes and step counts are admitted as memory frees up, advance together,
-and leave when done. Each result must be the same alone and in the mix (bit for bit: the pool's
-kernels treat every domain independently), and the FP16-storage permeability must stay close to
-the FP64 one.
+and leave when done; both drives are covered (pressure planes with exact sphere q, whose lists live
+in the pool's arena, and the periodic body force). Each result must be the same alone and in the
+mix (bit for bit: the pool's kernels treat every domain independently), and the FP16-storage
+permeability must stay close to the FP64 one.
 """
 import numpy as np
 import pytest
@@ -13,17 +14,18 @@ from virtualfluids_b200.serving import Request, Server, poisson_stream, solve_al
 pytestmark = pytest.mark.gpu
 
 
-def _small_stream(n=7, seed=5):
-    reqs = poisson_stream(n, rate=1000.0, seed=seed, sides=(20, 40), steps=(100, 600))
+def _small_stream(n=7, seed=5, drive="pressure"):
+    reqs = poisson_stream(n, rate=1000.0, seed=seed, sides=(20, 40), steps=(100, 600), drive=drive)
     for r in reqs:
         r.geometry()
     return reqs
 
 
-def test_each_result_is_the_same_alone_and_in_the_mix(cuda):
-    reqs = _small_stream()
+@pytest.mark.parametrize("drive", ["pressure", "force"])
+def test_each_result_is_the_same_alone_and_in_the_mix(cuda, drive):
+    reqs = _small_stream(drive=drive)
     # an arena that holds about three of these solves at a time, so later ones queue for memory
-    per = max(r.side for r in reqs) ** 3 * (27 * 4 + 1) + 4096
+    per = max(r.side + 2 for r in reqs) ** 3 * (27 * 4 + 1 + 40) + 4096
     srv = Server(3 * per, storage="f32", keep_fields=True)
     results, stats = srv.run(reqs, realtime=False)
     srv.close()
@@ -48,8 +50,9 @@ def test_requests_arriving_during_others_are_admitted_before_those_finish(cuda):
     assert stats["p99_s"] >= stats["p50_s"] > 0 and stats["mlups"] > 0
 
 
-def test_fp16_storage_permeability_close_to_fp64(cuda):
-    req = Request(rid=0, arrival=0.0, side=40, steps=3000, seed=3, porosity=0.8)
+@pytest.mark.parametrize("drive", ["pressure", "force"])
+def test_fp16_storage_permeability_close_to_fp64(cuda, drive):
+    req = Request(rid=0, arrival=0.0, side=40, steps=3000, seed=3, porosity=0.8, drive=drive)
     k64, _ = solve_alone(req, storage="f64")
     k16, _ = solve_alone(req, storage="f16")
     k32, _ = solve_alone(req, storage="f32")

@@ -109,6 +109,13 @@ class DomainDesc(C.Structure):
                 ("omega", C.c_double), ("forces", C.c_double * 3), ("quadric_limiters", C.c_double * 3)]
 
 
+class DomainBCs(C.Structure):
+    _fields_ = [("noslip_variant", C.c_int32), ("noslip_k", C.c_void_p), ("noslip_q27", C.c_void_p),
+                ("number_of_noslip_nodes", C.c_uint32), ("pressure_variant", C.c_int32), ("pressure_k", C.c_void_p),
+                ("pressure_k_neighbor", C.c_void_p), ("pressure_rho", C.c_void_p), ("pressure_direction", C.c_void_p),
+                ("number_of_pressure_nodes", C.c_uint32)]
+
+
 BC_FN = C.CFUNCTYPE(C.c_int, C.POINTER(Level), C.POINTER(BC), C.c_void_p)
 DBC_FN = C.CFUNCTYPE(C.c_int, C.POINTER(Level), C.POINTER(DirectionalBC), C.c_void_p)
 
@@ -203,6 +210,10 @@ SIGNATURES = {
     "vfb_pool_destroy": (C.c_int, [C.c_void_p]),
     "vfb_pool_domain_bytes": (C.c_int, [C.c_void_p, C.POINTER(DomainDesc), C.c_int32, C.POINTER(C.c_uint64)]),
     "vfb_pool_add_domain": (C.c_int, [C.c_void_p, C.POINTER(DomainDesc), C.c_void_p, C.POINTER(C.c_uint32)]),
+    "vfb_pool_add_domain_with_bcs": (C.c_int, [C.c_void_p, C.POINTER(DomainDesc), C.c_void_p, C.POINTER(DomainBCs),
+                                               C.POINTER(C.c_uint32)]),
+    "vfb_pool_domain_bytes_with_bcs": (C.c_int, [C.c_void_p, C.POINTER(DomainDesc), C.c_int32, C.c_uint32, C.c_uint32,
+                                                 C.POINTER(C.c_uint64)]),
     "vfb_pool_remove_domain": (C.c_int, [C.c_void_p, C.c_uint32]),
     "vfb_pool_synchronize": (C.c_int, [C.c_void_p, C.c_void_p]),
     "vfb_pool_init_domain": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

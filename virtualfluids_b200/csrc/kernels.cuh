@@ -666,19 +666,16 @@ __device__ __forceinline__ C cdot_rt(int d, C ux, C uy, C uz)
 //                       form minus w drho (getInterpolatedDistributionForVeloWithPressureBC).
 enum : int { kBCCompressible = 0, kBCIncompressible = 1, kBCWithPressure = 2 };
 
-template <class S, bool EVEN, bool VELOCITY, int FORM = kBCCompressible>
-__global__ void __launch_bounds__(128) bc_interpolated_kernel(BCArgs a)
+// one BC node: its slot nodes, its q of every direction at q27[d * q_stride], the wall velocity
+template <class S, bool EVEN, bool VELOCITY, int FORM>
+__device__ __forceinline__ void bc_interpolated_node(S *base, uint64_t n, const uint32_t (&nodes)[8],
+                                                     const typename Codec<S>::compute *q27, uint64_t q_stride,
+                                                     double omega_real, typename Codec<S>::compute bx,
+                                                     typename Codec<S>::compute by, typename Codec<S>::compute bz)
 {
     using C = typename Codec<S>::compute;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.nbc)
-        return;
-    const uint32_t node = (uint32_t)a.k[i];
-    uint32_t nodes[8];
-    node_slots(node, a.nbx, a.nby, a.nbz, a.box, nodes);
-    S *base = static_cast<S *>(a.dist);
     C p[27];
-    gather_post<S, EVEN>(base, a.n, nodes, p);
+    gather_post<S, EVEN>(base, n, nodes, p);
     // plain-sum density and grouped momenta (NoSlipInterpolatedCompressible.cu:134-153)
     const C drho = p[21] + p[20] + p[19] + p[22] + p[25] + p[24] + p[23] + p[26] + p[17] + p[18] + p[15] + p[16] + p[13]
                  + p[14] + p[11] + p[12] + p[9] + p[10] + p[7] + p[8] + p[5] + p[6] + p[3] + p[4] + p[1] + p[2] + p[0];
@@ -694,17 +691,10 @@ __global__ void __launch_bounds__(128) bc_interpolated_kernel(BCArgs a)
     const C uz1 = FORM == kBCIncompressible ? vz : vz / r;
     const C cu_sq = FORM == kBCIncompressible ? C(1.5) * (ux1 * ux1 + uy1 * uy1 + uz1 * uz1)
                                               : C(1.5) * (ux1 * ux1 + uy1 * uy1 + uz1 * uz1) * (C(1) + drho);
-    const C omega = (C)a.omega;
-    const C *q27 = static_cast<const C *>(a.q27);
-    C bx = C(0), by = C(0), bz = C(0);
-    if (VELOCITY) {
-        bx = static_cast<const C *>(a.ux)[i];
-        by = static_cast<const C *>(a.uy)[i];
-        bz = static_cast<const C *>(a.uz)[i];
-    }
+    const C omega = (C)omega_real;
 #pragma unroll
     for (int d = 1; d < 27; ++d) {
-        const C q = q27[(uint64_t)d * a.nbc + i];
+        const C q = q27[(uint64_t)d * q_stride];
         if (q_active(q)) {
             const C w = weight_t<C>(d);
             const C vel = cdot_rt<C>(d, ux1, uy1, uz1);
@@ -725,9 +715,28 @@ __global__ void __launch_bounds__(128) bc_interpolated_kernel(BCArgs a)
                   + (q * (f + fi)) / (C(1) + q);
             }
             const int e = inv(d);
-            Codec<S>::store_at(base, (uint64_t)plane<!EVEN>(e) * a.n + nodes[shift_class(e)], v, e);
+            Codec<S>::store_at(base, (uint64_t)plane<!EVEN>(e) * n + nodes[shift_class(e)], v, e);
         }
     }
+}
+
+template <class S, bool EVEN, bool VELOCITY, int FORM = kBCCompressible>
+__global__ void __launch_bounds__(128) bc_interpolated_kernel(BCArgs a)
+{
+    using C = typename Codec<S>::compute;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nbc)
+        return;
+    uint32_t nodes[8];
+    node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.box, nodes);
+    C bx = C(0), by = C(0), bz = C(0);
+    if (VELOCITY) {
+        bx = static_cast<const C *>(a.ux)[i];
+        by = static_cast<const C *>(a.uy)[i];
+        bz = static_cast<const C *>(a.uz)[i];
+    }
+    bc_interpolated_node<S, EVEN, VELOCITY, FORM>(static_cast<S *>(a.dist), a.n, nodes,
+                                                  static_cast<const C *>(a.q27) + i, a.nbc, a.omega, bx, by, bz);
 }
 
 // feq - w of one direction in the form of the init and pressure kernels
@@ -746,19 +755,15 @@ __device__ __forceinline__ C feq_shifted(int d, C drho, C ux, C uy, C uz, C cusq
 // of the launch reads), so it has no counterpart here.
 // INCOMP: PressureNonEquilibriumIncompressible_Device (Pressure/PressureNonEquilibriumIncompressible.cu:45-314),
 // the same with getIncompressibleMacroscopicValues (u = momentum, not divided by rho)
-template <class S, bool EVEN, bool INCOMP = false>
-__global__ void __launch_bounds__(128) bc_pressure_neq_kernel(PressureArgs a)
+// one BC node: the slot nodes of the node (nk) and of its inward neighbour (nn)
+template <class S, bool EVEN, bool INCOMP>
+__device__ __forceinline__ void bc_pressure_neq_node(S *base, uint64_t n, const uint32_t (&nk)[8],
+                                                     const uint32_t (&nn)[8], typename Codec<S>::compute rbc,
+                                                     int direction)
 {
     using C = typename Codec<S>::compute;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.nbc)
-        return;
-    uint32_t nn[8], nk[8];
-    node_slots((uint32_t)a.kN[i], a.nbx, a.nby, a.nbz, a.box, nn);
-    node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.box, nk);
-    S *base = static_cast<S *>(a.dist);
     C f[27];
-    gather_pre<S, EVEN>(base, a.n, nn, f);
+    gather_pre<S, EVEN>(base, n, nn, f);
     const C drho1 = density_pyramid(f);
     C vx, vy, vz;
     if (INCOMP) {
@@ -772,17 +777,30 @@ __global__ void __launch_bounds__(128) bc_pressure_neq_kernel(PressureArgs a)
         vz = momentum_z(f) * inv_rho;
     }
     const C cusq = C(1.5) * (vx * vx + vy * vy + vz * vz);
-    const C rbc = static_cast<const C *>(a.rho_bc)[i];
-    const int axis = cx(a.direction) != 0 ? 0 : (cy(a.direction) != 0 ? 1 : 2);
-    const int sgn = axis == 0 ? cx(a.direction) : (axis == 1 ? cy(a.direction) : cz(a.direction));
+    const int axis = cx(direction) != 0 ? 0 : (cy(direction) != 0 ? 1 : 2);
+    const int sgn = axis == 0 ? cx(direction) : (axis == 1 ? cy(direction) : cz(direction));
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
         C v = f[d] - feq_shifted<C>(d, drho1, vx, vy, vz, cusq);
         v = v + feq_shifted<C>(d, rbc, vx, vy, vz, cusq);
         const int c = axis == 0 ? cx(d) : (axis == 1 ? cy(d) : cz(d));
         if (c != sgn)
-            Codec<S>::store_at(base, (uint64_t)plane<EVEN>(d) * a.n + nk[shift_class(d)], v, d);
+            Codec<S>::store_at(base, (uint64_t)plane<EVEN>(d) * n + nk[shift_class(d)], v, d);
     }
+}
+
+template <class S, bool EVEN, bool INCOMP = false>
+__global__ void __launch_bounds__(128) bc_pressure_neq_kernel(PressureArgs a)
+{
+    using C = typename Codec<S>::compute;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nbc)
+        return;
+    uint32_t nn[8], nk[8];
+    node_slots((uint32_t)a.kN[i], a.nbx, a.nby, a.nbz, a.box, nn);
+    node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.box, nk);
+    bc_pressure_neq_node<S, EVEN, INCOMP>(static_cast<S *>(a.dist), a.n, nk, nn, static_cast<const C *>(a.rho_bc)[i],
+                                          a.direction);
 }
 
 // OutflowNonReflecting_Device (Outflow/OutflowNonReflecting.cu:50-276) and, with CORRECTION,
@@ -1240,6 +1258,12 @@ struct PoolDomain {
     int flags;                   // bits 0-2: periodic x/y/z, bit 3: has a mask
     K17Rates<C> rates;
     C fx, fy, fz;                // half accelerations
+    double omega;                // the BC kernels' omega
+    uint64_t noslip_offset;      // bytes from the arena start: int32 k[n_noslip], then C q27[27 n_noslip]
+    uint64_t noslip_q_offset;
+    uint64_t pressure_offset;    // bytes: int32 k[n], int32 kN[n], int32 direction[n], then C drho[n]
+    uint64_t pressure_rho_offset;
+    uint32_t n_noslip, n_pressure;
 };
 
 enum : int { kPoolPeriodicX = 1, kPoolPeriodicY = 2, kPoolPeriodicZ = 4, kPoolMask = 8 };
@@ -1297,6 +1321,65 @@ __global__ void __launch_bounds__(256) k17_pool_kernel(PoolArgs<typename Codec<S
     }
 }
 
+
+// The boundary conditions of every domain of a pool, one launch per kind: a persistent grid over
+// {domain, first BC node} items of 128 BC nodes. No-slip: NoSlipInterpolatedCompressible after the
+// collision (current parity); pressure: PressureNonEquilibriumCompressible after the parity swap.
+// Box addressing per domain, as the structured box's BC lists.
+template <class C>
+struct PoolBCArgs {
+    void *arena;
+    const PoolDomain<C> *domains;
+    const uint2 *items;
+    const uint32_t *n_items;
+};
+
+template <class S, bool EVEN>
+__global__ void __launch_bounds__(128) pool_noslip_kernel(PoolBCArgs<typename Codec<S>::compute> a)
+{
+    using C = typename Codec<S>::compute;
+    const uint32_t n_items = __ldg(a.n_items);
+    for (uint32_t w = blockIdx.x; w < n_items; w += gridDim.x) {
+        const uint2 it = a.items[w];
+        const PoolDomain<C> &dm = a.domains[it.x];
+        const uint32_t i = it.y + threadIdx.x;
+        if (i >= dm.n_noslip)
+            continue;
+        const char *arena = static_cast<const char *>(a.arena);
+        const int32_t *k = reinterpret_cast<const int32_t *>(arena + dm.noslip_offset);
+        const C *q = reinterpret_cast<const C *>(arena + dm.noslip_q_offset);
+        const NodeAddr box{ dm.nx, dm.ny, dm.nz, dm.flags & 7 };
+        uint32_t nodes[8];
+        box_nodes((uint32_t)k[i], box, nodes);
+        bc_interpolated_node<S, EVEN, false, kBCCompressible>(static_cast<S *>(a.arena) + dm.dist_offset, dm.pitch,
+                                                              nodes, q + i, dm.n_noslip, dm.omega, C(0), C(0), C(0));
+    }
+}
+
+template <class S, bool EVEN>
+__global__ void __launch_bounds__(128) pool_pressure_kernel(PoolBCArgs<typename Codec<S>::compute> a)
+{
+    using C = typename Codec<S>::compute;
+    const uint32_t n_items = __ldg(a.n_items);
+    for (uint32_t w = blockIdx.x; w < n_items; w += gridDim.x) {
+        const uint2 it = a.items[w];
+        const PoolDomain<C> &dm = a.domains[it.x];
+        const uint32_t i = it.y + threadIdx.x;
+        if (i >= dm.n_pressure)
+            continue;
+        const char *arena = static_cast<const char *>(a.arena);
+        const int32_t *k = reinterpret_cast<const int32_t *>(arena + dm.pressure_offset);
+        const int32_t *kn = k + dm.n_pressure;
+        const int32_t *dir = kn + dm.n_pressure;
+        const C *rho = reinterpret_cast<const C *>(arena + dm.pressure_rho_offset);
+        const NodeAddr box{ dm.nx, dm.ny, dm.nz, dm.flags & 7 };
+        uint32_t nk[8], nn[8];
+        box_nodes((uint32_t)k[i], box, nk);
+        box_nodes((uint32_t)kn[i], box, nn);
+        bc_pressure_neq_node<S, EVEN, false>(static_cast<S *>(a.arena) + dm.dist_offset, dm.pitch, nk, nn, rho[i],
+                                             dir[i]);
+    }
+}
 
 // ---------------------------------------------------------------------------------------------
 // seeded per-step perturbation of a velocity inlet: u_i(t) = u0_i (1 + a (2 U - 1)), U uniform in

@@ -45,6 +45,18 @@ inline uint64_t box_blocks(const BoxState &b)
     return (uint64_t)((b.nx + bx - 1) / bx) * (uint64_t)b.ny * (uint64_t)b.nz * (uint64_t)(bx / 32);
 }
 
+// a pool domain's record as the host describes it (offsets in bytes from the arena start, except
+// dist_offset in elements)
+struct PoolDomainSpec {
+    uint64_t dist_offset, pitch, mask_offset;
+    int nx, ny, nz, flags;
+    double omega;
+    double lim[3];
+    double half_force[3];
+    uint64_t noslip_offset, noslip_q_offset, pressure_offset, pressure_rho_offset;
+    uint32_t n_noslip, n_pressure;
+};
+
 #define VFB_DECLARE_LAUNCHERS                                                                                        \
     template <class S>                                                                                               \
     struct Launchers {                                                                                               \
@@ -71,9 +83,10 @@ inline uint64_t box_blocks(const BoxState &b)
                                         unsigned block, cudaStream_t s);                                           \
         static const void *pool_kernel(bool even);                                                                \
         static size_t pool_domain_bytes();                                                                        \
-        static void pool_domain(void *out, uint64_t dist_offset, uint64_t pitch, uint64_t mask_offset, int nx,     \
-                                int ny, int nz, int flags, double omega, const double lim[3],                      \
-                                const double half_force[3]);                                                       \
+        static void pool_domain(void *out, const PoolDomainSpec &spec);                                            \
+        static cudaError_t pool_bcs(void *arena, const void *domains, const uint2 *noslip_items,                   \
+                                    const uint32_t *n_noslip_items, const uint2 *pressure_items,                   \
+                                    const uint32_t *n_pressure_items, bool even, unsigned grid, cudaStream_t s);   \
         static cudaError_t drag_lift(const vfb_level *L, const vfb_bc *bc, bool pre, double *dx, double *dy,        \
                                      double *dz, cudaStream_t s, const NodeAddr *box = nullptr);                     \
         static cudaError_t scale(const vfb_level *coarse, const vfb_level *fine, const vfb_interpolation_cells *cells, \

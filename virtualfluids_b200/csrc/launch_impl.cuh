@@ -218,23 +218,58 @@ size_t Launchers<S>::pool_domain_bytes()
 // the domain record in the compute type of S, with the rates and forces rounded as the box path
 // rounds them (so a domain in the pool and the same box alone compute the same bits)
 template <class S>
-void Launchers<S>::pool_domain(void *out, uint64_t dist_offset, uint64_t pitch, uint64_t mask_offset, int nx, int ny,
-                               int nz, int flags, double omega, const double lim[3], const double half_force[3])
+void Launchers<S>::pool_domain(void *out, const PoolDomainSpec &spec)
 {
     using C = typename Codec<S>::compute;
     PoolDomain<C> d;
-    d.dist_offset = dist_offset;
-    d.pitch = pitch;
-    d.mask_offset = mask_offset;
-    d.nx = nx;
-    d.ny = ny;
-    d.nz = nz;
-    d.flags = flags;
-    d.rates = rates_of<C>(omega, lim);
-    d.fx = (C)half_force[0];
-    d.fy = (C)half_force[1];
-    d.fz = (C)half_force[2];
+    std::memset(&d, 0, sizeof(d));
+    d.dist_offset = spec.dist_offset;
+    d.pitch = spec.pitch;
+    d.mask_offset = spec.mask_offset;
+    d.nx = spec.nx;
+    d.ny = spec.ny;
+    d.nz = spec.nz;
+    d.flags = spec.flags;
+    d.rates = rates_of<C>(spec.omega, spec.lim);
+    d.fx = (C)spec.half_force[0];
+    d.fy = (C)spec.half_force[1];
+    d.fz = (C)spec.half_force[2];
+    d.omega = spec.omega;
+    d.noslip_offset = spec.noslip_offset;
+    d.noslip_q_offset = spec.noslip_q_offset;
+    d.pressure_offset = spec.pressure_offset;
+    d.pressure_rho_offset = spec.pressure_rho_offset;
+    d.n_noslip = spec.n_noslip;
+    d.n_pressure = spec.n_pressure;
     std::memcpy(out, &d, sizeof(d));
+}
+
+template <class S>
+cudaError_t Launchers<S>::pool_bcs(void *arena, const void *domains, const uint2 *noslip_items,
+                                   const uint32_t *n_noslip_items, const uint2 *pressure_items,
+                                   const uint32_t *n_pressure_items, bool even, unsigned grid, cudaStream_t s)
+{
+    using C = typename Codec<S>::compute;
+    PoolBCArgs<C> a;
+    a.arena = arena;
+    a.domains = static_cast<const PoolDomain<C> *>(domains);
+    if (noslip_items) {
+        a.items = noslip_items;
+        a.n_items = n_noslip_items;
+        if (even) pool_noslip_kernel<S, true><<<grid, 128, 0, s>>>(a);
+        else pool_noslip_kernel<S, false><<<grid, 128, 0, s>>>(a);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess)
+            return e;
+    }
+    if (pressure_items) {
+        // after the parity swap
+        a.items = pressure_items;
+        a.n_items = n_pressure_items;
+        if (even) pool_pressure_kernel<S, false><<<grid, 128, 0, s>>>(a);
+        else pool_pressure_kernel<S, true><<<grid, 128, 0, s>>>(a);
+    }
+    return cudaGetLastError();
 }
 
 template <class S>

@@ -44,7 +44,9 @@ struct PoolOps {
                            cudaStream_t);
     const void *(*kernel)(bool);
     size_t (*domain_bytes)();
-    void (*domain)(void *, uint64_t, uint64_t, uint64_t, int, int, int, int, double, const double *, const double *);
+    void (*domain)(void *, const vfb::PoolDomainSpec &);
+    cudaError_t (*bcs)(void *, const void *, const uint2 *, const uint32_t *, const uint2 *, const uint32_t *, bool,
+                       unsigned, cudaStream_t);
     cudaError_t (*init)(const vfb::BoxState &, bool, const void *, const void *, const void *, const void *,
                         cudaStream_t);
     cudaError_t (*macros)(const vfb::BoxState &, bool, void *, void *, void *, void *, cudaStream_t);
@@ -53,8 +55,8 @@ struct PoolOps {
 template <class LA>
 PoolOps ops_of()
 {
-    return PoolOps{ LA::pool_collide, LA::pool_kernel, LA::pool_domain_bytes, LA::pool_domain, LA::box_init,
-                    LA::box_macros };
+    return PoolOps{ LA::pool_collide, LA::pool_kernel, LA::pool_domain_bytes, LA::pool_domain, LA::pool_bcs,
+                    LA::box_init, LA::box_macros };
 }
 
 bool select_ops(int storage, int arith, PoolOps &out)
@@ -125,9 +127,20 @@ struct DomainSlot {
     uint64_t nodes = 0, pitch = 0;
     uint64_t dist_offset = 0;      // bytes
     uint64_t mask_offset = 0;      // bytes
-    uint64_t bytes = 0;            // bytes taken (populations + mask)
+    uint64_t bytes = 0;            // bytes taken (populations, mask, boundary conditions)
     bool has_mask = false;
+    uint32_t n_noslip = 0, n_pressure = 0;
 };
+
+// a work list on the device: {domain, first node} items and their count (a device word, so that a
+// captured step keeps working after the list changes)
+struct DeviceList {
+    uint2 *items = nullptr;
+    uint32_t *count = nullptr;
+    size_t capacity = 0;
+};
+
+constexpr uint32_t kBCSpan = 128;   // BC nodes per item (one thread each)
 
 constexpr uint32_t kGraphSteps = 16;
 
@@ -154,6 +167,9 @@ struct vfb_pool {
     uint64_t launches = 0;
     void *staging = nullptr;           // host<->device field staging, outside the arena
     uint64_t staging_bytes = 0;
+    DeviceList noslip_list, pressure_list;   // BC work lists of the active domains
+    bool has_noslip = false, has_pressure = false;
+    unsigned bc_grid = 0;
 };
 
 namespace {
@@ -187,6 +203,7 @@ cudaError_t update_grid(vfb_pool *p)
     if (g != p->grid)
         drop_graph(p);
     p->grid = g;
+    p->bc_grid = (unsigned)(4 * sm_count_here());
     return cudaSuccess;
 }
 
@@ -198,6 +215,65 @@ void reclaim(vfb_pool *p)
             p->alloc.give(d.dist_offset, d.bytes);
             d = DomainSlot();
         }
+}
+
+// copies `items` into a device list, growing it (and dropping the captured steps that refer to the
+// old buffer) when needed; synchronous with respect to the host
+cudaError_t upload_list(vfb_pool *p, DeviceList &L, const std::vector<uint2> &items, cudaStream_t s)
+{
+    cudaError_t e = cudaSuccess;
+    if (!L.count) {
+        e = cudaMalloc((void **)&L.count, sizeof(uint32_t));
+        if (e != cudaSuccess)
+            return e;
+    }
+    if (items.size() > L.capacity) {
+        drop_graph(p);
+        e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess)
+            return e;
+        cudaFree(L.items);
+        L.items = nullptr;
+        const size_t cap = std::max<size_t>(items.size() + items.size() / 2, 1024);
+        e = cudaMalloc((void **)&L.items, cap * sizeof(uint2));
+        L.capacity = e == cudaSuccess ? cap : 0;
+        if (e != cudaSuccess)
+            return e;
+    }
+    if (!items.empty())
+        e = cudaMemcpyAsync(L.items, items.data(), items.size() * sizeof(uint2), cudaMemcpyHostToDevice, s);
+    const uint32_t n = (uint32_t)items.size();
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(L.count, &n, sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s);
+    return e;
+}
+
+// the boundary-condition work lists: per active domain with BC nodes one item per kBCSpan nodes
+cudaError_t rebuild_bc_lists(vfb_pool *p, cudaStream_t s)
+{
+    std::vector<uint2> ns, pr;
+    for (uint32_t id = 0; id < p->slots.size(); ++id) {
+        const DomainSlot &d = p->slots[id];
+        if (!d.live || !d.active)
+            continue;
+        for (uint32_t i = 0; i < d.n_noslip; i += kBCSpan)
+            ns.push_back(make_uint2(id, i));
+        for (uint32_t i = 0; i < d.n_pressure; i += kBCSpan)
+            pr.push_back(make_uint2(id, i));
+    }
+    const bool has_ns = !ns.empty(), has_pr = !pr.empty();
+    if (has_ns != p->has_noslip || has_pr != p->has_pressure)
+        drop_graph(p);              // the launches of a step change
+    p->has_noslip = has_ns;
+    p->has_pressure = has_pr;
+    cudaError_t e = cudaSuccess;
+    if (has_ns || p->noslip_list.count)
+        e = upload_list(p, p->noslip_list, ns, s);
+    if (e == cudaSuccess && (has_pr || p->pressure_list.count))
+        e = upload_list(p, p->pressure_list, pr, s);
+    return e;
 }
 
 // the work list: per active domain (in id order) one item per `threads * nodes_per_thread` nodes
@@ -236,17 +312,32 @@ cudaError_t rebuild_list(vfb_pool *p, cudaStream_t s)
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(s);
     if (e == cudaSuccess)
+        e = rebuild_bc_lists(p, s);
+    if (e == cudaSuccess)
         reclaim(p);
     p->active_nodes = nodes;
     p->list_dirty = false;
     return e;
 }
 
+// one step: the collision, then the no-slip BCs at its parity and the pressure BCs after the swap
 cudaError_t launch_step(vfb_pool *p, bool even, cudaStream_t s)
 {
     ++p->launches;
-    return p->ops.collide(p->arena, p->domain_table, p->items, p->n_items, p->nodes_per_thread, even, p->grid,
-                          (unsigned)p->threads, s);
+    cudaError_t e = p->ops.collide(p->arena, p->domain_table, p->items, p->n_items, p->nodes_per_thread, even, p->grid,
+                                   (unsigned)p->threads, s);
+    if (e == cudaSuccess && (p->has_noslip || p->has_pressure)) {
+        p->launches += (p->has_noslip ? 1 : 0) + (p->has_pressure ? 1 : 0);
+        e = p->ops.bcs(p->arena, p->domain_table, p->has_noslip ? p->noslip_list.items : nullptr,
+                       p->noslip_list.count, p->has_pressure ? p->pressure_list.items : nullptr,
+                       p->pressure_list.count, even, p->bc_grid, s);
+    }
+    return e;
+}
+
+uint32_t launches_per_step(const vfb_pool *p)
+{
+    return 1u + (p->has_noslip ? 1u : 0u) + (p->has_pressure ? 1u : 0u);
 }
 
 // kGraphSteps steps starting at the even parity, captured once and replayed
@@ -259,9 +350,10 @@ cudaError_t ensure_graph(vfb_pool *p, cudaStream_t s)
     cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess)
         return e;
+    const uint64_t launches = p->launches;
     for (uint32_t i = 0; i < kGraphSteps; ++i)
-        p->ops.collide(p->arena, p->domain_table, p->items, p->n_items, p->nodes_per_thread, (i & 1u) == 0, p->grid,
-                       (unsigned)p->threads, s);
+        launch_step(p, (i & 1u) == 0, s);
+    p->launches = launches;       // counted when the graph runs
     e = cudaStreamEndCapture(s, &g);
     if (e != cudaSuccess)
         return e;
@@ -342,6 +434,58 @@ void domain_sizes(const vfb_pool *p, const vfb_domain_desc *d, bool has_mask, ui
     mask_bytes = has_mask ? align_up(n) : 0;
 }
 
+// arena bytes of a domain's BC lists: no-slip k and q27, pressure k, kN, direction and drho
+struct BCSizes {
+    uint64_t noslip_k, noslip_q, pressure_i, pressure_rho;
+    uint64_t total() const { return noslip_k + noslip_q + pressure_i + pressure_rho; }
+};
+
+BCSizes bc_sizes(const vfb_pool *p, uint32_t n_noslip, uint32_t n_pressure)
+{
+    const uint64_t rs = real_size(p->desc.storage);
+    BCSizes b;
+    b.noslip_k = n_noslip ? align_up(4ull * n_noslip) : 0;
+    b.noslip_q = n_noslip ? align_up(27ull * n_noslip * rs) : 0;
+    b.pressure_i = n_pressure ? align_up(12ull * n_pressure) : 0;
+    b.pressure_rho = n_pressure ? align_up((uint64_t)n_pressure * rs) : 0;
+    return b;
+}
+
+bool is_axis_direction(int32_t d) { return d >= VFB_DIR_P00 && d <= VFB_DIR_00M; }
+
+// host-side checks of a domain's BC lists against its extents and mask (1 = fluid)
+int check_bcs(const vfb_domain_bcs *b, const vfb_domain_desc *d, const std::vector<uint8_t> *mask)
+{
+    if (!b)
+        return VFB_OK;
+    const uint64_t nodes = (uint64_t)d->nx * d->ny * d->nz;
+    if (b->number_of_noslip_nodes) {
+        if (b->noslip_variant != VFB_NOSLIP_INTERPOLATED_COMPRESSIBLE)
+            return pool_fail(VFB_ERR_UNSUPPORTED, "pools run NoSlipInterpolatedCompressible no-slip lists");
+        if (!b->noslip_k || !b->noslip_q27)
+            return pool_fail(VFB_ERR_INVALID_ARGUMENT, "no-slip arrays are NULL");
+    }
+    if (b->number_of_pressure_nodes) {
+        if (b->pressure_variant != VFB_PRESSURE_NON_EQUILIBRIUM_COMPRESSIBLE)
+            return pool_fail(VFB_ERR_UNSUPPORTED, "pools run PressureNonEquilibriumCompressible pressure lists");
+        if (!b->pressure_k || !b->pressure_k_neighbor || !b->pressure_rho || !b->pressure_direction)
+            return pool_fail(VFB_ERR_INVALID_ARGUMENT, "pressure arrays are NULL");
+    }
+    auto fluid = [&](int32_t k) {
+        return k >= 0 && (uint64_t)k < nodes && (!mask || (*mask)[(size_t)k] != 0);
+    };
+    for (uint32_t i = 0; i < b->number_of_noslip_nodes; ++i)
+        if (!fluid(b->noslip_k[i]))
+            return pool_fail(VFB_ERR_INVALID_ARGUMENT, "a no-slip BC node is outside the domain or not fluid");
+    for (uint32_t i = 0; i < b->number_of_pressure_nodes; ++i) {
+        if (!fluid(b->pressure_k[i]) || b->pressure_k_neighbor[i] < 0 || (uint64_t)b->pressure_k_neighbor[i] >= nodes)
+            return pool_fail(VFB_ERR_INVALID_ARGUMENT, "a pressure BC node or its neighbour is outside the domain");
+        if (!is_axis_direction(b->pressure_direction[i]))
+            return pool_fail(VFB_ERR_INVALID_ARGUMENT, "pressure directions are VFB_DIR_P00 ... VFB_DIR_00M");
+    }
+    return VFB_OK;
+}
+
 } // namespace
 
 extern "C" {
@@ -392,11 +536,21 @@ int vfb_pool_destroy(vfb_pool *p)
     cudaFree(p->items);
     cudaFree(p->n_items);
     cudaFree(p->staging);
+    for (DeviceList *L : { &p->noslip_list, &p->pressure_list }) {
+        cudaFree(L->items);
+        cudaFree(L->count);
+    }
     delete p;
     return VFB_OK;
 }
 
 int vfb_pool_domain_bytes(const vfb_pool *p, const vfb_domain_desc *d, int32_t has_mask, uint64_t *bytes)
+{
+    return vfb_pool_domain_bytes_with_bcs(p, d, has_mask, 0, 0, bytes);
+}
+
+int vfb_pool_domain_bytes_with_bcs(const vfb_pool *p, const vfb_domain_desc *d, int32_t has_mask,
+                                   uint32_t number_of_noslip_nodes, uint32_t number_of_pressure_nodes, uint64_t *bytes)
 {
     if (!p || !bytes)
         return pool_fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
@@ -405,11 +559,35 @@ int vfb_pool_domain_bytes(const vfb_pool *p, const vfb_domain_desc *d, int32_t h
         return st;
     uint64_t pitch, pop, mask;
     domain_sizes(p, d, needs_mask(d, has_mask != 0), pitch, pop, mask);
-    *bytes = pop + mask;
+    *bytes = pop + mask + bc_sizes(p, number_of_noslip_nodes, number_of_pressure_nodes).total();
     return VFB_OK;
 }
 
 int vfb_pool_add_domain(vfb_pool *p, const vfb_domain_desc *d, const uint8_t *user_mask, uint32_t *id)
+{
+    return vfb_pool_add_domain_with_bcs(p, d, user_mask, nullptr, id);
+}
+
+namespace {
+// host array of the pool's real type from doubles
+std::vector<unsigned char> to_real(const vfb_pool *p, const double *v, size_t n)
+{
+    const size_t rs = real_size(p->desc.storage);
+    std::vector<unsigned char> out(n * rs);
+    if (rs == 8) {
+        std::memcpy(out.data(), v, n * 8);
+    } else {
+        for (size_t i = 0; i < n; ++i) {
+            const float f = (float)v[i];
+            std::memcpy(out.data() + 4 * i, &f, 4);
+        }
+    }
+    return out;
+}
+} // namespace
+
+int vfb_pool_add_domain_with_bcs(vfb_pool *p, const vfb_domain_desc *d, const uint8_t *user_mask,
+                                 const vfb_domain_bcs *bcs, uint32_t *id)
 {
     if (!p || !id)
         return pool_fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
@@ -425,19 +603,10 @@ int vfb_pool_add_domain(vfb_pool *p, const vfb_domain_desc *d, const uint8_t *us
     ds.desc = *d;
     ds.nodes = (uint64_t)d->nx * d->ny * d->nz;
     ds.has_mask = needs_mask(d, user_mask != nullptr);
-    uint64_t pop, mask;
-    domain_sizes(p, d, ds.has_mask, ds.pitch, pop, mask);
-    uint64_t off = 0;
-    if (!p->alloc.take(pop + mask, off))
-        return pool_fail(VFB_ERR_OUT_OF_MEMORY, "the pool's arena has no room for this domain");
-    ds.dist_offset = off;
-    ds.mask_offset = off + pop;
-    ds.bytes = pop + mask;
-    ds.live = true;
-    cudaError_t e = cudaSuccess;
+    std::vector<uint8_t> m;
     if (ds.has_mask) {
         // walls of the non-periodic axes, then the caller's solid nodes
-        std::vector<uint8_t> m(ds.nodes, 1);
+        m.assign(ds.nodes, 1);
         const int nx = d->nx, ny = d->ny, nz = d->nz;
         for (int z = 0; z < nz; ++z)
             for (int y = 0; y < ny; ++y)
@@ -449,14 +618,67 @@ int vfb_pool_add_domain(vfb_pool *p, const vfb_domain_desc *d, const uint8_t *us
                     if (wall || (user_mask && user_mask[k] == 0))
                         m[k] = 0;
                 }
-        e = cudaMemcpy(static_cast<char *>(p->arena) + ds.mask_offset, m.data(), ds.nodes, cudaMemcpyHostToDevice);
+    }
+    st = check_bcs(bcs, d, ds.has_mask ? &m : nullptr);
+    if (st)
+        return st;
+    ds.n_noslip = bcs ? bcs->number_of_noslip_nodes : 0;
+    ds.n_pressure = bcs ? bcs->number_of_pressure_nodes : 0;
+    uint64_t pop, mask;
+    domain_sizes(p, d, ds.has_mask, ds.pitch, pop, mask);
+    const BCSizes bs = bc_sizes(p, ds.n_noslip, ds.n_pressure);
+    uint64_t off = 0;
+    if (!p->alloc.take(pop + mask + bs.total(), off))
+        return pool_fail(VFB_ERR_OUT_OF_MEMORY, "the pool's arena has no room for this domain");
+    ds.dist_offset = off;
+    ds.mask_offset = off + pop;
+    ds.bytes = pop + mask + bs.total();
+    ds.live = true;
+    vfb::PoolDomainSpec spec{};
+    spec.noslip_offset = off + pop + mask;
+    spec.noslip_q_offset = spec.noslip_offset + bs.noslip_k;
+    spec.pressure_offset = spec.noslip_q_offset + bs.noslip_q;
+    spec.pressure_rho_offset = spec.pressure_offset + bs.pressure_i;
+    char *arena = static_cast<char *>(p->arena);
+    cudaError_t e = cudaSuccess;
+    if (ds.has_mask)
+        e = cudaMemcpy(arena + ds.mask_offset, m.data(), ds.nodes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && ds.n_noslip) {
+        e = cudaMemcpy(arena + spec.noslip_offset, bcs->noslip_k, 4ull * ds.n_noslip, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) {
+            const auto q = to_real(p, bcs->noslip_q27, 27ull * ds.n_noslip);
+            e = cudaMemcpy(arena + spec.noslip_q_offset, q.data(), q.size(), cudaMemcpyHostToDevice);
+        }
+    }
+    if (e == cudaSuccess && ds.n_pressure) {
+        const uint64_t n4 = 4ull * ds.n_pressure;
+        e = cudaMemcpy(arena + spec.pressure_offset, bcs->pressure_k, n4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(arena + spec.pressure_offset + n4, bcs->pressure_k_neighbor, n4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(arena + spec.pressure_offset + 2 * n4, bcs->pressure_direction, n4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) {
+            const auto r = to_real(p, bcs->pressure_rho, ds.n_pressure);
+            e = cudaMemcpy(arena + spec.pressure_rho_offset, r.data(), r.size(), cudaMemcpyHostToDevice);
+        }
     }
     std::vector<unsigned char> rec(p->record_bytes);
-    const double half[3] = { d->forces[0] * 0.5, d->forces[1] * 0.5, d->forces[2] * 0.5 };
-    const int flags = (d->periodic_x ? 1 : 0) | (d->periodic_y ? 2 : 0) | (d->periodic_z ? 4 : 0) | (ds.has_mask ? 8 : 0);
     const uint64_t sb = storage_size(p->desc.storage);
-    p->ops.domain(rec.data(), ds.dist_offset / sb, ds.pitch, ds.mask_offset, d->nx, d->ny, d->nz, flags, d->omega,
-                  d->quadric_limiters, half);
+    spec.dist_offset = ds.dist_offset / sb;
+    spec.pitch = ds.pitch;
+    spec.mask_offset = ds.mask_offset;
+    spec.nx = d->nx;
+    spec.ny = d->ny;
+    spec.nz = d->nz;
+    spec.flags = (d->periodic_x ? 1 : 0) | (d->periodic_y ? 2 : 0) | (d->periodic_z ? 4 : 0) | (ds.has_mask ? 8 : 0);
+    spec.omega = d->omega;
+    for (int i = 0; i < 3; ++i) {
+        spec.lim[i] = d->quadric_limiters[i];
+        spec.half_force[i] = d->forces[i] * 0.5;
+    }
+    spec.n_noslip = ds.n_noslip;
+    spec.n_pressure = ds.n_pressure;
+    p->ops.domain(rec.data(), spec);
     if (e == cudaSuccess)
         e = cudaMemcpy(static_cast<char *>(p->domain_table) + (size_t)slot * p->record_bytes, rec.data(), p->record_bytes,
                        cudaMemcpyHostToDevice);
@@ -546,7 +768,7 @@ int vfb_pool_step(vfb_pool *p, uint32_t steps, void *stream)
             e = ensure_graph(p, s);
             if (e == cudaSuccess)
                 e = cudaGraphLaunch(p->graph, s);
-            p->launches += kGraphSteps;
+            p->launches += (uint64_t)kGraphSteps * launches_per_step(p);
             done += kGraphSteps;   // an even number of steps: the parity is unchanged
             continue;
         }

@@ -58,18 +58,51 @@ class Pool:
             d.quadric_limiters[i] = float(limiters[i])
         return d
 
-    def domain_bytes(self, shape, omega=1.8, periodic=(True, True, True), has_mask=False) -> int:
+    def domain_bytes(self, shape, omega=1.8, periodic=(True, True, True), has_mask=False, n_noslip=0,
+                     n_pressure=0) -> int:
         b = C.c_uint64()
-        N.check(N.lib().vfb_pool_domain_bytes(self._h, C.byref(self.desc(shape, omega, periodic)), int(has_mask),
-                                              C.byref(b)))
+        N.check(N.lib().vfb_pool_domain_bytes_with_bcs(self._h, C.byref(self.desc(shape, omega, periodic)),
+                                                       int(has_mask), int(n_noslip), int(n_pressure), C.byref(b)))
         return b.value
 
-    def add(self, shape, omega, periodic=(True, True, True), forces=(0.0, 0.0, 0.0), mask=None) -> int:
-        """Carve a domain; raises VfbError(VFB_ERR_OUT_OF_MEMORY) when the arena has no room."""
+    @staticmethod
+    def _bcs(bcs):
+        """vfb_domain_bcs from {"noslip": (k, q27[27, n]), "pressure": (k, kN, drho, direction)} (host
+        arrays); returns the struct and the arrays it points to."""
+        out = N.DomainBCs()
+        keep = []
+        if bcs and "noslip" in bcs:
+            k, q = bcs["noslip"]
+            k = np.ascontiguousarray(k, dtype=np.int32).reshape(-1)
+            q = np.ascontiguousarray(q, dtype=np.float64).reshape(27, k.size)
+            keep += [k, q]
+            out.noslip_variant = N.NOSLIP_INTERPOLATED_COMPRESSIBLE
+            out.noslip_k, out.noslip_q27, out.number_of_noslip_nodes = k.ctypes.data, q.ctypes.data, k.size
+        if bcs and "pressure" in bcs:
+            k, kn, rho, direction = bcs["pressure"]
+            k = np.ascontiguousarray(k, dtype=np.int32).reshape(-1)
+            arrs = [k, np.ascontiguousarray(kn, dtype=np.int32).reshape(-1),
+                    np.ascontiguousarray(np.broadcast_to(np.asarray(rho, dtype=np.float64), k.shape)),
+                    np.ascontiguousarray(np.broadcast_to(np.asarray(direction, dtype=np.int32), k.shape))]
+            keep += arrs
+            out.pressure_variant = N.PRESSURE_NON_EQUILIBRIUM_COMPRESSIBLE
+            out.pressure_k, out.pressure_k_neighbor, out.pressure_rho, out.pressure_direction = \
+                (a.ctypes.data for a in arrs)
+            out.number_of_pressure_nodes = k.size
+        return out, keep
+
+    def add(self, shape, omega, periodic=(True, True, True), forces=(0.0, 0.0, 0.0), mask=None, bcs=None) -> int:
+        """Carve a domain; raises VfbError(VFB_ERR_OUT_OF_MEMORY) when the arena has no room. bcs:
+        optional boundary-condition lists, {"noslip": (k, q27), "pressure": (k, k_neighbor, drho,
+        direction)} in box node indices (NoSlipInterpolatedCompressible and
+        PressureNonEquilibriumCompressible; drho and direction scalars or per node)."""
         d = self.desc(shape, omega, periodic, forces)
         m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8).reshape(-1)
         i = C.c_uint32()
-        N.check(N.lib().vfb_pool_add_domain(self._h, C.byref(d), m.ctypes.data if m is not None else None, C.byref(i)))
+        b, keep = self._bcs(bcs)
+        N.check(N.lib().vfb_pool_add_domain_with_bcs(self._h, C.byref(d), m.ctypes.data if m is not None else None,
+                                                     C.byref(b) if bcs else None, C.byref(i)))
+        del keep
         self.domains[i.value] = tuple(int(v) for v in shape)
         return i.value
 

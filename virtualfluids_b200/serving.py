@@ -8,11 +8,16 @@ Populations and masks stay resident on the device between steps. A solve compute
 computes alone (the pool's kernels treat every domain independently), so its result does not
 depend on what else is being served.
 
-The porous-block workload (config 5): a cube of random non-overlapping spheres, periodic on every
-axis, driven along x by the body force equivalent to the imposed pressure drop (dp / L = rho_0 g);
-the sphere surfaces are the reference's default no-slip (NoSlipDelayBounceBack: solid nodes are
-not updated). The result of a solve is its Darcy permeability k = nu <u_x> / g, with <u_x> the
-superficial velocity (the mean over all nodes, solid ones counting zero).
+The porous-block workload (config 5): a cube of random non-overlapping spheres. Two drives:
+
+* ``"pressure"`` (the default): the block lies between two pressure planes at x (drho = +-dp/2,
+  PressureNonEquilibriumCompressible), periodic in y and z; every link cut by a sphere carries the
+  exact q of its intersection (NoSlipInterpolatedCompressible). Both lists stay resident in the
+  pool's arena with the populations. Darcy permeability k = nu <u_x> L / (dp / 3);
+* ``"force"``: periodic on every axis, driven by the body force g equivalent to the pressure drop,
+  the spheres as staircase solids (NoSlipDelayBounceBack); k = nu <u_x> / g.
+
+<u_x> is the superficial velocity: the mean over the block's nodes, solid ones counting zero.
 """
 from __future__ import annotations
 
@@ -23,7 +28,7 @@ import numpy as np
 
 from . import _native as N
 from .pool import Pool
-from .workloads import porous_block
+from .workloads import porous_block, porous_block_bcs
 
 
 @dataclass
@@ -35,14 +40,38 @@ class Request:
     seed: int
     porosity: float
     nu: float = 1.0 / 60.0
-    g: float = 1e-6
-    mask: np.ndarray | None = field(default=None, repr=False)   # voxelised geometry, nonzero = fluid
+    g: float = 1e-6                   # body force of the "force" drive
+    drho: float = 3e-3                # density drop across the block of the "pressure" drive
+    drive: str = "pressure"
+    geo: dict | None = field(default=None, repr=False)
 
     def geometry(self):
-        """The request's voxelised porous block (built on first use)."""
-        if self.mask is None:
-            self.mask, _, _ = porous_block(self.side, self.seed, porosity=self.porosity)
-        return self.mask
+        """The request's domain (built on first use): shape, periodicity, mask, BC lists and the
+        slice of the block's nodes along x."""
+        if self.geo is None:
+            if self.drive == "pressure":
+                g = porous_block_bcs(self.side, self.seed, porosity=self.porosity, drho=self.drho)
+                g.update(periodic=(False, True, True), forces=(0.0, 0.0, 0.0), block=slice(1, self.side + 1))
+            else:
+                mask, spheres, phi = porous_block(self.side, self.seed, porosity=self.porosity)
+                g = {"shape": (self.side,) * 3, "mask": mask, "bcs": None, "spheres": spheres, "porosity": phi,
+                     "periodic": (True, True, True), "forces": (self.g, 0.0, 0.0), "block": slice(0, self.side)}
+            self.geo = g
+        return self.geo
+
+    @property
+    def fluid_nodes(self) -> int:
+        g = self.geometry()
+        nx, ny, nz = g["shape"]
+        return int(g["mask"].reshape(nz, ny, nx)[:, :, g["block"]].astype(bool).sum())
+
+    def permeability(self, ux) -> float:
+        """Darcy permeability from the velocity field (nz, ny, nx) of the domain."""
+        g = self.geometry()
+        mean = float(ux[:, :, g["block"]].astype(np.float64).mean())
+        if self.drive == "pressure":
+            return self.nu * mean * g["length"] / (g["drho"] / 3.0)
+        return self.nu * mean / self.g
 
 
 @dataclass
@@ -61,9 +90,10 @@ class Result:
         return self.finished - self.arrival
 
 
-def poisson_stream(count, rate, seed=20261203, sides=(32, 192), steps=(1000, 20000), porosity=(0.5, 0.9)):
+def poisson_stream(count, rate, seed=20261203, sides=(32, 192), steps=(1000, 20000), porosity=(0.5, 0.9),
+                   drive="pressure"):
     """`count` porous-block requests with exponential inter-arrival times of mean 1 / rate seconds.
-    A request carries its geometry (voxelised by Request.geometry, before it is submitted)."""
+    A request carries its geometry (built by Request.geometry, before it is submitted)."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
@@ -71,12 +101,12 @@ def poisson_stream(count, rate, seed=20261203, sides=(32, 192), steps=(1000, 200
         t += float(rng.exponential(1.0 / rate))
         out.append(Request(rid=i, arrival=t, side=int(rng.integers(sides[0], sides[1] + 1)),
                            steps=int(rng.integers(steps[0], steps[1] + 1)), seed=int(rng.integers(1 << 31)),
-                           porosity=float(rng.uniform(*porosity))))
+                           porosity=float(rng.uniform(*porosity)), drive=drive))
     return out
 
 
 def request_work(req: Request):
-    """Node updates of a request (all nodes x steps)."""
+    """Node updates of a request (the block's nodes x steps)."""
     return req.side ** 3 * req.steps
 
 
@@ -109,12 +139,12 @@ class Server:
         return self._zeros[:n]
 
     def _try_admit(self, req):
-        omega = 1.0 / (3.0 * req.nu + 0.5)
-        d = self.pool.try_add((req.side,) * 3, omega, periodic=(True, True, True), forces=(req.g, 0.0, 0.0),
-                              mask=req.geometry())
+        g = req.geometry()
+        d = self.pool.try_add(g["shape"], 1.0 / (3.0 * req.nu + 0.5), periodic=g["periodic"], forces=g["forces"],
+                              mask=g["mask"], bcs=g["bcs"])
         if d is None:
             return None
-        z = self._rest(req.side ** 3)
+        z = self._rest(int(np.prod(g["shape"])))
         self.pool.init(d, z, z, z, z, stream=self.stream)
         return d
 
@@ -156,7 +186,7 @@ class Server:
                     continue
                 else:
                     continue
-            nodes = sum(v[0].side ** 3 for v in active.values())
+            nodes = sum(int(np.prod(v[0].geometry()["shape"])) for v in active.values())
             by_time = max(1, int(self.chunk_ms * 1e6 / (self.ns_per_node_step * nodes)))
             chunk = min(by_time, min(v[1] for v in active.values()))
             c0 = clock()
@@ -167,9 +197,8 @@ class Server:
             for d in [d for d, v in active.items() if v[1] == chunk]:
                 req, _, adm = active.pop(d)
                 rho, ux, uy, uz = self.pool.fields(d, stream=self.stream)
-                perm = req.nu * float(ux.astype(np.float64).mean()) / req.g
-                results[req.rid] = Result(req.rid, req.arrival, adm, clock() - t0, req.steps,
-                                          int(req.geometry().sum()), perm, ux.copy() if self.keep_fields else None)
+                results[req.rid] = Result(req.rid, req.arrival, adm, clock() - t0, req.steps, req.fluid_nodes,
+                                          req.permeability(ux), ux.copy() if self.keep_fields else None)
                 self.pool.remove(d)
             for v in active.values():
                 v[1] -= chunk
@@ -187,16 +216,19 @@ def solve_alone(req: Request, storage="f32", stream=None):
     """One request in a pool of its own (the reference result for the mix, and the FP64 run)."""
     import torch
     s = stream or torch.cuda.Stream()
-    mask = req.geometry()
+    g = req.geometry()
+    bcs = g["bcs"] or {}
+    n_ns = len(bcs["noslip"][0]) if "noslip" in bcs else 0
+    n_pr = len(bcs["pressure"][0]) if "pressure" in bcs else 0
     probe = Pool(1 << 20, storage=storage, max_domains=1)
-    need = probe.domain_bytes((req.side,) * 3, has_mask=True)
+    need = probe.domain_bytes(g["shape"], periodic=g["periodic"], has_mask=True, n_noslip=n_ns, n_pressure=n_pr)
     probe.close()
     pool = Pool(need + (1 << 20), storage=storage, max_domains=1)
-    d = pool.add((req.side,) * 3, 1.0 / (3.0 * req.nu + 0.5), periodic=(True, True, True), forces=(req.g, 0.0, 0.0),
-                 mask=mask)
+    d = pool.add(g["shape"], 1.0 / (3.0 * req.nu + 0.5), periodic=g["periodic"], forces=g["forces"], mask=g["mask"],
+                 bcs=g["bcs"])
     pool.init(d, stream=s)
     pool.step(req.steps, stream=s)
     s.synchronize()
     rho, ux, uy, uz = pool.fields(d, stream=s)
     pool.close()
-    return req.nu * float(ux.astype(np.float64).mean()) / req.g, ux
+    return req.permeability(ux), ux

@@ -100,14 +100,15 @@ def duct_batch(count, seed=20261203, sides=(16, 96), re_range=(10.0, 500.0), u_m
     return out
 
 
-def porous_block(side, seed, porosity=None, radius=(3.0, 8.0), max_tries=40000):
+def porous_block(side, seed, porosity=None, radius=(3.0, 8.0), max_tries=40000, x_margin=0):
     """A side^3 block of random non-overlapping spheres added one at a time (random sequential
     addition) until the solid fraction reaches 1 - porosity (porosity uniform in [0.5, 0.9] when
     not given). Returns the node mask (x fastest, nonzero = fluid), the spheres (cx, cy, cz, r) and
     the porosity reached. Sphere centres keep a margin of r from the block faces. Random sequential
     addition of non-overlapping spheres jams near a solid fraction of about 0.3-0.35, so low target
     porosities end at the jammed packing (the porosity reached is returned); the addition stops
-    after 8 batches of 256 candidates without a single accepted sphere, or after max_tries candidates."""
+    after 8 batches of 256 candidates without a single accepted sphere, or after max_tries candidates.
+    x_margin keeps the spheres that many nodes further from the x faces (room for pressure planes)."""
     rng = np.random.default_rng(seed)
     if porosity is None:
         porosity = float(rng.uniform(0.5, 0.9))
@@ -123,7 +124,9 @@ def porous_block(side, seed, porosity=None, radius=(3.0, 8.0), max_tries=40000):
     idle = 0
     while n_solid < target and tries < max_tries and idle < 8:
         r = rng.uniform(radius[0], radius[1], batch)
-        c = rng.uniform(0.0, 1.0, (batch, 3)) * (side - 1 - 2 * r)[:, None] + r[:, None]
+        lo_c = np.stack([r + x_margin, r, r], axis=1)
+        hi_c = np.stack([side - 1 - r - x_margin, side - 1 - r, side - 1 - r], axis=1)
+        c = rng.uniform(0.0, 1.0, (batch, 3)) * (hi_c - lo_c) + lo_c
         tries += batch
         accepted = 0
         for ci, ri in zip(c, r):
@@ -182,3 +185,107 @@ def cube_duct(nx=512, ny=256, nz=256, cube=32, x0=128, u_max=0.05, re=3000.0):
     g.add_box_obstacle((x0 - 0.5, y0 - 0.5, -0.5), (x0 + cube - 0.5, y0 + cube - 0.5, cube - 0.5))
     nu = u_max * cube / re
     return g, 1.0 / (3.0 * nu + 0.5), {"nu": nu, "u_max": u_max, "cube": cube, "area": float(cube * cube)}
+
+
+# D3Q27 directions in reference numbering (src/lbm/constants/D3Q27.h:42-72)
+_CX = np.array([0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1])
+_CY = np.array([0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1, 1, 1, -1, -1, 1, 1, -1, -1])
+_CZ = np.array([0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 1, 1, 1, 1, -1, -1, -1, -1])
+
+
+def sphere_link_q(points, centre, radius):
+    """q of the 26 links of each point (n, 3) against one sphere: the ray parameter t of
+    p + t c_d at which the link enters the sphere, as Sphere::getIntersection computes it
+    (geometries/Sphere/Sphere.cpp:124-169: the smaller non-negative root of |p + t c - centre|^2 =
+    r^2), kept where 0 <= t <= 1 (GridImp::calculateQs, GridImp.cpp:1561-1600); -1 elsewhere.
+    Returns (27, n)."""
+    rp = np.asarray(points, dtype=np.float64) - np.asarray(centre, dtype=np.float64)
+    q = np.full((27, rp.shape[0]), -1.0)
+    rr = (rp * rp).sum(axis=1) - float(radius) * float(radius)
+    big = np.float64(np.finfo(np.float32).max)
+    for d in range(1, 27):
+        c = np.array([_CX[d], _CY[d], _CZ[d]], dtype=np.float64)
+        dsq = float(c @ c)
+        pc = 2.0 * (rp @ c) / dsq
+        qc = rr / dsq
+        disc = 0.25 * pc * pc - qc
+        ok = disc >= 0.0
+        sq = np.sqrt(np.where(ok, disc, 0.0))
+        r1 = -0.5 * pc + sq
+        r2 = -0.5 * pc - sq
+        both_negative = (r1 < 0.0) & (r2 < 0.0)
+        r1 = np.where(r1 < 0.0, big, r1)
+        r2 = np.where(r2 < 0.0, big, r2)
+        t = np.minimum(r1, r2)
+        hit = ok & ~both_negative & (t <= 1.0) & (t >= 0.0)
+        q[d] = np.where(hit, t, -1.0)
+    return q
+
+
+def porous_block_bcs(side, seed, porosity=None, drho=3e-3, radius=(3.0, 8.0)):
+    """Config 5 as boundary-condition lists of a structured box: a side^3 porous block (spheres
+    as :func:`porous_block`, kept three nodes off the x faces) between two pressure planes.
+
+    The box is (side + 2) x side x side, periodic in y and z; its first and last x layers are solid
+    stoppers. The fluid layers x = 1 and x = side carry PressureNonEquilibriumCompressible at
+    drho = +drho/2 (outward normal M00, neighbour x = 2) and -drho/2 (P00, neighbour x = side - 1),
+    as a pressure side of the reference's grid builder sets them (Side.cpp:89-110). Every fluid node
+    with a link cut by a sphere is a NoSlipInterpolatedCompressible node with the exact q of each cut
+    link (the smallest over the spheres, GridImp.cpp:1561-1600), periodic images included.
+
+    Returns dict(shape, mask, bcs, spheres, porosity, length, drho): mask is the box's node mask
+    (nonzero = fluid, the stopper layers solid), bcs the lists for Pool.add / Box, length the
+    distance between the pressure planes (side - 1)."""
+    from . import _native as N
+    inner, spheres, phi = porous_block(side, seed, porosity=porosity, radius=radius, x_margin=3)
+    nx, ny, nz = side + 2, side, side
+    solid = np.ones((nz, ny, nx), dtype=bool)
+    solid[:, :, 1:side + 1] = inner.reshape(side, side, side) == 0
+    solid[:, :, 0] = True
+    solid[:, :, -1] = True
+    mask = (~solid).astype(np.uint8).reshape(-1)
+    keys_all, q_all = [], []
+    for (cx, cy, cz, r) in spheres:
+        for oy in (-side, 0, side):
+            for oz in (-side, 0, side):
+                c = np.array([cx + 1.0, cy + oy, cz + oz])
+                lo = np.floor(c - r - 2).astype(int)
+                hi = np.ceil(c + r + 2).astype(int)
+                if hi[1] < 0 or lo[1] >= ny or hi[2] < 0 or lo[2] >= nz:
+                    continue
+                xs = np.arange(max(lo[0], 1), min(hi[0], nx - 2) + 1)
+                ys = np.arange(max(lo[1], 0), min(hi[1], ny - 1) + 1)
+                zs = np.arange(max(lo[2], 0), min(hi[2], nz - 1) + 1)
+                Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+                X, Y, Z = X.reshape(-1), Y.reshape(-1), Z.reshape(-1)
+                d2 = (X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2
+                near = ~solid[Z, Y, X] & (d2 <= (r + 1.8) ** 2)
+                if not near.any():
+                    continue
+                pts = np.stack([X[near], Y[near], Z[near]], axis=1).astype(np.float64)
+                q = sphere_link_q(pts, c, r)
+                cut = (q >= 0.0).any(axis=0)
+                keys_all.append((X[near] + nx * (Y[near] + ny * Z[near]))[cut])
+                q_all.append(q[:, cut])
+    # per node and direction the smallest q over the spheres (uncut links stay -1)
+    if keys_all:
+        keys = np.concatenate(keys_all)
+        qs = np.concatenate(q_all, axis=1)
+        order = np.argsort(keys, kind="stable")
+        keys, qs = keys[order], np.where(qs[:, order] < 0.0, np.inf, qs[:, order])
+        k_ns, start = np.unique(keys, return_index=True)
+        q_ns = np.minimum.reduceat(qs, start, axis=1)
+        q_ns = np.where(np.isinf(q_ns), -1.0, q_ns)
+        k_ns = k_ns.astype(np.int32)
+    else:
+        k_ns, q_ns = np.zeros(0, dtype=np.int32), np.zeros((27, 0))
+    yy, zz = np.meshgrid(np.arange(ny), np.arange(nz), indexing="xy")
+    yy, zz = yy.reshape(-1), zz.reshape(-1)
+    k_in = 1 + nx * (yy + ny * zz)
+    k_out = side + nx * (yy + ny * zz)
+    pressure = (np.concatenate([k_in, k_out]).astype(np.int32),
+                np.concatenate([k_in + 1, k_out - 1]).astype(np.int32),
+                np.concatenate([np.full(k_in.size, 0.5 * drho), np.full(k_out.size, -0.5 * drho)]),
+                np.concatenate([np.full(k_in.size, N.DIR_M00), np.full(k_out.size, N.DIR_P00)]).astype(np.int32))
+    return {"shape": (nx, ny, nz), "mask": mask, "bcs": {"noslip": (k_ns, q_ns), "pressure": pressure},
+            "spheres": spheres, "porosity": phi, "length": float(side - 1), "drho": float(drho)}
