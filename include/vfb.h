@@ -388,6 +388,11 @@ int vfb_box_kernel_launches(const vfb_box *box, uint64_t *count);
 int vfb_box_set_launch_shape(vfb_box *box, int32_t blocks_per_sm, int32_t smem_kb);
 /* raw access to the population planes for checks: pointer, plane pitch (elements), parity */
 int vfb_box_populations(const vfb_box *box, void **dist, uint64_t *pitch, int32_t *is_even);
+/* the 27 population planes without their padding (plane d at d * nx*ny*nz, the storage type, as
+   stored) and the parity, out of or into the box: restart files (RestartObject::serialize /
+   deserialize). Host memory when to_host / from_host (the call then synchronises the stream). */
+int vfb_box_read_populations(vfb_box *box, void *out, int32_t to_host, int32_t *is_even, void *stream);
+int vfb_box_write_populations(vfb_box *box, const void *src, int32_t from_host, int32_t is_even, void *stream);
 
 /* ---- (2c) domain pools: batches of independent boxes in one persistent launch ---------------
    No counterpart in the reference (one level of one domain per Simulation there). A pool owns one

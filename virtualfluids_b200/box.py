@@ -179,6 +179,41 @@ class Box:
         configuration in KB to pad to; 0 = defaults). Results do not depend on it."""
         N.check(N.lib().vfb_box_set_launch_shape(self._h, int(blocks_per_sm), int(smem_kb)))
 
+    def _storage_np(self):
+        return {N.STORAGE_F64: np.float64, N.STORAGE_F32: np.float32}.get(self.storage, np.uint16)
+
+    def read_populations(self):
+        """The 27 population planes (27 * nx*ny*nz values as stored, 16-bit forms as raw uint16)
+        and the parity."""
+        out = np.empty(27 * self.n, dtype=self._storage_np())
+        ev = C.c_int32()
+        N.check(N.lib().vfb_box_read_populations(self._h, out.ctypes.data, 1, C.byref(ev), None))
+        return out, bool(ev.value)
+
+    def write_populations(self, planes, is_even=True):
+        a = np.ascontiguousarray(planes, dtype=self._storage_np()).reshape(-1)
+        if a.size != 27 * self.n:
+            raise ValueError(f"{a.size} values, {27 * self.n} expected")
+        N.check(N.lib().vfb_box_write_populations(self._h, a.ctypes.data, 1, int(bool(is_even)), None))
+
+    def save_restart(self, path):
+        """The box's populations in the layout of the reference's binary restart file (one level),
+        `path` + ".bin"; box node order."""
+        from .output import save_restart
+        save_restart(path, [self.read_populations()[0]])
+
+    def load_restart(self, path, is_even=True):
+        from .output import load_restart
+        (a,) = load_restart(path, [self._storage_np()])
+        self.write_populations(a, is_even)
+
+    def write_vtk(self, path, spacing=1.0, origin=(0.0, 0.0, 0.0)):
+        """drho and velocity of every node as a legacy VTK image (STRUCTURED_POINTS)."""
+        from .output import write_vtk_image
+        f = self.fields()
+        write_vtk_image(path, self.shape, {"drho": f["rho"], "velocity": np.stack([f["vx"], f["vy"], f["vz"]])},
+                        origin=origin, spacing=spacing)
+
     def populations(self):
         """(device pointer, plane pitch in elements, is_even) of the population array."""
         p, pitch, ev = C.c_void_p(), C.c_uint64(), C.c_int32()

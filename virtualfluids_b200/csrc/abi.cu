@@ -1700,6 +1700,39 @@ int vfb_box_set_launch_shape(vfb_box *box, int32_t blocks_per_sm, int32_t smem_k
     return VFB_OK;
 }
 
+static int box_copy_populations(vfb_box *box, void *host_or_dev, const void *src_any, bool out, int32_t on_host,
+                                void *stream)
+{
+    const size_t sb = storage_bytes(box->desc.storage);
+    const size_t row = (size_t)box->n * sb, pitch = (size_t)box->state.pitch * sb;
+    cudaStream_t s = as_stream(stream);
+    const cudaMemcpyKind kind = on_host ? (out ? cudaMemcpyDeviceToHost : cudaMemcpyHostToDevice)
+                                        : cudaMemcpyDeviceToDevice;
+    cudaError_t e = out ? cudaMemcpy2DAsync(host_or_dev, row, box->dist, pitch, row, 27, kind, s)
+                        : cudaMemcpy2DAsync(box->dist, pitch, src_any, row, row, 27, kind, s);
+    if (e == cudaSuccess && on_host)
+        e = cudaStreamSynchronize(s);
+    return cuda_status(e, "box population copy");
+}
+
+int vfb_box_read_populations(vfb_box *box, void *out, int32_t to_host, int32_t *is_even, void *stream)
+{
+    if (!box || !out || !is_even)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    *is_even = box->even ? 1 : 0;
+    return box_copy_populations(box, out, nullptr, true, to_host, stream);
+}
+
+int vfb_box_write_populations(vfb_box *box, const void *src, int32_t from_host, int32_t is_even, void *stream)
+{
+    if (!box || !src)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    const int st = box_copy_populations(box, nullptr, src, false, from_host, stream);
+    if (st == VFB_OK)
+        box->even = is_even != 0;
+    return st;
+}
+
 int vfb_box_populations(const vfb_box *box, void **dist, uint64_t *pitch, int32_t *is_even)
 {
     if (!box || !dist || !pitch || !is_even)

@@ -415,3 +415,48 @@ class Simulation:
     def populations(self, level=0):
         N.check(N.lib().vfb_synchronize(None))
         return self.levels[level].dist.double().cpu().numpy()
+
+    def _raw(self, level):
+        """The population array of a level as stored (16-bit storage as raw uint16)."""
+        t = _torch()
+        N.check(N.lib().vfb_synchronize(None))
+        d = self.levels[level].dist
+        if d.dtype in (t.float16, t.bfloat16):
+            return d.view(t.int16).cpu().numpy().view(np.uint16)
+        return d.cpu().numpy()
+
+    def write_vtk(self, path, level=0):
+        """drho, velocity and pressure of a level's fluid nodes at their positions (units of the
+        coarsest spacing), as a legacy VTK file."""
+        from .output import write_vtk_points
+        m = self.macroscopic(level)
+        f = self.levels[level].grid.fluid
+        write_vtk_points(path, self.multilevel.positions(level)[:, f],
+                         {"drho": m["rho"][f], "velocity": np.stack([m["vx"][f], m["vy"][f], m["vz"][f]]),
+                          "pressure": m["pressure"][f]}, title=f"level {level}")
+
+    def save_restart(self, path):
+        """RestartObject::serialize (binary): every level's population array, `path` + ".bin"."""
+        from .output import save_restart
+        save_restart(path, [self._raw(i) for i in range(len(self.levels))])
+
+    def load_restart(self, path, timestep=0):
+        """RestartObject::deserialize: the population arrays of every level; the coarsest level is
+        at the parity of `timestep` (even when it is even), finer levels at the even parity."""
+        from .output import load_restart
+        t = _torch()
+        dts = [self._raw(i).dtype for i in range(len(self.levels))]
+        arrs = load_restart(path, dts)
+        for i, (S, a) in enumerate(zip(self.levels, arrs)):
+            if a.size != S.dist.numel():
+                raise ValueError(f"level {i}: {a.size} values in the file, {S.dist.numel()} expected")
+            src = t.from_numpy(a.view(np.int16) if a.dtype == np.uint16 else a)
+            if S.dist.dtype in (t.float16, t.bfloat16):
+                S.dist.view(t.int16).copy_(src)
+            else:
+                S.dist.copy_(src)
+            S.level.is_even_timestep = int(timestep % 2 == 0) if i == 0 else 1
+            N.check(N.lib().vfb_simulation_use_level(self._sim, i))
+            N.check(N.lib().vfb_simulation_set_level(self._sim, C.byref(S.level), _ptr(S.fluid),
+                                                     int(S.grid.fluid.size)))
+        N.check(N.lib().vfb_simulation_use_level(self._sim, 0))
