@@ -394,6 +394,56 @@ def run_tgv_forms(args):
         print(json.dumps(line), flush=True)
 
 
+def run_list_path(args, n, omega, fields, dev):
+    """The same TGV through the drop-in path: vfb_simulation_run over the reference's layout (node
+    list with the dummy node 0, neighborX/Y/Z, planes of number_of_nodes elements), FP64. Reports
+    MLUPS and the collision kernel's algorithmic HBM throughput (CUDA events on the launching
+    stream; the driver's step is the collision kernel alone on a periodic box)."""
+    import torch
+
+    import virtualfluids_b200 as vfb
+    from virtualfluids_b200 import _native as N
+
+    out = {"path": "vfb_simulation_run (K17CompressibleNavierStokes over neighborX/Y/Z with neighbour slot tables)",
+           "kernel": "k17_list_kernel<double>"}
+    peak, peak_kind = measured_peak()
+    out["peak_source"] = peak_kind
+    # node numbering as the reference's grid builder (first node 1, planes of n^3 + 1 nodes), and
+    # aligned (first node 32, planes padded to 32 nodes)
+    for align, key in ((1, "reference_numbering"), (32, "aligned_numbering")):
+        g = vfb.ListGrid(n, n, n, periodic=(True, True, True), align=align)
+        p = vfb.Parameter()
+        p.set_viscosity_lb((1.0 / omega - 0.5) / 3.0)
+        p.configure_main_kernel("K17CompressibleNavierStokes")
+        p.storage, p.arith = N.STORAGE_F64, N.ARITH_EXACT if args.arith == "exact" else N.ARITH_FAST
+        sim = vfb.Simulation(p, g, vfb.BoundaryConditionFactory())
+        full = [np.zeros(g.number_of_nodes) for _ in range(4)]
+        for dst, a in zip(full, fields):
+            dst[g.first_node:g.first_node + nodes_of(n)] = a
+        sim.init(*full)
+        sim.run(args.warmup)
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        steps = max(args.steps, 1)
+        ev0.record()
+        sim.run(steps)           # the legacy stream, as the reference's default
+        ev1.record()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / steps
+        nodes = int(g.fluid.size)
+        achieved = BYTES_PER_NODE["f64"] * nodes / (ms / 1e3) / 1e9
+        sim.close()
+        del sim
+        torch.cuda.empty_cache()
+        out[key] = {"mlups": round(nodes / (ms / 1e3) / 1e6, 1), "ms_per_step": round(ms, 4),
+                    "hbm_achieved_gbs": round(achieved, 1), "frac": round(achieved / peak, 4)}
+    return out
+
+
+def nodes_of(n):
+    return n * n * n
+
+
 def run_serving(args):
     """Config 5: a Poisson stream of porous-block solves served by continuous batching in one domain
     pool whose arena is the HBM budget. Offered loads are fractions of the measured capacity (node
@@ -479,6 +529,7 @@ def main():
     ap.add_argument("--n", type=int, default=N_SIDE)
     ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-list", action="store_true", help="skip the reference-layout (list) measurement")
     ap.add_argument("--arith", default="fast", choices=["fast", "exact"],
                     help="exact: every operation rounded as the reference's host build (bitwise oracle parity)")
     ap.add_argument("--kernel", default="auto", choices=["auto", "direct", "tma", "async"])
@@ -637,6 +688,11 @@ def main():
             del b
             torch.cuda.empty_cache()
 
+    # ---- the reference layout: the drop-in step driver over neighborX/Y/Z lists (device resident) ----
+    ref_layout = None
+    if not args.no_list:
+        ref_layout = run_list_path(args, n, omega, fields, dev)
+
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline()
@@ -659,6 +715,8 @@ def main():
             "forms": forms,
             "kinetic_energy": {"first": float(e_host[1]), "last": float(e_host[-1])},
         }
+        if ref_layout:
+            line["reference_layout"] = ref_layout
         if cb:
             line["cpu_baseline"] = cb
         print(json.dumps(line), flush=True)

@@ -281,11 +281,16 @@ int vfb_simulation_destroy(vfb_simulation *sim);
    (Parameter::getParD(level)) */
 int vfb_simulation_use_level(vfb_simulation *sim, int32_t level);
 int vfb_simulation_number_of_levels(const vfb_simulation *sim, int32_t *number_of_levels);
-/* Neighbour slot tables (default on): vfb_simulation_set_level builds, in library-owned device
-   memory (28 bytes per fluid node), the seven +1 neighbours of every fluid node, which the driver's
-   collision then reads with one coalesced load each instead of the neighborX/Y/Z chain; same
-   results. Set the level again after changing its neighbour arrays or fluid-node list. 0 frees them. */
-int vfb_simulation_set_neighbor_tables(vfb_simulation *sim, int32_t enable);
+/* Neighbour slot tables: vfb_simulation_set_level builds, in library-owned device memory (32 bytes
+   per fluid node), each fluid node and its seven +1 neighbours, and the driver's collision reads
+   them instead of walking the neighborX/Y/Z chain, with the same results. mode 1 (default): one
+   coalesced load per slot; 2: the tables staged in shared memory by bulk asynchronous copies two
+   tiles ahead (persistent warps); 0: no tables (the chain). Set the level again after changing its
+   neighbour arrays or fluid-node list. */
+int vfb_simulation_set_neighbor_tables(vfb_simulation *sim, int32_t mode);
+/* synchronises the stream and reads the status word the staged collision sets when a bounded wait
+   for its copies gave up (0 = fine); returns VFB_ERR_CUDA when it is nonzero */
+int vfb_simulation_status(vfb_simulation *sim, int32_t *device_status, void *stream);
 /* the selected level's description, copied; device memory stays caller-owned; level->level must be
    the selected level (forces are scaled by 2^-level) */
 int vfb_simulation_set_level(vfb_simulation *sim, const vfb_level *level, const uint32_t *fluid_node_indices,

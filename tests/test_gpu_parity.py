@@ -4,6 +4,8 @@ Tolerances: the exact arithmetic variant (no FMA contraction) must reproduce the
 bit; the default variant (FMA) must stay within 1e-12 relative L-inf in density and velocity
 (relative to the field's maximum magnitude), the bar of the FP64 form.
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -280,7 +282,8 @@ def test_box_inlet_perturbation_is_seeded(cuda):
 
 @pytest.mark.parametrize("storage", [N.STORAGE_F64, N.STORAGE_F16], ids=["f64", "f16"])
 def test_neighbor_slot_tables_change_nothing(cuda, storage):
-    """The driver's neighbour slot tables give the same bits as the neighborX/Y/Z chain."""
+    """The driver's neighbour slot tables, loaded directly or staged by bulk copies, give the same bits
+    as the neighborX/Y/Z chain."""
     g = ListGrid(12, 10, 9)
     for side in ("MX", "PX", "MY", "PY", "MZ"):
         g.add_side(side, "noslip")
@@ -289,10 +292,13 @@ def test_neighbor_slot_tables_change_nothing(cuda, storage):
     bcf.set_velocity_boundary_condition(BCF.VelocityBC.VelocityInterpolatedCompressible)
     bcf.set_no_slip_boundary_condition(BCF.NoSlipBC.NoSlipInterpolatedCompressible)
     out = []
-    for tables in (False, True):
+    for tables in (0, 1, 2):
         sim = Simulation(make_para(1.8, storage), g, bcf, neighbor_tables=tables)
         sim.init(*smooth_fields(g, 5))
         sim.run(7)
         out.append(sim.populations())
+        st = C.c_int32()
+        N.check(N.lib().vfb_simulation_status(sim._sim, C.byref(st), None))
+        assert st.value == 0
         sim.close()
-    assert np.array_equal(out[0], out[1])
+    assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])

@@ -183,6 +183,7 @@ SIGNATURES = {
     "vfb_box_read_populations": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.c_void_p]),
     "vfb_box_write_populations": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]),
     "vfb_simulation_set_neighbor_tables": (C.c_int, [C.c_void_p, C.c_int32]),
+    "vfb_simulation_status": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.c_void_p]),
     "vfb_simulation_number_of_levels": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "vfb_simulation_set_scaling_factory": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "vfb_simulation_set_interpolation_cells": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(InterpolationCells),

@@ -149,10 +149,12 @@ class Box:
     @classmethod
     def from_grid(cls, grid, omega, bc_factory, storage="f64", arith="fast", forces=(0.0, 0.0, 0.0)):
         """The structured-box form of a ListGrid level: the box spans the grid with its stopper shell
-        (box node k = list node k + 1), the mask marks the fluid nodes, and the grid's BC lists
-        become box BC lists with the factory's kernels. It computes what the list form computes."""
+        (list node k = box node k + grid.first_node), the mask marks the fluid nodes, and the grid's
+        BC lists become box BC lists with the factory's kernels. It computes what the list form
+        computes."""
         Dx, Dy, Dz = grid.dims
-        mask = (grid.geo[1:] == N.GEO_FLUID).astype(np.uint8)
+        f0 = grid.first_node
+        mask = (grid.geo[f0:f0 + Dx * Dy * Dz] == N.GEO_FLUID).astype(np.uint8)
         box = cls(Dx, Dy, Dz, omega, periodic=grid.periodic, storage=storage, arith=arith, forces=forces, mask=mask)
         for kind, variant in (("velocity", bc_factory.velocity), ("noslip", bc_factory.noslip),
                               ("geometry", bc_factory.geometry)):
@@ -160,11 +162,11 @@ class Box:
             if m is None:
                 continue
             k, q, vel = m
-            box.set_bc(kind, k.astype(np.int64) - 1, q, int(variant), velocity=vel if kind == "velocity" else None)
+            box.set_bc(kind, k.astype(np.int64) - f0, q, int(variant), velocity=vel if kind == "velocity" else None)
         from .grid import SIDE_DIR
         for b in grid.bcs:
             if b.kind == "pressure":
-                box.add_pressure_bc(b.k.astype(np.int64) - 1, b.k_neighbor.astype(np.int64) - 1, b.rho,
+                box.add_pressure_bc(b.k.astype(np.int64) - f0, b.k_neighbor.astype(np.int64) - f0, b.rho,
                                     SIDE_DIR[b.side], variant=int(bc_factory.pressure))
         return box
 

@@ -283,15 +283,15 @@ const char *vfb_kernel_name(int index)
 // (1) reference-layout entry points
 // ---------------------------------------------------------------------------------------------
 static int run_k17(const vfb_level *level, const uint32_t *idx, uint32_t size, int32_t tmpl, const uint32_t *slots,
-                   void *stream);
+                   uint64_t slots_stride, void *stream);
 
 int vfb_k17_run_on_indices(const vfb_level *level, const uint32_t *idx, uint32_t size, int32_t tmpl, void *stream)
 {
-    return run_k17(level, idx, size, tmpl, nullptr, stream);
+    return run_k17(level, idx, size, tmpl, nullptr, 0, stream);
 }
 
 static int run_k17(const vfb_level *level, const uint32_t *idx, uint32_t size, int32_t tmpl, const uint32_t *slots,
-                   void *stream)
+                   uint64_t slots_stride, void *stream)
 {
     int st = check_level(level);
     if (st)
@@ -307,7 +307,7 @@ static int run_k17(const vfb_level *level, const uint32_t *idx, uint32_t size, i
     if (bf && (!level->body_force_x || !level->body_force_y || !level->body_force_z))
         return fail(VFB_ERR_INVALID_ARGUMENT, "body force arrays are NULL");
     const cudaError_t e = VFB_DISPATCH(level->storage, level->arith,
-                                       LA::k17_list(level, idx, size, tmpl, as_stream(stream), slots));
+                                       LA::k17_list(level, idx, size, tmpl, as_stream(stream), slots, slots_stride));
     return cuda_status(e, "K17CompressibleNavierStokes launch");
 }
 
@@ -655,15 +655,18 @@ struct SimLevel {
     vfb_interpolation_cells fc{}, cf{};
     vfb_interpolation_cell_neighbor fc_offsets{}, cf_offsets{};
     // neighbour slot table of the fluid-node list (library-owned, built by set_level)
-    uint32_t *slots = nullptr;
+    uint32_t *slots = nullptr;        // 8 arrays of slots_stride entries, then the kernels' status word
+    uint64_t slots_stride = 0;
     size_t slots_nodes = 0;
     const void *slots_key[4] = { nullptr, nullptr, nullptr, nullptr };
 
+    int *status() const { return reinterpret_cast<int *>(slots + 8 * slots_stride); }
     void free_slots()
     {
         if (slots)
             cudaFree(slots);
         slots = nullptr;
+        slots_stride = 0;
         slots_nodes = 0;
         for (auto &p : slots_key)
             p = nullptr;
@@ -684,7 +687,7 @@ struct SimLevel {
             geometry = o.geometry; geometry_fn = o.geometry_fn; geometry_set = o.geometry_set;
             drag_work = o.drag_work; drag_history = o.drag_history; drag_history_len = o.drag_history_len;
             drag_steps = o.drag_steps; fc = o.fc; cf = o.cf; fc_offsets = o.fc_offsets; cf_offsets = o.cf_offsets;
-            slots = o.slots; slots_nodes = o.slots_nodes;
+            slots = o.slots; slots_stride = o.slots_stride; slots_nodes = o.slots_nodes;
             for (int i = 0; i < 4; ++i)
                 slots_key[i] = o.slots_key[i];
             o.slots = nullptr;
@@ -699,7 +702,7 @@ struct vfb_simulation {
     int kernel_id = 0;
     std::vector<SimLevel> levels = std::vector<SimLevel>(1);
     int32_t cursor = 0;               // the level the setters configure
-    bool neighbor_tables = true;      // build slot tables for the collision
+    int32_t neighbor_tables = 1;      // 0 chain, 1 slot tables, 2 slot tables staged by bulk copies
     bool scaling_set = false;         // GridScalingFactory given
     vfb_scaling_fn scale_fc = nullptr;
     vfb_scaling_fn scale_cf = nullptr;
@@ -712,7 +715,7 @@ static SimLevel &current(vfb_simulation *sim) { return sim->levels[(size_t)sim->
 // (the order of the kernels' ListIndices: slot bit 0 = +x, bit 1 = +y, bit 2 = +z)
 __global__ void list_slots_kernel(const uint32_t *__restrict__ idx, uint32_t n_idx, const uint32_t *__restrict__ nbx,
                                   const uint32_t *__restrict__ nby, const uint32_t *__restrict__ nbz,
-                                  uint32_t *__restrict__ slots)
+                                  uint32_t *__restrict__ slots, uint64_t stride)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_idx)
@@ -720,10 +723,10 @@ __global__ void list_slots_kernel(const uint32_t *__restrict__ idx, uint32_t n_i
     const uint32_t k = __ldg(idx + i);
     const uint32_t kx = __ldg(nbx + k), ky = __ldg(nby + k), kz = __ldg(nbz + k);
     const uint32_t kxy = __ldg(nby + kx);
-    const uint32_t out[7] = { kx, ky, kxy, kz, __ldg(nbz + kx), __ldg(nbz + ky), __ldg(nbz + kxy) };
+    const uint32_t out[8] = { k, kx, ky, kxy, kz, __ldg(nbz + kx), __ldg(nbz + ky), __ldg(nbz + kxy) };
 #pragma unroll
-    for (int j = 0; j < 7; ++j)
-        slots[(size_t)j * n_idx + i] = out[j];
+    for (int j = 0; j < 8; ++j)
+        slots[(size_t)j * stride + i] = out[j];
 }
 
 // The slot table of a level (the seven +1 neighbours of each fluid node, one array per slot),
@@ -739,15 +742,22 @@ static int build_slots(vfb_simulation *sim, SimLevel &S)
     if (S.slots && S.slots_nodes == S.n_fluid && std::equal(key, key + 4, S.slots_key))
         return VFB_OK;
     S.free_slots();
-    if (cudaMalloc(&S.slots, (size_t)7 * S.n_fluid * sizeof(uint32_t)) != cudaSuccess) {
+    // whole 32-entry tiles (the staged kernel copies 128-byte rows), padding entries = node 0
+    const uint64_t stride = ((uint64_t)S.n_fluid + 31) / 32 * 32;
+    const size_t bytes = (size_t)8 * stride * sizeof(uint32_t) + 16;
+    if (cudaMalloc(&S.slots, bytes) != cudaSuccess) {
         cudaGetLastError();
         S.slots = nullptr;
         return fail(VFB_ERR_OUT_OF_MEMORY, "no device memory for the neighbour slot table");
     }
+    S.slots_stride = stride;
+    cudaError_t e = cudaMemset(S.slots, 0, bytes);
     const unsigned B = 256, G = (unsigned)((S.n_fluid + B - 1) / B);
-    list_slots_kernel<<<G, B>>>(S.fluid, S.n_fluid, S.level.neighbor_x, S.level.neighbor_y, S.level.neighbor_z,
-                                S.slots);
-    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+        list_slots_kernel<<<G, B>>>(S.fluid, S.n_fluid, S.level.neighbor_x, S.level.neighbor_y, S.level.neighbor_z,
+                                    S.slots, stride);
+    if (e == cudaSuccess)
+        e = cudaGetLastError();
     if (e == cudaSuccess)
         e = cudaDeviceSynchronize();   // visible to every stream the level is later run on
     if (e != cudaSuccess) {
@@ -798,7 +808,9 @@ int vfb_simulation_set_neighbor_tables(vfb_simulation *sim, int32_t enable)
 {
     if (!sim)
         return fail(VFB_ERR_INVALID_ARGUMENT, "NULL simulation");
-    sim->neighbor_tables = enable != 0;
+    if (enable < 0 || enable > 2)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "neighbour tables: 0 off, 1 direct loads, 2 staged copies");
+    sim->neighbor_tables = enable;
     for (SimLevel &S : sim->levels) {
         if (!S.has_level)
             continue;
@@ -807,6 +819,25 @@ int vfb_simulation_set_neighbor_tables(vfb_simulation *sim, int32_t enable)
             return st;
     }
     return VFB_OK;
+}
+
+int vfb_simulation_status(vfb_simulation *sim, int32_t *device_status, void *stream)
+{
+    if (!sim || !device_status)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    cudaError_t e = cudaStreamSynchronize(as_stream(stream));
+    int32_t worst = 0;
+    for (SimLevel &S : sim->levels) {
+        if (!S.slots || e != cudaSuccess)
+            continue;
+        int v = 0;
+        e = cudaMemcpy(&v, S.status(), sizeof(int), cudaMemcpyDeviceToHost);
+        worst = std::max(worst, (int32_t)v);
+    }
+    *device_status = worst;
+    if (e != cudaSuccess)
+        return cuda_status(e, "simulation status");
+    return worst ? fail(VFB_ERR_CUDA, "a kernel gave up waiting for its staged copies") : VFB_OK;
 }
 
 int vfb_simulation_number_of_levels(const vfb_simulation *sim, int32_t *n)
@@ -1036,10 +1067,18 @@ static int run_geometry_pre(SimLevel &S, void *stream)
 
 // one time step of one level: collision, post-collision BCs (velocity, no-slip, geometry), parity
 // toggle, pre-collision BCs (pressure) (UpdateGrid27.cpp:66-84)
-static int step_level(SimLevel &S, void *stream)
+static int step_level(const vfb_simulation *sim, SimLevel &S, void *stream)
 {
     vfb_level &L = S.level;
-    int st = run_k17(&L, S.fluid, S.n_fluid, VFB_COLLISION_DEFAULT, S.slots, stream);
+    int st;
+    if (S.slots && sim->neighbor_tables == 2) {
+        const cudaError_t e = VFB_DISPATCH(L.storage, L.arith,
+                                           LA::k17_list_staged(&L, S.slots, S.slots_stride, S.n_fluid, S.status(),
+                                                               as_stream(stream)));
+        st = cuda_status(e, "K17CompressibleNavierStokes launch");
+    } else {
+        st = run_k17(&L, S.fluid, S.n_fluid, VFB_COLLISION_DEFAULT, S.slots, S.slots_stride, stream);
+    }
     if (st)
         return st;
     if (S.velocity_fn && S.velocity.number_of_bc_nodes) {
@@ -1083,7 +1122,7 @@ static int update_level(vfb_simulation *sim, size_t l, void *stream)
             return st;
     }
     SimLevel &S = sim->levels[l];
-    if ((st = step_level(S, stream)) != VFB_OK)
+    if ((st = step_level(sim, S, stream)) != VFB_OK)
         return st;
     if (has_finer) {
         SimLevel &F = sim->levels[l + 1];

@@ -32,7 +32,8 @@ struct ListCollideArgs {
     const uint32_t *nbx, *nby, *nbz;
     const uint32_t *idx;        // fluid node indices
     uint32_t n_idx;
-    const uint32_t *slots;      // optional: the seven +1 neighbour nodes of idx[i] at [(j - 1) n_idx + i]
+    const uint32_t *slots;      // optional slot table: node j (0 = idx[i], then the seven +1
+    uint64_t slots_stride;      //   neighbours) of entry i at slots[j * slots_stride + i]
     K17Rates<C> rates;
     C fx, fy, fz;               // forces * 1/2 * 2^-level (RunCollision.cuh:112-114)
     C force0, force1, force2;   // forces, for the body-force variant
@@ -190,11 +191,11 @@ __global__ void __launch_bounds__(128) k17_list_kernel(ListCollideArgs<typename 
     }
     uint32_t nodes[8];
     if (a.slots) {
-        // neighbour table built once per level: one coalesced load per slot, no dependent chain
+        // slot table built once per level: one coalesced load per slot, no dependent chain
         nodes[0] = k;
 #pragma unroll
         for (int j = 1; j < 8; ++j)
-            nodes[j] = __ldg(a.slots + (size_t)(j - 1) * a.n_idx + i);
+            nodes[j] = __ldg(a.slots + (size_t)j * a.slots_stride + i);
     } else {
         list_nodes(k, a.nbx, a.nby, a.nbz, nodes);
     }
@@ -210,6 +211,98 @@ __global__ void __launch_bounds__(128) k17_list_kernel(ListCollideArgs<typename 
         a.rho[k] = drho;
     }
     scatter_post<S, EVEN>(base, a.n, nodes, f);
+}
+
+// ---------------------------------------------------------------------------------------------
+// The same collision over the reference layout with the slot table staged in shared memory: every
+// warp walks tiles of 32 list entries and keeps the eight node indices of its next two tiles in
+// flight as bulk asynchronous copies (TMA, one 128-byte copy per slot array, counted on a per-warp
+// mbarrier), so the population loads of a tile never wait for its indices. The table's arrays
+// have a stride that is a multiple of 32 entries (16-byte aligned tiles); entries past n_idx are
+// read but not computed. Waits are bounded: a copy that never lands sets *status and ends the warp.
+// ---------------------------------------------------------------------------------------------
+struct ListTile {
+    static constexpr int N = 32;                  // entries per warp tile
+    static constexpr int WARPS = 4;
+    static constexpr int STAGES = 2;
+    static constexpr uint32_t STAGE_WORDS = 8u * N;
+    static constexpr size_t SMEM = WARPS * (STAGES * STAGE_WORDS * sizeof(uint32_t) + STAGES * sizeof(uint64_t));
+};
+
+__device__ __forceinline__ void list_issue_tile(const uint32_t *slots, uint64_t stride, int64_t t, uint32_t *stage,
+                                                uint64_t *bar, int lane)
+{
+    if (lane == 0)
+        mbar_arrive_expect_tx(bar, 8u * ListTile::N * (uint32_t)sizeof(uint32_t));
+    __syncwarp();
+    if (lane < 8)
+        bulk_copy_g2s(stage + lane * ListTile::N, slots + (uint64_t)lane * stride + (uint64_t)t * ListTile::N,
+                      ListTile::N * (uint32_t)sizeof(uint32_t), bar);
+}
+
+template <class S, bool EXACT, bool EVEN>
+__global__ void __launch_bounds__(128) k17_list_staged_kernel(ListCollideArgs<typename Codec<S>::compute> a, int *status)
+{
+    using C = typename Codec<S>::compute;
+    using T = ListTile;
+    __shared__ __align__(128) uint32_t tiles[T::WARPS][T::STAGES][T::STAGE_WORDS];
+    __shared__ __align__(8) uint64_t bars[T::WARPS][T::STAGES];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint64_t *bar = bars[warp];
+    const int64_t ntiles = ((int64_t)a.n_idx + T::N - 1) / T::N;
+    const int64_t first = (int64_t)blockIdx.x * T::WARPS + warp;
+    const int64_t stride = (int64_t)gridDim.x * T::WARPS;
+    if (lane == 0) {
+        for (int s = 0; s < T::STAGES; ++s)
+            mbar_init(&bar[s], 1);
+        fence_barrier_init();
+    }
+    __syncwarp();
+    for (int s = 0; s < T::STAGES; ++s) {
+        const int64_t t = first + s * stride;
+        if (t < ntiles)
+            list_issue_tile(a.slots, a.slots_stride, t, tiles[warp][s], &bar[s], lane);
+    }
+    S *base = static_cast<S *>(a.dist);
+    uint32_t parity = 0;
+    bool failed = false;
+    int it = 0;
+    for (int64_t t = first; t < ntiles; t += stride, ++it) {
+        const int s = it & 1;
+        const bool ok = mbar_wait(&bar[s], (parity >> s) & 1u);
+        if (__any_sync(0xffffffffu, !ok)) {
+            failed = true;
+            break;
+        }
+        parity ^= 1u << s;
+        const uint32_t *tile = tiles[warp][s];
+        uint32_t nodes[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            nodes[j] = tile[j * T::N + lane];
+        // the warp is done reading the stage: order the reads before the next copies into it
+        fence_proxy_async_smem();
+        __syncwarp();
+        const int64_t tn = t + (int64_t)T::STAGES * stride;
+        if (tn < ntiles)
+            list_issue_tile(a.slots, a.slots_stride, tn, tiles[warp][s], &bar[s], lane);
+        if ((uint64_t)t * T::N + lane < a.n_idx) {
+            C f[27];
+            gather_pre<S, EVEN>(base, a.n, nodes, f);
+            C drho, vx, vy, vz;
+            collide<C, EXACT>(f, a.rates, a.fx, a.fy, a.fz, drho, vx, vy, vz);
+            scatter_post<S, EVEN>(base, a.n, nodes, f);
+        }
+    }
+    if (failed) {
+        if (lane == 0) {
+            atomicExch(status, (int)kDevWaitTimeout);
+            // let copies still in flight land before the block's shared memory is released
+            for (int s = 0; s < T::STAGES; ++s)
+                mbar_wait(&bar[s], (parity >> s) & 1u, 1u << 16);
+        }
+        __syncwarp();
+    }
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -61,7 +61,9 @@ struct PoolDomainSpec {
     template <class S>                                                                                               \
     struct Launchers {                                                                                               \
         static cudaError_t k17_list(const vfb_level *L, const uint32_t *idx, uint32_t n, int tmpl, cudaStream_t s,   \
-                                    const uint32_t *slots = nullptr);                                        \
+                                    const uint32_t *slots = nullptr, uint64_t slots_stride = 0);             \
+        static cudaError_t k17_list_staged(const vfb_level *L, const uint32_t *slots, uint64_t slots_stride,       \
+                                           uint32_t n, int *status, cudaStream_t s);                               \
         static cudaError_t bc(const vfb_level *L, const vfb_bc *bc, int kind, cudaStream_t s,                        \
                               const NodeAddr *box = nullptr);                                                        \
         static cudaError_t pressure(const vfb_level *L, const vfb_directional_bc *bc, cudaStream_t s,                \

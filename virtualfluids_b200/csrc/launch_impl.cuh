@@ -36,7 +36,7 @@ C force_factor(int level)
 
 template <class S>
 cudaError_t Launchers<S>::k17_list(const vfb_level *L, const uint32_t *idx, uint32_t n, int tmpl, cudaStream_t s,
-                                   const uint32_t *slots)
+                                   const uint32_t *slots, uint64_t slots_stride)
 {
     using C = typename Codec<S>::compute;
     if (n == 0)
@@ -50,6 +50,7 @@ cudaError_t Launchers<S>::k17_list(const vfb_level *L, const uint32_t *idx, uint
     a.idx = idx;
     a.n_idx = n;
     a.slots = slots;
+    a.slots_stride = slots_stride;
     a.rates = rates_of<C>(L->omega, L->quadric_limiters);
     const C ff = force_factor<C>(L->level);
     a.fx = (C)L->forces[0] * C(0.5) * ff;
@@ -83,6 +84,43 @@ cudaError_t Launchers<S>::k17_list(const vfb_level *L, const uint32_t *idx, uint
         else VFB_K17L(false, false, false);
     }
 #undef VFB_K17L
+    return cudaGetLastError();
+}
+
+// the default collision template over a staged slot table: persistent warps, as many blocks as
+// are resident on the device
+template <class S>
+cudaError_t Launchers<S>::k17_list_staged(const vfb_level *L, const uint32_t *slots, uint64_t slots_stride, uint32_t n,
+                                          int *status, cudaStream_t s)
+{
+    using C = typename Codec<S>::compute;
+    if (n == 0)
+        return cudaSuccess;
+    ListCollideArgs<C> a{};
+    a.dist = L->distributions;
+    a.n = L->number_of_nodes;
+    a.n_idx = n;
+    a.slots = slots;
+    a.slots_stride = slots_stride;
+    a.rates = rates_of<C>(L->omega, L->quadric_limiters);
+    const C ff = force_factor<C>(L->level);
+    a.fx = (C)L->forces[0] * C(0.5) * ff;
+    a.fy = (C)L->forces[1] * C(0.5) * ff;
+    a.fz = (C)L->forces[2] * C(0.5) * ff;
+    const bool even = L->is_even_timestep != 0;
+    const void *fn = even ? reinterpret_cast<const void *>(k17_list_staged_kernel<S, VFB_EXACT, true>)
+                          : reinterpret_cast<const void *>(k17_list_staged_kernel<S, VFB_EXACT, false>);
+    int dev = 0, sms = 1, occ = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 128, 0);
+    if (e != cudaSuccess)
+        return e;
+    const int64_t tiles = ((int64_t)n + ListTile::N - 1) / ListTile::N;
+    const int64_t want = (tiles + ListTile::WARPS - 1) / ListTile::WARPS;
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)std::max(occ, 1) * sms));
+    if (even) k17_list_staged_kernel<S, VFB_EXACT, true><<<grid, 128, 0, s>>>(a, status);
+    else k17_list_staged_kernel<S, VFB_EXACT, false><<<grid, 128, 0, s>>>(a, status);
     return cudaGetLastError();
 }
 

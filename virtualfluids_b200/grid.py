@@ -4,7 +4,10 @@ A box of fluid nodes is laid out as the reference's GridGenerator lays out a uni
 (src/gpu/GridGenerator/grid/GridImp.cpp):
 
 * sparse node list in x-fastest order, shifted by one so that node 0 is the dummy sink that
-  every missing neighbour points to (GridImp.cpp:974, getNodeValues :2146-2185);
+  every missing neighbour points to (GridImp.cpp:974, getNodeValues :2146-2185); with align > 1
+  the grid starts at node `align` instead and the node count is padded to a multiple of it (the
+  unused nodes are solid and point nowhere), so every direction plane and every x-row of a box
+  whose row length is a multiple of `align` starts on an aligned boundary;
 * a one-node layer of stopper nodes around the fluid on every non-periodic side; stoppers are
   in the node list but never collided (geo GEO_SOLID);
 * neighborX/Y/Z[k] = the node at +1 in x/y/z, wrapped on periodic axes (setNeighborIndices
@@ -61,25 +64,31 @@ class ListGrid:
     fluid: np.ndarray | None = None         # uint32 fluid node indices
     coords: np.ndarray | None = None        # int64 [3, n] fluid-box coordinates (shell at -1 / n)
     bcs: list = field(default_factory=list)
+    align: int = 1                          # > 1: grid nodes start at index `align`, planes padded to it
 
     def __post_init__(self):
         self.shell = tuple(0 if p else 1 for p in self.periodic)
         self.dims = (self.nx + 2 * self.shell[0], self.ny + 2 * self.shell[1], self.nz + 2 * self.shell[2])
         Dx, Dy, Dz = self.dims
         n_grid = Dx * Dy * Dz
-        self.number_of_nodes = n_grid + 1
+        # node 0 is the dummy; with align > 1 the unused nodes 1 .. align - 1 put the grid's first
+        # node, and the padded node count every direction plane, on a multiple of `align` nodes
+        a0 = int(self.align)
+        self.first_node = a0 if a0 > 1 else 1
+        self.number_of_nodes = (self.first_node + n_grid + a0 - 1) // a0 * a0 if a0 > 1 else n_grid + 1
+        g0, g1 = self.first_node, self.first_node + n_grid
         i = np.arange(n_grid, dtype=np.int64)
         gx, gy, gz = i % Dx, (i // Dx) % Dy, i // (Dx * Dy)
         # coordinates in fluid-box units: fluid nodes 0..n-1, shell at -1 and n
-        coords = np.zeros((3, self.number_of_nodes), dtype=np.int64)
-        coords[0, 1:] = gx - self.shell[0]
-        coords[1, 1:] = gy - self.shell[1]
-        coords[2, 1:] = gz - self.shell[2]
-        coords[:, 0] = -(10 ** 9)
+        coords = np.full((3, self.number_of_nodes), -(10 ** 9), dtype=np.int64)
+        coords[0, g0:g1] = gx - self.shell[0]
+        coords[1, g0:g1] = gy - self.shell[1]
+        coords[2, g0:g1] = gz - self.shell[2]
         self.coords = coords
         fluid_mask = np.zeros(self.number_of_nodes, dtype=bool)
-        fluid_mask[1:] = ((coords[0, 1:] >= 0) & (coords[0, 1:] < self.nx) & (coords[1, 1:] >= 0) & (coords[1, 1:] < self.ny)
-                          & (coords[2, 1:] >= 0) & (coords[2, 1:] < self.nz))
+        c = coords[:, g0:g1]
+        fluid_mask[g0:g1] = ((c[0] >= 0) & (c[0] < self.nx) & (c[1] >= 0) & (c[1] < self.ny)
+                             & (c[2] >= 0) & (c[2] < self.nz))
         self.geo = np.where(fluid_mask, N.GEO_FLUID, N.GEO_SOLID).astype(np.uint32)
         self.fluid = np.nonzero(fluid_mask)[0].astype(np.uint32)
         nb = np.zeros((3, self.number_of_nodes), dtype=np.uint32)
@@ -93,8 +102,8 @@ class ListGrid:
                 ok = nxt < self.dims[a]
             comp = list(g)
             comp[a] = np.where(ok, nxt, 0)
-            idx = comp[0] + Dx * (comp[1] + Dy * comp[2]) + 1
-            nb[a, 1:] = np.where(ok, idx, 0).astype(np.uint32)
+            idx = comp[0] + Dx * (comp[1] + Dy * comp[2]) + g0
+            nb[a, g0:g1] = np.where(ok, idx, 0).astype(np.uint32)
         self.neighbor = nb
         self._bc_sides_set = []
 
@@ -105,7 +114,7 @@ class ListGrid:
         gx = np.asarray(x) + self.shell[0]
         gy = np.asarray(y) + self.shell[1]
         gz = np.asarray(z) + self.shell[2]
-        return (gx + Dx * (gy + Dy * gz) + 1).astype(np.int64)
+        return (gx + Dx * (gy + Dy * gz) + self.first_node).astype(np.int64)
 
     def is_stopper(self, x, y, z):
         inside = ((x >= 0) & (x < self.nx) & (y >= 0) & (y < self.ny) & (z >= 0) & (z < self.nz))

@@ -284,7 +284,8 @@ class Simulation:
     grid is a :class:`ListGrid` (one level) or a :class:`MultiLevelGrid`; with more than one level
     the scaling factory (GridScalingFactory) chooses the interpolation between them, as the
     reference's ``Simulation(para, gridBuilder, bcFactory, scalingFactory)``. neighbor_tables selects
-    the collision's neighbour slot tables (``vfb_simulation_set_neighbor_tables``). The attributes
+    the collision's neighbour slot tables (``vfb_simulation_set_neighbor_tables``: 0 none, 1 direct
+    loads, 2 staged by bulk copies; True = 1). The attributes
     ``grid``, ``level``, ``dist``, ``rho`` ... are those of the coarsest level; ``levels`` holds all."""
 
     def __init__(self, para: Parameter, grid, bc_factory: BoundaryConditionFactory,
@@ -303,7 +304,7 @@ class Simulation:
         sim = C.c_void_p()
         N.check(N.lib().vfb_simulation_create(para.main_kernel.encode(), C.byref(sim)))
         self._sim = sim
-        N.check(N.lib().vfb_simulation_set_neighbor_tables(sim, int(bool(neighbor_tables))))
+        N.check(N.lib().vfb_simulation_set_neighbor_tables(sim, int(neighbor_tables)))
         for i, S in enumerate(self.levels):
             N.check(N.lib().vfb_simulation_use_level(sim, i))
             N.check(N.lib().vfb_simulation_set_level(sim, C.byref(S.level), _ptr(S.fluid), int(S.grid.fluid.size)))
