@@ -1524,9 +1524,11 @@ int vfb_box_status(vfb_box *box, int32_t *device_status, void *stream)
 
 int vfb_box_set_kernel_variant(vfb_box *box, int32_t variant)
 {
-    if (!box || variant < 0 || variant > 3)
-        return fail(VFB_ERR_INVALID_ARGUMENT,
-                    "variant must be 0 (choose), 1 (direct loads), 2 (TMA-staged) or 3 (per-thread async copies)");
+    if (!box || variant < 0 || variant > 4)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "variant must be 0 (choose), 1 (direct loads), 2 (TMA-staged), "
+                                              "3 (per-thread async copies) or 4 (packed FP32x2 pairs)");
+    if (variant == 4 && (box->desc.storage == VFB_STORAGE_F64 || box->desc.arith == VFB_ARITH_EXACT))
+        return fail(VFB_ERR_UNSUPPORTED, "packed FP32x2 pairs: FP32 arithmetic (F32, F16, BF16 storage), FMA variant");
     if (variant == 3 && box->desc.storage > VFB_STORAGE_F32)
         return fail(VFB_ERR_UNSUPPORTED, "per-thread async copies move 4 or 8 bytes: F64 and F32 storage only");
     if (variant == 2 && box->desc.nx % 32 != 0)

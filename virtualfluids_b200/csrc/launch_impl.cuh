@@ -2,6 +2,7 @@
 // per-storage translation units, which explicitly instantiate one storage type each.
 #pragma once
 #include <algorithm>
+#include <type_traits>
 #include <cstring>
 
 #include "kernels.cuh"
@@ -598,6 +599,29 @@ cudaError_t Launchers<S>::box_collide(const BoxState &b, bool even, double *part
             else VFB_K17A(false, false, false);
         }
 #undef VFB_K17A
+        }
+    }
+    if constexpr (std::is_same<C, float>::value && !VFB_EXACT) {
+        if (b.variant == 4) {
+            // two rows per block row of the grid, packed FP32x2 arithmetic
+            const int bx = box_block_x(b.nx);
+            const dim3 G((unsigned)((b.nx + bx - 1) / bx), (unsigned)((b.ny + 1) / 2), (unsigned)b.nz), B(bx);
+            if (n_partials)
+                *n_partials = (uint64_t)G.x * G.y * G.z * (B.x / 32);
+#define VFB_K17P(E, M, N) k17_box_pair_kernel<S, E, M, N><<<G, B, 0, s>>>(a)
+            if (even) {
+                if (mask && energy) VFB_K17P(true, true, true);
+                else if (mask) VFB_K17P(true, true, false);
+                else if (energy) VFB_K17P(true, false, true);
+                else VFB_K17P(true, false, false);
+            } else {
+                if (mask && energy) VFB_K17P(false, true, true);
+                else if (mask) VFB_K17P(false, true, false);
+                else if (energy) VFB_K17P(false, false, true);
+                else VFB_K17P(false, false, false);
+            }
+#undef VFB_K17P
+            return cudaGetLastError();
         }
     }
     const bool tma = b.variant == 2 && (b.nx % TmaTile<S>::BX) == 0 && b.status != nullptr;
