@@ -483,6 +483,17 @@ int vfb_pool_stats(const vfb_pool *pool, uint32_t *active_domains, uint64_t *act
                    uint64_t *free_bytes);
 /* kernels the pool has launched (graph replays count their kernels) */
 int vfb_pool_kernel_launches(const vfb_pool *pool, uint64_t *count);
+/* FP64 mass sum(1 + drho) over the fluid nodes of every active domain, at the state the next step
+   reads: mass[id] for id < max_domains (0 for inactive ids), host memory; synchronises the stream.
+   Per domain the sum runs in a fixed order. */
+int vfb_pool_domain_mass(vfb_pool *pool, double *mass, void *stream);
+/* The watchdog: the domain masses as above; a domain fails when its mass is not finite (a NaN or
+   infinite population anywhere in it) or has drifted by more than max_relative_drift from its
+   mass at the first check after its initialisation. Up to `capacity` failing ids go to `failed`,
+   their number to *n_failed; VFB_ERR_WATCHDOG when any failed. Nothing is removed: the caller
+   decides (a serving loop fails the request, not the process). */
+int vfb_pool_watchdog(vfb_pool *pool, double max_relative_drift, uint32_t *failed, uint32_t capacity,
+                      uint32_t *n_failed, void *stream);
 
 #ifdef __cplusplus
 }

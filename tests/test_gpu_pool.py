@@ -230,3 +230,30 @@ def test_pool_rejects_bad_boundary_condition_lists(cuda):
             pool.add(g["shape"], 1.8, periodic=(False, True, True), mask=g["mask"], bcs=bad)
         assert e.value.status == N.VFB_ERR_INVALID_ARGUMENT
     assert pool.stats()["used_bytes"] == 0
+
+
+def test_watchdog_flags_only_the_diverged_domain(cuda):
+    """A domain initialised with a NaN velocity is reported by the watchdog; the others keep their
+    FP64 mass (periodic: conserved to round-off) and run on after it is removed."""
+    s = _stream()
+    pool = Pool(1 << 27, storage="f64", max_domains=8)
+    shapes = [(12, 10, 8), (9, 9, 9), (16, 6, 7)]
+    ids = []
+    for i, shape in enumerate(shapes):
+        d = pool.add(shape, 1.8)
+        f = _fields(shape, 30 + i)
+        if i == 1:
+            f[1] = f[1].copy()
+            f[1][5] = np.nan
+        pool.init(d, *f, stream=s)
+        ids.append(d)
+    assert pool.watchdog(stream=s) == [ids[1]]
+    m0 = pool.domain_mass(stream=s)
+    assert np.isnan(m0[ids[1]]) and np.isfinite(m0[ids[0]]) and np.isfinite(m0[ids[2]])
+    pool.remove(ids[1])
+    pool.step(50, stream=s)
+    assert pool.watchdog(stream=s) == []
+    m1 = pool.domain_mass(stream=s)
+    for d in (ids[0], ids[2]):
+        assert abs(m1[d] - m0[d]) <= 1e-12 * m0[d]
+    assert abs(m0[ids[0]] - np.prod(shapes[0])) < 1.0      # sum(1 + drho) ~ node count

@@ -59,3 +59,27 @@ def test_fp16_storage_permeability_close_to_fp64(cuda, drive):
     assert k64 > 0
     assert abs(k32 - k64) <= 1e-4 * k64
     assert abs(k16 - k64) <= 1e-2 * k64
+
+
+def test_a_diverging_request_fails_alone(cuda):
+    """A request whose initial state holds a NaN is stopped by the watchdog with status "watchdog";
+    every other request completes with the result it has alone."""
+    reqs = _small_stream(n=5, seed=9)
+    bad = reqs[2]
+    g = bad.geometry()
+    n = int(np.prod(g["shape"]))
+    ux = np.zeros(n, dtype=np.float32)
+    fluid = np.nonzero(g["mask"])[0]
+    ux[fluid[fluid.size // 2]] = np.nan          # a fluid node: solid nodes are never initialised
+    bad.initial = (np.zeros(n, dtype=np.float32), ux, np.zeros(n, dtype=np.float32), np.zeros(n, dtype=np.float32))
+    srv = Server(1 << 30, storage="f32", keep_fields=True)
+    results, stats = srv.run(reqs, realtime=False)
+    srv.close()
+    assert stats["failed"] == 1
+    for req, res in zip(reqs, results):
+        if req is bad:
+            assert res.status == "watchdog" and np.isnan(res.permeability)
+            continue
+        assert res.status == "ok"
+        perm, ux_alone = solve_alone(req, storage="f32")
+        assert np.array_equal(res.ux, ux_alone), req.rid

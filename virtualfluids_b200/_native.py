@@ -180,6 +180,9 @@ SIGNATURES = {
     "vfb_simulation_is_even_timestep": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "vfb_simulation_level_is_even_timestep": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
     "vfb_simulation_use_level": (C.c_int, [C.c_void_p, C.c_int32]),
+    "vfb_pool_domain_mass": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "vfb_pool_watchdog": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32),
+                                    C.c_void_p]),
     "vfb_box_read_populations": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.c_void_p]),
     "vfb_box_write_populations": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]),
     "vfb_simulation_set_neighbor_tables": (C.c_int, [C.c_void_p, C.c_int32]),

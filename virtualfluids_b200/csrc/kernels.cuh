@@ -1493,6 +1493,46 @@ __global__ void __launch_bounds__(256) k17_pool_kernel(PoolArgs<typename Codec<S
 }
 
 
+// FP64 mass sum(1 + drho) of the fluid nodes of every work item of a pool, one block per item, at
+// the parity the next step reads (the watchdog's reduction: a non-finite population makes the sum
+// non-finite). Fixed order within a block: per-thread sums, warp shuffles, then the warps in order.
+template <class S, bool EVEN>
+__global__ void __launch_bounds__(256) pool_mass_kernel(PoolArgs<typename Codec<S>::compute> a, double *partials)
+{
+    using C = typename Codec<S>::compute;
+    const uint2 it = a.items[blockIdx.x];
+    const PoolDomain<C> &dm = a.domains[it.x];
+    const uint32_t nodes_total = (uint32_t)dm.nx * (uint32_t)dm.ny * (uint32_t)dm.nz;
+    const uint32_t span = blockDim.x * (uint32_t)a.nodes_per_thread;
+    const uint32_t end = min(it.y + span, nodes_total);
+    const S *base = static_cast<const S *>(a.arena) + dm.dist_offset;
+    const uint8_t *mask = (dm.flags & kPoolMask) ? static_cast<const uint8_t *>(a.arena) + dm.mask_offset : nullptr;
+    const NodeAddr box{ dm.nx, dm.ny, dm.nz, dm.flags & 7 };
+    double m = 0.0;
+    for (uint32_t k = it.y + threadIdx.x; k < end; k += blockDim.x) {
+        if (mask && __ldg(mask + k) == 0)
+            continue;
+        uint32_t nodes[8];
+        box_nodes(k, box, nodes);
+        C f[27];
+        gather_pre<S, EVEN>(base, dm.pitch, nodes, f);
+        m += 1.0 + (double)density_pyramid(f);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        m += __shfl_down_sync(0xffffffffu, m, o);
+    __shared__ double warp_sums[8];
+    if ((threadIdx.x & 31) == 0)
+        warp_sums[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (unsigned w = 0; w < (blockDim.x + 31) / 32; ++w)
+            t += warp_sums[w];
+        partials[blockIdx.x] = t;
+    }
+}
+
 // The boundary conditions of every domain of a pool, one launch per kind: a persistent grid over
 // {domain, first BC node} items of 128 BC nodes. No-slip: NoSlipInterpolatedCompressible after the
 // collision (current parity); pressure: PressureNonEquilibriumCompressible after the parity swap.

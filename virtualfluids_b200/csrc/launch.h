@@ -86,6 +86,9 @@ struct PoolDomainSpec {
         static const void *pool_kernel(bool even);                                                                \
         static size_t pool_domain_bytes();                                                                        \
         static void pool_domain(void *out, const PoolDomainSpec &spec);                                            \
+        static cudaError_t pool_mass(void *arena, const void *domains, const uint2 *items, uint32_t n_items,       \
+                                     int nodes_per_thread, int threads, bool even, double *partials,              \
+                                     cudaStream_t s);                                                              \
         static cudaError_t pool_bcs(void *arena, const void *domains, const uint2 *noslip_items,                   \
                                     const uint32_t *n_noslip_items, const uint2 *pressure_items,                   \
                                     const uint32_t *n_pressure_items, bool even, unsigned grid, cudaStream_t s);   \

@@ -284,6 +284,24 @@ void Launchers<S>::pool_domain(void *out, const PoolDomainSpec &spec)
 }
 
 template <class S>
+cudaError_t Launchers<S>::pool_mass(void *arena, const void *domains, const uint2 *items, uint32_t n_items,
+                                    int nodes_per_thread, int threads, bool even, double *partials, cudaStream_t s)
+{
+    using C = typename Codec<S>::compute;
+    if (n_items == 0)
+        return cudaSuccess;
+    PoolArgs<C> a;
+    a.arena = arena;
+    a.domains = static_cast<const PoolDomain<C> *>(domains);
+    a.items = items;
+    a.n_items = nullptr;
+    a.nodes_per_thread = nodes_per_thread;
+    if (even) pool_mass_kernel<S, true><<<n_items, threads, 0, s>>>(a, partials);
+    else pool_mass_kernel<S, false><<<n_items, threads, 0, s>>>(a, partials);
+    return cudaGetLastError();
+}
+
+template <class S>
 cudaError_t Launchers<S>::pool_bcs(void *arena, const void *domains, const uint2 *noslip_items,
                                    const uint32_t *n_noslip_items, const uint2 *pressure_items,
                                    const uint32_t *n_pressure_items, bool even, unsigned grid, cudaStream_t s)

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <string>
@@ -47,6 +48,7 @@ struct PoolOps {
     void (*domain)(void *, const vfb::PoolDomainSpec &);
     cudaError_t (*bcs)(void *, const void *, const uint2 *, const uint32_t *, const uint2 *, const uint32_t *, bool,
                        unsigned, cudaStream_t);
+    cudaError_t (*mass)(void *, const void *, const uint2 *, uint32_t, int, int, bool, double *, cudaStream_t);
     cudaError_t (*init)(const vfb::BoxState &, bool, const void *, const void *, const void *, const void *,
                         cudaStream_t);
     cudaError_t (*macros)(const vfb::BoxState &, bool, void *, void *, void *, void *, cudaStream_t);
@@ -56,7 +58,7 @@ template <class LA>
 PoolOps ops_of()
 {
     return PoolOps{ LA::pool_collide, LA::pool_kernel, LA::pool_domain_bytes, LA::pool_domain, LA::pool_bcs,
-                    LA::box_init, LA::box_macros };
+                    LA::pool_mass, LA::box_init, LA::box_macros };
 }
 
 bool select_ops(int storage, int arith, PoolOps &out)
@@ -130,6 +132,8 @@ struct DomainSlot {
     uint64_t bytes = 0;            // bytes taken (populations, mask, boundary conditions)
     bool has_mask = false;
     uint32_t n_noslip = 0, n_pressure = 0;
+    double ref_mass = 0.0;         // watchdog: the mass at the first check after the initialisation
+    bool has_ref = false;
 };
 
 // a work list on the device: {domain, first node} items and their count (a device word, so that a
@@ -170,6 +174,9 @@ struct vfb_pool {
     DeviceList noslip_list, pressure_list;   // BC work lists of the active domains
     bool has_noslip = false, has_pressure = false;
     unsigned bc_grid = 0;
+    std::vector<uint2> host_items;     // the collision work list as uploaded (watchdog sums)
+    double *mass_partials = nullptr;   // one FP64 partial per work item
+    size_t mass_capacity = 0;
 };
 
 namespace {
@@ -309,6 +316,7 @@ cudaError_t rebuild_list(vfb_pool *p, cudaStream_t s)
     const uint32_t n = (uint32_t)items.size();
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(p->n_items, &n, sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+    p->host_items = items;
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(s);
     if (e == cudaSuccess)
@@ -536,6 +544,7 @@ int vfb_pool_destroy(vfb_pool *p)
     cudaFree(p->items);
     cudaFree(p->n_items);
     cudaFree(p->staging);
+    cudaFree(p->mass_partials);
     for (DeviceList *L : { &p->noslip_list, &p->pressure_list }) {
         cudaFree(L->items);
         cudaFree(L->count);
@@ -750,6 +759,7 @@ int vfb_pool_init_domain(vfb_pool *p, uint32_t id, const void *rho, const void *
         d.active = true;
         p->list_dirty = true;
     }
+    d.has_ref = false;
     return pool_cuda(e, "pool init domain");
 }
 
@@ -908,6 +918,79 @@ int vfb_pool_stats(const vfb_pool *p, uint32_t *active_domains, uint64_t *active
         *used_bytes = p->alloc.used();
     if (free_bytes)
         *free_bytes = p->desc.arena_bytes - p->alloc.used();
+    return VFB_OK;
+}
+
+int vfb_pool_domain_mass(vfb_pool *p, double *mass, void *stream)
+{
+    if (!p || !mass)
+        return pool_fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaSuccess;
+    if (p->list_dirty)
+        e = rebuild_list(p, s);
+    const size_t n = p->host_items.size();
+    if (e == cudaSuccess && n > p->mass_capacity) {
+        e = cudaStreamSynchronize(s);
+        if (e == cudaSuccess) {
+            cudaFree(p->mass_partials);
+            p->mass_partials = nullptr;
+            p->mass_capacity = 0;
+            e = cudaMalloc((void **)&p->mass_partials, n * sizeof(double));
+            if (e == cudaSuccess)
+                p->mass_capacity = n;
+        }
+    }
+    if (e == cudaSuccess)
+        e = p->ops.mass(p->arena, p->domain_table, p->items, (uint32_t)n, p->nodes_per_thread, p->threads, p->even,
+                        p->mass_partials, s);
+    std::vector<double> partial(n);
+    if (e == cudaSuccess && n)
+        e = cudaMemcpyAsync(partial.data(), p->mass_partials, n * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess)
+        return pool_cuda(e, "pool domain mass");
+    ++p->launches;
+    for (size_t i = 0; i < p->slots.size(); ++i)
+        mass[i] = 0.0;
+    // items are grouped by domain in id order: a fixed summation order per domain
+    for (size_t i = 0; i < n; ++i)
+        mass[p->host_items[i].x] += partial[i];
+    return VFB_OK;
+}
+
+int vfb_pool_watchdog(vfb_pool *p, double max_relative_drift, uint32_t *failed, uint32_t capacity, uint32_t *n_failed,
+                      void *stream)
+{
+    if (!p || !n_failed || (capacity && !failed) || !(max_relative_drift > 0.0))
+        return pool_fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument or non-positive drift bound");
+    std::vector<double> mass(p->slots.size());
+    int st = vfb_pool_domain_mass(p, mass.data(), stream);
+    if (st)
+        return st;
+    uint32_t bad = 0;
+    for (uint32_t id = 0; id < p->slots.size(); ++id) {
+        DomainSlot &d = p->slots[id];
+        if (!d.live || !d.active)
+            continue;
+        const double m = mass[id];
+        bool ok = std::isfinite(m);
+        if (ok && !d.has_ref) {
+            d.ref_mass = m;
+            d.has_ref = true;
+        } else if (ok) {
+            ok = std::fabs(m - d.ref_mass) <= max_relative_drift * std::fabs(d.ref_mass);
+        }
+        if (!ok) {
+            if (bad < capacity)
+                failed[bad] = id;
+            ++bad;
+        }
+    }
+    *n_failed = bad;
+    if (bad)
+        return pool_fail(VFB_ERR_WATCHDOG, "non-finite populations or mass drift in a pool domain");
     return VFB_OK;
 }
 

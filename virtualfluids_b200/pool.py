@@ -34,6 +34,7 @@ class Pool:
         self._h = h
         self.storage = storage
         self.real = np.float64 if storage == "f64" else np.float32
+        self.max_domains = int(max_domains)
         self.domains = {}
 
     def close(self):
@@ -168,6 +169,26 @@ class Pool:
         a, n, u, f = C.c_uint32(), C.c_uint64(), C.c_uint64(), C.c_uint64()
         N.check(N.lib().vfb_pool_stats(self._h, C.byref(a), C.byref(n), C.byref(u), C.byref(f)))
         return {"active_domains": a.value, "active_nodes": n.value, "used_bytes": u.value, "free_bytes": f.value}
+
+    def domain_mass(self, stream=None):
+        """FP64 mass sum(1 + drho) of every domain id (0 for inactive ids), at the current state."""
+        out = np.zeros(len(self._mass_ids()), dtype=np.float64)
+        N.check(N.lib().vfb_pool_domain_mass(self._h, out.ctypes.data, _stream_ptr(stream)))
+        return out
+
+    def _mass_ids(self):
+        return range(self.max_domains)
+
+    def watchdog(self, max_relative_drift=0.5, stream=None):
+        """Ids of the domains whose mass is non-finite or drifted beyond max_relative_drift from their
+        mass at the first check after initialisation (vfb_pool_watchdog); [] when all are sound."""
+        failed = np.zeros(self.max_domains, dtype=np.uint32)
+        n = C.c_uint32()
+        st = N.lib().vfb_pool_watchdog(self._h, float(max_relative_drift), failed.ctypes.data, failed.size, C.byref(n),
+                                        _stream_ptr(stream))
+        if st not in (N.VFB_OK, N.VFB_ERR_WATCHDOG):
+            N.check(st)
+        return [int(i) for i in failed[:n.value]]
 
     def kernel_launches(self) -> int:
         c = C.c_uint64()

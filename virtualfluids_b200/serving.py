@@ -44,6 +44,7 @@ class Request:
     drho: float = 3e-3                # density drop across the block of the "pressure" drive
     drive: str = "pressure"
     geo: dict | None = field(default=None, repr=False)
+    initial: tuple | None = field(default=None, repr=False)   # (drho, ux, uy, uz) host arrays; None = rest
 
     def geometry(self):
         """The request's domain (built on first use): shape, periodicity, mask, BC lists and the
@@ -84,6 +85,7 @@ class Result:
     fluid_nodes: int
     permeability: float
     ux: np.ndarray | None = field(default=None, repr=False)
+    status: str = "ok"                # "watchdog": stopped for non-finite populations or mass drift
 
     @property
     def time_to_solution(self) -> float:
@@ -113,14 +115,18 @@ def request_work(req: Request):
 class Server:
     """Continuous batching of porous-block solves in one domain pool.
 
-    arena_bytes is the HBM budget of populations and masks. Between two scheduling points (arrivals
-    admitted, finished solves read out and released) the pool runs a chunk of steps sized to about
-    chunk_ms of GPU time and never past the next completion, so admissions wait for at most one
-    chunk while the GPU stays busy."""
+    arena_bytes is the HBM budget of populations, masks and BC lists. Between two scheduling points
+    (arrivals admitted, finished solves read out and released) the pool runs a chunk of steps sized
+    to about chunk_ms of GPU time and never past the next completion, so admissions wait for at
+    most one chunk while the GPU stays busy. After every chunk the pool's watchdog (FP64 mass per
+    domain) stops any solve whose populations went non-finite or whose mass drifted by more than
+    max_mass_drift: that request ends with status "watchdog", the others go on."""
 
-    def __init__(self, arena_bytes, storage="f32", max_domains=1024, chunk_ms=40.0, stream=None, keep_fields=False):
+    def __init__(self, arena_bytes, storage="f32", max_domains=1024, chunk_ms=40.0, stream=None, keep_fields=False,
+                 max_mass_drift=0.5, pool=None):
         import torch
-        self.pool = Pool(arena_bytes, storage=storage, max_domains=max_domains)
+        self.pool = pool if pool is not None else Pool(arena_bytes, storage=storage, max_domains=max_domains)
+        self.max_mass_drift = float(max_mass_drift)
         self.storage = storage
         self.chunk_ms = float(chunk_ms)
         self.stream = stream or torch.cuda.Stream()
@@ -144,8 +150,11 @@ class Server:
                               mask=g["mask"], bcs=g["bcs"])
         if d is None:
             return None
-        z = self._rest(int(np.prod(g["shape"])))
-        self.pool.init(d, z, z, z, z, stream=self.stream)
+        if req.initial is not None:
+            self.pool.init(d, *req.initial, stream=self.stream)
+        else:
+            z = self._rest(int(np.prod(g["shape"])))
+            self.pool.init(d, z, z, z, z, stream=self.stream)
         return d
 
     def run(self, requests, realtime=True, clock=time.perf_counter):
@@ -159,6 +168,7 @@ class Server:
         t0 = clock()
         launches0 = self.pool.kernel_launches()
         peak_active = 0
+        failed = 0
         while pending or waiting or active:
             now = clock() - t0
             while pending and (not realtime or pending[0].arrival <= now):
@@ -194,6 +204,13 @@ class Server:
             self.stream.synchronize()
             el = clock() - c0
             self.ns_per_node_step = 0.7 * self.ns_per_node_step + 0.3 * (el * 1e9 / (chunk * nodes))
+            # the watchdog fails a diverging request, not the loop
+            for d in self.pool.watchdog(self.max_mass_drift, stream=self.stream):
+                req, _, adm = active.pop(d)
+                results[req.rid] = Result(req.rid, req.arrival, adm, clock() - t0, req.steps, req.fluid_nodes,
+                                          float("nan"), status="watchdog")
+                self.pool.remove(d)
+                failed += 1
             for d in [d for d, v in active.items() if v[1] == chunk]:
                 req, _, adm = active.pop(d)
                 rho, ux, uy, uz = self.pool.fields(d, stream=self.stream)
@@ -205,10 +222,11 @@ class Server:
         self.stream.synchronize()
         wall = clock() - t0
         tts = np.array([results[r.rid].time_to_solution for r in requests])
-        fluid_updates = sum(results[r.rid].fluid_nodes * r.steps for r in requests)
+        fluid_updates = sum(results[r.rid].fluid_nodes * r.steps for r in requests if results[r.rid].status == "ok")
         stats = {"requests": len(requests), "wall_s": wall, "p50_s": float(np.quantile(tts, 0.5)),
                  "p99_s": float(np.quantile(tts, 0.99)), "mlups": fluid_updates / wall / 1e6,
-                 "peak_concurrent": peak_active, "gpu_launches": self.pool.kernel_launches() - launches0}
+                 "peak_concurrent": peak_active, "gpu_launches": self.pool.kernel_launches() - launches0,
+                 "failed": failed}
         return [results[r.rid] for r in requests], stats
 
 
