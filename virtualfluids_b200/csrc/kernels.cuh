@@ -1435,6 +1435,7 @@ struct PoolDomain {
     uint64_t pressure_offset;    // bytes: int32 k[n], int32 kN[n], int32 direction[n], then C drho[n]
     uint64_t pressure_rho_offset;
     uint32_t n_noslip, n_pressure;
+    FastDiv div_nx, div_ny;      // node k -> (x, y, z) without hardware division
 };
 
 enum : int { kPoolPeriodicX = 1, kPoolPeriodicY = 2, kPoolPeriodicZ = 4, kPoolMask = 8 };
@@ -1466,8 +1467,8 @@ __global__ void __launch_bounds__(256) k17_pool_kernel(PoolArgs<typename Codec<S
         for (uint32_t k = it.y + threadIdx.x; k < end; k += blockDim.x) {
             if (mask && __ldg(mask + k) == 0)
                 continue;
-            const uint32_t x = k % (uint32_t)nx, yz = k / (uint32_t)nx;
-            const uint32_t y = yz % (uint32_t)ny, z = yz / (uint32_t)ny;
+            const uint32_t yz = fast_div(k, dm.div_nx), x = k - yz * (uint32_t)nx;
+            const uint32_t z = fast_div(yz, dm.div_ny), y = yz - z * (uint32_t)ny;
             const int xp = ((int)x + 1 < nx) ? (int)x + 1 : ((flags & kPoolPeriodicX) ? 0 : (int)x);
             const int yp = ((int)y + 1 < ny) ? (int)y + 1 : ((flags & kPoolPeriodicY) ? 0 : (int)y);
             const int zp = ((int)z + 1 < nz) ? (int)z + 1 : ((flags & kPoolPeriodicZ) ? 0 : (int)z);

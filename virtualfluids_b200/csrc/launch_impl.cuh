@@ -270,6 +270,8 @@ void Launchers<S>::pool_domain(void *out, const PoolDomainSpec &spec)
     d.nz = spec.nz;
     d.flags = spec.flags;
     d.rates = rates_of<C>(spec.omega, spec.lim);
+    d.div_nx = make_fast_div((uint32_t)spec.nx);
+    d.div_ny = make_fast_div((uint32_t)spec.ny);
     d.fx = (C)spec.half_force[0];
     d.fy = (C)spec.half_force[1];
     d.fz = (C)spec.half_force[2];
