@@ -9,6 +9,7 @@
 #include "oracle.h"
 
 #include <math.h>
+#include <stdio.h>
 #include <stddef.h>
 #include <stdlib.h>
 #include <string.h>
@@ -166,19 +167,36 @@ static inline double signed_sum(int d, double ux, double uy, double uz)
 
 static inline int q_active(double q) { return q >= 0.0 && q <= 1.0; }
 
+/* The post-collision populations of every node of a BC list, read before the list writes anything
+   ([i * 27 + d]). Where two nodes of one list are joined by a link cut from both ends, each node's
+   write lands in a slot the other reads; reading first gives every node the collision's values,
+   as a parallel kernel whose reads all precede its writes does, independent of the list order. */
+static double *read_posts(const orc_level *L, const int32_t *k, uint32_t nbc, int is_even)
+{
+    double *all = (double *)malloc(sizeof(double) * 27 * (size_t)(nbc ? nbc : 1));
+    if (!all) {
+        fprintf(stderr, "oracle: out of memory for a BC list of %u nodes\n", nbc);
+        abort();
+    }
+    for (uint32_t i = 0; i < nbc; ++i)
+        read_post(L, (uint32_t)k[i], is_even, all + 27 * (size_t)i);
+    return all;
+}
+
 /* NoSlipBounceBack_Device (BoundaryConditions/NoSlip/NoSlipBounceBack.cu:44-179) */
 void orc_bc_noslip_bounce_back(orc_level *L, const int32_t *k, const double *q27, uint32_t nbc, int is_even)
 {
     int map_next[27];
     orc_pointer_map(!is_even, map_next);
+    double *all = read_posts(L, k, nbc, is_even);
     for (uint32_t i = 0; i < nbc; ++i) {
         const uint32_t node = (uint32_t)k[i];
-        double post[27];
-        read_post(L, node, is_even, post);
+        const double *post = all + 27 * (size_t)i;
         for (int d = 1; d < 27; ++d)
             if (q_active(q27[(uint64_t)d * nbc + i]))
                 write_pre_dir(L, node, map_next, ORC_INV[d], post[d]);
     }
+    free(all);
 }
 
 /* VelocityBounceBack_Device (BoundaryConditions/Velocity/VelocityBounceBack.cu:44-188):
@@ -188,10 +206,10 @@ void orc_bc_velocity_bounce_back(orc_level *L, const int32_t *k, const double *q
 {
     int map_next[27];
     orc_pointer_map(!is_even, map_next);
+    double *all = read_posts(L, k, nbc, is_even);
     for (uint32_t i = 0; i < nbc; ++i) {
         const uint32_t node = (uint32_t)k[i];
-        double post[27];
-        read_post(L, node, is_even, post);
+        const double *post = all + 27 * (size_t)i;
         for (int d = 1; d < 27; ++d) {
             if (!q_active(q27[(uint64_t)d * nbc + i]))
                 continue;
@@ -201,6 +219,7 @@ void orc_bc_velocity_bounce_back(orc_level *L, const int32_t *k, const double *q
             write_pre_dir(L, node, map_next, e, post[d] + coef * signed_sum(e, ux[i], uy[i], uz[i]));
         }
     }
+    free(all);
 }
 
 /* macroscopic values the interpolated kernels compute from post-collision populations
@@ -255,10 +274,11 @@ void orc_bc_noslip_interpolated(orc_level *L, const int32_t *k, const double *q2
 {
     int map_next[27];
     orc_pointer_map(!is_even, map_next);
+    double *all = read_posts(L, k, nbc, is_even);
     for (uint32_t i = 0; i < nbc; ++i) {
         const uint32_t node = (uint32_t)k[i];
-        double post[27], drho, vx, vy, vz, cu_sq;
-        read_post(L, node, is_even, post);
+        const double *post = all + 27 * (size_t)i;
+        double drho, vx, vy, vz, cu_sq;
         bc_macros(post, &drho, &vx, &vy, &vz, &cu_sq);
         for (int d = 1; d < 27; ++d) {
             const double q = q27[(uint64_t)d * nbc + i];
@@ -268,6 +288,7 @@ void orc_bc_noslip_interpolated(orc_level *L, const int32_t *k, const double *q2
             write_pre_dir(L, node, map_next, ORC_INV[d], interp_noslip(q, post[d], post[ORC_INV[d]], feq, omega));
         }
     }
+    free(all);
 }
 
 /* VelocityInterpolatedCompressible_Device (Velocity/VelocityInterpolatedCompressible.cu:44-420) */
@@ -276,10 +297,11 @@ void orc_bc_velocity_interpolated(orc_level *L, const int32_t *k, const double *
 {
     int map_next[27];
     orc_pointer_map(!is_even, map_next);
+    double *all = read_posts(L, k, nbc, is_even);
     for (uint32_t i = 0; i < nbc; ++i) {
         const uint32_t node = (uint32_t)k[i];
-        double post[27], drho, vx, vy, vz, cu_sq;
-        read_post(L, node, is_even, post);
+        const double *post = all + 27 * (size_t)i;
+        double drho, vx, vy, vz, cu_sq;
         bc_macros(post, &drho, &vx, &vy, &vz, &cu_sq);
         for (int d = 1; d < 27; ++d) {
             const double q = q27[(uint64_t)d * nbc + i];
@@ -291,6 +313,7 @@ void orc_bc_velocity_interpolated(orc_level *L, const int32_t *k, const double *
                           interp_velocity(q, post[d], post[ORC_INV[d]], feq, omega, vbc, ORC_W[d]));
         }
     }
+    free(all);
 }
 
 /* feq - w for one direction in the form of the pressure/init kernels: w (drho + (drho+1)(3cu + 4.5cu^2 - cusq)) */

@@ -224,6 +224,31 @@ def test_obstacle_geometry_bc_and_drag_lift(oracle, cuda, arith):
         assert np.all(np.abs(got - want) <= 1e-9 * scale)
 
 
+def test_sphere_geometry_bc_and_drag_exact_is_bitwise(oracle, cuda):
+    """A sphere in a channel with the exact q of Sphere::getIntersection on every cut link, the
+    interpolated geometry BC and the FP64 drag of every step: bitwise against the oracle."""
+    g = ListGrid(26, 14, 14, periodic=(False, True, True))
+    g.add_side("MX", "velocity", velocity=(0.03, 0.0, 0.0))
+    g.add_side("PX", "pressure", rho=0.0)
+    g.add_sphere_obstacle((9.4, 6.7, 6.2), 3.3)
+    bcf = BCF()
+    bcf.set_velocity_boundary_condition(BCF.VelocityBC.VelocityInterpolatedCompressible)
+    bcf.set_pressure_boundary_condition(BCF.PressureBC.PressureNonEquilibriumCompressible)
+    bcf.set_geometry_boundary_condition(BCF.NoSlipBC.NoSlipInterpolatedCompressible)
+    steps = 40
+    sim = Simulation(make_para(1.85, N.STORAGE_F64, N.ARITH_EXACT), g, bcf)
+    orc = oracle.OracleLevel(g, omega=sim.para.omega, velocity_kind=2, noslip_kind=2, geometry_kind=2, drag_lift=True)
+    sim.init()
+    orc.init()
+    sim.enable_drag_lift(history_steps=steps)
+    sim.run(steps)
+    orc.run(steps)
+    assert np.array_equal(sim.populations(), orc.f)
+    got, want = sim.drag_lift_history(), np.array(orc.drag_history)
+    assert want[-1, 0] > 0.0
+    assert np.all(np.abs(got - want) <= 1e-12 * np.abs(want).max(axis=0))
+
+
 def test_drag_lift_history_ring_keeps_the_last_steps(oracle, cuda):
     g, bcf = _cube_channel()
     sim = Simulation(make_para(1.8, N.STORAGE_F64, N.ARITH_EXACT), g, bcf)

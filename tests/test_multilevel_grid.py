@@ -93,3 +93,26 @@ def test_oracle_refined_shear_wave_decays_at_the_analytic_rate(oracle):
         amp = (ux * s).sum() / (s * s).sum()
         assert abs(amp / want - 1.0) < 1.5e-2
         assert np.abs(ux - amp * s).max() < 1e-2 * U
+
+
+def test_sphere_obstacle_cuts_every_link_into_it_exactly():
+    """ListGrid.add_sphere_obstacle: every link from a fluid node to a node inside the sphere has
+    q in [0, 1], and p + q c lies on the sphere (to round-off)."""
+    from virtualfluids_b200.grid import CX, CY, CZ
+    g = ListGrid(20, 16, 16)
+    c, r = np.array([9.3, 7.6, 8.1]), 3.7
+    bc = g.add_sphere_obstacle(c, r)
+    row = {int(k): i for i, k in enumerate(bc.k)}
+    pos = g.coords.astype(np.float64)
+    checked = 0
+    for k in g.fluid:
+        for d in range(1, 27):
+            cd = np.array([CX[d], CY[d], CZ[d]], dtype=np.float64)
+            if ((pos[:, k] + cd - c) ** 2).sum() > r * r:
+                continue
+            i = row[int(k)]
+            q = bc.q[d, i]
+            assert 0.0 <= q <= 1.0
+            assert abs(np.linalg.norm(pos[:, k] + q * cd - c) - r) < 1e-12
+            checked += 1
+    assert checked > 500

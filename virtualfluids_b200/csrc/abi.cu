@@ -311,7 +311,8 @@ static int run_k17(const vfb_level *level, const uint32_t *idx, uint32_t size, i
     return cuda_status(e, "K17CompressibleNavierStokes launch");
 }
 
-static int run_bc(const vfb_level *level, const vfb_bc *bc, int kind, bool velocity, void *stream)
+static int run_bc(const vfb_level *level, const vfb_bc *bc, int kind, bool velocity, void *stream,
+                  void *snap = nullptr)
 {
     int st = check_level(level);
     if (st)
@@ -322,7 +323,8 @@ static int run_bc(const vfb_level *level, const vfb_bc *bc, int kind, bool veloc
         return fail(VFB_ERR_INVALID_ARGUMENT, "bc node indices or q27 are NULL");
     if (velocity && bc->number_of_bc_nodes && (!bc->vx || !bc->vy || !bc->vz))
         return fail(VFB_ERR_INVALID_ARGUMENT, "bc velocities are NULL");
-    const cudaError_t e = VFB_DISPATCH(level->storage, level->arith, LA::bc(level, bc, kind, as_stream(stream)));
+    const cudaError_t e = VFB_DISPATCH(level->storage, level->arith,
+                                       LA::bc(level, bc, kind, as_stream(stream), nullptr, snap));
     return cuda_status(e, "boundary condition launch");
 }
 
@@ -655,6 +657,10 @@ struct SimLevel {
     vfb_interpolation_cells fc{}, cf{};
     vfb_interpolation_cell_neighbor fc_offsets{}, cf_offsets{};
     // neighbour slot table of the fluid-node list (library-owned, built by set_level)
+    // per post-collision BC list: its post-collision values taken before the list writes (27 doubles
+    // per node, enough for every storage), so that the BCs of a list never read each other's writes
+    void *snap[3] = { nullptr, nullptr, nullptr };   // velocity, no-slip, geometry
+    uint32_t snap_nodes[3] = { 0, 0, 0 };
     uint32_t *slots = nullptr;        // 8 arrays of slots_stride entries, then the kernels' status word
     uint64_t slots_stride = 0;
     size_t slots_nodes = 0;
@@ -671,7 +677,20 @@ struct SimLevel {
         for (auto &p : slots_key)
             p = nullptr;
     }
-    ~SimLevel() { free_slots(); }
+    void free_snaps()
+    {
+        for (int i = 0; i < 3; ++i) {
+            if (snap[i])
+                cudaFree(snap[i]);
+            snap[i] = nullptr;
+            snap_nodes[i] = 0;
+        }
+    }
+    ~SimLevel()
+    {
+        free_slots();
+        free_snaps();
+    }
     SimLevel() = default;
     SimLevel(const SimLevel &) = delete;
     SimLevel &operator=(const SimLevel &) = delete;
@@ -680,6 +699,13 @@ struct SimLevel {
     {
         if (this != &o) {
             free_slots();
+            free_snaps();
+            for (int i = 0; i < 3; ++i) {
+                snap[i] = o.snap[i];
+                snap_nodes[i] = o.snap_nodes[i];
+                o.snap[i] = nullptr;
+                o.snap_nodes[i] = 0;
+            }
             has_level = o.has_level; level = o.level; fluid = o.fluid; n_fluid = o.n_fluid;
             velocity = o.velocity; velocity_fn = o.velocity_fn; velocity_set = o.velocity_set;
             noslip = o.noslip; noslip_fn = o.noslip_fn; noslip_set = o.noslip_set;
@@ -1032,6 +1058,45 @@ int vfb_simulation_check(const vfb_simulation *sim)
     return VFB_OK;
 }
 
+// the kernel kind behind a factory function, for the driver's snapshot launches
+static int bc_kind_of(vfb_bc_fn fn, bool &velocity)
+{
+    velocity = true;
+    if (fn == vfb_velocity_bounce_back) return vfb::kVelocityBB;
+    if (fn == vfb_velocity_interpolated_compressible) return vfb::kVelocityInterp;
+    if (fn == vfb_velocity_interpolated_incompressible) return vfb::kVelocityInterpIncomp;
+    if (fn == vfb_velocity_with_pressure_interpolated_compressible) return vfb::kVelocityWithPressure;
+    velocity = false;
+    if (fn == vfb_noslip_bounce_back) return vfb::kNoSlipBB;
+    if (fn == vfb_noslip_interpolated_compressible) return vfb::kNoSlipInterp;
+    if (fn == vfb_noslip_interpolated_incompressible) return vfb::kNoSlipInterpIncomp;
+    return -1;
+}
+
+// a post-collision BC list through its factory function, reading the list's snapshot
+static int run_list(SimLevel &S, int which, vfb_bc_fn fn, const vfb_bc &bc, void *stream)
+{
+    if (!fn || bc.number_of_bc_nodes == 0)
+        return VFB_OK;
+    bool velocity = false;
+    const int kind = bc_kind_of(fn, velocity);
+    if (kind < 0)
+        return fn(&S.level, &bc, stream);
+    if (S.snap_nodes[which] < bc.number_of_bc_nodes) {
+        if (S.snap[which])
+            cudaFree(S.snap[which]);
+        S.snap[which] = nullptr;
+        S.snap_nodes[which] = 0;
+        if (cudaMalloc(&S.snap[which], (size_t)27 * bc.number_of_bc_nodes * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            S.snap[which] = nullptr;
+            return fail(VFB_ERR_OUT_OF_MEMORY, "no device memory for a boundary-condition snapshot");
+        }
+        S.snap_nodes[which] = bc.number_of_bc_nodes;
+    }
+    return run_bc(&S.level, &bc, kind, velocity, stream, S.snap[which]);
+}
+
 static int run_geometry_post(SimLevel &S, void *stream)
 {
     vfb_level &L = S.level;
@@ -1044,7 +1109,7 @@ static int run_geometry_post(SimLevel &S, void *stream)
         if (st)
             return st;
     }
-    return S.geometry_fn ? S.geometry_fn(&L, &S.geometry, stream) : VFB_OK;
+    return run_list(S, 2, S.geometry_fn, S.geometry, stream);
 }
 
 static int run_geometry_pre(SimLevel &S, void *stream)
@@ -1081,16 +1146,10 @@ static int step_level(const vfb_simulation *sim, SimLevel &S, void *stream)
     }
     if (st)
         return st;
-    if (S.velocity_fn && S.velocity.number_of_bc_nodes) {
-        st = S.velocity_fn(&L, &S.velocity, stream);
-        if (st)
-            return st;
-    }
-    if (S.noslip_fn && S.noslip.number_of_bc_nodes) {
-        st = S.noslip_fn(&L, &S.noslip, stream);
-        if (st)
-            return st;
-    }
+    if ((st = run_list(S, 0, S.velocity_fn, S.velocity, stream)) != VFB_OK)
+        return st;
+    if ((st = run_list(S, 1, S.noslip_fn, S.noslip, stream)) != VFB_OK)
+        return st;
     st = run_geometry_post(S, stream);
     if (st)
         return st;
@@ -1188,6 +1247,7 @@ struct vfb_box {
         vfb_bc_fn fn = nullptr;
         int kind = -1;              // vfb::BCKind, -1 = no kernel
         std::vector<void *> owned;
+        void *snap = nullptr;       // post-collision values of the list, taken before its writes
     } velocity, noslip, geometry;
     struct Pressure {
         vfb_directional_bc bc{};
@@ -1388,7 +1448,9 @@ cudaError_t box_run_list(vfb_box *b, const vfb_box::List &l, cudaStream_t s)
     const vfb_level L = box_level(b);
     const vfb::NodeAddr a = box_addr(b);
     ++b->launches;
-    return VFB_DISPATCH(b->desc.storage, b->desc.arith, LA::bc(&L, &l.bc, l.kind, s, &a));
+    if (l.snap)
+        ++b->launches;
+    return VFB_DISPATCH(b->desc.storage, b->desc.arith, LA::bc(&L, &l.bc, l.kind, s, &a, l.snap));
 }
 
 // one step's boundary work around the collision, in the order of vfb_simulation_run
@@ -1583,12 +1645,14 @@ int vfb_box_set_bc(vfb_box *box, int32_t kind, int32_t variant, const int32_t *k
         box->drag_history = nullptr;
     }
     const size_t rb = real_bytes(box->desc.storage);
-    void *dk = nullptr, *dq = nullptr, *dv = nullptr;
+    void *dk = nullptr, *dq = nullptr, *dv = nullptr, *ds = nullptr;
     cudaError_t e = cudaSuccess;
     if (n) {
         e = cudaMalloc(&dk, n * sizeof(int32_t));
         if (e == cudaSuccess)
             e = cudaMemcpy(dk, k, n * sizeof(int32_t), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMalloc(&ds, (size_t)27 * n * rb);   // the list's snapshot of post-collision values
         if (e == cudaSuccess)
             e = cudaMalloc(&dq, (size_t)27 * n * rb);
         if (e == cudaSuccess)
@@ -1604,9 +1668,11 @@ int vfb_box_set_bc(vfb_box *box, int32_t kind, int32_t variant, const int32_t *k
         cudaFree(dk);
         cudaFree(dq);
         cudaFree(dv);
+        cudaFree(ds);
         return cuda_status(e, "box BC upload");
     }
-    l.owned = { dk, dq, dv };
+    l.owned = { dk, dq, dv, ds };
+    l.snap = ds;
     l.bc.k = static_cast<const int32_t *>(dk);
     l.bc.q27 = dq;
     l.bc.number_of_bc_nodes = n;

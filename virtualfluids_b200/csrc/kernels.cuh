@@ -69,6 +69,8 @@ struct BCArgs {
     uint32_t nbc;
     const void *ux, *uy, *uz;   // wall / inlet velocity per BC node, compute type
     double omega;
+    const void *snap;           // optional: the list's post-collision populations taken before any BC
+                                // write, snap[d * nbc + i] (compute type); read instead of the slots
 };
 
 struct PressureArgs {
@@ -769,7 +771,13 @@ __global__ void __launch_bounds__(128) bc_bounce_back_kernel(BCArgs a)
     node_slots(node, a.nbx, a.nby, a.nbz, a.box, nodes);
     S *base = static_cast<S *>(a.dist);
     C post[27];
-    gather_post<S, EVEN>(base, a.n, nodes, post);
+    if (a.snap) {
+#pragma unroll
+        for (int d = 0; d < 27; ++d)
+            post[d] = static_cast<const C *>(a.snap)[(uint64_t)d * a.nbc + i];
+    } else {
+        gather_post<S, EVEN>(base, a.n, nodes, post);
+    }
     const C *q27 = static_cast<const C *>(a.q27);
     C ux = C(0), uy = C(0), uz = C(0);
     if (VELOCITY) {
@@ -842,11 +850,19 @@ template <class S, bool EVEN, bool VELOCITY, int FORM>
 __device__ __forceinline__ void bc_interpolated_node(S *base, uint64_t n, const uint32_t (&nodes)[8],
                                                      const typename Codec<S>::compute *q27, uint64_t q_stride,
                                                      double omega_real, typename Codec<S>::compute bx,
-                                                     typename Codec<S>::compute by, typename Codec<S>::compute bz)
+                                                     typename Codec<S>::compute by, typename Codec<S>::compute bz,
+                                                     const typename Codec<S>::compute *snap = nullptr,
+                                                     uint64_t snap_stride = 0)
 {
     using C = typename Codec<S>::compute;
     C p[27];
-    gather_post<S, EVEN>(base, n, nodes, p);
+    if (snap) {
+#pragma unroll
+        for (int d = 0; d < 27; ++d)
+            p[d] = snap[(uint64_t)d * snap_stride];
+    } else {
+        gather_post<S, EVEN>(base, n, nodes, p);
+    }
     // plain-sum density and grouped momenta (NoSlipInterpolatedCompressible.cu:134-153)
     const C drho = p[21] + p[20] + p[19] + p[22] + p[25] + p[24] + p[23] + p[26] + p[17] + p[18] + p[15] + p[16] + p[13]
                  + p[14] + p[11] + p[12] + p[9] + p[10] + p[7] + p[8] + p[5] + p[6] + p[3] + p[4] + p[1] + p[2] + p[0];
@@ -906,8 +922,30 @@ __global__ void __launch_bounds__(128) bc_interpolated_kernel(BCArgs a)
         by = static_cast<const C *>(a.uy)[i];
         bz = static_cast<const C *>(a.uz)[i];
     }
+    const C *snap = a.snap ? static_cast<const C *>(a.snap) + i : nullptr;
     bc_interpolated_node<S, EVEN, VELOCITY, FORM>(static_cast<S *>(a.dist), a.n, nodes,
-                                                  static_cast<const C *>(a.q27) + i, a.nbc, a.omega, bx, by, bz);
+                                                  static_cast<const C *>(a.q27) + i, a.nbc, a.omega, bx, by, bz,
+                                                  snap, a.nbc);
+}
+
+// The post-collision populations of every node of a BC list into snap[d * nbc + i], taken before
+// the list's BC kernel writes anything: where two BC nodes of one list are joined by a link cut
+// from both ends, each node's write lands in a slot the other reads, so reading the snapshot
+// makes the result independent of thread order (every node sees the collision's values).
+template <class S, bool EVEN>
+__global__ void __launch_bounds__(128) bc_snapshot_kernel(BCArgs a, typename Codec<S>::compute *snap)
+{
+    using C = typename Codec<S>::compute;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nbc)
+        return;
+    uint32_t nodes[8];
+    node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.box, nodes);
+    C p[27];
+    gather_post<S, EVEN>(static_cast<const S *>(a.dist), a.n, nodes, p);
+#pragma unroll
+    for (int d = 0; d < 27; ++d)
+        snap[(uint64_t)d * a.nbc + i] = p[d];
 }
 
 // feq - w of one direction in the form of the init and pressure kernels
@@ -1432,6 +1470,7 @@ struct PoolDomain {
     double omega;                // the BC kernels' omega
     uint64_t noslip_offset;      // bytes from the arena start: int32 k[n_noslip], then C q27[27 n_noslip]
     uint64_t noslip_q_offset;
+    uint64_t noslip_snap_offset; // bytes: C snapshot[27 n_noslip] of the list's post-collision values
     uint64_t pressure_offset;    // bytes: int32 k[n], int32 kN[n], int32 direction[n], then C drho[n]
     uint64_t pressure_rho_offset;
     uint32_t n_noslip, n_pressure;
@@ -1546,6 +1585,32 @@ struct PoolBCArgs {
     const uint32_t *n_items;
 };
 
+// the no-slip lists' post-collision populations into each domain's snapshot (bc_snapshot_kernel)
+template <class S, bool EVEN>
+__global__ void __launch_bounds__(128) pool_noslip_snapshot_kernel(PoolBCArgs<typename Codec<S>::compute> a)
+{
+    using C = typename Codec<S>::compute;
+    const uint32_t n_items = __ldg(a.n_items);
+    for (uint32_t w = blockIdx.x; w < n_items; w += gridDim.x) {
+        const uint2 it = a.items[w];
+        const PoolDomain<C> &dm = a.domains[it.x];
+        const uint32_t i = it.y + threadIdx.x;
+        if (i >= dm.n_noslip)
+            continue;
+        char *arena = static_cast<char *>(a.arena);
+        const int32_t *k = reinterpret_cast<const int32_t *>(arena + dm.noslip_offset);
+        C *snap = reinterpret_cast<C *>(arena + dm.noslip_snap_offset);
+        const NodeAddr box{ dm.nx, dm.ny, dm.nz, dm.flags & 7 };
+        uint32_t nodes[8];
+        box_nodes((uint32_t)k[i], box, nodes);
+        C p[27];
+        gather_post<S, EVEN>(static_cast<const S *>(a.arena) + dm.dist_offset, dm.pitch, nodes, p);
+#pragma unroll
+        for (int d = 0; d < 27; ++d)
+            snap[(uint64_t)d * dm.n_noslip + i] = p[d];
+    }
+}
+
 template <class S, bool EVEN>
 __global__ void __launch_bounds__(128) pool_noslip_kernel(PoolBCArgs<typename Codec<S>::compute> a)
 {
@@ -1563,8 +1628,10 @@ __global__ void __launch_bounds__(128) pool_noslip_kernel(PoolBCArgs<typename Co
         const NodeAddr box{ dm.nx, dm.ny, dm.nz, dm.flags & 7 };
         uint32_t nodes[8];
         box_nodes((uint32_t)k[i], box, nodes);
+        const C *snap = reinterpret_cast<const C *>(arena + dm.noslip_snap_offset) + i;
         bc_interpolated_node<S, EVEN, false, kBCCompressible>(static_cast<S *>(a.arena) + dm.dist_offset, dm.pitch,
-                                                              nodes, q + i, dm.n_noslip, dm.omega, C(0), C(0), C(0));
+                                                              nodes, q + i, dm.n_noslip, dm.omega, C(0), C(0), C(0),
+                                                              snap, dm.n_noslip);
     }
 }
 

@@ -126,7 +126,8 @@ cudaError_t Launchers<S>::k17_list_staged(const vfb_level *L, const uint32_t *sl
 }
 
 template <class S>
-cudaError_t Launchers<S>::bc(const vfb_level *L, const vfb_bc *bc, int kind, cudaStream_t s, const NodeAddr *box)
+cudaError_t Launchers<S>::bc(const vfb_level *L, const vfb_bc *bc, int kind, cudaStream_t s, const NodeAddr *box,
+                             void *snap)
 {
     if (bc->number_of_bc_nodes == 0)
         return cudaSuccess;
@@ -144,8 +145,15 @@ cudaError_t Launchers<S>::bc(const vfb_level *L, const vfb_bc *bc, int kind, cud
     a.uy = bc->vy;
     a.uz = bc->vz;
     a.omega = L->omega;
+    a.snap = nullptr;
     const unsigned B = 128, G = grid1d(a.nbc, B);
     const bool even = L->is_even_timestep != 0;
+    if (snap) {
+        using C = typename Codec<S>::compute;
+        if (even) bc_snapshot_kernel<S, true><<<G, B, 0, s>>>(a, static_cast<C *>(snap));
+        else bc_snapshot_kernel<S, false><<<G, B, 0, s>>>(a, static_cast<C *>(snap));
+        a.snap = snap;
+    }
     switch (kind) {
     case kNoSlipBB:
         if (even) bc_bounce_back_kernel<S, true, false><<<G, B, 0, s>>>(a);
@@ -278,6 +286,7 @@ void Launchers<S>::pool_domain(void *out, const PoolDomainSpec &spec)
     d.omega = spec.omega;
     d.noslip_offset = spec.noslip_offset;
     d.noslip_q_offset = spec.noslip_q_offset;
+    d.noslip_snap_offset = spec.noslip_snap_offset;
     d.pressure_offset = spec.pressure_offset;
     d.pressure_rho_offset = spec.pressure_rho_offset;
     d.n_noslip = spec.n_noslip;
@@ -315,6 +324,8 @@ cudaError_t Launchers<S>::pool_bcs(void *arena, const void *domains, const uint2
     if (noslip_items) {
         a.items = noslip_items;
         a.n_items = n_noslip_items;
+        if (even) pool_noslip_snapshot_kernel<S, true><<<grid, 128, 0, s>>>(a);
+        else pool_noslip_snapshot_kernel<S, false><<<grid, 128, 0, s>>>(a);
         if (even) pool_noslip_kernel<S, true><<<grid, 128, 0, s>>>(a);
         else pool_noslip_kernel<S, false><<<grid, 128, 0, s>>>(a);
         const cudaError_t e = cudaGetLastError();

@@ -335,7 +335,7 @@ cudaError_t launch_step(vfb_pool *p, bool even, cudaStream_t s)
     cudaError_t e = p->ops.collide(p->arena, p->domain_table, p->items, p->n_items, p->nodes_per_thread, even, p->grid,
                                    (unsigned)p->threads, s);
     if (e == cudaSuccess && (p->has_noslip || p->has_pressure)) {
-        p->launches += (p->has_noslip ? 1 : 0) + (p->has_pressure ? 1 : 0);
+        p->launches += (p->has_noslip ? 2 : 0) + (p->has_pressure ? 1 : 0);   // snapshot + no-slip, pressure
         e = p->ops.bcs(p->arena, p->domain_table, p->has_noslip ? p->noslip_list.items : nullptr,
                        p->noslip_list.count, p->has_pressure ? p->pressure_list.items : nullptr,
                        p->pressure_list.count, even, p->bc_grid, s);
@@ -345,7 +345,7 @@ cudaError_t launch_step(vfb_pool *p, bool even, cudaStream_t s)
 
 uint32_t launches_per_step(const vfb_pool *p)
 {
-    return 1u + (p->has_noslip ? 1u : 0u) + (p->has_pressure ? 1u : 0u);
+    return 1u + (p->has_noslip ? 2u : 0u) + (p->has_pressure ? 1u : 0u);
 }
 
 // kGraphSteps steps starting at the even parity, captured once and replayed
@@ -444,8 +444,8 @@ void domain_sizes(const vfb_pool *p, const vfb_domain_desc *d, bool has_mask, ui
 
 // arena bytes of a domain's BC lists: no-slip k and q27, pressure k, kN, direction and drho
 struct BCSizes {
-    uint64_t noslip_k, noslip_q, pressure_i, pressure_rho;
-    uint64_t total() const { return noslip_k + noslip_q + pressure_i + pressure_rho; }
+    uint64_t noslip_k, noslip_q, noslip_snap, pressure_i, pressure_rho;
+    uint64_t total() const { return noslip_k + noslip_q + noslip_snap + pressure_i + pressure_rho; }
 };
 
 BCSizes bc_sizes(const vfb_pool *p, uint32_t n_noslip, uint32_t n_pressure)
@@ -454,6 +454,7 @@ BCSizes bc_sizes(const vfb_pool *p, uint32_t n_noslip, uint32_t n_pressure)
     BCSizes b;
     b.noslip_k = n_noslip ? align_up(4ull * n_noslip) : 0;
     b.noslip_q = n_noslip ? align_up(27ull * n_noslip * rs) : 0;
+    b.noslip_snap = b.noslip_q;      // the list's post-collision values, taken before its BC writes
     b.pressure_i = n_pressure ? align_up(12ull * n_pressure) : 0;
     b.pressure_rho = n_pressure ? align_up((uint64_t)n_pressure * rs) : 0;
     return b;
@@ -646,7 +647,8 @@ int vfb_pool_add_domain_with_bcs(vfb_pool *p, const vfb_domain_desc *d, const ui
     vfb::PoolDomainSpec spec{};
     spec.noslip_offset = off + pop + mask;
     spec.noslip_q_offset = spec.noslip_offset + bs.noslip_k;
-    spec.pressure_offset = spec.noslip_q_offset + bs.noslip_q;
+    spec.noslip_snap_offset = spec.noslip_q_offset + bs.noslip_q;
+    spec.pressure_offset = spec.noslip_snap_offset + bs.noslip_snap;
     spec.pressure_rho_offset = spec.pressure_offset + bs.pressure_i;
     char *arena = static_cast<char *>(p->arena);
     cudaError_t e = cudaSuccess;

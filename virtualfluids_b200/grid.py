@@ -232,6 +232,34 @@ class ListGrid:
         self.bcs.append(bc)
         return bc
 
+    def add_sphere_obstacle(self, centre, radius, kind="geometry"):
+        """A solid sphere (fluid-box coordinates). Nodes with |p - centre| <= radius become solid and
+        leave the fluid list; every fluid node with a link that enters the sphere within one link
+        length gets that link's q (Sphere::getIntersection, geometries/Sphere/Sphere.cpp:124-169, the
+        smallest non-negative root kept when 0 <= q <= 1, GridImp::calculateQs, GridImp.cpp:1561-1600).
+        Those nodes form a BC list of the given kind. Periodic images of the sphere are not added."""
+        from .workloads import sphere_link_q
+        c = np.asarray(centre, dtype=np.float64)
+        r = float(radius)
+        pos = self.coords.astype(np.float64)
+        d2 = ((pos - c[:, None]) ** 2).sum(axis=0)
+        inside = d2 <= r * r
+        inside[0] = False
+        solid = inside & (self.geo == N.GEO_FLUID)
+        self.geo = np.where(solid, N.GEO_SOLID, self.geo).astype(np.uint32)
+        self.fluid = np.nonzero(self.geo == N.GEO_FLUID)[0].astype(np.uint32)
+        for b in self.bcs:
+            keep = ~solid[b.k]
+            b.k, b.q = b.k[keep], b.q[:, keep]
+            if b.k_neighbor is not None:
+                b.k_neighbor = b.k_neighbor[keep]
+        near = self.fluid[d2[self.fluid] <= (r + 1.8) ** 2].astype(np.int64)
+        q = sphere_link_q(pos[:, near].T, c, r)
+        cut = (q >= 0).any(axis=0)
+        bc = SideBC(side="obstacle", kind=kind, k=near[cut].astype(np.int32), q=q[:, cut])
+        self.bcs.append(bc)
+        return bc
+
     def merged(self, kind):
         """All BCs of one kind concatenated, as allocArrays_BoundaryValues fills one struct per kind."""
         parts = [b for b in self.bcs if b.kind == kind]
