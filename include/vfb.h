@@ -435,7 +435,10 @@ int vfb_pool_add_domain(vfb_pool *pool, const vfb_domain_desc *desc, const uint8
    (NoSlipInterpolatedCompressible, NoSlipInterpolatedCompressible.cu:44-381), the pressure list after
    the parity swap (PressureNonEquilibriumCompressible, PressureNonEquilibriumCompressible.cu:45-314,
    one outward normal per node, so inlet and outlet share a list). Other variants give
-   VFB_ERR_UNSUPPORTED. A domain computes what a vfb_box with the same lists computes. */
+   VFB_ERR_UNSUPPORTED. A domain computes what a vfb_box with the same lists computes. Where a
+   link joins two no-slip nodes and is cut from both ends (curved geometry), the values each reads
+   and the other overwrites are saved before the writes (a per-node direction mask built here), so
+   the result does not depend on thread order. */
 typedef struct vfb_domain_bcs {
     int32_t noslip_variant;           /* VFB_NOSLIP_INTERPOLATED_COMPRESSIBLE */
     const int32_t *noslip_k;
@@ -450,8 +453,9 @@ typedef struct vfb_domain_bcs {
 } vfb_domain_bcs;
 int vfb_pool_add_domain_with_bcs(vfb_pool *pool, const vfb_domain_desc *desc, const uint8_t *mask,
                                  const vfb_domain_bcs *bcs, uint32_t *id);
+/* device bytes of a domain with these BC lists (NULL: none) */
 int vfb_pool_domain_bytes_with_bcs(const vfb_pool *pool, const vfb_domain_desc *desc, int32_t has_mask,
-                                   uint32_t number_of_noslip_nodes, uint32_t number_of_pressure_nodes, uint64_t *bytes);
+                                   const vfb_domain_bcs *bcs, uint64_t *bytes);
 /* the domain stops taking part in steps; its arena range and id become reusable once the pool's
    stream has drained (the next vfb_pool_step that changes the work list, or vfb_pool_synchronize).
    All calls on one pool must use one stream. */

@@ -218,7 +218,7 @@ SIGNATURES = {
     "vfb_pool_add_domain": (C.c_int, [C.c_void_p, C.POINTER(DomainDesc), C.c_void_p, C.POINTER(C.c_uint32)]),
     "vfb_pool_add_domain_with_bcs": (C.c_int, [C.c_void_p, C.POINTER(DomainDesc), C.c_void_p, C.POINTER(DomainBCs),
                                                C.POINTER(C.c_uint32)]),
-    "vfb_pool_domain_bytes_with_bcs": (C.c_int, [C.c_void_p, C.POINTER(DomainDesc), C.c_int32, C.c_uint32, C.c_uint32,
+    "vfb_pool_domain_bytes_with_bcs": (C.c_int, [C.c_void_p, C.POINTER(DomainDesc), C.c_int32, C.POINTER(DomainBCs),
                                                  C.POINTER(C.c_uint64)]),
     "vfb_pool_remove_domain": (C.c_int, [C.c_void_p, C.c_uint32]),
     "vfb_pool_synchronize": (C.c_int, [C.c_void_p, C.c_void_p]),

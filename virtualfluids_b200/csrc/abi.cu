@@ -8,6 +8,7 @@
 #include <string>
 #include <vector>
 
+#include "guards.h"
 #include "k17.cuh"
 #include "launch.h"
 #include "vfb.h"
@@ -1247,7 +1248,8 @@ struct vfb_box {
         vfb_bc_fn fn = nullptr;
         int kind = -1;              // vfb::BCKind, -1 = no kernel
         std::vector<void *> owned;
-        void *snap = nullptr;       // post-collision values of the list, taken before its writes
+        uint32_t *guard = nullptr;  // guard table of the list (guards.h), nullptr when nothing is guarded
+        void *saved = nullptr;      // the guarded values, saved before the list writes
     } velocity, noslip, geometry;
     struct Pressure {
         vfb_directional_bc bc{};
@@ -1448,9 +1450,9 @@ cudaError_t box_run_list(vfb_box *b, const vfb_box::List &l, cudaStream_t s)
     const vfb_level L = box_level(b);
     const vfb::NodeAddr a = box_addr(b);
     ++b->launches;
-    if (l.snap)
+    if (l.guard)
         ++b->launches;
-    return VFB_DISPATCH(b->desc.storage, b->desc.arith, LA::bc(&L, &l.bc, l.kind, s, &a, l.snap));
+    return VFB_DISPATCH(b->desc.storage, b->desc.arith, LA::bc(&L, &l.bc, l.kind, s, &a, nullptr, l.guard, l.saved));
 }
 
 // one step's boundary work around the collision, in the order of vfb_simulation_run
@@ -1645,14 +1647,28 @@ int vfb_box_set_bc(vfb_box *box, int32_t kind, int32_t variant, const int32_t *k
         box->drag_history = nullptr;
     }
     const size_t rb = real_bytes(box->desc.storage);
-    void *dk = nullptr, *dq = nullptr, *dv = nullptr, *ds = nullptr;
+    void *dk = nullptr, *dq = nullptr, *dv = nullptr, *dg = nullptr, *ds = nullptr;
     cudaError_t e = cudaSuccess;
+    // links cut from both ends between nodes of this list: which post-collision values to save
+    std::vector<uint32_t> table;
+    const int periodic = (box->desc.periodic_x ? 1 : 0) | (box->desc.periodic_y ? 2 : 0) | (box->desc.periodic_z ? 4 : 0);
+    uint32_t n_saved = 0;
+    if (n)
+        n_saved = rb == 8 ? vfb::bc_guard_tables(k, static_cast<const double *>(q27), n, box->desc.nx, box->desc.ny,
+                                                 box->desc.nz, periodic, table)
+                          : vfb::bc_guard_tables(k, static_cast<const float *>(q27), n, box->desc.nx, box->desc.ny,
+                                                 box->desc.nz, periodic, table);
     if (n) {
         e = cudaMalloc(&dk, n * sizeof(int32_t));
         if (e == cudaSuccess)
             e = cudaMemcpy(dk, k, n * sizeof(int32_t), cudaMemcpyHostToDevice);
-        if (e == cudaSuccess)
-            e = cudaMalloc(&ds, (size_t)27 * n * rb);   // the list's snapshot of post-collision values
+        if (e == cudaSuccess && n_saved) {
+            e = cudaMalloc(&dg, table.size() * sizeof(uint32_t));
+            if (e == cudaSuccess)
+                e = cudaMemcpy(dg, table.data(), table.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+            if (e == cudaSuccess)
+                e = cudaMalloc(&ds, (size_t)n_saved * rb);
+        }
         if (e == cudaSuccess)
             e = cudaMalloc(&dq, (size_t)27 * n * rb);
         if (e == cudaSuccess)
@@ -1668,11 +1684,13 @@ int vfb_box_set_bc(vfb_box *box, int32_t kind, int32_t variant, const int32_t *k
         cudaFree(dk);
         cudaFree(dq);
         cudaFree(dv);
+        cudaFree(dg);
         cudaFree(ds);
         return cuda_status(e, "box BC upload");
     }
-    l.owned = { dk, dq, dv, ds };
-    l.snap = ds;
+    l.owned = { dk, dq, dv, dg, ds };
+    l.guard = static_cast<uint32_t *>(dg);
+    l.saved = ds;
     l.bc.k = static_cast<const int32_t *>(dk);
     l.bc.q27 = dq;
     l.bc.number_of_bc_nodes = n;

@@ -71,6 +71,8 @@ struct BCArgs {
     double omega;
     const void *snap;           // optional: the list's post-collision populations taken before any BC
                                 // write, snap[d * nbc + i] (compute type); read instead of the slots
+    const uint32_t *guard;      // optional guard table (guards.h): mask[i], then first[nbc + i]
+    const void *saved;          // the guarded values, saved before the list's writes (compute type)
 };
 
 struct PressureArgs {
@@ -777,6 +779,15 @@ __global__ void __launch_bounds__(128) bc_bounce_back_kernel(BCArgs a)
             post[d] = static_cast<const C *>(a.snap)[(uint64_t)d * a.nbc + i];
     } else {
         gather_post<S, EVEN>(base, a.n, nodes, post);
+        const uint32_t mask = a.guard ? a.guard[i] : 0u;
+        if (mask) {
+            const C *saved = static_cast<const C *>(a.saved) + a.guard[a.nbc + i];
+            int r = 0;
+#pragma unroll
+            for (int d = 1; d < 27; ++d)
+                if ((mask >> d) & 1u)
+                    post[d] = saved[r++];
+        }
     }
     const C *q27 = static_cast<const C *>(a.q27);
     C ux = C(0), uy = C(0), uz = C(0);
@@ -852,7 +863,8 @@ __device__ __forceinline__ void bc_interpolated_node(S *base, uint64_t n, const 
                                                      double omega_real, typename Codec<S>::compute bx,
                                                      typename Codec<S>::compute by, typename Codec<S>::compute bz,
                                                      const typename Codec<S>::compute *snap = nullptr,
-                                                     uint64_t snap_stride = 0)
+                                                     uint64_t snap_stride = 0, uint32_t guard_mask = 0,
+                                                     const typename Codec<S>::compute *guard = nullptr)
 {
     using C = typename Codec<S>::compute;
     C p[27];
@@ -862,6 +874,14 @@ __device__ __forceinline__ void bc_interpolated_node(S *base, uint64_t n, const 
             p[d] = snap[(uint64_t)d * snap_stride];
     } else {
         gather_post<S, EVEN>(base, n, nodes, p);
+        // directions whose slot another node of the list overwrites: the value saved before
+        if (guard_mask) {
+            int r = 0;
+#pragma unroll
+            for (int d = 1; d < 27; ++d)
+                if ((guard_mask >> d) & 1u)
+                    p[d] = guard[r++];
+        }
     }
     // plain-sum density and grouped momenta (NoSlipInterpolatedCompressible.cu:134-153)
     const C drho = p[21] + p[20] + p[19] + p[22] + p[25] + p[24] + p[23] + p[26] + p[17] + p[18] + p[15] + p[16] + p[13]
@@ -923,9 +943,32 @@ __global__ void __launch_bounds__(128) bc_interpolated_kernel(BCArgs a)
         bz = static_cast<const C *>(a.uz)[i];
     }
     const C *snap = a.snap ? static_cast<const C *>(a.snap) + i : nullptr;
+    const uint32_t mask = a.guard ? a.guard[i] : 0u;
+    const C *saved = mask ? static_cast<const C *>(a.saved) + a.guard[a.nbc + i] : nullptr;
     bc_interpolated_node<S, EVEN, VELOCITY, FORM>(static_cast<S *>(a.dist), a.n, nodes,
                                                   static_cast<const C *>(a.q27) + i, a.nbc, a.omega, bx, by, bz,
-                                                  snap, a.nbc);
+                                                  snap, a.nbc, mask, saved);
+}
+
+// the guarded post-collision values of a list (guards.h), saved before the list's BC kernel writes
+template <class S, bool EVEN>
+__global__ void __launch_bounds__(128) bc_guard_kernel(BCArgs a, typename Codec<S>::compute *saved)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.nbc)
+        return;
+    const uint32_t mask = a.guard[i];
+    if (!mask)
+        return;
+    uint32_t nodes[8];
+    node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.box, nodes);
+    const S *base = static_cast<const S *>(a.dist);
+    typename Codec<S>::compute *out = saved + a.guard[a.nbc + i];
+    int r = 0;
+#pragma unroll
+    for (int d = 1; d < 27; ++d)
+        if ((mask >> d) & 1u)
+            out[r++] = Codec<S>::load(base + (uint64_t)plane<EVEN>(inv(d)) * a.n + nodes[shift_class(inv(d))], d);
 }
 
 // The post-collision populations of every node of a BC list into snap[d * nbc + i], taken before
@@ -1470,7 +1513,8 @@ struct PoolDomain {
     double omega;                // the BC kernels' omega
     uint64_t noslip_offset;      // bytes from the arena start: int32 k[n_noslip], then C q27[27 n_noslip]
     uint64_t noslip_q_offset;
-    uint64_t noslip_snap_offset; // bytes: C snapshot[27 n_noslip] of the list's post-collision values
+    uint64_t noslip_guard_offset; // bytes: uint32 mask[n_noslip], uint32 first[n_noslip] (guarded directions)
+    uint64_t noslip_saved_offset; // bytes: C saved[] (their post-collision values, taken before the writes)
     uint64_t pressure_offset;    // bytes: int32 k[n], int32 kN[n], int32 direction[n], then C drho[n]
     uint64_t pressure_rho_offset;
     uint32_t n_noslip, n_pressure;
@@ -1585,9 +1629,12 @@ struct PoolBCArgs {
     const uint32_t *n_items;
 };
 
-// the no-slip lists' post-collision populations into each domain's snapshot (bc_snapshot_kernel)
+// Links cut from both ends (two BC nodes of one list joined by a link that clips the geometry):
+// each node's write lands in the slot the other reads. Before the no-slip kernel writes anything,
+// the values in those slots (bit d of a node's mask: its post-collision population d) are saved,
+// and the no-slip kernel reads them from there, so every node sees the collision's values.
 template <class S, bool EVEN>
-__global__ void __launch_bounds__(128) pool_noslip_snapshot_kernel(PoolBCArgs<typename Codec<S>::compute> a)
+__global__ void __launch_bounds__(128) pool_noslip_guard_kernel(PoolBCArgs<typename Codec<S>::compute> a)
 {
     using C = typename Codec<S>::compute;
     const uint32_t n_items = __ldg(a.n_items);
@@ -1598,16 +1645,21 @@ __global__ void __launch_bounds__(128) pool_noslip_snapshot_kernel(PoolBCArgs<ty
         if (i >= dm.n_noslip)
             continue;
         char *arena = static_cast<char *>(a.arena);
+        const uint32_t *guard = reinterpret_cast<const uint32_t *>(arena + dm.noslip_guard_offset);
+        const uint32_t mask = guard[i];
+        if (!mask)
+            continue;
         const int32_t *k = reinterpret_cast<const int32_t *>(arena + dm.noslip_offset);
-        C *snap = reinterpret_cast<C *>(arena + dm.noslip_snap_offset);
+        C *saved = reinterpret_cast<C *>(arena + dm.noslip_saved_offset) + guard[dm.n_noslip + i];
         const NodeAddr box{ dm.nx, dm.ny, dm.nz, dm.flags & 7 };
         uint32_t nodes[8];
         box_nodes((uint32_t)k[i], box, nodes);
-        C p[27];
-        gather_post<S, EVEN>(static_cast<const S *>(a.arena) + dm.dist_offset, dm.pitch, nodes, p);
+        const S *base = static_cast<const S *>(a.arena) + dm.dist_offset;
+        int r = 0;
 #pragma unroll
-        for (int d = 0; d < 27; ++d)
-            snap[(uint64_t)d * dm.n_noslip + i] = p[d];
+        for (int d = 1; d < 27; ++d)
+            if ((mask >> d) & 1u)
+                saved[r++] = Codec<S>::load(base + (uint64_t)plane<EVEN>(inv(d)) * dm.pitch + nodes[shift_class(inv(d))], d);
     }
 }
 
@@ -1628,10 +1680,13 @@ __global__ void __launch_bounds__(128) pool_noslip_kernel(PoolBCArgs<typename Co
         const NodeAddr box{ dm.nx, dm.ny, dm.nz, dm.flags & 7 };
         uint32_t nodes[8];
         box_nodes((uint32_t)k[i], box, nodes);
-        const C *snap = reinterpret_cast<const C *>(arena + dm.noslip_snap_offset) + i;
+        const uint32_t *guard = reinterpret_cast<const uint32_t *>(arena + dm.noslip_guard_offset);
+        const uint32_t mask = guard[i];
+        const C *saved = mask ? reinterpret_cast<const C *>(arena + dm.noslip_saved_offset) + guard[dm.n_noslip + i]
+                              : nullptr;
         bc_interpolated_node<S, EVEN, false, kBCCompressible>(static_cast<S *>(a.arena) + dm.dist_offset, dm.pitch,
                                                               nodes, q + i, dm.n_noslip, dm.omega, C(0), C(0), C(0),
-                                                              snap, dm.n_noslip);
+                                                              nullptr, 0, mask, saved);
     }
 }
 

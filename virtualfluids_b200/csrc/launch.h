@@ -53,7 +53,8 @@ struct PoolDomainSpec {
     double omega;
     double lim[3];
     double half_force[3];
-    uint64_t noslip_offset, noslip_q_offset, noslip_snap_offset, pressure_offset, pressure_rho_offset;
+    uint64_t noslip_offset, noslip_q_offset, noslip_guard_offset, noslip_saved_offset, pressure_offset,
+        pressure_rho_offset;
     uint32_t n_noslip, n_pressure;
 };
 
@@ -65,7 +66,8 @@ struct PoolDomainSpec {
         static cudaError_t k17_list_staged(const vfb_level *L, const uint32_t *slots, uint64_t slots_stride,       \
                                            uint32_t n, int *status, cudaStream_t s);                               \
         static cudaError_t bc(const vfb_level *L, const vfb_bc *bc, int kind, cudaStream_t s,                        \
-                              const NodeAddr *box = nullptr, void *snap = nullptr);                                  \
+                              const NodeAddr *box = nullptr, void *snap = nullptr,                                   \
+                              const uint32_t *guard = nullptr, void *saved = nullptr);                               \
         static cudaError_t pressure(const vfb_level *L, const vfb_directional_bc *bc, cudaStream_t s,                \
                                     const NodeAddr *box = nullptr, int kind = 0);                                    \
         static cudaError_t inlet_perturbation(const void *base, void *vel, uint32_t n, uint64_t seed,                \

@@ -127,7 +127,7 @@ cudaError_t Launchers<S>::k17_list_staged(const vfb_level *L, const uint32_t *sl
 
 template <class S>
 cudaError_t Launchers<S>::bc(const vfb_level *L, const vfb_bc *bc, int kind, cudaStream_t s, const NodeAddr *box,
-                             void *snap)
+                             void *snap, const uint32_t *guard, void *saved)
 {
     if (bc->number_of_bc_nodes == 0)
         return cudaSuccess;
@@ -146,13 +146,20 @@ cudaError_t Launchers<S>::bc(const vfb_level *L, const vfb_bc *bc, int kind, cud
     a.uz = bc->vz;
     a.omega = L->omega;
     a.snap = nullptr;
+    a.guard = nullptr;
+    a.saved = nullptr;
     const unsigned B = 128, G = grid1d(a.nbc, B);
     const bool even = L->is_even_timestep != 0;
+    using C = typename Codec<S>::compute;
     if (snap) {
-        using C = typename Codec<S>::compute;
         if (even) bc_snapshot_kernel<S, true><<<G, B, 0, s>>>(a, static_cast<C *>(snap));
         else bc_snapshot_kernel<S, false><<<G, B, 0, s>>>(a, static_cast<C *>(snap));
         a.snap = snap;
+    } else if (guard) {
+        a.guard = guard;
+        if (even) bc_guard_kernel<S, true><<<G, B, 0, s>>>(a, static_cast<C *>(saved));
+        else bc_guard_kernel<S, false><<<G, B, 0, s>>>(a, static_cast<C *>(saved));
+        a.saved = saved;
     }
     switch (kind) {
     case kNoSlipBB:
@@ -286,7 +293,8 @@ void Launchers<S>::pool_domain(void *out, const PoolDomainSpec &spec)
     d.omega = spec.omega;
     d.noslip_offset = spec.noslip_offset;
     d.noslip_q_offset = spec.noslip_q_offset;
-    d.noslip_snap_offset = spec.noslip_snap_offset;
+    d.noslip_guard_offset = spec.noslip_guard_offset;
+    d.noslip_saved_offset = spec.noslip_saved_offset;
     d.pressure_offset = spec.pressure_offset;
     d.pressure_rho_offset = spec.pressure_rho_offset;
     d.n_noslip = spec.n_noslip;
@@ -324,8 +332,8 @@ cudaError_t Launchers<S>::pool_bcs(void *arena, const void *domains, const uint2
     if (noslip_items) {
         a.items = noslip_items;
         a.n_items = n_noslip_items;
-        if (even) pool_noslip_snapshot_kernel<S, true><<<grid, 128, 0, s>>>(a);
-        else pool_noslip_snapshot_kernel<S, false><<<grid, 128, 0, s>>>(a);
+        if (even) pool_noslip_guard_kernel<S, true><<<grid, 128, 0, s>>>(a);
+        else pool_noslip_guard_kernel<S, false><<<grid, 128, 0, s>>>(a);
         if (even) pool_noslip_kernel<S, true><<<grid, 128, 0, s>>>(a);
         else pool_noslip_kernel<S, false><<<grid, 128, 0, s>>>(a);
         const cudaError_t e = cudaGetLastError();

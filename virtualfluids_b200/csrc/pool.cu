@@ -14,6 +14,7 @@
 #include <string>
 #include <vector>
 
+#include "guards.h"
 #include "launch.h"
 #include "vfb.h"
 
@@ -444,20 +445,35 @@ void domain_sizes(const vfb_pool *p, const vfb_domain_desc *d, bool has_mask, ui
 
 // arena bytes of a domain's BC lists: no-slip k and q27, pressure k, kN, direction and drho
 struct BCSizes {
-    uint64_t noslip_k, noslip_q, noslip_snap, pressure_i, pressure_rho;
-    uint64_t total() const { return noslip_k + noslip_q + noslip_snap + pressure_i + pressure_rho; }
+    uint64_t noslip_k, noslip_q, noslip_guard, noslip_saved, pressure_i, pressure_rho;
+    uint64_t total() const { return noslip_k + noslip_q + noslip_guard + noslip_saved + pressure_i + pressure_rho; }
 };
 
-BCSizes bc_sizes(const vfb_pool *p, uint32_t n_noslip, uint32_t n_pressure)
+BCSizes bc_sizes(const vfb_pool *p, uint32_t n_noslip, uint32_t n_saved, uint32_t n_pressure)
 {
     const uint64_t rs = real_size(p->desc.storage);
     BCSizes b;
     b.noslip_k = n_noslip ? align_up(4ull * n_noslip) : 0;
     b.noslip_q = n_noslip ? align_up(27ull * n_noslip * rs) : 0;
-    b.noslip_snap = b.noslip_q;      // the list's post-collision values, taken before its BC writes
+    b.noslip_guard = n_noslip ? align_up(8ull * n_noslip) : 0;
+    b.noslip_saved = n_saved ? align_up((uint64_t)n_saved * rs) : 0;
     b.pressure_i = n_pressure ? align_up(12ull * n_pressure) : 0;
     b.pressure_rho = n_pressure ? align_up((uint64_t)n_pressure * rs) : 0;
     return b;
+}
+
+// the guard tables of a domain's no-slip list (guards.h)
+uint32_t guard_tables(const vfb_domain_desc *d, const vfb_domain_bcs *b, std::vector<uint32_t> &mask,
+                      std::vector<uint32_t> &first)
+{
+    const uint32_t n = b ? b->number_of_noslip_nodes : 0;
+    std::vector<uint32_t> table;
+    const int periodic = (d->periodic_x ? 1 : 0) | (d->periodic_y ? 2 : 0) | (d->periodic_z ? 4 : 0);
+    const uint32_t saved = n ? vfb::bc_guard_tables(b->noslip_k, b->noslip_q27, n, d->nx, d->ny, d->nz, periodic, table)
+                             : 0;
+    mask.assign(table.begin(), table.begin() + n);
+    first.assign(table.begin() + n, table.end());
+    return saved;
 }
 
 bool is_axis_direction(int32_t d) { return d >= VFB_DIR_P00 && d <= VFB_DIR_00M; }
@@ -556,20 +572,26 @@ int vfb_pool_destroy(vfb_pool *p)
 
 int vfb_pool_domain_bytes(const vfb_pool *p, const vfb_domain_desc *d, int32_t has_mask, uint64_t *bytes)
 {
-    return vfb_pool_domain_bytes_with_bcs(p, d, has_mask, 0, 0, bytes);
+    return vfb_pool_domain_bytes_with_bcs(p, d, has_mask, nullptr, bytes);
 }
 
 int vfb_pool_domain_bytes_with_bcs(const vfb_pool *p, const vfb_domain_desc *d, int32_t has_mask,
-                                   uint32_t number_of_noslip_nodes, uint32_t number_of_pressure_nodes, uint64_t *bytes)
+                                   const vfb_domain_bcs *bcs, uint64_t *bytes)
 {
     if (!p || !bytes)
         return pool_fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
-    const int st = check_desc(d);
+    int st = check_desc(d);
+    if (st)
+        return st;
+    st = check_bcs(bcs, d, nullptr);
     if (st)
         return st;
     uint64_t pitch, pop, mask;
     domain_sizes(p, d, needs_mask(d, has_mask != 0), pitch, pop, mask);
-    *bytes = pop + mask + bc_sizes(p, number_of_noslip_nodes, number_of_pressure_nodes).total();
+    std::vector<uint32_t> gm, gf;
+    const uint32_t n_saved = guard_tables(d, bcs, gm, gf);
+    *bytes = pop + mask + bc_sizes(p, bcs ? bcs->number_of_noslip_nodes : 0, n_saved,
+                                   bcs ? bcs->number_of_pressure_nodes : 0).total();
     return VFB_OK;
 }
 
@@ -634,9 +656,11 @@ int vfb_pool_add_domain_with_bcs(vfb_pool *p, const vfb_domain_desc *d, const ui
         return st;
     ds.n_noslip = bcs ? bcs->number_of_noslip_nodes : 0;
     ds.n_pressure = bcs ? bcs->number_of_pressure_nodes : 0;
+    std::vector<uint32_t> guard_mask, guard_first;
+    const uint32_t n_saved = guard_tables(d, bcs, guard_mask, guard_first);
     uint64_t pop, mask;
     domain_sizes(p, d, ds.has_mask, ds.pitch, pop, mask);
-    const BCSizes bs = bc_sizes(p, ds.n_noslip, ds.n_pressure);
+    const BCSizes bs = bc_sizes(p, ds.n_noslip, n_saved, ds.n_pressure);
     uint64_t off = 0;
     if (!p->alloc.take(pop + mask + bs.total(), off))
         return pool_fail(VFB_ERR_OUT_OF_MEMORY, "the pool's arena has no room for this domain");
@@ -647,8 +671,9 @@ int vfb_pool_add_domain_with_bcs(vfb_pool *p, const vfb_domain_desc *d, const ui
     vfb::PoolDomainSpec spec{};
     spec.noslip_offset = off + pop + mask;
     spec.noslip_q_offset = spec.noslip_offset + bs.noslip_k;
-    spec.noslip_snap_offset = spec.noslip_q_offset + bs.noslip_q;
-    spec.pressure_offset = spec.noslip_snap_offset + bs.noslip_snap;
+    spec.noslip_guard_offset = spec.noslip_q_offset + bs.noslip_q;
+    spec.noslip_saved_offset = spec.noslip_guard_offset + bs.noslip_guard;
+    spec.pressure_offset = spec.noslip_saved_offset + bs.noslip_saved;
     spec.pressure_rho_offset = spec.pressure_offset + bs.pressure_i;
     char *arena = static_cast<char *>(p->arena);
     cudaError_t e = cudaSuccess;
@@ -660,6 +685,12 @@ int vfb_pool_add_domain_with_bcs(vfb_pool *p, const vfb_domain_desc *d, const ui
             const auto q = to_real(p, bcs->noslip_q27, 27ull * ds.n_noslip);
             e = cudaMemcpy(arena + spec.noslip_q_offset, q.data(), q.size(), cudaMemcpyHostToDevice);
         }
+        if (e == cudaSuccess)
+            e = cudaMemcpy(arena + spec.noslip_guard_offset, guard_mask.data(), 4ull * ds.n_noslip,
+                           cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(arena + spec.noslip_guard_offset + 4ull * ds.n_noslip, guard_first.data(),
+                           4ull * ds.n_noslip, cudaMemcpyHostToDevice);
     }
     if (e == cudaSuccess && ds.n_pressure) {
         const uint64_t n4 = 4ull * ds.n_pressure;

@@ -102,7 +102,9 @@ struct Codec<__half> {
         base[off0] = __ushort_as_half((unsigned short)(h >> 16));
         base[off1] = __ushort_as_half((unsigned short)(h & 0xffffu));
     }
-    __device__ __forceinline__ static float load(const __half *p, int d) { return __half2float(*p) * float(weight(d)); }
+    // the decoding product is rounded on its own (never fused into a later addition), so a decoded
+    // value is the same float wherever it is used or saved
+    __device__ __forceinline__ static float load(const __half *p, int d) { return __fmul_rn(__half2float(*p), float(weight(d))); }
     __device__ __forceinline__ static void store_at(__half *base, uint64_t off, float v, int d)
     {
         const float s = v * float(1.0 / weight(d));
@@ -124,7 +126,7 @@ struct Codec<__nv_bfloat16> {
     }
     __device__ __forceinline__ static float load(const __nv_bfloat16 *p, int d)
     {
-        return __bfloat162float(*p) * float(weight(d));
+        return __fmul_rn(__bfloat162float(*p), float(weight(d)));   // rounded on its own, as for FP16
     }
     __device__ __forceinline__ static void store_at(__nv_bfloat16 *base, uint64_t off, float v, int d)
     {

@@ -59,11 +59,13 @@ class Pool:
             d.quadric_limiters[i] = float(limiters[i])
         return d
 
-    def domain_bytes(self, shape, omega=1.8, periodic=(True, True, True), has_mask=False, n_noslip=0,
-                     n_pressure=0) -> int:
+    def domain_bytes(self, shape, omega=1.8, periodic=(True, True, True), has_mask=False, bcs=None) -> int:
+        """Arena bytes of a domain of this shape with these BC lists (as for add)."""
         b = C.c_uint64()
+        st, keep = self._bcs(bcs)
         N.check(N.lib().vfb_pool_domain_bytes_with_bcs(self._h, C.byref(self.desc(shape, omega, periodic)),
-                                                       int(has_mask), int(n_noslip), int(n_pressure), C.byref(b)))
+                                                       int(has_mask), C.byref(st) if bcs else None, C.byref(b)))
+        del keep
         return b.value
 
     @staticmethod

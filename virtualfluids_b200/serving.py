@@ -235,11 +235,8 @@ def solve_alone(req: Request, storage="f32", stream=None):
     import torch
     s = stream or torch.cuda.Stream()
     g = req.geometry()
-    bcs = g["bcs"] or {}
-    n_ns = len(bcs["noslip"][0]) if "noslip" in bcs else 0
-    n_pr = len(bcs["pressure"][0]) if "pressure" in bcs else 0
     probe = Pool(1 << 20, storage=storage, max_domains=1)
-    need = probe.domain_bytes(g["shape"], periodic=g["periodic"], has_mask=True, n_noslip=n_ns, n_pressure=n_pr)
+    need = probe.domain_bytes(g["shape"], periodic=g["periodic"], has_mask=True, bcs=g["bcs"])
     probe.close()
     pool = Pool(need + (1 << 20), storage=storage, max_domains=1)
     d = pool.add(g["shape"], 1.0 / (3.0 * req.nu + 0.5), periodic=g["periodic"], forces=g["forces"], mask=g["mask"],
