@@ -329,13 +329,28 @@ cudaError_t Launchers<S>::pool_bcs(void *arena, const void *domains, const uint2
     PoolBCArgs<C> a;
     a.arena = arena;
     a.domains = static_cast<const PoolDomain<C> *>(domains);
+    (void)grid;
+    // persistent grids of exactly the resident blocks of each kernel: a grid one block per SM larger
+    // than the registers allow runs as a second, mostly empty wave
+    int dev = 0, sms = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    auto resident = [sms](const void *fn) {
+        int occ = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 128, 0) != cudaSuccess || occ < 1)
+            occ = 1;
+        return (unsigned)(occ * sms);
+    };
     if (noslip_items) {
         a.items = noslip_items;
         a.n_items = n_noslip_items;
-        if (even) pool_noslip_guard_kernel<S, true><<<grid, 128, 0, s>>>(a);
-        else pool_noslip_guard_kernel<S, false><<<grid, 128, 0, s>>>(a);
-        if (even) pool_noslip_kernel<S, true><<<grid, 128, 0, s>>>(a);
-        else pool_noslip_kernel<S, false><<<grid, 128, 0, s>>>(a);
+        const void *g = even ? (const void *)pool_noslip_guard_kernel<S, true>
+                             : (const void *)pool_noslip_guard_kernel<S, false>;
+        const void *k = even ? (const void *)pool_noslip_kernel<S, true> : (const void *)pool_noslip_kernel<S, false>;
+        if (even) pool_noslip_guard_kernel<S, true><<<resident(g), 128, 0, s>>>(a);
+        else pool_noslip_guard_kernel<S, false><<<resident(g), 128, 0, s>>>(a);
+        if (even) pool_noslip_kernel<S, true><<<resident(k), 128, 0, s>>>(a);
+        else pool_noslip_kernel<S, false><<<resident(k), 128, 0, s>>>(a);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess)
             return e;
@@ -344,8 +359,9 @@ cudaError_t Launchers<S>::pool_bcs(void *arena, const void *domains, const uint2
         // after the parity swap
         a.items = pressure_items;
         a.n_items = n_pressure_items;
-        if (even) pool_pressure_kernel<S, false><<<grid, 128, 0, s>>>(a);
-        else pool_pressure_kernel<S, true><<<grid, 128, 0, s>>>(a);
+        const void *k = even ? (const void *)pool_pressure_kernel<S, false> : (const void *)pool_pressure_kernel<S, true>;
+        if (even) pool_pressure_kernel<S, false><<<resident(k), 128, 0, s>>>(a);
+        else pool_pressure_kernel<S, true><<<resident(k), 128, 0, s>>>(a);
     }
     return cudaGetLastError();
 }
