@@ -444,6 +444,86 @@ def nodes_of(n):
     return n * n * n
 
 
+def run_porous(args):
+    """The serving pool's step without arrivals: porous blocks (cube sides --porous-sides, porosity
+    0.75, exact-q spheres, pressure planes along x) resident in one domain pool and advanced
+    together, FP32 and FP16 storage. The same blocks are also timed with the spheres as staircase
+    solids and no BC lists (body-force drive), which isolates the cost of the lists. Algorithmic
+    bytes per step: collision 2 x 27 values per fluid node + the node mask; no-slip list 27 gathered
+    values, 26 q and the node index and guard word per BC node + one value per cut link; pressure
+    planes 27 gathered + 18 written values and 16 bytes of row data per node."""
+    import torch
+
+    from virtualfluids_b200 import Pool
+    from virtualfluids_b200.workloads import porous_block_bcs
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    geos = [porous_block_bcs(s, 20261203 + 7 * rank + i, porosity=0.75) for i, s in enumerate(args.porous_sides)]
+    fluid = sum(int(np.count_nonzero(g["mask"])) for g in geos)
+    box_nodes = sum(int(np.prod(g["shape"])) for g in geos)
+    n_bc = sum(int(g["bcs"]["noslip"][0].size) for g in geos)
+    cut = sum(int(((g["bcs"]["noslip"][1][1:] >= 0) & (g["bcs"]["noslip"][1][1:] <= 1)).sum()) for g in geos)
+    n_pr = sum(int(g["bcs"]["pressure"][0].size) for g in geos)
+    peak, peak_src = measured_peak()
+    omega = 1.0 / (3.0 / 60.0 + 0.5)
+    out = {}
+    for storage in ("f32", "f16"):
+        rs = 4 if storage == "f32" else 2
+        parts = {"collision": 2 * 27 * rs * fluid + box_nodes,
+                 "noslip": n_bc * (27 * rs + 26 * 4 + 8) + cut * rs,
+                 "pressure": n_pr * (45 * rs + 16)}
+        res = {}
+        for lists in (True, False):
+            probe = Pool(1 << 20, storage=storage, max_domains=1)
+            need = sum(probe.domain_bytes(g["shape"], omega, periodic=(False, True, True), has_mask=True,
+                                          bcs=g["bcs"] if lists else None) for g in geos)
+            probe.close()
+            pool = Pool(need + (1 << 20), storage=storage, max_domains=len(geos))
+            for g in geos:
+                d = pool.add(g["shape"], omega, periodic=(False, True, True) if lists else (True, True, True),
+                             forces=(0.0, 0.0, 0.0) if lists else (1e-6, 0.0, 0.0), mask=g["mask"],
+                             bcs=g["bcs"] if lists else None)
+                pool.init(d, stream=stream)
+            pool.step(args.warmup, stream=stream)
+            stream.synchronize()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            l0 = pool.kernel_launches()
+            with ClockSampler(local) as clk:
+                ev0.record(stream)
+                pool.step(args.steps, stream=stream)
+                ev1.record(stream)
+                stream.synchronize()
+            ms = ev0.elapsed_time(ev1) / args.steps
+            launches = pool.kernel_launches() - l0
+            pool.close()
+            del pool
+            torch.cuda.empty_cache()
+            nbytes = sum(parts.values()) if lists else parts["collision"]
+            res["lists" if lists else "staircase"] = {
+                "ms_per_step": round(ms, 4), "mlups": round(fluid / (ms / 1e3) / 1e6, 1),
+                "algorithmic_bytes_per_step": nbytes, "achieved_gbs": round(nbytes / (ms / 1e3) / 1e9, 1),
+                "frac": round(nbytes / (ms / 1e3) / 1e9 / peak, 4), "gpu_launches": launches, "clocks": clk.summary()}
+        res["list_share_of_step"] = round(1.0 - res["staircase"]["ms_per_step"] / res["lists"]["ms_per_step"], 3)
+        res["bytes_by_part"] = parts
+        out[storage] = res
+    if rank == 0:
+        f32 = out["f32"]["lists"]
+        line = {"metric": "MLUPS (porous-block pool step with exact-q no-slip and pressure lists, FP32)",
+                "value": f32["mlups"], "unit": "MLUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": f32["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "porous blocks of the serving stream resident in one pool, no arrivals",
+                           "sides": list(args.porous_sides), "porosity": 0.75, "fluid_nodes": fluid,
+                           "box_nodes": box_nodes, "noslip_nodes": n_bc, "cut_links": cut, "pressure_nodes": n_pr,
+                           "omega": omega, "l2": "inputs larger than L2, no flush"},
+                "roofline": {"bound": "hbm", "achieved": f32["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                             "frac": f32["frac"], "peak_source": peak_src, "scope": "whole pool step"},
+                "gpu_launches": f32["gpu_launches"], "forms": out}
+        print(json.dumps(line), flush=True)
+
+
 def run_serving(args):
     """Config 5: a Poisson stream of porous-block solves served by continuous batching in one domain
     pool whose arena is the HBM budget. Offered loads are fractions of the measured capacity (node
@@ -533,13 +613,15 @@ def main():
     ap.add_argument("--arith", default="fast", choices=["fast", "exact"],
                     help="exact: every operation rounded as the reference's host build (bitwise oracle parity)")
     ap.add_argument("--kernel", default="auto", choices=["auto", "direct", "tma", "async"])
-    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "serving", "tgv-forms", "cube"],
+    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "serving", "tgv-forms", "cube", "porous"],
                     help="tgv: the headline (TGV 256^3 FP64); batch: 4096 ducts in one domain pool; "
-                         "serving: a Poisson stream of porous-block solves; tgv-forms: storage-form accuracy")
+                         "serving: a Poisson stream of porous-block solves; tgv-forms: storage-form accuracy; "
+                         "cube: duct past a wall-mounted cube; porous: the serving pool's step on fixed blocks")
     ap.add_argument("--form-steps", type=int, default=10000)
     ap.add_argument("--cube-dims", type=int, nargs=5, default=[512, 256, 256, 32, 128],
                     metavar=("NX", "NY", "NZ", "CUBE", "X0"))
     ap.add_argument("--domains", type=int, default=4096)
+    ap.add_argument("--porous-sides", type=int, nargs="+", default=[96, 128, 160, 112])
     ap.add_argument("--check-steps", type=int, default=0)
     ap.add_argument("--requests", type=int, default=32)
     ap.add_argument("--hbm-gb", type=float, default=24.0)
@@ -560,6 +642,9 @@ def main():
         return
     if args.workload == "cube":
         run_cube(args)
+        return
+    if args.workload == "porous":
+        run_porous(args)
         return
 
     import torch

@@ -107,10 +107,9 @@ __device__ __forceinline__ void list_nodes(uint32_t k, const uint32_t *__restric
 }
 
 // the eight slot nodes of a node on a structured box
-__device__ __forceinline__ void box_nodes(uint32_t k, const NodeAddr &b, uint32_t (&nodes)[8])
+__device__ __forceinline__ void box_nodes_at(uint32_t k, uint32_t x, uint32_t y, uint32_t z, const NodeAddr &b,
+                                             uint32_t (&nodes)[8])
 {
-    const uint32_t x = k % (uint32_t)b.nx, yz = k / (uint32_t)b.nx;
-    const uint32_t y = yz % (uint32_t)b.ny, z = yz / (uint32_t)b.ny;
     const int xp = ((int)x + 1 < b.nx) ? (int)x + 1 : ((b.periodic & 1) ? 0 : (int)x);
     const int yp = ((int)y + 1 < b.ny) ? (int)y + 1 : ((b.periodic & 2) ? 0 : (int)y);
     const int zp = ((int)z + 1 < b.nz) ? (int)z + 1 : ((b.periodic & 4) ? 0 : (int)z);
@@ -125,6 +124,22 @@ __device__ __forceinline__ void box_nodes(uint32_t k, const NodeAddr &b, uint32_
     nodes[5] = k + sx + sz;
     nodes[6] = k + sy + sz;
     nodes[7] = k + sx + sy + sz;
+}
+
+__device__ __forceinline__ void box_nodes(uint32_t k, const NodeAddr &b, uint32_t (&nodes)[8])
+{
+    const uint32_t x = k % (uint32_t)b.nx, yz = k / (uint32_t)b.nx;
+    const uint32_t y = yz % (uint32_t)b.ny, z = yz / (uint32_t)b.ny;
+    box_nodes_at(k, x, y, z, b, nodes);
+}
+
+// the same with the divisions by nx and ny as multiply-shifts (k < 2^31)
+__device__ __forceinline__ void box_nodes(uint32_t k, const NodeAddr &b, FastDiv div_nx, FastDiv div_ny,
+                                          uint32_t (&nodes)[8])
+{
+    const uint32_t yz = fast_div(k, div_nx), x = k - yz * (uint32_t)b.nx;
+    const uint32_t z = fast_div(yz, div_ny), y = yz - z * (uint32_t)b.ny;
+    box_nodes_at(k, x, y, z, b, nodes);
 }
 
 __device__ __forceinline__ void node_slots(uint32_t k, const uint32_t *nbx, const uint32_t *nby, const uint32_t *nbz,
@@ -856,6 +871,56 @@ __device__ __forceinline__ C cdot_rt(int d, C ux, C uy, C uz)
 //                       form minus w drho (getInterpolatedDistributionForVeloWithPressureBC).
 enum : int { kBCCompressible = 0, kBCIncompressible = 1, kBCWithPressure = 2 };
 
+// density, velocity and c_s^2-scaled u^2 of a BC node's post-collision populations
+// (NoSlipInterpolatedCompressible.cu:134-153: plain-sum density, grouped momenta)
+template <class C>
+struct BCMoments {
+    C drho, ux, uy, uz, cu_sq;
+};
+
+template <class C, int FORM>
+__device__ __forceinline__ BCMoments<C> bc_moments(const C (&p)[27])
+{
+    BCMoments<C> m;
+    m.drho = p[21] + p[20] + p[19] + p[22] + p[25] + p[24] + p[23] + p[26] + p[17] + p[18] + p[15] + p[16] + p[13]
+           + p[14] + p[11] + p[12] + p[9] + p[10] + p[7] + p[8] + p[5] + p[6] + p[3] + p[4] + p[1] + p[2] + p[0];
+    const C r = C(1) + m.drho;
+    const C vx = (((((p[21] - p[24]) - (p[20] - p[25])) + ((p[19] - p[26]) - (p[22] - p[23]))) + ((p[13] - p[14]) + (p[11] - p[12])))
+                  + ((p[9] - p[10]) + (p[7] - p[8]))) + (p[1] - p[2]);
+    const C vy = (((((-(p[21] - p[24])) + (p[20] - p[25])) + ((p[19] - p[26]) - (p[22] - p[23]))) + ((p[17] - p[18]) + (p[15] - p[16])))
+                  + ((-(p[9] - p[10])) + (p[7] - p[8]))) + (p[3] - p[4]);
+    const C vz = (((((p[21] - p[24]) + (p[20] - p[25])) + ((p[19] - p[26]) + (p[22] - p[23]))) + ((-(p[17] - p[18])) + (p[15] - p[16])))
+                  + ((p[11] - p[12]) - (p[13] - p[14]))) + (p[5] - p[6]);
+    m.ux = FORM == kBCIncompressible ? vx : vx / r;
+    m.uy = FORM == kBCIncompressible ? vy : vy / r;
+    m.uz = FORM == kBCIncompressible ? vz : vz / r;
+    m.cu_sq = FORM == kBCIncompressible ? C(1.5) * (m.ux * m.ux + m.uy * m.uy + m.uz * m.uz)
+                                        : C(1.5) * (m.ux * m.ux + m.uy * m.uy + m.uz * m.uz) * (C(1) + m.drho);
+    return m;
+}
+
+// the value written for one cut link: f = p[d], fi = p[inv d], w and vel = c_d . u of direction d,
+// vbc = c_d . u_wall (velocity kernels)
+template <class C, bool VELOCITY, int FORM>
+__device__ __forceinline__ C bc_link_value(C f, C fi, C q, C w, C vel, C vbc, const BCMoments<C> &m, C omega)
+{
+    // the incompressible velocity kernel writes feq inline without (1 + drho); the incompressible
+    // no-slip kernel keeps getEquilibriumForBC, which carries it
+    const C feq = (FORM == kBCIncompressible && VELOCITY) ? w * (m.drho + C(4.5) * vel * vel - m.cu_sq)
+                                                          : w * (m.drho + C(4.5) * vel * vel * (C(1) + m.drho) - m.cu_sq);
+    C v;
+    if (VELOCITY) {
+        v = (C(1) - q) / (C(1) + q) * (f - fi + (f + fi - C(2) * feq * omega) / (C(1) - omega)) * C(0.5)
+          + (q * (f + fi) - C(6) * w * vbc) / (C(1) + q);
+        if (FORM == kBCWithPressure)
+            v = v - w * m.drho;
+    } else {
+        v = (C(1) - q) / (C(1) + q) * (f - fi + (f + fi - C(2) * feq * omega) / (C(1) - omega)) * C(0.5)
+          + (q * (f + fi)) / (C(1) + q);
+    }
+    return v;
+}
+
 // one BC node: its slot nodes, its q of every direction at q27[d * q_stride], the wall velocity
 template <class S, bool EVEN, bool VELOCITY, int FORM>
 __device__ __forceinline__ void bc_interpolated_node(S *base, uint64_t n, const uint32_t (&nodes)[8],
@@ -883,44 +948,14 @@ __device__ __forceinline__ void bc_interpolated_node(S *base, uint64_t n, const 
                     p[d] = guard[r++];
         }
     }
-    // plain-sum density and grouped momenta (NoSlipInterpolatedCompressible.cu:134-153)
-    const C drho = p[21] + p[20] + p[19] + p[22] + p[25] + p[24] + p[23] + p[26] + p[17] + p[18] + p[15] + p[16] + p[13]
-                 + p[14] + p[11] + p[12] + p[9] + p[10] + p[7] + p[8] + p[5] + p[6] + p[3] + p[4] + p[1] + p[2] + p[0];
-    const C r = C(1) + drho;
-    const C vx = (((((p[21] - p[24]) - (p[20] - p[25])) + ((p[19] - p[26]) - (p[22] - p[23]))) + ((p[13] - p[14]) + (p[11] - p[12])))
-                  + ((p[9] - p[10]) + (p[7] - p[8]))) + (p[1] - p[2]);
-    const C vy = (((((-(p[21] - p[24])) + (p[20] - p[25])) + ((p[19] - p[26]) - (p[22] - p[23]))) + ((p[17] - p[18]) + (p[15] - p[16])))
-                  + ((-(p[9] - p[10])) + (p[7] - p[8]))) + (p[3] - p[4]);
-    const C vz = (((((p[21] - p[24]) + (p[20] - p[25])) + ((p[19] - p[26]) + (p[22] - p[23]))) + ((-(p[17] - p[18])) + (p[15] - p[16])))
-                  + ((p[11] - p[12]) - (p[13] - p[14]))) + (p[5] - p[6]);
-    const C ux1 = FORM == kBCIncompressible ? vx : vx / r;
-    const C uy1 = FORM == kBCIncompressible ? vy : vy / r;
-    const C uz1 = FORM == kBCIncompressible ? vz : vz / r;
-    const C cu_sq = FORM == kBCIncompressible ? C(1.5) * (ux1 * ux1 + uy1 * uy1 + uz1 * uz1)
-                                              : C(1.5) * (ux1 * ux1 + uy1 * uy1 + uz1 * uz1) * (C(1) + drho);
+    const BCMoments<C> m = bc_moments<C, FORM>(p);
     const C omega = (C)omega_real;
 #pragma unroll
     for (int d = 1; d < 27; ++d) {
         const C q = q27[(uint64_t)d * q_stride];
         if (q_active(q)) {
-            const C w = weight_t<C>(d);
-            const C vel = cdot_rt<C>(d, ux1, uy1, uz1);
-            // the incompressible velocity kernel writes feq inline without (1 + drho); the
-            // incompressible no-slip kernel keeps getEquilibriumForBC, which carries it
-            const C feq = (FORM == kBCIncompressible && VELOCITY) ? w * (drho + C(4.5) * vel * vel - cu_sq)
-                                                                  : w * (drho + C(4.5) * vel * vel * (C(1) + drho) - cu_sq);
-            const C f = p[d], fi = p[inv(d)];
-            C v;
-            if (VELOCITY) {
-                const C vbc = cdot_rt<C>(d, bx, by, bz);
-                v = (C(1) - q) / (C(1) + q) * (f - fi + (f + fi - C(2) * feq * omega) / (C(1) - omega)) * C(0.5)
-                  + (q * (f + fi) - C(6) * w * vbc) / (C(1) + q);
-                if (FORM == kBCWithPressure)
-                    v = v - w * drho;
-            } else {
-                v = (C(1) - q) / (C(1) + q) * (f - fi + (f + fi - C(2) * feq * omega) / (C(1) - omega)) * C(0.5)
-                  + (q * (f + fi)) / (C(1) + q);
-            }
+            const C v = bc_link_value<C, VELOCITY, FORM>(p[d], p[inv(d)], q, weight_t<C>(d), cdot_rt<C>(d, m.ux, m.uy, m.uz),
+                                                         VELOCITY ? cdot_rt<C>(d, bx, by, bz) : C(0), m, omega);
             const int e = inv(d);
             Codec<S>::store_at(base, (uint64_t)plane<!EVEN>(e) * n + nodes[shift_class(e)], v, e);
         }
@@ -1511,8 +1546,10 @@ struct PoolDomain {
     K17Rates<C> rates;
     C fx, fy, fz;                // half accelerations
     double omega;                // the BC kernels' omega
-    uint64_t noslip_offset;      // bytes from the arena start: int32 k[n_noslip], then C q27[27 n_noslip]
-    uint64_t noslip_q_offset;
+    uint64_t noslip_offset;      // bytes from the arena start: int32 k[n_noslip]
+    uint64_t noslip_cut_offset;  // bytes: uint32 cut[n_noslip] (bit d: q_d in [0, 1]), uint32 first[ceil(n / 32)]
+    uint64_t noslip_q_offset;    // bytes: C q[] of the cut links, node by node, directions ascending;
+                                 // first[c] = the links of nodes 0 .. 32 c - 1
     uint64_t noslip_guard_offset; // bytes: uint32 mask[n_noslip], uint32 first[n_noslip] (guarded directions)
     uint64_t noslip_saved_offset; // bytes: C saved[] (their post-collision values, taken before the writes)
     uint64_t pressure_offset;    // bytes: int32 k[n], int32 kN[n], int32 direction[n], then C drho[n]
@@ -1663,30 +1700,124 @@ __global__ void __launch_bounds__(128) pool_noslip_guard_kernel(PoolBCArgs<typen
     }
 }
 
+// c_d . u for a run-time direction, with the operations of cdot_rt
+template <class C>
+__device__ __forceinline__ C cdot_link(int d, C ux, C uy, C uz)
+{
+    const bool xp = (kMaskXP >> d) & 1u, xm = (kMaskXM >> d) & 1u;
+    const bool yp = (kMaskYP >> d) & 1u, ym = (kMaskYM >> d) & 1u;
+    const bool zp = (kMaskZP >> d) & 1u, zm = (kMaskZM >> d) & 1u;
+    C s = C(0);
+    bool first = true;
+    if (xp || xm) { s = xp ? ux : -ux; first = false; }
+    if (yp || ym) { s = first ? (yp ? uy : -uy) : (yp ? s + uy : s - uy); first = false; }
+    if (zp || zm) { s = first ? (zp ? uz : -uz) : (zp ? s + uz : s - uz); }
+    return s;
+}
+
+// Interpolated no-slip over the pool's lists, one warp per 32 BC nodes, in two phases.
+//   nodes: lane i gathers node i's post-collision populations (guarded ones from the saved copy),
+//          forms its moments, and puts both with its slot nodes in the warp's shared memory;
+//   links: the warp's cut links (node, direction), listed in node order with directions
+//          ascending, are spread over the lanes, each computing and storing one link's value.
+// Every lane does useful work in the second phase, where a thread per node would step through all
+// 26 directions with the lanes of uncut ones idle. The arithmetic is bc_moments / bc_link_value,
+// as in bc_interpolated_node, so the values are the same bits.
+constexpr int kLinkWarps = 4;        // warps per block of the link kernel
+constexpr int kLinkRow = 33;         // padded row of the shared tables (a link's node and direction spread its bank)
+
+template <class C>
+struct LinkTile {
+    C p[27 * kLinkRow];
+    C m[5 * 32];                     // drho, ux, uy, uz, cu_sq
+    uint32_t nodes[8 * kLinkRow];
+    uint16_t links[32 * 26];         // lane | direction << 5
+};
+
 template <class S, bool EVEN>
 __global__ void __launch_bounds__(128) pool_noslip_kernel(PoolBCArgs<typename Codec<S>::compute> a)
 {
     using C = typename Codec<S>::compute;
+    __shared__ LinkTile<C> tiles[kLinkWarps];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    LinkTile<C> &t = tiles[warp];
     const uint32_t n_items = __ldg(a.n_items);
     for (uint32_t w = blockIdx.x; w < n_items; w += gridDim.x) {
         const uint2 it = a.items[w];
         const PoolDomain<C> &dm = a.domains[it.x];
-        const uint32_t i = it.y + threadIdx.x;
-        if (i >= dm.n_noslip)
+        const uint32_t i0 = it.y + 32u * warp;
+        if (i0 >= dm.n_noslip)
             continue;
         const char *arena = static_cast<const char *>(a.arena);
-        const int32_t *k = reinterpret_cast<const int32_t *>(arena + dm.noslip_offset);
-        const C *q = reinterpret_cast<const C *>(arena + dm.noslip_q_offset);
-        const NodeAddr box{ dm.nx, dm.ny, dm.nz, dm.flags & 7 };
-        uint32_t nodes[8];
-        box_nodes((uint32_t)k[i], box, nodes);
-        const uint32_t *guard = reinterpret_cast<const uint32_t *>(arena + dm.noslip_guard_offset);
-        const uint32_t mask = guard[i];
-        const C *saved = mask ? reinterpret_cast<const C *>(arena + dm.noslip_saved_offset) + guard[dm.n_noslip + i]
-                              : nullptr;
-        bc_interpolated_node<S, EVEN, false, kBCCompressible>(static_cast<S *>(a.arena) + dm.dist_offset, dm.pitch,
-                                                              nodes, q + i, dm.n_noslip, dm.omega, C(0), C(0), C(0),
-                                                              nullptr, 0, mask, saved);
+        S *base = static_cast<S *>(a.arena) + dm.dist_offset;
+        const uint32_t *cut_mask = reinterpret_cast<const uint32_t *>(arena + dm.noslip_cut_offset);
+        const uint32_t i = i0 + lane;
+        uint32_t cut = 0;
+        if (i < dm.n_noslip) {
+            const int32_t *k = reinterpret_cast<const int32_t *>(arena + dm.noslip_offset);
+            const uint32_t *guard = reinterpret_cast<const uint32_t *>(arena + dm.noslip_guard_offset);
+            const NodeAddr box{ dm.nx, dm.ny, dm.nz, dm.flags & 7 };
+            uint32_t nodes[8];
+            box_nodes((uint32_t)k[i], box, dm.div_nx, dm.div_ny, nodes);
+            cut = cut_mask[i];
+            const uint32_t gm = guard[i];
+            C p[27];
+            gather_post<S, EVEN>(base, dm.pitch, nodes, p);
+            if (gm) {
+                const C *saved = reinterpret_cast<const C *>(arena + dm.noslip_saved_offset) + guard[dm.n_noslip + i];
+                int r = 0;
+#pragma unroll
+                for (int d = 1; d < 27; ++d)
+                    if ((gm >> d) & 1u)
+                        p[d] = saved[r++];
+            }
+            const BCMoments<C> m = bc_moments<C, kBCCompressible>(p);
+#pragma unroll
+            for (int d = 0; d < 27; ++d)
+                t.p[d * kLinkRow + lane] = p[d];
+#pragma unroll
+            for (int c = 0; c < 8; ++c)
+                t.nodes[c * kLinkRow + lane] = nodes[c];
+            t.m[0 * 32 + lane] = m.drho;
+            t.m[1 * 32 + lane] = m.ux;
+            t.m[2 * 32 + lane] = m.uy;
+            t.m[3 * 32 + lane] = m.uz;
+            t.m[4 * 32 + lane] = m.cu_sq;
+        }
+        // the warp's link list: an exclusive scan of the lanes' link counts
+        const uint32_t count = __popc(cut);
+        uint32_t incl = count;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (uint32_t)o)
+                incl += v;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        uint32_t slot = incl - count;
+        for (uint32_t b = cut; b; b &= b - 1u)
+            t.links[slot++] = (uint16_t)(lane | ((uint32_t)(__ffs(b) - 1) << 5));
+        __syncwarp();
+        const C *q = reinterpret_cast<const C *>(arena + dm.noslip_q_offset) + cut_mask[dm.n_noslip + i0 / 32u];
+        const C omega = (C)dm.omega;
+        for (uint32_t l = lane; l < total; l += 32u) {
+            const uint32_t e = t.links[l];
+            const uint32_t nl = e & 31u;
+            const int d = (int)(e >> 5);
+            const int di = inv(d);
+            BCMoments<C> m;
+            m.drho = t.m[0 * 32 + nl];
+            m.ux = t.m[1 * 32 + nl];
+            m.uy = t.m[2 * 32 + nl];
+            m.uz = t.m[3 * 32 + nl];
+            m.cu_sq = t.m[4 * 32 + nl];
+            const C v = bc_link_value<C, false, kBCCompressible>(t.p[d * kLinkRow + nl], t.p[di * kLinkRow + nl], q[l],
+                                                                 weight_rt<C>(d), cdot_link<C>(d, m.ux, m.uy, m.uz), C(0),
+                                                                 m, omega);
+            Codec<S>::store_at_rt(base, (uint64_t)plane<!EVEN>(di) * dm.pitch + t.nodes[shift_class_rt(di) * kLinkRow + nl],
+                                  v, di);
+        }
+        __syncwarp();
     }
 }
 

@@ -61,6 +61,37 @@ __host__ __device__ constexpr int plane(int d)
     return EVEN ? d : inv(d);
 }
 
+// Directions with a given component, as bit masks (bit d): the lattice for code whose direction
+// is a run-time value, e.g. a thread working on one cut link of a list.
+__host__ __device__ constexpr uint32_t component_mask(int axis, int sign)
+{
+    uint32_t m = 0;
+    for (int d = 0; d < kQ; ++d)
+        if ((axis == 0 ? cx(d) : axis == 1 ? cy(d) : cz(d)) == sign)
+            m |= 1u << d;
+    return m;
+}
+constexpr uint32_t kMaskXP = component_mask(0, 1), kMaskXM = component_mask(0, -1);
+constexpr uint32_t kMaskYP = component_mask(1, 1), kMaskYM = component_mask(1, -1);
+constexpr uint32_t kMaskZP = component_mask(2, 1), kMaskZM = component_mask(2, -1);
+
+__host__ __device__ __forceinline__ int shift_class_rt(int d)
+{
+    return (int)(((kMaskXM >> d) & 1u) | (((kMaskYM >> d) & 1u) << 1) | (((kMaskZM >> d) & 1u) << 2));
+}
+__host__ __device__ __forceinline__ int order_rt(int d)
+{
+    return (int)(((kMaskXP | kMaskXM) >> d) & 1u) + (int)(((kMaskYP | kMaskYM) >> d) & 1u) +
+           (int)(((kMaskZP | kMaskZM) >> d) & 1u);
+}
+// weight_t<T>(d) for a run-time d: the same four constants
+template <class T>
+__host__ __device__ __forceinline__ T weight_rt(int d)
+{
+    const int o = order_rt(d);
+    return o == 0 ? weight_t<T>(0) : o == 1 ? weight_t<T>(1) : o == 2 ? weight_t<T>(7) : weight_t<T>(19);
+}
+
 // signed sum of a velocity along direction d, spelled as the reference kernels spell it
 // (x, then y, then z; a leading negative component is negated, later ones subtracted)
 template <int D, class T>

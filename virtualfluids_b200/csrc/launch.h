@@ -53,8 +53,8 @@ struct PoolDomainSpec {
     double omega;
     double lim[3];
     double half_force[3];
-    uint64_t noslip_offset, noslip_q_offset, noslip_guard_offset, noslip_saved_offset, pressure_offset,
-        pressure_rho_offset;
+    uint64_t noslip_offset, noslip_cut_offset, noslip_q_offset, noslip_guard_offset, noslip_saved_offset,
+        pressure_offset, pressure_rho_offset;
     uint32_t n_noslip, n_pressure;
 };
 

@@ -292,6 +292,7 @@ void Launchers<S>::pool_domain(void *out, const PoolDomainSpec &spec)
     d.fz = (C)spec.half_force[2];
     d.omega = spec.omega;
     d.noslip_offset = spec.noslip_offset;
+    d.noslip_cut_offset = spec.noslip_cut_offset;
     d.noslip_q_offset = spec.noslip_q_offset;
     d.noslip_guard_offset = spec.noslip_guard_offset;
     d.noslip_saved_offset = spec.noslip_saved_offset;

@@ -443,18 +443,23 @@ void domain_sizes(const vfb_pool *p, const vfb_domain_desc *d, bool has_mask, ui
     mask_bytes = has_mask ? align_up(n) : 0;
 }
 
-// arena bytes of a domain's BC lists: no-slip k and q27, pressure k, kN, direction and drho
+// arena bytes of a domain's BC lists: no-slip k, cut masks with the first link of every 32 nodes,
+// the q of the cut links, guard tables and saved values; pressure k, kN, direction and drho
 struct BCSizes {
-    uint64_t noslip_k, noslip_q, noslip_guard, noslip_saved, pressure_i, pressure_rho;
-    uint64_t total() const { return noslip_k + noslip_q + noslip_guard + noslip_saved + pressure_i + pressure_rho; }
+    uint64_t noslip_k, noslip_cut, noslip_q, noslip_guard, noslip_saved, pressure_i, pressure_rho;
+    uint64_t total() const
+    {
+        return noslip_k + noslip_cut + noslip_q + noslip_guard + noslip_saved + pressure_i + pressure_rho;
+    }
 };
 
-BCSizes bc_sizes(const vfb_pool *p, uint32_t n_noslip, uint32_t n_saved, uint32_t n_pressure)
+BCSizes bc_sizes(const vfb_pool *p, uint32_t n_noslip, uint64_t n_links, uint32_t n_saved, uint32_t n_pressure)
 {
     const uint64_t rs = real_size(p->desc.storage);
     BCSizes b;
     b.noslip_k = n_noslip ? align_up(4ull * n_noslip) : 0;
-    b.noslip_q = n_noslip ? align_up(27ull * n_noslip * rs) : 0;
+    b.noslip_cut = n_noslip ? align_up(4ull * n_noslip + 4ull * ((n_noslip + 31) / 32)) : 0;
+    b.noslip_q = n_links ? align_up(n_links * rs) : 0;
     b.noslip_guard = n_noslip ? align_up(8ull * n_noslip) : 0;
     b.noslip_saved = n_saved ? align_up((uint64_t)n_saved * rs) : 0;
     b.pressure_i = n_pressure ? align_up(12ull * n_pressure) : 0;
@@ -462,18 +467,70 @@ BCSizes bc_sizes(const vfb_pool *p, uint32_t n_noslip, uint32_t n_saved, uint32_
     return b;
 }
 
-// the guard tables of a domain's no-slip list (guards.h)
-uint32_t guard_tables(const vfb_domain_desc *d, const vfb_domain_bcs *b, std::vector<uint32_t> &mask,
-                      std::vector<uint32_t> &first)
+// the guard tables of a domain's no-slip list (guards.h), with q tested in the pool's real type
+uint32_t guard_tables(const vfb_pool *p, const vfb_domain_desc *d, const vfb_domain_bcs *b,
+                      std::vector<uint32_t> &mask, std::vector<uint32_t> &first)
 {
     const uint32_t n = b ? b->number_of_noslip_nodes : 0;
     std::vector<uint32_t> table;
     const int periodic = (d->periodic_x ? 1 : 0) | (d->periodic_y ? 2 : 0) | (d->periodic_z ? 4 : 0);
-    const uint32_t saved = n ? vfb::bc_guard_tables(b->noslip_k, b->noslip_q27, n, d->nx, d->ny, d->nz, periodic, table)
-                             : 0;
+    uint32_t saved = 0;
+    if (n && real_size(p->desc.storage) == 8) {
+        saved = vfb::bc_guard_tables(b->noslip_k, b->noslip_q27, n, d->nx, d->ny, d->nz, periodic, table);
+    } else if (n) {
+        const std::vector<float> q(b->noslip_q27, b->noslip_q27 + 27ull * n);
+        saved = vfb::bc_guard_tables(b->noslip_k, q.data(), n, d->nx, d->ny, d->nz, periodic, table);
+    }
     mask.assign(table.begin(), table.begin() + n);
     first.assign(table.begin() + n, table.end());
     return saved;
+}
+
+// The no-slip list in the link form of the pool's kernel: per node a mask of its cut directions
+// (q in [0, 1] in the pool's real type, the test the kernels make), after the masks the first link
+// of every 32 nodes, and the q of the links node by node, directions ascending. With
+// q_out == nullptr only the link count is returned.
+uint64_t noslip_links(const vfb_pool *p, const vfb_domain_bcs *b, std::vector<uint32_t> *cut_first,
+                      std::vector<unsigned char> *q_out)
+{
+    const uint32_t n = b ? b->number_of_noslip_nodes : 0;
+    const bool wide = real_size(p->desc.storage) == 8;
+    auto active = [wide](double q) {
+        if (wide)
+            return q >= 0.0 && q <= 1.0;
+        const float f = (float)q;
+        return f >= 0.0f && f <= 1.0f;
+    };
+    if (cut_first)
+        cut_first->assign((size_t)n + (n + 31) / 32, 0u);
+    if (q_out)
+        q_out->clear();
+    uint64_t links = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (cut_first && i % 32 == 0)
+            (*cut_first)[(size_t)n + i / 32] = (uint32_t)links;
+        uint32_t cut = 0;
+        for (int d = 1; d < 27; ++d) {
+            const double q = b->noslip_q27[(size_t)d * n + i];
+            if (!active(q))
+                continue;
+            cut |= 1u << d;
+            ++links;
+            if (q_out) {
+                if (wide) {
+                    const unsigned char *c = reinterpret_cast<const unsigned char *>(&q);
+                    q_out->insert(q_out->end(), c, c + 8);
+                } else {
+                    const float f = (float)q;
+                    const unsigned char *c = reinterpret_cast<const unsigned char *>(&f);
+                    q_out->insert(q_out->end(), c, c + 4);
+                }
+            }
+        }
+        if (cut_first)
+            (*cut_first)[i] = cut;
+    }
+    return links;
 }
 
 bool is_axis_direction(int32_t d) { return d >= VFB_DIR_P00 && d <= VFB_DIR_00M; }
@@ -589,9 +646,9 @@ int vfb_pool_domain_bytes_with_bcs(const vfb_pool *p, const vfb_domain_desc *d, 
     uint64_t pitch, pop, mask;
     domain_sizes(p, d, needs_mask(d, has_mask != 0), pitch, pop, mask);
     std::vector<uint32_t> gm, gf;
-    const uint32_t n_saved = guard_tables(d, bcs, gm, gf);
-    *bytes = pop + mask + bc_sizes(p, bcs ? bcs->number_of_noslip_nodes : 0, n_saved,
-                                   bcs ? bcs->number_of_pressure_nodes : 0).total();
+    const uint32_t n_saved = guard_tables(p, d, bcs, gm, gf);
+    *bytes = pop + mask + bc_sizes(p, bcs ? bcs->number_of_noslip_nodes : 0, noslip_links(p, bcs, nullptr, nullptr),
+                                   n_saved, bcs ? bcs->number_of_pressure_nodes : 0).total();
     return VFB_OK;
 }
 
@@ -657,10 +714,13 @@ int vfb_pool_add_domain_with_bcs(vfb_pool *p, const vfb_domain_desc *d, const ui
     ds.n_noslip = bcs ? bcs->number_of_noslip_nodes : 0;
     ds.n_pressure = bcs ? bcs->number_of_pressure_nodes : 0;
     std::vector<uint32_t> guard_mask, guard_first;
-    const uint32_t n_saved = guard_tables(d, bcs, guard_mask, guard_first);
+    const uint32_t n_saved = guard_tables(p, d, bcs, guard_mask, guard_first);
     uint64_t pop, mask;
     domain_sizes(p, d, ds.has_mask, ds.pitch, pop, mask);
-    const BCSizes bs = bc_sizes(p, ds.n_noslip, n_saved, ds.n_pressure);
+    std::vector<uint32_t> cut_first;
+    std::vector<unsigned char> link_q;
+    const uint64_t n_links = noslip_links(p, bcs, &cut_first, &link_q);
+    const BCSizes bs = bc_sizes(p, ds.n_noslip, n_links, n_saved, ds.n_pressure);
     uint64_t off = 0;
     if (!p->alloc.take(pop + mask + bs.total(), off))
         return pool_fail(VFB_ERR_OUT_OF_MEMORY, "the pool's arena has no room for this domain");
@@ -670,7 +730,8 @@ int vfb_pool_add_domain_with_bcs(vfb_pool *p, const vfb_domain_desc *d, const ui
     ds.live = true;
     vfb::PoolDomainSpec spec{};
     spec.noslip_offset = off + pop + mask;
-    spec.noslip_q_offset = spec.noslip_offset + bs.noslip_k;
+    spec.noslip_cut_offset = spec.noslip_offset + bs.noslip_k;
+    spec.noslip_q_offset = spec.noslip_cut_offset + bs.noslip_cut;
     spec.noslip_guard_offset = spec.noslip_q_offset + bs.noslip_q;
     spec.noslip_saved_offset = spec.noslip_guard_offset + bs.noslip_guard;
     spec.pressure_offset = spec.noslip_saved_offset + bs.noslip_saved;
@@ -681,10 +742,11 @@ int vfb_pool_add_domain_with_bcs(vfb_pool *p, const vfb_domain_desc *d, const ui
         e = cudaMemcpy(arena + ds.mask_offset, m.data(), ds.nodes, cudaMemcpyHostToDevice);
     if (e == cudaSuccess && ds.n_noslip) {
         e = cudaMemcpy(arena + spec.noslip_offset, bcs->noslip_k, 4ull * ds.n_noslip, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) {
-            const auto q = to_real(p, bcs->noslip_q27, 27ull * ds.n_noslip);
-            e = cudaMemcpy(arena + spec.noslip_q_offset, q.data(), q.size(), cudaMemcpyHostToDevice);
-        }
+        if (e == cudaSuccess)
+            e = cudaMemcpy(arena + spec.noslip_cut_offset, cut_first.data(), 4ull * cut_first.size(),
+                           cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !link_q.empty())
+            e = cudaMemcpy(arena + spec.noslip_q_offset, link_q.data(), link_q.size(), cudaMemcpyHostToDevice);
         if (e == cudaSuccess)
             e = cudaMemcpy(arena + spec.noslip_guard_offset, guard_mask.data(), 4ull * ds.n_noslip,
                            cudaMemcpyHostToDevice);

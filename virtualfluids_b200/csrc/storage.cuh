@@ -12,8 +12,9 @@
 // small corner populations do not fall into the subnormal range. 1/w is 27/8, 27/2, 54 or 216.
 // The 16-bit formats round stochastically (below).
 //
-// The direction argument d is always a loop index of a fully unrolled 27-direction loop, so
-// weight(d) folds to a constant.
+// The direction argument d of load / store_at is always a loop index of a fully unrolled
+// 27-direction loop, so weight(d) folds to a constant; store_at_rt takes a run-time direction and
+// picks the same constant by the direction's order.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -29,6 +30,14 @@ enum StorageKind : int { kStoreF64 = 0, kStoreF32 = 1, kStoreF16 = 2, kStoreBF16
 template <class S>
 struct Codec;
 
+// float(1 / w_d) for a run-time d: the constants the 16-bit stores scale by
+__device__ __forceinline__ float inv_weight_rt(int d)
+{
+    const int o = order_rt(d);
+    return o == 0 ? float(1.0 / weight(0)) : o == 1 ? float(1.0 / weight(1)) : o == 2 ? float(1.0 / weight(7))
+                                                                                  : float(1.0 / weight(19));
+}
+
 template <>
 struct Codec<double> {
     using compute = double;
@@ -36,6 +45,7 @@ struct Codec<double> {
     __device__ __forceinline__ static double load(const double *p, int) { return *p; }
     __device__ __forceinline__ static void store(double *p, double v, int) { *p = v; }
     __device__ __forceinline__ static void store_at(double *base, uint64_t off, double v, int) { base[off] = v; }
+    __device__ __forceinline__ static void store_at_rt(double *base, uint64_t off, double v, int) { base[off] = v; }
 };
 
 template <>
@@ -45,6 +55,7 @@ struct Codec<float> {
     __device__ __forceinline__ static float load(const float *p, int) { return *p; }
     __device__ __forceinline__ static void store(float *p, float v, int) { *p = v; }
     __device__ __forceinline__ static void store_at(float *base, uint64_t off, float v, int) { base[off] = v; }
+    __device__ __forceinline__ static void store_at_rt(float *base, uint64_t off, float v, int) { base[off] = v; }
 };
 
 // Stochastic rounding of the 16-bit stores. Rounding to nearest drops every change smaller than
@@ -110,6 +121,12 @@ struct Codec<__half> {
         const float s = v * float(1.0 / weight(d));
         base[off] = half_sr(s, sr_bits(s, off));
     }
+    // store_at for a direction known only at run time (the same scale factors)
+    __device__ __forceinline__ static void store_at_rt(__half *base, uint64_t off, float v, int d)
+    {
+        const float s = v * inv_weight_rt(d);
+        base[off] = half_sr(s, sr_bits(s, off));
+    }
 };
 
 template <>
@@ -131,6 +148,11 @@ struct Codec<__nv_bfloat16> {
     __device__ __forceinline__ static void store_at(__nv_bfloat16 *base, uint64_t off, float v, int d)
     {
         const float s = v * float(1.0 / weight(d));
+        base[off] = bf16_sr(s, sr_bits(s, off));
+    }
+    __device__ __forceinline__ static void store_at_rt(__nv_bfloat16 *base, uint64_t off, float v, int d)
+    {
+        const float s = v * inv_weight_rt(d);
         base[off] = bf16_sr(s, sr_bits(s, off));
     }
 };
