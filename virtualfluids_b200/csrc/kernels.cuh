@@ -1550,11 +1550,12 @@ struct PoolDomain {
     uint64_t noslip_cut_offset;  // bytes: uint32 cut[n_noslip] (bit d: q_d in [0, 1]), uint32 first[ceil(n / 32)]
     uint64_t noslip_q_offset;    // bytes: C q[] of the cut links, node by node, directions ascending;
                                  // first[c] = the links of nodes 0 .. 32 c - 1
-    uint64_t noslip_guard_offset; // bytes: uint32 mask[n_noslip], uint32 first[n_noslip] (guarded directions)
+    uint64_t noslip_guard_offset; // bytes: uint32 mask[n_noslip], uint32 first[n_noslip] (guarded directions),
+                                  // uint32 guarded[n_guarded] (the list positions with a nonzero mask)
     uint64_t noslip_saved_offset; // bytes: C saved[] (their post-collision values, taken before the writes)
     uint64_t pressure_offset;    // bytes: int32 k[n], int32 kN[n], int32 direction[n], then C drho[n]
     uint64_t pressure_rho_offset;
-    uint32_t n_noslip, n_pressure;
+    uint32_t n_noslip, n_pressure, n_guarded;
     FastDiv div_nx, div_ny;      // node k -> (x, y, z) without hardware division
 };
 
@@ -1669,7 +1670,8 @@ struct PoolBCArgs {
 // Links cut from both ends (two BC nodes of one list joined by a link that clips the geometry):
 // each node's write lands in the slot the other reads. Before the no-slip kernel writes anything,
 // the values in those slots (bit d of a node's mask: its post-collision population d) are saved,
-// and the no-slip kernel reads them from there, so every node sees the collision's values.
+// and the no-slip kernel reads them from there, so every node sees the collision's values. The
+// work list runs over the guarded nodes only ({domain, first position in guarded[]} items).
 template <class S, bool EVEN>
 __global__ void __launch_bounds__(128) pool_noslip_guard_kernel(PoolBCArgs<typename Codec<S>::compute> a)
 {
@@ -1678,19 +1680,18 @@ __global__ void __launch_bounds__(128) pool_noslip_guard_kernel(PoolBCArgs<typen
     for (uint32_t w = blockIdx.x; w < n_items; w += gridDim.x) {
         const uint2 it = a.items[w];
         const PoolDomain<C> &dm = a.domains[it.x];
-        const uint32_t i = it.y + threadIdx.x;
-        if (i >= dm.n_noslip)
+        const uint32_t g = it.y + threadIdx.x;
+        if (g >= dm.n_guarded)
             continue;
         char *arena = static_cast<char *>(a.arena);
         const uint32_t *guard = reinterpret_cast<const uint32_t *>(arena + dm.noslip_guard_offset);
+        const uint32_t i = guard[2ull * dm.n_noslip + g];
         const uint32_t mask = guard[i];
-        if (!mask)
-            continue;
         const int32_t *k = reinterpret_cast<const int32_t *>(arena + dm.noslip_offset);
         C *saved = reinterpret_cast<C *>(arena + dm.noslip_saved_offset) + guard[dm.n_noslip + i];
         const NodeAddr box{ dm.nx, dm.ny, dm.nz, dm.flags & 7 };
         uint32_t nodes[8];
-        box_nodes((uint32_t)k[i], box, nodes);
+        box_nodes((uint32_t)k[i], box, dm.div_nx, dm.div_ny, nodes);
         const S *base = static_cast<const S *>(a.arena) + dm.dist_offset;
         int r = 0;
 #pragma unroll

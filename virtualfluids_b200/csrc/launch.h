@@ -55,7 +55,7 @@ struct PoolDomainSpec {
     double half_force[3];
     uint64_t noslip_offset, noslip_cut_offset, noslip_q_offset, noslip_guard_offset, noslip_saved_offset,
         pressure_offset, pressure_rho_offset;
-    uint32_t n_noslip, n_pressure;
+    uint32_t n_noslip, n_guarded, n_pressure;
 };
 
 #define VFB_DECLARE_LAUNCHERS                                                                                        \
@@ -92,7 +92,8 @@ struct PoolDomainSpec {
                                      int nodes_per_thread, int threads, bool even, double *partials,              \
                                      cudaStream_t s);                                                              \
         static cudaError_t pool_bcs(void *arena, const void *domains, const uint2 *noslip_items,                   \
-                                    const uint32_t *n_noslip_items, const uint2 *pressure_items,                   \
+                                    const uint32_t *n_noslip_items, const uint2 *guard_items,                      \
+                                    const uint32_t *n_guard_items, const uint2 *pressure_items,                    \
                                     const uint32_t *n_pressure_items, bool even, unsigned grid, cudaStream_t s);   \
         static cudaError_t drag_lift(const vfb_level *L, const vfb_bc *bc, bool pre, double *dx, double *dy,        \
                                      double *dz, cudaStream_t s, const NodeAddr *box = nullptr);                     \

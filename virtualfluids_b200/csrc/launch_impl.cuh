@@ -299,6 +299,7 @@ void Launchers<S>::pool_domain(void *out, const PoolDomainSpec &spec)
     d.pressure_offset = spec.pressure_offset;
     d.pressure_rho_offset = spec.pressure_rho_offset;
     d.n_noslip = spec.n_noslip;
+    d.n_guarded = spec.n_guarded;
     d.n_pressure = spec.n_pressure;
     std::memcpy(out, &d, sizeof(d));
 }
@@ -323,7 +324,8 @@ cudaError_t Launchers<S>::pool_mass(void *arena, const void *domains, const uint
 
 template <class S>
 cudaError_t Launchers<S>::pool_bcs(void *arena, const void *domains, const uint2 *noslip_items,
-                                   const uint32_t *n_noslip_items, const uint2 *pressure_items,
+                                   const uint32_t *n_noslip_items, const uint2 *guard_items,
+                                   const uint32_t *n_guard_items, const uint2 *pressure_items,
                                    const uint32_t *n_pressure_items, bool even, unsigned grid, cudaStream_t s)
 {
     using C = typename Codec<S>::compute;
@@ -342,14 +344,19 @@ cudaError_t Launchers<S>::pool_bcs(void *arena, const void *domains, const uint2
             occ = 1;
         return (unsigned)(occ * sms);
     };
+    if (noslip_items && guard_items) {
+        // the guarded values, saved before any no-slip write
+        a.items = guard_items;
+        a.n_items = n_guard_items;
+        const void *g = even ? (const void *)pool_noslip_guard_kernel<S, true>
+                             : (const void *)pool_noslip_guard_kernel<S, false>;
+        if (even) pool_noslip_guard_kernel<S, true><<<resident(g), 128, 0, s>>>(a);
+        else pool_noslip_guard_kernel<S, false><<<resident(g), 128, 0, s>>>(a);
+    }
     if (noslip_items) {
         a.items = noslip_items;
         a.n_items = n_noslip_items;
-        const void *g = even ? (const void *)pool_noslip_guard_kernel<S, true>
-                             : (const void *)pool_noslip_guard_kernel<S, false>;
         const void *k = even ? (const void *)pool_noslip_kernel<S, true> : (const void *)pool_noslip_kernel<S, false>;
-        if (even) pool_noslip_guard_kernel<S, true><<<resident(g), 128, 0, s>>>(a);
-        else pool_noslip_guard_kernel<S, false><<<resident(g), 128, 0, s>>>(a);
         if (even) pool_noslip_kernel<S, true><<<resident(k), 128, 0, s>>>(a);
         else pool_noslip_kernel<S, false><<<resident(k), 128, 0, s>>>(a);
         const cudaError_t e = cudaGetLastError();

@@ -47,8 +47,8 @@ struct PoolOps {
     const void *(*kernel)(bool);
     size_t (*domain_bytes)();
     void (*domain)(void *, const vfb::PoolDomainSpec &);
-    cudaError_t (*bcs)(void *, const void *, const uint2 *, const uint32_t *, const uint2 *, const uint32_t *, bool,
-                       unsigned, cudaStream_t);
+    cudaError_t (*bcs)(void *, const void *, const uint2 *, const uint32_t *, const uint2 *, const uint32_t *,
+                       const uint2 *, const uint32_t *, bool, unsigned, cudaStream_t);
     cudaError_t (*mass)(void *, const void *, const uint2 *, uint32_t, int, int, bool, double *, cudaStream_t);
     cudaError_t (*init)(const vfb::BoxState &, bool, const void *, const void *, const void *, const void *,
                         cudaStream_t);
@@ -133,6 +133,7 @@ struct DomainSlot {
     uint64_t bytes = 0;            // bytes taken (populations, mask, boundary conditions)
     bool has_mask = false;
     uint32_t n_noslip = 0, n_pressure = 0;
+    uint32_t n_guarded = 0;        // no-slip nodes with guarded directions
     double ref_mass = 0.0;         // watchdog: the mass at the first check after the initialisation
     bool has_ref = false;
 };
@@ -173,7 +174,8 @@ struct vfb_pool {
     void *staging = nullptr;           // host<->device field staging, outside the arena
     uint64_t staging_bytes = 0;
     DeviceList noslip_list, pressure_list;   // BC work lists of the active domains
-    bool has_noslip = false, has_pressure = false;
+    DeviceList guard_list;                   // the guarded no-slip nodes of the active domains
+    bool has_noslip = false, has_pressure = false, has_guard = false;
     unsigned bc_grid = 0;
     std::vector<uint2> host_items;     // the collision work list as uploaded (watchdog sums)
     double *mass_partials = nullptr;   // one FP64 partial per work item
@@ -261,24 +263,29 @@ cudaError_t upload_list(vfb_pool *p, DeviceList &L, const std::vector<uint2> &it
 // the boundary-condition work lists: per active domain with BC nodes one item per kBCSpan nodes
 cudaError_t rebuild_bc_lists(vfb_pool *p, cudaStream_t s)
 {
-    std::vector<uint2> ns, pr;
+    std::vector<uint2> ns, pr, gd;
     for (uint32_t id = 0; id < p->slots.size(); ++id) {
         const DomainSlot &d = p->slots[id];
         if (!d.live || !d.active)
             continue;
         for (uint32_t i = 0; i < d.n_noslip; i += kBCSpan)
             ns.push_back(make_uint2(id, i));
+        for (uint32_t i = 0; i < d.n_guarded; i += kBCSpan)
+            gd.push_back(make_uint2(id, i));
         for (uint32_t i = 0; i < d.n_pressure; i += kBCSpan)
             pr.push_back(make_uint2(id, i));
     }
-    const bool has_ns = !ns.empty(), has_pr = !pr.empty();
-    if (has_ns != p->has_noslip || has_pr != p->has_pressure)
+    const bool has_ns = !ns.empty(), has_pr = !pr.empty(), has_gd = !gd.empty();
+    if (has_ns != p->has_noslip || has_pr != p->has_pressure || has_gd != p->has_guard)
         drop_graph(p);              // the launches of a step change
     p->has_noslip = has_ns;
     p->has_pressure = has_pr;
+    p->has_guard = has_gd;
     cudaError_t e = cudaSuccess;
     if (has_ns || p->noslip_list.count)
         e = upload_list(p, p->noslip_list, ns, s);
+    if (e == cudaSuccess && (has_gd || p->guard_list.count))
+        e = upload_list(p, p->guard_list, gd, s);
     if (e == cudaSuccess && (has_pr || p->pressure_list.count))
         e = upload_list(p, p->pressure_list, pr, s);
     return e;
@@ -336,17 +343,18 @@ cudaError_t launch_step(vfb_pool *p, bool even, cudaStream_t s)
     cudaError_t e = p->ops.collide(p->arena, p->domain_table, p->items, p->n_items, p->nodes_per_thread, even, p->grid,
                                    (unsigned)p->threads, s);
     if (e == cudaSuccess && (p->has_noslip || p->has_pressure)) {
-        p->launches += (p->has_noslip ? 2 : 0) + (p->has_pressure ? 1 : 0);   // snapshot + no-slip, pressure
+        p->launches += (p->has_noslip ? 1 : 0) + (p->has_guard ? 1 : 0) + (p->has_pressure ? 1 : 0);
         e = p->ops.bcs(p->arena, p->domain_table, p->has_noslip ? p->noslip_list.items : nullptr,
-                       p->noslip_list.count, p->has_pressure ? p->pressure_list.items : nullptr,
-                       p->pressure_list.count, even, p->bc_grid, s);
+                       p->noslip_list.count, p->has_guard ? p->guard_list.items : nullptr, p->guard_list.count,
+                       p->has_pressure ? p->pressure_list.items : nullptr, p->pressure_list.count, even, p->bc_grid,
+                       s);
     }
     return e;
 }
 
 uint32_t launches_per_step(const vfb_pool *p)
 {
-    return 1u + (p->has_noslip ? 2u : 0u) + (p->has_pressure ? 1u : 0u);
+    return 1u + (p->has_noslip ? 1u : 0u) + (p->has_guard ? 1u : 0u) + (p->has_pressure ? 1u : 0u);
 }
 
 // kGraphSteps steps starting at the even parity, captured once and replayed
@@ -453,23 +461,25 @@ struct BCSizes {
     }
 };
 
-BCSizes bc_sizes(const vfb_pool *p, uint32_t n_noslip, uint64_t n_links, uint32_t n_saved, uint32_t n_pressure)
+BCSizes bc_sizes(const vfb_pool *p, uint32_t n_noslip, uint64_t n_links, uint32_t n_guarded, uint32_t n_saved,
+                 uint32_t n_pressure)
 {
     const uint64_t rs = real_size(p->desc.storage);
     BCSizes b;
     b.noslip_k = n_noslip ? align_up(4ull * n_noslip) : 0;
     b.noslip_cut = n_noslip ? align_up(4ull * n_noslip + 4ull * ((n_noslip + 31) / 32)) : 0;
     b.noslip_q = n_links ? align_up(n_links * rs) : 0;
-    b.noslip_guard = n_noslip ? align_up(8ull * n_noslip) : 0;
+    b.noslip_guard = n_noslip ? align_up(8ull * n_noslip + 4ull * n_guarded) : 0;
     b.noslip_saved = n_saved ? align_up((uint64_t)n_saved * rs) : 0;
     b.pressure_i = n_pressure ? align_up(12ull * n_pressure) : 0;
     b.pressure_rho = n_pressure ? align_up((uint64_t)n_pressure * rs) : 0;
     return b;
 }
 
-// the guard tables of a domain's no-slip list (guards.h), with q tested in the pool's real type
+// the guard tables of a domain's no-slip list (guards.h), with q tested in the pool's real type, and
+// the list positions of its guarded nodes (the guard kernel's work)
 uint32_t guard_tables(const vfb_pool *p, const vfb_domain_desc *d, const vfb_domain_bcs *b,
-                      std::vector<uint32_t> &mask, std::vector<uint32_t> &first)
+                      std::vector<uint32_t> &mask, std::vector<uint32_t> &first, std::vector<uint32_t> &guarded)
 {
     const uint32_t n = b ? b->number_of_noslip_nodes : 0;
     std::vector<uint32_t> table;
@@ -483,6 +493,10 @@ uint32_t guard_tables(const vfb_pool *p, const vfb_domain_desc *d, const vfb_dom
     }
     mask.assign(table.begin(), table.begin() + n);
     first.assign(table.begin() + n, table.end());
+    guarded.clear();
+    for (uint32_t i = 0; i < n; ++i)
+        if (mask[i])
+            guarded.push_back(i);
     return saved;
 }
 
@@ -619,7 +633,7 @@ int vfb_pool_destroy(vfb_pool *p)
     cudaFree(p->n_items);
     cudaFree(p->staging);
     cudaFree(p->mass_partials);
-    for (DeviceList *L : { &p->noslip_list, &p->pressure_list }) {
+    for (DeviceList *L : { &p->noslip_list, &p->guard_list, &p->pressure_list }) {
         cudaFree(L->items);
         cudaFree(L->count);
     }
@@ -645,10 +659,10 @@ int vfb_pool_domain_bytes_with_bcs(const vfb_pool *p, const vfb_domain_desc *d, 
         return st;
     uint64_t pitch, pop, mask;
     domain_sizes(p, d, needs_mask(d, has_mask != 0), pitch, pop, mask);
-    std::vector<uint32_t> gm, gf;
-    const uint32_t n_saved = guard_tables(p, d, bcs, gm, gf);
+    std::vector<uint32_t> gm, gf, gi;
+    const uint32_t n_saved = guard_tables(p, d, bcs, gm, gf, gi);
     *bytes = pop + mask + bc_sizes(p, bcs ? bcs->number_of_noslip_nodes : 0, noslip_links(p, bcs, nullptr, nullptr),
-                                   n_saved, bcs ? bcs->number_of_pressure_nodes : 0).total();
+                                   (uint32_t)gi.size(), n_saved, bcs ? bcs->number_of_pressure_nodes : 0).total();
     return VFB_OK;
 }
 
@@ -713,14 +727,15 @@ int vfb_pool_add_domain_with_bcs(vfb_pool *p, const vfb_domain_desc *d, const ui
         return st;
     ds.n_noslip = bcs ? bcs->number_of_noslip_nodes : 0;
     ds.n_pressure = bcs ? bcs->number_of_pressure_nodes : 0;
-    std::vector<uint32_t> guard_mask, guard_first;
-    const uint32_t n_saved = guard_tables(p, d, bcs, guard_mask, guard_first);
+    std::vector<uint32_t> guard_mask, guard_first, guarded;
+    const uint32_t n_saved = guard_tables(p, d, bcs, guard_mask, guard_first, guarded);
+    ds.n_guarded = (uint32_t)guarded.size();
     uint64_t pop, mask;
     domain_sizes(p, d, ds.has_mask, ds.pitch, pop, mask);
     std::vector<uint32_t> cut_first;
     std::vector<unsigned char> link_q;
     const uint64_t n_links = noslip_links(p, bcs, &cut_first, &link_q);
-    const BCSizes bs = bc_sizes(p, ds.n_noslip, n_links, n_saved, ds.n_pressure);
+    const BCSizes bs = bc_sizes(p, ds.n_noslip, n_links, ds.n_guarded, n_saved, ds.n_pressure);
     uint64_t off = 0;
     if (!p->alloc.take(pop + mask + bs.total(), off))
         return pool_fail(VFB_ERR_OUT_OF_MEMORY, "the pool's arena has no room for this domain");
@@ -753,6 +768,9 @@ int vfb_pool_add_domain_with_bcs(vfb_pool *p, const vfb_domain_desc *d, const ui
         if (e == cudaSuccess)
             e = cudaMemcpy(arena + spec.noslip_guard_offset + 4ull * ds.n_noslip, guard_first.data(),
                            4ull * ds.n_noslip, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && ds.n_guarded)
+            e = cudaMemcpy(arena + spec.noslip_guard_offset + 8ull * ds.n_noslip, guarded.data(),
+                           4ull * ds.n_guarded, cudaMemcpyHostToDevice);
     }
     if (e == cudaSuccess && ds.n_pressure) {
         const uint64_t n4 = 4ull * ds.n_pressure;
@@ -781,6 +799,7 @@ int vfb_pool_add_domain_with_bcs(vfb_pool *p, const vfb_domain_desc *d, const ui
         spec.half_force[i] = d->forces[i] * 0.5;
     }
     spec.n_noslip = ds.n_noslip;
+    spec.n_guarded = ds.n_guarded;
     spec.n_pressure = ds.n_pressure;
     p->ops.domain(rec.data(), spec);
     if (e == cudaSuccess)
