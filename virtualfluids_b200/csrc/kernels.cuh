@@ -1701,21 +1701,6 @@ __global__ void __launch_bounds__(128) pool_noslip_guard_kernel(PoolBCArgs<typen
     }
 }
 
-// c_d . u for a run-time direction, with the operations of cdot_rt
-template <class C>
-__device__ __forceinline__ C cdot_link(int d, C ux, C uy, C uz)
-{
-    const bool xp = (kMaskXP >> d) & 1u, xm = (kMaskXM >> d) & 1u;
-    const bool yp = (kMaskYP >> d) & 1u, ym = (kMaskYM >> d) & 1u;
-    const bool zp = (kMaskZP >> d) & 1u, zm = (kMaskZM >> d) & 1u;
-    C s = C(0);
-    bool first = true;
-    if (xp || xm) { s = xp ? ux : -ux; first = false; }
-    if (yp || ym) { s = first ? (yp ? uy : -uy) : (yp ? s + uy : s - uy); first = false; }
-    if (zp || zm) { s = first ? (zp ? uz : -uz) : (zp ? s + uz : s - uz); }
-    return s;
-}
-
 // Interpolated no-slip over the pool's lists, one warp per 32 BC nodes, in two phases.
 //   nodes: lane i gathers node i's post-collision populations (guarded ones from the saved copy),
 //          forms its moments, and puts both with its slot nodes in the warp's shared memory;

@@ -92,6 +92,22 @@ __host__ __device__ __forceinline__ T weight_rt(int d)
     return o == 0 ? weight_t<T>(0) : o == 1 ? weight_t<T>(1) : o == 2 ? weight_t<T>(7) : weight_t<T>(19);
 }
 
+// c_d . u for a run-time direction, with the operations of signed_sum: x, then y, then z; a
+// leading negative component negated, later ones subtracted
+template <class C>
+__host__ __device__ __forceinline__ C cdot_link(int d, C ux, C uy, C uz)
+{
+    const bool xp = (kMaskXP >> d) & 1u, xm = (kMaskXM >> d) & 1u;
+    const bool yp = (kMaskYP >> d) & 1u, ym = (kMaskYM >> d) & 1u;
+    const bool zp = (kMaskZP >> d) & 1u, zm = (kMaskZM >> d) & 1u;
+    C s = C(0);
+    bool first = true;
+    if (xp || xm) { s = xp ? ux : -ux; first = false; }
+    if (yp || ym) { s = first ? (yp ? uy : -uy) : (yp ? s + uy : s - uy); first = false; }
+    if (zp || zm) { s = first ? (zp ? uz : -uz) : (zp ? s + uz : s - uz); }
+    return s;
+}
+
 // signed sum of a velocity along direction d, spelled as the reference kernels spell it
 // (x, then y, then z; a leading negative component is negated, later ones subtracted)
 template <int D, class T>
