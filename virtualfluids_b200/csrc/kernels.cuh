@@ -1542,7 +1542,7 @@ struct PoolDomain {
     uint64_t pitch;              // elements per direction plane
     uint64_t mask_offset;        // bytes from the arena start to the node mask (nonzero = fluid)
     int nx, ny, nz;
-    int flags;                   // bits 0-2: periodic x/y/z, bit 3: has a mask
+    int flags;                   // bits 0-2: periodic x/y/z, bit 3: has a mask, bit 4: compacted collision
     K17Rates<C> rates;
     C fx, fy, fz;                // half accelerations
     double omega;                // the BC kernels' omega
@@ -1559,7 +1559,8 @@ struct PoolDomain {
     FastDiv div_nx, div_ny;      // node k -> (x, y, z) without hardware division
 };
 
-enum : int { kPoolPeriodicX = 1, kPoolPeriodicY = 2, kPoolPeriodicZ = 4, kPoolMask = 8 };
+// flags of a pool domain; kPoolCompact: the collision queues the fluid nodes of each warp
+enum : int { kPoolPeriodicX = 1, kPoolPeriodicY = 2, kPoolPeriodicZ = 4, kPoolMask = 8, kPoolCompact = 16 };
 
 template <class C>
 struct PoolArgs {
@@ -1570,47 +1571,92 @@ struct PoolArgs {
     int nodes_per_thread;
 };
 
+// one node of a pool domain: its slots, the K17 collision and the ET scatter
+template <class S, bool EXACT, bool EVEN>
+__device__ __forceinline__ void pool_collide_node(S *base, const PoolDomain<typename Codec<S>::compute> &dm, uint32_t k)
+{
+    using C = typename Codec<S>::compute;
+    const int nx = dm.nx, ny = dm.ny, nz = dm.nz, flags = dm.flags;
+    const uint32_t yz = fast_div(k, dm.div_nx), x = k - yz * (uint32_t)nx;
+    const uint32_t z = fast_div(yz, dm.div_ny), y = yz - z * (uint32_t)ny;
+    const int xp = ((int)x + 1 < nx) ? (int)x + 1 : ((flags & kPoolPeriodicX) ? 0 : (int)x);
+    const int yp = ((int)y + 1 < ny) ? (int)y + 1 : ((flags & kPoolPeriodicY) ? 0 : (int)y);
+    const int zp = ((int)z + 1 < nz) ? (int)z + 1 : ((flags & kPoolPeriodicZ) ? 0 : (int)z);
+    const uint32_t sx = (uint32_t)(xp - (int)x);
+    const uint32_t sy = (uint32_t)((yp - (int)y) * nx);
+    const uint32_t sz = (uint32_t)((int64_t)(zp - (int)z) * nx * ny);
+    uint32_t nodes[8];
+    nodes[0] = k;
+    nodes[1] = k + sx;
+    nodes[2] = k + sy;
+    nodes[3] = k + sx + sy;
+    nodes[4] = k + sz;
+    nodes[5] = k + sx + sz;
+    nodes[6] = k + sy + sz;
+    nodes[7] = k + sx + sy + sz;
+    C f[27];
+    gather_pre<S, EVEN>(base, dm.pitch, nodes, f);
+    C drho, vx, vy, vz;
+    collide<C, EXACT>(f, dm.rates, dm.fx, dm.fy, dm.fz, drho, vx, vy, vz);
+    scatter_post<S, EVEN>(base, dm.pitch, nodes, f);
+}
+
+// The pool's collision: a persistent grid over {domain, first node} items of blockDim x
+// nodes_per_thread nodes. Warp w of a block owns the 32-node segments it.y + w 32 + j blockDim.
+// By default every lane collides its node of each segment, skipping solid nodes. In a domain
+// flagged kPoolCompact (porous media, where most segments mix fluid and solid nodes) the warp
+// queues the fluid nodes of its segments in shared memory (a ballot per segment, in node order)
+// and collides them 32 at a time, so lanes are not left idle on solid nodes. Each node's arithmetic
+// is the same either way.
 template <class S, bool EXACT, bool EVEN>
 __global__ void __launch_bounds__(256) k17_pool_kernel(PoolArgs<typename Codec<S>::compute> a)
 {
     using C = typename Codec<S>::compute;
+    __shared__ uint32_t queue[8][64];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t lanes_below = (1u << lane) - 1u;
     const uint32_t n_items = __ldg(a.n_items);
     const uint32_t span = blockDim.x * (uint32_t)a.nodes_per_thread;
     for (uint32_t w = blockIdx.x; w < n_items; w += gridDim.x) {
         const uint2 it = a.items[w];
         const PoolDomain<C> &dm = a.domains[it.x];
-        const int nx = dm.nx, ny = dm.ny, nz = dm.nz, flags = dm.flags;
-        const uint32_t nodes_total = (uint32_t)nx * (uint32_t)ny * (uint32_t)nz;
+        const uint32_t nodes_total = (uint32_t)dm.nx * (uint32_t)dm.ny * (uint32_t)dm.nz;
         S *base = static_cast<S *>(a.arena) + dm.dist_offset;
-        const uint8_t *mask = (flags & kPoolMask) ? static_cast<const uint8_t *>(a.arena) + dm.mask_offset : nullptr;
         const uint32_t end = min(it.y + span, nodes_total);
+        const uint8_t *mask = (dm.flags & kPoolMask) ? static_cast<const uint8_t *>(a.arena) + dm.mask_offset : nullptr;
+        if (!(dm.flags & kPoolCompact)) {
 #pragma unroll 1
-        for (uint32_t k = it.y + threadIdx.x; k < end; k += blockDim.x) {
-            if (mask && __ldg(mask + k) == 0)
-                continue;
-            const uint32_t yz = fast_div(k, dm.div_nx), x = k - yz * (uint32_t)nx;
-            const uint32_t z = fast_div(yz, dm.div_ny), y = yz - z * (uint32_t)ny;
-            const int xp = ((int)x + 1 < nx) ? (int)x + 1 : ((flags & kPoolPeriodicX) ? 0 : (int)x);
-            const int yp = ((int)y + 1 < ny) ? (int)y + 1 : ((flags & kPoolPeriodicY) ? 0 : (int)y);
-            const int zp = ((int)z + 1 < nz) ? (int)z + 1 : ((flags & kPoolPeriodicZ) ? 0 : (int)z);
-            const uint32_t sx = (uint32_t)(xp - (int)x);
-            const uint32_t sy = (uint32_t)((yp - (int)y) * nx);
-            const uint32_t sz = (uint32_t)((int64_t)(zp - (int)z) * nx * ny);
-            uint32_t nodes[8];
-            nodes[0] = k;
-            nodes[1] = k + sx;
-            nodes[2] = k + sy;
-            nodes[3] = k + sx + sy;
-            nodes[4] = k + sz;
-            nodes[5] = k + sx + sz;
-            nodes[6] = k + sy + sz;
-            nodes[7] = k + sx + sy + sz;
-            C f[27];
-            gather_pre<S, EVEN>(base, dm.pitch, nodes, f);
-            C drho, vx, vy, vz;
-            collide<C, EXACT>(f, dm.rates, dm.fx, dm.fy, dm.fz, drho, vx, vy, vz);
-            scatter_post<S, EVEN>(base, dm.pitch, nodes, f);
+            for (uint32_t k = it.y + threadIdx.x; k < end; k += blockDim.x) {
+                if (mask && __ldg(mask + k) == 0)
+                    continue;
+                pool_collide_node<S, EXACT, EVEN>(base, dm, k);
+            }
+            continue;
         }
+        uint32_t *q = queue[warp];
+        uint32_t pending = 0;            // queued fluid nodes (the same in every lane)
+#pragma unroll 1
+        for (uint32_t seg = it.y + 32u * warp; seg < end; seg += blockDim.x) {
+            const uint32_t k = seg + lane;
+            const bool fluid = k < end && __ldg(mask + k) != 0;
+            const uint32_t ballot = __ballot_sync(0xffffffffu, fluid);
+            if (fluid)
+                q[pending + __popc(ballot & lanes_below)] = k;
+            pending += __popc(ballot);
+            __syncwarp();
+            if (pending >= 32u) {
+                pool_collide_node<S, EXACT, EVEN>(base, dm, q[lane]);
+                pending -= 32u;
+                const uint32_t rest = lane < pending ? q[32u + lane] : 0u;
+                __syncwarp();
+                if (lane < pending)
+                    q[lane] = rest;
+                __syncwarp();
+            }
+        }
+        if (lane < pending)
+            pool_collide_node<S, EXACT, EVEN>(base, dm, q[lane]);
+        __syncwarp();
     }
 }
 

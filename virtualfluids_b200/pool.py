@@ -153,7 +153,7 @@ class Pool:
                                                _stream_ptr(stream)))
         return [a.reshape(shape[2], shape[1], shape[0]) for a in out]
 
-    def set_launch(self, threads=128, nodes_per_thread=1, blocks_per_sm=0, use_graph=True):
+    def set_launch(self, threads=128, nodes_per_thread=4, blocks_per_sm=0, use_graph=True):
         N.check(N.lib().vfb_pool_set_launch(self._h, int(threads), int(nodes_per_thread), int(blocks_per_sm),
                                             int(use_graph)))
 
