@@ -1548,8 +1548,8 @@ struct PoolDomain {
     double omega;                // the BC kernels' omega
     uint64_t noslip_offset;      // bytes from the arena start: int32 k[n_noslip]
     uint64_t noslip_cut_offset;  // bytes: uint32 cut[n_noslip] (bit d: q_d in [0, 1]), uint32 first[ceil(n / 32)]
-    uint64_t noslip_q_offset;    // bytes: C q[] of the cut links, node by node, directions ascending;
-                                 // first[c] = the links of nodes 0 .. 32 c - 1
+    uint64_t noslip_q_offset;    // bytes: C q[] of the cut links, per 32 nodes direction by direction
+                                 // (nodes ascending); first[c] = the links of nodes 0 .. 32 c - 1
     uint64_t noslip_guard_offset; // bytes: uint32 mask[n_noslip], uint32 first[n_noslip] (guarded directions),
                                   // uint32 guarded[n_guarded] (the list positions with a nonzero mask)
     uint64_t noslip_saved_offset; // bytes: C saved[] (their post-collision values, taken before the writes)
@@ -1750,7 +1750,7 @@ __global__ void __launch_bounds__(128) pool_noslip_guard_kernel(PoolBCArgs<typen
 // Interpolated no-slip over the pool's lists, one warp per 32 BC nodes, in two phases.
 //   nodes: lane i gathers node i's post-collision populations (guarded ones from the saved copy),
 //          forms its moments, and puts both with its slot nodes in the warp's shared memory;
-//   links: the warp's cut links (node, direction), listed in node order with directions
+//   links: the warp's cut links (node, direction), listed direction by direction with the nodes
 //          ascending, are spread over the lanes, each computing and storing one link's value.
 // Every lane does useful work in the second phase, where a thread per node would step through all
 // 26 directions with the lanes of uncut ones idle. The arithmetic is bc_moments / bc_link_value,
@@ -1816,19 +1816,20 @@ __global__ void __launch_bounds__(128) pool_noslip_kernel(PoolBCArgs<typename Co
             t.m[3 * 32 + lane] = m.uz;
             t.m[4 * 32 + lane] = m.cu_sq;
         }
-        // the warp's link list: an exclusive scan of the lanes' link counts
-        const uint32_t count = __popc(cut);
-        uint32_t incl = count;
+        // the warp's link list, direction by direction and the nodes in order within a direction
+        // (the order of the link q in the arena): 32 consecutive links mostly share a direction,
+        // so their shared-memory rows are read from distinct banks and their stores land in one
+        // plane at neighbouring nodes
+        const uint32_t lanes_below = (1u << lane) - 1u;
+        uint32_t total = 0;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= (uint32_t)o)
-                incl += v;
+        for (int d = 1; d < 27; ++d) {
+            const bool has = (cut >> d) & 1u;
+            const uint32_t ballot = __ballot_sync(0xffffffffu, has);
+            if (has)
+                t.links[total + __popc(ballot & lanes_below)] = (uint16_t)(lane | ((uint32_t)d << 5));
+            total += __popc(ballot);
         }
-        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-        uint32_t slot = incl - count;
-        for (uint32_t b = cut; b; b &= b - 1u)
-            t.links[slot++] = (uint16_t)(lane | ((uint32_t)(__ffs(b) - 1) << 5));
         __syncwarp();
         const C *q = reinterpret_cast<const C *>(arena + dm.noslip_q_offset) + cut_mask[dm.n_noslip + i0 / 32u];
         const C omega = (C)dm.omega;

@@ -502,8 +502,9 @@ uint32_t guard_tables(const vfb_pool *p, const vfb_domain_desc *d, const vfb_dom
 
 // The no-slip list in the link form of the pool's kernel: per node a mask of its cut directions
 // (q in [0, 1] in the pool's real type, the test the kernels make), after the masks the first link
-// of every 32 nodes, and the q of the links node by node, directions ascending. With
-// q_out == nullptr only the link count is returned.
+// of every 32 nodes, and the q of the links, per 32 nodes direction by direction with the nodes
+// ascending (the order in which a warp of pool_noslip_kernel lists them). With q_out == nullptr
+// only the link count is returned.
 uint64_t noslip_links(const vfb_pool *p, const vfb_domain_bcs *b, std::vector<uint32_t> *cut_first,
                       std::vector<unsigned char> *q_out)
 {
@@ -515,34 +516,36 @@ uint64_t noslip_links(const vfb_pool *p, const vfb_domain_bcs *b, std::vector<ui
         const float f = (float)q;
         return f >= 0.0f && f <= 1.0f;
     };
+    auto put = [wide, q_out](double q) {
+        if (wide) {
+            const unsigned char *c = reinterpret_cast<const unsigned char *>(&q);
+            q_out->insert(q_out->end(), c, c + 8);
+        } else {
+            const float f = (float)q;
+            const unsigned char *c = reinterpret_cast<const unsigned char *>(&f);
+            q_out->insert(q_out->end(), c, c + 4);
+        }
+    };
     if (cut_first)
         cut_first->assign((size_t)n + (n + 31) / 32, 0u);
     if (q_out)
         q_out->clear();
     uint64_t links = 0;
-    for (uint32_t i = 0; i < n; ++i) {
-        if (cut_first && i % 32 == 0)
-            (*cut_first)[(size_t)n + i / 32] = (uint32_t)links;
-        uint32_t cut = 0;
-        for (int d = 1; d < 27; ++d) {
-            const double q = b->noslip_q27[(size_t)d * n + i];
-            if (!active(q))
-                continue;
-            cut |= 1u << d;
-            ++links;
-            if (q_out) {
-                if (wide) {
-                    const unsigned char *c = reinterpret_cast<const unsigned char *>(&q);
-                    q_out->insert(q_out->end(), c, c + 8);
-                } else {
-                    const float f = (float)q;
-                    const unsigned char *c = reinterpret_cast<const unsigned char *>(&f);
-                    q_out->insert(q_out->end(), c, c + 4);
-                }
-            }
-        }
+    for (uint32_t c0 = 0; c0 < n; c0 += 32) {
+        const uint32_t c1 = std::min(n, c0 + 32);
         if (cut_first)
-            (*cut_first)[i] = cut;
+            (*cut_first)[(size_t)n + c0 / 32] = (uint32_t)links;
+        for (int d = 1; d < 27; ++d)
+            for (uint32_t i = c0; i < c1; ++i) {
+                const double q = b->noslip_q27[(size_t)d * n + i];
+                if (!active(q))
+                    continue;
+                ++links;
+                if (cut_first)
+                    (*cut_first)[i] |= 1u << d;
+                if (q_out)
+                    put(q);
+            }
     }
     return links;
 }
