@@ -1766,8 +1766,11 @@ struct LinkTile {
     uint16_t links[32 * 26];         // lane | direction << 5
 };
 
+// resident blocks per SM: 8 for FP32 storage (64 registers; 8 shared tiles fit), 7 for the 16-bit
+// forms, 4 for FP64 (its tiles are twice as large)
 template <class S, bool EVEN>
-__global__ void __launch_bounds__(128) pool_noslip_kernel(PoolBCArgs<typename Codec<S>::compute> a)
+__global__ void __launch_bounds__(128, sizeof(S) == 8 ? 4 : (sizeof(S) == 4 ? 8 : 7))
+    pool_noslip_kernel(PoolBCArgs<typename Codec<S>::compute> a)
 {
     using C = typename Codec<S>::compute;
     __shared__ LinkTile<C> tiles[kLinkWarps];
