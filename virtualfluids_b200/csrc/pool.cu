@@ -16,6 +16,7 @@
 
 #include "guards.h"
 #include "launch.h"
+#include "pool_tables.h"
 #include "vfb.h"
 
 namespace {
@@ -500,74 +501,12 @@ uint32_t guard_tables(const vfb_pool *p, const vfb_domain_desc *d, const vfb_dom
     return saved;
 }
 
-// The no-slip list in the link form of the pool's kernel: per node a mask of its cut directions
-// (q in [0, 1] in the pool's real type, the test the kernels make), after the masks the first link
-// of every 32 nodes, and the q of the links, per 32 nodes direction by direction with the nodes
-// ascending (the order in which a warp of pool_noslip_kernel lists them). With q_out == nullptr
-// only the link count is returned.
+// the no-slip list in the link form of the pool's kernel (pool_tables.h)
 uint64_t noslip_links(const vfb_pool *p, const vfb_domain_bcs *b, std::vector<uint32_t> *cut_first,
                       std::vector<unsigned char> *q_out)
 {
-    const uint32_t n = b ? b->number_of_noslip_nodes : 0;
-    const bool wide = real_size(p->desc.storage) == 8;
-    auto active = [wide](double q) {
-        if (wide)
-            return q >= 0.0 && q <= 1.0;
-        const float f = (float)q;
-        return f >= 0.0f && f <= 1.0f;
-    };
-    auto put = [wide, q_out](double q) {
-        if (wide) {
-            const unsigned char *c = reinterpret_cast<const unsigned char *>(&q);
-            q_out->insert(q_out->end(), c, c + 8);
-        } else {
-            const float f = (float)q;
-            const unsigned char *c = reinterpret_cast<const unsigned char *>(&f);
-            q_out->insert(q_out->end(), c, c + 4);
-        }
-    };
-    if (cut_first)
-        cut_first->assign((size_t)n + (n + 31) / 32, 0u);
-    if (q_out)
-        q_out->clear();
-    uint64_t links = 0;
-    for (uint32_t c0 = 0; c0 < n; c0 += 32) {
-        const uint32_t c1 = std::min(n, c0 + 32);
-        if (cut_first)
-            (*cut_first)[(size_t)n + c0 / 32] = (uint32_t)links;
-        for (int d = 1; d < 27; ++d)
-            for (uint32_t i = c0; i < c1; ++i) {
-                const double q = b->noslip_q27[(size_t)d * n + i];
-                if (!active(q))
-                    continue;
-                ++links;
-                if (cut_first)
-                    (*cut_first)[i] |= 1u << d;
-                if (q_out)
-                    put(q);
-            }
-    }
-    return links;
-}
-
-// Whether the collision of a masked domain queues its fluid nodes per warp (k17_pool_kernel): when
-// the lanes that 32-node segments mixing fluid and solid nodes would leave idle are at least 15 %
-// of the fluid nodes. Porous blocks at porosity 0.75 leave 30-36 %, ducts whose solid nodes are
-// whole wall rows 2 % (at most 14 % for the smallest); below the threshold the queue costs more
-// than the idle lanes.
-bool compact_collision(const std::vector<uint8_t> &m)
-{
-    uint64_t fluid = 0, idle = 0;
-    for (size_t s = 0; s < m.size(); s += 32) {
-        const size_t e = std::min(m.size(), s + 32);
-        uint32_t f = 0;
-        for (size_t k = s; k < e; ++k)
-            f += m[k] != 0;
-        fluid += f;
-        if (f > 0 && f < 32)
-            idle += 32 - f;
-    }
-    return fluid > 0 && idle * 100 >= fluid * 15;
+    return vfb::noslip_link_tables(b ? b->noslip_q27 : nullptr, b ? b->number_of_noslip_nodes : 0,
+                                   real_size(p->desc.storage) == 8, cut_first, q_out);
 }
 
 bool is_axis_direction(int32_t d) { return d >= VFB_DIR_P00 && d <= VFB_DIR_00M; }
@@ -816,7 +755,7 @@ int vfb_pool_add_domain_with_bcs(vfb_pool *p, const vfb_domain_desc *d, const ui
     spec.ny = d->ny;
     spec.nz = d->nz;
     spec.flags = (d->periodic_x ? 1 : 0) | (d->periodic_y ? 2 : 0) | (d->periodic_z ? 4 : 0) | (ds.has_mask ? 8 : 0) |
-                 (ds.has_mask && compact_collision(m) ? 16 : 0);
+                 (ds.has_mask && vfb::compact_collision(m) ? 16 : 0);
     spec.omega = d->omega;
     for (int i = 0; i < 3; ++i) {
         spec.lim[i] = d->quadric_limiters[i];
