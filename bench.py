@@ -2,7 +2,9 @@
 
 One "step" is one LBM time step over the whole 256^3 box (16.78 M fluid nodes). Metric: MLUPS
 (million fluid-node updates per second, whole job). The population array (3.62 GB in FP64) is
-far larger than the 126 MB L2, so no L2 flush is needed between steps.
+far larger than the 126 MB L2, so no L2 flush is needed between steps. The headline form is the
+exact FP64 arithmetic (every operation rounded as the reference's host build rounds it, so the
+result is the CPU reference's bit for bit); --arith fast times the FMA form instead.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
 
@@ -12,14 +14,18 @@ ranks' node updates / that time ("scaling": "weak").
 
 The JSON line also carries:
   roofline     : achieved HBM bytes/s of the collision kernel (432 B algorithmic per node update
-                 in FP64: 27 reads + 27 writes of 8 B) over its CUDA-event launch time, against the
-                 measured copy bandwidth of MEASURED_PEAKS.json
+                 in FP64: 27 reads + 27 writes of 8 B) over its CUDA-event launch time averaged
+                 over 200 launches, against the measured copy bandwidth of MEASURED_PEAKS.json
   e2e          : the same metric through the public API with host buffers (pinned): initial
                  fields host->device, the steps with the per-step FP64 kinetic energy read back to
                  the host, final fields device->host, all inside the timed region
-  cpu_baseline : the reference's K17 header (oracle/_ref) driven over the same layout on this
-                 box's host cores, on a bounded sample of the workload
-  forms        : MLUPS of the FP32, FP16 and BF16 shifted-population storage forms
+  forms        : the other arithmetic / storage forms (FMA FP64, FP32, FP16, BF16): MLUPS, kernel
+                 roofline and velocity error against the exact FP64 run at the same step
+  cpu_baseline : the reference's K17 header built with its Release flags (oracle/_ref), driven over
+                 the same layout on this box's host cores, on this same 256^3 workload, and on
+                 the 64^3 lid-driven cavity at Re 100 (2000 steps)
+  parity       : the cavity run on the GPU in each FP64 form against that CPU run (relative L-inf
+                 of drho and u)
 """
 from __future__ import annotations
 
@@ -42,10 +48,14 @@ N_SIDE = 256
 U0 = 0.04
 RE = 1600.0
 BYTES_PER_NODE = {"f64": 432, "f32": 216, "f16": 108, "bf16": 108}
-# DRAM bytes (read + write) per node of one launch of the FP64 direct-load collision kernel, from
-# one ncu capture at 128^3 (profiles/k17_box_kernel_f64_tgv128.md: 453.0 MB + 395.8 MB over
-# 2,097,152 nodes); traffic grows with the node count, so it is scaled to the bench's box
-NCU_DRAM_BYTES_PER_NODE_F64 = (453.033728e6 + 395.824384e6) / 2097152
+# DRAM bytes (read + write) per node of one launch of the FP64 direct-load collision kernel of each
+# arithmetic, from one ncu capture at 128^3 (2,097,152 nodes); traffic grows with the node count,
+# so it is scaled to the bench's box
+NCU_DRAM_BYTES_PER_NODE_F64 = {"fast": (453.033728e6 + 395.824384e6) / 2097152, "exact": None}
+# launches averaged for the roofline figure, whatever --steps is (a sustained, not a burst, figure)
+ROOFLINE_LAUNCHES = 200
+# most timed steps of the reference arm (CPU, about 0.3 s per 256^3 step on 16 cores)
+REFERENCE_MAX_STEPS = 60
 METRIC = "MLUPS (TGV 256^3 D3Q27 K17, FP64)"
 
 
@@ -143,57 +153,160 @@ def dist_env():
     return world, rank, local
 
 
-def cpu_baseline(seconds=12.0, threads=None):
-    """The reference K17 header (oracle/_ref) over the ET layout, all host cores, bounded sample:
-    a 64^3 periodic TGV box, as many whole steps as fit in about `seconds`."""
+def tgv_config(n, world, arith, kernel):
+    """The workload of the headline line (the reference arm reports the same one)."""
+    return {"workload": f"Taylor-Green vortex {n}^3 periodic, u0={U0}, Re={int(RE)}, D3Q27 K17 cumulant + "
+                        f"esoteric-twist streaming, FP64, per-step FP64 kinetic energy",
+            "nodes_per_gpu": n ** 3, "omega": omega_tgv(n), "replicas": world, "arith": arith, "kernel": kernel,
+            "l2": f"inputs larger than L2 ({27 * 8 * n ** 3 / 1e9:.2f} GB populations per GPU), no flush"}
+
+
+def _reference_cpu():
+    """The reference's K17 header for the host: the Release-flag build when present, else the
+    parity build, else None (the oracle's restatement is then timed)."""
+    from oracle import pyoracle
+    rel = pyoracle.ref64_release()
+    if rel is not None:
+        return rel, "reference", "reference K17 header, Release flags -O3 -funroll-all-loops"
+    par = pyoracle.ref64()
+    if par is not None:
+        return par, "reference", "reference K17 header, -O2 -ffp-contract=off"
+    return None, "port", "oracle restatement of the K17 header, -O2 -ffp-contract=off"
+
+
+def cpu_tgv(n, steps=None, seconds=None, threads=None, warmup=1):
+    """The reference CPU path on TGV n^3 periodic: the reference's K17 header over the esoteric-twist
+    layout, OpenMP over nodes on `threads` host cores, whole time steps. Either `steps` steps, or
+    as many as fit in about `seconds`. Returns (MLUPS, steps, seconds, kind, build)."""
     from oracle import pyoracle
     from virtualfluids_b200.grid import ListGrid
     threads = threads or os.cpu_count()
-    n = 64
+    ref, kind, build = _reference_cpu()
     g = ListGrid(n, n, n, periodic=(True, True, True))
-    lv = pyoracle.OracleLevel(g, omega=omega_tgv(N_SIDE))
+    lv = pyoracle.OracleLevel(g, omega=omega_tgv(n))
     lv.init(*(np.concatenate([[0.0], a]) for a in tgv_fields(n, U0)))
-    ref = pyoracle.ref64()
-    kind = "reference" if ref is not None else "port"
-    nb = lv.nb
     lim = np.full(3, 0.01)
-    steps, t0, even = 0, time.perf_counter(), 1
-    while True:
+    zero = np.zeros(3)
+
+    def sweep():
+        ev = lv.is_even.value
         if ref is not None:
-            ref.ref_collision_sweep_f64(pyoracle.ptr(lv.f), lv.n, *(pyoracle.ptr(a) for a in nb), pyoracle.ptr(lv.fluid),
-                                        lv.fluid.size, even, lv.omega, pyoracle.ptr(lim), threads)
+            ref.ref_collision_sweep_f64(pyoracle.ptr(lv.f), lv.n, *(pyoracle.ptr(a) for a in lv.nb),
+                                        pyoracle.ptr(lv.fluid), lv.fluid.size, ev, lv.omega, pyoracle.ptr(lim), threads)
         else:
-            pyoracle.lib().orc_collision(C.byref(lv.L), pyoracle.ptr(lv.fluid), lv.fluid.size, even, lv.omega,
-                                         pyoracle.ptr(lim), pyoracle.ptr(np.zeros(3)), 0, None, None, None, None,
-                                         threads)
-        even = 1 - even
-        steps += 1
+            pyoracle.lib().orc_collision(C.byref(lv.L), pyoracle.ptr(lv.fluid), lv.fluid.size, ev, lv.omega,
+                                         pyoracle.ptr(lim), pyoracle.ptr(zero), 0, None, None, None, None, threads)
+        lv.is_even.value = 1 - ev
+
+    for _ in range(warmup):
+        sweep()
+    done, t0 = 0, time.perf_counter()
+    while True:
+        sweep()
+        done += 1
         el = time.perf_counter() - t0
-        if el >= seconds and steps >= 2:
+        if (steps is not None and done >= steps) or (steps is None and el >= seconds and done >= 3):
             break
-    mlups = g.fluid.size * steps / el / 1e6
+    return g.fluid.size * done / el / 1e6, done, el, kind, build
+
+
+def cavity_grid(n):
+    """The lid-driven cavity: lid +z moving in +x, the other five sides halfway bounce-back walls."""
+    from virtualfluids_b200.grid import ListGrid
+    g = ListGrid(n, n, n)
+    for side in ("PX", "MX", "PY", "MY", "MZ"):
+        g.add_side(side, "noslip")
+    g.add_side("PZ", "velocity", velocity=(0.05, 0.0, 0.0))
+    return g
+
+
+def cpu_cavity(threads=None, steps=2000):
+    """The lid-driven cavity on the CPU: 64^3, Re 100, FP64, 2000 steps; the collision by the reference's
+    K17 header, the bounce-back BCs by the oracle's restatement of the GPU BC kernels (the reference
+    has no host form of them). Returns the timing and the final fields."""
+    from oracle import pyoracle
+    threads = threads or os.cpu_count()
+    ref, kind, build = _reference_cpu()
+    n = 64
+    g = cavity_grid(n)
+    lv = pyoracle.OracleLevel(g, omega=1.0 / (3.0 * (0.05 * n / 100.0) + 0.5))
+    lv.init()
+    t0 = time.perf_counter()
+    if ref is not None:
+        lv.run_reference_collision(ref, steps, threads=threads)
+    else:
+        lv.run(steps, threads=threads)
+    el = time.perf_counter() - t0
+    return {"mlups": round(g.fluid.size * steps / el / 1e6, 2), "steps": steps, "seconds": round(el, 2),
+            "kind": kind, "build": build}, (g, lv.omega, lv.macroscopic())
+
+
+def cpu_baseline(n, threads=None, seconds=12.0):
+    """cpu_baseline of the headline line: the reference CPU path on this same TGV n^3 workload (as
+    many whole steps as fit in about `seconds` on all host cores), plus the 64^3 cavity's 2000 steps."""
+    threads = threads or os.cpu_count()
+    mlups, steps, el, kind, build = cpu_tgv(n, seconds=seconds, threads=threads)
+    cav, cav_fields = cpu_cavity(threads)
     return {"value": round(mlups, 2), "unit": "MLUPS", "cores": threads, "kind": kind,
-            "sample": f"{steps} steps of TGV {n}^3 periodic (K17 FP64, reference header for the collision, "
-                      f"esoteric-twist layout), {el:.1f} s"}
+            "sample": f"{steps} whole steps of the same TGV {n}^3 periodic box ({build}, esoteric-twist layout, "
+                      f"OpenMP over nodes), {el:.1f} s",
+            "same_config": True, "cavity_64_2000_steps": cav, "_cavity_fields": cav_fields}
+
+
+def cavity_parity(cpu, dev):
+    """The 64^3 cavity (Re 100, 2000 steps) on the GPU through the drop-in step driver (the reference layout), in each FP64
+    form, against the CPU run: relative L-inf of drho and of each velocity component over the
+    fluid nodes."""
+    import virtualfluids_b200 as vfb
+    from virtualfluids_b200 import _native as N
+    g, omega, want = cpu
+    fl = g.geo == N.GEO_FLUID
+    out = {"workload": "64^3 lid-driven cavity, lid u = 0.05, Re 100, bounce-back walls and lid, FP64, 2000 steps",
+           "against": "cpu_baseline.cavity_64_2000_steps (reference K17 header + oracle BCs on the host)"}
+    for arith in ("exact", "fast"):
+        p = vfb.Parameter()
+        p.set_viscosity_lb((1.0 / omega - 0.5) / 3.0)
+        p.configure_main_kernel("K17CompressibleNavierStokes")
+        p.storage, p.arith = N.STORAGE_F64, (N.ARITH_EXACT if arith == "exact" else N.ARITH_FAST)
+        bcf = vfb.BoundaryConditionFactory()
+        bcf.set_no_slip_boundary_condition(bcf.NoSlipBC.NoSlipBounceBack)
+        bcf.set_velocity_boundary_condition(bcf.VelocityBC.VelocityBounceBack)
+        sim = vfb.Simulation(p, g, bcf, device=dev)
+        sim.init()
+        sim.run(2000)
+        got = sim.macroscopic()
+        sim.close()
+        err = {k: float(np.abs(got[k][fl] - want[k][fl]).max() / np.abs(want[k][fl]).max())
+               for k in ("rho", "vx", "vy", "vz")}
+        out["f64_" + arith] = {"rel_linf": err, "max_rel_linf": max(err.values()),
+                               "within_1e-12": bool(max(err.values()) <= 1e-12)}
+    return out
 
 
 def run_reference(args):
+    """The reference arm: the reference's CPU path (its K17 header, Release flags, over the same
+    esoteric-twist layout, all host cores) on the headline's own workload, TGV 256^3 FP64: W whole
+    untimed steps, then min(K, REFERENCE_MAX_STEPS) timed steps. Rank 0 only."""
     world, rank, _ = dist_env()
     if rank != 0:
         return
-    cb = cpu_baseline(seconds=max(2.0, 3.0 * args.steps / 100.0))
+    threads = os.cpu_count()
+    steps = max(1, min(args.steps, REFERENCE_MAX_STEPS))
+    mlups, done, el, kind, build = cpu_tgv(args.n, steps=steps, threads=threads, warmup=min(args.warmup, 3))
+    cb = {"value": round(mlups, 2), "unit": "MLUPS", "cores": threads, "kind": kind,
+          "sample": f"{done} timed whole steps (after {min(args.warmup, 3)} untimed) of TGV {args.n}^3 periodic "
+                    f"({build}, esoteric-twist layout, OpenMP over nodes), {el:.1f} s"}
     line = {"metric": METRIC, "value": cb["value"], "unit": "MLUPS", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "Taylor-Green vortex periodic D3Q27 K17 (reference CPU path, bounded sample)",
-                       "nodes_per_step": 64 ** 3},
+            "warmup": args.warmup, "ms_per_step": round(el / done * 1e3, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": tgv_config(args.n, 1, "exact", "auto"),
             "impl": "reference", "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 def run_batch(args):
-    """Config 4: rectangular-duct Poiseuille domains of uneven sizes in one domain pool, advanced by
+    """Batch of rectangular-duct Poiseuille domains of uneven sizes in one domain pool, advanced by
     one persistent launch per step (CUDA-graph replay, autotuned launch shape), FP32 and FP16
     storage. With --check-steps S > 0 every domain also runs S steps in FP64, FP32 and FP16 and its
     x-averaged profile is compared with the analytic start-up series and with the FP64 run."""
@@ -280,7 +393,7 @@ def run_batch(args):
 
 
 def run_cube(args):
-    """Config 3: duct flow past a wall-mounted cube (512 x 256 x 256 fluid nodes, FP32 storage) on a
+    """Duct flow past a wall-mounted cube (512 x 256 x 256 fluid nodes, FP32 storage) on a
     structured box with the reference layout's BC lists: interpolated no-slip walls, interpolated
     velocity inlet (parabolic, seeded +-1 % per node and step), non-equilibrium pressure outlet,
     interpolated bounce-back on the cube with the FP64 drag/lift every step."""
@@ -327,7 +440,7 @@ def run_cube(args):
                 "value": round(fluid / (ms / 1e3) / 1e6, 1), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "config 3: cube 32^3 on the z = 0 wall at x = 128, parabolic inlet u_max 0.05 "
+                "config": {"workload": "duct past a wall-mounted cube: cube 32^3 on the z = 0 wall at x = 128, parabolic inlet u_max 0.05 "
                                        "+-1 % per node and step (Philox), pressure outlet, Re 3000 on the cube height",
                            "fluid_nodes": fluid, "box": [Dx, Dy, Dz], "omega": omega, "setup_s": round(setup_s, 2),
                            "l2": "inputs larger than L2, no flush"},
@@ -339,7 +452,7 @@ def run_cube(args):
 
 
 def run_tgv_forms(args):
-    """Config 2 accuracy: the 256^3 Taylor-Green vortex for --form-steps steps in FP64, FP32, FP16
+    """Storage-form accuracy: the 256^3 Taylor-Green vortex for --form-steps steps in FP64, FP32, FP16
     and BF16 storage (FMA arithmetic), the FP64 kinetic-energy decay every 100 steps, and the L2 /
     L-inf velocity error of each form against the FP64 run at steps 1000, 5000 and 10000 (relative
     to the FP64 field's RMS / maximum speed)."""
@@ -525,7 +638,7 @@ def run_porous(args):
 
 
 def run_serving(args):
-    """Config 5: a Poisson stream of porous-block solves served by continuous batching in one domain
+    """Serving: a Poisson stream of porous-block solves served by continuous batching in one domain
     pool whose arena is the HBM budget. Offered loads are fractions of the measured capacity (node
     updates per second of a full pool / the mean work of a request). Reports p50/p99 time to
     solution and aggregate MLUPS in FP32 and FP16 storage, and the permeability error against each
@@ -610,8 +723,9 @@ def main():
     ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-list", action="store_true", help="skip the reference-layout (list) measurement")
-    ap.add_argument("--arith", default="fast", choices=["fast", "exact"],
-                    help="exact: every operation rounded as the reference's host build (bitwise oracle parity)")
+    ap.add_argument("--arith", default="exact", choices=["fast", "exact"],
+                    help="the headline's FP64 arithmetic. exact: every operation rounded as the reference's host "
+                         "build (bitwise oracle parity); fast: FMA contraction and a rearranged K17")
     ap.add_argument("--kernel", default="auto", choices=["auto", "direct", "tma", "async"])
     ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "serving", "tgv-forms", "cube", "porous"],
                     help="tgv: the headline (TGV 256^3 FP64); batch: 4096 ducts in one domain pool; "
@@ -647,6 +761,13 @@ def main():
         run_porous(args)
         return
 
+    run_tgv(args)
+
+
+def run_tgv(args):
+    """The headline: TGV 256^3 FP64 through the structured box, with the roofline loop, the end-to-end
+    run through the C ABI, the other forms with their errors against FP64, the reference layout,
+    and (rank 0, one GPU) the CPU baseline on this same workload plus the cavity's parity."""
     import torch
 
     import virtualfluids_b200 as vfb
@@ -678,6 +799,15 @@ def main():
     def max_over_ranks(x):
         return max_over_ranks_of(x, pg, dev)
 
+    def timed_steps(box, steps, energy=None):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            box.step(steps, energy=energy, stream=sp)
+            ev1.record(stream)
+        stream.synchronize()
+        return ev0.elapsed_time(ev1)
+
     # ---- device-resident throughput: K steps with the per-step FP64 energy kept on the device ----
     box = vfb.Box(n, n, n, omega, storage="f64", arith=args.arith)
     box.set_kernel_variant(args.kernel)
@@ -685,36 +815,27 @@ def main():
     energy = torch.zeros(2 * max(args.steps, args.warmup), dtype=torch.float64, device=dev)
     box.step(args.warmup, energy=energy, stream=sp)
     barrier()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     launches0 = box.kernel_launches()
     with ClockSampler(local) as clk:
-        with torch.cuda.stream(stream):
-            ev0.record(stream)
-            box.step(args.steps, energy=energy, stream=sp)
-            ev1.record(stream)
-        stream.synchronize()
+        t_local = timed_steps(box, args.steps, energy)
     launches = box.kernel_launches() - launches0
     barrier()
-    t_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    t_ms = max_over_ranks(t_local)
     value = whole_job_mlups(nodes * args.steps, world, t_ms)
     clocks = clk.summary()
 
-    # ---- the collision kernel alone: average launch time for the roofline ----
-    kb = min(args.steps, 200)
-    with torch.cuda.stream(stream):
-        ev0.record(stream)
-        box.step(kb, stream=sp)
-        ev1.record(stream)
-    stream.synchronize()
-    k_ms = ev0.elapsed_time(ev1) / kb
+    # ---- the collision kernel alone: average of ROOFLINE_LAUNCHES launches, whatever --steps is ----
+    k_ms = timed_steps(box, ROOFLINE_LAUNCHES) / ROOFLINE_LAUNCHES
     peak, peak_kind = measured_peak()
     achieved = BYTES_PER_NODE["f64"] * nodes / (k_ms / 1e3) / 1e9
+    per_node = NCU_DRAM_BYTES_PER_NODE_F64.get(args.arith) if args.kernel in ("auto", "direct") else None
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                "traffic": round(NCU_DRAM_BYTES_PER_NODE_F64 * nodes) if args.kernel in ("auto", "direct") else None,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 128^3 launch, "
-                                  "scaled by nodes",
-                "kernel": "k17_box_kernel<double> (collision + ET streaming)", "kernel_ms": round(k_ms, 4),
+                "traffic": round(per_node * nodes) if per_node else None,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 128^3 launch of the "
+                                  "same kernel, scaled by nodes",
+                "kernel": f"k17_box_kernel<double> ({args.arith} arithmetic; collision + ET streaming)",
+                "kernel_ms": round(k_ms, 4), "launches_timed": ROOFLINE_LAUNCHES,
                 "algorithmic_bytes_per_launch": BYTES_PER_NODE["f64"] * nodes}
     e_host = energy[: 2 * args.steps].cpu().numpy()
     box.status()
@@ -724,7 +845,7 @@ def main():
     # ---- end to end through the public API with pinned host buffers ----
     host_in = [torch.from_numpy(a).pin_memory() for a in fields]
     host_out = [torch.empty(nodes, dtype=torch.float64).pin_memory() for _ in range(4)]
-    host_energy = torch.zeros(2 * args.steps, dtype=torch.float64).pin_memory()
+    host_energy = torch.zeros(2 * max(args.steps, args.warmup), dtype=torch.float64).pin_memory()
     box = vfb.Box(n, n, n, omega, storage="f64", arith=args.arith)
     box.set_kernel_variant(args.kernel)
     lib = N.lib()
@@ -733,6 +854,7 @@ def main():
     N.check(lib.vfb_box_step(box._h, args.warmup, C.c_void_p(host_energy.data_ptr()), 1, sp))
     stream.synchronize()
     barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0 = time.perf_counter()
     with torch.cuda.stream(stream):
         ev0.record(stream)
@@ -747,51 +869,60 @@ def main():
     e2e_value = whole_job_mlups(nodes * args.steps, world, e2e_ms)
     h2d = 4 * nodes * 8
     d2h = 4 * nodes * 8 + 16 * args.steps
-    ek = host_energy.numpy()[1::2]
+    ek = host_energy.numpy()[1: 2 * args.steps: 2]
     assert np.all(np.isfinite(host_out[1].numpy())) and ek[-1] < ek[0], "e2e run produced no decaying vortex"
     del box
     torch.cuda.empty_cache()
 
-    # ---- other storage forms (device resident) ----
+    # ---- the other forms: roofline loop each, and the velocity error against the exact FP64 run
+    # at the same step (W warm-up + ROOFLINE_LAUNCHES steps) ----
     forms = {}
     if not args.no_forms:
-        for st in ("f32", "f16", "bf16"):
-            b = vfb.Box(n, n, n, omega, storage=st)
-            if args.kernel != "async" or st == "f32":
+        cmp_steps = args.warmup + ROOFLINE_LAUNCHES
+        ref = vfb.Box(n, n, n, omega, storage="f64", arith="exact")
+        ref.init(*(torch.from_numpy(a).to(dev) for a in fields), stream=sp)
+        ref.step(cmp_steps, stream=sp)
+        want = ref.fields(stream=sp)
+        del ref
+        torch.cuda.empty_cache()
+        other = "f64_fast" if args.arith == "exact" else "f64_exact"
+        for name in (other, "f32", "f16", "bf16"):
+            st = "f64" if name.startswith("f64") else name
+            ar = name[4:] if name.startswith("f64") else "fast"
+            dt = np.float64 if st == "f64" else np.float32
+            b = vfb.Box(n, n, n, omega, storage=st, arith=ar)
+            if args.kernel != "async" or st in ("f64", "f32"):
                 b.set_kernel_variant(args.kernel)
-            b.init(*(torch.from_numpy(a.astype(np.float32)).to(dev) for a in fields), stream=sp)
+            b.init(*(torch.from_numpy(a.astype(dt)).to(dev) for a in fields), stream=sp)
             b.step(args.warmup, stream=sp)
-            ks = min(args.steps, 200)
-            with torch.cuda.stream(stream):
-                ev0.record(stream)
-                b.step(ks, stream=sp)
-                ev1.record(stream)
-            stream.synchronize()
-            ms = ev0.elapsed_time(ev1) / ks
-            forms[st] = {"mlups": round(nodes / (ms / 1e3) / 1e6, 1),
-                         "hbm_gbs": round(BYTES_PER_NODE[st] * nodes / (ms / 1e3) / 1e9, 1)}
+            ms = timed_steps(b, ROOFLINE_LAUNCHES) / ROOFLINE_LAUNCHES
+            got = b.fields(stream=sp)
+            gbs = BYTES_PER_NODE[st] * nodes / (ms / 1e3) / 1e9
+            forms[name] = {"mlups": round(nodes / (ms / 1e3) / 1e6, 1), "kernel_ms": round(ms, 4),
+                           "hbm_gbs": round(gbs, 1), "frac": round(gbs / peak, 4),
+                           "error_vs_f64_exact": field_errors(got, want, cmp_steps)}
             del b
             torch.cuda.empty_cache()
+        if "f16" in forms:
+            forms["f16"]["speedup_vs_headline_kernel"] = round(k_ms / forms["f16"]["kernel_ms"], 3)
+            forms["bf16"]["speedup_vs_headline_kernel"] = round(k_ms / forms["bf16"]["kernel_ms"], 3)
 
     # ---- the reference layout: the drop-in step driver over neighborX/Y/Z lists (device resident) ----
     ref_layout = None
     if not args.no_list:
         ref_layout = run_list_path(args, n, omega, fields, dev)
 
-    cb = None
+    cb = parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cb = cpu_baseline()
+        cb = cpu_baseline(n, threads=os.cpu_count())
+        parity = cavity_parity(cb.pop("_cavity_fields"), dev)
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(t_ms / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"Taylor-Green vortex {n}^3 periodic, u0={U0}, Re={int(RE)}, D3Q27 K17 cumulant + "
-                                   f"esoteric-twist streaming, FP64, per-step FP64 kinetic energy",
-                       "nodes_per_gpu": nodes, "omega": omega, "replicas": world, "arith": args.arith,
-                       "kernel": args.kernel,
-                       "l2": "inputs larger than L2 (3.62 GB populations per GPU), no flush"},
+            "config": tgv_config(n, world, args.arith, args.kernel),
             "roofline": roofline,
             "e2e": {"value": round(e2e_value, 1), "unit": "MLUPS", "h2d_bytes_per_step": h2d // args.steps,
                     "d2h_bytes_per_step": d2h // args.steps, "wall_s": round(wall_e2e, 3)},
@@ -804,10 +935,26 @@ def main():
             line["reference_layout"] = ref_layout
         if cb:
             line["cpu_baseline"] = cb
+        if parity:
+            line["parity"] = parity
         print(json.dumps(line), flush=True)
     if pg:
         pg.destroy_process_group()
 
+
+def field_errors(got, want, steps):
+    """Velocity error of a form against the exact FP64 run at the same step: relative L2 (RMS of the
+    speed of the difference over the RMS speed) and relative L-inf (largest speed of the difference
+    over the largest speed); for the FP64 forms also the relative L-inf of drho."""
+    u = np.stack([got["vx"], got["vy"], got["vz"]]).astype(np.float64)
+    w = np.stack([want["vx"], want["vy"], want["vz"]])
+    d2 = ((u - w) ** 2).sum(axis=0)
+    w2 = (w ** 2).sum(axis=0)
+    out = {"step": steps, "u_l2_rel": float(np.sqrt(d2.mean() / w2.mean())),
+           "u_linf_rel": float(np.sqrt(d2.max() / w2.max()))}
+    if got["rho"].dtype == np.float64:
+        out["drho_linf_rel"] = float(np.abs(got["rho"] - want["rho"]).max() / np.abs(want["rho"]).max())
+    return out
 
 if __name__ == "__main__":
     main()

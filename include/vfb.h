@@ -234,9 +234,11 @@ int vfb_mass_energy(const vfb_level *level, const uint32_t *node_indices, uint32
    counterpart in the reference. The per-block partial sums live in a fixed array inside the
    library's device memory (about 1 MiB on every GPU that loads the library, held until the
    process exits), so the node count is limited to VFB_NO_ALLOC_MAX_NODES; larger sizes are
-   rejected with VFB_ERR_INVALID_ARGUMENT. The first call on a device looks the array's device
-   address up (make it before any stream capture). All calls share the array, so calls that
-   overlap on the GPU race; each call overwrites what it reads back. Synchronises the stream. */
+   rejected with VFB_ERR_INVALID_ARGUMENT; the level is checked as vfb_mass_energy checks it.
+   Every call looks the array's device address up on the current device; the first call on a
+   device also loads the library's device code there, so make it before any stream capture. All
+   calls share the array, so calls that overlap on the GPU race; each call overwrites what it
+   reads back. Synchronises the stream. */
 #define VFB_NO_ALLOC_MAX_NODES (1u << 24)
 int vfb_mass_energy_no_alloc(const vfb_level *level, const uint32_t *node_indices, uint32_t size, double out[2],
                              void *stream);

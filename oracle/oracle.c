@@ -143,6 +143,46 @@ void orc_collision(orc_level *L, const uint32_t *idx, uint32_t n_idx, int is_eve
     }
 }
 
+/* RunCollision.cuh:75-143 for every CollisionTemplate: the body-force variant adds the node's body
+   force to the global forcing before the half-force scaling ((forces[c] + bodyForce[k]) * c1o2 *
+   forceFactor, :88-90) and resets the node's body force (:93-95); the macroscopic variant writes
+   drho and the velocity after the collision (:133-138). Sequential over the list. */
+void orc_collision_template(orc_level *L, const uint32_t *idx, uint32_t n_idx, int is_even, double omega,
+                            const double lim[3], const double forces[3], int level, int write_macro, int body_force,
+                            double *rho, double *vx, double *vy, double *vz, double *bfx, double *bfy, double *bfz)
+{
+    double factor = 1.0;
+    for (int i = 1; i <= level; ++i)
+        factor *= 2.0;
+    factor = 1.0 / factor;
+    for (uint32_t i = 0; i < n_idx; ++i) {
+        const uint32_t k = idx[i];
+        double fx, fy, fz;
+        if (body_force) {
+            fx = (forces[0] + bfx[k]) * 0.5 * factor;
+            fy = (forces[1] + bfy[k]) * 0.5 * factor;
+            fz = (forces[2] + bfz[k]) * 0.5 * factor;
+            bfx[k] = 0.0;
+            bfy[k] = 0.0;
+            bfz[k] = 0.0;
+        } else {
+            fx = forces[0] * 0.5 * factor;
+            fy = forces[1] * 0.5 * factor;
+            fz = forces[2] * 0.5 * factor;
+        }
+        double f[27], macro[4];
+        orc_read_pre(L, k, is_even, f);
+        orc_k17_f64(f, omega, lim, fx, fy, fz, macro);
+        if (write_macro) {
+            vx[k] = macro[1];
+            vy[k] = macro[2];
+            vz[k] = macro[3];
+            rho[k] = macro[0];
+        }
+        orc_write_post(L, k, is_even, f);
+    }
+}
+
 /* ---------------- boundary conditions ---------------- */
 
 /* c . u as the reference kernels spell it: signed sum in x, y, z order (e.g. -vx1 - vx2 + vx3) */
@@ -178,7 +218,11 @@ static double *read_posts(const orc_level *L, const int32_t *k, uint32_t nbc, in
         fprintf(stderr, "oracle: out of memory for a BC list of %u nodes\n", nbc);
         abort();
     }
-    for (uint32_t i = 0; i < nbc; ++i)
+    /* each node fills its own row */
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+    for (int64_t i = 0; i < (int64_t)nbc; ++i)
         read_post(L, (uint32_t)k[i], is_even, all + 27 * (size_t)i);
     return all;
 }
@@ -189,7 +233,11 @@ void orc_bc_noslip_bounce_back(orc_level *L, const int32_t *k, const double *q27
     int map_next[27];
     orc_pointer_map(!is_even, map_next);
     double *all = read_posts(L, k, nbc, is_even);
-    for (uint32_t i = 0; i < nbc; ++i) {
+    /* all reads are done: every entry writes only its own node's slots */
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+    for (int64_t i = 0; i < (int64_t)nbc; ++i) {
         const uint32_t node = (uint32_t)k[i];
         const double *post = all + 27 * (size_t)i;
         for (int d = 1; d < 27; ++d)
@@ -207,7 +255,11 @@ void orc_bc_velocity_bounce_back(orc_level *L, const int32_t *k, const double *q
     int map_next[27];
     orc_pointer_map(!is_even, map_next);
     double *all = read_posts(L, k, nbc, is_even);
-    for (uint32_t i = 0; i < nbc; ++i) {
+    /* all reads are done: every entry writes only its own node's slots */
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+    for (int64_t i = 0; i < (int64_t)nbc; ++i) {
         const uint32_t node = (uint32_t)k[i];
         const double *post = all + 27 * (size_t)i;
         for (int d = 1; d < 27; ++d) {
@@ -275,7 +327,11 @@ void orc_bc_noslip_interpolated(orc_level *L, const int32_t *k, const double *q2
     int map_next[27];
     orc_pointer_map(!is_even, map_next);
     double *all = read_posts(L, k, nbc, is_even);
-    for (uint32_t i = 0; i < nbc; ++i) {
+    /* all reads are done: every entry writes only its own node's slots */
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+    for (int64_t i = 0; i < (int64_t)nbc; ++i) {
         const uint32_t node = (uint32_t)k[i];
         const double *post = all + 27 * (size_t)i;
         double drho, vx, vy, vz, cu_sq;
@@ -298,7 +354,11 @@ void orc_bc_velocity_interpolated(orc_level *L, const int32_t *k, const double *
     int map_next[27];
     orc_pointer_map(!is_even, map_next);
     double *all = read_posts(L, k, nbc, is_even);
-    for (uint32_t i = 0; i < nbc; ++i) {
+    /* all reads are done: every entry writes only its own node's slots */
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+    for (int64_t i = 0; i < (int64_t)nbc; ++i) {
         const uint32_t node = (uint32_t)k[i];
         const double *post = all + 27 * (size_t)i;
         double drho, vx, vy, vz, cu_sq;
@@ -361,7 +421,11 @@ void orc_init(orc_level *L, const uint32_t *geo, const double *rho, const double
 {
     int map[27];
     orc_pointer_map(is_even, map);
-    for (uint64_t k = 0; k < L->n; ++k) {
+    /* every node writes its own 27 slots: the loop runs in parallel */
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+    for (int64_t k = 0; k < (int64_t)L->n; ++k) {
         if (geo[k] == 15u || geo[k] == 16u)
             continue;
         const double drho = rho[k], vx = ux[k], vy = uy[k], vz = uz[k];

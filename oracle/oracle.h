@@ -63,6 +63,12 @@ void orc_write_post(orc_level *L, uint32_t k, int is_even, const double in[27]);
 void orc_collision(orc_level *L, const uint32_t *idx, uint32_t n_idx, int is_even, double omega,
                    const double lim[3], const double forces[3], int level,
                    double *rho, double *vx, double *vy, double *vz, int n_threads);
+/* the same with the features of a CollisionTemplate (K17CompressibleNavierStokes.cu:114-139):
+   body_force reads (forces + bodyForce[k]) * 0.5 * 2^-level and resets bodyForce[k] to zero
+   (RunCollision.cuh:88-98); write_macro stores drho and u at k (:133-138) */
+void orc_collision_template(orc_level *L, const uint32_t *idx, uint32_t n_idx, int is_even, double omega,
+                            const double lim[3], const double forces[3], int level, int write_macro, int body_force,
+                            double *rho, double *vx, double *vy, double *vz, double *bfx, double *bfy, double *bfz);
 
 /* boundary conditions, QforBoundaryConditions layout: k[nbc], q27[dir*nbc + i] */
 void orc_bc_noslip_bounce_back(orc_level *L, const int32_t *k, const double *q27, uint32_t nbc, int is_even);

@@ -19,7 +19,9 @@ HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
 REF64 = HERE / "_ref" / "libvfref64.so"
 REF32 = HERE / "_ref" / "libvfref32.so"
+REF64_RELEASE = HERE / "_ref" / "libvfref64_release.so"
 REFGPU = HERE / "_ref" / "libvfref_gpu64.so"
+REFGPU32 = HERE / "_ref" / "libvfref_gpu32.so"
 
 _P = C.c_void_p
 _lib = None
@@ -28,7 +30,7 @@ _lib = None
 def build(reference: str | None = None) -> None:
     """Build liboracle.so, and the reference pins when the reference tree is present."""
     subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
-    ref = reference or "/root/reference"
+    ref = reference or os.environ.get("VFB_REFERENCE_DIR", "/root/reference")
     if Path(ref).is_dir():
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={ref}"], check=True)
 
@@ -48,6 +50,7 @@ def lib():
         L.orc_macro_compressible_f64.argtypes = [_P, _P, _P, _P, _P, _P]
         L.orc_chimera_f64.argtypes = [i, _P, d, d, d, d]
         L.orc_collision.argtypes = [_P, _P, u, i, d, _P, _P, i, _P, _P, _P, _P, i]
+        L.orc_collision_template.argtypes = [_P, _P, u, i, d, _P, _P, i, i, i] + [_P] * 7
         L.orc_bc_noslip_bounce_back.argtypes = [_P, _P, _P, u, i]
         L.orc_bc_noslip_interpolated.argtypes = [_P, _P, _P, u, i, d]
         L.orc_bc_velocity_bounce_back.argtypes = [_P, _P, _P, u, i, _P, _P, _P]
@@ -92,13 +95,29 @@ def ref32():
     return L
 
 
-def refgpu():
-    """The reference's own CUDA kernels (FP64, built from the reference tree), or None."""
-    if not REFGPU.exists():
+def ref64_release():
+    """The FP64 reference-header shim built with the reference's Release flags (-O3
+    -funroll-all-loops), the timed CPU baseline; None if it has not been built."""
+    if not REF64_RELEASE.exists():
         return None
-    L = C.CDLL(str(REFGPU))
-    u, i, d, u64 = C.c_uint32, C.c_int, C.c_double, C.c_uint64
+    L = C.CDLL(str(REF64_RELEASE))
+    d = C.c_double
+    L.ref_k17_f64.argtypes = [_P, d, _P, d, d, d, _P]
+    L.ref_collision_sweep_f64.argtypes = [_P, C.c_uint64, _P, _P, _P, _P, C.c_uint32, C.c_int, d, _P, C.c_int]
+    return L
+
+
+def refgpu(real_bytes: int = 8):
+    """The reference's own CUDA kernels built from the reference tree, or None: FP64
+    (real_bytes = 8) or FP32 (real_bytes = 4, real = float)."""
+    path = REFGPU if real_bytes == 8 else REFGPU32
+    if not path.exists():
+        return None
+    L = C.CDLL(str(path))
+    u, i, u64 = C.c_uint32, C.c_int, C.c_uint64
+    d = C.c_double if real_bytes == 8 else C.c_float
     L.refgpu_k17.argtypes = [_P, u64, _P, _P, _P, _P, u, i, d, _P, _P, d]
+    L.refgpu_k17_template.argtypes = [_P, u64, _P, _P, _P, _P, u, i, d, _P, _P, d] + [_P] * 7 + [i]
     L.refgpu_noslip_bounce_back.argtypes = [_P, _P, _P, u, _P, _P, _P, u64, i]
     L.refgpu_noslip_interpolated.argtypes = [_P, _P, _P, u, d, _P, _P, _P, u64, i]
     L.refgpu_velocity_bounce_back.argtypes = [_P, _P, _P, _P, _P, _P, u, _P, _P, _P, u64, i]
@@ -119,7 +138,9 @@ def refgpu():
 
 
 def ptr(a: np.ndarray):
-    return C.c_void_p(a.ctypes.data) if a is not None else C.c_void_p(0)
+    """A void pointer to the array's data that keeps the array alive while the pointer lives (so
+    a temporary array passed straight into a call is not freed before the call reads it)."""
+    return a.ctypes.data_as(C.c_void_p) if a is not None else C.c_void_p(0)
 
 
 class _Level(C.Structure):
@@ -212,6 +233,37 @@ class OracleLevel:
             raise MemoryError("oracle step driver could not allocate its drag workspace")
         if hist is not None:
             self.drag_history.extend(hist)
+
+    def run_reference_collision(self, ref, steps, threads=0):
+        """The same time steps with the collision sweep of the reference's own K17 header (`ref`,
+        ref64() or ref64_release(): ref_collision_sweep_f64 over the esoteric-twist layout) and the
+        boundary conditions of the oracle, in UpdateGrid27 order (collision, velocity BC, no-slip
+        BC, parity toggle). Levels with forcing, a geometry BC or pressure BCs are not supported."""
+        if self.geo_bc is not None or self.n_pr or np.any(self.forces != 0.0) or self.level != 0:
+            raise ValueError("run_reference_collision covers unforced single levels with velocity and no-slip BCs")
+        L = lib()
+        lim = np.ascontiguousarray(self.lim)
+        for _ in range(int(steps)):
+            ev = self.is_even.value
+            ref.ref_collision_sweep_f64(ptr(self.f), self.n, *(ptr(a) for a in self.nb), ptr(self.fluid),
+                                        self.fluid.size, ev, self.omega, ptr(lim), int(threads))
+            v = self.vel
+            if v is not None and v.n:
+                if v.kind == 1:
+                    L.orc_bc_velocity_bounce_back(C.byref(self.L), v.k, v.q, v.n, ev, v.ux, v.uy, v.uz)
+                elif v.kind == 2:
+                    L.orc_bc_velocity_interpolated(C.byref(self.L), v.k, v.q, v.n, ev, self.omega, v.ux, v.uy, v.uz)
+                else:
+                    raise ValueError("velocity BC kind not covered")
+            b = self.ns
+            if b is not None and b.n:
+                if b.kind == 1:
+                    L.orc_bc_noslip_bounce_back(C.byref(self.L), b.k, b.q, b.n, ev)
+                elif b.kind == 2:
+                    L.orc_bc_noslip_interpolated(C.byref(self.L), b.k, b.q, b.n, ev, self.omega)
+                else:
+                    raise ValueError("no-slip BC kind not covered")
+            self.is_even.value = 1 - ev
 
     def macroscopic(self):
         out = [np.zeros(self.n) for _ in range(5)]

@@ -3,7 +3,8 @@
  *
  * The reference's own GPU kernels of the hot path, compiled with nvcc from the reference source
  * tree where it lies (the kernel sources are included by path; nothing is copied) into
- * _ref/libvfref_gpu64.so (FP64, real = double). Plain C entry points take device pointers and
+ * _ref/libvfref_gpu64.so (FP64, real = double) and _ref/libvfref_gpu32.so (FP32, real = float; the
+ * collision entry points only are used from it). Plain C entry points take device pointers and
  * launch the reference kernels with a one-dimensional grid, which their index calculation
  * (cuda_helper/CudaIndexCalculation.h get1DIndexFrom2DBlock) maps onto the same node indices as
  * the reference's own launchers. Built with -fmad=false, so every operation rounds on its own as
@@ -91,6 +92,36 @@ int refgpu_k17(real *dist, uint64_t n, unsigned *nbx, unsigned *nby, unsigned *n
     };
     vf::gpu::runCollision<decltype(collision), vf::lbm::TurbulenceModel::None, false, false>
         <<<blocks_for(n_fluid), kThreads>>>(collision, p);
+    return done();
+}
+
+/* K17CompressibleNavierStokes<None>::runOnIndices with any CollisionTemplate: the template
+   switch of K17CompressibleNavierStokes.cu:114-139 (WriteMacroVars -> runCollision<.., true, false>,
+   ApplyBodyForce -> <false, true>, AllFeatures and SubDomainBorder -> <true, true>); rho, vx, vy, vz
+   receive the macroscopic values, bfx/bfy/bfz are the per-node body forces (read, then reset) */
+int refgpu_k17_template(real *dist, uint64_t n, unsigned *nbx, unsigned *nby, unsigned *nbz, const unsigned *fluid,
+                        unsigned n_fluid, int is_even, real omega, real *forces, real *limiters, real force_factor,
+                        real *rho, real *vx, real *vy, real *vz, real *bfx, real *bfy, real *bfz, int tmpl)
+{
+    if (n_fluid == 0)
+        return 0;
+    vf::gpu::GPUCollisionParameter p { omega,   nbx,  nby,  nbz,  dist, rho,  vx,  vy,  vz,  nullptr, 0, (int)n,
+                                       force_factor, forces, bfx,  bfy,  bfz, limiters, is_even != 0, fluid, n_fluid };
+    auto collision = [] __device__(vf::lbm::CollisionParameter & parameter, vf::lbm::MacroscopicValues & macroscopicValues,
+                                   vf::lbm::TurbulentViscosity & turbulentViscosity) {
+        return vf::lbm::runK17CompressibleNavierStokes<vf::lbm::TurbulenceModel::None>(parameter, macroscopicValues,
+                                                                                        turbulentViscosity);
+    };
+    using F = decltype(collision);
+    constexpr auto none = vf::lbm::TurbulenceModel::None;
+    switch (tmpl) {
+    case 0: vf::gpu::runCollision<F, none, false, false><<<blocks_for(n_fluid), kThreads>>>(collision, p); break;
+    case 1: vf::gpu::runCollision<F, none, true, false><<<blocks_for(n_fluid), kThreads>>>(collision, p); break;
+    case 2: vf::gpu::runCollision<F, none, false, true><<<blocks_for(n_fluid), kThreads>>>(collision, p); break;
+    case 3:
+    case 4: vf::gpu::runCollision<F, none, true, true><<<blocks_for(n_fluid), kThreads>>>(collision, p); break;
+    default: return -1;
+    }
     return done();
 }
 

@@ -151,7 +151,7 @@ def test_mass_energy_and_macros_match_oracle(oracle, cuda):
 
 @pytest.mark.parametrize("arith", [N.ARITH_EXACT, N.ARITH_FAST])
 def test_lid_driven_cavity_64_2000_steps(oracle, cuda, arith):
-    """Config 1: 64^3 cavity, lid u=0.05 in +x, Re=100, FP64, 2000 steps, bounce-back walls and lid.
+    """The 64^3 lid-driven cavity: lid u=0.05 in +x, Re=100, FP64, 2000 steps, bounce-back walls and lid.
 
     Exact arithmetic reproduces the oracle bit for bit (so within any tolerance, 1e-12 included).
     With FMA contraction the result differs from the oracle by the amplified rounding: the oracle
@@ -168,7 +168,7 @@ def test_lid_driven_cavity_64_2000_steps(oracle, cuda, arith):
     a, b = sim.macroscopic(), orc.macroscopic()
     fl = g.geo == N.GEO_FLUID
     errs = {k: rel_linf(a[k], b[k], fl) for k in ("rho", "vx", "vy", "vz")}
-    print("config 1 relative L-inf vs oracle:", "exact" if arith == N.ARITH_EXACT else "fma", errs)
+    print("64^3 cavity relative L-inf vs oracle:", "exact" if arith == N.ARITH_EXACT else "fma", errs)
     (m1, _), (m2, _) = sim.mass_energy(), orc.mass_energy()
     assert np.abs(b["vx"][fl]).max() > 0.01  # the flow is developed
     if arith == N.ARITH_EXACT:

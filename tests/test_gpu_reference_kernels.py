@@ -187,7 +187,7 @@ def test_cavity_bounce_back_matches_reference_gpu_kernels_bitwise(ref, cuda):
 
 
 def test_lid_driven_cavity_64_2000_steps_matches_reference_gpu_kernels_bitwise(ref, cuda):
-    """Config 1 (64^3 cavity, lid 0.05, Re = 100, FP64, 2000 steps) through the reference's own
+    """The 64^3 lid-driven cavity (lid 0.05, Re = 100, FP64, 2000 steps) through the reference's own
     kernels and through the library: identical populations, hence identical fields and mass."""
     n = 64
     omega = 1.0 / (3.0 * (0.05 * n / 100.0) + 0.5)

@@ -154,6 +154,26 @@ def test_oracle_cavity_bounce_back_conserves_mass(oracle):
     assert e1 > 0.0                     # the lid drives the flow
 
 
+def test_cpu_baseline_step_equals_oracle_step_bitwise(oracle):
+    """The timed CPU baseline advances a level with the reference header's collision sweep (the
+    parity build and the Release-flag build) and the oracle's boundary conditions; both give the
+    oracle's own time step bit for bit, on a cavity with bounce-back and with interpolated BCs."""
+    builds = [b for b in (oracle.ref64(), oracle.ref64_release()) if b is not None]
+    if not builds:
+        pytest.skip("reference pins not built here")
+    for kind in (1, 2):
+        g = _ldc_grid(10)
+        want = oracle.OracleLevel(g, omega=1.7, velocity_kind=kind, noslip_kind=kind)
+        want.init()
+        want.run(25)
+        for ref in builds:
+            got = oracle.OracleLevel(g, omega=1.7, velocity_kind=kind, noslip_kind=kind)
+            got.init()
+            got.run_reference_collision(ref, 25, threads=2)
+            assert got.is_even.value == want.is_even.value
+            assert np.array_equal(got.f, want.f)
+
+
 # refinement interpolation (InterpolationCoefficients.h, InterpolationCF.h, InterpolationFC.h).
 # The oracle forms the same polynomial with its sums in another order, so the pin is a tolerance:
 # per cell, the largest deviation relative to the largest population.

@@ -5,7 +5,8 @@ allocation on the GPU, a solver loop that runs under a strict no-allocation rule
 not call cudaMalloc because that call can stall the whole device. For them the reduction keeps its
 scratch space (the per-block partial sums) in a fixed array inside the library's own device
 memory. These tests call that entry point through the C ABI and check it against the regular
-entry point, which takes caller-provided workspace, on two calls in a row.
+entry point, which takes caller-provided workspace, on two calls in a row. Both run the same
+partial-sum kernel and the same fixed-order reduction, so the results must be the same bits.
 """
 import ctypes as C
 
@@ -19,7 +20,7 @@ from virtualfluids_b200 import _native as N
 pytestmark = pytest.mark.gpu
 
 
-def _cavity_simulation(n=16, storage=N.STORAGE_F64):
+def _cavity_simulation(n=16, storage=N.STORAGE_F64, arith=N.ARITH_FAST):
     g = ListGrid(n, n, n)
     for s in ("PX", "MX", "PY", "MY", "MZ"):
         g.add_side(s, "noslip")
@@ -28,6 +29,7 @@ def _cavity_simulation(n=16, storage=N.STORAGE_F64):
     p.set_viscosity_lb(0.05 * n / 100.0)
     p.configure_main_kernel("K17CompressibleNavierStokes")
     p.storage = storage
+    p.arith = arith
     bcf = BCF()
     bcf.set_no_slip_boundary_condition(BCF.NoSlipBC.NoSlipBounceBack)
     bcf.set_velocity_boundary_condition(BCF.VelocityBC.VelocityBounceBack)
@@ -49,9 +51,11 @@ def _no_alloc(sim):
     return out[0], out[1]
 
 
-@pytest.mark.parametrize("storage", [N.STORAGE_F64, N.STORAGE_F32])
-def test_no_alloc_reduction_matches_workspace_reduction_twice(cuda, storage):
-    sim = _cavity_simulation(storage=storage)
+@pytest.mark.parametrize("storage, arith", [
+    (N.STORAGE_F64, N.ARITH_FAST), (N.STORAGE_F32, N.ARITH_FAST), (N.STORAGE_F16, N.ARITH_FAST),
+    (N.STORAGE_BF16, N.ARITH_FAST), (N.STORAGE_F64, N.ARITH_EXACT), (N.STORAGE_F32, N.ARITH_EXACT)])
+def test_no_alloc_reduction_matches_workspace_reduction_twice(cuda, storage, arith):
+    sim = _cavity_simulation(storage=storage, arith=arith)
     sim.run(30)
     first_ref = _with_workspace(sim)
     first = _no_alloc(sim)
@@ -60,7 +64,7 @@ def test_no_alloc_reduction_matches_workspace_reduction_twice(cuda, storage):
     second_ref = _with_workspace(sim)
     second = _no_alloc(sim)
     for got, ref in ((first, first_ref), (second, second_ref)):
-        np.testing.assert_allclose(got, ref, rtol=1e-14, atol=0.0)
+        assert np.array_equal(np.array(got), np.array(ref)), (got, ref)
     assert second[1] != first[1]  # the flow developed between the calls
     assert first[1] > 0.0
 
@@ -73,3 +77,18 @@ def test_no_alloc_rejects_more_nodes_than_its_scratch_holds(cuda):
                                               None)
     assert status == N.VFB_ERR_INVALID_ARGUMENT
     assert b"VFB_NO_ALLOC_MAX_NODES" in N.lib().vfb_last_error()
+
+
+def test_no_alloc_rejects_the_levels_vfb_mass_energy_rejects(cuda):
+    """A bad level is refused by both entry points with the same status, also for an empty list."""
+    sim = _cavity_simulation(n=8)
+    out = (C.c_double * 2)()
+    bad = type(sim.level).from_buffer_copy(sim.level)
+    bad.arith = 7
+    for size in (0, int(sim.grid.fluid.size)):
+        st = N.lib().vfb_mass_energy_no_alloc(C.byref(bad), C.c_void_p(sim.fluid.data_ptr()), size, out, None)
+        assert st == N.VFB_ERR_INVALID_ARGUMENT
+    bad = type(sim.level).from_buffer_copy(sim.level)
+    bad.omega = 2.5
+    st = N.lib().vfb_mass_energy_no_alloc(C.byref(bad), C.c_void_p(sim.fluid.data_ptr()), 0, out, None)
+    assert st == N.VFB_ERR_INVALID_ARGUMENT

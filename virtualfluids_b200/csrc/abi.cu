@@ -183,6 +183,9 @@ cudaError_t drag_lift_sum(const double *const pre[3], const double *const post[3
 
 void set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
 
+int check_level_status(const vfb_level *level) { return check_level(level); }
+int cuda_error_status(cudaError_t e, const char *what) { return cuda_status(e, what); }
+
 cudaError_t reduce_partials(const double *partials, uint64_t blocks, double *out, cudaStream_t s)
 {
     reduce_partials_kernel<<<1, 1024, 0, s>>>(partials, blocks, blocks, out);

@@ -25,6 +25,12 @@ struct K17Rates {
     T factorA, factorB;         // 4th order diffusion parameters (K17...h:272-273)
     T neg_iwm;                  // -(1/omega - 1/2)
     T qP, qM, qD;               // quadric limiters (Parameter.cpp:69 default 0.01)
+    // omega-only subexpressions of the collision, each rounded as the reference rounds it in place
+    T mhw;                      // 1/2 * (-omega) (exact)
+    T w32;                      // omega * 3/2
+    T m3w;                      // -3 * omega
+    T c3a;                      // 3 * (1 + 1/2 * (-omega))
+    T omOxyz, omOP, omOM;       // 1 - Oxyz, 1 - OxyyPxzz, 1 - OxyyMxzz
 };
 
 // host computation of the omega-only rates, expression for expression as the reference
@@ -43,6 +49,13 @@ inline K17Rates<T> make_k17_rates(T omega, T qP, T qM, T qD)
     r.qP = qP;
     r.qM = qM;
     r.qD = qD;
+    r.mhw = T(0.5) * (-w);
+    r.w32 = w * (T(3) / T(2));
+    r.m3w = -T(3) * w;
+    r.c3a = T(3) * (T(1) + T(0.5) * (-w));
+    r.omOxyz = T(1) - r.Oxyz;
+    r.omOP = T(1) - r.OxyyPxzz;
+    r.omOM = T(1) - r.OxyyMxzz;
     return r;
 }
 
@@ -86,6 +99,51 @@ __host__ __device__ __forceinline__ void bwd(T &a, T &b, T &c, T v, T v2)
     const T ra = (c + a * (v2 - v)) * h + b * (v - h);
     const T rb = ((a - c) - a * v2) - T(2) * b * v;
     c = (c + a * (v2 + v)) * h + b * (v + h);
+    b = rb;
+    a = ra;
+}
+
+// The transforms of the exact collision. They round exactly as fwd_k / bwd_k / bwd above, with
+// fewer operations:
+//  * 2 s v is formed as s (2 v), 2 v once per axis: (2 s) v and s (2 v) are the same real number,
+//    rounded once;
+//  * X (v^2 -+ v) 1/2 is formed as X ((v^2 -+ v) 1/2), the halved factor once per axis: halving is
+//    exact, so both round X (v^2 -+ v) / 2 once. This holds for every operand whose products stay
+//    out of the subnormal range (|X (v^2 -+ v)| >= 2^-1021 or zero); a velocity component of a
+//    state made of finite populations of magnitude above 1e-300 never comes near it;
+//  * x h + y (h = 1/2) is one fma(x, h, y): the product is exact, so the fused operation rounds
+//    once where the reference rounds the exact product and then the sum.
+template <class T>
+__host__ __device__ __forceinline__ void fwd_kx(T &a, T &b, T &c, T v, T v2, T twov, T kinv, T k)
+{
+    const T s2 = a + c;
+    const T s1 = c - a;
+    T s0 = s2 + b;
+    a = s0;
+    s0 *= kinv;
+    s0 += T(1);
+    b = (s1 * kinv - s0 * v) * k;
+    c = ((s2 - s1 * twov) * kinv + v2 * s0) * k;
+}
+template <class T>
+__host__ __device__ __forceinline__ void bwd_kx(T &a, T &b, T &c, T v, T v2, T twov, T v2mv_h, T v2pv_h, T kinv, T k)
+{
+    const T h = T(0.5);
+    const T a1 = a * kinv + T(1);
+    const T bv = b * v;
+    const T r0 = (fma(c - b, h, bv) * kinv + a1 * v2mv_h) * k;
+    const T r1 = (((a - c) - b * twov) * kinv + a1 * (-v2)) * k;
+    c = (fma(c + b, h, bv) * kinv + a1 * v2pv_h) * k;
+    a = r0;
+    b = r1;
+}
+template <class T>
+__host__ __device__ __forceinline__ void bwdx(T &a, T &b, T &c, T v, T v2, T twov)
+{
+    const T h = T(0.5);
+    const T ra = fma(c + a * (v2 - v), h, b * (v - h));
+    const T rb = ((a - c) - a * v2) - b * twov;
+    c = fma(c + a * (v2 + v), h, b * (v + h));
     b = rb;
     a = ra;
 }
@@ -157,6 +215,7 @@ __host__ __device__ __forceinline__ void k17_collide(T *f, const K17Rates<T> &r,
     vy += fy;
     vz += fz;
     const T vx2 = vx * vx, vy2 = vy * vy, vz2 = vz * vz;
+    const T twovx = T(2) * vx, twovy = T(2) * vy, twovz = T(2) * vz;
 
     T m[27];
 #pragma unroll
@@ -168,7 +227,7 @@ __host__ __device__ __forceinline__ void k17_collide(T *f, const K17Rates<T> &r,
     for (int a = 0; a < 3; ++a)
 #pragma unroll
         for (int b = 0; b < 3; ++b)
-            fwd_k(M(a, b, 0), M(a, b, 1), M(a, b, 2), vz, vz2, kinv_z<T>(a, b), k_z<T>(a, b));
+            fwd_kx(M(a, b, 0), M(a, b, 1), M(a, b, 2), vz, vz2, twovz, kinv_z<T>(a, b), k_z<T>(a, b));
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -176,18 +235,18 @@ __host__ __device__ __forceinline__ void k17_collide(T *f, const K17Rates<T> &r,
             if (c == 1)
                 fwd(M(a, 0, 1), M(a, 1, 1), M(a, 2, 1), vy, vy2);
             else
-                fwd_k(M(a, 0, c), M(a, 1, c), M(a, 2, c), vy, vy2, kinv_y<T>(a, c), k_y<T>(a, c));
+                fwd_kx(M(a, 0, c), M(a, 1, c), M(a, 2, c), vy, vy2, twovy, kinv_y<T>(a, c), k_y<T>(a, c));
         }
 #pragma unroll
     for (int b = 0; b < 3; ++b)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             if (b == 0 && c == 0)
-                fwd_k(M(0, 0, 0), M(1, 0, 0), M(2, 0, 0), vx, vx2, T(1), T(1));
+                fwd_kx(M(0, 0, 0), M(1, 0, 0), M(2, 0, 0), vx, vx2, twovx, T(1), T(1));
             else if (b == 2 && c == 2) // K17...h:222: K^-1 = 3, K = 1/9 on this line
-                fwd_k(M(0, 2, 2), M(1, 2, 2), M(2, 2, 2), vx, vx2, T(3), T(1) / T(9));
+                fwd_kx(M(0, 2, 2), M(1, 2, 2), M(2, 2, 2), vx, vx2, twovx, T(3), T(1) / T(9));
             else if ((b == 2 && c == 0) || (b == 0 && c == 2))
-                fwd_k(M(0, b, c), M(1, b, c), M(2, b, c), vx, vx2, T(3), T(1) / T(3));
+                fwd_kx(M(0, b, c), M(1, b, c), M(2, b, c), vx, vx2, twovx, T(3), T(1) / T(3));
             else
                 fwd(M(0, b, c), M(1, b, c), M(2, b, c), vx, vx2);
         }
@@ -207,42 +266,43 @@ __host__ __device__ __forceinline__ void k17_collide(T *f, const K17Rates<T> &r,
     T mxyyMxzz = M(1, 2, 0) - M(1, 0, 2);
 
     // velocity gradients times rho (K17...h:347-352), OxxPyyPzz = 1
-    const T Dxy = -T(3) * omega * M(1, 1, 0);
-    const T Dxz = -T(3) * omega * M(1, 0, 1);
-    const T Dyz = -T(3) * omega * M(0, 1, 1);
-    const T dxux = h * (-omega) * (mxxMyy + mxxMzz) + h * T(1) * (M(0, 0, 0) - mxxPyyPzz);
-    const T dyuy = dxux + omega * (T(3) / T(2)) * mxxMyy;
-    const T dzuz = dxux + omega * (T(3) / T(2)) * mxxMzz;
+    // (the omega-only factors -3 omega, 1/2 (-omega), omega 3/2 come rounded from the host)
+    const T Dxy = r.m3w * M(1, 1, 0);
+    const T Dxz = r.m3w * M(1, 0, 1);
+    const T Dyz = r.m3w * M(0, 1, 1);
+    const T dxux = fma(M(0, 0, 0) - mxxPyyPzz, h, r.mhw * (mxxMyy + mxxMzz));
+    const T dyuy = dxux + r.w32 * mxxMyy;
+    const T dzuz = dxux + r.w32 * mxxMzz;
 
     // second order relaxation with correction (K17...h:375-387)
     mxxPyyPzz += T(1) * (M(0, 0, 0) - mxxPyyPzz) - T(3) * (T(1) - h * T(1)) * (vx2 * dxux + vy2 * dyuy + vz2 * dzuz);
-    mxxMyy += omega * (-mxxMyy) - T(3) * (T(1) + h * (-omega)) * (vx2 * dxux - vy2 * dyuy);
-    mxxMzz += omega * (-mxxMzz) - T(3) * (T(1) + h * (-omega)) * (vx2 * dxux - vz2 * dzuz);
+    mxxMyy += omega * (-mxxMyy) - r.c3a * (vx2 * dxux - vy2 * dyuy);
+    mxxMzz += omega * (-mxxMzz) - r.c3a * (vx2 * dxux - vz2 * dzuz);
     M(0, 1, 1) += omega * (-M(0, 1, 1));
     M(1, 0, 1) += omega * (-M(1, 0, 1));
     M(1, 1, 0) += omega * (-M(1, 1, 0));
 
     // third order with the quartic limiter (K17...h:397-410)
     T wadj;
-    wadj = r.Oxyz + (T(1) - r.Oxyz) * fabs(M(1, 1, 1)) / (fabs(M(1, 1, 1)) + r.qD);
+    wadj = r.Oxyz + r.omOxyz * fabs(M(1, 1, 1)) / (fabs(M(1, 1, 1)) + r.qD);
     M(1, 1, 1) += wadj * (-M(1, 1, 1));
-    wadj = r.OxyyPxzz + (T(1) - r.OxyyPxzz) * fabs(mxxyPyzz) / (fabs(mxxyPyzz) + r.qP);
+    wadj = r.OxyyPxzz + r.omOP * fabs(mxxyPyzz) / (fabs(mxxyPyzz) + r.qP);
     mxxyPyzz += wadj * (-mxxyPyzz);
-    wadj = r.OxyyMxzz + (T(1) - r.OxyyMxzz) * fabs(mxxyMyzz) / (fabs(mxxyMyzz) + r.qM);
+    wadj = r.OxyyMxzz + r.omOM * fabs(mxxyMyzz) / (fabs(mxxyMyzz) + r.qM);
     mxxyMyzz += wadj * (-mxxyMyzz);
-    wadj = r.OxyyPxzz + (T(1) - r.OxyyPxzz) * fabs(mxxzPyyz) / (fabs(mxxzPyyz) + r.qP);
+    wadj = r.OxyyPxzz + r.omOP * fabs(mxxzPyyz) / (fabs(mxxzPyyz) + r.qP);
     mxxzPyyz += wadj * (-mxxzPyyz);
-    wadj = r.OxyyMxzz + (T(1) - r.OxyyMxzz) * fabs(mxxzMyyz) / (fabs(mxxzMyyz) + r.qM);
+    wadj = r.OxyyMxzz + r.omOM * fabs(mxxzMyyz) / (fabs(mxxzMyyz) + r.qM);
     mxxzMyyz += wadj * (-mxxzMyyz);
-    wadj = r.OxyyPxzz + (T(1) - r.OxyyPxzz) * fabs(mxyyPxzz) / (fabs(mxyyPxzz) + r.qP);
+    wadj = r.OxyyPxzz + r.omOP * fabs(mxyyPxzz) / (fabs(mxyyPxzz) + r.qP);
     mxyyPxzz += wadj * (-mxyyPxzz);
-    wadj = r.OxyyMxzz + (T(1) - r.OxyyMxzz) * fabs(mxyyMxzz) / (fabs(mxyyMxzz) + r.qM);
+    wadj = r.OxyyMxzz + r.omOM * fabs(mxyyMxzz) / (fabs(mxyyMxzz) + r.qM);
     mxyyMxzz += wadj * (-mxyyMxzz);
 
     // back from the linear combinations (K17...h:424-433)
     M(2, 0, 0) = c13 * (mxxMyy + mxxMzz + mxxPyyPzz);
-    M(0, 2, 0) = c13 * (-T(2) * mxxMyy + mxxMzz + mxxPyyPzz);
-    M(0, 0, 2) = c13 * (mxxMyy - T(2) * mxxMzz + mxxPyyPzz);
+    M(0, 2, 0) = c13 * (fma(T(-2), mxxMyy, mxxMzz) + mxxPyyPzz);
+    M(0, 0, 2) = c13 * (fma(T(-2), mxxMzz, mxxMyy) + mxxPyyPzz);
     M(2, 1, 0) = (mxxyMyzz + mxxyPyzz) * h;
     M(0, 1, 2) = (-mxxyMyzz + mxxyPyzz) * h;
     M(2, 0, 1) = (mxxzMyyz + mxxzPyyz) * h;
@@ -264,25 +324,28 @@ __host__ __device__ __forceinline__ void k17_collide(T *f, const K17Rates<T> &r,
     M(2, 1, 1) = cm211 + c13 * ((T(3) * M(2, 0, 0) + T(1)) * M(0, 1, 1) + T(6) * M(1, 1, 0) * M(1, 0, 1)) * oneOverRho;
     M(1, 2, 1) = cm121 + c13 * ((T(3) * M(0, 2, 0) + T(1)) * M(1, 0, 1) + T(6) * M(1, 1, 0) * M(0, 1, 1)) * oneOverRho;
     M(1, 1, 2) = cm112 + c13 * ((T(3) * M(0, 0, 2) + T(1)) * M(1, 1, 0) + T(6) * M(1, 0, 1) * M(0, 1, 1)) * oneOverRho;
-    M(2, 2, 0) = cm220 + (((M(2, 0, 0) * M(0, 2, 0) + T(2) * M(1, 1, 0) * M(1, 1, 0)) * T(9) + T(3) * (M(2, 0, 0) + M(0, 2, 0))) * oneOverRho - (drho * oneOverRho)) * c19;
-    M(2, 0, 2) = cm202 + (((M(2, 0, 0) * M(0, 0, 2) + T(2) * M(1, 0, 1) * M(1, 0, 1)) * T(9) + T(3) * (M(2, 0, 0) + M(0, 0, 2))) * oneOverRho - (drho * oneOverRho)) * c19;
-    M(0, 2, 2) = cm022 + (((M(0, 0, 2) * M(0, 2, 0) + T(2) * M(0, 1, 1) * M(0, 1, 1)) * T(9) + T(3) * (M(0, 0, 2) + M(0, 2, 0))) * oneOverRho - (drho * oneOverRho)) * c19;
+    // products with a power of two are exact: (2 m) m = 2 (m m), and a sum with it is one fma
+    const T sq110 = M(1, 1, 0) * M(1, 1, 0), sq101 = M(1, 0, 1) * M(1, 0, 1), sq011 = M(0, 1, 1) * M(0, 1, 1);
+    M(2, 2, 0) = cm220 + ((fma(T(2), sq110, M(2, 0, 0) * M(0, 2, 0)) * T(9) + T(3) * (M(2, 0, 0) + M(0, 2, 0))) * oneOverRho - (drho * oneOverRho)) * c19;
+    M(2, 0, 2) = cm202 + ((fma(T(2), sq101, M(2, 0, 0) * M(0, 0, 2)) * T(9) + T(3) * (M(2, 0, 0) + M(0, 0, 2))) * oneOverRho - (drho * oneOverRho)) * c19;
+    M(0, 2, 2) = cm022 + ((fma(T(2), sq011, M(0, 0, 2) * M(0, 2, 0)) * T(9) + T(3) * (M(0, 0, 2) + M(0, 2, 0))) * oneOverRho - (drho * oneOverRho)) * c19;
 
-    const T t122 = c13 * (T(3) * (M(0, 0, 2) * M(1, 2, 0) + M(0, 2, 0) * M(1, 0, 2) + T(4) * M(0, 1, 1) * M(1, 1, 1) + T(2) * (M(1, 0, 1) * M(0, 2, 1) + M(1, 1, 0) * M(0, 1, 2))) + (M(1, 2, 0) + M(1, 0, 2))) * oneOverRho;
-    const T t212 = c13 * (T(3) * (M(0, 0, 2) * M(2, 1, 0) + M(2, 0, 0) * M(0, 1, 2) + T(4) * M(1, 0, 1) * M(1, 1, 1) + T(2) * (M(0, 1, 1) * M(2, 0, 1) + M(1, 1, 0) * M(1, 0, 2))) + (M(2, 1, 0) + M(0, 1, 2))) * oneOverRho;
-    const T t221 = c13 * (T(3) * (M(2, 0, 0) * M(0, 2, 1) + M(0, 2, 0) * M(2, 0, 1) + T(4) * M(1, 1, 0) * M(1, 1, 1) + T(2) * (M(1, 0, 1) * M(1, 2, 0) + M(0, 1, 1) * M(2, 1, 0))) + (M(0, 2, 1) + M(2, 0, 1))) * oneOverRho;
+    const T t122 = c13 * (T(3) * fma(T(2), M(1, 0, 1) * M(0, 2, 1) + M(1, 1, 0) * M(0, 1, 2), fma(T(4), M(0, 1, 1) * M(1, 1, 1), M(0, 0, 2) * M(1, 2, 0) + M(0, 2, 0) * M(1, 0, 2))) + (M(1, 2, 0) + M(1, 0, 2))) * oneOverRho;
+    const T t212 = c13 * (T(3) * fma(T(2), M(0, 1, 1) * M(2, 0, 1) + M(1, 1, 0) * M(1, 0, 2), fma(T(4), M(1, 0, 1) * M(1, 1, 1), M(0, 0, 2) * M(2, 1, 0) + M(2, 0, 0) * M(0, 1, 2))) + (M(2, 1, 0) + M(0, 1, 2))) * oneOverRho;
+    const T t221 = c13 * (T(3) * fma(T(2), M(1, 0, 1) * M(1, 2, 0) + M(0, 1, 1) * M(2, 1, 0), fma(T(4), M(1, 1, 0) * M(1, 1, 1), M(2, 0, 0) * M(0, 2, 1) + M(0, 2, 0) * M(2, 0, 1))) + (M(0, 2, 1) + M(2, 0, 1))) * oneOverRho;
     M(1, 2, 2) = EXACT ? z + t122 : t122;
     M(2, 1, 2) = EXACT ? z + t212 : t212;
     M(2, 2, 1) = EXACT ? z + t221 : t221;
 
-    const T b222 = (-T(4) * M(1, 1, 1) * M(1, 1, 1) - (M(2, 0, 0) * M(0, 2, 2) + M(0, 2, 0) * M(2, 0, 2) + M(0, 0, 2) * M(2, 2, 0))
-                    - T(4) * (M(0, 1, 1) * M(2, 1, 1) + M(1, 0, 1) * M(1, 2, 1) + M(1, 1, 0) * M(1, 1, 2))
-                    - T(2) * (M(1, 2, 0) * M(1, 0, 2) + M(2, 1, 0) * M(0, 1, 2) + M(2, 0, 1) * M(0, 2, 1))) * oneOverRho
-                 + (T(4) * (M(1, 0, 1) * M(1, 0, 1) * M(0, 2, 0) + M(0, 1, 1) * M(0, 1, 1) * M(2, 0, 0) + M(1, 1, 0) * M(1, 1, 0) * M(0, 0, 2))
-                    + T(2) * (M(2, 0, 0) * M(0, 2, 0) * M(0, 0, 2)) + T(16) * M(1, 1, 0) * M(1, 0, 1) * M(0, 1, 1)) * oneOverRho * oneOverRho
+    const T b222 = fma(T(-2), M(1, 2, 0) * M(1, 0, 2) + M(2, 1, 0) * M(0, 1, 2) + M(2, 0, 1) * M(0, 2, 1),
+                       fma(T(-4), M(0, 1, 1) * M(2, 1, 1) + M(1, 0, 1) * M(1, 2, 1) + M(1, 1, 0) * M(1, 1, 2),
+                           fma(T(-4), M(1, 1, 1) * M(1, 1, 1), -(M(2, 0, 0) * M(0, 2, 2) + M(0, 2, 0) * M(2, 0, 2) + M(0, 0, 2) * M(2, 2, 0))))) * oneOverRho
+                 + fma(T(16), M(1, 1, 0) * M(1, 0, 1) * M(0, 1, 1),
+                       fma(T(4), sq101 * M(0, 2, 0) + sq011 * M(2, 0, 0) + sq110 * M(0, 0, 2),
+                           T(2) * (M(2, 0, 0) * M(0, 2, 0) * M(0, 0, 2)))) * oneOverRho * oneOverRho
                  - c13 * (M(0, 2, 2) + M(2, 0, 2) + M(2, 2, 0)) * oneOverRho - c19 * (M(2, 0, 0) + M(0, 2, 0) + M(0, 0, 2)) * oneOverRho
-                 + (T(2) * (M(1, 0, 1) * M(1, 0, 1) + M(0, 1, 1) * M(0, 1, 1) + M(1, 1, 0) * M(1, 1, 0))
-                    + (M(0, 0, 2) * M(0, 2, 0) + M(0, 0, 2) * M(2, 0, 0) + M(0, 2, 0) * M(2, 0, 0)) + c13 * (M(0, 0, 2) + M(0, 2, 0) + M(2, 0, 0))) * oneOverRho * oneOverRho * c23
+                 + (fma(T(2), sq101 + sq011 + sq110, M(0, 0, 2) * M(0, 2, 0) + M(0, 0, 2) * M(2, 0, 0) + M(0, 2, 0) * M(2, 0, 0))
+                    + c13 * (M(0, 0, 2) + M(0, 2, 0) + M(2, 0, 0))) * oneOverRho * oneOverRho * c23
                  + c127 * ((drho * drho - drho) * oneOverRho * oneOverRho);
     M(2, 2, 2) = EXACT ? z - b222 : -b222;
 
@@ -291,33 +354,36 @@ __host__ __device__ __forceinline__ void k17_collide(T *f, const K17Rates<T> &r,
     M(0, 1, 0) = -M(0, 1, 0);
     M(0, 0, 1) = -M(0, 0, 1);
 
+    const T x2mvh = (vx2 - vx) * h, x2pvh = (vx2 + vx) * h, y2mvh = (vy2 - vy) * h, y2pvh = (vy2 + vy) * h;
+    const T z2mvh = (vz2 - vz) * h, z2pvh = (vz2 + vz) * h;
+
 #pragma unroll
     for (int b = 0; b < 3; ++b)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             if (b == 0 && c == 0)
-                bwd_k(M(0, 0, 0), M(1, 0, 0), M(2, 0, 0), vx, vx2, T(1), T(1));
+                bwd_kx(M(0, 0, 0), M(1, 0, 0), M(2, 0, 0), vx, vx2, twovx, x2mvh, x2pvh, T(1), T(1));
             else if (b == 2 && c == 2)
-                bwd_k(M(0, 2, 2), M(1, 2, 2), M(2, 2, 2), vx, vx2, T(9), T(1) / T(9));
+                bwd_kx(M(0, 2, 2), M(1, 2, 2), M(2, 2, 2), vx, vx2, twovx, x2mvh, x2pvh, T(9), T(1) / T(9));
             else if ((b == 2 && c == 0) || (b == 0 && c == 2))
-                bwd_k(M(0, b, c), M(1, b, c), M(2, b, c), vx, vx2, T(3), T(1) / T(3));
+                bwd_kx(M(0, b, c), M(1, b, c), M(2, b, c), vx, vx2, twovx, x2mvh, x2pvh, T(3), T(1) / T(3));
             else
-                bwd(M(0, b, c), M(1, b, c), M(2, b, c), vx, vx2);
+                bwdx(M(0, b, c), M(1, b, c), M(2, b, c), vx, vx2, twovx);
         }
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             if (c == 1)
-                bwd(M(a, 0, 1), M(a, 1, 1), M(a, 2, 1), vy, vy2);
+                bwdx(M(a, 0, 1), M(a, 1, 1), M(a, 2, 1), vy, vy2, twovy);
             else
-                bwd_k(M(a, 0, c), M(a, 1, c), M(a, 2, c), vy, vy2, kinv_y<T>(a, c), k_y<T>(a, c));
+                bwd_kx(M(a, 0, c), M(a, 1, c), M(a, 2, c), vy, vy2, twovy, y2mvh, y2pvh, kinv_y<T>(a, c), k_y<T>(a, c));
         }
 #pragma unroll
     for (int a = 0; a < 3; ++a)
 #pragma unroll
         for (int b = 0; b < 3; ++b)
-            bwd_k(M(a, b, 0), M(a, b, 1), M(a, b, 2), vz, vz2, kinv_z<T>(a, b), k_z<T>(a, b));
+            bwd_kx(M(a, b, 0), M(a, b, 1), M(a, b, 2), vz, vz2, twovz, z2mvh, z2pvh, kinv_z<T>(a, b), k_z<T>(a, b));
 #undef M
 
 #pragma unroll

@@ -329,8 +329,14 @@ __global__ void __launch_bounds__(128) k17_list_staged_kernel(ListCollideArgs<ty
 // collision + streaming on a structured box: neighbours by index arithmetic, one node per
 // thread, x fastest so every direction plane is read and written by whole warps in order.
 // ---------------------------------------------------------------------------------------------
+// resident blocks per SM the register budget must allow: three for FP64 arithmetic (at most 168
+// registers; an unbounded build of the exact energy variant takes 170, which rounds to 176 and
+// leaves two), four for FP32 arithmetic (at most 128)
+template <class S>
+constexpr int box_min_blocks() { return sizeof(typename Codec<S>::compute) == 8 ? 3 : 4; }
+
 template <class S, bool EXACT, bool EVEN, bool MASK, bool ENERGY, bool WRITE_MACRO>
-__global__ void __launch_bounds__(128) k17_box_kernel(BoxCollideArgs<typename Codec<S>::compute> a)
+__global__ void __launch_bounds__(128, box_min_blocks<S>()) k17_box_kernel(BoxCollideArgs<typename Codec<S>::compute> a)
 {
     using C = typename Codec<S>::compute;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;

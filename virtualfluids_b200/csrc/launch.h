@@ -117,6 +117,12 @@ VFB_DECLARE_LAUNCHERS
 
 // message for vfb_last_error() of the calling thread
 void set_last_error(const char *msg);
+// the argument checks every reference-layout entry point applies to a level (VFB_OK or the status,
+// with the message set)
+int check_level_status(const vfb_level *level);
+// VFB_OK for cudaSuccess, else the status the entry points report for e (out of memory or a CUDA
+// error), with "what: <CUDA message>" as the message
+int cuda_error_status(cudaError_t e, const char *what);
 
 // deterministic reduction of per-block {mass, energy} partials into out[2] (device)
 cudaError_t reduce_partials(const double *partials, uint64_t blocks, double *out, cudaStream_t s);

@@ -7,15 +7,16 @@
 // fixed array in this file's device memory instead.
 //
 // The array is a file-scope __device__ variable: every GPU that loads the library holds it
-// (about 1 MiB) until the process exits. Its host-side name is only a stand-in, so the device
-// address is looked up with cudaGetSymbolAddress, once per device, the first time the entry point
-// runs on that device; that first call should therefore come before any stream capture. All calls
-// share the array: each call overwrites every entry it reads back (nothing has to start at zero),
-// and calls that overlap on the GPU race on it.
+// (about 1 MiB) until the process exits. Its host-side name is only a stand-in, so every call
+// looks the array's device address up with cudaGetSymbolAddress on the current device. The first
+// such lookup on a device loads the library's device code there, so the first call on a device
+// should come before any stream capture; later lookups are cheap. The address is not cached: a
+// cudaDeviceReset can reload the module at another address. All calls share the array: each call
+// overwrites every entry it reads back (nothing has to start at zero), and calls that overlap on
+// the GPU race on it.
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <mutex>
 
 #include "launch.h"
 #include "vfb.h"
@@ -29,28 +30,14 @@ static_assert(VFB_NO_ALLOC_MAX_NODES % kThreadsPerBlock == 0, "the node limit is
 // per-block {mass, energy} partials, then the two reduced sums
 __device__ __align__(256) double g_mass_energy_scratch[2 * kMaxBlocks + 2];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mutex;
-double *g_scratch_ptr[kMaxDevices] = {};
-
-// device address of the scratch array on the current device (looked up once per device)
+// device address of the scratch array on the current device
 cudaError_t scratch_address(double **out)
 {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_mass_energy_scratch);
     if (e != cudaSuccess)
         return e;
-    if (dev < 0 || dev >= kMaxDevices)
-        return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_scratch_ptr[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_mass_energy_scratch);
-        if (e != cudaSuccess)
-            return e;
-        g_scratch_ptr[dev] = static_cast<double *>(p);
-    }
-    *out = g_scratch_ptr[dev];
+    *out = static_cast<double *>(p);
     return cudaSuccess;
 }
 
@@ -67,7 +54,11 @@ extern "C" {
 int vfb_mass_energy_no_alloc(const vfb_level *level, const uint32_t *node_indices, uint32_t size, double out[2],
                              void *stream)
 {
-    if (!level || !out || (size && !node_indices))
+    // the same level checks as vfb_mass_energy, before any early return
+    const int st = vfb::check_level_status(level);
+    if (st)
+        return st;
+    if (!out || (size && !node_indices))
         return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
     if (size > VFB_NO_ALLOC_MAX_NODES)
         return fail(VFB_ERR_INVALID_ARGUMENT,
@@ -77,15 +68,10 @@ int vfb_mass_energy_no_alloc(const vfb_level *level, const uint32_t *node_indice
         out[0] = out[1] = 0.0;
         return VFB_OK;
     }
-    if (level->storage < VFB_STORAGE_F64 || level->storage > VFB_STORAGE_BF16 || !level->distributions ||
-        !level->neighbor_x || !level->neighbor_y || !level->neighbor_z)
-        return fail(VFB_ERR_INVALID_ARGUMENT, "level description is incomplete");
-    if (level->arith == VFB_ARITH_EXACT && level->storage > VFB_STORAGE_F32)
-        return fail(VFB_ERR_UNSUPPORTED, "exact arithmetic is built for F64 and F32 storage only");
     double *scratch = nullptr;
     cudaError_t e = scratch_address(&scratch);
     if (e != cudaSuccess)
-        return fail(VFB_ERR_CUDA, "cudaGetSymbolAddress of the reduction scratch array failed");
+        return vfb::cuda_error_status(e, "cudaGetSymbolAddress of the reduction scratch array");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const uint64_t blocks = (size + kThreadsPerBlock - 1) / kThreadsPerBlock;
     double *partials = scratch;
@@ -110,9 +96,7 @@ int vfb_mass_energy_no_alloc(const vfb_level *level, const uint32_t *node_indice
         e = cudaMemcpyAsync(out, result, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess)
-        return fail(VFB_ERR_CUDA, cudaGetErrorString(e));
-    return VFB_OK;
+    return vfb::cuda_error_status(e, "mass/energy reduction (no allocation)");
 }
 
 } // extern "C"

@@ -8,7 +8,7 @@ Populations and masks stay resident on the device between steps. A solve compute
 computes alone (the pool's kernels treat every domain independently), so its result does not
 depend on what else is being served.
 
-The porous-block workload (config 5): a cube of random non-overlapping spheres. Two drives:
+The porous-block workload: a cube of random non-overlapping spheres. Two drives:
 
 * ``"pressure"`` (the default): the block lies between two pressure planes at x (drho = +-dp/2,
   PressureNonEquilibriumCompressible), periodic in y and z; every link cut by a sphere carries the

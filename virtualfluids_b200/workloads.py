@@ -162,7 +162,7 @@ def porous_block(side, seed, porosity=None, radius=(3.0, 8.0), max_tries=40000, 
 
 
 def cube_duct(nx=512, ny=256, nz=256, cube=32, x0=128, u_max=0.05, re=3000.0):
-    """Config 3: duct flow past a wall-mounted cube. Fluid box nx x ny x nz (stopper shell around
+    """Duct flow past a wall-mounted cube. Fluid box nx x ny x nz (stopper shell around
     it); no-slip walls on the y and z faces (interpolated bounce-back, q = 1/2); the inlet at x = 0
     carries u_x = u_max 16 eta (1 - eta) zeta (1 - zeta) (eta, zeta the cross-section coordinates
     between the wall planes); the outlet at x = nx - 1 holds drho = 0 (non-equilibrium pressure BC,
@@ -223,7 +223,7 @@ def sphere_link_q(points, centre, radius):
 
 
 def porous_block_bcs(side, seed, porosity=None, drho=3e-3, radius=(3.0, 8.0)):
-    """Config 5 as boundary-condition lists of a structured box: a side^3 porous block (spheres
+    """The porous-block serving workload as boundary-condition lists of a structured box: a side^3 porous block (spheres
     as :func:`porous_block`, kept three nodes off the x faces) between two pressure planes.
 
     The box is (side + 2) x side x side, periodic in y and z; its first and last x layers are solid
