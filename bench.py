@@ -283,10 +283,70 @@ def cavity_parity(cpu, dev):
     return out
 
 
+def reference_gpu_kernel(n, launches=ROOFLINE_LAUNCHES):
+    """The reference's own GPU collision, runCollision with the K17 functor (K17CompressibleNavierStokes.cu
+    :85-100), compiled from its sources with its own CUDA flags (FMA contraction on), 64 threads per
+    block (Parameter.cpp:400), over TGV n^3 in the reference layout on this GPU: the average CUDA-event
+    time of `launches` launches (alternating parity), FP64 and FP32. None without a GPU or the builds."""
+    import torch
+    from oracle import pyoracle
+    from virtualfluids_b200.grid import ListGrid
+    if not torch.cuda.is_available():
+        return None
+    g = ListGrid(n, n, n, periodic=(True, True, True))
+    ptr = lambda t: C.c_void_p(t.data_ptr())
+    nb = [torch.from_numpy(g.neighbor[a].astype(np.int32)).cuda() for a in range(3)]
+    fluid = torch.from_numpy(g.fluid.astype(np.int32)).cuda()
+    geo = torch.from_numpy(g.geo.astype(np.int32)).cuda()
+    fields = [np.concatenate([[0.0], a]) for a in tgv_fields(n, U0)]
+    peak, _ = measured_peak()
+    omega = omega_tgv(n)
+    out = {"kernel": "vf::gpu::runCollision<K17, TurbulenceModel::None> (reference sources, nvcc -O3 "
+                     "--extended-lambda, default FMA contraction), 64 threads per block",
+           "workload": f"TGV {n}^3 periodic, reference layout (neighborX/Y/Z, fluid-node list)",
+           "launches_timed": launches}
+    for rb, dt, key in ((8, torch.float64, "f64"), (4, torch.float32, "f32")):
+        L = pyoracle.refgpu(rb, release=True)
+        if L is None:
+            continue
+        dist = torch.zeros(27 * g.number_of_nodes, dtype=dt, device="cuda")
+        arrs = [torch.from_numpy(a).to("cuda", dt) for a in fields]
+        for ev in (0, 1):
+            assert L.refgpu_init(*(ptr(x) for x in nb), ptr(geo), *(ptr(a) for a in arrs), g.number_of_nodes,
+                                 ptr(dist), ev) == 0
+        forces = torch.zeros(3, dtype=dt, device="cuda")
+        lim = torch.full((3,), 0.01, dtype=dt, device="cuda")
+        ev = 1
+
+        def launch():
+            nonlocal ev
+            assert L.refgpu_k17(ptr(dist), g.number_of_nodes, *(ptr(x) for x in nb), ptr(fluid), int(g.fluid.size),
+                                ev, omega, ptr(forces), ptr(lim), 1.0) == 0
+            ev = 1 - ev
+
+        for _ in range(5):
+            launch()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(launches):
+            launch()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / launches
+        gbs = 2 * 27 * rb * g.fluid.size / (ms / 1e3) / 1e9
+        out[key] = {"kernel_ms": round(ms, 4), "mlups": round(g.fluid.size / (ms / 1e3) / 1e6, 1),
+                    "hbm_gbs_algorithmic": round(gbs, 1), "frac": round(gbs / peak, 4)}
+        del dist, arrs
+        torch.cuda.empty_cache()
+    return out
+
+
 def run_reference(args):
     """The reference arm: the reference's CPU path (its K17 header, Release flags, over the same
     esoteric-twist layout, all host cores) on the headline's own workload, TGV 256^3 FP64: W whole
-    untimed steps, then min(K, REFERENCE_MAX_STEPS) timed steps. Rank 0 only."""
+    untimed steps, then min(K, REFERENCE_MAX_STEPS) timed steps. Rank 0 only. Beside it, the
+    reference's own GPU collision kernel on the same workload (reference_gpu_kernel)."""
     world, rank, _ = dist_env()
     if rank != 0:
         return
@@ -302,6 +362,13 @@ def run_reference(args):
             "config": tgv_config(args.n, 1, "exact", "auto"),
             "impl": "reference", "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_gpu_reference:
+        try:
+            gk = reference_gpu_kernel(args.n)
+        except (AssertionError, RuntimeError, OSError) as e:   # reported, never fatal for the CPU arm
+            gk = {"unavailable": f"{type(e).__name__}: {e}"}
+        if gk:
+            line["reference_gpu_kernel"] = gk
     print(json.dumps(line), flush=True)
 
 
@@ -469,9 +536,13 @@ def run_tgv_forms(args):
     every = 100
     ref = {}
     out = {}
-    for st in ("f64", "f32", "f16", "bf16"):
+    names = args.tgv_forms.split(",")
+    if not names[0].startswith("f64"):
+        raise SystemExit("--tgv-forms: the first form is the FP64 reference (f64 or f64:exact)")
+    for name in names:
+        st, _, ar = name.partition(":")
         dt = torch.float64 if st == "f64" else torch.float32
-        box = vfb.Box(n, n, n, omega_tgv(n), storage=st)
+        box = vfb.Box(n, n, n, omega_tgv(n), storage=st, arith=ar or "fast")
         box.init(*(torch.from_numpy(a).to(dev, dt) for a in fields))
         done, ek, errs = 0, [], {}
         t0 = time.perf_counter()
@@ -484,16 +555,16 @@ def run_tgv_forms(args):
                 done += k
             f = box.fields()
             u = np.stack([f["vx"], f["vy"], f["vz"]]).astype(np.float64)
-            if st == "f64":
+            if name == names[0]:
                 ref[c] = u
             else:
                 d = u - ref[c]
                 rms = np.sqrt((ref[c] ** 2).sum(axis=0).mean())
                 errs[c] = {"l2_rel": float(np.sqrt((d ** 2).sum(axis=0).mean()) / rms),
                            "linf_rel": float(np.sqrt((d ** 2).sum(axis=0)).max() / np.sqrt((ref[c] ** 2).sum(axis=0)).max())}
-        out[st] = {"wall_s": round(time.perf_counter() - t0, 2), "kinetic_energy_every_100_steps": ek}
+        out[name] = {"wall_s": round(time.perf_counter() - t0, 2), "kinetic_energy_every_100_steps": ek}
         if errs:
-            out[st]["velocity_error_vs_fp64"] = errs
+            out[name]["velocity_error_vs_fp64"] = errs
         del box
         torch.cuda.empty_cache()
     if rank == 0:
@@ -722,16 +793,20 @@ def main():
     ap.add_argument("--n", type=int, default=N_SIDE)
     ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-gpu-reference", action="store_true",
+                    help="--impl reference: skip timing the reference's own GPU kernel beside its CPU path")
     ap.add_argument("--no-list", action="store_true", help="skip the reference-layout (list) measurement")
     ap.add_argument("--arith", default="exact", choices=["fast", "exact"],
                     help="the headline's FP64 arithmetic. exact: every operation rounded as the reference's host "
                          "build (bitwise oracle parity); fast: FMA contraction and a rearranged K17")
-    ap.add_argument("--kernel", default="auto", choices=["auto", "direct", "tma", "async"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "direct", "tma", "async", "pipe"])
     ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "serving", "tgv-forms", "cube", "porous"],
                     help="tgv: the headline (TGV 256^3 FP64); batch: 4096 ducts in one domain pool; "
                          "serving: a Poisson stream of porous-block solves; tgv-forms: storage-form accuracy; "
                          "cube: duct past a wall-mounted cube; porous: the serving pool's step on fixed blocks")
     ap.add_argument("--form-steps", type=int, default=10000)
+    ap.add_argument("--tgv-forms", default="f64,f32,f16,bf16",
+                    help="tgv-forms: comma-separated storage[:arith] forms, the first the FP64 reference")
     ap.add_argument("--cube-dims", type=int, nargs=5, default=[512, 256, 256, 32, 128],
                     metavar=("NX", "NY", "NZ", "CUBE", "X0"))
     ap.add_argument("--domains", type=int, default=4096)

@@ -367,7 +367,8 @@ int vfb_box_status(vfb_box *box, int32_t *device_status, void *stream);
 /* collision kernel: 0 = choose (direct loads, the fastest measured on B200 for every storage),
    1 = direct loads, 2 = TMA-staged warp tiles (nx % 32 == 0),
    3 = per-thread asynchronous copies (F64 and F32 storage),
-   4 = two nodes per thread in packed FP32x2 arithmetic (F32, F16, BF16 storage, FMA arithmetic) */
+   4 = two nodes per thread in packed FP32x2 arithmetic (F32, F16, BF16 storage, FMA arithmetic),
+   5 = persistent blocks with the next node's loads in flight while the current node is collided */
 int vfb_box_set_kernel_variant(vfb_box *box, int32_t variant);
 /* Boundary conditions on a box, run by vfb_box_step in the order of vfb_simulation_run: velocity,
    no-slip, geometry (with the drag's post part before it), parity toggle, the drag's pre part and

@@ -107,10 +107,13 @@ def ref64_release():
     return L
 
 
-def refgpu(real_bytes: int = 8):
+def refgpu(real_bytes: int = 8, release: bool = False):
     """The reference's own CUDA kernels built from the reference tree, or None: FP64
-    (real_bytes = 8) or FP32 (real_bytes = 4, real = float)."""
+    (real_bytes = 8) or FP32 (real_bytes = 4, real = float); without FMA contraction (the parity
+    pins) or, with release=True, with the reference's own build flags (FMA contraction on)."""
     path = REFGPU if real_bytes == 8 else REFGPU32
+    if release:
+        path = HERE / "_ref" / f"libvfref_gpu{8 * real_bytes}_release.so"
     if not path.exists():
         return None
     L = C.CDLL(str(path))

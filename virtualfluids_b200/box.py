@@ -99,10 +99,11 @@ class Box:
 
     def set_kernel_variant(self, variant: str):
         """'auto', 'direct' (plain loads), 'tma' (bulk copies staged in shared memory), 'async'
-        (per-thread asynchronous copies of the next node) or 'pairs' (two nodes per thread in packed
-        FP32x2 arithmetic; FP32-arithmetic forms)."""
+        (per-thread asynchronous copies of the next node), 'pairs' (two nodes per thread in packed
+        FP32x2 arithmetic; FP32-arithmetic forms) or 'pipe' (persistent blocks, the next node's loads
+        in flight in registers while the current node is collided)."""
         N.check(N.lib().vfb_box_set_kernel_variant(
-            self._h, {"auto": 0, "direct": 1, "tma": 2, "async": 3, "pairs": 4}[variant]))
+            self._h, {"auto": 0, "direct": 1, "tma": 2, "async": 3, "pairs": 4, "pipe": 5}[variant]))
 
     # -- boundary conditions (vfb_box_set_bc / vfb_box_add_pressure_bc) -------------------------
     def set_bc(self, kind: str, k, q27, variant, velocity=None):

@@ -1591,9 +1591,10 @@ int vfb_box_status(vfb_box *box, int32_t *device_status, void *stream)
 
 int vfb_box_set_kernel_variant(vfb_box *box, int32_t variant)
 {
-    if (!box || variant < 0 || variant > 4)
+    if (!box || variant < 0 || variant > 5)
         return fail(VFB_ERR_INVALID_ARGUMENT, "variant must be 0 (choose), 1 (direct loads), 2 (TMA-staged), "
-                                              "3 (per-thread async copies) or 4 (packed FP32x2 pairs)");
+                                              "3 (per-thread async copies), 4 (packed FP32x2 pairs) or 5 "
+                                              "(persistent, next node's loads in flight)");
     if (variant == 4 && (box->desc.storage == VFB_STORAGE_F64 || box->desc.arith == VFB_ARITH_EXACT))
         return fail(VFB_ERR_UNSUPPORTED, "packed FP32x2 pairs: FP32 arithmetic (F32, F16, BF16 storage), FMA variant");
     if (variant == 3 && box->desc.storage > VFB_STORAGE_F32)

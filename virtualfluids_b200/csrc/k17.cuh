@@ -477,6 +477,26 @@ __host__ __device__ __forceinline__ float fast_rcp<float>(float x)
 #endif
 }
 
+// 1/rho for the velocity: correctly rounded in both precisions. u = j (1/rho) feeds the moment
+// transforms, and the backward transform puts back j' = rho u + (the negated first central moment
+// rho (j/rho - u)), so any error in u changes the node's momentum by twice that error times rho.
+// A reciprocal that errs to one side (an approximate one) therefore makes the momentum drift step
+// after step; a correctly rounded one errs both ways equally often.
+template <class T>
+__host__ __device__ __forceinline__ T rho_rcp(T x)
+{
+    return T(1) / x;
+}
+template <>
+__host__ __device__ __forceinline__ float rho_rcp<float>(float x)
+{
+#ifdef __CUDA_ARCH__
+    return __frcp_rn(x);
+#else
+    return 1.0f / x;
+#endif
+}
+
 // the seven limiter reciprocals: in double one division and back-substitution through the
 // running products (the denominators are >= the limiters, so the product stays far above the
 // double range limit); in float seven fast divisions (a float product could underflow)
@@ -531,7 +551,7 @@ __host__ __device__ __forceinline__ void k17_collide_fast(T *f, const K17FastCon
     const T jy = (((t19 - t21) + (t23 - t25)) + ((t7 - t9) + (t15 + t17))) + t3;
     const T jz = (((t19 + t21) - (t23 + t25)) + ((t11 - t13) + (t15 - t17))) + t5;
 
-    const T oneOverRho = fast_rcp(drho + T(1));
+    const T oneOverRho = rho_rcp(drho + T(1));
     const T vx = fma(jx, oneOverRho, fx), vy = fma(jy, oneOverRho, fy), vz = fma(jz, oneOverRho, fz);
     const T vx2 = vx * vx, vy2 = vy * vy, vz2 = vz * vz;
     const T twovx = T(2) * vx, twovy = T(2) * vy, twovz = T(2) * vz;

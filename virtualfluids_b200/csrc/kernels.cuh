@@ -400,6 +400,103 @@ __global__ void __launch_bounds__(128, box_min_blocks<S>()) k17_box_kernel(BoxCo
 }
 
 // ---------------------------------------------------------------------------------------------
+// The box collision as a persistent, software-pipelined loop. A block walks rows of blockDim.x
+// nodes along x (tile t = (x tile, y, z)); before a thread collides and stores its node of the
+// current tile it issues the 27 loads of its node in the next tile into registers, so the loads of
+// one tile are in flight while the arithmetic of the one before runs. Reading the next tile's slots
+// before the current tile's stores is safe: in esoteric-twist streaming every slot is read and
+// written by exactly one node per step. The energy partials are per warp over all of its tiles (a
+// fixed order for a fixed grid).
+// ---------------------------------------------------------------------------------------------
+template <class S>
+constexpr int pipe_min_blocks() { return sizeof(typename Codec<S>::compute) == 8 ? 2 : 3; }
+
+template <class C>
+__device__ __forceinline__ bool pipe_node(const BoxCollideArgs<C> &a, uint32_t tiles_x, int64_t t, uint32_t (&nodes)[8])
+{
+    const uint32_t tt = (uint32_t)t;
+    const uint32_t row = tt / tiles_x;
+    const int x = (int)((tt - row * tiles_x) * blockDim.x + threadIdx.x);
+    const int y = (int)(row % (uint32_t)a.ny), z = (int)(row / (uint32_t)a.ny);
+    if (x >= a.nx)
+        return false;
+    const int xp = (x + 1 < a.nx) ? x + 1 : (a.periodic_x ? 0 : x);
+    const int yp = (y + 1 < a.ny) ? y + 1 : (a.periodic_y ? 0 : y);
+    const int zp = (z + 1 < a.nz) ? z + 1 : (a.periodic_z ? 0 : z);
+    const uint32_t k = (uint32_t)((uint64_t)a.nx * ((uint64_t)y + (uint64_t)a.ny * (uint64_t)z) + (uint64_t)x);
+    const uint32_t sx = (uint32_t)(xp - x);
+    const uint32_t sy = (uint32_t)((yp - y) * a.nx);
+    const uint32_t sz = (uint32_t)((int64_t)(zp - z) * a.nx * a.ny);
+    nodes[0] = k;
+    nodes[1] = k + sx;
+    nodes[2] = k + sy;
+    nodes[3] = k + sx + sy;
+    nodes[4] = k + sz;
+    nodes[5] = k + sx + sz;
+    nodes[6] = k + sy + sz;
+    nodes[7] = k + sx + sy + sz;
+    return true;
+}
+
+template <class S, bool EXACT, bool EVEN, bool MASK, bool ENERGY>
+__global__ void __launch_bounds__(128, pipe_min_blocks<S>()) k17_box_pipe_kernel(BoxCollideArgs<typename Codec<S>::compute> a)
+{
+    using C = typename Codec<S>::compute;
+    const uint32_t tiles_x = ((uint32_t)a.nx + blockDim.x - 1) / blockDim.x;
+    const int64_t ntiles = (int64_t)tiles_x * a.ny * a.nz;
+    S *base = static_cast<S *>(a.dist);
+    double m_acc = 0.0, e_acc = 0.0;
+
+    C fn[27];
+    uint32_t nn[8];
+    int64_t t = blockIdx.x;
+    bool an = t < ntiles && pipe_node(a, tiles_x, t, nn);
+    if (MASK && an)
+        an = __ldg(a.mask + nn[0]) != 0;
+    if (an)
+        gather_pre<S, EVEN>(base, a.pitch, nn, fn);
+    for (; t < ntiles; t += gridDim.x) {
+        C f[27];
+        uint32_t nodes[8];
+        const bool act = an;
+#pragma unroll
+        for (int d = 0; d < 27; ++d)
+            f[d] = fn[d];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            nodes[j] = nn[j];
+        // the next tile's loads go out before this tile's arithmetic
+        const int64_t tn = t + gridDim.x;
+        an = tn < ntiles && pipe_node(a, tiles_x, tn, nn);
+        if (MASK && an)
+            an = __ldg(a.mask + nn[0]) != 0;
+        if (an)
+            gather_pre<S, EVEN>(base, a.pitch, nn, fn);
+        if (act) {
+            C drho, vx, vy, vz;
+            collide<C, EXACT>(f, a.rates, a.fx, a.fy, a.fz, drho, vx, vy, vz);
+            scatter_post<S, EVEN>(base, a.pitch, nodes, f);
+            if (ENERGY) {
+                m_acc += 1.0 + (double)drho;
+                e_acc += 0.5 * (1.0 + (double)drho) * ((double)vx * vx + (double)vy * vy + (double)vz * vz);
+            }
+        }
+    }
+    if (ENERGY) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            m_acc += __shfl_down_sync(0xffffffffu, m_acc, o);
+            e_acc += __shfl_down_sync(0xffffffffu, e_acc, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            const uint64_t w = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+            a.energy_partials[2 * w] = m_acc;
+            a.energy_partials[2 * w + 1] = e_acc;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // The box collision for the FP32-arithmetic forms with two nodes per thread, (x, y) and (x, y + 1),
 // collided together in packed FP32x2 arithmetic (packed.cuh): the arithmetic issues about half the
 // instructions, the loads and stores stay coalesced per row. FMA arithmetic only.

@@ -638,6 +638,30 @@ cudaError_t launch_box_async(const BoxCollideArgs<typename Codec<S>::compute> &a
         *n_partials = (uint64_t)grid;
     return cudaGetLastError();
 }
+
+// the software-pipelined persistent box kernel: as many blocks as stay resident, each walking
+// rows of box_block_x(nx) nodes
+template <class S, bool E, bool M, bool N>
+cudaError_t launch_box_pipe(const BoxCollideArgs<typename Codec<S>::compute> &a, uint64_t *n_partials, cudaStream_t s)
+{
+    auto kern = k17_box_pipe_kernel<S, VFB_EXACT, E, M, N>;
+    const int B = box_block_x(a.nx);
+    static int cached_block = -1, cached_bps = 0;
+    if (cached_block != B) {
+        int bps = 0;
+        const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, B, 0);
+        if (e != cudaSuccess)
+            return e;
+        cached_bps = bps > 0 ? bps : 1;
+        cached_block = B;
+    }
+    const int64_t ntiles = (int64_t)((a.nx + B - 1) / B) * a.ny * a.nz;
+    const int64_t grid = std::min<int64_t>(ntiles, (int64_t)cached_bps * sm_count());
+    kern<<<(unsigned)grid, (unsigned)B, 0, s>>>(a);
+    if (n_partials)
+        *n_partials = (uint64_t)grid * (uint64_t)(B / 32);
+    return cudaGetLastError();
+}
 } // namespace
 
 template <class S>
@@ -663,6 +687,21 @@ cudaError_t Launchers<S>::box_collide(const BoxState &b, bool even, double *part
         }
 #undef VFB_K17A
         }
+    }
+    if (b.variant == 5) {
+#define VFB_K17Q(E, M, N) return launch_box_pipe<S, E, M, N>(a, n_partials, s)
+        if (even) {
+            if (mask && energy) VFB_K17Q(true, true, true);
+            else if (mask) VFB_K17Q(true, true, false);
+            else if (energy) VFB_K17Q(true, false, true);
+            else VFB_K17Q(true, false, false);
+        } else {
+            if (mask && energy) VFB_K17Q(false, true, true);
+            else if (mask) VFB_K17Q(false, true, false);
+            else if (energy) VFB_K17Q(false, false, true);
+            else VFB_K17Q(false, false, false);
+        }
+#undef VFB_K17Q
     }
     if constexpr (std::is_same<C, float>::value && !VFB_EXACT) {
         if (b.variant == 4) {

@@ -74,6 +74,11 @@ __host__ __device__ __forceinline__ f2 fast_rcp<f2>(f2 x)
     return f2(fast_rcp<float>(x.v.x), fast_rcp<float>(x.v.y));
 }
 template <>
+__host__ __device__ __forceinline__ f2 rho_rcp<f2>(f2 x)
+{
+    return f2(rho_rcp<float>(x.v.x), rho_rcp<float>(x.v.y));
+}
+template <>
 __host__ __device__ __forceinline__ void limiter_inverses<f2>(const f2 (&d)[7], f2 (&iv)[7])
 {
 #pragma unroll
