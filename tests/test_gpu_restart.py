@@ -77,3 +77,35 @@ def test_box_restart_continues_bitwise(cuda, tmp_path, storage):
     back = read_vtk(tmp_path / "box.vtk")
     assert back["dimensions"] == (n, n, n)
     assert np.array_equal(back["velocity"][0], a.fields()["vx"].astype(np.float64))
+
+
+def test_simulation_vtu_output_holds_the_oracle_fields(cuda, oracle, tmp_path):
+    """Simulation.write_vtu after an exact-arithmetic cavity run: the part file equals the one the
+    same writer makes from the oracle's fields of the same run (so the file carries the reference's
+    values), and the time series lists both written steps."""
+    from virtualfluids_b200.output import FileWriter
+    g = ListGrid(10, 10, 10)
+    for s in ("PX", "MX", "PY", "MY", "MZ"):
+        g.add_side(s, "noslip")
+    g.add_side("PZ", "velocity", velocity=(0.05, 0.0, 0.0))
+    p = _para(0.05 * 10 / 100.0)
+    p.arith = N.ARITH_EXACT
+    bcf = BCF()
+    bcf.set_no_slip_boundary_condition(BCF.NoSlipBC.NoSlipBounceBack)
+    bcf.set_velocity_boundary_condition(BCF.VelocityBC.VelocityBounceBack)
+    sim = Simulation(p, g, bcf)
+    sim.init()
+    w, first = sim.write_vtu(tmp_path / "sim", 0)
+    sim.run(30)
+    w, files = sim.write_vtu(tmp_path / "sim", 30, last=True, writer=w)
+    orc = oracle.OracleLevel(g, omega=p.omega)
+    orc.init()
+    orc.run(30)
+    m = orc.macroscopic()
+    ref = FileWriter(tmp_path / "orc").write_timestep(
+        30, [dict(coords=g.coords.astype(np.float64), spacing=1.0, geo=g.geo, neighbor=g.neighbor, **{
+            "rho": m["rho"], "vx": m["vx"], "vy": m["vy"], "vz": m["vz"], "pressure": m["pressure"]})])
+    from pathlib import Path
+    assert Path(files[0]).read_bytes() == Path(ref[0]).read_bytes()
+    pvd = Path([f for f in files if f.endswith(".pvd")][0]).read_text()
+    assert 'timestep="0"' in pvd and 'timestep="30"' in pvd

@@ -436,6 +436,23 @@ class Simulation:
                          {"drho": m["rho"][f], "velocity": np.stack([m["vx"][f], m["vy"][f], m["vz"][f]]),
                           "pressure": m["pressure"][f]}, title=f"level {level}")
 
+    def write_vtu(self, prefix, timestep, last=False, writer=None):
+        """Every level's fields in the reference's output files (FileWriter::writeTimestep,
+        Output/FileWriter.cpp:104-137): part files of octs with press, rho, vx1, vx2, vx3 and geo,
+        the time step's .pvtu collection and, with last=True, the .pvd time series. Positions are
+        in units of the coarsest spacing. Pass the same `writer` (output.FileWriter) for every time
+        step of a run so that the time series lists them all; returns (writer, files)."""
+        from .output import FileWriter
+        writer = writer or FileWriter(prefix)
+        levels = []
+        for lev, S in enumerate(self.levels):
+            m = self.macroscopic(lev)
+            g = S.grid
+            levels.append(dict(coords=self.multilevel.positions(lev), spacing=float(self.multilevel.spacing[lev]),
+                               geo=g.geo, neighbor=g.neighbor, rho=m["rho"], vx=m["vx"], vy=m["vy"], vz=m["vz"],
+                               pressure=m["pressure"]))
+        return writer, writer.write_timestep(timestep, levels, last=last)
+
     def save_restart(self, path):
         """RestartObject::serialize (binary): every level's population array, `path` + ".bin"."""
         from .output import save_restart
