@@ -122,6 +122,16 @@ int vfb_abi_version(void);
 const char *vfb_last_error(void);
 const char *vfb_status_string(int status);
 int vfb_synchronize(void *stream);
+/* Bounds-checked build (libvfb_checked.so, compiled with -DVFB_BOUNDS_CHECK; no counterpart in the
+   reference, which range-checks host containers only): every node index a kernel takes from the
+   caller's arrays (fluid-node lists, neighborX/Y/Z, BC node lists, interpolation cells) is compared
+   with its level's node count; an index out of range is replaced by the dummy node 0, so no access
+   leaves the arrays, and the first one is recorded. vfb_bounds_checked() is 1 in that build.
+   vfb_bounds_check_status synchronises the device, returns the first recorded index and the node
+   count it exceeded (VFB_ERR_INVALID_ARGUMENT when there is one, VFB_OK when none) and clears the
+   record; in the default build it returns VFB_ERR_UNSUPPORTED. */
+int vfb_bounds_checked(void);
+int vfb_bounds_check_status(uint64_t *bad_index, uint64_t *node_count);
 /* D3Q27 tables as the kernels use them (for host-side checks) */
 int vfb_lattice_tables(int32_t cx[27], int32_t cy[27], int32_t cz[27], int32_t inv[27], double w[27]);
 /* the omega-only K17 relaxation rates as precomputed on the host:

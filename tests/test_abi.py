@@ -256,3 +256,20 @@ def test_scaling_argument_validation_without_launching():
         # no cells: nothing to launch, nothing to check
         empty = N.InterpolationCells(0, 0, 0)
         assert f(C.byref(coarse), C.byref(fine), C.byref(empty), C.byref(bad), None) == N.VFB_OK
+
+
+def test_bounds_checked_build_loads_and_reports_itself():
+    """libvfb_checked.so (built by build(checked=True)) exports the same ABI and says it is the
+    checked build; the default build answers that it has no checks. No CUDA call is made."""
+    from virtualfluids_b200 import _native as N
+    from virtualfluids_b200 import build as vbuild
+    if not vbuild.LIB_CHECKED.exists():
+        pytest.skip("libvfb_checked.so not built here")
+    checked = C.CDLL(str(vbuild.LIB_CHECKED))
+    assert checked.vfb_bounds_checked() == 1
+    assert N.lib().vfb_bounds_checked() == 0
+    bad, n = C.c_uint64(7), C.c_uint64(7)
+    assert N.lib().vfb_bounds_check_status(C.byref(bad), C.byref(n)) == N.VFB_ERR_UNSUPPORTED
+    assert bad.value == 0 and n.value == 0
+    missing = [name for name in _declared_symbols() if not hasattr(checked, name)]
+    assert not missing, missing

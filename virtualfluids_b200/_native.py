@@ -9,7 +9,9 @@ import ctypes as C
 import os
 from pathlib import Path
 
-_LIB_PATH = Path(__file__).resolve().parent / "libvfb.so"
+# VFB_LIBRARY=checked loads the bounds-checked build (libvfb_checked.so) instead of the default one
+_LIB_PATH = Path(__file__).resolve().parent / (
+    "libvfb_checked.so" if os.environ.get("VFB_LIBRARY", "") == "checked" else "libvfb.so")
 
 VFB_OK = 0
 VFB_ERR_INVALID_ARGUMENT = 1
@@ -125,6 +127,8 @@ SIGNATURES = {
     "vfb_last_error": (C.c_char_p, []),
     "vfb_status_string": (C.c_char_p, [C.c_int]),
     "vfb_synchronize": (C.c_int, [C.c_void_p]),
+    "vfb_bounds_checked": (C.c_int, []),
+    "vfb_bounds_check_status": (C.c_int, [C.c_void_p, C.c_void_p]),
     "vfb_lattice_tables": (C.c_int, [C.c_void_p] * 5),
     "vfb_k17_rates": (C.c_int, [C.c_double, C.c_void_p]),
     "vfb_kernel_lookup": (C.c_int, [C.c_char_p, C.POINTER(C.c_int32)]),

@@ -3,7 +3,10 @@
 Every translation unit under ``csrc/`` is compiled by nvcc for ``sm_100a`` into the package
 directory, so the shared object travels with the source tree. The ``k_exact_*`` units are
 compiled without FMA contraction (``-fmad=false``): they are the bit-reproducible arithmetic
-variant. Run ``python -m virtualfluids_b200.build`` or call :func:`build`.
+variant. ``build(checked=True)`` (``python -m virtualfluids_b200.build --checked``) makes
+``libvfb_checked.so``, the same sources with ``-DVFB_BOUNDS_CHECK``: every node index taken from a
+caller's array is checked against its level's node count (vfb_bounds_check_status). Run
+``python -m virtualfluids_b200.build`` or call :func:`build`.
 """
 from __future__ import annotations
 
@@ -18,6 +21,8 @@ CSRC = PKG / "csrc"
 INCLUDE = PKG.parent / "include"
 BUILD = PKG / "_build"
 LIB = PKG / "libvfb.so"
+BUILD_CHECKED = PKG / "_build_checked"
+LIB_CHECKED = PKG / "libvfb_checked.so"
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -29,10 +34,12 @@ def _sources():
     return sorted(CSRC.glob("*.cu"))
 
 
-def _flags(src: Path):
+def _flags(src: Path, checked: bool = False):
     flags = list(COMMON) + ARCH
     if src.name.startswith("k_exact_"):
         flags.append("-fmad=false")
+    if checked:
+        flags.append("-DVFB_BOUNDS_CHECK")
     return flags
 
 
@@ -44,32 +51,33 @@ def _needs(obj: Path, src: Path) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
-def _compile(src: Path, verbose: bool):
-    obj = BUILD / (src.stem + ".o")
+def _compile(src: Path, verbose: bool, checked: bool = False):
+    obj = (BUILD_CHECKED if checked else BUILD) / (src.stem + ".o")
     if not _needs(obj, src):
         return obj
-    cmd = [NVCC] + _flags(src) + ["-c", str(src), "-o", str(obj)]
+    cmd = [NVCC] + _flags(src, checked) + ["-c", str(src), "-o", str(obj)]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)
     return obj
 
 
-def build(verbose: bool = False, jobs: int | None = None) -> Path:
-    """Compile and link ``libvfb.so``; returns its path. Incremental on file times."""
-    BUILD.mkdir(exist_ok=True)
+def build(verbose: bool = False, jobs: int | None = None, checked: bool = False) -> Path:
+    """Compile and link ``libvfb.so`` (``libvfb_checked.so`` with checked=True); returns its path.
+    Incremental on file times."""
+    out_dir, lib = (BUILD_CHECKED, LIB_CHECKED) if checked else (BUILD, LIB)
+    out_dir.mkdir(exist_ok=True)
     srcs = _sources()
     jobs = jobs or min(len(srcs), os.cpu_count() or 4)
     with ThreadPoolExecutor(max_workers=jobs) as ex:
-        objs = list(ex.map(lambda s: _compile(s, verbose), srcs))
-    if not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", str(LIB)] + [str(o) for o in objs] + ["-lcudart_static"]
+        objs = list(ex.map(lambda s: _compile(s, verbose, checked), srcs))
+    if not lib.exists() or any(o.stat().st_mtime > lib.stat().st_mtime for o in objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", str(lib)] + [str(o) for o in objs] + ["-lcudart_static"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
-    build(verbose="-v" in sys.argv)
-    print(LIB)
+    print(build(verbose="-v" in sys.argv, checked="--checked" in sys.argv))

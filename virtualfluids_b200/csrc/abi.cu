@@ -229,6 +229,44 @@ const char *vfb_status_string(int status)
     }
 }
 
+int vfb_bounds_checked(void)
+{
+#ifdef VFB_BOUNDS_CHECK
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+int vfb_bounds_check_status(uint64_t *bad_index, uint64_t *node_count)
+{
+    if (!bad_index || !node_count)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    *bad_index = 0;
+    *node_count = 0;
+#ifndef VFB_BOUNDS_CHECK
+    return fail(VFB_ERR_UNSUPPORTED, "this library is built without bounds checks (libvfb_checked.so has them)");
+#else
+    cudaError_t e = cudaDeviceSynchronize();
+    uint64_t recs[6] = {};
+    if (e == cudaSuccess) e = vfb::exact::Launchers<double>::bounds_error(&recs[0]);
+    if (e == cudaSuccess) e = vfb::exact::Launchers<float>::bounds_error(&recs[1]);
+    if (e == cudaSuccess) e = vfb::fast::Launchers<double>::bounds_error(&recs[2]);
+    if (e == cudaSuccess) e = vfb::fast::Launchers<float>::bounds_error(&recs[3]);
+    if (e == cudaSuccess) e = vfb::fast::Launchers<__half>::bounds_error(&recs[4]);
+    if (e == cudaSuccess) e = vfb::fast::Launchers<__nv_bfloat16>::bounds_error(&recs[5]);
+    if (e != cudaSuccess)
+        return cuda_status(e, "bounds-check record");
+    for (uint64_t r : recs)
+        if (r) {
+            *bad_index = (r & 0xffffffffull) - 1;
+            *node_count = r >> 32;
+            return fail(VFB_ERR_INVALID_ARGUMENT, "a kernel met a node index beyond its level's node count");
+        }
+    return VFB_OK;
+#endif
+}
+
 int vfb_synchronize(void *stream)
 {
     return cuda_status(stream ? cudaStreamSynchronize(as_stream(stream)) : cudaDeviceSynchronize(), "synchronize");

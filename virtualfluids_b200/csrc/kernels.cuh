@@ -24,6 +24,28 @@ namespace vfb {
 namespace VFB_NS {
 
 // ---------------------------------------------------------------------------------------------
+// Bounds-checked build (-DVFB_BOUNDS_CHECK, libvfb_checked.so): every node index a kernel takes
+// from a caller's array (fluid-node lists, neighbour lists, BC node lists, interpolation cells,
+// slot tables) is compared with the node count of its level before it is used. An index out of
+// range is recorded -- the first one since the last read, as (bound << 32) | (index + 1) -- and
+// replaced by the dummy node 0, so no access leaves the arrays; the host reads the record with
+// vfb_bounds_check_status. In the default build VFB_NODE is the index itself.
+// ---------------------------------------------------------------------------------------------
+#ifdef VFB_BOUNDS_CHECK
+static __device__ unsigned long long g_bounds_error;
+__device__ __forceinline__ uint32_t checked_node(uint32_t v, uint64_t n)
+{
+    if ((uint64_t)v < n)
+        return v;
+    atomicCAS(&g_bounds_error, 0ull, ((unsigned long long)(n & 0xffffffffull) << 32) | ((unsigned long long)v + 1ull));
+    return 0u;
+}
+#define VFB_NODE(v, n) checked_node((v), (n))
+#else
+#define VFB_NODE(v, n) (v)
+#endif
+
+// ---------------------------------------------------------------------------------------------
 // argument packs
 // ---------------------------------------------------------------------------------------------
 template <class C>
@@ -91,19 +113,22 @@ struct PressureArgs {
 // ---------------------------------------------------------------------------------------------
 
 // ListIndices (KernelUtilities.h:221-250) by shift class: bit0 x+1, bit1 y+1, bit2 z+1
+// (n: node count of the level, the bound of the bounds-checked build)
 __device__ __forceinline__ void list_nodes(uint32_t k, const uint32_t *__restrict__ nbx, const uint32_t *__restrict__ nby,
-                                           const uint32_t *__restrict__ nbz, uint32_t (&nodes)[8])
+                                           const uint32_t *__restrict__ nbz, uint64_t n, uint32_t (&nodes)[8])
 {
-    const uint32_t kx = __ldg(nbx + k), ky = __ldg(nby + k), kz = __ldg(nbz + k);
-    const uint32_t kxy = __ldg(nby + kx);
+    (void)n;
+    k = VFB_NODE(k, n);
+    const uint32_t kx = VFB_NODE(__ldg(nbx + k), n), ky = VFB_NODE(__ldg(nby + k), n), kz = VFB_NODE(__ldg(nbz + k), n);
+    const uint32_t kxy = VFB_NODE(__ldg(nby + kx), n);
     nodes[0] = k;
     nodes[1] = kx;
     nodes[2] = ky;
     nodes[3] = kxy;
     nodes[4] = kz;
-    nodes[5] = __ldg(nbz + kx);
-    nodes[6] = __ldg(nbz + ky);
-    nodes[7] = __ldg(nbz + kxy);
+    nodes[5] = VFB_NODE(__ldg(nbz + kx), n);
+    nodes[6] = VFB_NODE(__ldg(nbz + ky), n);
+    nodes[7] = VFB_NODE(__ldg(nbz + kxy), n);
 }
 
 // the eight slot nodes of a node on a structured box
@@ -128,6 +153,7 @@ __device__ __forceinline__ void box_nodes_at(uint32_t k, uint32_t x, uint32_t y,
 
 __device__ __forceinline__ void box_nodes(uint32_t k, const NodeAddr &b, uint32_t (&nodes)[8])
 {
+    k = VFB_NODE(k, (uint64_t)b.nx * (uint64_t)b.ny * (uint64_t)b.nz);
     const uint32_t x = k % (uint32_t)b.nx, yz = k / (uint32_t)b.nx;
     const uint32_t y = yz % (uint32_t)b.ny, z = yz / (uint32_t)b.ny;
     box_nodes_at(k, x, y, z, b, nodes);
@@ -137,16 +163,17 @@ __device__ __forceinline__ void box_nodes(uint32_t k, const NodeAddr &b, uint32_
 __device__ __forceinline__ void box_nodes(uint32_t k, const NodeAddr &b, FastDiv div_nx, FastDiv div_ny,
                                           uint32_t (&nodes)[8])
 {
+    k = VFB_NODE(k, (uint64_t)b.nx * (uint64_t)b.ny * (uint64_t)b.nz);
     const uint32_t yz = fast_div(k, div_nx), x = k - yz * (uint32_t)b.nx;
     const uint32_t z = fast_div(yz, div_ny), y = yz - z * (uint32_t)b.ny;
     box_nodes_at(k, x, y, z, b, nodes);
 }
 
 __device__ __forceinline__ void node_slots(uint32_t k, const uint32_t *nbx, const uint32_t *nby, const uint32_t *nbz,
-                                           const NodeAddr &b, uint32_t (&nodes)[8])
+                                           uint64_t n, const NodeAddr &b, uint32_t (&nodes)[8])
 {
     if (nbx)
-        list_nodes(k, nbx, nby, nbz, nodes);
+        list_nodes(k, nbx, nby, nbz, n, nodes);
     else
         box_nodes(k, b, nodes);
 }
@@ -199,7 +226,7 @@ __global__ void __launch_bounds__(128) k17_list_kernel(ListCollideArgs<typename 
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n_idx)
         return;
-    const uint32_t k = __ldg(a.idx + i);
+    const uint32_t k = VFB_NODE(__ldg(a.idx + i), a.n);
     C fx = a.fx, fy = a.fy, fz = a.fz;
     if (BODY_FORCE) {
         fx = (a.force0 + a.bfx[k]) * C(0.5) * a.force_factor;
@@ -215,9 +242,9 @@ __global__ void __launch_bounds__(128) k17_list_kernel(ListCollideArgs<typename 
         nodes[0] = k;
 #pragma unroll
         for (int j = 1; j < 8; ++j)
-            nodes[j] = __ldg(a.slots + (size_t)j * a.slots_stride + i);
+            nodes[j] = VFB_NODE(__ldg(a.slots + (size_t)j * a.slots_stride + i), a.n);
     } else {
-        list_nodes(k, a.nbx, a.nby, a.nbz, nodes);
+        list_nodes(k, a.nbx, a.nby, a.nbz, a.n, nodes);
     }
     S *base = static_cast<S *>(a.dist);
     C f[27];
@@ -888,7 +915,7 @@ __global__ void __launch_bounds__(128) bc_bounce_back_kernel(BCArgs a)
         return;
     const uint32_t node = (uint32_t)a.k[i];
     uint32_t nodes[8];
-    node_slots(node, a.nbx, a.nby, a.nbz, a.box, nodes);
+    node_slots(node, a.nbx, a.nby, a.nbz, a.n, a.box, nodes);
     S *base = static_cast<S *>(a.dist);
     C post[27];
     if (a.snap) {
@@ -1073,7 +1100,7 @@ __global__ void __launch_bounds__(128) bc_interpolated_kernel(BCArgs a)
     if (i >= a.nbc)
         return;
     uint32_t nodes[8];
-    node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.box, nodes);
+    node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.n, a.box, nodes);
     C bx = C(0), by = C(0), bz = C(0);
     if (VELOCITY) {
         bx = static_cast<const C *>(a.ux)[i];
@@ -1099,7 +1126,7 @@ __global__ void __launch_bounds__(128) bc_guard_kernel(BCArgs a, typename Codec<
     if (!mask)
         return;
     uint32_t nodes[8];
-    node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.box, nodes);
+    node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.n, a.box, nodes);
     const S *base = static_cast<const S *>(a.dist);
     typename Codec<S>::compute *out = saved + a.guard[a.nbc + i];
     int r = 0;
@@ -1121,7 +1148,7 @@ __global__ void __launch_bounds__(128) bc_snapshot_kernel(BCArgs a, typename Cod
     if (i >= a.nbc)
         return;
     uint32_t nodes[8];
-    node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.box, nodes);
+    node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.n, a.box, nodes);
     C p[27];
     gather_post<S, EVEN>(static_cast<const S *>(a.dist), a.n, nodes, p);
 #pragma unroll
@@ -1187,8 +1214,8 @@ __global__ void __launch_bounds__(128) bc_pressure_neq_kernel(PressureArgs a)
     if (i >= a.nbc)
         return;
     uint32_t nn[8], nk[8];
-    node_slots((uint32_t)a.kN[i], a.nbx, a.nby, a.nbz, a.box, nn);
-    node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.box, nk);
+    node_slots((uint32_t)a.kN[i], a.nbx, a.nby, a.nbz, a.n, a.box, nn);
+    node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.n, a.box, nk);
     bc_pressure_neq_node<S, EVEN, INCOMP>(static_cast<S *>(a.dist), a.n, nk, nn, static_cast<const C *>(a.rho_bc)[i],
                                           a.direction);
 }
@@ -1209,14 +1236,14 @@ __global__ void __launch_bounds__(128) bc_outflow_kernel(PressureArgs a, double 
     if (i >= a.nbc)
         return;
     uint32_t nk[8], nn[8];
-    node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.box, nk);
+    node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.n, a.box, nk);
     if (CORRECTION) {
 #pragma unroll
         for (int c = 0; c < 8; ++c)
             nn[c] = nk[c];
         nn[0] = (uint32_t)a.kN[i];
     } else {
-        node_slots((uint32_t)a.kN[i], a.nbx, a.nby, a.nbz, a.box, nn);
+        node_slots((uint32_t)a.kN[i], a.nbx, a.nby, a.nbz, a.n, a.box, nn);
     }
     S *base = static_cast<S *>(a.dist);
     C f[27], fn[27];
@@ -1259,7 +1286,7 @@ __global__ void __launch_bounds__(128) init_list_kernel(void *dist, uint64_t n, 
     if (g == kGeoSolid || g == kGeoVoid)
         return;
     uint32_t nodes[8];
-    list_nodes((uint32_t)k, nbx, nby, nbz, nodes);
+    list_nodes((uint32_t)k, nbx, nby, nbz, n, nodes);
     const C drho = static_cast<const C *>(rho)[k];
     const C vx = static_cast<const C *>(ux)[k], vy = static_cast<const C *>(uy)[k], vz = static_cast<const C *>(uz)[k];
     const C cu_sq = C(1.5) * (vx * vx + vy * vy + vz * vz);
@@ -1333,7 +1360,7 @@ __global__ void __launch_bounds__(128) macros_list_kernel(const void *dist, uint
     if (geo[k] != kGeoFluid)
         return;
     uint32_t nodes[8];
-    list_nodes((uint32_t)k, nbx, nby, nbz, nodes);
+    list_nodes((uint32_t)k, nbx, nby, nbz, n, nodes);
     C f[27];
     gather_pre<S, EVEN>(static_cast<const S *>(dist), n, nodes, f);
     const C r = density_pyramid(f);
@@ -1393,7 +1420,7 @@ __global__ void __launch_bounds__(256) energy_list_kernel(const void *dist, uint
     double m = 0.0, e = 0.0;
     if (i < n_idx) {
         uint32_t nodes[8];
-        list_nodes(__ldg(idx + i), nbx, nby, nbz, nodes);
+        list_nodes(__ldg(idx + i), nbx, nby, nbz, n, nodes);
         C f[27];
         gather_pre<S, EVEN>(static_cast<const S *>(dist), n, nodes, f);
         const C r = density_pyramid(f);
@@ -1448,15 +1475,17 @@ struct ScaleArgs {
 
 // corner c = ix + 2 iy + 4 iz of the cell whose MMM node is `base`, stepping x, then y, then z
 __device__ __forceinline__ uint32_t cell_corner(uint32_t base, int c, const uint32_t *__restrict__ nbx,
-                                                const uint32_t *__restrict__ nby, const uint32_t *__restrict__ nbz)
+                                                const uint32_t *__restrict__ nby, const uint32_t *__restrict__ nbz,
+                                                uint64_t n)
 {
-    uint32_t k = base;
+    (void)n;
+    uint32_t k = VFB_NODE(base, n);
     if (c & 1)
-        k = __ldg(nbx + k);
+        k = VFB_NODE(__ldg(nbx + k), n);
     if (c & 2)
-        k = __ldg(nby + k);
+        k = VFB_NODE(__ldg(nby + k), n);
     if (c & 4)
-        k = __ldg(nbz + k);
+        k = VFB_NODE(__ldg(nbz + k), n);
     return k;
 }
 
@@ -1474,7 +1503,7 @@ __device__ __forceinline__ void cell_coefficients_of_group(const S *base, uint64
     C m[9];
     if (valid) {
         uint32_t nodes[8];
-        list_nodes(k, nbx, nby, nbz, nodes);
+        list_nodes(k, nbx, nby, nbz, n, nodes);
         C f[27];
         gather_pre<S, EVEN>(base, n, nodes, f);
         interp_node_moments(f, omega, m);
@@ -1503,7 +1532,7 @@ __global__ void __launch_bounds__(128) scale_cf_kernel(ScaleArgs a)
     uint32_t k = 0;
     C xo = C(0), yo = C(0), zo = C(0);
     if (valid) {
-        k = cell_corner(__ldg(a.coarse_cells + cell), corner, a.nbx_c, a.nby_c, a.nbz_c);
+        k = cell_corner(__ldg(a.coarse_cells + cell), corner, a.nbx_c, a.nby_c, a.nbz_c, a.n_coarse);
         xo = static_cast<const C *>(a.ox)[cell];
         yo = static_cast<const C *>(a.oy)[cell];
         zo = static_cast<const C *>(a.oz)[cell];
@@ -1518,8 +1547,8 @@ __global__ void __launch_bounds__(128) scale_cf_kernel(ScaleArgs a)
     interp_point<C, false>(coef, (C)a.omega_fine, C(0.5), (corner & 1) ? q : -q, (corner & 2) ? q : -q,
                            (corner & 4) ? q : -q, f);
     uint32_t nodes[8];
-    list_nodes(cell_corner(__ldg(a.fine_cells + cell), corner, a.nbx_f, a.nby_f, a.nbz_f), a.nbx_f, a.nby_f, a.nbz_f,
-               nodes);
+    list_nodes(cell_corner(__ldg(a.fine_cells + cell), corner, a.nbx_f, a.nby_f, a.nbz_f, a.n_fine), a.nbx_f, a.nby_f,
+               a.nbz_f, a.n_fine, nodes);
     S *fine = static_cast<S *>(a.dist_fine);
 #pragma unroll
     for (int d = 0; d < 27; ++d)
@@ -1541,7 +1570,7 @@ __global__ void __launch_bounds__(128) scale_fc_kernel(ScaleArgs a)
     uint32_t k = 0;
     C xo = C(0), yo = C(0), zo = C(0);
     if (valid) {
-        k = cell_corner(__ldg(a.fine_cells + cell), corner, a.nbx_f, a.nby_f, a.nbz_f);
+        k = cell_corner(__ldg(a.fine_cells + cell), corner, a.nbx_f, a.nby_f, a.nbz_f, a.n_fine);
         xo = static_cast<const C *>(a.ox)[cell];
         yo = static_cast<const C *>(a.oy)[cell];
         zo = static_cast<const C *>(a.oz)[cell];
@@ -1554,7 +1583,7 @@ __global__ void __launch_bounds__(128) scale_fc_kernel(ScaleArgs a)
     C f[27];
     interp_point<C, true>(coef, (C)a.omega_coarse, C(2), C(0), C(0), C(0), f);
     uint32_t nodes[8];
-    list_nodes(__ldg(a.coarse_cells + cell), a.nbx_c, a.nby_c, a.nbz_c, nodes);
+    list_nodes(__ldg(a.coarse_cells + cell), a.nbx_c, a.nby_c, a.nbz_c, a.n_coarse, nodes);
     S *coarse = static_cast<S *>(a.dist_coarse);
 #pragma unroll
     for (int d = 0; d < 27; ++d)
@@ -1614,7 +1643,7 @@ __global__ void __launch_bounds__(128) drag_lift_kernel(DragArgs a)
     if (i >= a.nbc)
         return;
     uint32_t nodes[8];
-    node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.box, nodes);
+    node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.n, a.box, nodes);
     const S *base = static_cast<const S *>(a.dist);
     C fc[27];
     if constexpr (PRE)

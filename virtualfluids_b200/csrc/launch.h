@@ -97,6 +97,7 @@ struct PoolDomainSpec {
                                     const uint32_t *n_pressure_items, bool even, unsigned grid, cudaStream_t s);   \
         static cudaError_t drag_lift(const vfb_level *L, const vfb_bc *bc, bool pre, double *dx, double *dy,        \
                                      double *dz, cudaStream_t s, const NodeAddr *box = nullptr);                     \
+        static cudaError_t bounds_error(uint64_t *record);                                                        \
         static cudaError_t scale(const vfb_level *coarse, const vfb_level *fine, const vfb_interpolation_cells *cells, \
                                  const vfb_interpolation_cell_neighbor *offsets, bool fine_to_coarse, cudaStream_t s); \
     };

@@ -761,6 +761,24 @@ cudaError_t Launchers<S>::box_collide(const BoxState &b, bool even, double *part
     return cudaGetLastError();
 }
 
+// the bounds record of this translation unit's kernels (bounds-checked build), read and cleared;
+// 0 in the default build
+template <class S>
+cudaError_t Launchers<S>::bounds_error(uint64_t *record)
+{
+#ifdef VFB_BOUNDS_CHECK
+    unsigned long long v = 0, zero = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&v, g_bounds_error, sizeof(v));
+    if (e == cudaSuccess)
+        e = cudaMemcpyToSymbol(g_bounds_error, &zero, sizeof(zero));
+    *record = v;
+    return e;
+#else
+    *record = 0;
+    return cudaSuccess;
+#endif
+}
+
 template <class S>
 cudaError_t Launchers<S>::box_init(const BoxState &b, bool even, const void *rho, const void *ux, const void *uy,
                                    const void *uz, cudaStream_t s)

@@ -436,6 +436,13 @@ class Simulation:
                          {"drho": m["rho"][f], "velocity": np.stack([m["vx"][f], m["vy"][f], m["vz"][f]]),
                           "pressure": m["pressure"][f]}, title=f"level {level}")
 
+    def check_slots(self):
+        """The host check of every level's esoteric-twist write pattern (checks.check_grid): each
+        slot written once per step by the collision and by the BC lists, in both parities. Returns
+        the per-level reports; raises ValueError on the first level with a conflict."""
+        from .checks import assert_slots_written_once
+        return [assert_slots_written_once(S.grid) for S in self.levels]
+
     def write_vtu(self, prefix, timestep, last=False, writer=None):
         """Every level's fields in the reference's output files (FileWriter::writeTimestep,
         Output/FileWriter.cpp:104-137): part files of octs with press, rho, vx1, vx2, vx3 and geo,
