@@ -211,7 +211,7 @@ class OracleLevel:
             if b.kind != "pressure":
                 continue
             arrs = [np.ascontiguousarray(b.k.astype(np.int32)), np.ascontiguousarray(b.k_neighbor.astype(np.int32)),
-                    np.full(b.k.size, float(b.rho))]
+                    np.ascontiguousarray(np.broadcast_to(np.asarray(b.rho, dtype=np.float64), (b.k.size,)))]
             self._keep += arrs
             pr.append(_Pressure(arrs[0].ctypes.data, arrs[1].ctypes.data, arrs[2].ctypes.data, b.k.size, SIDE_DIR[b.side]))
         self.pr = (_Pressure * max(len(pr), 1))(*pr) if pr else None
@@ -364,3 +364,118 @@ def interp_fc_cell(f8, omega_fine, omega_coarse, offset=(0.0, 0.0, 0.0)):
     out = np.zeros(27)
     L.orc_interp_point(ptr(coef), omega_coarse, 2.0, 0.0, 0.0, 0.0, 1, ptr(out))
     return out
+
+
+# ---------------------------------------------------------------------------------------------
+# the reference's own grid generator (_ref/libvfref_gridgen.so)
+# ---------------------------------------------------------------------------------------------
+REFGG = HERE / "_ref" / "libvfref_gridgen.so"
+SIDE_INDEX = {"MX": 0, "PX": 1, "MY": 2, "PY": 3, "MZ": 4, "PZ": 5, "GEOMETRY": 6}
+
+
+def refgg():
+    """The reference's GridGenerator behind ref_gridgen_shim.cpp, or None where it is not built."""
+    if not REFGG.exists():
+        return None
+    L = C.CDLL(str(REFGG))
+    d, i, u = C.c_double, C.c_int, C.c_uint32
+    L.refgg_create.restype = _P
+    L.refgg_create.argtypes = [d] * 7
+    for name in ("refgg_build", "refgg_find_fluid_nodes", "refgg_destroy"):
+        getattr(L, name).argtypes = [_P]
+    L.refgg_add_refinement.argtypes = [_P] + [d] * 6 + [i]
+    L.refgg_add_geometry.argtypes = [_P, i] + [d] * 6
+    L.refgg_set_periodic.argtypes = [_P, i, i, i]
+    L.refgg_set_noslip.argtypes = [_P, i]
+    L.refgg_set_velocity.argtypes = [_P, i, d, d, d]
+    L.refgg_set_pressure.argtypes = [_P, i, d]
+    L.refgg_levels.argtypes = [_P]
+    L.refgg_delta.argtypes = [_P, i]
+    L.refgg_delta.restype = d
+    for name in ("refgg_nodes", "refgg_fluid_count", "refgg_velocity_size", "refgg_geometry_size", "refgg_cf_count",
+                 "refgg_fc_count"):
+        getattr(L, name).argtypes = [_P, i]
+        getattr(L, name).restype = u
+    L.refgg_node_values.argtypes = [_P, i] + [_P] * 8
+    L.refgg_fluid.argtypes = [_P, i, _P]
+    L.refgg_velocity.argtypes = [_P, i] + [_P] * 5
+    L.refgg_pressure_count.argtypes = [_P, i]
+    L.refgg_pressure_size.argtypes = [_P, i, i]
+    L.refgg_pressure_size.restype = u
+    L.refgg_pressure.argtypes = [_P, i, i] + [_P] * 4
+    L.refgg_geometry.argtypes = [_P, i] + [_P] * 5
+    L.refgg_interface.argtypes = [_P, i] + [_P] * 10
+    assert L.refgg_real_bytes() == 8
+    return L
+
+
+def reference_grid(box, delta, refinements=(), geometries=(), periodic=(False, False, False), noslip=(),
+                   velocity=(), pressure=(), geometry_noslip=False):
+    """Build a grid with the reference's MultipleGridBuilder and return the arrays its getters hand
+    to the solver (the dicts virtualfluids_b200.gridgen.import_levels takes), as
+    (levels, interfaces). box: (x0, y0, z0, x1, y1, z1); refinements: ((x0..z1), level_fine);
+    geometries: ("sphere", cx, cy, cz, r) or ("cuboid", x0, y0, z0, x1, y1, z1); noslip: side names;
+    velocity: (side, vx, vy, vz); pressure: (side, rho). The order of the calls is the reference
+    apps' (DrivenCavity.cpp:95-146): grids, periodicity, build, then boundary conditions."""
+    L = refgg()
+    if L is None:
+        raise FileNotFoundError("oracle/_ref/libvfref_gridgen.so is not built (make -C oracle ref)")
+    h = L.refgg_create(*(float(x) for x in box), float(delta))
+    try:
+        for b, lev in refinements:
+            L.refgg_add_refinement(h, *(float(x) for x in b), int(lev))
+        for g in geometries:
+            vals = [float(x) for x in g[1:]] + [0.0] * (7 - len(g))
+            L.refgg_add_geometry(h, 0 if g[0] == "sphere" else 1, *vals[:6])
+        L.refgg_set_periodic(h, *(int(bool(p)) for p in periodic))
+        L.refgg_build(h)
+        for s in noslip:
+            L.refgg_set_noslip(h, SIDE_INDEX[s])
+        for s, vx, vy, vz in velocity:
+            L.refgg_set_velocity(h, SIDE_INDEX[s], vx, vy, vz)
+        for s, rho in pressure:
+            L.refgg_set_pressure(h, SIDE_INDEX[s], rho)
+        if geometry_noslip:
+            L.refgg_set_noslip(h, SIDE_INDEX["GEOMETRY"])
+        L.refgg_find_fluid_nodes(h)
+        levels, interfaces = [], []
+        for lev in range(L.refgg_levels(h)):
+            n = L.refgg_nodes(h, lev)
+            xyz = [np.zeros(n) for _ in range(3)]
+            nb = [np.zeros(n, dtype=np.uint32) for _ in range(5)]
+            L.refgg_node_values(h, lev, *(ptr(a) for a in xyz), *(ptr(a) for a in nb))
+            fl = np.zeros(L.refgg_fluid_count(h, lev), dtype=np.uint32)
+            L.refgg_fluid(h, lev, ptr(fl))
+            nv = L.refgg_velocity_size(h, lev)
+            vel = {"k": np.zeros(nv, dtype=np.int32), "q27": np.zeros(27 * nv),
+                   **{c: np.zeros(nv) for c in ("vx", "vy", "vz")}}
+            if nv:
+                L.refgg_velocity(h, lev, ptr(vel["vx"]), ptr(vel["vy"]), ptr(vel["vz"]), ptr(vel["k"]), ptr(vel["q27"]))
+            press = []
+            for j in range(L.refgg_pressure_count(h, lev)):
+                m = L.refgg_pressure_size(h, lev, j)
+                p = {"k": np.zeros(m, dtype=np.int32), "k_neighbor": np.zeros(m, dtype=np.int32), "rho": np.zeros(m),
+                     "q27": np.zeros(27 * m)}
+                if m:
+                    p["direction"] = L.refgg_pressure(h, lev, j, ptr(p["rho"]), ptr(p["k"]), ptr(p["k_neighbor"]),
+                                                      ptr(p["q27"]))
+                    press.append(p)
+            ng = L.refgg_geometry_size(h, lev)
+            geom = {"k": np.zeros(ng, dtype=np.int32), "q27": np.zeros(27 * ng),
+                    **{c: np.zeros(ng) for c in ("vx", "vy", "vz")}}
+            if ng:
+                L.refgg_geometry(h, lev, ptr(geom["k"]), ptr(geom["q27"]), ptr(geom["vx"]), ptr(geom["vy"]),
+                                 ptr(geom["vz"]))
+            levels.append({"number_of_nodes": n, "delta": L.refgg_delta(h, lev), "coords": xyz, "neighbor": nb[:3],
+                           "neighbor_inverse": nb[3], "geo": nb[4], "fluid": fl, "velocity": vel, "pressure": press,
+                           "geometry": geom})
+        for lev in range(L.refgg_levels(h) - 1):
+            ncf, nfc = L.refgg_cf_count(h, lev), L.refgg_fc_count(h, lev)
+            idx = [np.zeros(m, dtype=np.uint32) for m in (ncf, ncf, nfc, nfc)]
+            off = [np.zeros(m) for m in (ncf, ncf, ncf, nfc, nfc, nfc)]
+            L.refgg_interface(h, lev, *(ptr(a) for a in idx), *(ptr(a) for a in off))
+            interfaces.append({"cf_coarse": idx[0], "cf_fine": idx[1], "fc_coarse": idx[2], "fc_fine": idx[3],
+                               "offsets_cf": np.stack(off[:3]), "offsets_fc": np.stack(off[3:])})
+        return levels, interfaces
+    finally:
+        L.refgg_destroy(h)

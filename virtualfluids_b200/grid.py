@@ -9,7 +9,7 @@ A box of fluid nodes is laid out as the reference's GridGenerator lays out a uni
   unused nodes are solid and point nowhere), so every direction plane and every x-row of a box
   whose row length is a multiple of `align` starts on an aligned boundary;
 * a one-node layer of stopper nodes around the fluid on every non-periodic side; stoppers are
-  in the node list but never collided (geo GEO_SOLID);
+  in the node list but never collided (geo GEO_VOID, as getNodeValues marks every non-fluid node);
 * neighborX/Y/Z[k] = the node at +1 in x/y/z, wrapped on periodic axes (setNeighborIndices
   :1012-1032, getNeighborIndex :1071-1080); stoppers get their in-grid +1 neighbours only
   (setStopperNeighborCoords :1034-1057);
@@ -89,7 +89,7 @@ class ListGrid:
         c = coords[:, g0:g1]
         fluid_mask[g0:g1] = ((c[0] >= 0) & (c[0] < self.nx) & (c[1] >= 0) & (c[1] < self.ny)
                              & (c[2] >= 0) & (c[2] < self.nz))
-        self.geo = np.where(fluid_mask, N.GEO_FLUID, N.GEO_SOLID).astype(np.uint32)
+        self.geo = np.where(fluid_mask, N.GEO_FLUID, N.GEO_VOID).astype(np.uint32)
         self.fluid = np.nonzero(fluid_mask)[0].astype(np.uint32)
         nb = np.zeros((3, self.number_of_nodes), dtype=np.uint32)
         g = [gx, gy, gz]
@@ -198,7 +198,7 @@ class ListGrid:
         inside[0] = False
         was_fluid = self.geo == N.GEO_FLUID
         solid = inside & was_fluid
-        self.geo = np.where(solid, N.GEO_SOLID, self.geo).astype(np.uint32)
+        self.geo = np.where(solid, N.GEO_VOID, self.geo).astype(np.uint32)
         self.fluid = np.nonzero(self.geo == N.GEO_FLUID)[0].astype(np.uint32)
         for b in self.bcs:
             keep = ~solid[b.k]
@@ -246,7 +246,7 @@ class ListGrid:
         inside = d2 <= r * r
         inside[0] = False
         solid = inside & (self.geo == N.GEO_FLUID)
-        self.geo = np.where(solid, N.GEO_SOLID, self.geo).astype(np.uint32)
+        self.geo = np.where(solid, N.GEO_VOID, self.geo).astype(np.uint32)
         self.fluid = np.nonzero(self.geo == N.GEO_FLUID)[0].astype(np.uint32)
         for b in self.bcs:
             keep = ~solid[b.k]

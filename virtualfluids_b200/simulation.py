@@ -272,7 +272,7 @@ class _LevelState:
                 continue
             kt = t.from_numpy(b.k.astype(np.int32)).to(device)
             knt = t.from_numpy(b.k_neighbor.astype(np.int32)).to(device)
-            rt = t.full((b.k.size,), float(b.rho), dtype=rd, device=device)
+            rt = t.from_numpy(np.broadcast_to(np.asarray(b.rho, dtype=np.float64), (b.k.size,)).copy()).to(device, rd)
             self.keep += [kt, knt, rt]
             self.pressure.append(N.DirectionalBC(kt.data_ptr(), knt.data_ptr(), rt.data_ptr(), b.k.size, SIDE_DIR[b.side]))
 
@@ -294,7 +294,8 @@ class Simulation:
             raise N.VfbError(N.VFB_ERR_UNKNOWN_KERNEL, "no main kernel configured")
         t = _torch()
         self.para, self.bcf, self.device = para, bc_factory, device
-        self.multilevel = grid if isinstance(grid, MultiLevelGrid) else MultiLevelGrid.uniform(grid)
+        # nested levels (MultiLevelGrid, or an imported gridgen.ImportedGrid), or a single level
+        self.multilevel = grid if hasattr(grid, "interfaces") else MultiLevelGrid.uniform(grid)
         self.levels = [_LevelState(para, g, i, device) for i, g in enumerate(self.multilevel.levels)]
         base = self.levels[0]
         self.grid, self.level, self.dist, self.fluid = base.grid, base.level, base.dist, base.fluid
