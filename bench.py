@@ -459,6 +459,75 @@ def run_batch(args):
         print(json.dumps(line), flush=True)
 
 
+def run_tgv_slab(args):
+    """The headline's TGV 256^3 box as ONE domain split into z slabs over the ranks (one process per
+    GPU): every step collides each slab's two border planes, exchanges the border planes with the
+    neighbouring ranks by NCCL point-to-point transfers straight out of and into the population
+    arrays on a second stream, collides the interior planes meanwhile, and toggles the parity.
+    Total work is fixed as N grows ("scaling": "strong"); with one rank the slab's ghost plane wraps
+    onto itself by a device copy."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from virtualfluids_b200.slab import DistTransport, Slab, slab_bounds, step
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    n = args.n
+    z0, nzl = slab_bounds(n, world, rank)
+    omega = omega_tgv(n)
+    fields = tgv_fields(n, U0)
+    planes = n * n
+    s = Slab(n, n, n, z0, nzl, omega, storage="f64", arith=args.arith)
+    s.init(*(a[z0 * planes:(z0 + nzl) * planes] for a in fields))
+    tr = DistTransport(s)
+    compute, comm = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    with torch.cuda.stream(compute):
+        for _ in range(args.warmup):
+            step([s], tr, compute=compute, comm=comm)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(compute):
+            e0.record(compute)
+            for _ in range(args.steps):
+                step([s], tr, compute=compute, comm=comm)
+            e1.record(compute)
+        torch.cuda.synchronize()
+    t_ms = max_over_ranks_of(e0.elapsed_time(e1), dist if world > 1 else None, torch.device("cuda", local))
+    f = s.fields()
+    finite = bool(np.all(np.isfinite(f["vx"])))
+    s.close()
+    if rank == 0:
+        mlups = n ** 3 * args.steps / (t_ms / 1e3) / 1e6
+        peak, peak_src = measured_peak()
+        gbs = BYTES_PER_NODE["f64"] * n ** 3 * args.steps / (t_ms / 1e3) / 1e9
+        line = {"metric": f"MLUPS (TGV {n}^3 as one domain in z slabs over the GPUs, FP64)", "value": round(mlups, 1),
+                "unit": "MLUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(t_ms / args.steps, 4), "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": f"Taylor-Green vortex {n}^3 periodic, {world} slab(s) of {nzl} planes, "
+                                       "border-first collision, NCCL halo exchange of 2 x 9 direction planes per "
+                                       "step on a second stream", "arith": args.arith,
+                           "halo_bytes_per_step_per_rank": 2 * 9 * planes * 8 * 2,
+                           "l2": "inputs larger than L2, no flush"},
+                "hbm_gbs_algorithmic": round(gbs / world, 1), "frac_per_gpu": round(gbs / world / peak, 4),
+                "peak_source": peak_src, "finite": finite, "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def run_cube(args):
     """Duct flow past a wall-mounted cube (512 x 256 x 256 fluid nodes, FP32 storage) on a
     structured box with the reference layout's BC lists: interpolated no-slip walls, interpolated
@@ -800,10 +869,12 @@ def main():
                     help="the headline's FP64 arithmetic. exact: every operation rounded as the reference's host "
                          "build (bitwise oracle parity); fast: FMA contraction and a rearranged K17")
     ap.add_argument("--kernel", default="auto", choices=["auto", "direct", "tma", "async", "pipe"])
-    ap.add_argument("--workload", default="tgv", choices=["tgv", "batch", "serving", "tgv-forms", "cube", "porous"],
+    ap.add_argument("--workload", default="tgv",
+                    choices=["tgv", "batch", "serving", "tgv-forms", "cube", "porous", "tgv-slab"],
                     help="tgv: the headline (TGV 256^3 FP64); batch: 4096 ducts in one domain pool; "
                          "serving: a Poisson stream of porous-block solves; tgv-forms: storage-form accuracy; "
-                         "cube: duct past a wall-mounted cube; porous: the serving pool's step on fixed blocks")
+                         "cube: duct past a wall-mounted cube; porous: the serving pool's step on fixed blocks; "
+                         "tgv-slab: the TGV as one domain in z slabs over the GPUs (NCCL halo exchange)")
     ap.add_argument("--form-steps", type=int, default=10000)
     ap.add_argument("--tgv-forms", default="f64,f32,f16,bf16",
                     help="tgv-forms: comma-separated storage[:arith] forms, the first the FP64 reference")
@@ -834,6 +905,9 @@ def main():
         return
     if args.workload == "porous":
         run_porous(args)
+        return
+    if args.workload == "tgv-slab":
+        run_tgv_slab(args)
         return
 
     run_tgv(args)

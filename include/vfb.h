@@ -407,6 +407,14 @@ int vfb_box_kernel_launches(const vfb_box *box, uint64_t *count);
 int vfb_box_set_launch_shape(vfb_box *box, int32_t blocks_per_sm, int32_t smem_kb);
 /* raw access to the population planes for checks: pointer, plane pitch (elements), parity */
 int vfb_box_populations(const vfb_box *box, void **dist, uint64_t *pitch, int32_t *is_even);
+/* A time step in parts, for drivers that overlap work with the collision (no counterpart in the
+   reference, whose CollisionAndExchange_streams splits the step by node lists instead,
+   Calculation/CollisisionStrategy.cpp:100-135): vfb_box_collide_planes collides the box's planes
+   z in [z_begin, z_end) at its current parity (direct-load kernel, the box's mask respected; no BC
+   lists, no energy), on `stream`; vfb_box_toggle_parity ends the step. A step is the planes in any
+   order and any split, then one toggle: every slot is read and written by one node per step. */
+int vfb_box_collide_planes(vfb_box *box, int32_t z_begin, int32_t z_end, void *stream);
+int vfb_box_toggle_parity(vfb_box *box);
 /* the 27 population planes without their padding (plane d at d * nx*ny*nz, the storage type, as
    stored) and the parity, out of or into the box: restart files (RestartObject::serialize /
    deserialize). Host memory when to_host / from_host (the call then synchronises the stream). */

@@ -214,6 +214,8 @@ SIGNATURES = {
     "vfb_box_set_drag_lift": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
     "vfb_box_kernel_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     "vfb_box_set_launch_shape": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+    "vfb_box_collide_planes": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]),
+    "vfb_box_toggle_parity": (C.c_int, [C.c_void_p]),
     "vfb_box_populations": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64),
                                       C.POINTER(C.c_int32)]),
     "vfb_pool_create": (C.c_int, [C.POINTER(PoolDesc), C.POINTER(C.c_void_p)]),

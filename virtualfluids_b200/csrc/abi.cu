@@ -1900,6 +1900,28 @@ int vfb_box_write_populations(vfb_box *box, const void *src, int32_t from_host, 
     return st;
 }
 
+int vfb_box_collide_planes(vfb_box *box, int32_t z_begin, int32_t z_end, void *stream)
+{
+    if (!box)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL box");
+    if (z_begin < 0 || z_end > box->desc.nz || z_begin > z_end)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "planes must satisfy 0 <= z_begin <= z_end <= nz");
+    const cudaError_t e = VFB_DISPATCH(box->desc.storage, box->desc.arith,
+                                       LA::box_collide_planes(box->state, box->even, z_begin, z_end, as_stream(stream)));
+    if (z_end > z_begin)
+        ++box->launches;
+    return cuda_status(e, "box collision of planes");
+}
+
+int vfb_box_toggle_parity(vfb_box *box)
+{
+    if (!box)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL box");
+    box->even = !box->even;
+    ++box->steps;
+    return VFB_OK;
+}
+
 int vfb_box_populations(const vfb_box *box, void **dist, uint64_t *pitch, int32_t *is_even)
 {
     if (!box || !dist || !pitch || !is_even)

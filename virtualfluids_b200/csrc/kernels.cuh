@@ -76,6 +76,7 @@ struct BoxCollideArgs {
     C fx, fy, fz;
     double *energy_partials;    // optional: per block {sum(1+drho), sum(0.5 (1+drho) u^2)}
     C *rho, *vx, *vy, *vz;      // optional macroscopic outputs
+    int z_begin;                // the direct kernel collides planes z_begin + blockIdx.z (0: the whole box)
 };
 
 // where a node's eight slot nodes are: from the neighbour lists (reference layout), or, when
@@ -368,7 +369,7 @@ __global__ void __launch_bounds__(128, box_min_blocks<S>()) k17_box_kernel(BoxCo
     using C = typename Codec<S>::compute;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
-    const int z = blockIdx.z;
+    const int z = blockIdx.z + a.z_begin;
     const bool active_x = x < a.nx;
     const uint64_t row = (uint64_t)a.nx * ((uint64_t)y + (uint64_t)a.ny * (uint64_t)z);
     const uint32_t k = (uint32_t)(row + (uint64_t)x);

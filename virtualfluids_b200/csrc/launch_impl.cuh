@@ -523,6 +523,7 @@ BoxCollideArgs<C> box_args(const BoxState &b)
     a.fz = (C)b.fz;
     a.energy_partials = nullptr;
     a.rho = a.vx = a.vy = a.vz = nullptr;
+    a.z_begin = 0;
     return a;
 }
 inline dim3 box_grid(const BoxState &b)
@@ -777,6 +778,30 @@ cudaError_t Launchers<S>::bounds_error(uint64_t *record)
     *record = 0;
     return cudaSuccess;
 #endif
+}
+
+// the direct collision kernel over the planes [z0, z1) only (no energy, no macroscopic output): a
+// time step split into parts, e.g. the border planes of a slab before its interior
+template <class S>
+cudaError_t Launchers<S>::box_collide_planes(const BoxState &b, bool even, int z0, int z1, cudaStream_t s)
+{
+    using C = typename Codec<S>::compute;
+    if (z1 <= z0)
+        return cudaSuccess;
+    BoxCollideArgs<C> a = box_args<C>(b);
+    a.z_begin = z0;
+    dim3 G = box_grid(b);
+    G.z = (unsigned)(z1 - z0);
+    const dim3 B(box_block_x(b.nx));
+    const bool mask = b.mask != nullptr;
+    if (even) {
+        if (mask) k17_box_kernel<S, VFB_EXACT, true, true, false, false><<<G, B, 0, s>>>(a);
+        else k17_box_kernel<S, VFB_EXACT, true, false, false, false><<<G, B, 0, s>>>(a);
+    } else {
+        if (mask) k17_box_kernel<S, VFB_EXACT, false, true, false, false><<<G, B, 0, s>>>(a);
+        else k17_box_kernel<S, VFB_EXACT, false, false, false, false><<<G, B, 0, s>>>(a);
+    }
+    return cudaGetLastError();
 }
 
 template <class S>
