@@ -51,7 +51,8 @@ BYTES_PER_NODE = {"f64": 432, "f32": 216, "f16": 108, "bf16": 108}
 # DRAM bytes (read + write) per node of one launch of the FP64 direct-load collision kernel of each
 # arithmetic, from one ncu capture at 128^3 (2,097,152 nodes); traffic grows with the node count,
 # so it is scaled to the bench's box
-NCU_DRAM_BYTES_PER_NODE_F64 = {"fast": (453.033728e6 + 395.824384e6) / 2097152, "exact": None}
+NCU_DRAM_BYTES_PER_NODE_F64 = {"fast": (453.033728e6 + 395.824384e6) / 2097152,
+                               "exact": (453.048832e6 + 395.543040e6) / 2097152}
 # launches averaged for the roofline figure, whatever --steps is (a sustained, not a burst, figure)
 ROOFLINE_LAUNCHES = 200
 # most timed steps of the reference arm (CPU, about 0.3 s per 256^3 step on 16 cores)
