@@ -55,8 +55,10 @@ typedef enum vfb_storage {
 
 /* rounding mode of the arithmetic */
 typedef enum vfb_arith {
-    VFB_ARITH_FAST = 0,    /* products contracted into FMAs (default) */
-    VFB_ARITH_EXACT = 1    /* every operation rounded separately, as the reference built without FMA */
+    VFB_ARITH_FAST = 0,    /* products contracted into FMAs (the Python classes' default) */
+    VFB_ARITH_EXACT = 1    /* every operation rounded separately, as the reference built without FMA
+                              (the reference-side adapter's default): bit for bit the reference's
+                              host arithmetic */
 } vfb_arith;
 
 /* CollisionTemplate (src/gpu/core/Calculation/Calculation.h:55-67) */
