@@ -481,7 +481,10 @@ __host__ __device__ __forceinline__ float fast_rcp<float>(float x)
 // transforms, and the backward transform puts back j' = rho u + (the negated first central moment
 // rho (j/rho - u)), so any error in u changes the node's momentum by twice that error times rho.
 // A reciprocal that errs to one side (an approximate one) therefore makes the momentum drift step
-// after step; a correctly rounded one errs both ways equally often.
+// after step; a correctly rounded one errs both ways equally often. In float the rounded
+// reciprocal flushes subnormals (rcp.rn.ftz): rho is near 1, so the bits are those of the IEEE
+// reciprocal, and the form without flushing carries a slow path whose call raised the 16-bit
+// pool kernel from 128 to 172 registers.
 template <class T>
 __host__ __device__ __forceinline__ T rho_rcp(T x)
 {
@@ -491,7 +494,9 @@ template <>
 __host__ __device__ __forceinline__ float rho_rcp<float>(float x)
 {
 #ifdef __CUDA_ARCH__
-    return __frcp_rn(x);
+    float y;
+    asm("rcp.rn.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
 #else
     return 1.0f / x;
 #endif

@@ -1704,9 +1704,46 @@ struct PoolArgs {
     int nodes_per_thread;
 };
 
+// What the collision of a pool domain's nodes needs of its record, read once per work item into
+// the block's shared memory: the stores of the node loop may alias the record's global memory as
+// far as the compiler can tell, so fields read through a reference to it are loaded again from
+// global memory for every node (held in registers instead, they would cost occupancy).
+template <class C>
+struct PoolNodeCtx {
+    uint64_t pitch;
+    int nx, ny, nz, flags;
+    FastDiv div_nx, div_ny;
+    K17Rates<C> rates;
+    C fx, fy, fz;
+};
+template <class C>
+__device__ __forceinline__ PoolNodeCtx<C> load_pool_ctx(const PoolDomain<C> *p)
+{
+    PoolNodeCtx<C> c;
+    c.pitch = __ldg(&p->pitch);
+    c.nx = __ldg(&p->nx);
+    c.ny = __ldg(&p->ny);
+    c.nz = __ldg(&p->nz);
+    c.flags = __ldg(&p->flags);
+    c.div_nx.m = __ldg(&p->div_nx.m);
+    c.div_nx.shift = __ldg(&p->div_nx.shift);
+    c.div_ny.m = __ldg(&p->div_ny.m);
+    c.div_ny.shift = __ldg(&p->div_ny.shift);
+    static_assert(sizeof(K17Rates<C>) % sizeof(C) == 0, "K17Rates holds values of its type only");
+    const C *src = reinterpret_cast<const C *>(&p->rates);
+    C *dst = reinterpret_cast<C *>(&c.rates);
+#pragma unroll
+    for (int i = 0; i < (int)(sizeof(K17Rates<C>) / sizeof(C)); ++i)
+        dst[i] = __ldg(src + i);
+    c.fx = __ldg(&p->fx);
+    c.fy = __ldg(&p->fy);
+    c.fz = __ldg(&p->fz);
+    return c;
+}
+
 // one node of a pool domain: its slots, the K17 collision and the ET scatter
 template <class S, bool EXACT, bool EVEN>
-__device__ __forceinline__ void pool_collide_node(S *base, const PoolDomain<typename Codec<S>::compute> &dm, uint32_t k)
+__device__ __forceinline__ void pool_collide_node(S *base, const PoolNodeCtx<typename Codec<S>::compute> &dm, uint32_t k)
 {
     using C = typename Codec<S>::compute;
     const int nx = dm.nx, ny = dm.ny, nz = dm.nz, flags = dm.flags;
@@ -1741,22 +1778,34 @@ __device__ __forceinline__ void pool_collide_node(S *base, const PoolDomain<type
 // queues the fluid nodes of its segments in shared memory (a ballot per segment, in node order)
 // and collides them 32 at a time, so lanes are not left idle on solid nodes. Each node's arithmetic
 // is the same either way.
+// two resident blocks of 256 threads (or four of 128) for the FP32-arithmetic forms: at most 128
+// registers, the budget every FP32 collision fits without spills; FP64 takes what it needs
+template <class S>
+constexpr int pool_min_blocks() { return sizeof(typename Codec<S>::compute) == 8 ? 1 : 2; }
+
 template <class S, bool EXACT, bool EVEN>
-__global__ void __launch_bounds__(256) k17_pool_kernel(PoolArgs<typename Codec<S>::compute> a)
+__global__ void __launch_bounds__(256, pool_min_blocks<S>()) k17_pool_kernel(PoolArgs<typename Codec<S>::compute> a)
 {
     using C = typename Codec<S>::compute;
     __shared__ uint32_t queue[8][64];
+    __shared__ PoolNodeCtx<C> ctx;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t lanes_below = (1u << lane) - 1u;
     const uint32_t n_items = __ldg(a.n_items);
     const uint32_t span = blockDim.x * (uint32_t)a.nodes_per_thread;
     for (uint32_t w = blockIdx.x; w < n_items; w += gridDim.x) {
         const uint2 it = a.items[w];
-        const PoolDomain<C> &dm = a.domains[it.x];
+        const PoolDomain<C> *dp = a.domains + it.x;
+        __syncthreads();                 // every thread is done with the previous item's record
+        if (threadIdx.x == 0)
+            ctx = load_pool_ctx(dp);
+        __syncthreads();
+        const PoolNodeCtx<C> &dm = ctx;
         const uint32_t nodes_total = (uint32_t)dm.nx * (uint32_t)dm.ny * (uint32_t)dm.nz;
-        S *base = static_cast<S *>(a.arena) + dm.dist_offset;
+        S *base = static_cast<S *>(a.arena) + __ldg(&dp->dist_offset);
         const uint32_t end = min(it.y + span, nodes_total);
-        const uint8_t *mask = (dm.flags & kPoolMask) ? static_cast<const uint8_t *>(a.arena) + dm.mask_offset : nullptr;
+        const uint8_t *mask =
+            (dm.flags & kPoolMask) ? static_cast<const uint8_t *>(a.arena) + __ldg(&dp->mask_offset) : nullptr;
         if (!(dm.flags & kPoolCompact)) {
 #pragma unroll 1
             for (uint32_t k = it.y + threadIdx.x; k < end; k += blockDim.x) {
