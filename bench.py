@@ -460,6 +460,91 @@ def run_batch(args):
         print(json.dumps(line), flush=True)
 
 
+def run_pool_shapes(args):
+    """The pool kernel against the box kernel on the same node counts: one pool each for one
+    periodic 256^3 domain, 64 periodic 64^3 domains, the shapes of 1024 ducts with every node
+    fluid, and the same ducts with their walls; then a Box of 256^3. FP32 and FP16 storage, the
+    pool's default launch shape (128 threads x 4 nodes, resident blocks from the occupancy API),
+    graph replay, CUDA events on the pool's stream. MLUPS count fluid nodes."""
+    import torch
+
+    import virtualfluids_b200 as vfb
+    from virtualfluids_b200 import Pool
+    from virtualfluids_b200.workloads import duct_batch
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+
+    def duct_mask(nx, ny, nz):
+        m = np.ones((nz, ny, nx), dtype=np.uint8)
+        m[0] = m[-1] = 0
+        m[:, 0] = m[:, -1] = 0
+        return m.reshape(-1)
+
+    def time_pool(shapes, walls, storage):
+        periodic = (True, False, False) if walls else (True, True, True)
+        probe = Pool(1 << 20, storage=storage, max_domains=1)
+        need = sum(probe.domain_bytes(s, 1.8, periodic=periodic, has_mask=walls) for s in shapes)
+        probe.close()
+        pool = Pool(need + (1 << 20), storage=storage, max_domains=len(shapes))
+        for s in shapes:
+            i = pool.add(s, 1.8, periodic=periodic, mask=duct_mask(*s) if walls else None)
+            pool.init(i, stream=stream)
+        pool.set_launch(128, 4, 0, True)
+        pool.step(args.warmup, stream=stream)
+        stream.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        pool.step(args.steps, stream=stream)
+        ev1.record(stream)
+        stream.synchronize()
+        pool.close()
+        return ev0.elapsed_time(ev1) / args.steps
+
+    specs = duct_batch(1024)
+    ducts = [d["shape"] for d in specs]
+    cases = [("one periodic 256^3 domain", [(256, 256, 256)], False, 256 ** 3),
+             ("64 periodic 64^3 domains", [(64, 64, 64)] * 64, False, 64 * 64 ** 3),
+             ("1024 duct shapes, every node fluid", ducts, False, int(sum(np.prod(s) for s in ducts))),
+             ("1024 ducts with walls", ducts, True, int(sum(d["fluid_nodes"] for d in specs)))]
+    out = {}
+    for storage in ("f32", "f16"):
+        res = {}
+        for name, shapes, walls, fluid in cases:
+            ms = time_pool(shapes, walls, storage)
+            res["pool: " + name] = {"ms_per_step": round(ms, 4), "mlups": round(fluid / (ms / 1e3) / 1e6, 1)}
+        n = 256
+        sp = C.c_void_p(stream.cuda_stream)
+        b = vfb.Box(n, n, n, 1.8, storage=storage)
+        z = torch.zeros(n ** 3, dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        b.init(z, z, z, z, stream=sp)
+        b.step(args.warmup, stream=sp)
+        stream.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        b.step(args.steps, stream=sp)
+        ev1.record(stream)
+        stream.synchronize()
+        ms = ev0.elapsed_time(ev1) / args.steps
+        res["box 256^3"] = {"ms_per_step": round(ms, 4), "mlups": round(n ** 3 / (ms / 1e3) / 1e6, 1)}
+        del b
+        torch.cuda.empty_cache()
+        out[storage] = res
+    if rank == 0:
+        line = {"metric": "MLUPS of the pool kernel on one 256^3 domain (FP32 storage)",
+                "value": out["f32"]["pool: one periodic 256^3 domain"]["mlups"], "unit": "MLUPS",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": out["f32"]["pool: one periodic 256^3 domain"]["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": "pool kernel vs box kernel on the same shapes, fluid at rest, omega 1.8",
+                           "l2": "inputs larger than L2, no flush"},
+                "forms": out}
+        print(json.dumps(line), flush=True)
+
+
 def run_tgv_slab(args):
     """The headline's TGV 256^3 box as ONE domain split into z slabs over the ranks (one process per
     GPU): every step collides each slab's two border planes, exchanges the border planes with the
@@ -871,11 +956,12 @@ def main():
                          "build (bitwise oracle parity); fast: FMA contraction and a rearranged K17")
     ap.add_argument("--kernel", default="auto", choices=["auto", "direct", "tma", "async", "pipe"])
     ap.add_argument("--workload", default="tgv",
-                    choices=["tgv", "batch", "serving", "tgv-forms", "cube", "porous", "tgv-slab"],
+                    choices=["tgv", "batch", "serving", "tgv-forms", "cube", "porous", "tgv-slab", "pool-shapes"],
                     help="tgv: the headline (TGV 256^3 FP64); batch: 4096 ducts in one domain pool; "
                          "serving: a Poisson stream of porous-block solves; tgv-forms: storage-form accuracy; "
                          "cube: duct past a wall-mounted cube; porous: the serving pool's step on fixed blocks; "
-                         "tgv-slab: the TGV as one domain in z slabs over the GPUs (NCCL halo exchange)")
+                         "tgv-slab: the TGV as one domain in z slabs over the GPUs (NCCL halo exchange); "
+                         "pool-shapes: the pool kernel against the box kernel on the same shapes")
     ap.add_argument("--form-steps", type=int, default=10000)
     ap.add_argument("--tgv-forms", default="f64,f32,f16,bf16",
                     help="tgv-forms: comma-separated storage[:arith] forms, the first the FP64 reference")
@@ -909,6 +995,9 @@ def main():
         return
     if args.workload == "tgv-slab":
         run_tgv_slab(args)
+        return
+    if args.workload == "pool-shapes":
+        run_pool_shapes(args)
         return
 
     run_tgv(args)
