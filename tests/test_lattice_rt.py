@@ -2,7 +2,9 @@
 masks, shift_class_rt, order_rt, weight_rt, cdot_link) against the compile-time lattice
 functions of the unrolled kernels. The check compiles tests/lattice_rt_check.cu as host code with
 nvcc and runs it on the CPU; results must agree bit for bit, so a kernel that picks a direction at
-run time computes what the unrolled kernels compute."""
+run time computes what the unrolled kernels compute. It also checks the esoteric-twist plane map
+and the direction numbering against the known answers of the reference's KernelUtilitiesTests.cpp
+(getDistributionReferences27 on even and odd steps)."""
 import shutil
 import subprocess
 from pathlib import Path

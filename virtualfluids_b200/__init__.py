@@ -14,9 +14,10 @@ from ._native import VfbError, lib
 from .box import Box
 from .grid import Interface, ListGrid, MultiLevelGrid, refine_box
 from .pool import Pool
-from .simulation import (BoundaryConditionFactory, GridScalingFactory, InterpolationCells, Parameter, Simulation,
-                         scale_coarse_to_fine, scale_fine_to_coarse)
+from .simulation import (BoundaryConditionFactory, GridScalingFactory, InterpolationCells, K17ParameterWarning,
+                         Parameter, Simulation, scale_coarse_to_fine, scale_fine_to_coarse)
 
-__all__ = ["Box", "BoundaryConditionFactory", "GridScalingFactory", "Interface", "InterpolationCells", "ListGrid",
+__all__ = ["Box", "BoundaryConditionFactory", "GridScalingFactory", "Interface", "InterpolationCells",
+           "K17ParameterWarning", "ListGrid",
            "MultiLevelGrid", "Parameter", "Pool", "Simulation", "VfbError", "lib", "refine_box", "scale_coarse_to_fine",
            "scale_fine_to_coarse", "_native"]

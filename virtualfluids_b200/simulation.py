@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import ctypes as C
 import enum
+import warnings
 
 import numpy as np
 
@@ -84,6 +85,34 @@ class Parameter:
     def omega_of_level(self, level: int) -> float:
         """omega of a refinement level: nu 2^level in that level's units (Parameter.cpp:404-406)."""
         return 1.0 / (3.0 * (self.viscosity_lb * 2.0 ** level) + 0.5)
+
+    # Parameter::checkParameterValidityCumulantK17 (Parameter.cpp:424-445): K17 with its
+    # 4th-order modified equilibrium is unstable above these values
+    K17_VISCOSITY_LIMIT = 1.0 / 42.0
+    K17_VELOCITY_LIMIT = 0.1
+
+    def check_parameter_validity_cumulant_k17(self, finest_level: int = 0) -> list:
+        """The reference's K17 checks: a warning (K17ParameterWarning) when the viscosity of the
+        finest level exceeds 1/42 or the velocity set by set_velocity_lb exceeds 0.1, nothing for
+        another main kernel. Simulation runs it once, as the reference's initLBMSimulationParameter
+        does. Returns the warning texts."""
+        if self.main_kernel != "K17CompressibleNavierStokes":
+            return []
+        out = []
+        nu = self.viscosity_lb * 2.0 ** finest_level
+        if nu > self.K17_VISCOSITY_LIMIT:
+            out.append(f"The viscosity (in LB units) at level {finest_level} is {nu:1.3g}. It is recommended to keep "
+                       f"it smaller than {self.K17_VISCOSITY_LIMIT:1.3g} for the CumulantK17 collision kernel.")
+        if self.velocity_lb > self.K17_VELOCITY_LIMIT:
+            out.append(f"The velocity (in LB units) is {self.velocity_lb:1.4g}. It is recommended to keep it smaller "
+                       f"than {self.K17_VELOCITY_LIMIT:1.4g} for the CumulantK17 collision kernel.")
+        for msg in out:
+            warnings.warn(msg, K17ParameterWarning, stacklevel=2)
+        return out
+
+
+class K17ParameterWarning(UserWarning):
+    """A K17 parameter outside the range the reference recommends (the reference logs a warning)."""
 
 
 class BoundaryConditionFactory:
@@ -294,6 +323,8 @@ class Simulation:
             raise N.VfbError(N.VFB_ERR_UNKNOWN_KERNEL, "no main kernel configured")
         t = _torch()
         self.para, self.bcf, self.device = para, bc_factory, device
+        finest = len(grid.levels) - 1 if hasattr(grid, "levels") else 0
+        para.check_parameter_validity_cumulant_k17(finest)
         # nested levels (MultiLevelGrid, or an imported gridgen.ImportedGrid), or a single level
         self.multilevel = grid if hasattr(grid, "interfaces") else MultiLevelGrid.uniform(grid)
         self.levels = [_LevelState(para, g, i, device) for i, g in enumerate(self.multilevel.levels)]
