@@ -47,7 +47,7 @@ sys.path.insert(0, str(ROOT))
 N_SIDE = 256
 U0 = 0.04
 RE = 1600.0
-BYTES_PER_NODE = {"f64": 432, "f32": 216, "f16": 108, "bf16": 108}
+BYTES_PER_NODE = {"f64": 432, "f32": 216, "f16": 108, "bf16": 108, "e3m12": 108}
 # DRAM bytes (read + write) per node of one launch of the FP64 direct-load collision kernel of each
 # arithmetic, from one ncu capture at 128^3 (2,097,152 nodes); traffic grows with the node count,
 # so it is scaled to the bench's box
@@ -963,7 +963,7 @@ def main():
                          "tgv-slab: the TGV as one domain in z slabs over the GPUs (NCCL halo exchange); "
                          "pool-shapes: the pool kernel against the box kernel on the same shapes")
     ap.add_argument("--form-steps", type=int, default=10000)
-    ap.add_argument("--tgv-forms", default="f64,f32,f16,bf16",
+    ap.add_argument("--tgv-forms", default="f64,f32,f16,bf16,e3m12",
                     help="tgv-forms: comma-separated storage[:arith] forms, the first the FP64 reference")
     ap.add_argument("--cube-dims", type=int, nargs=5, default=[512, 256, 256, 32, 128],
                     metavar=("NX", "NY", "NZ", "CUBE", "X0"))
@@ -1125,7 +1125,7 @@ def run_tgv(args):
         del ref
         torch.cuda.empty_cache()
         other = "f64_fast" if args.arith == "exact" else "f64_exact"
-        for name in (other, "f32", "f16", "bf16"):
+        for name in (other, "f32", "f16", "bf16", "e3m12"):
             st = "f64" if name.startswith("f64") else name
             ar = name[4:] if name.startswith("f64") else "fast"
             dt = np.float64 if st == "f64" else np.float32
@@ -1145,6 +1145,7 @@ def run_tgv(args):
         if "f16" in forms:
             forms["f16"]["speedup_vs_headline_kernel"] = round(k_ms / forms["f16"]["kernel_ms"], 3)
             forms["bf16"]["speedup_vs_headline_kernel"] = round(k_ms / forms["bf16"]["kernel_ms"], 3)
+            forms["e3m12"]["speedup_vs_headline_kernel"] = round(k_ms / forms["e3m12"]["kernel_ms"], 3)
 
     # ---- the reference layout: the drop-in step driver over neighborX/Y/Z lists (device resident) ----
     ref_layout = None

@@ -50,7 +50,10 @@ typedef enum vfb_storage {
     VFB_STORAGE_F64 = 0,   /* f - w in double, arithmetic in double */
     VFB_STORAGE_F32 = 1,   /* f - w in float, arithmetic in float */
     VFB_STORAGE_F16 = 2,   /* (f - w)/w in IEEE half, arithmetic in float */
-    VFB_STORAGE_BF16 = 3   /* (f - w)/w in bfloat16, arithmetic in float */
+    VFB_STORAGE_BF16 = 3,  /* (f - w)/w in bfloat16, arithmetic in float */
+    VFB_STORAGE_E3M12 = 4  /* (f - w)/w in a 16-bit float of 1 sign, 3 exponent, 12 significand bits
+                              (|values| < 2, subnormal steps of 2^-18, no infinity or NaN: out-of-range
+                              values saturate), arithmetic in float; no counterpart in the reference */
 } vfb_storage;
 
 /* rounding mode of the arithmetic */

@@ -60,7 +60,7 @@ def _alone(shape, periodic, omega, forces, storage, arith, seed, steps):
 
 
 @pytest.mark.parametrize("storage,arith", [("f64", "exact"), ("f64", "fast"), ("f32", "fast"), ("f16", "fast"),
-                                           ("bf16", "fast")])
+                                           ("bf16", "fast"), ("e3m12", "fast")])
 def test_pool_domains_match_boxes_alone_bitwise(cuda, storage, arith):
     steps = 37
     s = _stream()

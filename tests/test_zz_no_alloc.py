@@ -53,7 +53,8 @@ def _no_alloc(sim):
 
 @pytest.mark.parametrize("storage, arith", [
     (N.STORAGE_F64, N.ARITH_FAST), (N.STORAGE_F32, N.ARITH_FAST), (N.STORAGE_F16, N.ARITH_FAST),
-    (N.STORAGE_BF16, N.ARITH_FAST), (N.STORAGE_F64, N.ARITH_EXACT), (N.STORAGE_F32, N.ARITH_EXACT)])
+    (N.STORAGE_BF16, N.ARITH_FAST), (N.STORAGE_E3M12, N.ARITH_FAST), (N.STORAGE_F64, N.ARITH_EXACT),
+    (N.STORAGE_F32, N.ARITH_EXACT)])
 def test_no_alloc_reduction_matches_workspace_reduction_twice(cuda, storage, arith):
     sim = _cavity_simulation(storage=storage, arith=arith)
     sim.run(30)

@@ -23,7 +23,7 @@ VFB_ERR_OUT_OF_MEMORY = 6
 VFB_ERR_UNSUPPORTED = 7
 VFB_ERR_WATCHDOG = 8
 
-STORAGE_F64, STORAGE_F32, STORAGE_F16, STORAGE_BF16 = 0, 1, 2, 3
+STORAGE_F64, STORAGE_F32, STORAGE_F16, STORAGE_BF16, STORAGE_E3M12 = 0, 1, 2, 3, 4
 ARITH_FAST, ARITH_EXACT = 0, 1
 
 COLLISION_DEFAULT = 0

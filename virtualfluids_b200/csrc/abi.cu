@@ -33,7 +33,7 @@ int cuda_status(cudaError_t e, const char *what)
 
 inline cudaStream_t as_stream(void *s) { return static_cast<cudaStream_t>(s); }
 
-bool storage_ok(int s) { return s >= VFB_STORAGE_F64 && s <= VFB_STORAGE_BF16; }
+bool storage_ok(int s) { return s >= VFB_STORAGE_F64 && s <= VFB_STORAGE_E3M12; }
 size_t storage_bytes(int s) { return s == VFB_STORAGE_F64 ? 8 : s == VFB_STORAGE_F32 ? 4 : 2; }
 size_t real_bytes(int s) { return s == VFB_STORAGE_F64 ? 8 : 4; }
 
@@ -71,6 +71,7 @@ int check_level(const vfb_level *L)
         case VFB_STORAGE_F32: { using LA = vfb::fast::Launchers<float>; return CALL; }                                  \
         case VFB_STORAGE_F16: { using LA = vfb::fast::Launchers<__half>; return CALL; }                                 \
         case VFB_STORAGE_BF16: { using LA = vfb::fast::Launchers<__nv_bfloat16>; return CALL; }                         \
+        case VFB_STORAGE_E3M12: { using LA = vfb::fast::Launchers<vfb::e3m12_t>; return CALL; }                         \
         default: return cudaErrorInvalidValue;                                                                         \
         }                                                                                                              \
     }()
@@ -248,13 +249,14 @@ int vfb_bounds_check_status(uint64_t *bad_index, uint64_t *node_count)
     return fail(VFB_ERR_UNSUPPORTED, "this library is built without bounds checks (libvfb_checked.so has them)");
 #else
     cudaError_t e = cudaDeviceSynchronize();
-    uint64_t recs[6] = {};
+    uint64_t recs[7] = {};
     if (e == cudaSuccess) e = vfb::exact::Launchers<double>::bounds_error(&recs[0]);
     if (e == cudaSuccess) e = vfb::exact::Launchers<float>::bounds_error(&recs[1]);
     if (e == cudaSuccess) e = vfb::fast::Launchers<double>::bounds_error(&recs[2]);
     if (e == cudaSuccess) e = vfb::fast::Launchers<float>::bounds_error(&recs[3]);
     if (e == cudaSuccess) e = vfb::fast::Launchers<__half>::bounds_error(&recs[4]);
     if (e == cudaSuccess) e = vfb::fast::Launchers<__nv_bfloat16>::bounds_error(&recs[5]);
+    if (e == cudaSuccess) e = vfb::fast::Launchers<vfb::e3m12_t>::bounds_error(&recs[6]);
     if (e != cudaSuccess)
         return cuda_status(e, "bounds-check record");
     for (uint64_t r : recs)
@@ -1634,7 +1636,8 @@ int vfb_box_set_kernel_variant(vfb_box *box, int32_t variant)
                                               "3 (per-thread async copies), 4 (packed FP32x2 pairs) or 5 "
                                               "(persistent, next node's loads in flight)");
     if (variant == 4 && (box->desc.storage == VFB_STORAGE_F64 || box->desc.arith == VFB_ARITH_EXACT))
-        return fail(VFB_ERR_UNSUPPORTED, "packed FP32x2 pairs: FP32 arithmetic (F32, F16, BF16 storage), FMA variant");
+        return fail(VFB_ERR_UNSUPPORTED, "packed FP32x2 pairs: FP32 arithmetic (F32, F16, BF16, E3M12 storage), FMA "
+                                         "variant");
     if (variant == 3 && box->desc.storage > VFB_STORAGE_F32)
         return fail(VFB_ERR_UNSUPPORTED, "per-thread async copies move 4 or 8 bytes: F64 and F32 storage only");
     if (variant == 2 && box->desc.nx % 32 != 0)

@@ -14,6 +14,10 @@
 #include "vfb.h"
 
 namespace vfb {
+struct e3m12_t; // the E3M12 storage element (storage.cuh)
+}
+
+namespace vfb {
 
 // a structured box as the kernels see it
 struct BoxState {

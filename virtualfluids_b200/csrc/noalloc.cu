@@ -87,6 +87,9 @@ int vfb_mass_energy_no_alloc(const vfb_level *level, const uint32_t *node_indice
         case VFB_STORAGE_F64: e = vfb::fast::Launchers<double>::energy_list(level, node_indices, size, partials, s); break;
         case VFB_STORAGE_F32: e = vfb::fast::Launchers<float>::energy_list(level, node_indices, size, partials, s); break;
         case VFB_STORAGE_F16: e = vfb::fast::Launchers<__half>::energy_list(level, node_indices, size, partials, s); break;
+        case VFB_STORAGE_E3M12:
+            e = vfb::fast::Launchers<vfb::e3m12_t>::energy_list(level, node_indices, size, partials, s);
+            break;
         default: e = vfb::fast::Launchers<__nv_bfloat16>::energy_list(level, node_indices, size, partials, s); break;
         }
     }

@@ -75,6 +75,7 @@ bool select_ops(int storage, int arith, PoolOps &out)
     case VFB_STORAGE_F32: out = ops_of<vfb::fast::Launchers<float>>(); return true;
     case VFB_STORAGE_F16: out = ops_of<vfb::fast::Launchers<__half>>(); return true;
     case VFB_STORAGE_BF16: out = ops_of<vfb::fast::Launchers<__nv_bfloat16>>(); return true;
+    case VFB_STORAGE_E3M12: out = ops_of<vfb::fast::Launchers<vfb::e3m12_t>>(); return true;
     default: return false;
     }
 }

@@ -14,7 +14,8 @@ import numpy as np
 
 from . import _native as N
 
-_STORAGE = {"f64": N.STORAGE_F64, "f32": N.STORAGE_F32, "f16": N.STORAGE_F16, "bf16": N.STORAGE_BF16}
+_STORAGE = {"f64": N.STORAGE_F64, "f32": N.STORAGE_F32, "f16": N.STORAGE_F16, "bf16": N.STORAGE_BF16,
+            "e3m12": N.STORAGE_E3M12}
 
 
 def _stream_ptr(stream):

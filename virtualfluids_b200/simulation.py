@@ -24,7 +24,8 @@ import numpy as np
 from . import _native as N
 from .grid import ListGrid, MultiLevelGrid
 
-STORAGE = {"f64": N.STORAGE_F64, "f32": N.STORAGE_F32, "f16": N.STORAGE_F16, "bf16": N.STORAGE_BF16}
+STORAGE = {"f64": N.STORAGE_F64, "f32": N.STORAGE_F32, "f16": N.STORAGE_F16, "bf16": N.STORAGE_BF16,
+           "e3m12": N.STORAGE_E3M12}
 
 
 def _torch():
@@ -34,7 +35,8 @@ def _torch():
 
 def storage_dtype(storage: int):
     t = _torch()
-    return {N.STORAGE_F64: t.float64, N.STORAGE_F32: t.float32, N.STORAGE_F16: t.float16, N.STORAGE_BF16: t.bfloat16}[storage]
+    return {N.STORAGE_F64: t.float64, N.STORAGE_F32: t.float32, N.STORAGE_F16: t.float16, N.STORAGE_BF16: t.bfloat16,
+            N.STORAGE_E3M12: t.int16}[storage]
 
 
 def real_dtype(storage: int):
@@ -446,7 +448,12 @@ class Simulation:
         return np.concatenate([h[start:], h[:start]])
 
     def populations(self, level=0):
+        """The population array of a level as float64 values: f - w for F64 / F32 storage, (f - w)/w
+        for the 16-bit forms (E3M12 decoded)."""
         N.check(N.lib().vfb_synchronize(None))
+        if self.para.storage == N.STORAGE_E3M12:
+            from .formats import decode
+            return decode(self._raw(level))
         return self.levels[level].dist.double().cpu().numpy()
 
     def _raw(self, level):
@@ -454,7 +461,7 @@ class Simulation:
         t = _torch()
         N.check(N.lib().vfb_synchronize(None))
         d = self.levels[level].dist
-        if d.dtype in (t.float16, t.bfloat16):
+        if d.dtype in (t.float16, t.bfloat16, t.int16):
             return d.view(t.int16).cpu().numpy().view(np.uint16)
         return d.cpu().numpy()
 

@@ -90,7 +90,8 @@ class Slab:
         dist, pitch, even = C.c_void_p(), C.c_uint64(), C.c_int32()
         N.check(N.lib().vfb_box_populations(self.box._h, C.byref(dist), C.byref(pitch), C.byref(even)))
         dt = {N.STORAGE_F64: (torch.float64, "<f8"), N.STORAGE_F32: (torch.float32, "<f4"),
-              N.STORAGE_F16: (torch.float16, "<f2"), N.STORAGE_BF16: (torch.int16, "<i2")}[self.box.storage]
+              N.STORAGE_F16: (torch.float16, "<f2"), N.STORAGE_BF16: (torch.int16, "<i2"),
+              N.STORAGE_E3M12: (torch.int16, "<i2")}[self.box.storage]
         # the population array as a (27, pitch) tensor on the device, aliasing the box's memory
         self.f = torch.as_tensor(_Device(dist.value, (27, pitch.value), dt[1]), device="cuda")
         if dt[0] == torch.int16:
