@@ -345,6 +345,23 @@ int vfb_simulation_check(const vfb_simulation *sim);
    parity toggle, drag/lift, pressure BCs. A level with a finer one lets that one take two steps
    first and after its own step interpolates fine to coarse, then coarse to fine. */
 int vfb_simulation_run(vfb_simulation *sim, uint32_t steps, void *stream);
+
+/* Phase timers (Output/TimeStepTimer.h: the reference's collision, post- and pre-collision BC
+   timers, here with the two interpolation directions). Every phase of a run is an NVTX range of
+   the phase's name (visible to ncu --nvtx and other NVTX tools). With timing on, each phase is also
+   bracketed by CUDA events on the run's stream, and vfb_simulation_run synchronises that stream
+   once at its end to add the device times up; phase_times returns the sums in milliseconds, over
+   all levels, and the coarse steps they cover (reset != 0 clears them). Off by default. */
+enum {
+    VFB_PHASE_COLLISION = 0,
+    VFB_PHASE_POST_COLLISION_BC = 1,   /* velocity, no-slip, geometry BCs and the drag's post part */
+    VFB_PHASE_PRE_COLLISION_BC = 2,    /* the drag's pre part and sum, pressure BCs */
+    VFB_PHASE_SCALING_FC = 3,
+    VFB_PHASE_SCALING_CF = 4,
+    VFB_PHASES = 5
+};
+int vfb_simulation_set_timing(vfb_simulation *sim, int32_t on);
+int vfb_simulation_phase_times(vfb_simulation *sim, double *ms, uint64_t *steps, int32_t reset);
 /* parity of the coarsest level / of a given level */
 int vfb_simulation_is_even_timestep(const vfb_simulation *sim, int32_t *is_even);
 int vfb_simulation_level_is_even_timestep(const vfb_simulation *sim, int32_t level, int32_t *is_even);

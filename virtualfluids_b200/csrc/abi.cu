@@ -1,6 +1,7 @@
 // C ABI of the library (include/vfb.h): argument checks, dispatch on storage and arithmetic,
 // the kernel and boundary-condition registries, the step driver and structured boxes.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cstdio>
@@ -768,6 +769,97 @@ struct SimLevel {
 };
 } // namespace
 
+// Phase timers of the step driver, in the phases of the reference's TimeStepTimer
+// (Output/TimeStepTimer.h: collision, post- and pre-collision BCs) plus the two interpolation
+// directions. With timing on, each phase of a run is bracketed by CUDA events on the run's stream;
+// the run synchronises once at its end and adds the elapsed times up. The events are reused.
+struct PhaseTimers {
+    bool on = false;
+    double ms[VFB_PHASES] = {};
+    uint64_t steps = 0;
+    std::vector<cudaEvent_t> free_events;
+    struct Pending {
+        int phase;
+        cudaEvent_t start, stop;
+    };
+    std::vector<Pending> pending;
+    cudaEvent_t take()
+    {
+        if (!free_events.empty()) {
+            cudaEvent_t e = free_events.back();
+            free_events.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        return e;
+    }
+    // add up the pending phases (the caller has synchronised their stream)
+    cudaError_t collect()
+    {
+        cudaError_t err = cudaSuccess;
+        for (const Pending &p : pending) {
+            float t = 0.0f;
+            const cudaError_t e = cudaEventElapsedTime(&t, p.start, p.stop);
+            if (e == cudaSuccess)
+                ms[p.phase] += t;
+            else if (err == cudaSuccess)
+                err = e;
+            free_events.push_back(p.start);
+            free_events.push_back(p.stop);
+        }
+        pending.clear();
+        return err;
+    }
+    ~PhaseTimers()
+    {
+        for (const Pending &p : pending) {
+            cudaEventDestroy(p.start);
+            cudaEventDestroy(p.stop);
+        }
+        for (cudaEvent_t e : free_events)
+            cudaEventDestroy(e);
+    }
+};
+
+const char *const kPhaseNames[VFB_PHASES] = { "collision", "postCollisionBC", "preCollisionBC", "scalingFineToCoarse",
+                                              "scalingCoarseToFine" };
+
+// an NVTX range of the phase's name and, with timing on, its two events
+class PhaseScope {
+public:
+    PhaseScope(PhaseTimers &t, int phase, void *stream) : t_(t), phase_(phase), stream_(static_cast<cudaStream_t>(stream))
+    {
+        nvtxRangePushA(kPhaseNames[phase]);
+        if (t_.on && (start_ = t_.take()) != nullptr)
+            cudaEventRecord(start_, stream_);
+    }
+    ~PhaseScope()
+    {
+        if (start_) {
+            cudaEvent_t stop = t_.take();
+            if (stop) {
+                cudaEventRecord(stop, stream_);
+                t_.pending.push_back({ phase_, start_, stop });
+            } else {
+                t_.free_events.push_back(start_);
+            }
+        }
+        nvtxRangePop();
+    }
+    PhaseScope(const PhaseScope &) = delete;
+    PhaseScope &operator=(const PhaseScope &) = delete;
+
+private:
+    PhaseTimers &t_;
+    int phase_;
+    cudaStream_t stream_;
+    cudaEvent_t start_ = nullptr;
+};
+
 struct vfb_simulation {
     int kernel_id = 0;
     std::vector<SimLevel> levels = std::vector<SimLevel>(1);
@@ -776,6 +868,7 @@ struct vfb_simulation {
     bool scaling_set = false;         // GridScalingFactory given
     vfb_scaling_fn scale_fc = nullptr;
     vfb_scaling_fn scale_cf = nullptr;
+    PhaseTimers timers;
 };
 
 static SimLevel &current(vfb_simulation *sim) { return sim->levels[(size_t)sim->cursor]; }
@@ -1176,10 +1269,12 @@ static int run_geometry_pre(SimLevel &S, void *stream)
 
 // one time step of one level: collision, post-collision BCs (velocity, no-slip, geometry), parity
 // toggle, pre-collision BCs (pressure) (UpdateGrid27.cpp:66-84)
-static int step_level(const vfb_simulation *sim, SimLevel &S, void *stream)
+static int step_level(vfb_simulation *sim, SimLevel &S, void *stream)
 {
     vfb_level &L = S.level;
     int st;
+    {
+    PhaseScope phase(sim->timers, VFB_PHASE_COLLISION, stream);
     if (S.slots && sim->neighbor_tables == 2) {
         const cudaError_t e = VFB_DISPATCH(L.storage, L.arith,
                                            LA::k17_list_staged(&L, S.slots, S.slots_stride, S.n_fluid, S.status(),
@@ -1190,14 +1285,19 @@ static int step_level(const vfb_simulation *sim, SimLevel &S, void *stream)
     }
     if (st)
         return st;
-    if ((st = run_list(S, 0, S.velocity_fn, S.velocity, stream)) != VFB_OK)
-        return st;
-    if ((st = run_list(S, 1, S.noslip_fn, S.noslip, stream)) != VFB_OK)
-        return st;
-    st = run_geometry_post(S, stream);
-    if (st)
-        return st;
+    }
+    {
+        PhaseScope phase(sim->timers, VFB_PHASE_POST_COLLISION_BC, stream);
+        if ((st = run_list(S, 0, S.velocity_fn, S.velocity, stream)) != VFB_OK)
+            return st;
+        if ((st = run_list(S, 1, S.noslip_fn, S.noslip, stream)) != VFB_OK)
+            return st;
+        st = run_geometry_post(S, stream);
+        if (st)
+            return st;
+    }
     L.is_even_timestep = !L.is_even_timestep;
+    PhaseScope phase(sim->timers, VFB_PHASE_PRE_COLLISION_BC, stream);
     st = run_geometry_pre(S, stream);
     if (st)
         return st;
@@ -1229,12 +1329,16 @@ static int update_level(vfb_simulation *sim, size_t l, void *stream)
         return st;
     if (has_finer) {
         SimLevel &F = sim->levels[l + 1];
-        if (sim->scale_fc && S.fc.number_of_cells &&
-            (st = sim->scale_fc(&S.level, &F.level, &S.fc, &S.fc_offsets, stream)) != VFB_OK)
-            return st;
-        if (sim->scale_cf && S.cf.number_of_cells &&
-            (st = sim->scale_cf(&S.level, &F.level, &S.cf, &S.cf_offsets, stream)) != VFB_OK)
-            return st;
+        if (sim->scale_fc && S.fc.number_of_cells) {
+            PhaseScope phase(sim->timers, VFB_PHASE_SCALING_FC, stream);
+            if ((st = sim->scale_fc(&S.level, &F.level, &S.fc, &S.fc_offsets, stream)) != VFB_OK)
+                return st;
+        }
+        if (sim->scale_cf && S.cf.number_of_cells) {
+            PhaseScope phase(sim->timers, VFB_PHASE_SCALING_CF, stream);
+            if ((st = sim->scale_cf(&S.level, &F.level, &S.cf, &S.cf_offsets, stream)) != VFB_OK)
+                return st;
+        }
     }
     return VFB_OK;
 }
@@ -1244,9 +1348,42 @@ int vfb_simulation_run(vfb_simulation *sim, uint32_t steps, void *stream)
     int st = vfb_simulation_check(sim);
     if (st)
         return st;
-    for (uint32_t t = 0; t < steps; ++t)
-        if ((st = update_level(sim, 0, stream)) != VFB_OK)
-            return st;
+    nvtxRangePushA("vfb_simulation_run");
+    for (uint32_t t = 0; t < steps && st == VFB_OK; ++t)
+        st = update_level(sim, 0, stream);
+    nvtxRangePop();
+    if (sim->timers.on && !sim->timers.pending.empty()) {
+        cudaError_t e = cudaStreamSynchronize(as_stream(stream));
+        if (e == cudaSuccess)
+            e = sim->timers.collect();
+        if (e != cudaSuccess && st == VFB_OK)
+            st = cuda_status(e, "phase timers");
+        sim->timers.steps += steps;
+    }
+    return st;
+}
+
+int vfb_simulation_set_timing(vfb_simulation *sim, int32_t on)
+{
+    if (!sim)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL simulation");
+    sim->timers.on = on != 0;
+    return VFB_OK;
+}
+
+int vfb_simulation_phase_times(vfb_simulation *sim, double *ms, uint64_t *steps, int32_t reset)
+{
+    if (!sim || !ms)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    for (int i = 0; i < VFB_PHASES; ++i)
+        ms[i] = sim->timers.ms[i];
+    if (steps)
+        *steps = sim->timers.steps;
+    if (reset) {
+        for (double &v : sim->timers.ms)
+            v = 0.0;
+        sim->timers.steps = 0;
+    }
     return VFB_OK;
 }
 

@@ -88,6 +88,27 @@ class Parameter:
         """omega of a refinement level: nu 2^level in that level's units (Parameter.cpp:404-406)."""
         return 1.0 / (3.0 * (self.viscosity_lb * 2.0 ** level) + 0.5)
 
+    @classmethod
+    def from_configuration_file(cls, path) -> "Parameter":
+        """A Parameter from a configuration file of the reference (basics/config/ConfigurationFile
+        read by Parameter::readConfigData, Parameter.cpp:80-300): the keys of this path --
+        Viscosity_LB, Velocity_LB, ForcingX/Y/Z (0 when absent), QuadricLimiterP/M/D (0.01 when
+        absent) and MainKernelName -- with the reference's meaning. Every key of the file stays
+        readable in ``config`` (strings)."""
+        cfg = load_configuration_file(path)
+        p = cls()
+        p.config = cfg
+        if "Viscosity_LB" in cfg:
+            p.set_viscosity_lb(float(cfg["Viscosity_LB"]))
+        if "Velocity_LB" in cfg:
+            p.set_velocity_lb(float(cfg["Velocity_LB"]))
+        p.set_forcing(*(float(cfg.get(k, 0.0)) for k in ("ForcingX", "ForcingY", "ForcingZ")))
+        p.set_quadric_limiters(*(float(cfg.get(k, 0.01)) for k in ("QuadricLimiterP", "QuadricLimiterM",
+                                                                     "QuadricLimiterD")))
+        if "MainKernelName" in cfg:
+            p.configure_main_kernel(cfg["MainKernelName"])
+        return p
+
     # Parameter::checkParameterValidityCumulantK17 (Parameter.cpp:424-445): K17 with its
     # 4th-order modified equilibrium is unstable above these values
     K17_VISCOSITY_LIMIT = 1.0 / 42.0
@@ -111,6 +132,30 @@ class Parameter:
         for msg in out:
             warnings.warn(msg, K17ParameterWarning, stacklevel=2)
         return out
+
+
+def load_configuration_file(path) -> dict:
+    """key = value lines as the reference's ConfigurationFile::load reads them
+    (basics/config/ConfigurationFile.cpp:60-100): everything after '#' is a comment, key and value
+    are trimmed of spaces, tabs and line ends, lines without '=' or with an empty key or value are
+    skipped, a later line wins. A missing file is an error (std::invalid_argument there,
+    FileNotFoundError here)."""
+    out = {}
+    with open(path, "r") as f:
+        for line in f:
+            line = line.split("#", 1)[0]
+            if "=" not in line:
+                continue
+            key, value = line.split("=", 1)
+            key, value = key.strip(" \t\n\r"), value.strip(" \t\n\r")
+            if key and value:
+                out[key] = value
+    return out
+
+
+def config_bool(value: str) -> bool:
+    """ConfigurationFile's bool: true only for the text 'true' (ConfigurationFile.cpp:50-53)."""
+    return value == "true"
 
 
 class K17ParameterWarning(UserWarning):
@@ -393,6 +438,21 @@ class Simulation:
         N.check(N.lib().vfb_simulation_use_level(self._sim, level))
         N.check(N.lib().vfb_simulation_set_level(self._sim, C.byref(L), _ptr(S.fluid), int(S.grid.fluid.size)))
         N.check(N.lib().vfb_simulation_use_level(self._sim, 0))
+
+    PHASES = ("collision", "postCollisionBC", "preCollisionBC", "scalingFineToCoarse", "scalingCoarseToFine")
+
+    def set_timing(self, on: bool = True):
+        """Phase timers of the step driver (the reference's TimeStepTimer phases plus the two
+        interpolation directions): device time per phase from CUDA events, added up once at the end
+        of every run call (which then synchronises)."""
+        N.check(N.lib().vfb_simulation_set_timing(self._sim, int(bool(on))))
+
+    def phase_times(self, reset: bool = False):
+        """{phase: milliseconds} summed over the timed runs and all levels, and the coarse steps."""
+        ms = (C.c_double * len(self.PHASES))()
+        steps = C.c_uint64()
+        N.check(N.lib().vfb_simulation_phase_times(self._sim, ms, C.byref(steps), int(bool(reset))))
+        return dict(zip(self.PHASES, ms)), steps.value
 
     def run(self, steps: int):
         """steps time steps of the coarsest level (each finer level takes twice its coarser one's)."""
