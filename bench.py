@@ -557,7 +557,7 @@ def run_tgv_slab(args):
     import torch
     import torch.distributed as dist
 
-    from virtualfluids_b200.slab import DistTransport, Slab, slab_bounds, step
+    from virtualfluids_b200.slab import DistPeerTransport, DistTransport, Slab, slab_bounds, step
 
     world, rank, local = dist_env()
     torch.cuda.set_device(local)
@@ -570,7 +570,7 @@ def run_tgv_slab(args):
     planes = n * n
     s = Slab(n, n, n, z0, nzl, omega, storage="f64", arith=args.arith)
     s.init(*(a[z0 * planes:(z0 + nzl) * planes] for a in fields))
-    tr = DistTransport(s)
+    tr = DistPeerTransport(s) if args.slab_transport == "fused" else DistTransport(s)
     compute, comm = torch.cuda.Stream(), torch.cuda.Stream()
 
     def barrier():
@@ -593,6 +593,8 @@ def run_tgv_slab(args):
     t_ms = max_over_ranks_of(e0.elapsed_time(e1), dist if world > 1 else None, torch.device("cuda", local))
     f = s.fields()
     finite = bool(np.all(np.isfinite(f["vx"])))
+    if hasattr(tr, "close"):
+        tr.close()
     s.close()
     if rank == 0:
         mlups = n ** 3 * args.steps / (t_ms / 1e3) / 1e6
@@ -603,8 +605,11 @@ def run_tgv_slab(args):
                 "ms_per_step": round(t_ms / args.steps, 4), "higher_is_better": True, "scaling": "strong",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": f"Taylor-Green vortex {n}^3 periodic, {world} slab(s) of {nzl} planes, "
-                                       "border-first collision, NCCL halo exchange of 2 x 9 direction planes per "
-                                       "step on a second stream", "arith": args.arith,
+                                       "border-first collision on a second stream, halo exchange "
+                                       + ("fused into the border planes' stores (peer writes over NVLink, one "
+                                          "NCCL all-reduce as the step barrier)" if args.slab_transport == "fused"
+                                          else "by NCCL point-to-point transfers of 2 x 9 direction planes"),
+                           "arith": args.arith, "transport": args.slab_transport,
                            "halo_bytes_per_step_per_rank": 2 * 9 * planes * 8 * 2,
                            "l2": "inputs larger than L2, no flush"},
                 "hbm_gbs_algorithmic": round(gbs / world, 1), "frac_per_gpu": round(gbs / world / peak, 4),
@@ -963,6 +968,9 @@ def main():
                          "tgv-slab: the TGV as one domain in z slabs over the GPUs (NCCL halo exchange); "
                          "pool-shapes: the pool kernel against the box kernel on the same shapes")
     ap.add_argument("--form-steps", type=int, default=10000)
+    ap.add_argument("--slab-transport", default="fused", choices=["fused", "nccl"],
+                    help="tgv-slab: border planes that store into the neighbours' arrays (fused), or NCCL "
+                         "point-to-point transfers after them")
     ap.add_argument("--tgv-forms", default="f64,f32,f16,bf16,e3m12",
                     help="tgv-forms: comma-separated storage[:arith] forms, the first the FP64 reference")
     ap.add_argument("--cube-dims", type=int, nargs=5, default=[512, 256, 256, 32, 128],

@@ -437,6 +437,25 @@ int vfb_box_populations(const vfb_box *box, void **dist, uint64_t *pitch, int32_
    order and any split, then one toggle: every slot is read and written by one node per step. */
 int vfb_box_collide_planes(vfb_box *box, int32_t z_begin, int32_t z_end, void *stream);
 int vfb_box_toggle_parity(vfb_box *box);
+/* The border plane z (0 <= z < nz - 1) of a box that is one slab of a domain cut along z, with the
+   halo exchange fused into its stores (the counterpart of the reference's border collision plus
+   ExchangeData27's collect / send / scatter, Communication/ExchangeData27.cpp:52-226): the slots the
+   plane writes in plane z + 1 for directions with a negative z component at this parity are stored
+   into plane 0 of `up` (the population array of the slab above), and the slots it writes in its own
+   plane for directions with a positive z component into the last plane of `down` (the slab below's
+   ghost plane); a null `up` or `down` keeps those stores local. `up` and `down` are population
+   arrays of boxes of the same extents and storage (this process's, or another GPU's opened with
+   vfb_ipc_open: the stores then cross NVLink as peer writes). No node of the receiving slab touches
+   those slots in the same step; the caller puts a barrier between steps (after every rank's border
+   planes, before any rank's next step). */
+int vfb_box_collide_border(vfb_box *box, int32_t z, void *up, void *down, void *stream);
+/* CUDA IPC of population arrays between the processes of one node: the handle
+   (VFB_IPC_HANDLE_BYTES bytes) of a box's population array, and its mapping in another process
+   (peer access enabled) and the mapping's release. */
+#define VFB_IPC_HANDLE_BYTES 64
+int vfb_box_ipc_handle(const vfb_box *box, void *handle);
+int vfb_ipc_open(const void *handle, void **ptr);
+int vfb_ipc_close(void *ptr);
 /* the 27 population planes without their padding (plane d at d * nx*ny*nz, the storage type, as
    stored) and the parity, out of or into the box: restart files (RestartObject::serialize /
    deserialize). Host memory when to_host / from_host (the call then synchronises the stream). */

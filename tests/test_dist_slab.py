@@ -2,7 +2,9 @@
 processes each advance one slab of a periodic box with the oracle's collision, exchange the border
 planes through the library's DistTransport (the same point-to-point code the GPUs run over NCCL),
 and after several steps every slab equals its planes of the undivided box bit for bit. One slab
-(the ghost plane wrapping onto itself) and the plane sets of the exchange are checked in-process."""
+(the ghost plane wrapping onto itself) and the plane sets of the exchange are checked in-process.
+The host side of the fused transport (DistPeerTransport: every rank's IPC handle gathered, the
+ranks above and below chosen) runs on gloo ranks with stand-in handles."""
 import ctypes as C
 import os
 import tempfile
@@ -14,7 +16,8 @@ import torch.distributed as dist
 import torch.multiprocessing as mp
 
 from virtualfluids_b200.gridgen import ImportedLevel
-from virtualfluids_b200.slab import DistTransport, LocalTransport, exchange_planes, slab_bounds
+from virtualfluids_b200.slab import (DistTransport, LocalTransport, exchange_handles, exchange_planes, neighbours,
+                                     slab_bounds)
 
 NX, NY, NZ = 6, 5, 12
 OMEGA = 1.8
@@ -139,3 +142,26 @@ def test_exchange_plane_sets():
         assert set(exchange_planes(not even)[1]) == set(up)
     with pytest.raises(ValueError):
         slab_bounds(10, 3, 0)
+
+
+def _handles_rank(rank, world, path, out):
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group("gloo", init_method=f"file://{path}", rank=rank, world_size=world)
+    try:
+        mine = bytes([rank + 1]) * 64                   # a stand-in for a 64-byte CUDA IPC handle
+        handles = exchange_handles(mine)
+        above, below = neighbours(rank, world)
+        np.save(os.path.join(out, f"h{rank}.npy"),
+                np.array([handles == [bytes([r + 1]) * 64 for r in range(world)], handles[above][0] - 1,
+                          handles[below][0] - 1]))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_fused_transport_host_side(world, tmp_path):
+    path = tempfile.mktemp(prefix="vfb_handles_")
+    mp.start_processes(_handles_rank, args=(world, path, str(tmp_path)), nprocs=world, join=True, start_method="spawn")
+    for r in range(world):
+        ok, above, below = np.load(tmp_path / f"h{r}.npy")
+        assert ok and above == (r + 1) % world and below == (r - 1) % world

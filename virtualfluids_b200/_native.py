@@ -24,6 +24,7 @@ VFB_ERR_UNSUPPORTED = 7
 VFB_ERR_WATCHDOG = 8
 
 STORAGE_F64, STORAGE_F32, STORAGE_F16, STORAGE_BF16, STORAGE_E3M12 = 0, 1, 2, 3, 4
+VFB_IPC_HANDLE_BYTES = 64
 ARITH_FAST, ARITH_EXACT = 0, 1
 
 COLLISION_DEFAULT = 0
@@ -217,6 +218,10 @@ SIGNATURES = {
     "vfb_box_kernel_launches": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     "vfb_box_set_launch_shape": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "vfb_box_collide_planes": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]),
+    "vfb_box_collide_border": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "vfb_box_ipc_handle": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "vfb_ipc_open": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "vfb_ipc_close": (C.c_int, [C.c_void_p]),
     "vfb_box_toggle_parity": (C.c_int, [C.c_void_p]),
     "vfb_box_populations": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64),
                                       C.POINTER(C.c_int32)]),

@@ -2053,6 +2053,48 @@ int vfb_box_collide_planes(vfb_box *box, int32_t z_begin, int32_t z_end, void *s
     return cuda_status(e, "box collision of planes");
 }
 
+int vfb_box_collide_border(vfb_box *box, int32_t z, void *up, void *down, void *stream)
+{
+    if (!box)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL box");
+    if (z < 0 || z + 1 >= box->desc.nz)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "the border plane must satisfy 0 <= z < nz - 1");
+    const cudaError_t e = VFB_DISPATCH(box->desc.storage, box->desc.arith,
+                                       LA::box_collide_border(box->state, box->even, z, up, down, as_stream(stream)));
+    ++box->launches;
+    return cuda_status(e, "box collision of a border plane");
+}
+
+int vfb_box_ipc_handle(const vfb_box *box, void *handle)
+{
+    if (!box || !handle)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    static_assert(sizeof(cudaIpcMemHandle_t) == VFB_IPC_HANDLE_BYTES, "IPC handle size");
+    cudaIpcMemHandle_t h;
+    const cudaError_t e = cudaIpcGetMemHandle(&h, box->dist);
+    if (e != cudaSuccess)
+        return cuda_status(e, "IPC handle of a population array");
+    std::memcpy(handle, &h, sizeof h);
+    return VFB_OK;
+}
+
+int vfb_ipc_open(const void *handle, void **ptr)
+{
+    if (!handle || !ptr)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    cudaIpcMemHandle_t h;
+    std::memcpy(&h, handle, sizeof h);
+    *ptr = nullptr;
+    return cuda_status(cudaIpcOpenMemHandle(ptr, h, cudaIpcMemLazyEnablePeerAccess), "opening an IPC handle");
+}
+
+int vfb_ipc_close(void *ptr)
+{
+    if (!ptr)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL pointer");
+    return cuda_status(cudaIpcCloseMemHandle(ptr), "closing an IPC mapping");
+}
+
 int vfb_box_toggle_parity(vfb_box *box)
 {
     if (!box)

@@ -428,6 +428,71 @@ __global__ void __launch_bounds__(128, box_min_blocks<S>()) k17_box_kernel(BoxCo
 }
 
 // ---------------------------------------------------------------------------------------------
+// One z plane of a box that is a slab of a larger domain, whose neighbouring slabs live in other
+// population arrays of the same shape (on this GPU, or on another through a peer mapping): the
+// collision of k17_box_kernel, with the stores that belong to a neighbour made straight into the
+// neighbour's array, so that no exchange step follows.
+//   up   : the slots this plane writes in plane z + 1 (directions with a negative z component at
+//          this parity) go to plane 0 of `up` (the slab above, whose bottom layer reads them);
+//   down : the slots this plane writes in its own plane for directions with a positive z
+//          component go to the last plane of `down` (the slab below's ghost plane, read by its top
+//          layer).
+// Either may be null (the store stays local). In the esoteric twist no node of the receiving slab
+// touches those slots in the same step, so the stores need no ordering against the neighbour's
+// kernels of that step; the caller orders the steps (a barrier between them).
+// ---------------------------------------------------------------------------------------------
+template <class S, bool EXACT, bool EVEN, bool MASK>
+__global__ void __launch_bounds__(128, box_min_blocks<S>())
+    k17_box_border_kernel(BoxCollideArgs<typename Codec<S>::compute> a, int z, S *up, S *down)
+{
+    using C = typename Codec<S>::compute;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= a.nx)
+        return;
+    const uint64_t plane_nodes = (uint64_t)a.nx * (uint64_t)a.ny;
+    const uint32_t k = (uint32_t)(plane_nodes * (uint64_t)z + (uint64_t)a.nx * (uint64_t)y + (uint64_t)x);
+    if (MASK && __ldg(a.mask + k) == 0)
+        return;
+    const int xp = (x + 1 < a.nx) ? x + 1 : (a.periodic_x ? 0 : x);
+    const int yp = (y + 1 < a.ny) ? y + 1 : (a.periodic_y ? 0 : y);
+    const int zp = (z + 1 < a.nz) ? z + 1 : (a.periodic_z ? 0 : z);
+    const uint32_t sx = (uint32_t)(xp - x);
+    const uint32_t sy = (uint32_t)((yp - y) * a.nx);
+    const uint32_t sz = (uint32_t)((int64_t)(zp - z) * a.nx * a.ny);
+    uint32_t nodes[8];
+    nodes[0] = k;
+    nodes[1] = k + sx;
+    nodes[2] = k + sy;
+    nodes[3] = k + sx + sy;
+    nodes[4] = k + sz;
+    nodes[5] = k + sx + sz;
+    nodes[6] = k + sy + sz;
+    nodes[7] = k + sx + sy + sz;
+    S *base = static_cast<S *>(a.dist);
+    C f[27];
+    gather_pre<S, EVEN>(base, a.pitch, nodes, f);
+    C drho, vx, vy, vz;
+    collide<C, EXACT>(f, a.rates, a.fx, a.fy, a.fz, drho, vx, vy, vz);
+    const uint64_t up_shift = plane_nodes * (uint64_t)(z + 1);                 // plane z + 1 -> plane 0
+    const uint64_t down_shift = plane_nodes * (uint64_t)(a.nz - 1 - z);        // plane z -> last plane
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        const uint64_t off = (uint64_t)plane<EVEN>(d) * a.pitch + nodes[shift_class(d)];
+        if (cz(d) < 0 && up != nullptr)
+            Codec<S>::store_at(up, off - up_shift, f[inv(d)], d);
+        else if (cz(d) > 0 && down != nullptr)
+            Codec<S>::store_at(down, off + down_shift, f[inv(d)], d);
+        else
+            Codec<S>::store_at(base, off, f[inv(d)], d);
+    }
+    // stores into another GPU's memory are made visible at system scope before the kernel ends, so
+    // the barrier that follows (an NCCL all-reduce) orders them for the neighbour
+    if (up != nullptr || down != nullptr)
+        __threadfence_system();
+}
+
+// ---------------------------------------------------------------------------------------------
 // The box collision as a persistent, software-pipelined loop. A block walks rows of blockDim.x
 // nodes along x (tile t = (x tile, y, z)); before a thread collides and stores its node of the
 // current tile it issues the 27 loads of its node in the next tile into registers, so the loads of

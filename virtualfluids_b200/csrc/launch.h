@@ -83,6 +83,8 @@ struct PoolDomainSpec {
         static cudaError_t box_collide(const BoxState &b, bool even, double *partials, uint64_t *n_partials,        \
                                        cudaStream_t s);                                                            \
         static cudaError_t box_collide_planes(const BoxState &b, bool even, int z0, int z1, cudaStream_t s);       \
+        static cudaError_t box_collide_border(const BoxState &b, bool even, int z, void *up, void *down,           \
+                                              cudaStream_t s);                                                     \
         static cudaError_t box_init(const BoxState &b, bool even, const void *rho, const void *ux, const void *uy, \
                                     const void *uz, cudaStream_t s);                                               \
         static cudaError_t box_macros(const BoxState &b, bool even, void *rho, void *ux, void *uy, void *uz,       \

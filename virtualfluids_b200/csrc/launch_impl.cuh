@@ -805,6 +805,26 @@ cudaError_t Launchers<S>::box_collide_planes(const BoxState &b, bool even, int z
 }
 
 template <class S>
+cudaError_t Launchers<S>::box_collide_border(const BoxState &b, bool even, int z, void *up, void *down, cudaStream_t s)
+{
+    using C = typename Codec<S>::compute;
+    BoxCollideArgs<C> a = box_args<C>(b);
+    dim3 G = box_grid(b);
+    G.z = 1;
+    const dim3 B(box_block_x(b.nx));
+    S *u = static_cast<S *>(up), *d = static_cast<S *>(down);
+    const bool mask = b.mask != nullptr;
+    if (even) {
+        if (mask) k17_box_border_kernel<S, VFB_EXACT, true, true><<<G, B, 0, s>>>(a, z, u, d);
+        else k17_box_border_kernel<S, VFB_EXACT, true, false><<<G, B, 0, s>>>(a, z, u, d);
+    } else {
+        if (mask) k17_box_border_kernel<S, VFB_EXACT, false, true><<<G, B, 0, s>>>(a, z, u, d);
+        else k17_box_border_kernel<S, VFB_EXACT, false, false><<<G, B, 0, s>>>(a, z, u, d);
+    }
+    return cudaGetLastError();
+}
+
+template <class S>
 cudaError_t Launchers<S>::box_init(const BoxState &b, bool even, const void *rho, const void *ux, const void *uy,
                                    const void *uz, cudaStream_t s)
 {

@@ -31,6 +31,14 @@ A step: the two border planes collide on a second stream and the exchange follow
 (NCCL point-to-point sends and receives grouped per step over NVLink, or device copies between
 slabs of one process), while the interior planes collide on the compute stream; then the parity
 toggles.
+
+The fused transports (LocalPeerTransport, DistPeerTransport) have no exchange step: each border
+plane's collision stores the slots a neighbour reads straight into the neighbour's population
+array (vfb_box_collide_border) -- an array of this process, or another GPU's opened through CUDA IPC,
+so that the stores cross NVLink as peer writes -- and a barrier between steps (a one-element NCCL
+all-reduce on the exchange stream, after every rank's border planes) orders them against the
+neighbour's next step. The stores go into exactly the slots the exchange would have copied, and no
+node of the receiving slab touches them in the same step.
 Initialisation: the slab's box is periodic in z, so each ghost node writes its slots of the
 negative-z directions into plane 0 -- the slots the node below the slab owns, which no node of the
 slab reads in the first step and the first exchange overwrites -- and never into the ghost-plane
@@ -120,6 +128,25 @@ class Slab:
     def collide(self, z_begin, z_end, stream=None):
         N.check(N.lib().vfb_box_collide_planes(self.box._h, int(z_begin), int(z_end), stream))
 
+    @property
+    def base(self):
+        """device address of the population array (what a neighbour's fused border stores target)"""
+        dist, pitch, even = C.c_void_p(), C.c_uint64(), C.c_int32()
+        N.check(N.lib().vfb_box_populations(self.box._h, C.byref(dist), C.byref(pitch), C.byref(even)))
+        return dist.value
+
+    def collide_border(self, z, up=None, down=None, stream=None):
+        """the border plane z with its neighbour stores fused (vfb_box_collide_border): up / down are
+        device addresses of the population arrays of the slabs above / below, or None"""
+        N.check(N.lib().vfb_box_collide_border(self.box._h, int(z), C.c_void_p(up) if up else None,
+                                               C.c_void_p(down) if down else None, stream))
+
+    def ipc_handle(self) -> bytes:
+        """the CUDA IPC handle of the population array (for a neighbour in another process)"""
+        h = (C.c_char * N.VFB_IPC_HANDLE_BYTES)()
+        N.check(N.lib().vfb_box_ipc_handle(self.box._h, h))
+        return bytes(h)
+
     def toggle(self):
         N.check(N.lib().vfb_box_toggle_parity(self.box._h))
 
@@ -183,6 +210,78 @@ class DistTransport:
             req.wait()
 
 
+def neighbours(rank, world):
+    """(above, below): the ranks whose slabs lie above and below rank's, periodically"""
+    return (rank + 1) % world, (rank - 1) % world
+
+
+class LocalPeerTransport:
+    """The fused exchange between slabs of one process: slabs[r] sits below slabs[r + 1],
+    periodically, and each border plane stores into its neighbour's array directly."""
+
+    fused = True
+
+    def __init__(self, slabs):
+        self.slabs = list(slabs)
+
+    def peers(self, r):
+        above, below = neighbours(r, len(self.slabs))
+        return self.slabs[above].base, self.slabs[below].base
+
+    def barrier(self):
+        pass
+
+
+class DistPeerTransport:
+    """The fused exchange of one slab per process over peer memory: the ranks swap the CUDA IPC
+    handles of their population arrays once (all_gather_object), each opens the arrays of the
+    ranks above and below it, and the border planes store into them directly. barrier() is a
+    one-element all-reduce on the current stream (NCCL: stream-ordered after the border planes on
+    every rank), so no rank starts its next step before its neighbours' stores of this step have
+    landed. One rank stores into its own array. close() releases the mappings."""
+
+    fused = True
+
+    def __init__(self, slab, group=None):
+        import torch
+        import torch.distributed as dist
+        self.dist, self.group, self.slab = dist, group, slab
+        self.world = dist.get_world_size(group) if dist.is_initialized() else 1
+        self.rank = dist.get_rank(group) if dist.is_initialized() else 0
+        self._opened = {}
+        if self.world == 1:
+            self._up = self._down = slab.base
+            return
+        handles = exchange_handles(slab.ipc_handle(), group)
+        above, below = neighbours(self.rank, self.world)
+        for r in {above, below}:
+            ptr = C.c_void_p()
+            N.check(N.lib().vfb_ipc_open(handles[r], C.byref(ptr)))
+            self._opened[r] = ptr.value
+        self._up, self._down = self._opened[above], self._opened[below]
+        self._flag = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+    def peers(self, r=0):
+        return self._up, self._down
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.all_reduce(self._flag, group=self.group)
+
+    def close(self):
+        for ptr in self._opened.values():
+            N.lib().vfb_ipc_close(C.c_void_p(ptr))
+        self._opened = {}
+
+
+def exchange_handles(handle: bytes, group=None) -> list:
+    """every rank's IPC handle, indexed by rank (all_gather_object)"""
+    import torch.distributed as dist
+    out = [None] * dist.get_world_size(group)
+    dist.all_gather_object(out, handle, group=group)
+    return out
+
+
 def step(slabs, transport, compute=None, comm=None):
     """One time step of slabs that share a transport. The interior planes collide on the compute
     stream while, on the comm stream, the two border planes collide and then the exchange runs: no
@@ -196,11 +295,19 @@ def step(slabs, transport, compute=None, comm=None):
     even = slabs[0].even
     comm.wait_stream(compute)
     cs, ms = C.c_void_p(compute.cuda_stream), C.c_void_p(comm.cuda_stream)
-    for s in slabs:
-        s.collide(0, 1, ms)
-        s.collide(s.nzl - 1, s.nzl, ms)
-    with torch.cuda.stream(comm):
-        transport.exchange(even)
+    if getattr(transport, "fused", False):
+        for r, s in enumerate(slabs):
+            up, down = transport.peers(r)
+            s.collide_border(s.nzl - 1, up=up, stream=ms)
+            s.collide_border(0, down=down, stream=ms)
+        with torch.cuda.stream(comm):
+            transport.barrier()
+    else:
+        for s in slabs:
+            s.collide(0, 1, ms)
+            s.collide(s.nzl - 1, s.nzl, ms)
+        with torch.cuda.stream(comm):
+            transport.exchange(even)
     for s in slabs:
         s.collide(1, s.nzl - 1, cs)
     compute.wait_stream(comm)
