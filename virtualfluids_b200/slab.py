@@ -265,8 +265,16 @@ class DistPeerTransport:
         return self._up, self._down
 
     def barrier(self):
-        if self.world > 1:
+        """NCCL: the stream-ordered all-reduce. Another backend (gloo) cannot order device work,
+        so the host waits for the current stream and then meets the other ranks."""
+        if self.world == 1:
+            return
+        if self.dist.get_backend(self.group) == "nccl":
             self.dist.all_reduce(self._flag, group=self.group)
+        else:
+            import torch
+            torch.cuda.current_stream().synchronize()
+            self.dist.barrier(group=self.group)
 
     def close(self):
         for ptr in self._opened.values():
