@@ -536,7 +536,9 @@ int vfb_pool_step(vfb_pool *pool, uint32_t steps, void *stream);
 int vfb_pool_domain_fields(vfb_pool *pool, uint32_t id, void *rho, void *ux, void *uy, void *uz, int32_t to_host,
                            void *stream);
 /* launch shape: threads per block (64, 128 or 256), nodes per thread per work item (1..8), resident
-   blocks per SM (0 = as many as fit), CUDA-graph replay (0/1); a new pool starts at 128, 4, 0, 1 */
+   blocks per SM of the persistent launch (0 = as many as fit; -1 = no persistent loop: one block per
+   work item, the grid following the work list, so a change of the list's length captures the step
+   graph again), CUDA-graph replay (0/1); a new pool starts at 128, 8, -1, 1 */
 int vfb_pool_set_launch(vfb_pool *pool, int32_t threads_per_block, int32_t nodes_per_thread, int32_t blocks_per_sm,
                         int32_t use_graph);
 int vfb_pool_get_launch(const vfb_pool *pool, int32_t out4[4]);

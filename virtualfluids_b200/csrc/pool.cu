@@ -168,7 +168,7 @@ struct vfb_pool {
     bool list_dirty = true;
     uint64_t active_nodes = 0;
     bool even = true;
-    int threads = 128, nodes_per_thread = 4, blocks_per_sm = 0, use_graph = 1;   // the default launch shape
+    int threads = 128, nodes_per_thread = 8, blocks_per_sm = -1, use_graph = 1;  // the default launch shape
     unsigned grid = 0;
     cudaGraphExec_t graph = nullptr;
     cudaStream_t graph_stream = nullptr;
@@ -204,6 +204,15 @@ int sm_count_here()
 
 cudaError_t update_grid(vfb_pool *p)
 {
+    if (p->blocks_per_sm < 0) {
+        // one block per work item, no persistent loop: the grid follows the list's item count
+        const unsigned g = (unsigned)std::max<size_t>(p->host_items.size(), 1);
+        if (g != p->grid)
+            drop_graph(p);
+        p->grid = g;
+        p->bc_grid = (unsigned)(4 * sm_count_here());
+        return cudaSuccess;
+    }
     int bps = p->blocks_per_sm;
     int occ = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, p->ops.kernel(true), p->threads, 0);
@@ -327,6 +336,8 @@ cudaError_t rebuild_list(vfb_pool *p, cudaStream_t s)
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(p->n_items, &n, sizeof(uint32_t), cudaMemcpyHostToDevice, s);
     p->host_items = items;
+    if (e == cudaSuccess && p->blocks_per_sm < 0)
+        e = update_grid(p);        // a captured step's grid is the old item count
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(s);
     if (e == cudaSuccess)
@@ -900,8 +911,8 @@ int vfb_pool_set_launch(vfb_pool *p, int32_t threads, int32_t nodes_per_thread, 
         return pool_fail(VFB_ERR_INVALID_ARGUMENT, "NULL pool");
     if (threads != 64 && threads != 128 && threads != 256)
         return pool_fail(VFB_ERR_INVALID_ARGUMENT, "threads_per_block must be 64, 128 or 256");
-    if (nodes_per_thread < 1 || nodes_per_thread > 8 || blocks_per_sm < 0 || blocks_per_sm > 32)
-        return pool_fail(VFB_ERR_INVALID_ARGUMENT, "nodes_per_thread must lie in [1, 8], blocks_per_sm in [0, 32]");
+    if (nodes_per_thread < 1 || nodes_per_thread > 8 || blocks_per_sm < -1 || blocks_per_sm > 32)
+        return pool_fail(VFB_ERR_INVALID_ARGUMENT, "nodes_per_thread must lie in [1, 8], blocks_per_sm in [-1, 32]");
     if (threads != p->threads || nodes_per_thread != p->nodes_per_thread) {
         p->list_dirty = true;
         drop_graph(p);
@@ -919,7 +930,7 @@ int vfb_pool_get_launch(const vfb_pool *p, int32_t out4[4])
         return pool_fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
     out4[0] = p->threads;
     out4[1] = p->nodes_per_thread;
-    out4[2] = (int32_t)(p->grid / (unsigned)sm_count_here());
+    out4[2] = p->blocks_per_sm < 0 ? -1 : (int32_t)(p->grid / (unsigned)sm_count_here());
     out4[3] = p->use_graph;
     return VFB_OK;
 }
@@ -931,7 +942,8 @@ int vfb_pool_autotune(vfb_pool *p, uint32_t trial_steps, void *stream, double *b
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     struct Shape { int t, npt, bps; };
     static const Shape kShapes[] = { { 128, 1, 0 }, { 128, 2, 0 }, { 128, 4, 0 }, { 64, 1, 0 }, { 64, 2, 0 },
-                                     { 256, 1, 0 }, { 256, 2, 0 }, { 128, 1, 2 }, { 128, 2, 2 } };
+                                     { 256, 1, 0 }, { 256, 2, 0 }, { 128, 1, 2 }, { 128, 2, 2 },
+                                     { 128, 4, -1 }, { 128, 8, -1 }, { 256, 4, -1 }, { 64, 8, -1 } };
     const int graph = p->use_graph;
     cudaEvent_t a = nullptr, b = nullptr;
     cudaError_t e = cudaEventCreate(&a);
