@@ -462,11 +462,12 @@ int vfb_ipc_close(void *ptr);
 int vfb_box_read_populations(vfb_box *box, void *out, int32_t to_host, int32_t *is_even, void *stream);
 int vfb_box_write_populations(vfb_box *box, const void *src, int32_t from_host, int32_t is_even, void *stream);
 
-/* ---- (2c) domain pools: batches of independent boxes in one persistent launch ---------------
+/* ---- (2c) domain pools: batches of independent boxes in one launch per step ---------------
    No counterpart in the reference (one level of one domain per Simulation there). A pool owns one
    device arena sized at creation; domains of uneven sizes are carved from it and released again,
    so a serving loop can admit solves against the HBM budget. Every step advances all active
-   domains with one persistent kernel that walks a work list of node blocks (domain, first node);
+   domains with one kernel launch over a work list of node blocks (domain, first node): one block
+   per item, or a persistent grid that walks the list (vfb_pool_set_launch);
    each domain computes exactly what a vfb_box of the same description computes. */
 typedef struct vfb_pool_desc {
     int32_t storage;                  /* vfb_storage */
@@ -529,7 +530,7 @@ int vfb_pool_synchronize(vfb_pool *pool, void *stream);
    pool keeps outside the arena (grown when a larger domain than before is staged). */
 int vfb_pool_init_domain(vfb_pool *pool, uint32_t id, const void *rho, const void *ux, const void *uy, const void *uz,
                          int32_t from_host, void *stream);
-/* advance every active domain by `steps` time steps (one persistent launch per step; with the
+/* advance every active domain by `steps` time steps (one collision launch per step; with the
    graph option the launches of 16 steps are replayed from one captured CUDA graph) */
 int vfb_pool_step(vfb_pool *pool, uint32_t steps, void *stream);
 /* drho, ux, uy, uz (real[nx*ny*nz]) of one domain, to host or device memory */
