@@ -754,12 +754,15 @@ def run_list_path(args, n, omega, fields, dev):
     out["peak_source"] = peak_kind
     # node numbering as the reference's grid builder (first node 1, planes of n^3 + 1 nodes), and
     # aligned (first node 32, planes padded to 32 nodes)
-    for align, key in ((1, "reference_numbering"), (32, "aligned_numbering")):
+    runs = [(1, "reference_numbering", args.arith), (32, "aligned_numbering", args.arith)]
+    if args.arith == "exact":
+        runs.append((32, "fma_aligned_numbering", "fast"))     # the FMA form of the same path, beside it
+    for align, key, arith in runs:
         g = vfb.ListGrid(n, n, n, periodic=(True, True, True), align=align)
         p = vfb.Parameter()
         p.set_viscosity_lb((1.0 / omega - 0.5) / 3.0)
         p.configure_main_kernel("K17CompressibleNavierStokes")
-        p.storage, p.arith = N.STORAGE_F64, N.ARITH_EXACT if args.arith == "exact" else N.ARITH_FAST
+        p.storage, p.arith = N.STORAGE_F64, N.ARITH_EXACT if arith == "exact" else N.ARITH_FAST
         sim = vfb.Simulation(p, g, vfb.BoundaryConditionFactory())
         full = [np.zeros(g.number_of_nodes) for _ in range(4)]
         for dst, a in zip(full, fields):
