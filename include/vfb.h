@@ -361,6 +361,15 @@ enum {
     VFB_PHASES = 5
 };
 int vfb_simulation_set_timing(vfb_simulation *sim, int32_t on);
+/* The step loop as a CUDA graph (the step loop of the reference launches every kernel of every step
+   from the host, UpdateGrid27.cpp:54-95): with steps > 0 (even, up to 1024), vfb_simulation_run on
+   a non-NULL stream runs its first step directly after any configuration change (so that buffers
+   made on first use exist), then captures `steps` coarse steps once and replays the graph while
+   enough steps remain, the rest directly. Every setter drops the graph; a run whose level
+   parities differ from those at capture captures again. Not used on the legacy (NULL) stream, with
+   timing on, or while a drag/lift history is kept (its per-step slot is chosen on the host).
+   Results are those of the direct loop, bit for bit. 0 (the default) turns it off. */
+int vfb_simulation_set_graph(vfb_simulation *sim, int32_t steps);
 int vfb_simulation_phase_times(vfb_simulation *sim, double *ms, uint64_t *steps, int32_t reset);
 /* parity of the coarsest level / of a given level */
 int vfb_simulation_is_even_timestep(const vfb_simulation *sim, int32_t *is_even);

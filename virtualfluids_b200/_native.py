@@ -183,6 +183,7 @@ SIGNATURES = {
     "vfb_simulation_check": (C.c_int, [C.c_void_p]),
     "vfb_simulation_run": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p]),
     "vfb_simulation_set_timing": (C.c_int, [C.c_void_p, C.c_int32]),
+    "vfb_simulation_set_graph": (C.c_int, [C.c_void_p, C.c_int32]),
     "vfb_simulation_phase_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.c_int32]),
     "vfb_simulation_is_even_timestep": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "vfb_simulation_level_is_even_timestep": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),

@@ -860,6 +860,27 @@ private:
     cudaEvent_t start_ = nullptr;
 };
 
+// The step loop captured as a CUDA graph: `steps` coarse steps (an even number, so every level
+// ends at the parity it started from) recorded once on a stream and replayed. Any change of the
+// configuration drops it; a replay is taken only when every level's parity equals the one it was
+// captured at, else the graph is captured again.
+struct StepGraph {
+    int32_t steps = 0;              // coarse steps per graph, 0 = off
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t stream = nullptr;
+    std::vector<int> parity;        // every level's parity at capture
+    bool warm = false;              // a step has run directly since the last change (lazy buffers exist)
+    void drop()
+    {
+        if (exec)
+            cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        stream = nullptr;
+        parity.clear();
+    }
+    ~StepGraph() { drop(); }
+};
+
 struct vfb_simulation {
     int kernel_id = 0;
     std::vector<SimLevel> levels = std::vector<SimLevel>(1);
@@ -869,7 +890,15 @@ struct vfb_simulation {
     vfb_scaling_fn scale_fc = nullptr;
     vfb_scaling_fn scale_cf = nullptr;
     PhaseTimers timers;
+    StepGraph graph;
 };
+
+// every setter: a captured step no longer matches the configuration
+static void config_changed(vfb_simulation *sim)
+{
+    sim->graph.drop();
+    sim->graph.warm = false;
+}
 
 static SimLevel &current(vfb_simulation *sim) { return sim->levels[(size_t)sim->cursor]; }
 
@@ -959,6 +988,7 @@ int vfb_simulation_use_level(vfb_simulation *sim, int32_t level)
 {
     if (!sim)
         return fail(VFB_ERR_INVALID_ARGUMENT, "NULL simulation");
+    config_changed(sim);
     if (level < 0 || level > (int32_t)sim->levels.size() || level >= VFB_MAX_LEVELS)
         return fail(VFB_ERR_INVALID_ARGUMENT, "levels are added one at a time, from the coarsest, up to VFB_MAX_LEVELS");
     if (level == (int32_t)sim->levels.size())
@@ -971,6 +1001,7 @@ int vfb_simulation_set_neighbor_tables(vfb_simulation *sim, int32_t enable)
 {
     if (!sim)
         return fail(VFB_ERR_INVALID_ARGUMENT, "NULL simulation");
+    config_changed(sim);
     if (enable < 0 || enable > 2)
         return fail(VFB_ERR_INVALID_ARGUMENT, "neighbour tables: 0 off, 1 direct loads, 2 staged copies");
     sim->neighbor_tables = enable;
@@ -1015,6 +1046,7 @@ int vfb_simulation_set_level(vfb_simulation *sim, const vfb_level *level, const 
 {
     if (!sim)
         return fail(VFB_ERR_INVALID_ARGUMENT, "NULL simulation");
+    config_changed(sim);
     int st = check_level(level);
     if (st)
         return st;
@@ -1034,6 +1066,7 @@ int vfb_simulation_set_velocity_bc(vfb_simulation *sim, const vfb_bc *bc, int32_
 {
     if (!sim || !bc)
         return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    config_changed(sim);
     vfb_bc_fn fn = nullptr;
     int st = vfb_bc_factory_velocity(variant, &fn);
     if (st)
@@ -1049,6 +1082,7 @@ int vfb_simulation_set_noslip_bc(vfb_simulation *sim, const vfb_bc *bc, int32_t 
 {
     if (!sim || !bc)
         return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    config_changed(sim);
     vfb_bc_fn fn = nullptr;
     int st = vfb_bc_factory_noslip(variant, &fn);
     if (st)
@@ -1064,6 +1098,7 @@ int vfb_simulation_add_pressure_bc(vfb_simulation *sim, const vfb_directional_bc
 {
     if (!sim || !bc)
         return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    config_changed(sim);
     vfb_directional_bc_fn fn = nullptr;
     int st = vfb_bc_factory_pressure(variant, &fn);
     if (st)
@@ -1080,6 +1115,7 @@ int vfb_simulation_set_geometry_bc(vfb_simulation *sim, const vfb_bc *bc, int32_
 {
     if (!sim || !bc)
         return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    config_changed(sim);
     vfb_bc_fn fn = nullptr;
     int st = vfb_bc_factory_noslip(variant, &fn);
     if (st)
@@ -1101,6 +1137,7 @@ int vfb_simulation_set_drag_lift(vfb_simulation *sim, void *workspace, size_t wo
 {
     if (!sim)
         return fail(VFB_ERR_INVALID_ARGUMENT, "NULL simulation");
+    config_changed(sim);
     SimLevel &S = current(sim);
     if (!workspace) {
         S.drag_work = nullptr;
@@ -1127,6 +1164,7 @@ int vfb_simulation_set_scaling_factory(vfb_simulation *sim, int32_t variant, int
 {
     if (!sim)
         return fail(VFB_ERR_INVALID_ARGUMENT, "NULL simulation");
+    config_changed(sim);
     vfb_scaling_fn fc = nullptr, cf = nullptr;
     int st = vfb_scaling_factory_fine_to_coarse(variant, has_turbulent_viscosity, &fc);
     if (st)
@@ -1148,6 +1186,7 @@ int vfb_simulation_set_interpolation_cells(vfb_simulation *sim, int32_t coarse_l
 {
     if (!sim || !fine_to_coarse || !fine_to_coarse_offsets || !coarse_to_fine || !coarse_to_fine_offsets)
         return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    config_changed(sim);
     if (coarse_level < 0 || coarse_level + 1 >= (int32_t)sim->levels.size())
         return fail(VFB_ERR_INVALID_ARGUMENT, "coarse_level and the level above it must have been added");
     const vfb_interpolation_cells *c[2] = { fine_to_coarse, coarse_to_fine };
@@ -1343,13 +1382,74 @@ static int update_level(vfb_simulation *sim, size_t l, void *stream)
     return VFB_OK;
 }
 
+static std::vector<int> parities(const vfb_simulation *sim)
+{
+    std::vector<int> p;
+    for (const SimLevel &S : sim->levels)
+        p.push_back(S.level.is_even_timestep);
+    return p;
+}
+
+// capture sim->graph.steps coarse steps on `stream` (nothing runs); the host's per-level parity
+// is put back to where the capture started, since the captured steps have not happened yet
+static int capture_steps(vfb_simulation *sim, cudaStream_t stream)
+{
+    StepGraph &G = sim->graph;
+    G.drop();
+    const std::vector<int> start = parities(sim);
+    cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess)
+        return cuda_status(e, "beginning the capture of the step loop");
+    int st = VFB_OK;
+    for (int32_t t = 0; t < G.steps && st == VFB_OK; ++t)
+        st = update_level(sim, 0, stream);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(stream, &g);
+    for (size_t l = 0; l < sim->levels.size(); ++l)
+        sim->levels[l].level.is_even_timestep = start[l];
+    if (st == VFB_OK && e == cudaSuccess)
+        e = cudaGraphInstantiate(&G.exec, g, 0);
+    if (g)
+        cudaGraphDestroy(g);
+    if (st != VFB_OK)
+        return st;
+    if (e != cudaSuccess) {
+        G.exec = nullptr;
+        return cuda_status(e, "capturing the step loop");
+    }
+    G.stream = stream;
+    G.parity = start;
+    return VFB_OK;
+}
+
 int vfb_simulation_run(vfb_simulation *sim, uint32_t steps, void *stream)
 {
     int st = vfb_simulation_check(sim);
     if (st)
         return st;
     nvtxRangePushA("vfb_simulation_run");
-    for (uint32_t t = 0; t < steps && st == VFB_OK; ++t)
+    uint32_t done = 0;
+    StepGraph &G = sim->graph;
+    bool drag = false;
+    for (const SimLevel &S : sim->levels)
+        drag = drag || (S.drag_work != nullptr && S.geometry_set && S.geometry.number_of_bc_nodes);
+    // graphs: a stream of the caller's (capture needs one), no event timers, no per-step drag history
+    if (G.steps > 0 && stream != nullptr && !sim->timers.on && !drag) {
+        const cudaStream_t s = as_stream(stream);
+        for (; !G.warm && done < steps && st == VFB_OK; ++done) {
+            st = update_level(sim, 0, stream);     // lazy buffers come to exist outside a capture
+            G.warm = st == VFB_OK;
+        }
+        while (st == VFB_OK && steps - done >= (uint32_t)G.steps) {
+            if (!G.exec || G.stream != s || G.parity != parities(sim))
+                st = capture_steps(sim, s);
+            if (st == VFB_OK)
+                st = cuda_status(cudaGraphLaunch(G.exec, s), "replaying the step loop");
+            if (st == VFB_OK)
+                done += (uint32_t)G.steps;    // an even number of steps: every parity as it was
+        }
+    }
+    for (uint32_t t = done; t < steps && st == VFB_OK; ++t)
         st = update_level(sim, 0, stream);
     nvtxRangePop();
     if (sim->timers.on && !sim->timers.pending.empty()) {
@@ -1363,10 +1463,22 @@ int vfb_simulation_run(vfb_simulation *sim, uint32_t steps, void *stream)
     return st;
 }
 
+int vfb_simulation_set_graph(vfb_simulation *sim, int32_t steps)
+{
+    if (!sim)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL simulation");
+    if (steps < 0 || steps % 2 != 0 || steps > 1024)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "steps per graph must be 0 (off) or an even number up to 1024");
+    config_changed(sim);
+    sim->graph.steps = steps;
+    return VFB_OK;
+}
+
 int vfb_simulation_set_timing(vfb_simulation *sim, int32_t on)
 {
     if (!sim)
         return fail(VFB_ERR_INVALID_ARGUMENT, "NULL simulation");
+    config_changed(sim);
     sim->timers.on = on != 0;
     return VFB_OK;
 }

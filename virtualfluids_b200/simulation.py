@@ -454,9 +454,22 @@ class Simulation:
         N.check(N.lib().vfb_simulation_phase_times(self._sim, ms, C.byref(steps), int(bool(reset))))
         return dict(zip(self.PHASES, ms)), steps.value
 
+    def set_graph(self, steps: int = 16):
+        """Run the step loop as a CUDA graph of `steps` coarse steps (even; 0 turns it off), replayed
+        on a stream of this simulation's own (vfb_simulation_set_graph). Results are the same bits."""
+        N.check(N.lib().vfb_simulation_set_graph(self._sim, int(steps)))
+        self._graph_stream = _torch().cuda.Stream() if steps else None
+
     def run(self, steps: int):
         """steps time steps of the coarsest level (each finer level takes twice its coarser one's)."""
-        N.check(N.lib().vfb_simulation_run(self._sim, int(steps), None))
+        gs = getattr(self, "_graph_stream", None)
+        if gs is None:
+            N.check(N.lib().vfb_simulation_run(self._sim, int(steps), None))
+        else:
+            t = _torch()
+            gs.wait_stream(t.cuda.current_stream())
+            N.check(N.lib().vfb_simulation_run(self._sim, int(steps), C.c_void_p(gs.cuda_stream)))
+            t.cuda.current_stream().wait_stream(gs)
         self._drag_steps = getattr(self, "_drag_steps", 0) + int(steps) if self._drag is not None else 0
         for i, S in enumerate(self.levels):
             ev = C.c_int32()
