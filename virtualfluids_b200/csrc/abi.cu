@@ -1813,6 +1813,7 @@ int vfb_box_step(vfb_box *box, uint32_t steps, double *energy, int32_t energy_on
 {
     if (!box)
         return fail(VFB_ERR_INVALID_ARGUMENT, "NULL box");
+    const vfb::NvtxRange range("vfb_box_step");
     cudaStream_t s = as_stream(stream);
     cudaError_t e = cudaSuccess;
     uint32_t done = 0;

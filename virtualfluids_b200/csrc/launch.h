@@ -7,6 +7,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 
@@ -15,7 +16,16 @@
 
 namespace vfb {
 struct e3m12_t; // the E3M12 storage element (storage.cuh)
-}
+
+// an NVTX range for the lifetime of the object (the steps of boxes and pools, for ncu --nvtx and
+// other NVTX tools; a no-op without one attached)
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
+} // namespace vfb
 
 namespace vfb {
 

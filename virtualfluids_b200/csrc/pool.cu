@@ -856,6 +856,7 @@ int vfb_pool_step(vfb_pool *p, uint32_t steps, void *stream)
 {
     if (!p)
         return pool_fail(VFB_ERR_INVALID_ARGUMENT, "NULL pool");
+    const vfb::NvtxRange range("vfb_pool_step");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaError_t e = cudaSuccess;
     if (p->list_dirty)
