@@ -688,7 +688,7 @@ def run_cube(args):
 
 def run_tgv_forms(args):
     """Storage-form accuracy: the 256^3 Taylor-Green vortex for --form-steps steps in FP64, FP32, FP16
-    and BF16 storage (FMA arithmetic), the FP64 kinetic-energy decay every 100 steps, and the L2 /
+    and BF16 storage (FMA arithmetic), the FP64 kinetic-energy decay every 10 steps, and the L2 /
     L-inf velocity error of each form against the FP64 run at steps 1000, 5000 and 10000 (relative
     to the FP64 field's RMS / maximum speed)."""
     import torch
@@ -719,7 +719,8 @@ def run_tgv_forms(args):
                 k = min(every, c - done)
                 e = np.zeros((k, 2))
                 box.step(k, energy=e)
-                ek.append(float(e[-1, 1]))
+                # the kinetic energy after every 10th step (the FP64 sum of every step is computed)
+                ek.extend(float(e[i, 1]) for i in range(k) if (done + i + 1) % 10 == 0)
                 done += k
             f = box.fields()
             u = np.stack([f["vx"], f["vy"], f["vz"]]).astype(np.float64)
@@ -730,7 +731,7 @@ def run_tgv_forms(args):
                 rms = np.sqrt((ref[c] ** 2).sum(axis=0).mean())
                 errs[c] = {"l2_rel": float(np.sqrt((d ** 2).sum(axis=0).mean()) / rms),
                            "linf_rel": float(np.sqrt((d ** 2).sum(axis=0)).max() / np.sqrt((ref[c] ** 2).sum(axis=0)).max())}
-        out[name] = {"wall_s": round(time.perf_counter() - t0, 2), "kinetic_energy_every_100_steps": ek}
+        out[name] = {"wall_s": round(time.perf_counter() - t0, 2), "kinetic_energy_every_10_steps": ek}
         if errs:
             out[name]["velocity_error_vs_fp64"] = errs
         del box
