@@ -368,7 +368,11 @@ int vfb_simulation_set_timing(vfb_simulation *sim, int32_t on);
    enough steps remain, the rest directly. Every setter drops the graph; a run whose level
    parities differ from those at capture captures again. Not used on the legacy (NULL) stream, with
    timing on, or while a drag/lift history is kept (its per-step slot is chosen on the host).
-   Results are those of the direct loop, bit for bit. 0 (the default) turns it off. */
+   Results are those of the direct loop, bit for bit. 0 (the default) turns it off.
+   The boundary-condition and scaling functions set on the simulation run once per captured step,
+   during the capture only: what they enqueue on the stream is replayed, but their host code is not
+   run again. Functions that change host-side state from step to step, or that synchronise the
+   stream, need the graph off. The library's own functions only enqueue work. */
 int vfb_simulation_set_graph(vfb_simulation *sim, int32_t steps);
 int vfb_simulation_phase_times(vfb_simulation *sim, double *ms, uint64_t *steps, int32_t reset);
 /* parity of the coarsest level / of a given level */
