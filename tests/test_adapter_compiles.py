@@ -28,6 +28,6 @@ def test_adapter_compiles_against_reference_headers(double_accuracy):
     if double_accuracy:
         cmd.insert(2, "-DVF_DOUBLE_ACCURACY")
     r = subprocess.run(cmd, capture_output=True, text=True)
-    errors = [l for l in r.stderr.splitlines() if "error" in l and "/root/reference" not in l.split(":")[0]]
+    errors = [l for l in r.stderr.splitlines() if "error" in l and str(REF) not in l.split(":")[0]]
     assert r.returncode == 0, r.stderr[-4000:]
     assert not errors
