@@ -475,7 +475,7 @@ def run_pool_shapes(args):
     """The pool kernel against the box kernel on the same node counts: one pool each for one
     periodic 256^3 domain, 64 periodic 64^3 domains, the shapes of 1024 ducts with every node
     fluid, and the same ducts with their walls; then a Box of 256^3. FP32 and FP16 storage, the
-    pool's default launch shape (128 threads x 4 nodes, resident blocks from the occupancy API),
+    pool's default launch shape (one block of 128 threads x 8 nodes per work item),
     graph replay, CUDA events on the pool's stream. MLUPS count fluid nodes."""
     import torch
 
@@ -502,7 +502,7 @@ def run_pool_shapes(args):
         for s in shapes:
             i = pool.add(s, 1.8, periodic=periodic, mask=duct_mask(*s) if walls else None)
             pool.init(i, stream=stream)
-        pool.set_launch(128, 4, 0, True)
+        pool.set_launch(128, 8, -1, True)           # the default shape of a new pool
         pool.step(args.warmup, stream=stream)
         stream.synchronize()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
