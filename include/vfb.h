@@ -549,7 +549,7 @@ int vfb_pool_step(vfb_pool *pool, uint32_t steps, void *stream);
 /* drho, ux, uy, uz (real[nx*ny*nz]) of one domain, to host or device memory */
 int vfb_pool_domain_fields(vfb_pool *pool, uint32_t id, void *rho, void *ux, void *uy, void *uz, int32_t to_host,
                            void *stream);
-/* launch shape: threads per block (64, 128 or 256), nodes per thread per work item (1..8), resident
+/* launch shape: threads per block (64, 128 or 256), nodes per thread per work item (1..32), resident
    blocks per SM of the persistent launch (0 = as many as fit; -1 = no persistent loop: one block per
    work item, the grid following the work list, so a change of the list's length captures the step
    graph again), CUDA-graph replay (0/1); a new pool starts at 128, 8, -1, 1 */

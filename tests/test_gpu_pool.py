@@ -98,11 +98,11 @@ def test_joining_late_leaving_early_graph_and_shapes_change_nothing(cuda):
     pool.remove(b)
     pool.set_launch(threads=256, nodes_per_thread=1, use_graph=True)
     pool.step(33, stream=s)                         # graph replays (16 + 16) and one direct step
-    pool.autotune(trial_steps=2, stream=s)          # 13 shapes x 4 steps = 52 more steps
+    pool.autotune(trial_steps=2, stream=s)          # 15 shapes x 4 steps = 60 more steps
     pool.step(20, stream=s)
     s.synchronize()
-    total_a = 5 + 11 + 33 + 52 + 20
-    total_c = 11 + 33 + 52 + 20
+    total_a = 5 + 11 + 33 + 60 + 20
+    total_c = 11 + 33 + 60 + 20
     for d, (shape, periodic, omega, forces), seed, steps in ((a, DOMAINS[0], 1, total_a), (c, DOMAINS[2], 3, total_c)):
         got = pool.fields(d, stream=s)
         want = _alone(shape, periodic, omega, forces, "f32", "fast", seed, steps)

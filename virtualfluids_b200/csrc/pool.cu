@@ -912,8 +912,8 @@ int vfb_pool_set_launch(vfb_pool *p, int32_t threads, int32_t nodes_per_thread, 
         return pool_fail(VFB_ERR_INVALID_ARGUMENT, "NULL pool");
     if (threads != 64 && threads != 128 && threads != 256)
         return pool_fail(VFB_ERR_INVALID_ARGUMENT, "threads_per_block must be 64, 128 or 256");
-    if (nodes_per_thread < 1 || nodes_per_thread > 8 || blocks_per_sm < -1 || blocks_per_sm > 32)
-        return pool_fail(VFB_ERR_INVALID_ARGUMENT, "nodes_per_thread must lie in [1, 8], blocks_per_sm in [-1, 32]");
+    if (nodes_per_thread < 1 || nodes_per_thread > 32 || blocks_per_sm < -1 || blocks_per_sm > 32)
+        return pool_fail(VFB_ERR_INVALID_ARGUMENT, "nodes_per_thread must lie in [1, 32], blocks_per_sm in [-1, 32]");
     if (threads != p->threads || nodes_per_thread != p->nodes_per_thread) {
         p->list_dirty = true;
         drop_graph(p);
@@ -944,7 +944,8 @@ int vfb_pool_autotune(vfb_pool *p, uint32_t trial_steps, void *stream, double *b
     struct Shape { int t, npt, bps; };
     static const Shape kShapes[] = { { 128, 1, 0 }, { 128, 2, 0 }, { 128, 4, 0 }, { 64, 1, 0 }, { 64, 2, 0 },
                                      { 256, 1, 0 }, { 256, 2, 0 }, { 128, 1, 2 }, { 128, 2, 2 },
-                                     { 128, 4, -1 }, { 128, 8, -1 }, { 256, 4, -1 }, { 64, 8, -1 } };
+                                     { 128, 4, -1 }, { 128, 8, -1 }, { 256, 4, -1 }, { 64, 8, -1 },
+                                     { 128, 16, -1 }, { 64, 16, -1 } };
     const int graph = p->use_graph;
     cudaEvent_t a = nullptr, b = nullptr;
     cudaError_t e = cudaEventCreate(&a);

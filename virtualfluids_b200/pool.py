@@ -155,7 +155,7 @@ class Pool:
         return [a.reshape(shape[2], shape[1], shape[0]) for a in out]
 
     def set_launch(self, threads=128, nodes_per_thread=8, blocks_per_sm=-1, use_graph=True):
-        """threads per block (64, 128, 256), nodes per thread per work item (1..8), resident blocks per
+        """threads per block (64, 128, 256), nodes per thread per work item (1..32), resident blocks per
         SM of the persistent launch (0: as many as fit; -1: one block per work item, no persistent
         loop), CUDA-graph replay. Results do not depend on the shape."""
         N.check(N.lib().vfb_pool_set_launch(self._h, int(threads), int(nodes_per_thread), int(blocks_per_sm),
