@@ -386,7 +386,7 @@ def run_reference(args):
 
 def run_batch(args):
     """Batch of rectangular-duct Poiseuille domains of uneven sizes in one domain pool, advanced by
-    one persistent launch per step (CUDA-graph replay, autotuned launch shape), FP32 and FP16
+    one collision launch per step (CUDA-graph replay, autotuned launch shape), FP32 and FP16
     storage. With --check-steps S > 0 every domain also runs S steps in FP64, FP32 and FP16 and its
     x-averaged profile is compared with the analytic start-up series and with the FP64 run."""
     import torch
