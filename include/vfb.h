@@ -236,6 +236,14 @@ int vfb_drag_lift_force(const double *pre_x, const double *pre_y, const double *
    current parity. PreProcessorImp::init (PreProcessorImp.cpp:50-58) calls it for the odd, then
    the even parity. */
 int vfb_init_navier_stokes_compressible(const vfb_level *level, void *stream);
+/* The same with Parameter::getUseInitNeq() (InitNavierStokesCompressible.cu:65-83,
+   InitNavierStokesCompressibleNonEquilibrium_Device): the equilibrium plus (1 + drho) times a
+   non-equilibrium part per direction pair, formed from central differences of the velocities at the
+   six face neighbours and level->omega, for the level's current parity. neighbor_inverse is
+   neighborInverse: per node, the node at -1 in x, y and z (device memory). Solid and void nodes get
+   96 in their rest slot, as in the reference. */
+int vfb_init_navier_stokes_compressible_non_equilibrium(const vfb_level *level, const uint32_t *neighbor_inverse,
+                                                        void *stream);
 /* calculateMacroscopicQuantitiesCompressible (PostProcessor/MacroscopicQuantities.cu:194) */
 int vfb_calc_macroscopic_compressible(const vfb_level *level, void *stream);
 /* FP64 sum over the listed nodes of (1 + drho) and 0.5 (1 + drho) |u|^2, into out[2] on the host.

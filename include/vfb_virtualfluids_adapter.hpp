@@ -90,6 +90,19 @@ inline vfb_level level_of(Parameter &para, int level_index, int32_t arith = VFB_
     return L;
 }
 
+//! InitNavierStokesCompressible::init (InitNavierStokesCompressible.cu:45-84) of one level at its
+//! current parity: the non-equilibrium init from the velocity gradients when
+//! Parameter::getUseInitNeq() is set (it reads neighborInverse), else the equilibrium
+inline void init_level(Parameter &para, int level_index, int32_t arith = VFB_ARITH_EXACT)
+{
+    const vfb_level L = level_of(para, level_index, arith);
+    if (para.getUseInitNeq())
+        check(vfb_init_navier_stokes_compressible_non_equilibrium(&L, para.getParD(level_index)->neighborInverse,
+                                                                  nullptr));
+    else
+        check(vfb_init_navier_stokes_compressible(&L, nullptr));
+}
+
 //! QforBoundaryConditions (Calculation.h:105-117) as the ABI's vfb_bc
 inline vfb_bc bc_of(const QforBoundaryConditions *q)
 {

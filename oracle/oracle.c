@@ -438,6 +438,79 @@ void orc_init(orc_level *L, const uint32_t *geo, const double *rho, const double
     }
 }
 
+/* InitNavierStokesCompressibleNonEquilibrium_Device (InitNavierStokesCompressible_Device.cu:216-501):
+   the equilibrium above plus (1 + drho) times a non-equilibrium part per direction pair, from central
+   differences of the velocities at the six face neighbours (the -1 ones reached from neighborInverse,
+   the node at -1 in x, y and z, then stepped back up with neighborY/Z, neighborX/Z and neighborX/Y)
+   and omega; the equilibrium is the stored value the part is added to. Solid and void nodes get 96 in
+   their rest slot. The parts follow the reference's expressions term by term (eps and op are 1). */
+void orc_init_neq(orc_level *L, const uint32_t *geo, const uint32_t *nb_inverse, const double *rho, const double *ux,
+                  const double *uy, const double *uz, double omega, int is_even)
+{
+    int map[27];
+    orc_pointer_map(is_even, map);
+    /* the part of each direction: rest, then the pairs E, N, T, NE, SE, TE, BE, TN, BN, TNE, TSW, TSE, TNW */
+    int part_of[27];
+    {
+        const int pairs[13][2] = { { D_P00, D_M00 }, { D_0P0, D_0M0 }, { D_00P, D_00M }, { D_PP0, D_MM0 },
+                                   { D_PM0, D_MP0 }, { D_P0P, D_M0M }, { D_P0M, D_M0P }, { D_0PP, D_0MM },
+                                   { D_0PM, D_0MP }, { D_PPP, D_MMM }, { D_PPM, D_MMP }, { D_PMP, D_MPM },
+                                   { D_PMM, D_MPP } };
+        part_of[D_000] = 0;
+        for (int p = 0; p < 13; ++p)
+            part_of[pairs[p][0]] = part_of[pairs[p][1]] = p + 1;
+    }
+    for (uint64_t k = 0; k < L->n; ++k) {
+        if (geo[k] == 15u || geo[k] == 16u) {
+            L->f[(uint64_t)map[D_000] * L->n + k] = 96.0;
+            continue;
+        }
+        const uint32_t m = nb_inverse[k];
+        const uint32_t plus[3] = { L->nbx[k], L->nby[k], L->nbz[k] };
+        const uint32_t minus[3] = { L->nbz[L->nby[m]], L->nbz[L->nbx[m]], L->nby[L->nbx[m]] };
+        const double *u[3] = { ux, uy, uz };
+        double g[3][3]; /* g[i][j] = d u_i / d x_j */
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                g[i][j] = (u[i][plus[j]] - u[i][minus[j]]) / 2.0;
+        const double ax = g[0][0], ay = g[0][1], az = g[0][2];
+        const double bx = g[1][0], by = g[1][1], bz = g[1][2];
+        const double cx = g[2][0], cy = g[2][1], cz = g[2][2];
+        const double o = omega, op = 1.0, eps = 1.0;
+        double p[14];
+        p[1] = eps * ((5. * ax * o + 5. * by * o + 5. * cz * o - 8. * ax * op + 4. * by * op + 4. * cz * op) / (54. * o * op));
+        p[2] = p[1] + eps * ((2. * (ax - by)) / (9. * o));
+        p[3] = p[1] + eps * ((2. * (ax - cz)) / (9. * o));
+        p[4] = eps * (-(5. * cz * o + 3. * (ay + bx) * op - 2. * cz * op + ax * (5. * o + op) + by * (5. * o + op))
+                      / (54. * o * op));
+        p[5] = p[4] + eps * ((ay + bx) / (9. * o));
+        p[6] = eps * (-(5. * cz * o + by * (5. * o - 2. * op) + 3. * (az + cx) * op + cz * op + ax * (5. * o + op))
+                      / (54. * o * op));
+        p[7] = p[6] + eps * ((az + cx) / (9. * o));
+        p[8] = eps * (-(5. * ax * o + 5. * by * o + 5. * cz * o - 2. * ax * op + by * op + 3. * bz * op + 3. * cy * op
+                        + cz * op) / (54. * o * op));
+        p[9] = p[8] + eps * ((bz + cy) / (9. * o));
+        p[0] = eps * ((5. * (ax + by + cz)) / (9. * op));
+        p[10] = eps * (-(ay + az + bx + bz + cx + cy) / (72. * o));
+        p[11] = -p[10] - eps * ((ay + bx) / (36. * o));
+        p[12] = -p[10] - eps * ((az + cx) / (36. * o));
+        p[13] = -p[10] - eps * ((bz + cy) / (36. * o));
+        const double drho = rho[k], vx = ux[k], vy = uy[k], vz = uz[k];
+        const double cu_sq = 1.5 * (vx * vx + vy * vy + vz * vz);
+        for (int d = 0; d < 27; ++d) {
+            double v;
+            if (d == D_000) {
+                v = ORC_W[0] * (drho - cu_sq * (1.0 + drho));
+            } else {
+                const double cu = signed_sum(d, vx, vy, vz);
+                v = ORC_W[d] * (drho + (1.0 + drho) * (3.0 * cu + 4.5 * cu * cu - cu_sq));
+            }
+            v = v + (1.0 + drho) * p[part_of[d]];
+            write_pre_dir(L, (uint32_t)k, map, d, v);
+        }
+    }
+}
+
 /* getPressure (MacroscopicQuantities.h:139) */
 static double pressure_of(const double *f, double rho, double vx, double vy, double vz)
 {

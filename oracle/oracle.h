@@ -83,6 +83,10 @@ void orc_bc_pressure_neq(orc_level *L, const int32_t *k, const int32_t *kN, cons
 /* InitNavierStokesCompressible_Device.cu:44-215 for one parity; geo: skip 15 (solid) and 16 (void) */
 void orc_init(orc_level *L, const uint32_t *geo, const double *rho, const double *ux, const double *uy,
               const double *uz, int is_even);
+/* InitNavierStokesCompressible_Device.cu:216-501 (the non-equilibrium init) for one parity; nb_inverse
+   is neighborInverse (the node at -1 in x, y and z); solid and void nodes get 96 in their rest slot */
+void orc_init_neq(orc_level *L, const uint32_t *geo, const uint32_t *nb_inverse, const double *rho, const double *ux,
+                  const double *uy, const double *uz, double omega, int is_even);
 /* MacroscopicQuantities.cu:194 compressible macros (rho, vx, vy, vz, pressure) for geo == 19 nodes */
 void orc_macros(const orc_level *L, const uint32_t *geo, int is_even, double *rho, double *vx, double *vy,
                 double *vz, double *press);

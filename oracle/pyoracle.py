@@ -57,6 +57,8 @@ def lib():
         L.orc_bc_velocity_interpolated.argtypes = [_P, _P, _P, u, i, d, _P, _P, _P]
         L.orc_bc_pressure_neq.argtypes = [_P, _P, _P, _P, u, i, i]
         L.orc_init.argtypes = [_P, _P, _P, _P, _P, _P, i]
+        L.orc_init_neq.argtypes = [_P, _P, _P, _P, _P, _P, _P, d, i]
+        L.orc_read_pre.argtypes = [_P, u, i, _P]
         L.orc_macros.argtypes = [_P, _P, i, _P, _P, _P, _P, _P]
         L.orc_mass_energy.argtypes = [_P, _P, u, i, _P]
         L.orc_interp_node_moments.argtypes = [_P, d, _P]
@@ -217,11 +219,18 @@ class OracleLevel:
         self.pr = (_Pressure * max(len(pr), 1))(*pr) if pr else None
         self.n_pr = len(pr)
 
-    def init(self, rho=None, ux=None, uy=None, uz=None):
+    def init(self, rho=None, ux=None, uy=None, uz=None, neq=False):
+        """PreProcessorImp::init: the odd, then the even parity; neq: the non-equilibrium init
+        (Parameter::setUseInitNeq), which reads the grid's neighborInverse."""
         z = np.zeros(self.n)
         arrs = [np.ascontiguousarray(a if a is not None else z, dtype=np.float64) for a in (rho, ux, uy, uz)]
-        lib().orc_init(C.byref(self.L), ptr(self.geo), *(ptr(a) for a in arrs), 0)
-        lib().orc_init(C.byref(self.L), ptr(self.geo), *(ptr(a) for a in arrs), 1)
+        if neq:
+            inv = np.ascontiguousarray(self.grid.neighbor_inverse, dtype=np.uint32)
+            for ev in (0, 1):
+                lib().orc_init_neq(C.byref(self.L), ptr(self.geo), ptr(inv), *(ptr(a) for a in arrs), self.omega, ev)
+        else:
+            lib().orc_init(C.byref(self.L), ptr(self.geo), *(ptr(a) for a in arrs), 0)
+            lib().orc_init(C.byref(self.L), ptr(self.geo), *(ptr(a) for a in arrs), 1)
         self.is_even.value = 1
 
     def run(self, steps, threads=0):
@@ -267,6 +276,12 @@ class OracleLevel:
                 else:
                     raise ValueError("no-slip BC kind not covered")
             self.is_even.value = 1 - ev
+
+    def pre(self, k):
+        """The 27 pre-collision populations f - w of node k at the current parity (getPreCollisionDistribution)."""
+        out = np.zeros(27)
+        lib().orc_read_pre(C.byref(self.L), int(k), self.is_even.value, ptr(out))
+        return out
 
     def macroscopic(self):
         out = [np.zeros(self.n) for _ in range(5)]

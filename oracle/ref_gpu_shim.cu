@@ -236,6 +236,14 @@ int refgpu_init(unsigned *nbx, unsigned *nby, unsigned *nbz, unsigned *geo, real
     return done();
 }
 
+int refgpu_init_neq(unsigned *nbx, unsigned *nby, unsigned *nbz, unsigned *nb_inverse, unsigned *geo, real *rho,
+                    real *ux, real *uy, real *uz, unsigned n, real *dist, real omega, int is_even)
+{
+    InitNavierStokesCompressibleNonEquilibrium_Device<<<blocks_for(n), kThreads>>>(
+        nbx, nby, nbz, nb_inverse, geo, rho, ux, uy, uz, n, dist, omega, is_even != 0);
+    return done();
+}
+
 int refgpu_macros(real *vx, real *vy, real *vz, real *rho, real *press, unsigned *geo, unsigned *nbx, unsigned *nby,
                   unsigned *nbz, uint64_t n, real *dist, int is_even)
 {

@@ -48,4 +48,5 @@ void adapter_compile_check(std::shared_ptr<Parameter> para)
     (void)cf;
     vfb_level L = vfb_adapter::level_of(*para, 0);
     (void)L;
+    vfb_adapter::init_level(*para, 0);
 }

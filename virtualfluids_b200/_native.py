@@ -161,6 +161,7 @@ SIGNATURES = {
     "vfb_velocity_interpolated_incompressible": (C.c_int, [C.POINTER(Level), C.POINTER(BC), C.c_void_p]),
     "vfb_velocity_with_pressure_interpolated_compressible": (C.c_int, [C.POINTER(Level), C.POINTER(BC), C.c_void_p]),
     "vfb_init_navier_stokes_compressible": (C.c_int, [C.POINTER(Level), C.c_void_p]),
+    "vfb_init_navier_stokes_compressible_non_equilibrium": (C.c_int, [C.POINTER(Level), C.c_void_p, C.c_void_p]),
     "vfb_calc_macroscopic_compressible": (C.c_int, [C.POINTER(Level), C.c_void_p]),
     "vfb_mass_energy_workspace_bytes": (C.c_size_t, [C.c_uint32]),
     "vfb_mass_energy": (C.c_int, [C.POINTER(Level), C.c_void_p, C.c_uint32, C.c_void_p, C.c_size_t, C.c_void_p,

@@ -541,6 +541,21 @@ int vfb_init_navier_stokes_compressible(const vfb_level *level, void *stream)
     return cuda_status(e, "InitNavierStokesCompressible launch");
 }
 
+int vfb_init_navier_stokes_compressible_non_equilibrium(const vfb_level *level, const uint32_t *neighbor_inverse,
+                                                        void *stream)
+{
+    int st = check_level(level);
+    if (st)
+        return st;
+    if (!level->type_of_grid_node || !level->rho || !level->velocity_x || !level->velocity_y || !level->velocity_z)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "init needs typeOfGridNode, rho and velocities");
+    if (!neighbor_inverse)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "the non-equilibrium init needs neighborInverse");
+    const cudaError_t e =
+        VFB_DISPATCH(level->storage, level->arith, LA::init_neq_list(level, neighbor_inverse, as_stream(stream)));
+    return cuda_status(e, "InitNavierStokesCompressibleNonEquilibrium launch");
+}
+
 int vfb_calc_macroscopic_compressible(const vfb_level *level, void *stream)
 {
     int st = check_level(level);

@@ -1370,6 +1370,100 @@ __global__ void __launch_bounds__(128) init_list_kernel(void *dist, uint64_t n, 
     }
 }
 
+// The non-equilibrium parts of InitNavierStokesCompressibleNonEquilibrium_Device
+// (InitNavierStokesCompressible_Device.cu:216-501), from the central-difference velocity gradients
+// a = grad ux, b = grad uy, c = grad uz and omega, as 14 coefficients shared by opposite directions:
+// 0 rest, 1 P00/M00, 2 0P0/0M0, 3 00P/00M, 4 PP0/MM0, 5 PM0/MP0, 6 P0P/M0M, 7 P0M/M0P, 8 0PP/0MM,
+// 9 0PM/0MP, 10 PPP/MMM, 11 PPM/MMP, 12 PMP/MPM, 13 PMM/MPP. Every operation keeps the reference's
+// order and types: its constants are double literals, so with real = float each coefficient is
+// formed in double from float operands (float where both operands of a product or sum are float)
+// and rounded to float once; the scale eps and the factor op are real 1.
+template <class C>
+__device__ __forceinline__ void init_neq_parts(C ax, C ay, C az, C bx, C by, C bz, C cx, C cy, C cz, C omega,
+                                               C (&p)[14])
+{
+    const C eps = C(1), op = C(1), o = omega;
+    p[1] = (C)(eps * ((5. * ax * o + 5. * by * o + 5. * cz * o - 8. * ax * op + 4. * by * op + 4. * cz * op)
+                      / (54. * o * op)));
+    p[2] = (C)(p[1] + eps * ((2. * (ax - by)) / (9. * o)));
+    p[3] = (C)(p[1] + eps * ((2. * (ax - cz)) / (9. * o)));
+    p[4] = (C)(eps * (-(5. * cz * o + 3. * (ay + bx) * op - 2. * cz * op + ax * (5. * o + op) + by * (5. * o + op))
+                      / (54. * o * op)));
+    p[5] = (C)(p[4] + eps * ((ay + bx) / (9. * o)));
+    p[6] = (C)(eps * (-(5. * cz * o + by * (5. * o - 2. * op) + 3. * (az + cx) * op + cz * op + ax * (5. * o + op))
+                      / (54. * o * op)));
+    p[7] = (C)(p[6] + eps * ((az + cx) / (9. * o)));
+    p[8] = (C)(eps * (-(5. * ax * o + 5. * by * o + 5. * cz * o - 2. * ax * op + by * op + 3. * bz * op + 3. * cy * op
+                        + cz * op)
+                      / (54. * o * op)));
+    p[9] = (C)(p[8] + eps * ((bz + cy) / (9. * o)));
+    p[0] = (C)(eps * ((5. * (ax + by + cz)) / (9. * op)));
+    p[10] = (C)(eps * (-(ay + az + bx + bz + cx + cy) / (72. * o)));
+    p[11] = (C)(-p[10] - eps * ((ay + bx) / (36. * o)));
+    p[12] = (C)(-p[10] - eps * ((az + cx) / (36. * o)));
+    p[13] = (C)(-p[10] - eps * ((bz + cy) / (36. * o)));
+}
+// the coefficient of direction d (D3Q27 numbering of lattice.cuh)
+__host__ __device__ constexpr int init_neq_part_of(int d)
+{
+    constexpr int8_t t[27] = { 0, 1, 1, 2, 2, 3, 3, 4, 4, 5, 5, 6, 6, 7, 7, 8, 8, 9, 9, 10, 13, 12, 11, 11, 12, 13, 10 };
+    return t[d];
+}
+
+// InitNavierStokesCompressibleNonEquilibrium_Device: the equilibrium of init_list_kernel plus
+// (1 + drho) times the direction's non-equilibrium part, from the velocities of the six face
+// neighbours (the -1 ones reached from neighborInverse, the node at -1 in x, y and z). The
+// equilibrium is rounded to the storage's real type before the part is added, as the reference
+// stores it and then adds; the 16-bit forms encode the sum once. Solid and void nodes get 96 in
+// their rest slot, as the reference writes there.
+template <class S, bool EVEN>
+__global__ void __launch_bounds__(128) init_neq_list_kernel(void *dist, uint64_t n, const uint32_t *nbx,
+                                                            const uint32_t *nby, const uint32_t *nbz,
+                                                            const uint32_t *nb_inverse, const uint32_t *geo,
+                                                            const void *rho, const void *ux, const void *uy,
+                                                            const void *uz, typename Codec<S>::compute omega)
+{
+    using C = typename Codec<S>::compute;
+    const uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (k >= n)
+        return;
+    S *base = static_cast<S *>(dist);
+    const uint32_t g = geo[k];
+    if (g == kGeoSolid || g == kGeoVoid) {
+        Codec<S>::store_at(base, (uint64_t)plane<EVEN>(0) * n + k, C(96), 0);
+        return;
+    }
+    uint32_t nodes[8];
+    list_nodes((uint32_t)k, nbx, nby, nbz, n, nodes);
+    const C *U = static_cast<const C *>(ux), *V = static_cast<const C *>(uy), *W = static_cast<const C *>(uz);
+    const C drho = static_cast<const C *>(rho)[k];
+    const C vx = U[k], vy = V[k], vz = W[k];
+    // face neighbours: +1 from the neighbour lists, -1 from the -1/-1/-1 node stepped back up
+    const uint32_t px = VFB_NODE(nbx[k], n), py = VFB_NODE(nby[k], n), pz = VFB_NODE(nbz[k], n);
+    const uint32_t mxyz = VFB_NODE(nb_inverse[k], n);
+    const uint32_t mx = VFB_NODE(nbz[VFB_NODE(nby[mxyz], n)], n);
+    const uint32_t my = VFB_NODE(nbz[VFB_NODE(nbx[mxyz], n)], n);
+    const uint32_t mz = VFB_NODE(nby[VFB_NODE(nbx[mxyz], n)], n);
+    const C ax = (U[px] - U[mx]) / C(2), ay = (U[py] - U[my]) / C(2), az = (U[pz] - U[mz]) / C(2);
+    const C bx = (V[px] - V[mx]) / C(2), by = (V[py] - V[my]) / C(2), bz = (V[pz] - V[mz]) / C(2);
+    const C cx = (W[px] - W[mx]) / C(2), cy = (W[py] - W[my]) / C(2), cz = (W[pz] - W[mz]) / C(2);
+    C part[14];
+    init_neq_parts<C>(ax, ay, az, bx, by, bz, cx, cy, cz, omega, part);
+    const C cu_sq = C(1.5) * (vx * vx + vy * vy + vz * vz);
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        C v;
+        if (d == 0) {
+            v = weight_t<C>(0) * (drho - cu_sq * (C(1) + drho));
+        } else {
+            const C cu = cdot_rt<C>(d, vx, vy, vz);
+            v = weight_t<C>(d) * (drho + (C(1) + drho) * (C(3) * cu + C(4.5) * cu * cu - cu_sq));
+        }
+        v = v + (C(1) + drho) * part[init_neq_part_of(d)];
+        Codec<S>::store_at(base, (uint64_t)plane<EVEN>(d) * n + nodes[shift_class(d)], v, d);
+    }
+}
+
 // the same equilibrium initialisation on a structured box (every node, or the masked ones)
 template <class S, bool EVEN>
 __global__ void __launch_bounds__(128) init_box_kernel(BoxCollideArgs<typename Codec<S>::compute> a, const void *rho,

@@ -87,6 +87,7 @@ struct PoolDomainSpec {
         static cudaError_t inlet_perturbation(const void *base, void *vel, uint32_t n, uint64_t seed,                \
                                               uint64_t step, double amplitude, cudaStream_t s);                      \
         static cudaError_t init_list(const vfb_level *L, cudaStream_t s);                                          \
+        static cudaError_t init_neq_list(const vfb_level *L, const uint32_t *nb_inverse, cudaStream_t s);          \
         static cudaError_t macros_list(const vfb_level *L, cudaStream_t s);                                        \
         static cudaError_t energy_list(const vfb_level *L, const uint32_t *idx, uint32_t n, double *partials,     \
                                        cudaStream_t s);                                                            \

@@ -473,6 +473,23 @@ cudaError_t Launchers<S>::init_list(const vfb_level *L, cudaStream_t s)
 }
 
 template <class S>
+cudaError_t Launchers<S>::init_neq_list(const vfb_level *L, const uint32_t *nb_inverse, cudaStream_t s)
+{
+    using C = typename Codec<S>::compute;
+    const unsigned B = 128, G = grid1d(L->number_of_nodes, B);
+    const C omega = (C)L->omega;
+    if (L->is_even_timestep)
+        init_neq_list_kernel<S, true><<<G, B, 0, s>>>(L->distributions, L->number_of_nodes, L->neighbor_x,
+                                                      L->neighbor_y, L->neighbor_z, nb_inverse, L->type_of_grid_node,
+                                                      L->rho, L->velocity_x, L->velocity_y, L->velocity_z, omega);
+    else
+        init_neq_list_kernel<S, false><<<G, B, 0, s>>>(L->distributions, L->number_of_nodes, L->neighbor_x,
+                                                       L->neighbor_y, L->neighbor_z, nb_inverse, L->type_of_grid_node,
+                                                       L->rho, L->velocity_x, L->velocity_y, L->velocity_z, omega);
+    return cudaGetLastError();
+}
+
+template <class S>
 cudaError_t Launchers<S>::macros_list(const vfb_level *L, cudaStream_t s)
 {
     const unsigned B = 128, G = grid1d(L->number_of_nodes, B);

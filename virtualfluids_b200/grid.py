@@ -107,6 +107,32 @@ class ListGrid:
         self.neighbor = nb
         self._bc_sides_set = []
 
+    @property
+    def neighbor_inverse(self) -> np.ndarray:
+        """neighborInverse (uint32 [n]): per node the node at -1 in x, y and z, wrapping on periodic
+        axes; 0 (the dummy node) where there is none. Made on first use."""
+        inv = getattr(self, "_neighbor_inverse", None)
+        if inv is None:
+            Dx, Dy, Dz = self.dims
+            n_grid = Dx * Dy * Dz
+            g0 = self.first_node
+            i = np.arange(n_grid, dtype=np.int64)
+            g = [i % Dx, (i // Dx) % Dy, i // (Dx * Dy)]
+            ok = np.ones(n_grid, dtype=bool)
+            prev = []
+            for a in range(3):
+                p = g[a] - 1
+                if self.periodic[a]:
+                    p = np.where(p < 0, self.dims[a] - 1, p)
+                else:
+                    ok &= p >= 0
+                prev.append(p)
+            idx = prev[0] + Dx * (prev[1] + Dy * prev[2]) + g0
+            inv = np.zeros(self.number_of_nodes, dtype=np.uint32)
+            inv[g0:g0 + n_grid] = np.where(ok, idx, 0).astype(np.uint32)
+            self._neighbor_inverse = inv
+        return inv
+
     # -- indexing ----------------------------------------------------------------------------
     def node_index(self, x, y, z):
         """Node index of fluid-box coordinates (shell allowed on non-periodic axes)."""

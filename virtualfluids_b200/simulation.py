@@ -56,6 +56,7 @@ class Parameter:
         self.storage = N.STORAGE_F64
         self.arith = N.ARITH_FAST
         self.outflow_pressure_correction_factor = 0.0
+        self.use_init_neq = False
 
     def set_viscosity_lb(self, nu: float):
         self.viscosity_lb = float(nu)
@@ -71,6 +72,11 @@ class Parameter:
 
     def set_quadric_limiters(self, p: float, m: float, d: float):
         self.quadric_limiters = (float(p), float(m), float(d))
+
+    def set_use_init_neq(self, use: bool):
+        """Parameter::setUseInitNeq: Simulation.init adds the non-equilibrium part from the velocity
+        gradients to the equilibrium (InitNavierStokesCompressibleNonEquilibrium_Device)."""
+        self.use_init_neq = bool(use)
 
     def set_outflow_pressure_correction_factor(self, factor: float):
         """Parameter::setOutflowPressureCorrectionFactor (OutflowNonReflectivePressureCorrection)."""
@@ -93,8 +99,8 @@ class Parameter:
         """A Parameter from a configuration file of the reference (basics/config/ConfigurationFile
         read by Parameter::readConfigData, Parameter.cpp:80-300): the keys of this path --
         Viscosity_LB, Velocity_LB, ForcingX/Y/Z (0 when absent), QuadricLimiterP/M/D (0.01 when
-        absent) and MainKernelName -- with the reference's meaning. Every key of the file stays
-        readable in ``config`` (strings)."""
+        absent), UseInitNeq and MainKernelName -- with the reference's meaning. Every key of the file
+        stays readable in ``config`` (strings)."""
         cfg = load_configuration_file(path)
         p = cls()
         p.config = cfg
@@ -105,6 +111,8 @@ class Parameter:
         p.set_forcing(*(float(cfg.get(k, 0.0)) for k in ("ForcingX", "ForcingY", "ForcingZ")))
         p.set_quadric_limiters(*(float(cfg.get(k, 0.01)) for k in ("QuadricLimiterP", "QuadricLimiterM",
                                                                      "QuadricLimiterD")))
+        if "UseInitNeq" in cfg:
+            p.set_use_init_neq(config_bool(cfg["UseInitNeq"]))
         if "MainKernelName" in cfg:
             p.configure_main_kernel(cfg["MainKernelName"])
         return p
@@ -297,6 +305,17 @@ def _ptr(t):
 class _LevelState:
     """Device arrays of one level (LBMSimulationParameter of that level) and its BC lists."""
 
+    def neighbor_inverse_device(self):
+        """neighborInverse of the level's grid on the device, uploaded on first use."""
+        inv = getattr(self, "_nb_inv", None)
+        if inv is None:
+            host = getattr(self.grid, "neighbor_inverse", None)
+            if host is None:
+                raise ValueError("the non-equilibrium init needs the grid's neighborInverse")
+            inv = _torch().from_numpy(np.asarray(host).astype(np.int32)).to(self.dist.device)
+            self._nb_inv = inv
+        return inv
+
     def __init__(self, para: Parameter, grid: ListGrid, level: int, device):
         t = _torch()
         self.grid = grid
@@ -421,7 +440,9 @@ class Simulation:
             pass
 
     def init(self, rho=None, vx=None, vy=None, vz=None, level=0):
-        """PreProcessorImp::init of one level: equilibrium for the odd, then the even parity; starts even."""
+        """PreProcessorImp::init of one level: equilibrium for the odd, then the even parity; starts even.
+        With Parameter.use_init_neq the non-equilibrium part from the velocity gradients is added
+        (InitNavierStokesCompressibleNonEquilibrium_Device; the grid's neighborInverse is needed)."""
         t = _torch()
         S = self.levels[level]
         rd = real_dtype(self.para.storage)
@@ -431,10 +452,15 @@ class Simulation:
             else:
                 dst.copy_(t.as_tensor(np.asarray(arr), dtype=rd))
         L = S.level
+        if self.para.use_init_neq:
+            inv = S.neighbor_inverse_device()
+            init = lambda: N.lib().vfb_init_navier_stokes_compressible_non_equilibrium(C.byref(L), _ptr(inv), None)
+        else:
+            init = lambda: N.lib().vfb_init_navier_stokes_compressible(C.byref(L), None)
         L.is_even_timestep = 0
-        N.check(N.lib().vfb_init_navier_stokes_compressible(C.byref(L), None))
+        N.check(init())
         L.is_even_timestep = 1
-        N.check(N.lib().vfb_init_navier_stokes_compressible(C.byref(L), None))
+        N.check(init())
         N.check(N.lib().vfb_simulation_use_level(self._sim, level))
         N.check(N.lib().vfb_simulation_set_level(self._sim, C.byref(L), _ptr(S.fluid), int(S.grid.fluid.size)))
         N.check(N.lib().vfb_simulation_use_level(self._sim, 0))
