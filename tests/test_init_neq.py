@@ -41,6 +41,14 @@ def test_neighbor_inverse_steps_back_to_the_node():
         assert inv[0] == 0
 
 
+def test_inverse_neighbours_from_the_plus_one_lists():
+    """Imported grids without neighborInverse get it from the +1 lists: the same as the box's own."""
+    from virtualfluids_b200.grid import inverse_neighbors
+    for periodic in ((True, True, True), (False, True, False), (False, False, False)):
+        g = ListGrid(6, 5, 4, periodic=periodic)
+        assert np.array_equal(inverse_neighbors(g.neighbor)[g.fluid], g.neighbor_inverse[g.fluid])
+
+
 def test_neq_init_keeps_density_and_velocity(oracle):
     for periodic in ((True, True, True), (False, True, False)):
         g = ListGrid(12, 10, 8, periodic=periodic)

@@ -51,6 +51,22 @@ class SideBC:
     k_neighbor: np.ndarray | None = None
 
 
+def inverse_neighbors(neighbor: np.ndarray) -> np.ndarray:
+    """neighborInverse from the +1 neighbour lists (uint32 [3, n]) of any grid: the node m whose +x,
+    then +y, then +z neighbour is k becomes inv[k]. Chains that end at the dummy node 0 are dropped,
+    and nodes that no chain reaches keep 0."""
+    nbx, nby, nbz = (np.asarray(neighbor[a], dtype=np.int64) for a in range(3))
+    n = nbx.size
+    m = np.arange(1, n, dtype=np.int64)
+    a = nbx[m]
+    b = np.where(a != 0, nby[a], 0)
+    target = np.where(b != 0, nbz[b], 0)
+    ok = target != 0
+    inv = np.zeros(n, dtype=np.uint32)
+    inv[target[ok]] = m[ok].astype(np.uint32)
+    return inv
+
+
 @dataclass
 class ListGrid:
     """One level of a fluid box nx*ny*nz in the reference layout (see module docstring)."""

@@ -310,8 +310,9 @@ class _LevelState:
         inv = getattr(self, "_nb_inv", None)
         if inv is None:
             host = getattr(self.grid, "neighbor_inverse", None)
-            if host is None:
-                raise ValueError("the non-equilibrium init needs the grid's neighborInverse")
+            if host is None:                      # an imported grid without it: from the +1 lists
+                from .grid import inverse_neighbors
+                host = inverse_neighbors(self.grid.neighbor)
             inv = _torch().from_numpy(np.asarray(host).astype(np.int32)).to(self.dist.device)
             self._nb_inv = inv
         return inv
