@@ -167,6 +167,10 @@ int vfb_noslip_interpolated_compressible(const vfb_level *level, const vfb_bc *b
 int vfb_velocity_bounce_back(const vfb_level *level, const vfb_bc *bc, void *stream);
 /* VelocityInterpolatedCompressible (Velocity/Velocity.cu:87) */
 int vfb_velocity_interpolated_compressible(const vfb_level *level, const vfb_bc *bc, void *stream);
+/* SlipCompressible (BoundaryConditions/Slip/Slip.cu:42, SlipCompressible_Device): the interpolated
+   velocity BC whose wall velocity is the node's own velocity, with the x (y, z) component zeroed when
+   the node's P00 or M00 (0P0 or 0M0, 00P or 00M) link is cut; no wall velocities are read */
+int vfb_slip_compressible(const vfb_level *level, const vfb_bc *bc, void *stream);
 /* PressureNonEquilibriumCompressible (BoundaryConditions/Pressure/Pressure.cu:63) */
 int vfb_pressure_non_equilibrium_compressible(const vfb_level *level, const vfb_directional_bc *bc, void *stream);
 /* PressureNonEquilibriumIncompressible (Pressure/Pressure.cu:43) */
@@ -274,6 +278,8 @@ enum { VFB_VELOCITY_BOUNCE_BACK = 0, VFB_VELOCITY_INTERPOLATED_INCOMPRESSIBLE = 
        VFB_VELOCITY_WITH_PRESSURE_INTERPOLATED_COMPRESSIBLE = 3, VFB_VELOCITY_NOT_SPECIFIED = 4 };
 enum { VFB_NOSLIP_DELAY_BOUNCE_BACK = 0, VFB_NOSLIP_BOUNCE_BACK = 1, VFB_NOSLIP_INTERPOLATED_INCOMPRESSIBLE = 2,
        VFB_NOSLIP_INTERPOLATED_COMPRESSIBLE = 3 };
+/* SlipBC (BoundaryConditionFactory.h:87-94) */
+enum { VFB_SLIP_COMPRESSIBLE = 0, VFB_SLIP_TURBULENT_VISCOSITY_COMPRESSIBLE = 1, VFB_SLIP_NOT_SPECIFIED = 2 };
 enum { VFB_PRESSURE_NON_EQUILIBRIUM_INCOMPRESSIBLE = 0, VFB_PRESSURE_NON_EQUILIBRIUM_COMPRESSIBLE = 1,
        VFB_PRESSURE_OUTFLOW_NON_REFLECTIVE = 2, VFB_PRESSURE_OUTFLOW_NON_REFLECTIVE_PRESSURE_CORRECTION = 3,
        VFB_PRESSURE_NOT_SPECIFIED = 4 };
@@ -282,6 +288,9 @@ enum { VFB_PRESSURE_NON_EQUILIBRIUM_INCOMPRESSIBLE = 0, VFB_PRESSURE_NON_EQUILIB
    node; NotSpecified). A value outside the enum gives VFB_ERR_INVALID_ARGUMENT. */
 int vfb_bc_factory_velocity(int32_t variant, vfb_bc_fn *fn);
 int vfb_bc_factory_noslip(int32_t variant, vfb_bc_fn *fn);
+/* SlipCompressible -> vfb_slip_compressible; NotSpecified -> NULL; SlipTurbulentViscosityCompressible
+   (it needs a turbulence model, outside this path) -> VFB_ERR_UNSUPPORTED */
+int vfb_bc_factory_slip(int32_t variant, vfb_bc_fn *fn);
 int vfb_bc_factory_pressure(int32_t variant, vfb_directional_bc_fn *fn);
 
 /* ---- grid-scaling factory (GridScaling/GridScalingFactory.h:47-66) ----------------------- */
@@ -334,10 +343,17 @@ int vfb_simulation_set_interpolation_cells(vfb_simulation *sim, int32_t coarse_l
 /* BC lists of the selected level (copied descriptors) and factory choices */
 int vfb_simulation_set_velocity_bc(vfb_simulation *sim, const vfb_bc *bc, int32_t variant);
 int vfb_simulation_set_noslip_bc(vfb_simulation *sim, const vfb_bc *bc, int32_t variant);
+/* the slip BC list (slipBC, a SlipBC value); it runs after the no-slip BC and before the geometry BC,
+   as runSlipBCKernelPost (UpdateGrid27.cpp:240) */
+int vfb_simulation_set_slip_bc(vfb_simulation *sim, const vfb_bc *bc, int32_t variant);
 int vfb_simulation_add_pressure_bc(vfb_simulation *sim, const vfb_directional_bc *bc, int32_t variant);
 /* the geometry BC list (BoundaryConditionFactory::setGeometryBoundaryCondition with a NoSlipBC
    value); it runs after the no-slip BC, as runGeoBCKernelPost (UpdateGrid27.cpp:247-248) */
 int vfb_simulation_set_geometry_bc(vfb_simulation *sim, const vfb_bc *bc, int32_t variant);
+/* the same with the variant's family, as setGeometryBoundaryCondition takes a VelocityBC, NoSlipBC or
+   SlipBC value (BoundaryConditionFactory.cpp:206-216); a velocity family needs the list's velocities */
+enum { VFB_GEOMETRY_VELOCITY = 0, VFB_GEOMETRY_NOSLIP = 1, VFB_GEOMETRY_SLIP = 2 };
+int vfb_simulation_set_geometry_bc_of(vfb_simulation *sim, const vfb_bc *bc, int32_t family, int32_t variant);
 /* drag and lift on the geometry nodes every step (Parameter::setCalcDragLift): DragLiftPost27 before
    the geometry BC, DragLiftPre27 and the FP64 sum after the parity swap, the force of step t into
    force_history[3 * (t % history_steps)] (device, no host synchronisation). Caller-owned device

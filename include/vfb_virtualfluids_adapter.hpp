@@ -230,6 +230,16 @@ inline boundaryCondition noslip_bc(BoundaryConditionFactory::NoSlipBC v, int32_t
     return nullptr;
 }
 
+//! getSlipBoundaryConditionPost for each SlipBC value (not virtual in the reference: its switch in
+//! BoundaryConditionFactory.cpp returns slip_bc(...)); the turbulent-viscosity form stays the
+//! reference's, as it reads the turbulence model's viscosity
+inline boundaryCondition slip_bc(BoundaryConditionFactory::SlipBC v, int32_t arith = VFB_ARITH_EXACT)
+{
+    if (v == BoundaryConditionFactory::SlipBC::SlipCompressible)
+        return bind_bc(vfb_slip_compressible, arith);
+    return nullptr;
+}
+
 //! getPressureBoundaryConditionPre for each PressureBC value (the directional form every
 //! implemented pressure kernel takes). The outflow with pressure correction reads its factor from
 //! the level view, so it binds the Parameter.

@@ -376,6 +376,40 @@ void orc_bc_velocity_interpolated(orc_level *L, const int32_t *k, const double *
     free(all);
 }
 
+/* SlipCompressible_Device (Slip/SlipCompressible.cu:44-550): the interpolated velocity BC above with
+   the node's own velocity as the wall velocity (slip length 1), except that the component along an
+   axis is zero when the node's link along that axis, either way, is cut. The reference visits the six
+   axis links first and zeroes the component there, so every diagonal link sees all three. */
+void orc_bc_slip(orc_level *L, const int32_t *k, const double *q27, uint32_t nbc, int is_even, double omega)
+{
+    int map_next[27];
+    orc_pointer_map(!is_even, map_next);
+    double *all = read_posts(L, k, nbc, is_even);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+    for (int64_t i = 0; i < (int64_t)nbc; ++i) {
+        const uint32_t node = (uint32_t)k[i];
+        const double *post = all + 27 * (size_t)i;
+        double drho, vx, vy, vz, cu_sq;
+        bc_macros(post, &drho, &vx, &vy, &vz, &cu_sq);
+        const int cut_x = q_active(q27[(uint64_t)D_P00 * nbc + i]) || q_active(q27[(uint64_t)D_M00 * nbc + i]);
+        const int cut_y = q_active(q27[(uint64_t)D_0P0 * nbc + i]) || q_active(q27[(uint64_t)D_0M0 * nbc + i]);
+        const int cut_z = q_active(q27[(uint64_t)D_00P * nbc + i]) || q_active(q27[(uint64_t)D_00M * nbc + i]);
+        const double wx = cut_x ? 0.0 : vx, wy = cut_y ? 0.0 : vy, wz = cut_z ? 0.0 : vz;
+        for (int d = 1; d < 27; ++d) {
+            const double q = q27[(uint64_t)d * nbc + i];
+            if (!q_active(q))
+                continue;
+            const double feq = feq_bc(drho, signed_sum(d, vx, vy, vz), cu_sq, ORC_W[d]);
+            const double vbc = signed_sum(d, wx, wy, wz);
+            write_pre_dir(L, node, map_next, ORC_INV[d],
+                          interp_velocity(q, post[d], post[ORC_INV[d]], feq, omega, vbc, ORC_W[d]));
+        }
+    }
+    free(all);
+}
+
 /* feq - w for one direction in the form of the pressure/init kernels: w (drho + (drho+1)(3cu + 4.5cu^2 - cusq)) */
 static inline double feq_dir(int d, double drho, double vx, double vy, double vz, double cusq)
 {

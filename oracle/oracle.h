@@ -77,6 +77,9 @@ void orc_bc_velocity_bounce_back(orc_level *L, const int32_t *k, const double *q
                                  const double *ux, const double *uy, const double *uz);
 void orc_bc_velocity_interpolated(orc_level *L, const int32_t *k, const double *q27, uint32_t nbc, int is_even,
                                   double omega, const double *ux, const double *uy, const double *uz);
+/* SlipCompressible (Slip/SlipCompressible.cu:44-550): the interpolated velocity BC with the node's own
+   velocity as the wall velocity, its component along an axis zeroed where that axis's links are cut */
+void orc_bc_slip(orc_level *L, const int32_t *k, const double *q27, uint32_t nbc, int is_even, double omega);
 void orc_bc_pressure_neq(orc_level *L, const int32_t *k, const int32_t *kN, const double *rho_bc, uint32_t nbc,
                          int is_even, int direction);
 

@@ -59,6 +59,7 @@ def lib():
         L.orc_init.argtypes = [_P, _P, _P, _P, _P, _P, i]
         L.orc_init_neq.argtypes = [_P, _P, _P, _P, _P, _P, _P, d, i]
         L.orc_read_pre.argtypes = [_P, u, i, _P]
+        L.orc_bc_slip.argtypes = [_P, _P, _P, u, i, d]
         L.orc_macros.argtypes = [_P, _P, i, _P, _P, _P, _P, _P]
         L.orc_mass_energy.argtypes = [_P, _P, u, i, _P]
         L.orc_interp_node_moments.argtypes = [_P, d, _P]

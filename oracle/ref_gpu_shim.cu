@@ -44,6 +44,7 @@
 #include "BoundaryConditions/Velocity/VelocityInterpolatedIncompressible.cu"
 #include "BoundaryConditions/Velocity/VelocityWithPressureInterpolatedCompressible.cu"
 #include "BoundaryConditions/NoSlip/NoSlipInterpolatedIncompressible.cu"
+#include "BoundaryConditions/Slip/SlipCompressible.cu"
 #include "BoundaryConditions/Pressure/PressureNonEquilibriumIncompressible.cu"
 #include "BoundaryConditions/Outflow/OutflowNonReflecting.cu"
 #include "BoundaryConditions/Outflow/OutflowNonReflectingPressureCorrection.cu"
@@ -141,6 +142,15 @@ int refgpu_noslip_interpolated(real *dist, int *k, real *q, unsigned nbc, real o
         return 0;
     NoSlipInterpolatedCompressible_Device<<<blocks_for(nbc), kThreads>>>(dist, k, q, nbc, omega, nbx, nby, nbz, n,
                                                                            is_even != 0);
+    return done();
+}
+
+int refgpu_slip(real *dist, int *k, real *q, unsigned nbc, real omega, unsigned *nbx, unsigned *nby, unsigned *nbz,
+                uint64_t n, int is_even)
+{
+    if (nbc == 0)
+        return 0;
+    SlipCompressible_Device<<<blocks_for(nbc), kThreads>>>(dist, k, q, nbc, omega, nbx, nby, nbz, n, is_even != 0);
     return done();
 }
 

@@ -49,4 +49,6 @@ void adapter_compile_check(std::shared_ptr<Parameter> para)
     vfb_level L = vfb_adapter::level_of(*para, 0);
     (void)L;
     vfb_adapter::init_level(*para, 0);
+    boundaryCondition slip = vfb_adapter::slip_bc(BCF::SlipBC::SlipCompressible);
+    (void)slip;
 }

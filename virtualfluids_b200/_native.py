@@ -46,6 +46,8 @@ NOSLIP_DELAY_BOUNCE_BACK = 0
 NOSLIP_BOUNCE_BACK = 1
 NOSLIP_INTERPOLATED_INCOMPRESSIBLE = 2
 NOSLIP_INTERPOLATED_COMPRESSIBLE = 3
+SLIP_COMPRESSIBLE, SLIP_TURBULENT_VISCOSITY_COMPRESSIBLE, SLIP_NOT_SPECIFIED = 0, 1, 2
+GEOMETRY_VELOCITY, GEOMETRY_NOSLIP, GEOMETRY_SLIP = 0, 1, 2
 PRESSURE_NON_EQUILIBRIUM_INCOMPRESSIBLE = 0
 PRESSURE_NON_EQUILIBRIUM_COMPRESSIBLE = 1
 PRESSURE_OUTFLOW_NON_REFLECTIVE = 2
@@ -138,6 +140,7 @@ SIGNATURES = {
     "vfb_k17_run_on_indices": (C.c_int, [C.POINTER(Level), C.c_void_p, C.c_uint32, C.c_int32, C.c_void_p]),
     "vfb_noslip_bounce_back": (C.c_int, [C.POINTER(Level), C.POINTER(BC), C.c_void_p]),
     "vfb_noslip_interpolated_compressible": (C.c_int, [C.POINTER(Level), C.POINTER(BC), C.c_void_p]),
+    "vfb_slip_compressible": (C.c_int, [C.POINTER(Level), C.POINTER(BC), C.c_void_p]),
     "vfb_velocity_bounce_back": (C.c_int, [C.POINTER(Level), C.POINTER(BC), C.c_void_p]),
     "vfb_velocity_interpolated_compressible": (C.c_int, [C.POINTER(Level), C.POINTER(BC), C.c_void_p]),
     "vfb_pressure_non_equilibrium_compressible": (C.c_int, [C.POINTER(Level), C.POINTER(DirectionalBC), C.c_void_p]),
@@ -169,6 +172,7 @@ SIGNATURES = {
     "vfb_mass_energy_no_alloc": (C.c_int, [C.POINTER(Level), C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     "vfb_bc_factory_velocity": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),
     "vfb_bc_factory_noslip": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),
+    "vfb_bc_factory_slip": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),
     "vfb_bc_factory_pressure": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),
     "vfb_scaling_factory_fine_to_coarse": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
     "vfb_scaling_factory_coarse_to_fine": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]),
@@ -179,6 +183,8 @@ SIGNATURES = {
     "vfb_simulation_set_noslip_bc": (C.c_int, [C.c_void_p, C.POINTER(BC), C.c_int32]),
     "vfb_simulation_add_pressure_bc": (C.c_int, [C.c_void_p, C.POINTER(DirectionalBC), C.c_int32]),
     "vfb_simulation_set_geometry_bc": (C.c_int, [C.c_void_p, C.POINTER(BC), C.c_int32]),
+    "vfb_simulation_set_geometry_bc_of": (C.c_int, [C.c_void_p, C.POINTER(BC), C.c_int32, C.c_int32]),
+    "vfb_simulation_set_slip_bc": (C.c_int, [C.c_void_p, C.POINTER(BC), C.c_int32]),
     "vfb_simulation_drag_lift_workspace_bytes": (C.c_size_t, [C.c_uint32]),
     "vfb_simulation_set_drag_lift": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_uint32]),
     "vfb_simulation_check": (C.c_int, [C.c_void_p]),

@@ -390,6 +390,11 @@ int vfb_velocity_interpolated_compressible(const vfb_level *level, const vfb_bc 
     return run_bc(level, bc, vfb::kVelocityInterp, true, stream);
 }
 
+int vfb_slip_compressible(const vfb_level *level, const vfb_bc *bc, void *stream)
+{
+    return run_bc(level, bc, vfb::kSlipInterp, false, stream);
+}
+
 int vfb_noslip_interpolated_incompressible(const vfb_level *level, const vfb_bc *bc, void *stream)
 {
     return run_bc(level, bc, vfb::kNoSlipInterpIncomp, false, stream);
@@ -637,6 +642,20 @@ int vfb_bc_factory_noslip(int32_t variant, vfb_bc_fn *fn)
     }
 }
 
+int vfb_bc_factory_slip(int32_t variant, vfb_bc_fn *fn)
+{
+    if (!fn)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL fn");
+    *fn = nullptr;
+    switch (variant) {
+    case VFB_SLIP_COMPRESSIBLE: *fn = vfb_slip_compressible; return VFB_OK;
+    case VFB_SLIP_NOT_SPECIFIED: return VFB_OK;
+    case VFB_SLIP_TURBULENT_VISCOSITY_COMPRESSIBLE:
+        return fail(VFB_ERR_UNSUPPORTED, "SlipTurbulentViscosityCompressible needs a turbulence model");
+    default: return fail(VFB_ERR_INVALID_ARGUMENT, "unknown SlipBC");
+    }
+}
+
 int vfb_bc_factory_pressure(int32_t variant, vfb_directional_bc_fn *fn)
 {
     if (!fn)
@@ -704,6 +723,9 @@ struct SimLevel {
     bool noslip_set = false;
     std::vector<vfb_directional_bc> pressure;
     std::vector<vfb_directional_bc_fn> pressure_fn;
+    vfb_bc slip{};
+    vfb_bc_fn slip_fn = nullptr;
+    bool slip_set = false;
     vfb_bc geometry{};
     vfb_bc_fn geometry_fn = nullptr;
     bool geometry_set = false;
@@ -719,8 +741,8 @@ struct SimLevel {
     // neighbour slot table of the fluid-node list (library-owned, built by set_level)
     // per post-collision BC list: its post-collision values taken before the list writes (27 doubles
     // per node, enough for every storage), so that the BCs of a list never read each other's writes
-    void *snap[3] = { nullptr, nullptr, nullptr };   // velocity, no-slip, geometry
-    uint32_t snap_nodes[3] = { 0, 0, 0 };
+    void *snap[4] = { nullptr, nullptr, nullptr, nullptr };   // velocity, no-slip, geometry, slip
+    uint32_t snap_nodes[4] = { 0, 0, 0, 0 };
     uint32_t *slots = nullptr;        // 8 arrays of slots_stride entries, then the kernels' status word
     uint64_t slots_stride = 0;
     size_t slots_nodes = 0;
@@ -739,7 +761,7 @@ struct SimLevel {
     }
     void free_snaps()
     {
-        for (int i = 0; i < 3; ++i) {
+        for (int i = 0; i < 4; ++i) {
             if (snap[i])
                 cudaFree(snap[i]);
             snap[i] = nullptr;
@@ -760,7 +782,7 @@ struct SimLevel {
         if (this != &o) {
             free_slots();
             free_snaps();
-            for (int i = 0; i < 3; ++i) {
+            for (int i = 0; i < 4; ++i) {
                 snap[i] = o.snap[i];
                 snap_nodes[i] = o.snap_nodes[i];
                 o.snap[i] = nullptr;
@@ -769,6 +791,7 @@ struct SimLevel {
             has_level = o.has_level; level = o.level; fluid = o.fluid; n_fluid = o.n_fluid;
             velocity = o.velocity; velocity_fn = o.velocity_fn; velocity_set = o.velocity_set;
             noslip = o.noslip; noslip_fn = o.noslip_fn; noslip_set = o.noslip_set;
+            slip = o.slip; slip_fn = o.slip_fn; slip_set = o.slip_set;
             pressure = std::move(o.pressure); pressure_fn = std::move(o.pressure_fn);
             geometry = o.geometry; geometry_fn = o.geometry_fn; geometry_set = o.geometry_set;
             drag_work = o.drag_work; drag_history = o.drag_history; drag_history_len = o.drag_history_len;
@@ -1109,6 +1132,22 @@ int vfb_simulation_set_noslip_bc(vfb_simulation *sim, const vfb_bc *bc, int32_t 
     return VFB_OK;
 }
 
+int vfb_simulation_set_slip_bc(vfb_simulation *sim, const vfb_bc *bc, int32_t variant)
+{
+    if (!sim || !bc)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    config_changed(sim);
+    vfb_bc_fn fn = nullptr;
+    int st = vfb_bc_factory_slip(variant, &fn);
+    if (st)
+        return st;
+    SimLevel &S = current(sim);
+    S.slip = *bc;
+    S.slip_fn = fn;
+    S.slip_set = true;
+    return VFB_OK;
+}
+
 int vfb_simulation_add_pressure_bc(vfb_simulation *sim, const vfb_directional_bc *bc, int32_t variant)
 {
     if (!sim || !bc)
@@ -1135,6 +1174,32 @@ int vfb_simulation_set_geometry_bc(vfb_simulation *sim, const vfb_bc *bc, int32_
     int st = vfb_bc_factory_noslip(variant, &fn);
     if (st)
         return st;
+    SimLevel &S = current(sim);
+    S.geometry = *bc;
+    S.geometry_fn = fn;
+    S.geometry_set = true;
+    return VFB_OK;
+}
+
+// BoundaryConditionFactory::getGeometryBoundaryConditionPost (BoundaryConditionFactory.cpp:206-216):
+// the geometry BC is a velocity, a no-slip or a slip BC
+int vfb_simulation_set_geometry_bc_of(vfb_simulation *sim, const vfb_bc *bc, int32_t family, int32_t variant)
+{
+    if (!sim || !bc)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    vfb_bc_fn fn = nullptr;
+    int st;
+    switch (family) {
+    case VFB_GEOMETRY_VELOCITY: st = vfb_bc_factory_velocity(variant, &fn); break;
+    case VFB_GEOMETRY_NOSLIP: st = vfb_bc_factory_noslip(variant, &fn); break;
+    case VFB_GEOMETRY_SLIP: st = vfb_bc_factory_slip(variant, &fn); break;
+    default: return fail(VFB_ERR_INVALID_ARGUMENT, "geometry BC family must be velocity, no-slip or slip");
+    }
+    if (st)
+        return st;
+    if (family == VFB_GEOMETRY_VELOCITY && bc->number_of_bc_nodes && (!bc->vx || !bc->vy || !bc->vz))
+        return fail(VFB_ERR_INVALID_ARGUMENT, "a velocity geometry BC needs its wall velocities");
+    config_changed(sim);
     SimLevel &S = current(sim);
     S.geometry = *bc;
     S.geometry_fn = fn;
@@ -1229,6 +1294,8 @@ int vfb_simulation_check(const vfb_simulation *sim)
             return fail(VFB_ERR_INVALID_ARGUMENT, "level " + std::to_string(l) + " is not set");
         if (S.velocity_set && S.velocity.number_of_bc_nodes > 0 && !S.velocity_fn)
             return fail(VFB_ERR_BC_UNSET, "Velocity boundary condition has nodes but no kernel");
+        if (S.slip_set && S.slip.number_of_bc_nodes > 0 && !S.slip_fn)
+            return fail(VFB_ERR_BC_UNSET, "Slip boundary condition has nodes but no kernel");
         for (size_t i = 0; i < S.pressure.size(); ++i)
             if (S.pressure[i].number_of_bc_nodes > 0 && !S.pressure_fn[i])
                 return fail(VFB_ERR_BC_UNSET, "Pressure boundary condition has nodes but no kernel");
@@ -1258,6 +1325,7 @@ static int bc_kind_of(vfb_bc_fn fn, bool &velocity)
     if (fn == vfb_velocity_interpolated_incompressible) return vfb::kVelocityInterpIncomp;
     if (fn == vfb_velocity_with_pressure_interpolated_compressible) return vfb::kVelocityWithPressure;
     velocity = false;
+    if (fn == vfb_slip_compressible) return vfb::kSlipInterp;
     if (fn == vfb_noslip_bounce_back) return vfb::kNoSlipBB;
     if (fn == vfb_noslip_interpolated_compressible) return vfb::kNoSlipInterp;
     if (fn == vfb_noslip_interpolated_incompressible) return vfb::kNoSlipInterpIncomp;
@@ -1345,6 +1413,8 @@ static int step_level(vfb_simulation *sim, SimLevel &S, void *stream)
         if ((st = run_list(S, 0, S.velocity_fn, S.velocity, stream)) != VFB_OK)
             return st;
         if ((st = run_list(S, 1, S.noslip_fn, S.noslip, stream)) != VFB_OK)
+            return st;
+        if ((st = run_list(S, 3, S.slip_fn, S.slip, stream)) != VFB_OK)    // UpdateGrid27.cpp:240
             return st;
         st = run_geometry_post(S, stream);
         if (st)

@@ -1064,8 +1064,12 @@ __device__ __forceinline__ C cdot_rt(int d, C ux, C uy, C uz)
 //                       the momenta are not divided by rho and cu_sq does not carry (1 + drho); feq drops
 //                       (1 + drho) in the velocity kernel only (the no-slip one calls getEquilibriumForBC);
 //   kBCWithPressure  — VelocityWithPressureInterpolatedCompressible.cu:44-422: the compressible
-//                       form minus w drho (getInterpolatedDistributionForVeloWithPressureBC).
-enum : int { kBCCompressible = 0, kBCIncompressible = 1, kBCWithPressure = 2 };
+//                       form minus w drho (getInterpolatedDistributionForVeloWithPressureBC);
+//   kBCSlip          — SlipCompressible_Device (Slip/SlipCompressible.cu:44-550): the compressible
+//                       velocity form whose wall velocity is the node's own velocity (slip length
+//                       1), with the component along an axis zeroed when either of that axis's two
+//                       links is cut.
+enum : int { kBCCompressible = 0, kBCIncompressible = 1, kBCWithPressure = 2, kBCSlip = 3 };
 
 // density, velocity and c_s^2-scaled u^2 of a BC node's post-collision populations
 // (NoSlipInterpolatedCompressible.cu:134-153: plain-sum density, grouped momenta)
@@ -1146,6 +1150,16 @@ __device__ __forceinline__ void bc_interpolated_node(S *base, uint64_t n, const 
     }
     const BCMoments<C> m = bc_moments<C, FORM>(p);
     const C omega = (C)omega_real;
+    if (FORM == kBCSlip) {
+        // the reference zeroes VeloX when the link P00 or M00 is cut, and so on; the links along the
+        // axes come first there, so every diagonal link sees the zeroing of all three axes
+        const bool cut_x = q_active(q27[1 * q_stride]) || q_active(q27[2 * q_stride]);
+        const bool cut_y = q_active(q27[3 * q_stride]) || q_active(q27[4 * q_stride]);
+        const bool cut_z = q_active(q27[5 * q_stride]) || q_active(q27[6 * q_stride]);
+        bx = cut_x ? C(0) : m.ux;
+        by = cut_y ? C(0) : m.uy;
+        bz = cut_z ? C(0) : m.uz;
+    }
 #pragma unroll
     for (int d = 1; d < 27; ++d) {
         const C q = q27[(uint64_t)d * q_stride];
@@ -1168,7 +1182,7 @@ __global__ void __launch_bounds__(128) bc_interpolated_kernel(BCArgs a)
     uint32_t nodes[8];
     node_slots((uint32_t)a.k[i], a.nbx, a.nby, a.nbz, a.n, a.box, nodes);
     C bx = C(0), by = C(0), bz = C(0);
-    if (VELOCITY) {
+    if (VELOCITY && FORM != kBCSlip) {
         bx = static_cast<const C *>(a.ux)[i];
         by = static_cast<const C *>(a.uy)[i];
         bz = static_cast<const C *>(a.uz)[i];

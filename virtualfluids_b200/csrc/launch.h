@@ -122,7 +122,7 @@ struct PoolDomainSpec {
 
 // BC kinds of Launchers::bc
 enum BCKind : int { kNoSlipBB = 0, kNoSlipInterp = 1, kVelocityBB = 2, kVelocityInterp = 3, kNoSlipInterpIncomp = 4,
-                    kVelocityInterpIncomp = 5, kVelocityWithPressure = 6 };
+                    kVelocityInterpIncomp = 5, kVelocityWithPressure = 6, kSlipInterp = 7 };
 // pressure-list kernels of Launchers::pressure
 enum PressureKind : int { kPressureNeqComp = 0, kPressureNeqIncomp = 1, kOutflowNonReflecting = 2,
                           kOutflowPressureCorrection = 3 };

@@ -190,6 +190,10 @@ cudaError_t Launchers<S>::bc(const vfb_level *L, const vfb_bc *bc, int kind, cud
         if (even) bc_interpolated_kernel<S, true, true, kBCWithPressure><<<G, B, 0, s>>>(a);
         else bc_interpolated_kernel<S, false, true, kBCWithPressure><<<G, B, 0, s>>>(a);
         break;
+    case kSlipInterp:
+        if (even) bc_interpolated_kernel<S, true, true, kBCSlip><<<G, B, 0, s>>>(a);
+        else bc_interpolated_kernel<S, false, true, kBCSlip><<<G, B, 0, s>>>(a);
+        break;
     default:
         return cudaErrorInvalidValue;
     }

@@ -43,7 +43,7 @@ SIDE_DIR = {"MX": N.DIR_M00, "PX": N.DIR_P00, "MY": N.DIR_0M0, "PY": N.DIR_0P0, 
 @dataclass
 class SideBC:
     side: str
-    kind: str                       # "noslip", "velocity", "pressure", "geometry"
+    kind: str                       # "noslip", "velocity", "slip", "pressure", "geometry"
     k: np.ndarray                   # int32 node indices
     q: np.ndarray                   # float64 [27, n]
     velocity: tuple | np.ndarray = (0.0, 0.0, 0.0)   # constant, or (3, n) per node

@@ -186,6 +186,11 @@ class BoundaryConditionFactory:
         NoSlipInterpolatedIncompressible = N.NOSLIP_INTERPOLATED_INCOMPRESSIBLE
         NoSlipInterpolatedCompressible = N.NOSLIP_INTERPOLATED_COMPRESSIBLE
 
+    class SlipBC(enum.IntEnum):
+        SlipCompressible = N.SLIP_COMPRESSIBLE
+        SlipTurbulentViscosityCompressible = N.SLIP_TURBULENT_VISCOSITY_COMPRESSIBLE
+        NotSpecified = N.SLIP_NOT_SPECIFIED
+
     class PressureBC(enum.IntEnum):
         PressureNonEquilibriumIncompressible = N.PRESSURE_NON_EQUILIBRIUM_INCOMPRESSIBLE
         PressureNonEquilibriumCompressible = N.PRESSURE_NON_EQUILIBRIUM_COMPRESSIBLE
@@ -198,6 +203,7 @@ class BoundaryConditionFactory:
         self.velocity = self.VelocityBC.NotSpecified
         self.noslip = self.NoSlipBC.NoSlipDelayBounceBack
         self.pressure = self.PressureBC.NotSpecified
+        self.slip = self.SlipBC.NotSpecified
         self.geometry = self.NoSlipBC.NoSlipDelayBounceBack
 
     def set_velocity_boundary_condition(self, v):
@@ -209,9 +215,23 @@ class BoundaryConditionFactory:
     def set_pressure_boundary_condition(self, v):
         self.pressure = self.PressureBC(v)
 
+    def set_slip_boundary_condition(self, v):
+        self.slip = self.SlipBC(v)
+
     def set_geometry_boundary_condition(self, v):
-        """setGeometryBoundaryCondition with a NoSlipBC value (the no-slip kernels on the geometry list)."""
-        self.geometry = self.NoSlipBC(v)
+        """setGeometryBoundaryCondition: a VelocityBC, NoSlipBC or SlipBC value (a plain int is a NoSlipBC)."""
+        if isinstance(v, (self.VelocityBC, self.SlipBC)):
+            self.geometry = v
+        else:
+            self.geometry = self.NoSlipBC(v)
+
+    def geometry_family(self) -> int:
+        """The family of the geometry BC for vfb_simulation_set_geometry_bc_of."""
+        if isinstance(self.geometry, self.VelocityBC):
+            return N.GEOMETRY_VELOCITY
+        if isinstance(self.geometry, self.SlipBC):
+            return N.GEOMETRY_SLIP
+        return N.GEOMETRY_NOSLIP
 
     def velocity_function(self):
         fn = C.c_void_p()
@@ -350,7 +370,7 @@ class _LevelState:
         self.level = L
         self.keep = []
         self.bcs = {}
-        for kind in ("velocity", "noslip", "geometry"):
+        for kind in ("velocity", "noslip", "slip", "geometry"):
             m = grid.merged(kind)
             if m is None:
                 continue
@@ -411,9 +431,12 @@ class Simulation:
                 N.check(N.lib().vfb_simulation_set_velocity_bc(sim, C.byref(S.bcs["velocity"]), int(bc_factory.velocity)))
             if "noslip" in S.bcs:
                 N.check(N.lib().vfb_simulation_set_noslip_bc(sim, C.byref(S.bcs["noslip"]), int(bc_factory.noslip)))
+            if "slip" in S.bcs:
+                N.check(N.lib().vfb_simulation_set_slip_bc(sim, C.byref(S.bcs["slip"]), int(bc_factory.slip)))
             if "geometry" in S.bcs:
-                N.check(N.lib().vfb_simulation_set_geometry_bc(sim, C.byref(S.bcs["geometry"]),
-                                                               int(bc_factory.geometry)))
+                N.check(N.lib().vfb_simulation_set_geometry_bc_of(sim, C.byref(S.bcs["geometry"]),
+                                                                  bc_factory.geometry_family(),
+                                                                  int(bc_factory.geometry)))
             for p in S.pressure:
                 N.check(N.lib().vfb_simulation_add_pressure_bc(sim, C.byref(p), int(bc_factory.pressure)))
         self._cells = []
