@@ -365,7 +365,7 @@ int vfb_simulation_set_drag_lift(vfb_simulation *sim, void *workspace, size_t wo
    and the GridScalingKernelManager ones (VFB_ERR_SCALING_UNSET); every level set, one storage and
    arithmetic for all */
 int vfb_simulation_check(const vfb_simulation *sim);
-/* run steps of the coarsest level. A level's step: collision, velocity, no-slip then geometry BCs,
+/* run steps of the coarsest level. A level's step: collision, velocity, no-slip, slip then geometry BCs,
    parity toggle, drag/lift, pressure BCs. A level with a finer one lets that one take two steps
    first and after its own step interpolates fine to coarse, then coarse to fine. */
 int vfb_simulation_run(vfb_simulation *sim, uint32_t steps, void *stream);
@@ -378,7 +378,7 @@ int vfb_simulation_run(vfb_simulation *sim, uint32_t steps, void *stream);
    all levels, and the coarse steps they cover (reset != 0 clears them). Off by default. */
 enum {
     VFB_PHASE_COLLISION = 0,
-    VFB_PHASE_POST_COLLISION_BC = 1,   /* velocity, no-slip, geometry BCs and the drag's post part */
+    VFB_PHASE_POST_COLLISION_BC = 1,   /* velocity, no-slip, slip, geometry BCs and the drag's post part */
     VFB_PHASE_PRE_COLLISION_BC = 2,    /* the drag's pre part and sum, pressure BCs */
     VFB_PHASE_SCALING_FC = 3,
     VFB_PHASE_SCALING_CF = 4,
