@@ -440,11 +440,12 @@ int vfb_box_status(vfb_box *box, int32_t *device_status, void *stream);
    5 = persistent blocks with the next node's loads in flight while the current node is collided */
 int vfb_box_set_kernel_variant(vfb_box *box, int32_t variant);
 /* Boundary conditions on a box, run by vfb_box_step in the order of vfb_simulation_run: velocity,
-   no-slip, geometry (with the drag's post part before it), parity toggle, the drag's pre part and
-   sum, pressure. Node indices are box indices k = x + nx (y + ny z) of fluid (mask nonzero) nodes;
+   no-slip, slip, geometry (with the drag's post part before it), parity toggle, the drag's pre part
+   and sum, pressure. Node indices are box indices k = x + nx (y + ny z) of fluid (mask nonzero) nodes;
    q27[d * n + i], velocities and rho are host arrays of the box's real type, copied into the box.
-   variant: the VelocityBC / NoSlipBC / PressureBC enum values. A new call replaces the list. */
-enum { VFB_BOX_BC_VELOCITY = 0, VFB_BOX_BC_NOSLIP = 1, VFB_BOX_BC_GEOMETRY = 2 };
+   variant: the VelocityBC / NoSlipBC / SlipBC / PressureBC enum values (the geometry list takes a
+   NoSlipBC value). A new call replaces the list. */
+enum { VFB_BOX_BC_VELOCITY = 0, VFB_BOX_BC_NOSLIP = 1, VFB_BOX_BC_GEOMETRY = 2, VFB_BOX_BC_SLIP = 3 };
 int vfb_box_set_bc(vfb_box *box, int32_t kind, int32_t variant, const int32_t *k, const void *q27, uint32_t n,
                    const void *ux, const void *uy, const void *uz);
 int vfb_box_add_pressure_bc(vfb_box *box, int32_t variant, const int32_t *k, const int32_t *k_neighbor, const void *rho,

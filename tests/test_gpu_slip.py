@@ -133,3 +133,29 @@ def test_slip_factory_values(cuda):
     N.check(N.lib().vfb_bc_factory_slip(N.SLIP_NOT_SPECIFIED, C.byref(fn)))
     assert not fn.value
     assert N.lib().vfb_bc_factory_slip(N.SLIP_TURBULENT_VISCOSITY_COMPRESSIBLE, C.byref(fn)) == N.VFB_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("storage", [N.STORAGE_F64, N.STORAGE_F32], ids=["f64", "f32"])
+def test_box_slip_walls_match_the_driver_bitwise(cuda, storage):
+    """The structured box's slip list (vfb_box_set_bc with VFB_BOX_BC_SLIP) computes the bits of the
+    driver's slip list on the same grid."""
+    from virtualfluids_b200 import Box
+    g = _grid()
+    sim = _sim(g, storage)
+    bcf = BCF()
+    bcf.set_slip_boundary_condition(BCF.SlipBC.SlipCompressible)
+    box = Box.from_grid(g, float(sim.levels[0].level.omega), bcf, storage="f64" if storage == N.STORAGE_F64 else "f32",
+                        arith="exact")
+    Dx, Dy, Dz = g.dims
+    f0 = g.first_node
+    fields = _fields(g, 5)
+    box.init(*(np.ascontiguousarray(a[f0:f0 + Dx * Dy * Dz]) for a in fields))
+    sim.run(STEPS)
+    box.step(STEPS)
+    got = box.fields()
+    want = sim.macroscopic()
+    for key in ("rho", "vx", "vy", "vz"):
+        a = np.asarray(got[key]).reshape(-1)[g.fluid - f0]
+        b = np.asarray(want[key]).reshape(-1)[g.fluid]
+        assert np.array_equal(a, b), key
+    sim.close()

@@ -54,7 +54,7 @@ PRESSURE_OUTFLOW_NON_REFLECTIVE = 2
 PRESSURE_OUTFLOW_NON_REFLECTIVE_PRESSURE_CORRECTION = 3
 PRESSURE_NOT_SPECIFIED = 4
 # GridScalingFactory::GridScaling (GridScalingFactory.h:50-56)
-BOX_BC_VELOCITY, BOX_BC_NOSLIP, BOX_BC_GEOMETRY = 0, 1, 2
+BOX_BC_VELOCITY, BOX_BC_NOSLIP, BOX_BC_GEOMETRY, BOX_BC_SLIP = 0, 1, 2, 3
 SCALE_COMPRESSIBLE = 0
 SCALE_NOT_SPECIFIED = 1
 

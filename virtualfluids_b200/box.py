@@ -107,7 +107,7 @@ class Box:
 
     # -- boundary conditions (vfb_box_set_bc / vfb_box_add_pressure_bc) -------------------------
     def set_bc(self, kind: str, k, q27, variant, velocity=None):
-        """kind: 'velocity', 'noslip' or 'geometry'; k: box node indices; q27: (27, n) q values;
+        """kind: 'velocity', 'noslip', 'slip' or 'geometry'; k: box node indices; q27: (27, n) q values;
         velocity: (3, n) wall velocities for 'velocity'; variant: the factory enum value."""
         kk = np.ascontiguousarray(np.asarray(k, dtype=np.int32).reshape(-1))
         n = kk.size
@@ -116,7 +116,8 @@ class Box:
         if kind == "velocity":
             v = np.asarray(velocity, dtype=self.real).reshape(3, n)
             vel = [np.ascontiguousarray(v[a]) for a in range(3)]
-        code = {"velocity": N.BOX_BC_VELOCITY, "noslip": N.BOX_BC_NOSLIP, "geometry": N.BOX_BC_GEOMETRY}[kind]
+        code = {"velocity": N.BOX_BC_VELOCITY, "noslip": N.BOX_BC_NOSLIP, "geometry": N.BOX_BC_GEOMETRY,
+                "slip": N.BOX_BC_SLIP}[kind]
         N.check(N.lib().vfb_box_set_bc(self._h, code, int(variant), kk.ctypes.data, q.ctypes.data, n,
                                        *(a.ctypes.data if a is not None else None for a in vel)))
         if kind == "geometry":
@@ -160,7 +161,7 @@ class Box:
         mask = (grid.geo[f0:f0 + Dx * Dy * Dz] == N.GEO_FLUID).astype(np.uint8)
         box = cls(Dx, Dy, Dz, omega, periodic=grid.periodic, storage=storage, arith=arith, forces=forces, mask=mask)
         for kind, variant in (("velocity", bc_factory.velocity), ("noslip", bc_factory.noslip),
-                              ("geometry", bc_factory.geometry)):
+                              ("slip", bc_factory.slip), ("geometry", bc_factory.geometry)):
             m = grid.merged(kind)
             if m is None:
                 continue

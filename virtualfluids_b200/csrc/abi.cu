@@ -1627,7 +1627,7 @@ struct vfb_box {
         std::vector<void *> owned;
         uint32_t *guard = nullptr;  // guard table of the list (guards.h), nullptr when nothing is guarded
         void *saved = nullptr;      // the guarded values, saved before the list writes
-    } velocity, noslip, geometry;
+    } velocity, noslip, slip, geometry;
     struct Pressure {
         vfb_directional_bc bc{};
         int kind = 0;                 // vfb::PressureKind
@@ -1660,6 +1660,7 @@ void box_free(vfb_box *b)
         return;
     free_list(b->velocity);
     free_list(b->noslip);
+    free_list(b->slip);
     free_list(b->geometry);
     for (auto &p : b->pressure)
         for (void *q : p.owned)
@@ -1847,6 +1848,8 @@ cudaError_t box_post_collision(vfb_box *b, cudaStream_t s)
         e = box_run_list(b, b->velocity, s);
     if (e == cudaSuccess)
         e = box_run_list(b, b->noslip, s);
+    if (e == cudaSuccess)
+        e = box_run_list(b, b->slip, s);        // runSlipBCKernelPost (UpdateGrid27.cpp:240)
     const uint32_t ng = b->geometry.bc.number_of_bc_nodes;
     if (e == cudaSuccess && b->drag_work && ng) {
         const vfb_level L = box_level(b);
@@ -1986,8 +1989,9 @@ int vfb_box_set_bc(vfb_box *box, int32_t kind, int32_t variant, const int32_t *k
 {
     if (!box)
         return fail(VFB_ERR_INVALID_ARGUMENT, "NULL box");
-    if (kind != VFB_BOX_BC_VELOCITY && kind != VFB_BOX_BC_NOSLIP && kind != VFB_BOX_BC_GEOMETRY)
-        return fail(VFB_ERR_INVALID_ARGUMENT, "kind must be VFB_BOX_BC_VELOCITY, _NOSLIP or _GEOMETRY");
+    if (kind != VFB_BOX_BC_VELOCITY && kind != VFB_BOX_BC_NOSLIP && kind != VFB_BOX_BC_GEOMETRY &&
+        kind != VFB_BOX_BC_SLIP)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "kind must be VFB_BOX_BC_VELOCITY, _NOSLIP, _GEOMETRY or _SLIP");
     if (n && (!k || !q27))
         return fail(VFB_ERR_INVALID_ARGUMENT, "node indices or q are NULL");
     if (kind == VFB_BOX_BC_VELOCITY && n && (!ux || !uy || !uz))
@@ -2002,6 +2006,12 @@ int vfb_box_set_bc(vfb_box *box, int32_t kind, int32_t variant, const int32_t *k
         case VFB_VELOCITY_NOT_SPECIFIED: break;
         default: return fail(VFB_ERR_UNSUPPORTED, "velocity BC variant not built for boxes");
         }
+    } else if (kind == VFB_BOX_BC_SLIP) {
+        switch (variant) {
+        case VFB_SLIP_COMPRESSIBLE: bc_kind = vfb::kSlipInterp; break;
+        case VFB_SLIP_NOT_SPECIFIED: break;
+        default: return fail(VFB_ERR_UNSUPPORTED, "slip BC variant not built for boxes");
+        }
     } else {
         switch (variant) {
         case VFB_NOSLIP_DELAY_BOUNCE_BACK: break;
@@ -2015,7 +2025,10 @@ int vfb_box_set_bc(vfb_box *box, int32_t kind, int32_t variant, const int32_t *k
     for (uint32_t i = 0; i < n; ++i)
         if (k[i] < 0 || (uint64_t)k[i] >= nn)
             return fail(VFB_ERR_INVALID_ARGUMENT, "a BC node index lies outside the box");
-    vfb_box::List &l = kind == VFB_BOX_BC_VELOCITY ? box->velocity : kind == VFB_BOX_BC_NOSLIP ? box->noslip : box->geometry;
+    vfb_box::List &l = kind == VFB_BOX_BC_VELOCITY ? box->velocity
+                     : kind == VFB_BOX_BC_NOSLIP ? box->noslip
+                     : kind == VFB_BOX_BC_SLIP   ? box->slip
+                                                 : box->geometry;
     free_list(l);
     if (kind == VFB_BOX_BC_VELOCITY) {
         cudaFree(box->velocity_base);
