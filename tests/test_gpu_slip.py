@@ -159,3 +159,45 @@ def test_box_slip_walls_match_the_driver_bitwise(cuda, storage):
         b = np.asarray(want[key]).reshape(-1)[g.fluid]
         assert np.array_equal(a, b), key
     sim.close()
+
+
+def test_velocity_geometry_bc_matches_oracle_bitwise(cuda, oracle):
+    """setGeometryBoundaryCondition with a VelocityBC value: the geometry list runs the interpolated
+    velocity kernel with the list's own wall velocities (here a moving obstacle)."""
+    g = ListGrid(14, 10, 9, periodic=(True, False, True))
+    for side in ("MY", "PY"):
+        g.add_side(side, "noslip")
+    g.add_box_obstacle((4.4, 3.4, 2.4), (8.6, 6.6, 5.6))
+    for b in g.bcs:                                 # the obstacle moves along x
+        if b.kind == "geometry":
+            b.velocity = (0.01, 0.0, 0.0)
+    p = Parameter()
+    p.set_viscosity_lb((1.0 / 1.8 - 0.5) / 3.0)
+    p.configure_main_kernel("K17CompressibleNavierStokes")
+    p.storage, p.arith = N.STORAGE_F64, N.ARITH_EXACT
+    bcf = BCF()
+    bcf.set_no_slip_boundary_condition(BCF.NoSlipBC.NoSlipInterpolatedCompressible)
+    bcf.set_geometry_boundary_condition(BCF.VelocityBC.VelocityInterpolatedCompressible)
+    sim = Simulation(p, g, bcf)
+    sim.init(*_fields(g, 5))
+    omega = float(sim.levels[0].level.omega)
+    lv = oracle.OracleLevel(g, omega)
+    lv.init(*_fields(g, 5))
+    lib, ptr = oracle.lib(), oracle.ptr
+    kn, qn, _ = g.merged("noslip")
+    kn, qn = np.ascontiguousarray(kn.astype(np.int32)), np.ascontiguousarray(qn.reshape(-1))
+    kg, qg, vg = g.merged("geometry")
+    kg, qg = np.ascontiguousarray(kg.astype(np.int32)), np.ascontiguousarray(qg.reshape(-1))
+    vg = [np.ascontiguousarray(vg[a], dtype=np.float64) for a in range(3)]
+    assert np.all(vg[0] == 0.01)
+    for _ in range(STEPS):
+        lib.orc_collision(C.byref(lv.L), ptr(lv.fluid), lv.fluid.size, lv.is_even.value, omega, ptr(lv.lim),
+                          ptr(lv.forces), 0, None, None, None, None, 0)
+        lib.orc_bc_noslip_interpolated(C.byref(lv.L), ptr(kn), ptr(qn), kn.size, lv.is_even.value, omega)
+        lib.orc_bc_velocity_interpolated(C.byref(lv.L), ptr(kg), ptr(qg), kg.size, lv.is_even.value, omega,
+                                         *(ptr(a) for a in vg))
+        lv.is_even.value = 1 - lv.is_even.value
+    sim.run(STEPS)
+    assert np.array_equal(sim.populations(), lv.f)
+    assert np.abs(sim.macroscopic()["vx"]).max() > 1e-4          # the moving obstacle drives the flow
+    sim.close()
