@@ -761,7 +761,8 @@ def run_list_path(args, n, omega, fields, dev):
     from virtualfluids_b200 import _native as N
 
     out = {"path": "vfb_simulation_run (K17CompressibleNavierStokes over neighborX/Y/Z with neighbour slot tables)",
-           "kernel": "k17_list_kernel<double>"}
+           "kernel": "k17_box_kernel<double> over the reference layout where the level is a regular periodic box "
+                     "(box_addressing), else k17_list_kernel<double>"}
     peak, peak_kind = measured_peak()
     out["peak_source"] = peak_kind
     # node numbering as the reference's grid builder (first node 1, planes of n^3 + 1 nodes), and
@@ -776,6 +777,8 @@ def run_list_path(args, n, omega, fields, dev):
         p.configure_main_kernel("K17CompressibleNavierStokes")
         p.storage, p.arith = N.STORAGE_F64, N.ARITH_EXACT if arith == "exact" else N.ARITH_FAST
         sim = vfb.Simulation(p, g, vfb.BoundaryConditionFactory())
+        box_addr = C.c_int32()
+        N.check(N.lib().vfb_simulation_level_box_addressing(sim._sim, 0, C.byref(box_addr)))
         full = [np.zeros(g.number_of_nodes) for _ in range(4)]
         for dst, a in zip(full, fields):
             dst[g.first_node:g.first_node + nodes_of(n)] = a
@@ -795,7 +798,8 @@ def run_list_path(args, n, omega, fields, dev):
         del sim
         torch.cuda.empty_cache()
         out[key] = {"mlups": round(nodes / (ms / 1e3) / 1e6, 1), "ms_per_step": round(ms, 4),
-                    "hbm_achieved_gbs": round(achieved, 1), "frac": round(achieved / peak, 4)}
+                    "hbm_achieved_gbs": round(achieved, 1), "frac": round(achieved / peak, 4),
+                    "box_addressing": bool(box_addr.value)}
     return out
 
 

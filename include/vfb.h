@@ -320,8 +320,15 @@ int vfb_simulation_number_of_levels(const vfb_simulation *sim, int32_t *number_o
    them instead of walking the neighborX/Y/Z chain, with the same results. mode 1 (default): one
    coalesced load per slot; 2: the tables staged in shared memory by bulk asynchronous copies two
    tiles ahead (persistent warps); 0: no tables (the chain). Set the level again after changing its
-   neighbour arrays or fluid-node list. */
+   neighbour arrays or fluid-node list.
+   With modes 1 and 2, an F64 or F32 level whose fluid list is a whole periodic box numbered x
+   fastest from its first node (as the reference's grid builder numbers a box without solids;
+   checked by vfb_simulation_set_level against every neighbour entry) is collided by the structured
+   box kernel over the same arrays: arithmetic neighbours instead of index loads, the same results.
+   The 16-bit forms keep the list kernel (their stochastic rounding hashes the slot offsets). */
 int vfb_simulation_set_neighbor_tables(vfb_simulation *sim, int32_t mode);
+/* 1 when the level's collision runs with that box addressing, else 0 */
+int vfb_simulation_level_box_addressing(const vfb_simulation *sim, int32_t level, int32_t *box_addressing);
 /* synchronises the stream and reads the status word the staged collision sets when a bounded wait
    for its copies gave up (0 = fine); returns VFB_ERR_CUDA when it is nonzero */
 int vfb_simulation_status(vfb_simulation *sim, int32_t *device_status, void *stream);

@@ -305,6 +305,36 @@ def test_box_inlet_perturbation_is_seeded(cuda):
     assert np.abs(runs[0] - runs[2]).max() < 1e-3
 
 
+@pytest.mark.parametrize("storage,arith,align", [(N.STORAGE_F64, N.ARITH_EXACT, 1), (N.STORAGE_F64, N.ARITH_EXACT, 32),
+                                                 (N.STORAGE_F32, N.ARITH_EXACT, 1), (N.STORAGE_F64, N.ARITH_FAST, 1),
+                                                 (N.STORAGE_F32, N.ARITH_FAST, 32)])
+def test_periodic_box_levels_take_box_addressing_with_the_same_bits(cuda, storage, arith, align):
+    """An F64 or F32 level whose fluid list is a whole periodic box (reference numbering from node 1,
+    or aligned from node 32) is collided by the box kernel over the reference layout: the same bits
+    as the neighborX/Y/Z chain, with forcing, in both arithmetics; a level with walls, and a 16-bit
+    level, keep the list kernel."""
+    g = ListGrid(20, 9, 7, periodic=(True, True, True), align=align)
+    out, used = [], []
+    for tables in (0, 1):
+        p = make_para(1.85, storage, arith, forcing=(2e-6, -1e-6, 5e-7))
+        sim = Simulation(p, g, BCF(), neighbor_tables=tables)
+        sim.init(*smooth_fields(g, 6))
+        sim.run(9)
+        out.append(sim.populations())
+        flag = C.c_int32()
+        N.check(N.lib().vfb_simulation_level_box_addressing(sim._sim, 0, C.byref(flag)))
+        used.append(flag.value)
+        sim.close()
+    assert used == [0, 1]
+    assert np.array_equal(out[0], out[1])
+    for grid, st in ((ListGrid(12, 10, 9), N.STORAGE_F64), (g, N.STORAGE_F16)):
+        sim = Simulation(make_para(1.8, st), grid, BCF())
+        flag = C.c_int32()
+        N.check(N.lib().vfb_simulation_level_box_addressing(sim._sim, 0, C.byref(flag)))
+        assert flag.value == 0
+        sim.close()
+
+
 @pytest.mark.parametrize("storage,dims", [(N.STORAGE_F64, (12, 10, 9)), (N.STORAGE_F16, (12, 10, 9)),
                                           (N.STORAGE_F64, (96, 40, 36)), (N.STORAGE_F32, (90, 37, 33))],
                          ids=["f64", "f16", "f64-loop", "f32-loop"])

@@ -185,6 +185,7 @@ SIGNATURES = {
     "vfb_simulation_set_geometry_bc": (C.c_int, [C.c_void_p, C.POINTER(BC), C.c_int32]),
     "vfb_simulation_set_geometry_bc_of": (C.c_int, [C.c_void_p, C.POINTER(BC), C.c_int32, C.c_int32]),
     "vfb_simulation_set_slip_bc": (C.c_int, [C.c_void_p, C.POINTER(BC), C.c_int32]),
+    "vfb_simulation_level_box_addressing": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]),
     "vfb_simulation_drag_lift_workspace_bytes": (C.c_size_t, [C.c_uint32]),
     "vfb_simulation_set_drag_lift": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_uint32]),
     "vfb_simulation_check": (C.c_int, [C.c_void_p]),

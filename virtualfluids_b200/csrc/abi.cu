@@ -743,6 +743,11 @@ struct SimLevel {
     // per node, enough for every storage), so that the BCs of a list never read each other's writes
     void *snap[4] = { nullptr, nullptr, nullptr, nullptr };   // velocity, no-slip, geometry, slip
     uint32_t snap_nodes[4] = { 0, 0, 0, 0 };
+    // a fluid list that is a whole periodic box in x-fastest order from node box_first (checked at
+    // set_level against the neighbour arrays): collided with arithmetic addressing
+    bool regular = false;
+    int box_dims[3] = { 0, 0, 0 };
+    uint32_t box_first = 0;
     uint32_t *slots = nullptr;        // 8 arrays of slots_stride entries, then the kernels' status word
     uint64_t slots_stride = 0;
     size_t slots_nodes = 0;
@@ -796,6 +801,9 @@ struct SimLevel {
             geometry = o.geometry; geometry_fn = o.geometry_fn; geometry_set = o.geometry_set;
             drag_work = o.drag_work; drag_history = o.drag_history; drag_history_len = o.drag_history_len;
             drag_steps = o.drag_steps; fc = o.fc; cf = o.cf; fc_offsets = o.fc_offsets; cf_offsets = o.cf_offsets;
+            regular = o.regular; box_first = o.box_first;
+            for (int i = 0; i < 3; ++i)
+                box_dims[i] = o.box_dims[i];
             slots = o.slots; slots_stride = o.slots_stride; slots_nodes = o.slots_nodes;
             for (int i = 0; i < 4; ++i)
                 slots_key[i] = o.slots_key[i];
@@ -959,6 +967,125 @@ __global__ void list_slots_kernel(const uint32_t *__restrict__ idx, uint32_t n_i
         slots[(size_t)j * stride + i] = out[j];
 }
 
+// every entry i of the fluid list must be node first + i and have the +1 neighbours of a periodic
+// dx * dy * dz box numbered x fastest from `first`; *bad counts the entries that are not
+__global__ void regular_box_check_kernel(const uint32_t *__restrict__ fluid, uint32_t n, const uint32_t *__restrict__ nbx,
+                                         const uint32_t *__restrict__ nby, const uint32_t *__restrict__ nbz,
+                                         uint32_t first, uint32_t dx, uint32_t dy, uint32_t dz, unsigned *bad)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const uint32_t x = i % dx, y = (i / dx) % dy, z = i / (dx * dy);
+    const uint32_t k = first + i;
+    bool ok = __ldg(fluid + i) == k;
+    ok = ok && __ldg(nbx + k) == first + (x + 1) % dx + dx * (y + dy * z);
+    ok = ok && __ldg(nby + k) == first + x + dx * ((y + 1) % dy + dy * z);
+    ok = ok && __ldg(nbz + k) == first + x + dx * (y + dy * ((z + 1) % dz));
+    if (!ok)
+        atomicAdd(bad, 1u);
+}
+
+// Whether a level's fluid list is a whole periodic box numbered x fastest (the numbering of the
+// reference's grid builder for a box without solids): the box's size comes from the first node's
+// +y and +z neighbours, and a kernel checks every entry and its three neighbours against it.
+static int detect_regular_box(SimLevel &S)
+{
+    S.regular = false;
+    const vfb_level &L = S.level;
+    const uint32_t n = S.n_fluid;
+    // the 16-bit forms hash each slot's offset into their stochastic rounding: a box over the
+    // shifted array would round differently, so they keep the list kernel
+    if (L.storage != VFB_STORAGE_F64 && L.storage != VFB_STORAGE_F32)
+        return VFB_OK;
+    if (n < 2 || !L.neighbor_x || !L.neighbor_y || !L.neighbor_z)
+        return VFB_OK;
+    uint32_t first = 0, last = 0, ny0 = 0, nz0 = 0;
+    cudaError_t e = cudaMemcpy(&first, S.fluid, sizeof first, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(&last, S.fluid + (n - 1), sizeof last, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+        return cuda_status(e, "reading the fluid list");
+    if ((uint64_t)first + n > L.number_of_nodes || (uint64_t)last != (uint64_t)first + n - 1)
+        return VFB_OK;
+    e = cudaMemcpy(&ny0, L.neighbor_y + first, sizeof ny0, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(&nz0, L.neighbor_z + first, sizeof nz0, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+        return cuda_status(e, "reading the neighbour arrays");
+    if (ny0 <= first || nz0 <= first)
+        return VFB_OK;
+    const uint64_t dx = ny0 - first, dxy = (uint64_t)nz0 - first;
+    if (dxy % dx != 0 || n % dxy != 0 || dx > (1u << 20) || dxy / dx > (1u << 20))
+        return VFB_OK;
+    const uint32_t dy = (uint32_t)(dxy / dx), dz = (uint32_t)(n / dxy);
+    unsigned *bad = nullptr;
+    e = cudaMalloc(&bad, sizeof(unsigned));
+    if (e == cudaSuccess)
+        e = cudaMemset(bad, 0, sizeof(unsigned));
+    if (e == cudaSuccess) {
+        regular_box_check_kernel<<<(n + 255) / 256, 256>>>(S.fluid, n, L.neighbor_x, L.neighbor_y, L.neighbor_z, first,
+                                                          (uint32_t)dx, dy, dz, bad);
+        e = cudaGetLastError();
+    }
+    unsigned n_bad = 1;
+    if (e == cudaSuccess)
+        e = cudaMemcpy(&n_bad, bad, sizeof n_bad, cudaMemcpyDeviceToHost);
+    cudaFree(bad);
+    if (e != cudaSuccess)
+        return cuda_status(e, "checking for a regular box");
+    if (n_bad == 0) {
+        S.regular = true;
+        S.box_first = first;
+        S.box_dims[0] = (int)dx;
+        S.box_dims[1] = (int)dy;
+        S.box_dims[2] = (int)dz;
+    }
+    return VFB_OK;
+}
+
+// the list collision's force along one axis, forces * 1/2 * 2^-level formed in the compute type
+// (double for F64 storage, float otherwise) as run_k17's launcher forms it, returned as a double
+// that converts back to the same value
+static double list_half_force(const vfb_level &L, int axis)
+{
+    if (L.storage == VFB_STORAGE_F64) {
+        double f = 1.0;
+        for (int i = 1; i <= L.level; ++i)
+            f *= 2.0;
+        return L.forces[axis] * 0.5 * (1.0 / f);
+    }
+    float f = 1.0f;
+    for (int i = 1; i <= L.level; ++i)
+        f *= 2.0f;
+    return (double)((float)L.forces[axis] * 0.5f * (1.0f / f));
+}
+
+// a regular level as a structured box over the reference layout: the populations of node
+// box_first + k at plane * numberOfNodes + box_first + k, the direct-load box kernel
+static vfb::BoxState regular_box_state(const SimLevel &S)
+{
+    const vfb_level &L = S.level;
+    const size_t elem = L.storage == VFB_STORAGE_F64 ? 8 : L.storage == VFB_STORAGE_F32 ? 4 : 2;
+    vfb::BoxState b{};
+    b.dist = static_cast<char *>(L.distributions) + (size_t)S.box_first * elem;
+    b.pitch = L.number_of_nodes;
+    b.nx = S.box_dims[0];
+    b.ny = S.box_dims[1];
+    b.nz = S.box_dims[2];
+    b.periodic_x = b.periodic_y = b.periodic_z = 1;
+    b.mask = nullptr;
+    b.omega = L.omega;
+    b.fx = list_half_force(L, 0);
+    b.fy = list_half_force(L, 1);
+    b.fz = list_half_force(L, 2);
+    for (int i = 0; i < 3; ++i)
+        b.lim[i] = L.quadric_limiters[i];
+    b.variant = 1;
+    b.status = nullptr;
+    return b;
+}
+
 // The slot table of a level (the seven +1 neighbours of each fluid node, one array per slot),
 // rebuilt when the fluid list or the neighbour arrays change. It costs 28 bytes per fluid node and
 // replaces the four-deep chain of dependent neighborX/Y/Z loads in every collision.
@@ -967,6 +1094,7 @@ static int build_slots(vfb_simulation *sim, SimLevel &S)
     const void *key[4] = { S.fluid, S.level.neighbor_x, S.level.neighbor_y, S.level.neighbor_z };
     if (!sim->neighbor_tables || S.n_fluid == 0) {
         S.free_slots();
+        S.regular = false;
         return VFB_OK;
     }
     if (S.slots && S.slots_nodes == S.n_fluid && std::equal(key, key + 4, S.slots_key))
@@ -996,7 +1124,7 @@ static int build_slots(vfb_simulation *sim, SimLevel &S)
     }
     S.slots_nodes = S.n_fluid;
     std::copy(key, key + 4, S.slots_key);
-    return VFB_OK;
+    return detect_regular_box(S);      // the same fluid list and neighbour arrays as the table
 }
 
 extern "C" {
@@ -1098,6 +1226,15 @@ int vfb_simulation_set_level(vfb_simulation *sim, const vfb_level *level, const 
     S.n_fluid = n;
     S.has_level = true;
     return build_slots(sim, S);
+}
+
+int vfb_simulation_level_box_addressing(const vfb_simulation *sim, int32_t level, int32_t *box_addressing)
+{
+    if (!sim || !box_addressing || level < 0 || level >= (int32_t)sim->levels.size())
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument or no such level");
+    const SimLevel &S = sim->levels[level];
+    *box_addressing = (S.regular && sim->neighbor_tables != 0) ? 1 : 0;
+    return VFB_OK;
 }
 
 int vfb_simulation_set_velocity_bc(vfb_simulation *sim, const vfb_bc *bc, int32_t variant)
@@ -1397,7 +1534,13 @@ static int step_level(vfb_simulation *sim, SimLevel &S, void *stream)
     int st;
     {
     PhaseScope phase(sim->timers, VFB_PHASE_COLLISION, stream);
-    if (S.slots && sim->neighbor_tables == 2) {
+    if (S.regular && sim->neighbor_tables != 0) {
+        const vfb::BoxState b = regular_box_state(S);
+        const cudaError_t e = VFB_DISPATCH(L.storage, L.arith,
+                                           LA::box_collide(b, L.is_even_timestep != 0, nullptr, nullptr,
+                                                           as_stream(stream)));
+        st = cuda_status(e, "K17CompressibleNavierStokes launch");
+    } else if (S.slots && sim->neighbor_tables == 2) {
         const cudaError_t e = VFB_DISPATCH(L.storage, L.arith,
                                            LA::k17_list_staged(&L, S.slots, S.slots_stride, S.n_fluid, S.status(),
                                                                as_stream(stream)));
