@@ -158,6 +158,20 @@ const char *vfb_kernel_name(int index);
    collision + esoteric-twist streaming of the listed fluid nodes, in place. */
 int vfb_k17_run_on_indices(const vfb_level *level, const uint32_t *fluid_node_indices, uint32_t size,
                            int32_t collision_template, void *stream);
+/* A prepared collision for a caller that keeps its own step loop (KernelImp::run / runOnIndices):
+   one fluid-node list of a level, with its slot table (library-owned device memory, 32 bytes per
+   entry) and, for an F64 or F32 list that is a whole periodic box numbered x fastest, box
+   addressing; both are built from the list and neighborX/Y/Z as they are at creation. Same results
+   as vfb_k17_run_on_indices. vfb_k17_plan_run takes the level of each call (parity, omega, forces,
+   arrays); its node count, neighbour arrays and storage must be the plan's. Create the plan again
+   after changing the list or the neighbour arrays. */
+typedef struct vfb_k17_plan vfb_k17_plan;
+int vfb_k17_plan_create(const vfb_level *level, const uint32_t *fluid_node_indices, uint32_t size,
+                        vfb_k17_plan **plan);
+int vfb_k17_plan_run(vfb_k17_plan *plan, const vfb_level *level, int32_t collision_template, void *stream);
+/* 1 when the plan's default-template collision runs with box addressing */
+int vfb_k17_plan_box_addressing(const vfb_k17_plan *plan, int32_t *box_addressing);
+int vfb_k17_plan_destroy(vfb_k17_plan *plan);
 
 /* NoSlipBounceBack (BoundaryConditions/NoSlip/NoSlip.cu:44) */
 int vfb_noslip_bounce_back(const vfb_level *level, const vfb_bc *bc, void *stream);

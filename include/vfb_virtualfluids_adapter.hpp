@@ -25,9 +25,11 @@
 
 #include <cstdint>
 #include <functional>
+#include <map>
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <variant>
 
 #include "BoundaryConditions/BoundaryConditionFactory.h"
@@ -148,14 +150,28 @@ public:
                      CudaStreamIndex::Legacy);
     }
 
-    //! K17CompressibleNavierStokes.cu:102-145: every CollisionTemplate, on the stream of the index
+    //! K17CompressibleNavierStokes.cu:102-145: every CollisionTemplate, on the stream of the index.
+    //! Each index list gets a prepared plan on its first call (its slot table, and box addressing for
+    //! a regular periodic box); the reference sets its lists and neighbour arrays up once. After
+    //! changing them, call invalidatePlans().
     void runOnIndices(const unsigned int *indices, unsigned int size_indices, CollisionTemplate collisionTemplate,
                       CudaStreamIndex streamIndex = CudaStreamIndex::Legacy) override
     {
         vfb_level L = level_of(*para, level, arith);
-        check(vfb_k17_run_on_indices(&L, indices, size_indices, static_cast<int32_t>(collisionTemplate),
-                                     para->getStreamManager()->getStream(streamIndex)));
+        vfb_k17_plan *&plan = plans[{ indices, size_indices }];
+        if (!plan)
+            check(vfb_k17_plan_create(&L, indices, size_indices, &plan));
+        check(vfb_k17_plan_run(plan, &L, static_cast<int32_t>(collisionTemplate),
+                               para->getStreamManager()->getStream(streamIndex)));
     }
+
+    void invalidatePlans()
+    {
+        for (auto &kv : plans)
+            vfb_k17_plan_destroy(kv.second);
+        plans.clear();
+    }
+    ~K17CompressibleNavierStokesB200() override { invalidatePlans(); }
 
     //! VFB_ARITH_EXACT (default): the reference's rounding bit for bit; VFB_ARITH_FAST: FMA arithmetic
     void setArithmetic(int32_t a) { arith = a; }
@@ -168,6 +184,7 @@ private:
         kernelUsesFluidNodeIndices = true;
     }
     int32_t arith = VFB_ARITH_EXACT;
+    std::map<std::pair<const unsigned int *, unsigned int>, vfb_k17_plan *> plans;
 };
 
 //! KernelFactoryImp::makeKernel's branch for the name (the reference throws for unknown names;

@@ -360,3 +360,45 @@ def test_neighbor_slot_tables_change_nothing(cuda, storage, dims):
         assert st.value == 0
         sim.close()
     assert all(np.array_equal(out[0], o) for o in out[1:])
+
+
+@pytest.mark.parametrize("periodic,storage,arith", [((True, True, True), N.STORAGE_F64, N.ARITH_EXACT),
+                                                    ((True, True, True), N.STORAGE_F32, N.ARITH_FAST),
+                                                    ((False, True, False), N.STORAGE_F64, N.ARITH_EXACT),
+                                                    ((True, True, True), N.STORAGE_F16, N.ARITH_FAST)],
+                         ids=["periodic-f64", "periodic-f32-fma", "walls-f64", "periodic-f16"])
+def test_k17_plans_match_the_stateless_entry_point(cuda, periodic, storage, arith):
+    """vfb_k17_plan_run (the adapter's runOnIndices) against vfb_k17_run_on_indices over the chain:
+    the same populations and macroscopic outputs, alternating the Default and WriteMacroVars
+    templates, with box addressing exactly for the regular F64/F32 levels."""
+    g = ListGrid(20, 9, 7, periodic=periodic)
+    lib = N.lib()
+    results, flags = [], []
+    for use_plan in (False, True):
+        sim = Simulation(make_para(1.85, storage, arith, forcing=(1e-6, 0.0, -2e-6)), g, BCF(), neighbor_tables=0)
+        sim.init(*smooth_fields(g, 4))
+        L = sim.levels[0].level
+        fluid, n = C.c_void_p(sim.fluid.data_ptr()), int(g.fluid.size)
+        plan = C.c_void_p()
+        if use_plan:
+            N.check(lib.vfb_k17_plan_create(C.byref(L), fluid, n, C.byref(plan)))
+            flag = C.c_int32()
+            N.check(lib.vfb_k17_plan_box_addressing(plan, C.byref(flag)))
+            flags.append(flag.value)
+        for step in range(8):
+            tmpl = (N.COLLISION_DEFAULT, N.COLLISION_WRITE_MACRO_VARS)[step % 2]
+            if use_plan:
+                N.check(lib.vfb_k17_plan_run(plan, C.byref(L), tmpl, None))
+            else:
+                N.check(lib.vfb_k17_run_on_indices(C.byref(L), fluid, n, tmpl, None))
+            L.is_even_timestep = 1 - L.is_even_timestep
+        N.check(lib.vfb_synchronize(None))
+        S = sim.levels[0]
+        results.append([sim.populations()] + [x.double().cpu().numpy() for x in (S.rho, S.vx, S.vy, S.vz)])
+        if use_plan:
+            N.check(lib.vfb_k17_plan_destroy(plan))
+        sim.close()
+    regular = all(periodic) and storage in (N.STORAGE_F64, N.STORAGE_F32)
+    assert flags == [1 if regular else 0]
+    for a, b in zip(*results):
+        assert np.array_equal(a, b)

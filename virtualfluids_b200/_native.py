@@ -138,6 +138,10 @@ SIGNATURES = {
     "vfb_kernel_count": (C.c_int, []),
     "vfb_kernel_name": (C.c_char_p, [C.c_int]),
     "vfb_k17_run_on_indices": (C.c_int, [C.POINTER(Level), C.c_void_p, C.c_uint32, C.c_int32, C.c_void_p]),
+    "vfb_k17_plan_create": (C.c_int, [C.POINTER(Level), C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]),
+    "vfb_k17_plan_run": (C.c_int, [C.c_void_p, C.POINTER(Level), C.c_int32, C.c_void_p]),
+    "vfb_k17_plan_box_addressing": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "vfb_k17_plan_destroy": (C.c_int, [C.c_void_p]),
     "vfb_noslip_bounce_back": (C.c_int, [C.POINTER(Level), C.POINTER(BC), C.c_void_p]),
     "vfb_noslip_interpolated_compressible": (C.c_int, [C.POINTER(Level), C.POINTER(BC), C.c_void_p]),
     "vfb_slip_compressible": (C.c_int, [C.POINTER(Level), C.POINTER(BC), C.c_void_p]),

@@ -1089,10 +1089,10 @@ static vfb::BoxState regular_box_state(const SimLevel &S)
 // The slot table of a level (the seven +1 neighbours of each fluid node, one array per slot),
 // rebuilt when the fluid list or the neighbour arrays change. It costs 28 bytes per fluid node and
 // replaces the four-deep chain of dependent neighborX/Y/Z loads in every collision.
-static int build_slots(vfb_simulation *sim, SimLevel &S)
+static int build_slots(int32_t tables, SimLevel &S)
 {
     const void *key[4] = { S.fluid, S.level.neighbor_x, S.level.neighbor_y, S.level.neighbor_z };
-    if (!sim->neighbor_tables || S.n_fluid == 0) {
+    if (!tables || S.n_fluid == 0) {
         S.free_slots();
         S.regular = false;
         return VFB_OK;
@@ -1174,7 +1174,7 @@ int vfb_simulation_set_neighbor_tables(vfb_simulation *sim, int32_t enable)
     for (SimLevel &S : sim->levels) {
         if (!S.has_level)
             continue;
-        int st = build_slots(sim, S);
+        int st = build_slots(sim->neighbor_tables, S);
         if (st)
             return st;
     }
@@ -1225,7 +1225,7 @@ int vfb_simulation_set_level(vfb_simulation *sim, const vfb_level *level, const 
     S.fluid = fluid;
     S.n_fluid = n;
     S.has_level = true;
-    return build_slots(sim, S);
+    return build_slots(sim->neighbor_tables, S);
 }
 
 int vfb_simulation_level_box_addressing(const vfb_simulation *sim, int32_t level, int32_t *box_addressing)
@@ -1234,6 +1234,75 @@ int vfb_simulation_level_box_addressing(const vfb_simulation *sim, int32_t level
         return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument or no such level");
     const SimLevel &S = sim->levels[level];
     *box_addressing = (S.regular && sim->neighbor_tables != 0) ? 1 : 0;
+    return VFB_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// prepared collisions: one fluid-node list of a level with its slot table and box addressing, for
+// callers that keep their own step loop (the reference's KernelImp::run / runOnIndices)
+// ---------------------------------------------------------------------------------------------
+struct vfb_k17_plan {
+    SimLevel S;
+};
+
+int vfb_k17_plan_create(const vfb_level *level, const uint32_t *idx, uint32_t size, vfb_k17_plan **plan)
+{
+    if (!plan)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL plan");
+    *plan = nullptr;
+    int st = check_level(level);
+    if (st)
+        return st;
+    if (size && !idx)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "fluid node indices are NULL");
+    auto *p = new vfb_k17_plan();
+    p->S.level = *level;
+    p->S.fluid = idx;
+    p->S.n_fluid = size;
+    p->S.has_level = true;
+    st = build_slots(1, p->S);
+    if (st) {
+        delete p;
+        return st;
+    }
+    *plan = p;
+    return VFB_OK;
+}
+
+int vfb_k17_plan_run(vfb_k17_plan *plan, const vfb_level *level, int32_t collision_template, void *stream)
+{
+    if (!plan)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL plan");
+    int st = check_level(level);
+    if (st)
+        return st;
+    SimLevel &S = plan->S;
+    if (level->number_of_nodes != S.level.number_of_nodes || level->neighbor_x != S.level.neighbor_x ||
+        level->neighbor_y != S.level.neighbor_y || level->neighbor_z != S.level.neighbor_z ||
+        level->storage != S.level.storage)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "the level's node count, neighbour arrays or storage differ from the plan's");
+    S.level = *level;                 // parity, omega, forces and the arrays of this call
+    if (collision_template == VFB_COLLISION_DEFAULT && S.regular) {
+        const vfb::BoxState b = regular_box_state(S);
+        const cudaError_t e = VFB_DISPATCH(level->storage, level->arith,
+                                           LA::box_collide(b, level->is_even_timestep != 0, nullptr, nullptr,
+                                                           as_stream(stream)));
+        return cuda_status(e, "K17CompressibleNavierStokes launch");
+    }
+    return run_k17(level, S.fluid, S.n_fluid, collision_template, S.slots, S.slots_stride, stream);
+}
+
+int vfb_k17_plan_box_addressing(const vfb_k17_plan *plan, int32_t *box_addressing)
+{
+    if (!plan || !box_addressing)
+        return fail(VFB_ERR_INVALID_ARGUMENT, "NULL argument");
+    *box_addressing = plan->S.regular ? 1 : 0;
+    return VFB_OK;
+}
+
+int vfb_k17_plan_destroy(vfb_k17_plan *plan)
+{
+    delete plan;
     return VFB_OK;
 }
 
