@@ -402,3 +402,24 @@ def test_k17_plans_match_the_stateless_entry_point(cuda, periodic, storage, arit
     assert flags == [1 if regular else 0]
     for a, b in zip(*results):
         assert np.array_equal(a, b)
+
+
+def test_box_addressing_needs_every_neighbour_entry_regular(cuda):
+    """One neighbour entry out of the box pattern (still a valid node), or a fluid list with a node
+    left out, keeps the list kernel; the untouched grid takes box addressing."""
+    def flag_of(grid):
+        sim = Simulation(make_para(1.8), grid, BCF())
+        f = C.c_int32()
+        N.check(N.lib().vfb_simulation_level_box_addressing(sim._sim, 0, C.byref(f)))
+        sim.close()
+        return f.value
+
+    g = ListGrid(10, 6, 5, periodic=(True, True, True))
+    assert flag_of(g) == 1
+    k = int(g.fluid[37])
+    bad = ListGrid(10, 6, 5, periodic=(True, True, True))
+    bad.neighbor[2][k] = bad.neighbor[2][int(bad.fluid[38])]      # a wrong +z neighbour
+    assert flag_of(bad) == 0
+    short = ListGrid(10, 6, 5, periodic=(True, True, True))
+    short.fluid = short.fluid[:-1].copy()                          # the last node left out
+    assert flag_of(short) == 0
